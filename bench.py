@@ -1,0 +1,422 @@
+#!/usr/bin/env python
+"""Grains3D DEM time step on B200: particle-steps/s for 1,000,000 polydisperse
+spheres in a triply periodic box (granular-gas cooling), FP32-split vs FP64.
+
+One step = one kick-drift-kick leapfrog step of the whole system: move,
+linked-cell binning (counting sort on the cell key), 27-cell pair search,
+narrow phase, HookeMemory contact force with hashed tangential history,
+per-particle force/torque reduction.  Inputs: the seeded FCC stand-in of the
+1M-sphere configuration (pacific_b200.scenarios.periodic_gas), synthetic.
+
+Multi-GPU: the workload does not shard without a halo exchange, so each rank
+runs an independent replica (weak scaling, no data-path collective); the
+timed region is bracketed by barriers and the max over ranks is reported.
+
+`--impl reference` times the CPU FP64 restatement of the reference's step
+(oracle/) on the host: the reference itself cannot be built here (it needs
+Xerces-C and MPI, neither present).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "particle-steps/s, 1M spheres: FP32-split vs FP64 on one B200, at stated error"
+UNIT = "particle-steps/s"
+
+
+# ------------------------------------------------------------------ clocks --
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.out = None
+
+    def __enter__(self):
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        time.sleep(0.2)
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.out.flush()
+        rows = []
+        for line in Path(self.out.name).read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                rows.append((float(f[1]), float(f[2]), float(f[3]), f[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        # samples under load: power well above idle
+        pmax = max(r[2] for r in rows)
+        load = [r for r in rows if r[2] > 0.5 * pmax] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in load for k in range(4) if r[3][k] == "Active"})
+        return {"sm_mhz": float(np.median([r[0] for r in load])), "sm_max_mhz": rows[0][1],
+                "reasons": reasons, "samples": len(load)}
+
+
+# --------------------------------------------------------------- roofline --
+def algorithmic_bytes(kernel, n, entries, contacts, ncells, fp64):
+    """Compulsory DRAM bytes of one launch of each phase (each input read
+    once, each output written once; neighbour re-reads assumed cache hits)."""
+    if kernel == "move":       # F T v w wbf x q + type inst | x v w wbf q + key rank + count
+        return n * (176 + 8 + 128 + 8 + 4)
+    if kernel == "gather":     # order id type inst key + state | state + ids + cell + compact
+        return n * (148 + 16 + 128 + 16 + (96 if fp64 else 64))
+    if kernel in ("pairs64", "pairs32"):
+        return n * ((32 if fp64 else 16) + 4 + 16 + 4) + 4 * entries + 8 * ncells
+    if kernel in ("forces64", "forces32"):
+        per_p = (96 if fp64 else 64) + 8 + 16 + 4 + 48 + (0 if fp64 else 24)
+        per_c = 2 * (8 + (72 if fp64 else 36))
+        return n * per_p + 4 * entries + contacts * per_c
+    if kernel == "kick":
+        return n * (128 + 4 + 72)
+    if kernel == "place":
+        return n * 16
+    if kernel == "scan":
+        return ncells * 8
+    if kernel == "cellsort":
+        return ncells * 8 + n * 8
+    return None
+
+
+def read_ncu_traffic(kernel):
+    """DRAM bytes per launch from the committed ncu summary, if any."""
+    for p in (ROOT / "profiles").glob("*.md"):
+        for line in p.read_text().splitlines():
+            if line.startswith(f"traffic_bytes_per_launch[{kernel}]:"):
+                try:
+                    return float(line.split(":", 1)[1])
+                except ValueError:
+                    return None
+    return None
+
+
+# ------------------------------------------------------------------ helpers --
+def dist_setup(world):
+    if world <= 1:
+        return None
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    return dist
+
+
+def barrier_sync(dist):
+    import torch
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def max_over_ranks(dist, value):
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def make_system(xml, sc, precision):
+    from pacific_b200 import Grains
+    g = Grains(xml, precision)
+    g.upload_state(sc.type, sc.x, sc.v, sc.w, sc.q)
+    g.do_before_time_stepping()
+    return g
+
+
+def timed_steps(g, dist, steps):
+    barrier_sync(dist)
+    g.step(steps)
+    barrier_sync(dist)
+    return max_over_ranks(dist, g.last_step_ms)
+
+
+def pinned(a):
+    import torch
+    t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+    t.numpy()[...] = a
+    return t
+
+
+def e2e_run(g, dist, steps):
+    """Public-API run with host buffers: the state goes up from pinned host
+    memory, each step reads back max/mean |v| (the per-step result Grains3D
+    writes to *_VelocityMaxMean.dat), the final state comes back down."""
+    s = g.download_state()
+    host = {k: pinned(s[k]) for k in ("x", "v", "w", "q", "F", "T")}
+    outs = {k: pinned(np.zeros_like(s[k])) for k in ("x", "v", "w", "q", "F", "T")}
+    barrier_sync(dist)
+    t0 = time.perf_counter()
+    g.set_state(host["x"].numpy(), host["v"].numpy(), host["w"].numpy(), host["q"].numpy(),
+                host["F"].numpy(), host["T"].numpy())
+    for _ in range(steps):
+        g.step(1)
+        g.velocity_stats()
+    from pacific_b200.grains import _dp, library
+    lib = library()
+    rc = lib.gdem_download_state(g._h, _dp(outs["x"].numpy()), _dp(outs["v"].numpy()),
+                                 _dp(outs["w"].numpy()), None, _dp(outs["q"].numpy()),
+                                 _dp(outs["F"].numpy()), _dp(outs["T"].numpy()))
+    assert rc == 0
+    barrier_sync(dist)
+    dt = max_over_ranks(dist, time.perf_counter() - t0)
+    n = g.n
+    up = n * 8 * (3 + 3 + 3 + 4 + 3 + 3)
+    down = up
+    return dt, up / steps, 16 + down / steps
+
+
+def error_sample(n_fcc, steps_before, precision):
+    """Per-particle force error of one GPU step against the FP64 oracle from
+    the same state (normaliser: the particle's sum of contact-force magnitudes)."""
+    from pacific_b200 import scenarios
+    from tests.helpers import (contact_scale, force_errors, gpu_from_oracle, oracle_for,
+                               radii_of)
+    sc = scenarios.periodic_gas(n_fcc=n_fcc, seed=1236)
+    with tempfile.TemporaryDirectory() as d:
+        xml = str(sc.write_xml(Path(d) / "err.xml"))
+        o = oracle_for(sc, xml)
+        o.init()
+        o.step(steps_before)
+        g = gpu_from_oracle(xml, sc, o, precision)
+        o.step(1)
+        g.step(1)
+        id0, id1, dl, pt, f = o.contacts()
+        scale = contact_scale(sc.n, id0, id1, f)
+        fe, te = force_errors(o.state(), g.download_state(), scale, radii_of(sc))
+        m = scale > 0
+        g.close()
+    return {"force_max": float(fe[m].max()), "force_p99": float(np.percentile(fe[m], 99)),
+            "torque_max": float(te[m].max()), "particles_in_contact": int(m.sum())}
+
+
+def cpu_baseline(sc, xml, budget_s=15.0):
+    """Times the CPU FP64 restatement on a bounded sample of the same workload."""
+    from tests.helpers import oracle_for
+    o = oracle_for(sc, xml)
+    o.init()
+    t0 = time.perf_counter()
+    o.step(1)
+    one = time.perf_counter() - t0
+    k = max(1, min(50, int(budget_s / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    o.step(k)
+    dt = time.perf_counter() - t0
+    o.close()
+    return {"value": sc.n * k / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{k} steps of the full {sc.n}-sphere system after 1 warm-up step "
+                      "(oracle/grains_oracle.cpp, FP64, single thread)"}
+
+
+# --------------------------------------------------------------- reference --
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from pacific_b200 import scenarios
+    from oracle import oracle as orc
+    orc.build()
+    sc = scenarios.periodic_gas(n_fcc=args.n_fcc, seed=1236)
+    with tempfile.TemporaryDirectory() as d:
+        xml = str(sc.write_xml(Path(d) / "gas.xml"))
+        from tests.helpers import oracle_for
+        o = oracle_for(sc, xml)
+        o.init()
+        # each step is a bounded sample: the whole --steps/--warmup run stays
+        # within a few minutes on one core
+        t0 = time.perf_counter()
+        o.step(1)
+        one = time.perf_counter() - t0
+        k = max(1, min(args.steps, int(60.0 / max(one, 1e-6))))
+        w = min(args.warmup, 2)
+        o.step(w)
+        t0 = time.perf_counter()
+        o.step(k)
+        dt = time.perf_counter() - t0
+    value = sc.n * k / dt
+    sample = (f"{k} of the requested {args.steps} steps of the full {sc.n}-sphere system "
+              f"after {1 + w} warm-up steps, CPU FP64 restatement of the reference step, "
+              "1 thread (the reference step is single-threaded per MPI rank)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": k, "warmup": 1 + w, "ms_per_step": 1e3 * dt / k,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": "periodic_gas_1M", "n": sc.n},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------- main --
+def main():
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n-fcc", type=int, default=63)
+    ap.add_argument("--e2e-steps", type=int, default=200)
+    ap.add_argument("--profile-steps", type=int, default=50)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-error", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = dist_setup(world)
+    from pacific_b200 import FP32_SPLIT, FP64, build, scenarios
+    if rank == 0:
+        build.build()
+    if dist is not None:
+        dist.barrier()
+    sc = scenarios.periodic_gas(n_fcc=args.n_fcc, seed=1236 + 1000 * rank)
+    tmp = tempfile.TemporaryDirectory()
+    xml = str(sc.write_xml(Path(tmp.name) / f"gas{rank}.xml"))
+    n = sc.n
+
+    res = {}
+    for name, prec in (("fp64", FP64), ("fp32_split", FP32_SPLIT)):
+        g = make_system(xml, sc, prec)
+        g.step(args.warmup)
+        if name == "fp32_split":
+            with ClockSampler(local) as clk:
+                ms = timed_steps(g, dist, args.steps)
+            clocks = clk.summary()
+        else:
+            ms = timed_steps(g, dist, args.steps)
+        st = g.status()
+        entries, contacts = g.pair_counts()
+        # per-phase device times with CUDA events (plain launches)
+        g.set_profiling(True)
+        g.step(args.profile_steps)
+        kt = g.kernel_times()
+        g.set_profiling(False)
+        res[name] = dict(ms=ms, status=st, entries=entries, contacts=contacts, kt=kt, g=g,
+                         ncells=int(np.prod(g.grid()[0])))
+        if name == "fp64":
+            g.close()
+
+    g = res["fp32_split"]["g"]
+    e2e_dt, h2d, d2h = e2e_run(g, dist, args.e2e_steps)
+    g.close()
+
+    if rank == 0:
+        fp32 = res["fp32_split"]
+        fp64 = res["fp64"]
+        value = world * n * args.steps / (fp32["ms"] * 1e-3)
+        v64 = world * n * args.steps / (fp64["ms"] * 1e-3)
+        # roofline of the dominant kernel of the FP32-split step
+        kt = fp32["kt"]
+        dom = max((k for k in kt if k not in ("cell_clear", "hist_clear")), key=lambda k: kt[k][0])
+        avg_ms = kt[dom][0] / kt[dom][1]
+        ncells = fp32["ncells"]
+        ab = algorithmic_bytes(dom, n, fp32["entries"], fp32["contacts"], ncells, False)
+        peaks = {}
+        pk = ROOT / "MEASURED_PEAKS.json"
+        if pk.exists():
+            peaks = json.loads(pk.read_text())
+        hbm = peaks.get("hbm_gbs")
+        peak_src = "measured" if hbm else "fallback"
+        hbm = hbm or 6650.0
+        achieved = ab / (avg_ms * 1e-3) / 1e9 if ab else None
+        traffic = read_ncu_traffic(dom)
+        phases = {k: {"total_ms": round(v[0], 4), "launches": v[1],
+                      "avg_us": round(1e3 * v[0] / v[1], 2)} for k, v in kt.items()}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": fp32["ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32-split (f64 leapfrog)",
+            "data": "synthetic",
+            "config": {"workload": "periodic_gas_1M", "n": n, "steps_config": 2000,
+                       "dt": sc.dt, "phi": scenarios.solid_fraction(sc),
+                       "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (~0.5 GB of state per replica)"},
+            "fp64": {"value": v64, "ms_per_step": fp64["ms"] / args.steps,
+                     "fp32_split_speedup": value / v64, "status": fp64["status"]},
+            "status": fp32["status"],
+            "pairs": {"directed_entries": fp32["entries"], "contacts": fp32["contacts"]},
+            "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm,
+                         "peak_source": peak_src, "unit": "GB/s",
+                         "frac": (achieved / hbm) if achieved else None,
+                         "algorithmic_bytes_per_launch": ab, "avg_launch_us": 1e3 * avg_ms,
+                         "traffic": traffic},
+            "phases_fp32_split": phases,
+            "phases_fp64": {k: {"total_ms": round(v[0], 4), "launches": v[1],
+                                "avg_us": round(1e3 * v[0] / v[1], 2)}
+                            for k, v in fp64["kt"].items()},
+            "clocks": clocks,
+            "e2e": {"value": world * n * args.e2e_steps / e2e_dt, "unit": UNIT,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": args.e2e_steps},
+            "gpu_launches": None,
+        }
+        # kernels launched in the timed region: per step move, scan(3), place,
+        # cellsort, gather, pairs, forces; plus the closing kick
+        line["gpu_launches"] = args.steps * 9 + 1
+        if not args.no_error:
+            line["error"] = {"sample": "periodic_gas n_fcc=20 (32,000 spheres), one step "
+                                       "after 100 oracle steps, vs the CPU FP64 oracle",
+                             "fp32_split": error_sample(20, 100, FP32_SPLIT),
+                             "fp64": error_sample(20, 100, FP64)}
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(sc, xml)
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    tmp.cleanup()
+
+
+if __name__ == "__main__":
+    main()

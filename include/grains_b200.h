@@ -1,0 +1,153 @@
+/* grains_b200.h -- C ABI of the B200-native Grains3D DEM time step.
+ *
+ * The reference (PacIFiC / Grains3D, GRAINS_V1/Grains) exposes its DEM step
+ * through C++ virtuals and one C ABI for the Basilisk coupling.  The entry
+ * points below replace, for the DEM step only:
+ *   - Grains::Construction / do_before_time_stepping
+ *       (Base/src/Grains.cpp:95-173, 535-1030)            -> gdem_create
+ *   - Grains reload of particle state (Format2024 reload:
+ *       Grains.cpp:784-845, AllComponents.cpp:1024-1290)  -> gdem_upload_*
+ *   - the leapfrog initial force evaluation
+ *       (Grains.cpp:168-173)                              -> gdem_init
+ *   - Grains::Simulation time loop, leapfrog branch
+ *       (Grains.cpp:271-452, 344-364)                     -> gdem_step
+ *   - particle state / contact output (Particle::write2014, Particle.cpp:
+ *       1167-1176; RawDataPostProcessingWriter)            -> gdem_download_*
+ *   - ContactError / MotionError / SimulationError exceptions
+ *       (Base/include/Error.hh:19-151)                    -> status bits
+ * Ownership: device memory belongs to the handle; host arrays belong to the
+ * caller and are not retained.  One host thread per handle.  Every call
+ * returns GDEM_OK (0) or a negative error; gdem_last_error() describes it.
+ */
+#ifndef GRAINS_B200_H
+#define GRAINS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct gdem_system* gdem_handle;
+
+/* precision modes */
+#define GDEM_FP64 0        /* all contact arithmetic in FP64 (reference order) */
+#define GDEM_FP32_SPLIT 1  /* cell + float-pair offsets, FP32 force law, FP64 leapfrog */
+
+/* return codes */
+#define GDEM_OK 0
+#define GDEM_ERR_INVALID (-1)   /* bad argument or XML */
+#define GDEM_ERR_CUDA (-2)      /* CUDA runtime error */
+#define GDEM_ERR_STATE (-3)     /* call out of sequence */
+
+/* simulation status bits (gdem_status): the reference's exceptions */
+#define GDEM_ST_CONTACT_OVERLAP 0x01  /* overlap >= crustA + crustB (ContactError) */
+#define GDEM_ST_MOTION 0x02           /* |dx| > crust in one step (MotionError) */
+#define GDEM_ST_OUT_OF_GRID 0x04      /* particle left the linked cell (SimulationError) */
+#define GDEM_ST_HASH_FULL 0x08        /* contact-history table full */
+#define GDEM_ST_GJK_MAXITER 0x10      /* GJK iteration cap reached */
+#define GDEM_ST_TIMEOUT 0x20          /* a bounded device wait gave up */
+#define GDEM_ST_PAIRS_FULL 0x40       /* per-particle candidate list overflowed */
+
+/* Builds a system from a Grains3D XML input (Construction: LinkedCell,
+ * Origin, Periodicity, Particles, Obstacles, ContactForceModels; Forces:
+ * Gravity; Simulation: TimeStep).  Replaces Grains::Construction
+ * (Base/src/Grains.cpp:535-1030) for the DEM step. */
+int gdem_create(const char* xml_path, int precision, gdem_handle* out);
+
+/* Same, for n independent instances stepped together (one XML each).
+ * Particle IDs are global: instance k owns IDs [base_k, base_k + n_k). */
+int gdem_create_batch(int n, const char* const* xml_paths, int precision, gdem_handle* out);
+
+/* Sets the particles (replaces the insertion / reload of particle state,
+ * Grains.cpp:784-845).  Arrays are indexed by particle ID (0..n-1); inst
+ * may be NULL for a single instance; type is the index of the <Particle>
+ * class within its instance.  x, v, w (space-fixed angular velocity) are
+ * 3 per particle, q is (qx, qy, qz, qw).  wbf (body-fixed angular velocity)
+ * may be NULL: it is then derived as q* w q (ParticleKinematics.cpp:220). */
+int gdem_upload_state(gdem_handle h, int64_t n, const int* inst, const int* type,
+                      const double* x, const double* v, const double* w,
+                      const double* wbf, const double* q);
+
+/* Force and torque of the last evaluation (the Format2024 reload carries
+ * them, SecondOrderLeapFrog.cpp:102-109); marks the leapfrog as started. */
+int gdem_upload_forces(gdem_handle h, const double* F, const double* T);
+
+/* Replaces the whole particle state of an uploaded system (same particle
+ * count) without allocating: x, v, w, q (and optionally wbf) by particle ID
+ * from caller memory (pinned memory gives full-speed copies).  With F and T
+ * the leapfrog continues from them (a reload, Grains.cpp:784-845); without
+ * them gdem_init must run before the next step.  Contact memory is kept. */
+int gdem_set_state(gdem_handle h, const double* x, const double* v, const double* w,
+                   const double* wbf, const double* q, const double* F, const double* T);
+
+/* Maximum and mean translational speed over the particles
+ * (AllComponents::ComputeMaxMeanVelocity, Component/src/AllComponents.cpp:
+ * 1781-1811), the quantity Grains3D writes to *_VelocityMaxMean.dat. */
+int gdem_velocity_stats(gdem_handle h, double* vmax, double* vmean);
+
+/* Per-kernel device timing with CUDA events (replaces the SCT_* phase timers,
+ * Base/include/solvercomputingtime.hh:46-75).  While on, gdem_step uses plain
+ * launches instead of graph replay.  gdem_kernel_times returns, per timed
+ * phase, its name (32 chars each), total milliseconds and launch count. */
+int gdem_set_profiling(gdem_handle h, int on);
+int gdem_kernel_times(gdem_handle h, int capacity, int* count, char* names, double* total_ms,
+                      int64_t* launches);
+
+/* Contact memory entries (Component::m_contactMap, Component.cpp:776-801):
+ * owner particle ID, partner ID (>= 0 particle, -(k+2) wall k of the
+ * owner's instance), kdelta, previous normal, spring torque (3 each). */
+int gdem_upload_history(gdem_handle h, int64_t n, const int* owner, const int* partner,
+                        const double* kdelta, const double* prevn, const double* spring);
+
+/* Leapfrog start (Grains.cpp:168-173): forces at t0, then zero the
+ * cumulative tangential and rolling memories. */
+int gdem_init(gdem_handle h);
+
+/* Advances nsteps kick-drift-kick leapfrog steps of size dt (from the XML).
+ * Equivalent to the loop body of Grains::Simulation (Grains.cpp:286-364). */
+int gdem_step(gdem_handle h, int nsteps);
+
+/* State by particle ID; any pointer may be NULL. */
+int gdem_download_state(gdem_handle h, double* x, double* v, double* w, double* wbf,
+                        double* q, double* F, double* T);
+
+/* Cell (i, j, k) of every particle, in Cell::GetCell numbering
+ * (Base/src/Cell.cpp:172-184), by particle ID. */
+int gdem_download_cells(gdem_handle h, int* ijk);
+
+/* Records overlaps during force evaluation (needed by gdem_download_contacts). */
+int gdem_set_diagnostics(gdem_handle h, int on);
+
+/* Contacts (overlap < 0) of the last force evaluation: *count receives the
+ * number of contacts; when capacity >= *count the arrays are filled with
+ * (id0 < id1) pairs and their overlap distance; walls appear as id1 = -(k+2). */
+int gdem_download_contacts(gdem_handle h, int64_t capacity, int64_t* count, int* id0,
+                           int* id1, double* delta);
+
+/* OR of the status bits raised since creation (or the last reset). */
+int gdem_status(gdem_handle h, int* bits, int reset);
+
+/* Linked-cell grid of instance k: cells per direction, edge, origin. */
+int gdem_grid(gdem_handle h, int k, int* nb, double* edge, double* origin);
+
+/* Sizes of the last force evaluation: directed pair-list entries (each
+ * candidate pair appears once per partner) and live contact-memory entries
+ * (active contacts, particle-particle and particle-wall). */
+int gdem_pair_counts(gdem_handle h, int64_t* entries, int64_t* contacts);
+
+/* Particle count and device time of the last gdem_step in ms. */
+int64_t gdem_num_particles(gdem_handle h);
+double gdem_last_step_ms(gdem_handle h);
+
+/* Runs gdem_step's loop as captured CUDA graphs (1) or plain launches (0). */
+int gdem_use_graphs(gdem_handle h, int on);
+
+const char* gdem_last_error(void);
+void gdem_destroy(gdem_handle h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GRAINS_B200_H */

@@ -1,0 +1,893 @@
+// grains_oracle.cpp -- CPU FP64 restatement of the Grains3D DEM time step.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is the checker that the CUDA path is
+// compared against; the product library never links, loads or calls it.
+// Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use it.
+//
+// It restates, in plain scalar C++ with the reference's own operation order
+// (compiled with -ffp-contract=off so no FMA is introduced), the serial
+// Type="Standard" leapfrog step of Grains3D (GRAINS_V1/Grains):
+//   * Grains::Simulation leapfrog branch        Base/src/Grains.cpp:344-364
+//   * Grains::computeParticlesForceAndTorque    Base/src/Grains.cpp:459-482
+//   * LinkedCell::set (grid sizing)             Base/src/LinkedCell.cpp:47-160
+//   * Cell::GetCell                             Base/src/Cell.cpp:172-184
+//   * Cell::add (push_front)                    Base/src/Cell.cpp:90-93
+//   * LinkedCell::LinkUpdateActiveParticle      Base/src/LinkedCell.cpp:1502-1547
+//   * LinkedCell::setCellContactNeighborhood    Base/src/LinkedCell.cpp:958-984
+//   * LinkedCell::ComputeForces                 Base/src/LinkedCell.cpp:1019-1103
+//   * Particle::InterAction                     Component/src/Particle.cpp:477-545
+//   * SimpleObstacle::InterAction               Component/src/SimpleObstacle.cpp:222-271
+//   * ClosestPointSPHERESPHERE / SPHEREBOX      Geometry/src/RigidBodyWithCrust.cpp:596-721
+//   * Box::IntersectionPointSPHERE & helpers    Geometry/src/Box.cpp:466-800
+//   * HookeMemoryContactForceModel              Component/src/HookeMemoryContactForceModel.cpp:12-249
+//   * Component contact memory map              Component/src/Component.cpp:570-689
+//   * Torsor::addForce                          Component/src/Torsor.cpp:184-189
+//   * SecondOrderLeapFrog::Move/advanceVelocity TimeIntegration/src/SecondOrderLeapFrog.cpp:44-94
+//   * ParticleKinematics::Move/advanceVelocity  Component/src/ParticleKinematics.cpp:62-128
+//   * ParticleKinematicsSphere angular accel    Component/src/ParticleKinematicsSphere.cpp:47-55
+//   * Quaternion ops                            Geometry/src/Quaternion.cpp:74-299,442-472
+//   * Transform::composeLeftByRotation          Geometry/src/Transform.cpp:140-159
+//
+// Periodic boundaries: the reference keeps periodic "clones" (same ID as the
+// master, LinkedCell.cpp:2008-2400) in two extra cell layers; this
+// restatement uses the equivalent minimum-image convention on the same grid
+// (cell indices are reported in the reference's numbering, i.e. with the
+// extra layer, so inner cells are 1..n).  A master that leaves the inner
+// domain is replaced by its clone at x +/- L, which is what the wrap below
+// does.  Forces agree with the clone formulation up to the rounding of the
+// periodic translation.
+//
+// Scope: spheres + axis-aligned box walls (the obstacle type of the north-star
+// configurations), HookeMemory (with rolling-friction memory), fluid-free
+// (coupling factor 1).
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <list>
+#include <map>
+#include <tuple>
+#include <vector>
+#include <algorithm>
+
+namespace {
+
+const double PI = 3.14159265358979323846;   // Basic.hh:22
+const double EPSILON = 1.0e-10;              // Basic.hh:26
+
+// ---------------------------------------------------------------- vectors --
+struct V3 {
+  double c[3];
+  V3() { c[0] = c[1] = c[2] = 0.; }
+  V3(double x, double y, double z) { c[0] = x; c[1] = y; c[2] = z; }
+  double& operator[](int i) { return c[i]; }
+  double operator[](int i) const { return c[i]; }
+};
+inline V3 operator+(V3 const& a, V3 const& b) { return V3(a[0]+b[0], a[1]+b[1], a[2]+b[2]); }
+inline V3 operator-(V3 const& a, V3 const& b) { return V3(a[0]-b[0], a[1]-b[1], a[2]-b[2]); }
+inline V3 operator-(V3 const& a) { return V3(-a[0], -a[1], -a[2]); }
+inline V3 operator*(V3 const& a, double d) { return V3(a[0]*d, a[1]*d, a[2]*d); }
+inline V3 operator*(double d, V3 const& a) { return V3(a[0]*d, a[1]*d, a[2]*d); }
+inline V3 operator/(V3 const& a, double d) { return V3(a[0]/d, a[1]/d, a[2]/d); }
+inline double dot(V3 const& a, V3 const& b) { return a[0]*b[0] + a[1]*b[1] + a[2]*b[2]; }
+// Vector3::operator^ (Geometry/src/Vector3.cpp:114-119)
+inline V3 cross(V3 const& a, V3 const& b) {
+  return V3(a[1]*b[2] - a[2]*b[1], - a[0]*b[2] + a[2]*b[0], a[0]*b[1] - a[1]*b[0]);
+}
+inline double norm(V3 const& a) { return std::sqrt(a[0]*a[0] + a[1]*a[1] + a[2]*a[2]); }
+// Group3::round (Geometry/src/Group3.cpp:390-395), default tol EPSILON
+inline void round3(V3& a) {
+  for (int i = 0; i < 3; ++i) a[i] = std::fabs(a[i]) < EPSILON ? 0. : a[i];
+}
+inline V3& operator+=(V3& a, V3 const& b) { a[0] += b[0]; a[1] += b[1]; a[2] += b[2]; return a; }
+inline V3& operator-=(V3& a, V3 const& b) { a[0] -= b[0]; a[1] -= b[1]; a[2] -= b[2]; return a; }
+
+// ------------------------------------------------------------ quaternions --
+struct Q { V3 v; double w; };   // [w, v]
+inline Q qmake(V3 const& v, double w) { Q q; q.v = v; q.w = w; return q; }
+inline Q conj(Q const& q) { return qmake(-q.v, q.w); }
+// Quaternion::operator* (Quaternion.cpp:442-448)
+inline Q qmul(Q const& a, Q const& b) {
+  double tmp = (a.w * b.w) - dot(a.v, b.v);
+  V3 vt = (cross(a.v, b.v) + (a.w * b.v)) + (b.w * a.v);
+  return qmake(vt, tmp);
+}
+// operator,(Vector3 lhs, Quaternion q) -> q.multLeftVec(lhs) (Quaternion.cpp:93-98,468-472)
+inline Q vecq(V3 const& lhs, Q const& q) {
+  double tmp = dot(-lhs, q.v);
+  V3 vt = cross(lhs, q.v) + (lhs * q.w);
+  return qmake(vt, tmp);
+}
+// Quaternion::multToVector3 (Quaternion.cpp:108-113)
+inline V3 multToVector3(Q const& a, Q const& rhs) {
+  return (cross(a.v, rhs.v) + (a.w * rhs.v)) + (rhs.w * a.v);
+}
+inline double qnorm(Q const& q) {
+  return std::sqrt(q.v[0]*q.v[0] + q.v[1]*q.v[1] + q.v[2]*q.v[2] + q.w*q.w);
+}
+// Quaternion::setRotFromTwoVectors (Quaternion.cpp:263-288)
+inline Q rotFromTwoVectors(V3 const& u, V3 const& v) {
+  double nn = std::sqrt(dot(u, u) * dot(v, v));
+  double real = nn + dot(u, v);
+  V3 vect;
+  if (real < 1.e-6 * nn) {
+    real = 0.;
+    vect = std::fabs(u[0]) > std::fabs(u[2]) ? V3(-u[1], u[0], 0.) : V3(0., -u[2], u[1]);
+  } else {
+    vect = cross(u, v);
+  }
+  Q qq = qmake(vect, real);
+  double s = 1. / qnorm(qq);
+  return qmake(qq.v * s, qq.w * s);
+}
+// Quaternion::rotateVector (Quaternion.cpp:293-299)
+inline V3 rotateVector(Q const& q, V3 const& v) {
+  double nv = norm(q.v);
+  return ((q.w * q.w - nv * nv) * v + (2. * dot(v, q.v)) * q.v) + (2. * q.w) * cross(q.v, v);
+}
+
+// ---------------------------------------------------------------- system ---
+struct Hist {                 // tuple<bool, kdelta, prev_normal, cumulSpringTorque>
+  bool active;
+  V3 kdelta, prevn, spring;
+};
+typedef std::tuple<int, int, int> Key;
+
+struct Model {
+  double kn, en, etat, muc, kt, mur, etarpf, epst;
+  double beta;
+  bool rolling;
+};
+
+struct Particle {
+  int id, type;
+  double radius, crust, mass, inertia, density, eqrad;
+  int matbit;
+  V3 weight;
+  V3 x, v, w, wbf;
+  Q q;
+  double basis[9];
+  V3 F, T, ref;
+  int cell[3];
+  int cellnum;
+  std::map<Key, Hist> cmap;
+};
+
+struct Wall {
+  int id;
+  V3 centre, extent;    // half lengths
+  double crust;
+  int matbit;
+};
+
+struct ContactRec {
+  int id0, id1;          // id1 < 0 : wall k as -(k+2)
+  double delta;
+  V3 point, overlap, force;
+};
+
+}  // namespace
+
+extern "C" {
+
+// Configuration passed by the test harness.  Field meanings follow the
+// Grains3D XML (Construction/LinkedCell, Origin, Periodicity, Particles,
+// Obstacles, ContactForceModels, Forces/Gravity, Simulation/TimeStep).
+typedef struct {
+  double origin[3];
+  double maxc[3];
+  int periodic[3];
+  double cell_size_factor;
+  double gravity[3];
+  double dt;
+  int n_types;
+  const double* type_radius;
+  const double* type_crust;
+  const double* type_density;
+  const int* type_matbit;
+  int n_walls;
+  const double* wall_centre;   // 3 per wall
+  const double* wall_extent;   // 3 per wall (half lengths)
+  const double* wall_crust;
+  const int* wall_matbit;
+  int n_models;
+  const int* model_mask;
+  const double* model_params;  // kn en etat muc kt mur etarpf epst
+} or_config;
+
+enum { OR_OK = 0, OR_ERR_CONTACT = 1, OR_ERR_MOTION = 2, OR_ERR_OUT_OF_GRID = 4 };
+
+}  // extern "C"
+
+namespace {
+
+struct System {
+  // grid
+  double dom_origin[3], dom_size[3];
+  int periodic[3];
+  int nb[3];
+  double edge[3];
+  double lc_origin[3];
+  std::vector<std::list<int>> cells;
+  std::vector<int> nbr_order;      // the 13 half-stencil offsets, in list order
+  double gravity[3], dt;
+  std::vector<Particle> parts;     // active list order == insertion order
+  std::vector<Wall> walls;
+  std::map<int, Model> models;
+  std::vector<double> type_radius, type_crust, type_density;
+  std::vector<int> type_matbit;
+  std::vector<ContactRec> contacts;
+  int err = 0;
+  double time = 0.;
+
+  int cellnum(int i, int j, int k) const { return j * nb[2] * nb[0] + k * nb[0] + i; }
+  bool valid(int i, int j, int k) const {
+    return -1 < i && i < nb[0] && -1 < j && j < nb[1] && -1 < k && k < nb[2];
+  }
+  void getCell(V3 const& p, int* id) const {   // Cell::GetCell
+    for (int d = 0; d < 3; ++d) id[d] = int(std::floor((p[d] - lc_origin[d]) / edge[d]));
+  }
+  Model const& model(int ma, int mb) const {
+    auto it = models.find(ma | mb);
+    return it->second;
+  }
+};
+
+const int STENCIL[3][13] = {{-1,  0, +1, +1, -1,  0, +1, -1,  0, +1, -1,  0, +1},
+                            { 0,  0,  0,  0, +1, +1, +1, +1, +1, +1, +1, +1, +1},
+                            {+1, +1, +1,  0, +1, +1, +1,  0,  0,  0, -1, -1, -1}};
+
+// LinkedCell::set (LinkedCell.cpp:47-160) with cellsize = 2 * factor * maxR
+// (Grains.cpp:1005-1022, 2522-2526)
+void setGrid(System& s, double cellsize) {
+  for (int d = 0; d < 3; ++d) {
+    int n = (int)((s.dom_size[d] + EPSILON) / cellsize);
+    if (!n) n = 1;
+    s.nb[d] = n;
+    s.edge[d] = s.dom_size[d] / n;
+    s.lc_origin[d] = s.dom_origin[d];
+  }
+  for (int d = 0; d < 3; ++d)
+    if (s.periodic[d]) {
+      s.lc_origin[d] += -s.edge[d];      // Point3::Move( -edge ) : += (-edge)
+      s.nb[d] += 2;
+    }
+  s.cells.assign((size_t)s.nb[0] * s.nb[1] * s.nb[2], std::list<int>());
+  // m_neighborsContact is filled with push_front: reverse order of STENCIL
+  s.nbr_order.clear();
+  for (int j = 12; j >= 0; --j) s.nbr_order.push_back(j);
+}
+
+// Periodic wrap: inner cells are 1..n-2 in a periodic direction.
+void wrapPeriodic(System& s, Particle& p) {
+  for (int d = 0; d < 3; ++d) {
+    if (!s.periodic[d]) continue;
+    int id[3];
+    s.getCell(p.x, id);
+    if (id[d] < 1) p.x[d] = p.x[d] + s.dom_size[d];
+    else if (id[d] > s.nb[d] - 2) p.x[d] = p.x[d] + (-s.dom_size[d]);
+  }
+}
+
+// Cell index of a (possibly periodic) neighbour cell; returns -1 when absent.
+// In a periodic direction the clone layer (0 or n-1) maps to the inner cell
+// holding the master, and the returned shift is the image translation.
+int neighbourCell(System const& s, int i, int j, int k, int* shift) {
+  int c[3] = {i, j, k};
+  for (int d = 0; d < 3; ++d) {
+    shift[d] = 0;
+    if (s.periodic[d]) {
+      int nin = s.nb[d] - 2;
+      if (c[d] < 1) { c[d] += nin; shift[d] = -1; }
+      else if (c[d] > nin) { c[d] -= nin; shift[d] = +1; }
+    }
+  }
+  if (!s.valid(c[0], c[1], c[2])) return -1;
+  return s.cellnum(c[0], c[1], c[2]);
+}
+
+// -------------------------------------------------------------- kinematics --
+// ParticleKinematicsSphere::computeAngularAccelerationBodyFixed
+inline V3 dOmega(Particle const& p, V3 const& tbf) {
+  double c = 1.;
+  return V3(tbf[0] / (c * p.inertia), tbf[1] / (c * p.inertia), tbf[2] / (c * p.inertia));
+}
+
+// ParticleKinematics::Move (ParticleKinematics.cpp:62-104); returns |dx|
+double moveParticle(Particle& p, double h, double dt) {
+  Q pc = conj(p.q);
+  V3 tbf = multToVector3(pc, vecq(p.T, p.q));
+  double c = 1.;
+  p.v += (p.F / (p.mass * c)) * h;
+  V3 dx = p.v * dt;
+  V3 K1 = dOmega(p, tbf); K1 = K1 * h;
+  V3 K2 = dOmega(p, tbf); K2 = K2 * h;
+  V3 K3 = dOmega(p, tbf); K3 = K3 * h;
+  p.wbf += ((K1 + K2) + 4. * K3) / 6.;
+  V3 meanw = p.wbf;
+  p.w = multToVector3(p.q, vecq(p.wbf, pc));
+  meanw = multToVector3(p.q, vecq(meanw, pc));
+  p.x += dx;                                      // composeLeftByTranslation
+  double nOmega = norm(meanw);
+  Q qdt;
+  if (nOmega > EPSILON) {
+    double cc = std::cos(nOmega * dt / 2.);
+    double ss = std::sin(nOmega * dt / 2.);
+    V3 t = (ss * 1. / nOmega) * meanw;
+    qdt = qmake(t, cc);
+  } else {
+    qdt = qmake(V3(0., 0., 0.), 1.);
+  }
+  p.q = qmul(qdt, p.q);
+  // Transform::composeLeftByRotation (Transform.cpp:140-159)
+  double* mm = p.basis;
+  double qx = qdt.v[0], qy = qdt.v[1], qz = qdt.v[2], qw = qdt.w;
+  double out[9];
+  for (int i = 0; i < 3; ++i) {
+    double px = qy * mm[6 + i] - qz * mm[3 + i] + qw * mm[0 + i];
+    double py = qz * mm[0 + i] - qx * mm[6 + i] + qw * mm[3 + i];
+    double pz = qx * mm[3 + i] - qy * mm[0 + i] + qw * mm[6 + i];
+    double pw = - qx * mm[0 + i] - qy * mm[3 + i] - qz * mm[6 + i];
+    out[0 + i] = qy * pz - qz * py - pw * qx + qw * px;
+    out[3 + i] = qz * px - qx * pz - pw * qy + qw * py;
+    out[6 + i] = qx * py - qy * px - pw * qz + qw * pz;
+  }
+  std::memcpy(p.basis, out, sizeof(out));
+  return norm(dx);
+}
+
+// ParticleKinematics::advanceVelocity (ParticleKinematics.cpp:110-128)
+void advanceVelocity(Particle& p, double h) {
+  Q pc = conj(p.q);
+  V3 tbf = multToVector3(pc, vecq(p.T, p.q));
+  double c = 1.;
+  p.v += (p.F / (p.mass * c)) * h;
+  V3 K1 = dOmega(p, tbf); K1 = K1 * h;
+  V3 K2 = dOmega(p, tbf); K2 = K2 * h;
+  V3 K3 = dOmega(p, tbf); K3 = K3 * h;
+  p.wbf += ((K1 + K2) + 4. * K3) / 6.;
+  p.w = multToVector3(p.q, vecq(p.wbf, pc));
+}
+
+// ------------------------------------------------------------ narrow phase --
+struct PointContact {
+  V3 point, overlap;
+  double dist;
+  bool contact;
+};
+
+// ClosestPointSPHERESPHERE (RigidBodyWithCrust.cpp:596-639).  xb is the
+// image position of B.  Sets *err when -distance >= crustA + crustB; the
+// reference then retries with a 10x crust shrink (RigidBodyWithCrust.cpp:
+// 534-588), which for spheres imposes an overlap of crustA + crustB along the
+// centre line and places the contact at the midpoint of the shrunk spheres'
+// witness points.
+PointContact sphereSphere(Particle const& a, V3 const& xb, Particle const& b, int* err) {
+  PointContact pc;
+  V3 AB = xb - a.x;
+  double rA = a.radius, rB = b.radius;
+  double distance = norm(AB) - (rA + rB);
+  if (distance > 0.) { pc.contact = false; pc.dist = distance; return pc; }
+  if (-distance >= a.crust + b.crust) {
+    *err |= OR_ERR_CONTACT;
+    auto shrunk = [](double r, double crust) {
+      double s = (r - 10. * crust) / r;   // getTransformWithCrust(factor, 0.5)
+      return r * (s > 0.5 ? s : 0.5);
+    };
+    double ra = shrunk(rA, a.crust), rb = shrunk(rB, b.crust);
+    double nAB = norm(AB);
+    V3 u = AB / nAB;
+    V3 pA = a.x + ra * u, pB = xb - rb * u;
+    V3 ba = pA - pB;
+    ba = ba / norm(ba);
+    double imp = 1. * (a.crust + b.crust);
+    pc.point = pA / 2.0 + pB / 2.0;
+    pc.overlap = imp * ba;
+    pc.dist = -imp;
+    pc.contact = true;
+    return pc;
+  }
+  double nAB = norm(AB);
+  pc.point = a.x + ((rA + 0.5 * distance) * AB) / nAB;
+  pc.overlap = distance * (AB / nAB);
+  pc.dist = distance;
+  pc.contact = true;
+  return pc;
+}
+
+// Box::ContactCornerSPHERE / ContactEdgeSPHERE (Box.cpp)
+V3 cornerOf(V3 const& e, int n) {
+  // m_corners numbering of Box (Box.cpp constructor): 0:(-,-,-) 1:(+,-,-)
+  // 2:(+,-,+) 3:(-,-,+) 4:(-,+,-) 5:(+,+,-) 6:(+,+,+) 7:(-,+,+)
+  static const int sg[8][3] = {{-1,-1,-1},{1,-1,-1},{1,-1,1},{-1,-1,1},
+                               {-1,1,-1},{1,1,-1},{1,1,1},{-1,1,1}};
+  return V3(sg[n][0] * e[0], sg[n][1] * e[1], sg[n][2] * e[2]);
+}
+V3 contactCorner(V3 const& e, V3 const& c, double r, int n, double& ov) {
+  V3 cp;
+  V3 dist = c - cornerOf(e, n);
+  double nd = norm(dist);
+  if (nd < r) { ov = nd - r; cp = c - (1. + 0.5 * ov / nd) * dist; }
+  return cp;
+}
+V3 contactEdge(V3 const& e, V3 const& c, double r, int n, int dir, double& ov) {
+  V3 cp, proj = c;
+  V3 cn = cornerOf(e, n);
+  proj[dir] = cn[dir];
+  V3 dist = proj - cn;
+  double nd = norm(dist);
+  if (nd < r) { ov = nd - r; cp = c - (1. + 0.5 * ov / nd) * dist; }
+  return cp;
+}
+// Box::IntersectionPointSPHERE (Box.cpp:466-676); e = half extents
+V3 boxSphere(V3 const& e, V3 const& c, double r, double& ov) {
+  V3 cp;
+  double gx = c[0], gy = c[1], gz = c[2];
+  ov = 1.;
+  const int X = 0, Y = 1, Z = 2;
+  if (gx > e[X]) {
+    if (gy > e[Y]) {
+      if (gz > e[Z]) cp = contactCorner(e, c, r, 6, ov);
+      else if (gz < -e[Z]) cp = contactCorner(e, c, r, 5, ov);
+      else cp = contactEdge(e, c, r, 5, Z, ov);
+    } else if (gy < -e[Y]) {
+      if (gz > e[Z]) cp = contactCorner(e, c, r, 2, ov);
+      else if (gz < -e[Z]) cp = contactCorner(e, c, r, 1, ov);
+      else cp = contactEdge(e, c, r, 1, Z, ov);
+    } else {
+      if (gz > e[Z]) cp = contactEdge(e, c, r, 6, Y, ov);
+      else if (gz < -e[Z]) cp = contactEdge(e, c, r, 1, Y, ov);
+      else {
+        double nd = gx - e[X];
+        if (nd < r) { ov = nd - r; cp = V3(e[X] + 0.5 * ov, c[Y], c[Z]); }
+      }
+    }
+  } else if (gx < -e[X]) {
+    if (gy > e[Y]) {
+      if (gz > e[Z]) cp = contactCorner(e, c, r, 7, ov);
+      else if (gz < -e[Z]) cp = contactCorner(e, c, r, 4, ov);
+      else cp = contactEdge(e, c, r, 4, Z, ov);
+    } else if (gy < -e[Y]) {
+      if (gz > e[Z]) cp = contactCorner(e, c, r, 3, ov);
+      else if (gz < -e[Z]) cp = contactCorner(e, c, r, 0, ov);
+      else cp = contactEdge(e, c, r, 0, Z, ov);
+    } else {
+      if (gz > e[Z]) cp = contactEdge(e, c, r, 3, Y, ov);
+      else if (gz < -e[Z]) cp = contactEdge(e, c, r, 0, Y, ov);
+      else {
+        double nd = -e[X] - gx;
+        if (nd < r) { ov = nd - r; cp = V3(-e[X] - 0.5 * ov, c[Y], c[Z]); }
+      }
+    }
+  } else {
+    if (gy > e[Y]) {
+      if (gz > e[Z]) cp = contactEdge(e, c, r, 6, X, ov);
+      else if (gz < -e[Z]) cp = contactEdge(e, c, r, 4, X, ov);
+      else {
+        double nd = gy - e[Y];
+        if (nd < r) { ov = nd - r; cp = V3(c[X], e[Y] + 0.5 * ov, c[Z]); }
+      }
+    } else if (gy < -e[Y]) {
+      if (gz > e[Z]) cp = contactEdge(e, c, r, 3, X, ov);
+      else if (gz < -e[Z]) cp = contactEdge(e, c, r, 0, X, ov);
+      else {
+        double nd = -e[Y] - gy;
+        if (nd < r) { ov = nd - r; cp = V3(c[X], -e[Y] - 0.5 * ov, c[Z]); }
+      }
+    } else {
+      if (gz > e[Z]) {
+        double nd = gz - e[Z];
+        if (nd < r) { ov = nd - r; cp = V3(c[X], c[Y], e[Z] + 0.5 * ov); }
+      } else if (gz < -e[Z]) {
+        double nd = -e[Z] - gz;
+        if (nd < r) { ov = nd - r; cp = V3(c[X], c[Y], -e[Z] - 0.5 * ov); }
+      } else {
+        ov = -10000.;
+      }
+    }
+  }
+  return cp;
+}
+
+// ClosestPointSPHEREBOX, sphere first (RigidBodyWithCrust.cpp:647-689).
+// Walls are axis aligned: the inverse transform is p - centre and the direct
+// transform is p + centre (Transform.cpp:71-77, 312-317 with identity basis).
+PointContact sphereWall(Particle const& a, Wall const& w, int* err) {
+  PointContact pc;
+  pc.contact = false;
+  V3 local = a.x - w.centre;
+  double ov = 0.;
+  V3 cpl = boxSphere(w.extent, local, a.radius, ov);
+  pc.dist = ov;
+  if (ov < 0.) {
+    if (-ov >= a.crust + w.crust) {
+      *err |= OR_ERR_CONTACT;
+      return pc;   // the reference falls back to GJK on shrunk bodies
+    }
+    V3 contact = cpl + w.centre;
+    V3 AB = contact - a.x;
+    pc.point = contact;
+    pc.overlap = (ov / norm(AB)) * AB;
+    pc.contact = true;
+  }
+  return pc;
+}
+
+// ------------------------------------------------------------ force model --
+// HookeMemoryContactForceModel::computeTangentialVector (:54-65)
+V3 tangentVector(Model const& m, double n_t, V3 const& ut, V3 const& kdelta) {
+  if (norm(ut) > 0.001) return (-ut) / norm(ut);
+  V3 s = kdelta + n_t * ut;
+  if ((norm(kdelta) > m.epst || norm(n_t * ut) > m.epst) && norm(s) > m.epst)
+    return (-s) / norm(s);
+  return V3(0., 0., 0.);
+}
+
+struct Body {      // view of p0 / p1 as the force model sees them
+  V3 x, v, w;
+  double mass, rad;
+  std::map<Key, Hist>* cmap;
+  int id;
+};
+
+// performForcesCalculus (:72-193) + computeForces (:200-249)
+void hookeMemory(Model const& m, Body& p0, Body& p1, double dt, PointContact const& ci,
+                 V3& fOn0, V3& mOn0) {
+  V3 pcp = ci.point;
+  V3 pen = ci.overlap;
+  Key id0 = std::make_tuple(1, p1.id, 1);
+  Key id1 = std::make_tuple(1, p0.id, 1);
+  V3 normal = pen;
+  normal = normal / norm(normal);
+  round3(normal);
+  V3 v0 = p0.v + cross(p0.w, pcp - p0.x);
+  V3 v1 = p1.v + cross(p1.w, pcp - p1.x);
+  V3 tmpV = v0 - v1;
+  V3 v_n = normal * dot(tmpV, normal);
+  V3 v_t = tmpV - v_n;
+  V3 delFN = m.kn * pen;
+  double avmass = 1. / (1. / p0.mass + 1. / p1.mass);
+  double gamman = -2. * m.beta * std::sqrt(avmass * m.kn);
+  delFN -= gamman * v_n;
+  double normFN = norm(delFN);
+  double etat = m.etat == -1. ? -m.beta * std::sqrt(m.kn / avmass) : m.etat;
+  double gammat = 2. * etat * avmass;
+  V3 viscousFT = -gammat * v_t;
+  // Component::getContactMemory (Component.cpp:634-670)
+  bool existed;
+  auto it = p0.cmap->find(id0);
+  if (it != p0.cmap->end()) { existed = true; it->second.active = true; }
+  else {
+    existed = false;
+    Hist h; h.active = true;
+    it = p0.cmap->insert(std::make_pair(id0, h)).first;
+  }
+  Hist& H = it->second;
+  Q qrot = qmake(V3(0., 0., 0.), 0.);
+  if (existed) {
+    qrot = rotFromTwoVectors(H.prevn, normal);
+    H.kdelta = rotateVector(qrot, H.kdelta);
+  }
+  H.kdelta += (dt * m.kt) * v_t;
+  H.prevn = normal;
+  V3 tij = tangentVector(m, gammat, v_t, H.kdelta);
+  double normFT = norm(-H.kdelta + viscousFT);
+  V3 delFT;
+  if (normFT <= m.muc * normFN) delFT = norm(-H.kdelta + viscousFT) * tij;
+  else {
+    if (m.kt) H.kdelta = ((-m.muc * normFN) * tij + viscousFT) / m.kt;
+    delFT = (m.muc * normFN) * tij;
+  }
+  V3 delM;
+  if (m.rolling) {
+    double Req = 1. / (1. / p0.rad + 1. / p1.rad);
+    double kr = 3. * m.kn * m.mur * m.mur * Req * Req;
+    double etar = 3. * gamman * m.mur * m.mur * Req * Req;
+    double maxM = m.mur * Req * normFN;
+    V3 wrel = p0.w - p1.w;
+    if (existed) H.spring = rotateVector(qrot, H.spring);
+    H.spring -= (kr * dt) * wrel;
+    double nM = norm(H.spring);
+    if (nM > maxM) H.spring = H.spring * (maxM / nM);
+    delM = H.spring - (m.etarpf * etar) * wrel;
+  }
+  // Component::addDeplContactInMap on p1 (Component.cpp:677-689)
+  if (p1.cmap) {
+    Hist& H1 = (*p1.cmap)[id1];
+    H1.active = true;
+    H1.kdelta = -H.kdelta;
+    H1.prevn = -normal;
+    H1.spring = -H.spring;
+  }
+  fOn0 = 1. * (delFN + delFT);
+  mOn0 = delM;
+}
+
+void addForce(Particle& p, V3 const& point, V3 const& f) {   // Torsor::addForce
+  p.F += f;
+  V3 a = point - p.ref;
+  p.T += cross(a, f);
+}
+
+// Particle::InterAction + HookeMemory::computeForces for a particle pair
+void interactPP(System& s, Particle& p0, Particle& p1, V3 const& shift) {
+  V3 xb = p1.x + shift;
+  PointContact pc = sphereSphere(p0, xb, p1, &s.err);
+  if (!pc.contact || !(pc.dist < 0.)) return;
+  Model const& m = s.model(p0.matbit, p1.matbit);
+  Body b0{p0.x, p0.v, p0.w, p0.mass, p0.eqrad, &p0.cmap, p0.id};
+  Body b1{xb, p1.v, p1.w, p1.mass, p1.eqrad, &p1.cmap, p1.id};
+  V3 f, mm;
+  hookeMemory(m, b0, b1, s.dt, pc, f, mm);
+  addForce(p0, pc.point, f);
+  if (m.rolling) p0.T += mm;
+  // p1 torque lever arm uses its own (image) reference point
+  V3 fm = (-f);
+  p1.F += fm;
+  V3 arm = pc.point - (p1.ref + shift);
+  p1.T += cross(arm, fm);
+  if (m.rolling) p1.T += (-mm);
+  ContactRec r{p0.id, p1.id, pc.dist, pc.point, pc.overlap, f};
+  s.contacts.push_back(r);
+}
+
+// SimpleObstacle::InterAction: the particle is p0, the wall p1
+void interactPW(System& s, Particle& p, Wall& w, int k) {
+  PointContact pc = sphereWall(p, w, &s.err);
+  if (!pc.contact || !(pc.dist < 0.)) return;
+  Model const& m = s.model(p.matbit, w.matbit);
+  Body b0{p.x, p.v, p.w, p.mass, p.eqrad, &p.cmap, p.id};
+  Body b1{V3(), V3(), V3(), 1.e20, 0., nullptr, w.id};   // Component::m_massObstacle
+  // Component::getEquivalentSphereRadius (Component.cpp:205-208) of the box
+  b1.x = w.centre;
+  b1.rad = std::pow((0.75 / PI) * (8. * w.extent[0] * w.extent[1] * w.extent[2]), 1. / 3.);
+  V3 f, mm;
+  hookeMemory(m, b0, b1, s.dt, pc, f, mm);
+  addForce(p, pc.point, f);
+  if (m.rolling) p.T += mm;
+  ContactRec r{p.id, w.id, pc.dist, pc.point, pc.overlap, f};
+  s.contacts.push_back(r);
+}
+
+// Grains::computeParticlesForceAndTorque + LinkedCell::ComputeForces
+void computeForces(System& s) {
+  s.contacts.clear();
+  for (auto& p : s.parts)
+    for (auto& kv : p.cmap) kv.second.active = false;    // setContactMapToFalse
+  for (auto& p : s.parts) {                              // InitializeForce
+    p.F = p.weight;
+    p.T = V3(0., 0., 0.);
+    p.ref = p.x;
+  }
+  std::vector<int> nbrs;
+  std::vector<V3> shifts;
+  for (size_t ip = 0; ip < s.parts.size(); ++ip) {
+    Particle& p = s.parts[ip];
+    int id[3];
+    s.getCell(p.x, id);
+    int cn = s.cellnum(id[0], id[1], id[2]);
+    nbrs.clear(); shifts.clear();
+    std::list<int>& own = s.cells[cn];
+    auto it = std::find(own.begin(), own.end(), p.id);
+    for (++it; it != own.end(); ++it) { nbrs.push_back(*it); shifts.push_back(V3()); }
+    for (int jn : s.nbr_order) {
+      int sh[3];
+      int c = neighbourCell(s, id[0] + STENCIL[0][jn], id[1] + STENCIL[1][jn],
+                            id[2] + STENCIL[2][jn], sh);
+      if (c < 0) continue;
+      V3 shift(sh[0] * s.dom_size[0], sh[1] * s.dom_size[1], sh[2] * s.dom_size[2]);
+      for (int q : s.cells[c]) { nbrs.push_back(q); shifts.push_back(shift); }
+    }
+    for (size_t n = 0; n < nbrs.size(); ++n)
+      if (nbrs[n] != p.id) interactPP(s, p, s.parts[nbrs[n]], shifts[n]);
+    for (size_t k = 0; k < s.walls.size(); ++k) interactPW(s, p, s.walls[k], (int)k);
+  }
+  for (auto& p : s.parts) {                              // updateContactMap
+    for (auto it = p.cmap.begin(); it != p.cmap.end();) {
+      if (!it->second.active) it = p.cmap.erase(it); else ++it;
+    }
+  }
+}
+
+// LinkedCell::LinkUpdateActiveParticle
+void linkUpdate(System& s) {
+  for (auto& p : s.parts) {
+    int id[3];
+    s.getCell(p.x, id);
+    if (!s.valid(id[0], id[1], id[2])) { s.err |= OR_ERR_OUT_OF_GRID; continue; }
+    int cn = s.cellnum(id[0], id[1], id[2]);
+    if (cn != p.cellnum) {
+      s.cells[cn].push_front(p.id);
+      s.cells[p.cellnum].remove(p.id);
+      p.cellnum = cn;
+    }
+    p.cell[0] = id[0]; p.cell[1] = id[1]; p.cell[2] = id[2];
+  }
+}
+
+void step(System& s) {
+  double dt = s.dt;
+  s.time += dt;
+  for (auto& p : s.parts) {
+    double depl = moveParticle(p, 0.5 * dt, dt);
+    if (depl > p.crust) s.err |= OR_ERR_MOTION;
+    wrapPeriodic(s, p);
+  }
+  linkUpdate(s);
+  computeForces(s);
+  for (auto& p : s.parts) advanceVelocity(p, 0.5 * dt);
+}
+
+}  // namespace
+
+extern "C" {
+
+void* or_create(or_config const* c) {
+  System* s = new System();
+  for (int d = 0; d < 3; ++d) {
+    s->dom_origin[d] = c->origin[d];
+    s->dom_size[d] = c->maxc[d] - c->origin[d];   // App::set_dimensions
+    s->periodic[d] = c->periodic[d] ? 1 : 0;
+    s->gravity[d] = c->gravity[d];
+  }
+  s->dt = c->dt;
+  for (int t = 0; t < c->n_types; ++t) {
+    s->type_radius.push_back(c->type_radius[t]);
+    s->type_crust.push_back(c->type_crust[t]);
+    s->type_density.push_back(c->type_density[t]);
+    s->type_matbit.push_back(c->type_matbit[t]);
+  }
+  for (int k = 0; k < c->n_walls; ++k) {
+    Wall w;
+    w.id = -(k + 2);
+    w.centre = V3(c->wall_centre[3*k], c->wall_centre[3*k+1], c->wall_centre[3*k+2]);
+    w.extent = V3(c->wall_extent[3*k], c->wall_extent[3*k+1], c->wall_extent[3*k+2]);
+    w.crust = c->wall_crust[k];
+    w.matbit = c->wall_matbit[k];
+    s->walls.push_back(w);
+  }
+  for (int k = 0; k < c->n_models; ++k) {
+    const double* q = c->model_params + 8 * k;
+    Model m;
+    m.kn = q[0]; m.en = q[1]; m.etat = q[2]; m.muc = q[3];
+    m.kt = q[4]; m.mur = q[5]; m.etarpf = q[6]; m.epst = q[7];
+    m.rolling = m.mur != 0.;
+    m.beta = std::log(m.en) / std::sqrt(PI * PI + std::log(m.en) * std::log(m.en));
+    s->models[c->model_mask[k]] = m;
+  }
+  double maxR = 0.;
+  for (double r : s->type_radius) maxR = std::max(maxR, r);
+  double coef = c->cell_size_factor < 1. ? 1. : c->cell_size_factor;
+  setGrid(*s, 2. * (coef * maxR));
+  return s;
+}
+
+void or_destroy(void* h) { delete static_cast<System*>(h); }
+
+// Particles are inserted in index order (ID = index) and linked to their
+// cell with push_front, as LinkedCell::Link does at insertion.
+int or_set_particles(void* h, int n, const int* type, const double* x, const double* v,
+                     const double* w, const double* q) {
+  System& s = *static_cast<System*>(h);
+  s.parts.clear();
+  for (auto& c : s.cells) c.clear();
+  s.parts.resize(n);
+  for (int i = 0; i < n; ++i) {
+    Particle& p = s.parts[i];
+    int t = type[i];
+    p.id = i; p.type = t;
+    p.radius = s.type_radius[t];
+    p.crust = s.type_crust[t];
+    p.density = s.type_density[t];
+    p.matbit = s.type_matbit[t];
+    double vol = 4.0 * PI * std::pow(p.radius, 3.) / 3.0;          // Sphere::getVolume
+    p.mass = p.density * vol;
+    p.eqrad = std::pow((0.75 / PI) * vol, 1. / 3.);
+    double I = 8.0 * PI * std::pow(p.radius, 5.) / 15.0;           // Sphere::BuildInertia
+    p.inertia = I * p.density;
+    p.weight = V3(s.gravity[0], s.gravity[1], s.gravity[2]) * (p.mass * (1. - 0. / p.density));
+    p.x = V3(x[3*i], x[3*i+1], x[3*i+2]);
+    p.v = V3(v[3*i], v[3*i+1], v[3*i+2]);
+    p.w = V3(w[3*i], w[3*i+1], w[3*i+2]);
+    p.q = qmake(V3(q[4*i], q[4*i+1], q[4*i+2]), q[4*i+3]);
+    // angular velocity in body frame: q* (w, q) (ParticleKinematics.cpp:220-221)
+    p.wbf = multToVector3(conj(p.q), vecq(p.w, p.q));
+    for (int k = 0; k < 9; ++k) p.basis[k] = (k % 4 == 0) ? 1. : 0.;
+    p.F = V3(); p.T = V3();
+    int id[3];
+    s.getCell(p.x, id);
+    if (!s.valid(id[0], id[1], id[2])) return OR_ERR_OUT_OF_GRID;
+    p.cellnum = s.cellnum(id[0], id[1], id[2]);
+    p.cell[0] = id[0]; p.cell[1] = id[1]; p.cell[2] = id[2];
+    s.cells[p.cellnum].push_front(i);
+  }
+  return OR_OK;
+}
+
+// Leapfrog start (Grains.cpp:168-173): forces at t0, then zero the
+// cumulative tangential and rolling memories.
+int or_init(void* h) {
+  System& s = *static_cast<System*>(h);
+  s.err = 0;
+  computeForces(s);
+  for (auto& p : s.parts)
+    for (auto& kv : p.cmap) { kv.second.kdelta = V3(); kv.second.spring = V3(); }
+  return s.err;
+}
+
+int or_step(void* h, int nsteps) {
+  System& s = *static_cast<System*>(h);
+  s.err = 0;
+  for (int k = 0; k < nsteps; ++k) step(s);
+  return s.err;
+}
+
+// State arrays are indexed by particle ID.  w is the space-fixed angular
+// velocity, wbf the body-fixed one.
+void or_get_state(void* h, double* x, double* v, double* w, double* wbf, double* q,
+                  double* F, double* T) {
+  System& s = *static_cast<System*>(h);
+  for (size_t i = 0; i < s.parts.size(); ++i) {
+    Particle& p = s.parts[i];
+    for (int d = 0; d < 3; ++d) {
+      if (x) x[3*i+d] = p.x[d];
+      if (v) v[3*i+d] = p.v[d];
+      if (w) w[3*i+d] = p.w[d];
+      if (wbf) wbf[3*i+d] = p.wbf[d];
+      if (F) F[3*i+d] = p.F[d];
+      if (T) T[3*i+d] = p.T[d];
+    }
+    if (q) { q[4*i] = p.q.v[0]; q[4*i+1] = p.q.v[1]; q[4*i+2] = p.q.v[2]; q[4*i+3] = p.q.w; }
+  }
+}
+
+void or_get_cells(void* h, int* ijk) {
+  System& s = *static_cast<System*>(h);
+  for (size_t i = 0; i < s.parts.size(); ++i)
+    for (int d = 0; d < 3; ++d) ijk[3*i+d] = s.parts[i].cell[d];
+}
+
+void or_get_grid(void* h, int* nb, double* edge, double* lc_origin) {
+  System& s = *static_cast<System*>(h);
+  for (int d = 0; d < 3; ++d) { nb[d] = s.nb[d]; edge[d] = s.edge[d]; lc_origin[d] = s.lc_origin[d]; }
+}
+
+int or_num_contacts(void* h) { return (int)static_cast<System*>(h)->contacts.size(); }
+
+// Contacts of the last force evaluation, in evaluation order.  id1 < 0 is a
+// wall k as -(k+2).  f is the force on id0.
+void or_get_contacts(void* h, int* id0, int* id1, double* delta, double* point, double* f) {
+  System& s = *static_cast<System*>(h);
+  for (size_t k = 0; k < s.contacts.size(); ++k) {
+    ContactRec& r = s.contacts[k];
+    id0[k] = r.id0; id1[k] = r.id1; delta[k] = r.delta;
+    for (int d = 0; d < 3; ++d) { point[3*k+d] = r.point[d]; f[3*k+d] = r.force[d]; }
+  }
+}
+
+int or_num_history(void* h) {
+  System& s = *static_cast<System*>(h);
+  int n = 0;
+  for (auto& p : s.parts) n += (int)p.cmap.size();
+  return n;
+}
+
+// Contact memory entries: owner ID, partner ID (wall: -(k+2)), kdelta,
+// previous normal, spring torque.
+void or_get_history(void* h, int* owner, int* partner, double* kdelta, double* prevn,
+                    double* spring) {
+  System& s = *static_cast<System*>(h);
+  int n = 0;
+  for (auto& p : s.parts)
+    for (auto& kv : p.cmap) {
+      owner[n] = p.id; partner[n] = std::get<1>(kv.first);
+      for (int d = 0; d < 3; ++d) {
+        kdelta[3*n+d] = kv.second.kdelta[d];
+        prevn[3*n+d] = kv.second.prevn[d];
+        spring[3*n+d] = kv.second.spring[d];
+      }
+      ++n;
+    }
+}
+
+}  // extern "C"

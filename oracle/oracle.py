@@ -1,0 +1,270 @@
+"""ctypes front end of the CPU FP64 restatement (grains_oracle.cpp).
+
+TEST INFRASTRUCTURE: used by tests/, __graft_entry__.smoke() and the CPU
+baseline leg of bench.py as the checker; never by the product path.
+
+The configuration is read from the Grains3D XML input with the standard
+library's ElementTree, independently of the product's own C++ XML reader, so
+the tests also cross-check that reader.  Materials get bits in order of first
+definition, particles first and obstacles next
+(ContactBuilderFactory::defineMaterial, Component/src/ContactBuilderFactory.cpp:
+176-192), and a contact model is keyed by the OR of its two material bits.
+"""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+import xml.etree.ElementTree as ET
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle_grains.so"
+SRC = HERE / "grains_oracle.cpp"
+
+OR_ERR_CONTACT = 1
+OR_ERR_MOTION = 2
+OR_ERR_OUT_OF_GRID = 4
+
+
+def build() -> Path:
+    """Compiles the restatement (scalar C++, no FMA contraction)."""
+    if not LIB.exists() or LIB.stat().st_mtime < SRC.stat().st_mtime:
+        subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared",
+                        "-o", str(LIB), str(SRC)], check=True)
+    return LIB
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [
+        ("origin", ctypes.c_double * 3),
+        ("maxc", ctypes.c_double * 3),
+        ("periodic", ctypes.c_int * 3),
+        ("cell_size_factor", ctypes.c_double),
+        ("gravity", ctypes.c_double * 3),
+        ("dt", ctypes.c_double),
+        ("n_types", ctypes.c_int),
+        ("type_radius", ctypes.POINTER(ctypes.c_double)),
+        ("type_crust", ctypes.POINTER(ctypes.c_double)),
+        ("type_density", ctypes.POINTER(ctypes.c_double)),
+        ("type_matbit", ctypes.POINTER(ctypes.c_int)),
+        ("n_walls", ctypes.c_int),
+        ("wall_centre", ctypes.POINTER(ctypes.c_double)),
+        ("wall_extent", ctypes.POINTER(ctypes.c_double)),
+        ("wall_crust", ctypes.POINTER(ctypes.c_double)),
+        ("wall_matbit", ctypes.POINTER(ctypes.c_int)),
+        ("n_models", ctypes.c_int),
+        ("model_mask", ctypes.POINTER(ctypes.c_int)),
+        ("model_params", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
+_lib = None
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        lib = ctypes.CDLL(str(build()))
+        V = ctypes.c_void_p
+        D = ctypes.POINTER(ctypes.c_double)
+        I = ctypes.POINTER(ctypes.c_int)
+        lib.or_create.argtypes = [ctypes.POINTER(_Config)]
+        lib.or_create.restype = V
+        lib.or_destroy.argtypes = [V]
+        lib.or_set_particles.argtypes = [V, ctypes.c_int, I, D, D, D, D]
+        lib.or_set_particles.restype = ctypes.c_int
+        lib.or_init.argtypes = [V]
+        lib.or_init.restype = ctypes.c_int
+        lib.or_step.argtypes = [V, ctypes.c_int]
+        lib.or_step.restype = ctypes.c_int
+        lib.or_get_state.argtypes = [V, D, D, D, D, D, D, D]
+        lib.or_get_cells.argtypes = [V, I]
+        lib.or_get_grid.argtypes = [V, I, D, D]
+        lib.or_num_contacts.argtypes = [V]
+        lib.or_num_contacts.restype = ctypes.c_int
+        lib.or_get_contacts.argtypes = [V, I, I, D, D, D]
+        lib.or_num_history.argtypes = [V]
+        lib.or_num_history.restype = ctypes.c_int
+        lib.or_get_history.argtypes = [V, I, I, D, D, D]
+        _lib = lib
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def read_xml(path):
+    """Parses the subset of the Grains3D input the DEM step uses."""
+    root = ET.parse(path).getroot()
+    cons = root.find("Construction")
+    lc = cons.find("LinkedCell")
+    o = cons.find("Origin")
+    per = cons.find("Periodicity")
+    cfg = dict(
+        maxc=[float(lc.get(k)) for k in ("MX", "MY", "MZ")],
+        origin=[float(o.get(k)) for k in ("OX", "OY", "OZ")] if o is not None else [0.0] * 3,
+        periodic=[int(per.get(k)) == 1 for k in ("PX", "PY", "PZ")] if per is not None else [0] * 3,
+        cell_size_factor=float(lc.get("CellSizeFactor", "1.")),
+    )
+    bits = {}
+
+    def matbit(name):
+        if name not in bits:
+            bits[name] = 1 << len(bits)
+        return bits[name]
+
+    types = []
+    for p in cons.find("Particles").findall("Particle"):
+        cv = p.find("Convex")
+        sph = cv.find("Sphere")
+        types.append(dict(radius=float(sph.get("Radius")), crust=float(cv.get("CrustThickness")),
+                          density=float(p.get("Density")),
+                          matbit=matbit(p.find("Material").text.strip())))
+    walls = []
+    obs = cons.find("Obstacles")
+    if obs is not None:
+        for on in obs.iter("Obstacle"):
+            cv = on.find("Convex")
+            bx = cv.find("Box")
+            c = on.find("Centre")
+            walls.append(dict(centre=[float(c.get(k)) for k in ("X", "Y", "Z")],
+                              extent=[0.5 * float(bx.get(k)) for k in ("LX", "LY", "LZ")],
+                              crust=float(cv.get("CrustThickness")),
+                              matbit=matbit(on.find("Material").text.strip())))
+    models = []
+    for cf in cons.find("ContactForceModels"):
+        m = cf.find("Material")
+        mask = matbit(m.get("materialA")) | matbit(m.get("materialB"))
+        law = cf.find("HookeMemory")
+
+        def val(tag, dflt=None):
+            e = law.find(tag)
+            return float(e.text) if e is not None else dflt
+
+        models.append(dict(mask=mask, params=[val("kn"), val("en"), val("etat", -1.0), val("muc"),
+                                              val("kt"), val("mur", 0.0), val("etarpf", 0.0),
+                                              val("epst", 0.0)]))
+    g = root.find("Forces").find("Gravity")
+    cfg.update(types=types, walls=walls, models=models,
+               gravity=[float(g.get(k)) for k in ("GX", "GY", "GZ")],
+               dt=float(root.find("Simulation").find("TimeStep").get("dt")))
+    return cfg
+
+
+class Oracle:
+    """CPU FP64 restatement of one Grains3D system."""
+
+    def __init__(self, xml_path):
+        lib = _load()
+        c = read_xml(xml_path)
+        self.cfg = c
+        self._keep = []
+
+        def arr(vals, dt):
+            a = np.ascontiguousarray(vals, dtype=dt).ravel()
+            self._keep.append(a)
+            return a
+
+        cf = _Config()
+        for d in range(3):
+            cf.origin[d] = c["origin"][d]
+            cf.maxc[d] = c["maxc"][d]
+            cf.periodic[d] = int(c["periodic"][d])
+            cf.gravity[d] = c["gravity"][d]
+        cf.cell_size_factor = c["cell_size_factor"]
+        cf.dt = c["dt"]
+        T = c["types"]
+        cf.n_types = len(T)
+        cf.type_radius = _dp(arr([t["radius"] for t in T], np.float64))
+        cf.type_crust = _dp(arr([t["crust"] for t in T], np.float64))
+        cf.type_density = _dp(arr([t["density"] for t in T], np.float64))
+        cf.type_matbit = _ip(arr([t["matbit"] for t in T], np.int32))
+        W = c["walls"]
+        cf.n_walls = len(W)
+        cf.wall_centre = _dp(arr([w["centre"] for w in W] or [[0, 0, 0]], np.float64))
+        cf.wall_extent = _dp(arr([w["extent"] for w in W] or [[0, 0, 0]], np.float64))
+        cf.wall_crust = _dp(arr([w["crust"] for w in W] or [0], np.float64))
+        cf.wall_matbit = _ip(arr([w["matbit"] for w in W] or [0], np.int32))
+        M = c["models"]
+        cf.n_models = len(M)
+        cf.model_mask = _ip(arr([m["mask"] for m in M], np.int32))
+        cf.model_params = _dp(arr([m["params"] for m in M], np.float64))
+        self._cf = cf
+        self._h = lib.or_create(ctypes.byref(cf))
+        self.n = 0
+
+    def close(self):
+        if self._h:
+            _load().or_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_particles(self, type, x, v, w, q):
+        n = len(type)
+        self._t = np.ascontiguousarray(type, np.int32)
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (x, v, w, q)]
+        rc = _load().or_set_particles(self._h, n, _ip(self._t), *[_dp(a) for a in arrs])
+        self.n = n
+        return rc
+
+    def init(self):
+        return _load().or_init(self._h)
+
+    def step(self, nsteps=1):
+        return _load().or_step(self._h, nsteps)
+
+    def state(self):
+        n = self.n
+        out = {k: np.empty((n, 3)) for k in ("x", "v", "w", "wbf", "F", "T")}
+        out["q"] = np.empty((n, 4))
+        _load().or_get_state(self._h, _dp(out["x"]), _dp(out["v"]), _dp(out["w"]),
+                             _dp(out["wbf"]), _dp(out["q"]), _dp(out["F"]), _dp(out["T"]))
+        return out
+
+    def cells(self):
+        ijk = np.empty((self.n, 3), np.int32)
+        _load().or_get_cells(self._h, _ip(ijk))
+        return ijk
+
+    def grid(self):
+        nb = np.empty(3, np.int32)
+        edge = np.empty(3)
+        org = np.empty(3)
+        _load().or_get_grid(self._h, _ip(nb), _dp(edge), _dp(org))
+        return nb, edge, org
+
+    def contacts(self):
+        """(id0, id1, delta, point, f) of the last force evaluation; walls as
+        id1 = -(k+2)."""
+        lib = _load()
+        m = lib.or_num_contacts(self._h)
+        id0 = np.empty(m, np.int32)
+        id1 = np.empty(m, np.int32)
+        dl = np.empty(m)
+        pt = np.empty((m, 3))
+        f = np.empty((m, 3))
+        lib.or_get_contacts(self._h, _ip(id0), _ip(id1), _dp(dl), _dp(pt), _dp(f))
+        return id0, id1, dl, pt, f
+
+    def history(self):
+        lib = _load()
+        m = lib.or_num_history(self._h)
+        own = np.empty(m, np.int32)
+        par = np.empty(m, np.int32)
+        kd = np.empty((m, 3))
+        pn = np.empty((m, 3))
+        sp = np.empty((m, 3))
+        lib.or_get_history(self._h, _ip(own), _ip(par), _dp(kd), _dp(pn), _dp(sp))
+        return own, par, kd, pn, sp

@@ -1,0 +1,323 @@
+// gdem_contact32.cu -- FP32-split mode contact kernels.
+//
+// Positions enter as the particle's cell (integer) plus its offset from the
+// cell's lower corner, held as an unevaluated float pair (hi + lo).  The
+// vector between two particles in neighbouring cells is then
+//     d = dc * edge + (off_b - off_a),      dc in {-1, 0, 1}
+// which is formed in float-float arithmetic (error-free two-sum / two-product
+// with fmaf), so the overlap  |d| - (ra + rb)  keeps ~44 bits although every
+// operation is an FP32 operation.  Everything after the overlap (normal,
+// contact point, relative velocity, HookeMemory force, tangential history,
+// reduction) is plain FP32.  Results are written to the FP64 force/torque
+// arrays that the FP64 leapfrog consumes.
+//
+// Reference functions restated: ClosestPointSPHERESPHERE
+// (Geometry/src/RigidBodyWithCrust.cpp:596-639), HookeMemoryContactForceModel
+// (Component/src/HookeMemoryContactForceModel.cpp:54-249), Torsor::addForce
+// (Component/src/Torsor.cpp:184-189).
+#include "gdem_contact_common.cuh"
+#include "gdem_kernels.cuh"
+
+namespace gdem {
+
+namespace {
+
+// ------------------------------------------------------ float-float ops --
+struct ff { float hi, lo; };
+__device__ __forceinline__ ff two_sum(float a, float b) {
+  float s = __fadd_rn(a, b);
+  float bb = __fadd_rn(s, -a);
+  float e = __fadd_rn(__fadd_rn(a, -__fadd_rn(s, -bb)), __fadd_rn(b, -bb));
+  return {s, e};
+}
+__device__ __forceinline__ ff quick_two_sum(float a, float b) {
+  float s = __fadd_rn(a, b);
+  return {s, __fadd_rn(b, -__fadd_rn(s, -a))};
+}
+__device__ __forceinline__ ff ff_add(ff a, ff b) {
+  ff s = two_sum(a.hi, b.hi);
+  return quick_two_sum(s.hi, __fadd_rn(s.lo, __fadd_rn(a.lo, b.lo)));
+}
+__device__ __forceinline__ ff ff_sqr(ff a) {
+  float p = __fmul_rn(a.hi, a.hi);
+  float e = fmaf(a.hi, a.hi, -p);
+  return quick_two_sum(p, __fadd_rn(e, __fmul_rn(__fmul_rn(2.f, a.hi), a.lo)));
+}
+__device__ __forceinline__ ff ff_sqrt(ff a) {
+  float x = __fsqrt_rn(a.hi);
+  float p = __fmul_rn(x, x);
+  float e = fmaf(x, x, -p);
+  float r = __fadd_rn(__fadd_rn(__fadd_rn(a.hi, -p), -e), a.lo);
+  return quick_two_sum(x, __fdiv_rn(r, __fmul_rn(2.f, x)));
+}
+// One component of d = dc * edge + (ob - oa)
+__device__ __forceinline__ ff relComp(int dc, float eh, float el, float oah, float oal,
+                                      float obh, float obl) {
+  ff s = two_sum(obh, -oah);
+  ff t = two_sum((float)dc * eh, s.hi);
+  float lo = __fadd_rn(__fadd_rn(__fadd_rn(s.lo, t.lo), __fadd_rn(obl, -oal)), (float)dc * el);
+  return quick_two_sum(t.hi, lo);
+}
+
+// ------------------------------------------------------------ float3 ops --
+__device__ __forceinline__ float3 f3(float a, float b, float c) { return make_float3(a, b, c); }
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator-(float3 a) { return f3(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ float3 operator*(float s, float3 a) { return f3(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ float3 operator*(float3 a, float s) { return f3(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ float dotf(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 crossf(float3 a, float3 b) {
+  return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float normf3(float3 a) { return sqrtf(dotf(a, a)); }
+
+// Quaternion::setRotFromTwoVectors + rotateVector in FP32
+__device__ __forceinline__ float3 rotateTo(float3 u, float3 v, float3 x, bool& ok) {
+  float nn = sqrtf(dotf(u, u) * dotf(v, v));
+  float real = nn + dotf(u, v);
+  float3 vect;
+  if (real < 1.e-6f * nn) {
+    real = 0.f;
+    vect = fabsf(u.x) > fabsf(u.z) ? f3(-u.y, u.x, 0.f) : f3(0.f, -u.z, u.y);
+  } else {
+    vect = crossf(u, v);
+  }
+  float nq = sqrtf(dotf(vect, vect) + real * real);
+  ok = nq > 0.f;
+  if (!ok) return x;
+  float s = 1.f / nq;
+  vect = vect * s; real *= s;
+  float nv2 = dotf(vect, vect);
+  return ((real * real - nv2) * x + (2.f * dotf(x, vect)) * vect) + (2.f * real) * crossf(vect, x);
+}
+
+// HookeMemory force in FP32, seen from p0 (same structure as hodc64).
+__device__ __forceinline__ void hodc32(ModelDesc const& m, float kn, float beta, float dt,
+                                       float3 lev0, float3 lev1, float3 pen,
+                                       float3 v0, float3 w0, float m0, float rad0,
+                                       float3 v1, float3 w1, float m1, float rad1,
+                                       bool existed, float3& kd, float3& pn, float3& sp,
+                                       float3& f, float3& mr) {
+  float npen = normf3(pen);
+  float3 normal = pen * (1.f / npen);
+  float3 tmpV = (v0 + crossf(w0, lev0)) - (v1 + crossf(w1, lev1));
+  float3 v_n = normal * dotf(tmpV, normal);
+  float3 v_t = tmpV - v_n;
+  float avmass = 1.f / (1.f / m0 + 1.f / m1);
+  float gamman = -2.f * beta * sqrtf(avmass * kn);
+  float3 delFN = kn * pen - gamman * v_n;
+  float normFN = normf3(delFN);
+  float etat = m.etat == -1. ? -beta * sqrtf(kn / avmass) : (float)m.etat;
+  float gammat = 2.f * etat * avmass;
+  float3 viscousFT = -gammat * v_t;
+  bool rot_ok = false;
+  if (!existed) { kd = f3(0.f, 0.f, 0.f); sp = f3(0.f, 0.f, 0.f); }
+  else kd = rotateTo(pn, normal, kd, rot_ok);
+  float kt = (float)m.kt;
+  kd = kd + (dt * kt) * v_t;
+  pn = normal;
+  // computeTangentialVector
+  float3 tij;
+  float nut = normf3(v_t);
+  float epst = (float)m.epst;
+  if (nut > 0.001f) tij = (-1.f / nut) * v_t;
+  else {
+    float3 s = kd + gammat * v_t;
+    float ns = normf3(s);
+    if ((normf3(kd) > epst || normf3(gammat * v_t) > epst) && ns > epst) tij = (-1.f / ns) * s;
+    else tij = f3(0.f, 0.f, 0.f);
+  }
+  float3 trial = -kd + viscousFT;
+  float normFT = normf3(trial);
+  float muc = (float)m.muc;
+  float3 delFT;
+  if (normFT <= muc * normFN) delFT = normFT * tij;
+  else {
+    if (kt != 0.f) kd = ((-muc * normFN) * tij + viscousFT) * (1.f / kt);
+    delFT = (muc * normFN) * tij;
+  }
+  mr = f3(0.f, 0.f, 0.f);
+  if (m.rolling) {
+    float mur = (float)m.mur;
+    float Req = 1.f / (1.f / rad0 + 1.f / rad1);
+    float kr = 3.f * kn * mur * mur * Req * Req;
+    float etar = 3.f * gamman * mur * mur * Req * Req;
+    float maxM = mur * Req * normFN;
+    float3 wrel = w0 - w1;
+    if (existed) { bool ok2; sp = rotateTo(pn, normal, sp, ok2); }
+    sp = sp - (kr * dt) * wrel;
+    float nM = normf3(sp);
+    if (nM > maxM) sp = sp * (maxM / nM);
+    mr = sp - ((float)m.etarpf * etar) * wrel;
+  }
+  f = delFN + delFT;
+}
+
+__device__ __forceinline__ void loadHistF(HistTable const& t, int slot, float3& kd, float3& pn, float3& sp) {
+  const float* v = static_cast<const float*>(t.vals) + 9 * (size_t)slot;
+  kd = f3(v[0], v[1], v[2]); pn = f3(v[3], v[4], v[5]); sp = f3(v[6], v[7], v[8]);
+}
+__device__ __forceinline__ void storeHistF(HistTable const& t, int slot, float3 kd, float3 pn, float3 sp) {
+  float* v = static_cast<float*>(t.vals) + 9 * (size_t)slot;
+  v[0] = kd.x; v[1] = kd.y; v[2] = kd.z; v[3] = pn.x; v[4] = pn.y; v[5] = pn.z;
+  v[6] = sp.x; v[7] = sp.y; v[8] = sp.z;
+}
+
+// Canonical relative vector (p0 = lower ID) from the split positions.
+struct Rel { ff d[3]; };
+__device__ __forceinline__ Rel relVec(GridDesc const& g, int dcx, int dcy, int dcz,
+                                      float4 h0, float4 l0, float4 h1, float4 l1) {
+  Rel r;
+  r.d[0] = relComp(dcx, g.edge_hi[0], g.edge_lo[0], h0.x, l0.x, h1.x, l1.x);
+  r.d[1] = relComp(dcy, g.edge_hi[1], g.edge_lo[1], h0.y, l0.y, h1.y, l1.y);
+  r.d[2] = relComp(dcz, g.edge_hi[2], g.edge_lo[2], h0.z, l0.z, h1.z, l1.z);
+  return r;
+}
+
+__global__ void __launch_bounds__(256) k_pairs32(DevState S) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= S.n) return;
+  const int4 cc = S.cellc[t];
+  GridDesc const& g = S.grids[cc.w];
+  const float4 ha = S.offh[t];
+  const int ida = S.id[t];
+  int* out = S.pairs + (size_t)t * kPairCap;
+  int cnt = 0;
+  for (int dj = -1; dj <= 1; ++dj)
+    for (int dk = -1; dk <= 1; ++dk)
+      for (int di = -1; di <= 1; ++di) {
+        int sh[3];
+        int key = neighbourKey(g, cc.x, cc.y, cc.z, di, dj, dk, sh);
+        if (key < 0) continue;
+        int b = S.cell_start[key], e = b + S.cell_count[key];
+        for (int u = b; u < e; ++u) {
+          if (u == t) continue;
+          const float4 hb = S.offh[u];
+          const int idb = S.id[u];
+          // evaluated in canonical orientation so both directions agree
+          float4 h0 = ida < idb ? ha : hb, h1 = ida < idb ? hb : ha;
+          int s = ida < idb ? 1 : -1;
+          float dx = fmaf((float)(s * di), g.edge_hi[0], h1.x - h0.x);
+          float dy = fmaf((float)(s * dj), g.edge_hi[1], h1.y - h0.y);
+          float dz = fmaf((float)(s * dk), g.edge_hi[2], h1.z - h0.z);
+          float R = (h0.w + h1.w) * (1.f + 4.e-6f);
+          if (dx * dx + dy * dy + dz * dz > R * R) continue;
+          if (cnt < kPairCap) out[cnt] = u | (offCode(di, dj, dk) << 27);
+          ++cnt;
+        }
+      }
+  if (cnt > kPairCap) { raise(S.status, kErrPairsFull); cnt = kPairCap; }
+  S.npairs[t] = cnt;
+}
+
+__global__ void __launch_bounds__(256) k_forces32(DevState S) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= S.n) return;
+  const int cap = S.cap;
+  const int4 cc = S.cellc[t];
+  GridDesc const& g = S.grids[cc.w];
+  const int ida = S.id[t];
+  TypeDesc const& ta = S.types[S.type[t]];
+  const float4 ha = S.offh[t], la = S.offl[t], va = S.velf[t], wa = S.omgf[t];
+  float3 Fs = f3(0.f, 0.f, 0.f), Ts = f3(0.f, 0.f, 0.f);
+  const float dt = (float)S.dt;
+  const int np = S.npairs[t];
+  const int* seg = S.pairs + (size_t)t * kPairCap;
+  for (int e = 0; e < np; ++e) {
+    const uint32_t ent = (uint32_t)seg[e];
+    const int u = (int)(ent & ((1u << 27) - 1));
+    int di, dj, dk;
+    offDecode((int)(ent >> 27), &di, &dj, &dk);
+    const int idb = S.id[u];
+    const float4 hb = S.offh[u], lb = S.offl[u];
+    const bool t0 = ida < idb;
+    Rel r = t0 ? relVec(g, di, dj, dk, ha, la, hb, lb) : relVec(g, -di, -dj, -dk, hb, lb, ha, la);
+    ff d2 = ff_add(ff_add(ff_sqr(r.d[0]), ff_sqr(r.d[1])), ff_sqr(r.d[2]));
+    ff nd = ff_sqrt(d2);
+    float4 h0 = t0 ? ha : hb, l0 = t0 ? la : lb, h1 = t0 ? hb : ha, l1 = t0 ? lb : la;
+    ff rs = two_sum(h0.w, h1.w);
+    ff R = quick_two_sum(rs.hi, __fadd_rn(rs.lo, __fadd_rn(l0.w, l1.w)));
+    ff dist = ff_add(nd, ff{-R.hi, -R.lo});
+    float dd = dist.hi;
+    if (S.diag) S.pair_delta[(size_t)t * kPairCap + e] = dd < 0.f ? dd : __int_as_float(0x7f800000);
+    if (!(dd < 0.f)) continue;
+    TypeDesc const& tb = S.types[S.type[u]];
+    const TypeDesc& tp0 = t0 ? ta : tb;
+    const TypeDesc& tp1 = t0 ? tb : ta;
+    if (-dd >= (float)(tp0.crust + tp1.crust)) raise(S.status, kErrContactOverlap);
+    float3 dh = f3(r.d[0].hi, r.d[1].hi, r.d[2].hi);
+    float inv = 1.f / nd.hi;
+    float3 un = dh * inv;
+    float3 lev0 = (h0.w + 0.5f * dd) * un;     // contact point - x0
+    float3 lev1 = lev0 - dh;                    // contact point - x1 (image)
+    float3 pen = dd * un;
+    const float4 vb = S.velf[u], wb = S.omgf[u];
+    float4 v0 = t0 ? va : vb, w0 = t0 ? wa : wb, v1 = t0 ? vb : va, w1 = t0 ? wb : wa;
+    ModelDesc const& m = S.models[g.model_base + tp0.mat * kMaxMat + tp1.mat];
+    const int id0 = t0 ? ida : idb, id1 = t0 ? idb : ida;
+    const unsigned long long key = pairKey(id0, id1);
+    int old = histFind(S.hist_old, key);
+    float3 kd, pn, sp, f, mr;
+    if (old >= 0) loadHistF(S.hist_old, old, kd, pn, sp);
+    hodc32(m, (float)m.kn, (float)m.beta, dt, lev0, lev1, pen, f3(v0.x, v0.y, v0.z),
+           f3(w0.x, w0.y, w0.z), v0.w, w0.w, f3(v1.x, v1.y, v1.z), f3(w1.x, w1.y, w1.z),
+           v1.w, w1.w, old >= 0, kd, pn, sp, f, mr);
+    if (t0) {
+      int slot = histInsert(S.hist_new, key);
+      if (slot < 0) raise(S.status, kErrHashFull);
+      else storeHistF(S.hist_new, slot, kd, pn, sp);
+      Fs = Fs + f;
+      Ts = Ts + crossf(lev0, f);
+      if (m.rolling) Ts = Ts + mr;
+    } else {
+      Fs = Fs - f;
+      Ts = Ts - crossf(lev1, f);
+      if (m.rolling) Ts = Ts - mr;
+    }
+  }
+  // walls: geometry from the FP64 master position, force law in FP32
+  d3 xt = ld3(S.x, cap, t);
+  for (int k = 0; k < g.wall_count; ++k) {
+    WallDesc const& wd = S.walls[g.wall_begin + k];
+    Contact64 ct = sphereWall64(xt, ta.radius, ta.crust, wd);
+    if (S.diag) S.wall_delta[(size_t)t * S.max_walls + k] = ct.contact ? ct.dist : __longlong_as_double(0x7ff0000000000000ll);
+    if (ct.error) raise(S.status, kErrContactOverlap);
+    if (!ct.contact || !(ct.dist < 0.)) continue;
+    ModelDesc const& m = S.models[g.model_base + ta.mat * kMaxMat + wd.mat];
+    const unsigned long long key = wallKey(ida, k);
+    int old = histFind(S.hist_old, key);
+    float3 kd, pn, sp, f, mr;
+    if (old >= 0) loadHistF(S.hist_old, old, kd, pn, sp);
+    d3 l0 = ct.point - xt;
+    d3 l1 = ct.point - mk(wd.centre[0], wd.centre[1], wd.centre[2]);
+    float3 lev0 = f3((float)l0.x, (float)l0.y, (float)l0.z);
+    float3 lev1 = f3((float)l1.x, (float)l1.y, (float)l1.z);
+    float3 pen = f3((float)ct.overlap.x, (float)ct.overlap.y, (float)ct.overlap.z);
+    float3 zero = f3(0.f, 0.f, 0.f);
+    hodc32(m, (float)m.kn, (float)m.beta, dt, lev0, lev1, pen, f3(va.x, va.y, va.z),
+           f3(wa.x, wa.y, wa.z), va.w, wa.w, zero, zero, 1.e20f, (float)wd.eqrad,
+           old >= 0, kd, pn, sp, f, mr);
+    int slot = histInsert(S.hist_new, key);
+    if (slot < 0) raise(S.status, kErrHashFull);
+    else storeHistF(S.hist_new, slot, kd, pn, sp);
+    Fs = Fs + f;
+    Ts = Ts + crossf(lev0, f);
+    if (m.rolling) Ts = Ts + mr;
+  }
+  S.F[t] = ta.weight[0] + (double)Fs.x;
+  S.F[cap + t] = ta.weight[1] + (double)Fs.y;
+  S.F[2 * cap + t] = ta.weight[2] + (double)Fs.z;
+  S.T[t] = (double)Ts.x; S.T[cap + t] = (double)Ts.y; S.T[2 * cap + t] = (double)Ts.z;
+}
+
+}  // namespace
+
+void launch_pairs32(DevState const& S, cudaStream_t st) {
+  if (S.n) k_pairs32<<<(S.n + 255) / 256, 256, 0, st>>>(S);
+}
+void launch_forces32(DevState const& S, cudaStream_t st) {
+  if (S.n) k_forces32<<<(S.n + 255) / 256, 256, 0, st>>>(S);
+}
+
+}  // namespace gdem

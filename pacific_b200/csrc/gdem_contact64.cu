@@ -1,0 +1,171 @@
+// gdem_contact64.cu -- FP64-mode broad phase, narrow phase, HODC force and
+// per-particle reduction.  Compiled with -fmad=false so that every FP64
+// expression rounds like the reference's scalar CPU code.
+//
+//   k_pairs64   27-cell stencil enumeration (the reference uses the 13-cell
+//               half stencil of LinkedCell::setCellContactNeighborhood,
+//               Base/src/LinkedCell.cpp:958-984; here each particle lists
+//               all its partners so that its forces can be reduced without
+//               atomics).  A candidate is kept when ClosestPointSPHERESPHERE
+//               reports contact (distance <= 0), evaluated with the lower-ID
+//               body first so both directions of a pair agree bit for bit.
+//   k_forces64  narrow phase + HookeMemory force + tangential history through
+//               the hashed pair table + deterministic segmented reduction of
+//               each particle's force and torque over its own pair segment,
+//               in list order, then its wall contacts (SimpleObstacle::
+//               InterAction, Component/src/SimpleObstacle.cpp:222-271).
+#include "gdem_contact_common.cuh"
+#include "gdem_kernels.cuh"
+
+namespace gdem {
+
+namespace {
+
+__global__ void __launch_bounds__(256) k_pairs64(DevState S) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= S.n) return;
+  const int4 cc = S.cellc[t];
+  GridDesc const& g = S.grids[cc.w];
+  const double4 pa = S.pos64[t];
+  const int ida = S.id[t];
+  int* out = S.pairs + (size_t)t * kPairCap;
+  int cnt = 0;
+  for (int dj = -1; dj <= 1; ++dj)
+    for (int dk = -1; dk <= 1; ++dk)
+      for (int di = -1; di <= 1; ++di) {
+        int sh[3];
+        int key = neighbourKey(g, cc.x, cc.y, cc.z, di, dj, dk, sh);
+        if (key < 0) continue;
+        int b = S.cell_start[key], e = b + S.cell_count[key];
+        d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
+        for (int u = b; u < e; ++u) {
+          if (u == t) continue;
+          const double4 pb = S.pos64[u];
+          const int idb = S.id[u];
+          d3 xa, xb;
+          if (ida < idb) { xa = mk(pa.x, pa.y, pa.z); xb = mk(pb.x, pb.y, pb.z) + shift; }
+          else { xa = mk(pb.x, pb.y, pb.z); xb = mk(pa.x, pa.y, pa.z) + (-shift); }
+          double distance = norm(xb - xa) - (pa.w + pb.w);
+          if (distance > 0.) continue;
+          if (cnt < kPairCap) out[cnt] = u | (offCode(di, dj, dk) << 27);
+          ++cnt;
+        }
+      }
+  if (cnt > kPairCap) { raise(S.status, kErrPairsFull); cnt = kPairCap; }
+  S.npairs[t] = cnt;
+}
+
+__device__ __forceinline__ void loadHist(HistTable const& t, int slot, d3& kd, d3& pn, d3& sp) {
+  const double* v = static_cast<const double*>(t.vals) + 9 * (size_t)slot;
+  kd = mk(v[0], v[1], v[2]); pn = mk(v[3], v[4], v[5]); sp = mk(v[6], v[7], v[8]);
+}
+__device__ __forceinline__ void storeHist(HistTable const& t, int slot, d3 kd, d3 pn, d3 sp) {
+  double* v = static_cast<double*>(t.vals) + 9 * (size_t)slot;
+  v[0] = kd.x; v[1] = kd.y; v[2] = kd.z; v[3] = pn.x; v[4] = pn.y; v[5] = pn.z;
+  v[6] = sp.x; v[7] = sp.y; v[8] = sp.z;
+}
+
+__global__ void __launch_bounds__(256) k_forces64(DevState S) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= S.n) return;
+  const int cap = S.cap;
+  const int4 cc = S.cellc[t];
+  GridDesc const& g = S.grids[cc.w];
+  const int ida = S.id[t];
+  TypeDesc const& ta = S.types[S.type[t]];
+  const double4 pa = S.pos64[t], va = S.vel64[t], wa = S.omg64[t];
+  const d3 xt = mk(pa.x, pa.y, pa.z), vt = mk(va.x, va.y, va.z), wt = mk(wa.x, wa.y, wa.z);
+  d3 F = mk(ta.weight[0], ta.weight[1], ta.weight[2]);
+  d3 T = mk(0., 0., 0.);
+  const double dt = S.dt;
+  const int np = S.npairs[t];
+  const int* seg = S.pairs + (size_t)t * kPairCap;
+  for (int e = 0; e < np; ++e) {
+    const uint32_t ent = (uint32_t)seg[e];
+    const int u = (int)(ent & ((1u << 27) - 1));
+    int di, dj, dk, sh[3];
+    offDecode((int)(ent >> 27), &di, &dj, &dk);
+    neighbourKey(g, cc.x, cc.y, cc.z, di, dj, dk, sh);
+    d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
+    const int idb = S.id[u];
+    TypeDesc const& tb = S.types[S.type[u]];
+    const double4 pb = S.pos64[u], vb = S.vel64[u], wb = S.omg64[u];
+    const bool t0 = ida < idb;
+    // canonical bodies: p0 = lower ID at its own position, p1 at its image
+    d3 x0, x1, v0, v1, w0, w1;
+    double r0, r1, c0, c1, m0, m1, q0, q1;
+    int mat0, mat1, id0, id1;
+    if (t0) {
+      x0 = xt; v0 = vt; w0 = wt; r0 = pa.w; m0 = va.w; q0 = wa.w; c0 = ta.crust; mat0 = ta.mat; id0 = ida;
+      x1 = mk(pb.x, pb.y, pb.z) + shift; v1 = mk(vb.x, vb.y, vb.z); w1 = mk(wb.x, wb.y, wb.z);
+      r1 = pb.w; m1 = vb.w; q1 = wb.w; c1 = tb.crust; mat1 = tb.mat; id1 = idb;
+    } else {
+      x0 = mk(pb.x, pb.y, pb.z); v0 = mk(vb.x, vb.y, vb.z); w0 = mk(wb.x, wb.y, wb.z);
+      r0 = pb.w; m0 = vb.w; q0 = wb.w; c0 = tb.crust; mat0 = tb.mat; id0 = idb;
+      x1 = xt + (-shift); v1 = vt; w1 = wt; r1 = pa.w; m1 = va.w; q1 = wa.w; c1 = ta.crust;
+      mat1 = ta.mat; id1 = ida;
+    }
+    Contact64 ct = sphereSphere64(x0, r0, c0, x1, r1, c1);
+    if (S.diag) S.pair_delta[(size_t)t * kPairCap + e] = ct.contact ? (float)ct.dist : __int_as_float(0x7f800000);
+    if (!ct.contact || !(ct.dist < 0.)) continue;
+    if (ct.error) raise(S.status, kErrContactOverlap);
+    ModelDesc const& m = S.models[g.model_base + mat0 * kMaxMat + mat1];
+    const unsigned long long key = pairKey(id0, id1);
+    int old = histFind(S.hist_old, key);
+    d3 kd, pn, sp;
+    if (old >= 0) loadHist(S.hist_old, old, kd, pn, sp);
+    d3 f, mr;
+    hodc64(m, dt, ct.point, ct.overlap, x0, v0, w0, m0, q0, x1, v1, w1, m1, q1, old >= 0,
+           kd, pn, sp, f, mr);
+    if (t0) {
+      int slot = histInsert(S.hist_new, key);
+      if (slot < 0) raise(S.status, kErrHashFull);
+      else storeHist(S.hist_new, slot, kd, pn, sp);
+      F = F + f;
+      T = T + cross(ct.point - x0, f);
+      if (m.rolling) T = T + mr;
+    } else {
+      d3 fm = -f;
+      F = F + fm;
+      T = T + cross(ct.point - x1, fm);
+      if (m.rolling) T = T + (-mr);
+    }
+  }
+  // walls: the particle is p0, the obstacle p1 (mass Component::m_massObstacle)
+  for (int k = 0; k < g.wall_count; ++k) {
+    WallDesc const& wd = S.walls[g.wall_begin + k];
+    Contact64 ct = sphereWall64(xt, pa.w, ta.crust, wd);
+    if (S.diag) S.wall_delta[(size_t)t * S.max_walls + k] = ct.contact ? ct.dist : __longlong_as_double(0x7ff0000000000000ll);
+    if (ct.error) raise(S.status, kErrContactOverlap);
+    if (!ct.contact || !(ct.dist < 0.)) continue;
+    ModelDesc const& m = S.models[g.model_base + ta.mat * kMaxMat + wd.mat];
+    const unsigned long long key = wallKey(ida, k);
+    int old = histFind(S.hist_old, key);
+    d3 kd, pn, sp;
+    if (old >= 0) loadHist(S.hist_old, old, kd, pn, sp);
+    d3 f, mr;
+    d3 zero = mk(0., 0., 0.);
+    hodc64(m, dt, ct.point, ct.overlap, xt, vt, wt, va.w, wa.w,
+           mk(wd.centre[0], wd.centre[1], wd.centre[2]), zero, zero, 1.e20, wd.eqrad,
+           old >= 0, kd, pn, sp, f, mr);
+    int slot = histInsert(S.hist_new, key);
+    if (slot < 0) raise(S.status, kErrHashFull);
+    else storeHist(S.hist_new, slot, kd, pn, sp);
+    F = F + f;
+    T = T + cross(ct.point - xt, f);
+    if (m.rolling) T = T + mr;
+  }
+  st3(S.F, cap, t, F);
+  st3(S.T, cap, t, T);
+}
+
+}  // namespace
+
+void launch_pairs64(DevState const& S, cudaStream_t st) {
+  if (S.n) k_pairs64<<<(S.n + 255) / 256, 256, 0, st>>>(S);
+}
+void launch_forces64(DevState const& S, cudaStream_t st) {
+  if (S.n) k_forces64<<<(S.n + 255) / 256, 256, 0, st>>>(S);
+}
+
+}  // namespace gdem

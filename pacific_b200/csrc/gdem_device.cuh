@@ -1,0 +1,196 @@
+// gdem_device.cuh -- device-side state and helpers for the Grains3D DEM step.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "gdem_types.h"
+
+namespace gdem {
+
+constexpr unsigned long long kEmptyKey = 0xFFFFFFFFFFFFFFFFull;
+constexpr uint32_t kWallBit = 0x80000000u;
+
+// Contact-history table: open addressing with linear probing, keyed on the
+// unordered particle pair (lower ID in the high word) or on (particle, wall).
+// Values are stored as seen from the lower-ID body (or the particle, for a
+// wall); the other body's view is the negation, as in the reference where p1
+// holds (-kdelta, -normal, -spring) (HookeMemoryContactForceModel.cpp:191-192).
+// Two tables alternate: the one written during step n is read during step
+// n+1, so entries not touched in a step disappear, which is what
+// Component::updateContactMap (Component.cpp:583-595) does.
+struct HistTable {
+  unsigned long long* keys;
+  void* vals;            // 9 values per slot (kdelta, prev normal, spring torque)
+  int log2cap;
+};
+
+__host__ __device__ inline unsigned long long pairKey(int ida, int idb) {
+  return ((unsigned long long)(uint32_t)ida << 32) | (uint32_t)idb;
+}
+__host__ __device__ inline unsigned long long wallKey(int id, int wall) {
+  return ((unsigned long long)(uint32_t)id << 32) | (kWallBit | (uint32_t)wall);
+}
+__host__ __device__ inline uint32_t hashSlot(unsigned long long k, int log2cap) {
+  k ^= k >> 33;
+  k *= 0xff51afd7ed558ccdull;
+  k ^= k >> 33;
+  k *= 0xc4ceb9fe1a85ec53ull;
+  k ^= k >> 33;
+  return (uint32_t)(k & ((1ull << log2cap) - 1));
+}
+// Returns the slot holding key, or -1.
+__device__ inline int histFind(HistTable const& t, unsigned long long key) {
+  uint32_t mask = (1u << t.log2cap) - 1;
+  uint32_t s = hashSlot(key, t.log2cap);
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    unsigned long long k = t.keys[s];
+    if (k == key) return (int)s;
+    if (k == kEmptyKey) return -1;
+    s = (s + 1) & mask;
+  }
+  return -1;
+}
+// Claims a slot for key (one writer per key); -1 when the table is full.
+__device__ inline int histInsert(HistTable const& t, unsigned long long key) {
+  uint32_t mask = (1u << t.log2cap) - 1;
+  uint32_t s = hashSlot(key, t.log2cap);
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    unsigned long long prev = atomicCAS(&t.keys[s], kEmptyKey, key);
+    if (prev == kEmptyKey || prev == key) return (int)s;
+    s = (s + 1) & mask;
+  }
+  return -1;
+}
+
+// Whole device state of one batch of instances.  Per-particle arrays are in
+// the current sorted (cell) order; component d of particle s of an n-vector
+// field lives at [d * cap + s] (structure of arrays).
+struct DevState {
+  int n;                  // particles
+  int cap;                // allocated particles (component stride)
+  int ncells;             // total cell keys of all instances
+  int ninst;
+  double dt;
+  int* id; int* type; int* inst; int* key;
+  double* x; double* v; double* w; double* wbf; double* q; double* F; double* T;
+  double* basis;          // 9 per particle, non-spherical shapes only
+  // permutation targets (swapped with the above after each binning)
+  int* id2; int* type2; int* inst2;
+  double* x2; double* v2; double* w2; double* wbf2; double* q2; double* basis2;
+  // binning
+  int* skey;              // cell key in the old order
+  int* rank;              // arrival rank within the cell
+  int* cell_count; int* cell_start; int* order;
+  int* scan_tmp;
+  // compact copies for the contact kernels (sorted order)
+  double4* pos64;         // x, y, z, radius
+  double4* vel64;         // v, mass
+  double4* omg64;         // w (space frame), equivalent radius
+  float4* offh;           // cell-relative offset, hi part; radius hi
+  float4* offl;           // lo parts; radius lo
+  float4* velf;           // v (float)
+  float4* omgf;           // w (float)
+  int4* cellc;            // cell i, j, k and instance
+  // pair list: per-particle segments of kPairCap entries
+  int* pairs; int* npairs;
+  float* pair_delta;      // diagnostics: overlap of each entry (+inf: no contact)
+  double* wall_delta;     // diagnostics: overlap with each wall slot
+  int diag;
+  HistTable hist_old, hist_new;
+  int* status;
+  GridDesc const* grids; TypeDesc const* types; ModelDesc const* models;
+  WallDesc const* walls;
+  int max_walls;          // walls of the largest instance
+};
+
+// ----------------------------------------------------------- FP64 helpers --
+struct d3 { double x, y, z; };
+__device__ __forceinline__ d3 mk(double a, double b, double c) { d3 r; r.x = a; r.y = b; r.z = c; return r; }
+__device__ __forceinline__ d3 operator+(d3 a, d3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ d3 operator-(d3 a, d3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ d3 operator-(d3 a) { return mk(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ d3 operator*(d3 a, double s) { return mk(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ d3 operator*(double s, d3 a) { return mk(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ d3 operator/(d3 a, double s) { return mk(a.x / s, a.y / s, a.z / s); }
+__device__ __forceinline__ double dot(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// Vector3::operator^ (Geometry/src/Vector3.cpp:114-119)
+__device__ __forceinline__ d3 cross(d3 a, d3 b) {
+  return mk(a.y * b.z - a.z * b.y, -a.x * b.z + a.z * b.x, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ double norm(d3 a) { return sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+__device__ __forceinline__ d3 ld3(const double* p, int cap, int s) {
+  return mk(p[s], p[cap + s], p[2 * cap + s]);
+}
+__device__ __forceinline__ void st3(double* p, int cap, int s, d3 a) {
+  p[s] = a.x; p[cap + s] = a.y; p[2 * cap + s] = a.z;
+}
+
+struct dq { d3 v; double w; };
+__device__ __forceinline__ dq qmk(d3 v, double w) { dq q; q.v = v; q.w = w; return q; }
+__device__ __forceinline__ dq conj(dq q) { return qmk(-q.v, q.w); }
+// Quaternion::operator* (Geometry/src/Quaternion.cpp:442-448)
+__device__ __forceinline__ dq qmul(dq a, dq b) {
+  double t = (a.w * b.w) - dot(a.v, b.v);
+  d3 vt = (cross(a.v, b.v) + (a.w * b.v)) + (b.w * a.v);
+  return qmk(vt, t);
+}
+// operator,(Vector3, Quaternion) = q.multLeftVec(lhs) (Quaternion.cpp:93-98)
+__device__ __forceinline__ dq vecq(d3 l, dq q) {
+  double t = dot(-l, q.v);
+  d3 vt = cross(l, q.v) + (l * q.w);
+  return qmk(vt, t);
+}
+// Quaternion::multToVector3 (Quaternion.cpp:108-113)
+__device__ __forceinline__ d3 multToVector3(dq a, dq r) {
+  return (cross(a.v, r.v) + (a.w * r.v)) + (r.w * a.v);
+}
+// Quaternion::setRotFromTwoVectors (Quaternion.cpp:263-288)
+__device__ __forceinline__ dq rotFromTwoVectors(d3 u, d3 v) {
+  double nn = sqrt(dot(u, u) * dot(v, v));
+  double real = nn + dot(u, v);
+  d3 vect;
+  if (real < 1.e-6 * nn) {
+    real = 0.;
+    vect = fabs(u.x) > fabs(u.z) ? mk(-u.y, u.x, 0.) : mk(0., -u.z, u.y);
+  } else {
+    vect = cross(u, v);
+  }
+  double nq = sqrt(vect.x * vect.x + vect.y * vect.y + vect.z * vect.z + real * real);
+  double s = 1. / nq;
+  return qmk(vect * s, real * s);
+}
+// Quaternion::rotateVector (Quaternion.cpp:293-299)
+__device__ __forceinline__ d3 rotateVector(dq q, d3 v) {
+  double nv = norm(q.v);
+  return ((q.w * q.w - nv * nv) * v + (2. * dot(v, q.v)) * q.v) + (2. * q.w) * cross(q.v, v);
+}
+
+__device__ __forceinline__ void raise(int* status, int bits) { atomicOr(status, bits); }
+
+// Cell of a neighbour offset (di, dj, dk) around (i, j, k) of grid g, with
+// the periodic minimum-image wrap.  Returns the global cell key or -1, and the
+// image shift (in units of the period) of the particles found there.
+__device__ __forceinline__ int neighbourKey(GridDesc const& g, int i, int j, int k,
+                                            int di, int dj, int dk, int* sh) {
+  int c[3] = {i + di, j + dj, k + dk};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    sh[d] = 0;
+    if (g.periodic[d]) {
+      int nin = g.nb[d] - 2;
+      if (c[d] < 1) { c[d] += nin; sh[d] = -1; }
+      else if (c[d] > nin) { c[d] -= nin; sh[d] = 1; }
+    } else if (c[d] < 0 || c[d] >= g.nb[d]) {
+      return -1;
+    }
+  }
+  return g.cell_offset + c[1] * g.nb[2] * g.nb[0] + c[2] * g.nb[0] + c[0];
+}
+
+// Code of a stencil offset in 0..26 and back.
+__device__ __forceinline__ int offCode(int di, int dj, int dk) { return (di + 1) + 3 * (dk + 1) + 9 * (dj + 1); }
+__device__ __forceinline__ void offDecode(int c, int* di, int* dj, int* dk) {
+  *di = c % 3 - 1; *dk = (c / 3) % 3 - 1; *dj = c / 9 - 1;
+}
+
+}  // namespace gdem

@@ -1,0 +1,951 @@
+// gdem_host.cu -- host runtime behind the C ABI of include/grains_b200.h.
+//
+// Builds the device descriptors from Grains3D XML input (same element and
+// attribute names as Grains::Construction, Base/src/Grains.cpp:535-1030, and
+// the contact-model factory, Component/src/ContactBuilderFactory.cpp:88-169),
+// owns every device buffer, and sequences the kernels of one leapfrog step
+// (Grains::Simulation, Grains.cpp:344-364):
+//
+//   memset(cell counts) -> k_move (kick dt/2 + drift dt, cell key, histogram)
+//   -> scan / place / cellsort / gather (counting sort into cell order)
+//   -> k_pairs (27-cell stencil) -> memset(new history keys)
+//   -> k_forces (narrow phase + HODC + history + per-particle reduction)
+//   -> [next step's k_move applies this step's closing kick first]
+//   -> k_kick (closing kick dt/2 of the last step of the call)
+//
+// Steps after the first of a gdem_step call are replayed from two captured
+// CUDA graphs (the double-buffered state and history tables alternate with
+// period two).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/grains_b200.h"
+#include "gdem_kernels.cuh"
+#include "xml_reader.hpp"
+
+namespace gdem {
+
+namespace {
+
+thread_local std::string g_last_error;
+const double PI = 3.14159265358979323846;
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+#define CK(call)                                                                     \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess)                                                           \
+      throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_));           \
+  } while (0)
+
+template <typename T>
+T* dalloc(size_t count) {
+  void* p = nullptr;
+  if (count == 0) count = 1;
+  CK(cudaMalloc(&p, count * sizeof(T)));
+  return static_cast<T*>(p);
+}
+
+int nextPow2Log(size_t n) {
+  int l = 10;
+  while ((size_t(1) << l) < n) ++l;
+  return l;
+}
+
+// ----------------------------------------------------------- XML import --
+struct InstanceDesc {
+  GridDesc grid;
+  std::vector<TypeDesc> types;
+  std::vector<WallDesc> walls;
+  ModelDesc models[kMaxMat * kMaxMat];
+  double gravity[3];
+  double dt;
+  int nmat;
+};
+
+int materialIndex(std::map<std::string, int>& mats, std::vector<std::string>& order,
+                  std::string const& name) {
+  auto it = mats.find(name);
+  if (it != mats.end()) return it->second;
+  int idx = (int)order.size();
+  if (idx >= kMaxMat) throw std::runtime_error("more than 8 materials");
+  mats[name] = idx;
+  order.push_back(name);
+  return idx;
+}
+
+double childD(XmlNode const* n, const char* name, bool required, double dflt) {
+  XmlNode const* c = n->child(name);
+  if (!c) {
+    if (required) throw std::runtime_error(std::string("missing <") + name + ">");
+    return dflt;
+  }
+  return c->valueD();
+}
+
+// HookeMemoryContactForceModel::defineParameters (:256-310) and
+// HookeContactForceModel::defineParameters.  A missing <epst> leaves epst at
+// zero in the reference (the default is stored under the key "eps").
+ModelDesc readModel(XmlNode const* law, std::string const& kind) {
+  ModelDesc m{};
+  m.kn = childD(law, "kn", true, 0.);
+  m.muc = childD(law, "muc", true, 0.);
+  m.en = childD(law, "en", true, 0.);
+  m.etat = childD(law, "etat", false, -1.);
+  m.mur = childD(law, "mur", false, 0.);
+  m.etarpf = childD(law, "etarpf", false, 0.);
+  m.kt = childD(law, "kt", kind == "HookeMemory", 0.);
+  m.epst = childD(law, "epst", false, 0.);
+  m.rolling = m.mur != 0. ? 1 : 0;
+  m.memory = kind == "HookeMemory" ? 1 : 0;
+  m.beta = std::log(m.en) / std::sqrt(PI * PI + std::log(m.en) * std::log(m.en));
+  m.valid = 1;
+  return m;
+}
+
+void collectObstacles(XmlNode const* n, std::vector<XmlNode const*>& out) {
+  for (auto const& c : n->children) {
+    if (c->name == "Obstacle") out.push_back(c.get());
+    else if (c->name == "Composite") collectObstacles(c.get(), out);
+  }
+}
+
+InstanceDesc readInstance(std::string const& path) {
+  auto doc = parseXmlFile(path);
+  XmlNode const* root = doc.get();
+  XmlNode const* cons = root->find("Construction");
+  if (!cons) throw std::runtime_error("no <Construction> in " + path);
+  InstanceDesc I{};
+  std::memset(&I.grid, 0, sizeof(I.grid));
+  XmlNode const* lc = cons->child("LinkedCell");
+  if (!lc) throw std::runtime_error("no <LinkedCell>");
+  double maxc[3] = {lc->attrD("MX"), lc->attrD("MY"), lc->attrD("MZ")};
+  double org[3] = {0., 0., 0.};
+  if (XmlNode const* o = cons->child("Origin")) {
+    org[0] = o->attrD("OX"); org[1] = o->attrD("OY"); org[2] = o->attrD("OZ");
+  }
+  int per[3] = {0, 0, 0};
+  if (XmlNode const* p = cons->child("Periodicity")) {
+    per[0] = p->attrI("PX") == 1; per[1] = p->attrI("PY") == 1; per[2] = p->attrI("PZ") == 1;
+  }
+  double lcf = lc->has("CellSizeFactor") ? lc->attrD("CellSizeFactor") : 1.;
+  if (lcf < 1.) lcf = 1.;
+
+  std::map<std::string, int> mats;
+  std::vector<std::string> morder;
+  // particle classes (Particle::Particle(DOMNode*), Component/src/Particle.cpp:120-160)
+  double maxR = 0.;
+  for (XmlNode const* pn : [&] {
+         std::vector<XmlNode const*> v;
+         if (XmlNode const* ps = cons->child("Particles")) v = ps->childrenNamed("Particle");
+         return v;
+       }()) {
+    TypeDesc t{};
+    double density = pn->attrD("Density");
+    XmlNode const* cv = pn->child("Convex");
+    if (!cv) throw std::runtime_error("<Particle> without <Convex>");
+    t.crust = cv->attrD("CrustThickness");
+    if (!(t.crust > 0.)) throw std::runtime_error("crust thickness must be > 0");
+    if (XmlNode const* sp = cv->child("Sphere")) {
+      double r = sp->attrD("Radius");
+      t.shape = 0;
+      t.radius = r;
+      double vol = 4.0 * PI * std::pow(r, 3.) / 3.0;                  // Sphere::getVolume
+      t.mass = density * vol;
+      double I0 = 8.0 * PI * std::pow(r, 5.) / 15.0;                  // Sphere::BuildInertia
+      t.inertia[0] = t.inertia[1] = t.inertia[2] = I0 * density;
+      t.eqrad = std::pow((0.75 / PI) * vol, 1. / 3.);                 // getEquivalentSphereRadius
+    } else {
+      throw std::runtime_error("unsupported particle shape in <Convex>");
+    }
+    XmlNode const* mat = pn->child("Material");
+    if (!mat) throw std::runtime_error("<Particle> without <Material>");
+    t.mat = materialIndex(mats, morder, mat->valueS());
+    t.r_hi = (float)t.radius;
+    t.r_lo = (float)(t.radius - (double)t.r_hi);
+    maxR = std::max(maxR, t.radius);
+    I.types.push_back(t);
+  }
+  if (I.types.empty()) throw std::runtime_error("no <Particle> class");
+  // obstacles: boxes with identity orientation
+  if (XmlNode const* obs = cons->child("Obstacles")) {
+    std::vector<XmlNode const*> list;
+    collectObstacles(obs, list);
+    for (XmlNode const* on : list) {
+      WallDesc w{};
+      XmlNode const* cv = on->child("Convex");
+      if (!cv) throw std::runtime_error("<Obstacle> without <Convex>");
+      w.crust = cv->attrD("CrustThickness");
+      XmlNode const* bx = cv->child("Box");
+      if (!bx) throw std::runtime_error("only <Box> obstacles are supported");
+      w.extent[0] = 0.5 * bx->attrD("LX");
+      w.extent[1] = 0.5 * bx->attrD("LY");
+      w.extent[2] = 0.5 * bx->attrD("LZ");
+      XmlNode const* ce = on->child("Centre");
+      if (!ce) throw std::runtime_error("<Obstacle> without <Centre>");
+      w.centre[0] = ce->attrD("X"); w.centre[1] = ce->attrD("Y"); w.centre[2] = ce->attrD("Z");
+      if (XmlNode const* ap = on->child("AngularPosition"))
+        if (ap->has("Type") && ap->attr("Type") != "Identity")
+          throw std::runtime_error("only Identity obstacle orientation is supported");
+      XmlNode const* mat = on->child("Material");
+      if (!mat) throw std::runtime_error("<Obstacle> without <Material>");
+      w.mat = materialIndex(mats, morder, mat->valueS());
+      double vol = 8. * w.extent[0] * w.extent[1] * w.extent[2];
+      w.eqrad = std::pow((0.75 / PI) * vol, 1. / 3.);
+      w.id = (int)I.walls.size();
+      I.walls.push_back(w);
+    }
+  }
+  I.nmat = (int)morder.size();
+  // contact force models keyed by the material pair
+  std::map<int, ModelDesc> bymask;
+  if (XmlNode const* cfm = cons->child("ContactForceModels")) {
+    for (auto const& c : cfm->children) {
+      int mask = 0;
+      if (c->name != "Default") {
+        XmlNode const* m = c->child("Material");
+        if (!m) throw std::runtime_error("<ContactForceModel> without <Material>");
+        int a = materialIndex(mats, morder, m->attr("materialA"));
+        int b = materialIndex(mats, morder, m->attr("materialB"));
+        mask = (1 << a) | (1 << b);
+      }
+      bool found = false;
+      for (auto const& law : c->children) {
+        if (law->name == "HookeMemory" || law->name == "Hooke") {
+          bymask[mask] = readModel(law.get(), law->name);
+          found = true;
+        } else if (law->name == "Hertz" || law->name == "HertzMemory") {
+          throw std::runtime_error("Hertz contact models are not supported");
+        }
+      }
+      if (!found) throw std::runtime_error("<ContactForceModel> without a known law");
+    }
+  }
+  I.nmat = (int)morder.size();
+  for (int a = 0; a < kMaxMat; ++a)
+    for (int b = 0; b < kMaxMat; ++b) {
+      ModelDesc m{};
+      if (a < I.nmat && b < I.nmat) {
+        auto it = bymask.find((1 << a) | (1 << b));
+        if (it != bymask.end()) m = it->second;
+      }
+      I.models[a * kMaxMat + b] = m;
+    }
+  for (auto const& t : I.types) {
+    for (auto const& t2 : I.types)
+      if (!I.models[t.mat * kMaxMat + t2.mat].valid)
+        throw std::runtime_error("no contact force model for a particle material pair");
+    for (auto const& w : I.walls)
+      if (!I.models[t.mat * kMaxMat + w.mat].valid)
+        throw std::runtime_error("no contact force model for a particle/obstacle material pair");
+  }
+  for (auto const& t : I.types)
+    if (!I.models[t.mat * kMaxMat + t.mat].memory)
+      throw std::runtime_error("only HookeMemory is implemented on the device");
+  // gravity and time step
+  I.gravity[0] = I.gravity[1] = I.gravity[2] = 0.;
+  if (XmlNode const* fo = root->find("Forces"))
+    if (XmlNode const* g = fo->child("Gravity")) {
+      I.gravity[0] = g->attrD("GX"); I.gravity[1] = g->attrD("GY"); I.gravity[2] = g->attrD("GZ");
+    }
+  XmlNode const* ts = root->find("TimeStep");
+  if (!ts) throw std::runtime_error("no <TimeStep>");
+  I.dt = ts->attrD("dt");
+  for (auto& t : I.types)
+    for (int d = 0; d < 3; ++d) t.weight[d] = I.gravity[d] * (t.mass * (1. - 0. / 1.));
+  // linked cell grid (LinkedCell::set, Base/src/LinkedCell.cpp:47-160)
+  double cellsize = 2. * (lcf * maxR);
+  GridDesc& g = I.grid;
+  for (int d = 0; d < 3; ++d) {
+    double size = maxc[d] - org[d];
+    int n = (int)((size + 1.0e-10) / cellsize);
+    if (!n) n = 1;
+    g.nb[d] = n;
+    g.edge[d] = size / n;
+    g.lc_origin[d] = org[d];
+    g.L[d] = size;
+    g.periodic[d] = per[d];
+    if (per[d]) {
+      if (n < 3) throw std::runtime_error("a periodic direction needs at least 3 cells");
+      g.lc_origin[d] += -g.edge[d];
+      g.nb[d] += 2;
+    }
+    g.edge_hi[d] = (float)g.edge[d];
+    g.edge_lo[d] = (float)(g.edge[d] - (double)g.edge_hi[d]);
+  }
+  return I;
+}
+
+// ---------------------------------------------------------------- system --
+struct System {
+  int precision = GDEM_FP64;
+  std::vector<InstanceDesc> inst;
+  std::vector<int> type_base;     // first global type of each instance
+  std::vector<int> id_base;       // first particle ID of each instance
+  std::vector<int> inst_n;
+  DevState S{};
+  GridDesc* d_grids = nullptr; TypeDesc* d_types = nullptr; ModelDesc* d_models = nullptr;
+  WallDesc* d_walls = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool have_state = false, started = false, diag = false, use_graphs = true;
+  double last_ms = 0.;
+  int status_host = 0;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  long parity = 0;                 // buffer swaps so far (state and history swap together)
+  long graph_parity = 0;           // parity at which graph[0] was captured
+  std::vector<void*> allocs;
+  double* d_stage = nullptr;       // AoS staging, ID order (x v w wbf q F T: 22 doubles/particle)
+  int* d_type_id = nullptr;        // particle class by ID
+  int* d_inst_id = nullptr;        // instance by ID
+  double* d_vstats = nullptr;      // velocity statistics: partials + result
+  // per-kernel CUDA-event timing
+  bool profiling = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evpool;
+  size_t evused = 0;
+  std::vector<std::pair<int, size_t>> pending;
+  std::vector<std::string> knames;
+  std::vector<double> ktotal;
+  std::vector<long> kcount;
+
+  ~System() { release(); }
+  void release() {
+    for (auto& gx : graph) if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
+    for (void* p : allocs) cudaFree(p);
+    allocs.clear();
+    if (d_grids) cudaFree(d_grids);
+    if (d_types) cudaFree(d_types);
+    if (d_models) cudaFree(d_models);
+    if (d_walls) cudaFree(d_walls);
+    d_grids = nullptr; d_types = nullptr; d_models = nullptr; d_walls = nullptr;
+    for (auto& e : evpool) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+    evpool.clear();
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    ev0 = ev1 = nullptr;
+    if (stream) cudaStreamDestroy(stream);
+    stream = nullptr;
+  }
+  template <typename T>
+  T* alloc(size_t n) {
+    T* p = dalloc<T>(n);
+    allocs.push_back(p);
+    return p;
+  }
+  void invalidateGraphs() {
+    for (auto& gx : graph) if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
+  }
+
+  // Runs f between two events when profiling (plain launches only).
+  template <typename Fn>
+  void timed(const char* name, Fn&& f) {
+    if (!profiling) { f(); return; }
+    if (evused == evpool.size()) {
+      cudaEvent_t a, b;
+      CK(cudaEventCreate(&a));
+      CK(cudaEventCreate(&b));
+      evpool.push_back({a, b});
+    }
+    size_t e = evused++;
+    int k = 0;
+    while (k < (int)knames.size() && knames[k] != name) ++k;
+    if (k == (int)knames.size()) { knames.push_back(name); ktotal.push_back(0.); kcount.push_back(0); }
+    CK(cudaEventRecord(evpool[e].first, stream));
+    f();
+    CK(cudaEventRecord(evpool[e].second, stream));
+    pending.push_back({k, e});
+  }
+  void collectTimes() {
+    if (pending.empty()) return;
+    CK(cudaStreamSynchronize(stream));
+    for (auto& p : pending) {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, evpool[p.second].first, evpool[p.second].second));
+      ktotal[p.first] += ms;
+      kcount[p.first] += 1;
+    }
+    pending.clear();
+    evused = 0;
+  }
+
+  void setupTables() {
+    std::vector<GridDesc> grids;
+    std::vector<TypeDesc> types;
+    std::vector<ModelDesc> models;
+    std::vector<WallDesc> walls;
+    int cell_offset = 0, max_walls = 1;
+    for (auto& I : inst) {
+      GridDesc g = I.grid;
+      g.cell_offset = cell_offset;
+      cell_offset += g.nb[0] * g.nb[1] * g.nb[2];
+      g.wall_begin = (int)walls.size();
+      g.wall_count = (int)I.walls.size();
+      g.model_base = (int)models.size();
+      type_base.push_back((int)types.size());
+      for (auto const& t : I.types) types.push_back(t);
+      for (auto const& w : I.walls) walls.push_back(w);
+      for (int k = 0; k < kMaxMat * kMaxMat; ++k) models.push_back(I.models[k]);
+      max_walls = std::max(max_walls, (int)I.walls.size());
+      grids.push_back(g);
+    }
+    S.ncells = cell_offset;
+    S.ninst = (int)inst.size();
+    S.max_walls = max_walls;
+    S.dt = inst[0].dt;
+    for (auto& I : inst)
+      if (I.dt != S.dt) throw std::runtime_error("all instances of a batch must share dt");
+    auto up = [&](auto*& dst, auto const& vec) {
+      using T = typename std::remove_reference<decltype(vec)>::type::value_type;
+      CK(cudaMalloc(reinterpret_cast<void**>(&dst), std::max<size_t>(1, vec.size()) * sizeof(T)));
+      if (!vec.empty()) CK(cudaMemcpy(dst, vec.data(), vec.size() * sizeof(T), cudaMemcpyHostToDevice));
+    };
+    up(d_grids, grids); up(d_types, types); up(d_models, models); up(d_walls, walls);
+    S.grids = d_grids; S.types = d_types; S.models = d_models; S.walls = d_walls;
+  }
+
+  void allocateParticles(int n) {
+    S.n = n;
+    S.cap = std::max(n, 1);
+    size_t c = (size_t)S.cap;
+    S.id = alloc<int>(c); S.type = alloc<int>(c); S.inst = alloc<int>(c); S.key = alloc<int>(c);
+    S.id2 = alloc<int>(c); S.type2 = alloc<int>(c); S.inst2 = alloc<int>(c);
+    S.x = alloc<double>(3 * c); S.v = alloc<double>(3 * c); S.w = alloc<double>(3 * c);
+    S.wbf = alloc<double>(3 * c); S.q = alloc<double>(4 * c);
+    S.x2 = alloc<double>(3 * c); S.v2 = alloc<double>(3 * c); S.w2 = alloc<double>(3 * c);
+    S.wbf2 = alloc<double>(3 * c); S.q2 = alloc<double>(4 * c);
+    S.F = alloc<double>(3 * c); S.T = alloc<double>(3 * c);
+    S.basis = nullptr; S.basis2 = nullptr;
+    S.skey = alloc<int>(c); S.rank = alloc<int>(c); S.order = alloc<int>(c);
+    S.cell_count = alloc<int>(S.ncells); S.cell_start = alloc<int>(S.ncells);
+    S.scan_tmp = alloc<int>((S.ncells + 1023) / 1024 + 1);
+    S.cellc = alloc<int4>(c);
+    if (precision == GDEM_FP64) {
+      S.pos64 = alloc<double4>(c); S.vel64 = alloc<double4>(c); S.omg64 = alloc<double4>(c);
+      S.offh = nullptr; S.offl = nullptr; S.velf = nullptr; S.omgf = nullptr;
+    } else {
+      S.offh = alloc<float4>(c); S.offl = alloc<float4>(c);
+      S.velf = alloc<float4>(c); S.omgf = alloc<float4>(c);
+      S.pos64 = nullptr; S.vel64 = nullptr; S.omg64 = nullptr;
+    }
+    S.pairs = alloc<int>(c * kPairCap); S.npairs = alloc<int>(c);
+    S.pair_delta = nullptr; S.wall_delta = nullptr; S.diag = 0;
+    int l2 = nextPow2Log((size_t)8 * c + 64);
+    size_t hc = size_t(1) << l2;
+    size_t vsz = precision == GDEM_FP64 ? sizeof(double) : sizeof(float);
+    for (HistTable* t : {&S.hist_old, &S.hist_new}) {
+      t->log2cap = l2;
+      t->keys = alloc<unsigned long long>(hc);
+      t->vals = alloc<char>(hc * 9 * vsz);
+      CK(cudaMemset(t->keys, 0xFF, hc * sizeof(unsigned long long)));
+    }
+    S.status = alloc<int>(1);
+    CK(cudaMemset(S.status, 0, sizeof(int)));
+    CK(cudaMemset(S.F, 0, 3 * c * sizeof(double)));
+    CK(cudaMemset(S.T, 0, 3 * c * sizeof(double)));
+    d_stage = alloc<double>(22 * c);
+    d_type_id = alloc<int>(c);
+    d_inst_id = alloc<int>(c);
+    d_vstats = alloc<double>(2 * ((c + 255) / 256) + 2);
+  }
+
+  // Host AoS arrays (by ID) -> staging -> SoA state in ID order.
+  void loadState(const double* x, const double* v, const double* w, const double* wbf,
+                 const double* q, const double* F, const double* T) {
+    size_t n = (size_t)S.n;
+    double* st = d_stage;
+    double *dx = st, *dv = st + 3 * n, *dw = st + 6 * n, *dwb = st + 9 * n, *dq = st + 12 * n,
+           *dF = st + 16 * n, *dT = st + 19 * n;
+    auto cp = [&](double* d, const double* h, size_t k) {
+      if (h) CK(cudaMemcpyAsync(d, h, k * n * sizeof(double), cudaMemcpyHostToDevice, stream));
+    };
+    cp(dx, x, 3); cp(dv, v, 3); cp(dw, w, 3); cp(dwb, wbf, 3); cp(dq, q, 4); cp(dF, F, 3); cp(dT, T, 3);
+    launch_load_state(S, dx, dv, dw, wbf ? dwb : nullptr, dq, F ? dF : nullptr, T ? dT : nullptr,
+                      d_type_id, d_inst_id, stream);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream));
+  }
+
+  void swapState() {
+    std::swap(S.id, S.id2); std::swap(S.type, S.type2); std::swap(S.inst, S.inst2);
+    std::swap(S.x, S.x2); std::swap(S.v, S.v2); std::swap(S.w, S.w2);
+    std::swap(S.wbf, S.wbf2); std::swap(S.q, S.q2); std::swap(S.basis, S.basis2);
+  }
+  void swapHist() { std::swap(S.hist_old, S.hist_new); }
+  void swapBoth() { swapState(); swapHist(); ++parity; }
+
+  // Sort into cell order (after k_move or k_bin) and build the pair list.
+  void binAndPairs() {
+    timed("scan", [&] { launch_scan(S, stream); });
+    timed("place", [&] { launch_place(S, stream); });
+    timed("cellsort", [&] { launch_cellsort(S, stream); });
+    timed("gather", [&] { launch_gather(S, stream); });
+    swapState();
+    ++parity;
+    if (precision == GDEM_FP64) timed("pairs64", [&] { launch_pairs64(S, stream); });
+    else timed("pairs32", [&] { launch_pairs32(S, stream); });
+  }
+  void forces() {
+    size_t hc = size_t(1) << S.hist_new.log2cap;
+    timed("hist_clear", [&] {
+      CK(cudaMemsetAsync(S.hist_new.keys, 0xFF, hc * sizeof(unsigned long long), stream));
+    });
+    if (precision == GDEM_FP64) timed("forces64", [&] { launch_forces64(S, stream); });
+    else timed("forces32", [&] { launch_forces32(S, stream); });
+    swapHist();
+  }
+  // One full step; pre_kick applies the previous step's closing kick first.
+  void stepBody(bool pre_kick) {
+    double dt = S.dt;
+    timed("cell_clear", [&] {
+      CK(cudaMemsetAsync(S.cell_count, 0, (size_t)S.ncells * sizeof(int), stream));
+    });
+    timed("move", [&] { launch_move(S, 0.5 * dt, dt, pre_kick ? 1 : 0, 0.5 * dt, stream); });
+    binAndPairs();
+    forces();
+  }
+  void init() {
+    CK(cudaMemsetAsync(S.cell_count, 0, (size_t)S.ncells * sizeof(int), stream));
+    launch_bin(S, stream);
+    binAndPairs();
+    forces();
+    launch_hist_zero_cumulative(S.hist_old, precision == GDEM_FP64, stream);
+    CK(cudaStreamSynchronize(stream));
+    collectTimes();
+    started = true;
+  }
+  void captureGraphs() {
+    invalidateGraphs();
+    for (int k = 0; k < 2; ++k) {
+      cudaGraph_t gph;
+      CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      stepBody(true);
+      CK(cudaStreamEndCapture(stream, &gph));
+      CK(cudaGraphInstantiate(&graph[k], gph, 0));
+      CK(cudaGraphDestroy(gph));
+    }
+    // capturing advanced the host-side buffer parity by two: back where it was
+    graph_parity = parity - 2;
+  }
+  void step(int nsteps) {
+    if (nsteps <= 0) return;
+    CK(cudaEventRecord(ev0, stream));
+    stepBody(false);
+    int rest = nsteps - 1;
+    if (rest > 0) {
+      if (use_graphs && !diag && !profiling) {
+        if (!graph[0]) captureGraphs();
+        int g = (int)((parity - graph_parity) & 1);
+        for (int k = 0; k < rest; ++k) { CK(cudaGraphLaunch(graph[g], stream)); g ^= 1; }
+        if (rest & 1) { swapBoth(); parity += rest - 1; }
+        else parity += rest;
+      } else {
+        for (int k = 0; k < rest; ++k) stepBody(true);
+      }
+    }
+    timed("kick", [&] { launch_kick(S, 0.5 * S.dt, stream); });
+    CK(cudaEventRecord(ev1, stream));
+    CK(cudaGetLastError());
+    CK(cudaEventSynchronize(ev1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ev0, ev1));
+    last_ms = ms;
+    collectTimes();
+  }
+  int readStatus() {
+    int st = 0;
+    CK(cudaMemcpy(&st, S.status, sizeof(int), cudaMemcpyDeviceToHost));
+    status_host |= st;
+    return status_host;
+  }
+};
+
+System* sys(gdem_handle h) { return reinterpret_cast<System*>(h); }
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    return f();
+  } catch (CudaError const& e) {
+    g_last_error = e.what();
+    return GDEM_ERR_CUDA;
+  } catch (std::exception const& e) {
+    g_last_error = e.what();
+    return GDEM_ERR_INVALID;
+  }
+}
+
+}  // namespace
+}  // namespace gdem
+
+using namespace gdem;
+
+extern "C" {
+
+const char* gdem_last_error(void) { return g_last_error.c_str(); }
+
+int gdem_create_batch(int n, const char* const* xml_paths, int precision, gdem_handle* out) {
+  return guarded([&] {
+    if (!out || n <= 0 || !xml_paths) throw std::runtime_error("invalid arguments");
+    if (precision != GDEM_FP64 && precision != GDEM_FP32_SPLIT)
+      throw std::runtime_error("unknown precision mode");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+      throw CudaError("no CUDA device: the Grains3D B200 step has no CPU fallback");
+    auto s = std::make_unique<System>();
+    s->precision = precision;
+    for (int k = 0; k < n; ++k) s->inst.push_back(readInstance(xml_paths[k]));
+    s->setupTables();
+    CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&s->ev0));
+    CK(cudaEventCreate(&s->ev1));
+    *out = reinterpret_cast<gdem_handle>(s.release());
+    return GDEM_OK;
+  });
+}
+
+int gdem_create(const char* xml_path, int precision, gdem_handle* out) {
+  const char* paths[1] = {xml_path};
+  return gdem_create_batch(1, paths, precision, out);
+}
+
+int gdem_upload_state(gdem_handle h, int64_t n, const int* inst, const int* type,
+                      const double* x, const double* v, const double* w, const double* wbf,
+                      const double* q) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || n <= 0 || n >= (int64_t(1) << 27) || !type || !x || !v || !w || !q)
+      throw std::runtime_error("invalid arguments");
+    if (s->have_state) throw std::runtime_error("state already uploaded");
+    int N = (int)n;
+    std::vector<int> hinst(N, 0), htype(N), hid(N);
+    s->inst_n.assign(s->inst.size(), 0);
+    for (int i = 0; i < N; ++i) {
+      int k = inst ? inst[i] : 0;
+      if (k < 0 || k >= (int)s->inst.size()) throw std::runtime_error("instance index out of range");
+      if (type[i] < 0 || type[i] >= (int)s->inst[k].types.size())
+        throw std::runtime_error("particle type out of range");
+      if (i > 0 && k < hinst[i - 1]) throw std::runtime_error("particles must be grouped by instance");
+      hinst[i] = k;
+      htype[i] = s->type_base[k] + type[i];
+      hid[i] = i;
+      s->inst_n[k]++;
+    }
+    s->id_base.assign(s->inst.size(), 0);
+    for (size_t k = 1; k < s->inst.size(); ++k) s->id_base[k] = s->id_base[k - 1] + s->inst_n[k - 1];
+    s->allocateParticles(N);
+    DevState& S = s->S;
+    (void)hid;
+    CK(cudaMemcpy(s->d_type_id, htype.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s->d_inst_id, hinst.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+    (void)S;
+    s->loadState(x, v, w, wbf, q, nullptr, nullptr);
+    s->have_state = true;
+    return GDEM_OK;
+  });
+}
+
+int gdem_upload_forces(gdem_handle h, const double* F, const double* T) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state || !F || !T) throw std::runtime_error("upload the state first");
+    if (s->started) throw std::runtime_error("forces can only be set before the first step");
+    // the state is still in ID order: copy F and T through the staging area
+    DevState& S = s->S;
+    size_t n = (size_t)S.n, c = (size_t)S.cap;
+    std::vector<double> hF(3 * c), hT(3 * c);
+    for (int d = 0; d < 3; ++d)
+      for (size_t i = 0; i < n; ++i) { hF[d * c + i] = F[3 * i + d]; hT[d * c + i] = T[3 * i + d]; }
+    CK(cudaMemcpy(S.F, hF.data(), 3 * c * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(S.T, hT.data(), 3 * c * sizeof(double), cudaMemcpyHostToDevice));
+    s->started = true;
+    return GDEM_OK;
+  });
+}
+
+int gdem_set_state(gdem_handle h, const double* x, const double* v, const double* w,
+                   const double* wbf, const double* q, const double* F, const double* T) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state || !x || !v || !w || !q)
+      throw std::runtime_error("gdem_set_state needs an uploaded system and x, v, w, q");
+    if ((F == nullptr) != (T == nullptr)) throw std::runtime_error("give both F and T, or neither");
+    s->loadState(x, v, w, wbf, q, F, T);
+    s->started = F != nullptr;
+    return GDEM_OK;
+  });
+}
+
+int gdem_velocity_stats(gdem_handle h, double* vmax, double* vmean) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state) throw std::runtime_error("no state");
+    DevState& S = s->S;
+    int nb = (S.n + 255) / 256;
+    double* out = s->d_vstats + 2 * nb;
+    launch_vstats(S, s->d_vstats, out, s->stream);
+    double r[2];
+    CK(cudaMemcpyAsync(r, out, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    if (vmax) *vmax = r[0];
+    if (vmean) *vmean = r[1];
+    return GDEM_OK;
+  });
+}
+
+int gdem_pair_counts(gdem_handle h, int64_t* entries, int64_t* contacts) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->started) throw std::runtime_error("no force evaluation yet");
+    unsigned long long* d = reinterpret_cast<unsigned long long*>(s->d_vstats);
+    launch_pair_counts(s->S, d, s->stream);
+    unsigned long long r[2];
+    CK(cudaMemcpyAsync(r, d, sizeof(r), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    if (entries) *entries = (int64_t)r[0];
+    if (contacts) *contacts = (int64_t)r[1];
+    return GDEM_OK;
+  });
+}
+
+int gdem_set_profiling(gdem_handle h, int on) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s) throw std::runtime_error("invalid handle");
+    s->profiling = on != 0;
+    s->knames.clear(); s->ktotal.clear(); s->kcount.clear();
+    return GDEM_OK;
+  });
+}
+
+int gdem_kernel_times(gdem_handle h, int capacity, int* count, char* names, double* total_ms,
+                      int64_t* launches) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !count) throw std::runtime_error("invalid arguments");
+    *count = (int)s->knames.size();
+    for (int k = 0; k < *count && k < capacity; ++k) {
+      if (names) {
+        std::memset(names + 32 * k, 0, 32);
+        std::strncpy(names + 32 * k, s->knames[k].c_str(), 31);
+      }
+      if (total_ms) total_ms[k] = s->ktotal[k];
+      if (launches) launches[k] = s->kcount[k];
+    }
+    return GDEM_OK;
+  });
+}
+
+int gdem_upload_history(gdem_handle h, int64_t n, const int* owner, const int* partner,
+                        const double* kdelta, const double* prevn, const double* spring) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state || n < 0) throw std::runtime_error("upload the state first");
+    DevState& S = s->S;
+    HistTable& t = S.hist_old;   // read by the next force evaluation
+    size_t hc = size_t(1) << t.log2cap;
+    std::vector<unsigned long long> keys(hc, kEmptyKey);
+    bool fp64 = s->precision == GDEM_FP64;
+    std::vector<double> vd(fp64 ? 9 * hc : 0);
+    std::vector<float> vf(fp64 ? 0 : 9 * hc);
+    for (int64_t e = 0; e < n; ++e) {
+      int a = owner[e], b = partner[e];
+      unsigned long long key;
+      if (b >= 0) {
+        if (!(a < b)) continue;   // the lower ID's view is stored
+        key = pairKey(a, b);
+      } else {
+        key = wallKey(a, -b - 2);
+      }
+      uint32_t slot = hashSlot(key, t.log2cap);
+      while (keys[slot] != kEmptyKey) slot = (slot + 1) & (uint32_t)(hc - 1);
+      keys[slot] = key;
+      double vals[9] = {kdelta[3 * e], kdelta[3 * e + 1], kdelta[3 * e + 2],
+                        prevn[3 * e], prevn[3 * e + 1], prevn[3 * e + 2],
+                        spring ? spring[3 * e] : 0., spring ? spring[3 * e + 1] : 0.,
+                        spring ? spring[3 * e + 2] : 0.};
+      for (int k = 0; k < 9; ++k) {
+        if (fp64) vd[9 * slot + k] = vals[k];
+        else vf[9 * slot + k] = (float)vals[k];
+      }
+    }
+    CK(cudaMemcpy(t.keys, keys.data(), hc * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+    if (fp64) CK(cudaMemcpy(t.vals, vd.data(), vd.size() * sizeof(double), cudaMemcpyHostToDevice));
+    else CK(cudaMemcpy(t.vals, vf.data(), vf.size() * sizeof(float), cudaMemcpyHostToDevice));
+    return GDEM_OK;
+  });
+}
+
+int gdem_init(gdem_handle h) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state) throw std::runtime_error("upload the state first");
+    s->invalidateGraphs();
+    s->init();
+    s->readStatus();
+    return GDEM_OK;
+  });
+}
+
+int gdem_step(gdem_handle h, int nsteps) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state) throw std::runtime_error("upload the state first");
+    if (!s->started) throw std::runtime_error("call gdem_init (or gdem_upload_forces) before stepping");
+    s->step(nsteps);
+    s->readStatus();
+    return GDEM_OK;
+  });
+}
+
+int gdem_download_state(gdem_handle h, double* x, double* v, double* w, double* wbf, double* q,
+                        double* F, double* T) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state) throw std::runtime_error("no state");
+    DevState& S = s->S;
+    size_t n = (size_t)S.n;
+    double* st = s->d_stage;
+    double* dx = st; double* dv = st + 3 * n; double* dw = st + 6 * n; double* dwb = st + 9 * n;
+    double* dq = st + 12 * n; double* dF = st + 16 * n; double* dT = st + 19 * n;
+    launch_scatter_by_id(S, x ? dx : nullptr, v ? dv : nullptr, w ? dw : nullptr,
+                         wbf ? dwb : nullptr, q ? dq : nullptr, F ? dF : nullptr,
+                         T ? dT : nullptr, 0, s->stream);
+    CK(cudaGetLastError());
+    struct { double* h; double* d; size_t k; } items[] = {
+        {x, dx, 3}, {v, dv, 3}, {w, dw, 3}, {wbf, dwb, 3}, {q, dq, 4}, {F, dF, 3}, {T, dT, 3}};
+    for (auto& it : items)
+      if (it.h) CK(cudaMemcpyAsync(it.h, it.d, it.k * n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return GDEM_OK;
+  });
+}
+
+int gdem_download_cells(gdem_handle h, int* ijk) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->started || !ijk) throw std::runtime_error("no binned state");
+    DevState& S = s->S;
+    int* d = reinterpret_cast<int*>(s->d_stage);
+    launch_cells_by_id(S, d, 0, s->stream);
+    CK(cudaMemcpyAsync(ijk, d, 3 * (size_t)S.n * sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return GDEM_OK;
+  });
+}
+
+int gdem_set_diagnostics(gdem_handle h, int on) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state) throw std::runtime_error("upload the state first");
+    DevState& S = s->S;
+    if (on && !S.pair_delta) {
+      S.pair_delta = s->alloc<float>((size_t)S.cap * kPairCap);
+      S.wall_delta = s->alloc<double>((size_t)S.cap * S.max_walls);
+    }
+    S.diag = on ? 1 : 0;
+    s->diag = on != 0;
+    s->invalidateGraphs();
+    return GDEM_OK;
+  });
+}
+
+int gdem_download_contacts(gdem_handle h, int64_t capacity, int64_t* count, int* id0, int* id1,
+                           double* delta) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->started || !count) throw std::runtime_error("invalid arguments");
+    DevState& S = s->S;
+    if (!S.pair_delta) throw std::runtime_error("enable diagnostics before the step");
+    size_t n = (size_t)S.n;
+    std::vector<int> ids(n), np(n), pairs(n * kPairCap);
+    std::vector<float> pd(n * kPairCap);
+    std::vector<double> wd(n * S.max_walls);
+    std::vector<int4> cells(n);
+    CK(cudaMemcpy(ids.data(), S.id, n * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(np.data(), S.npairs, n * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(pairs.data(), S.pairs, n * kPairCap * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(pd.data(), S.pair_delta, n * kPairCap * sizeof(float), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(wd.data(), S.wall_delta, n * S.max_walls * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(cells.data(), S.cellc, n * sizeof(int4), cudaMemcpyDeviceToHost));
+    int64_t c = 0;
+    for (size_t t = 0; t < n; ++t) {
+      for (int e = 0; e < np[t]; ++e) {
+        int u = pairs[t * kPairCap + e] & ((1 << 27) - 1);
+        float dl = pd[t * kPairCap + e];
+        if (!(dl < 0.f) || !(ids[t] < ids[u])) continue;
+        if (c < capacity && id0) { id0[c] = ids[t]; id1[c] = ids[u]; delta[c] = dl; }
+        ++c;
+      }
+      int nw = s->inst[cells[t].w].walls.size();
+      for (int k = 0; k < nw; ++k) {
+        double dl = wd[t * S.max_walls + k];
+        if (!(dl < 0.)) continue;
+        if (c < capacity && id0) { id0[c] = ids[t]; id1[c] = -(k + 2); delta[c] = dl; }
+        ++c;
+      }
+    }
+    *count = c;
+    return GDEM_OK;
+  });
+}
+
+int gdem_status(gdem_handle h, int* bits, int reset) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !bits) throw std::runtime_error("invalid arguments");
+    if (s->have_state) s->readStatus();
+    *bits = s->status_host;
+    if (reset) {
+      s->status_host = 0;
+      if (s->have_state) CK(cudaMemset(s->S.status, 0, sizeof(int)));
+    }
+    return GDEM_OK;
+  });
+}
+
+int gdem_grid(gdem_handle h, int k, int* nb, double* edge, double* origin) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || k < 0 || k >= (int)s->inst.size()) throw std::runtime_error("invalid arguments");
+    GridDesc const& g = s->inst[k].grid;
+    for (int d = 0; d < 3; ++d) {
+      if (nb) nb[d] = g.nb[d];
+      if (edge) edge[d] = g.edge[d];
+      if (origin) origin[d] = g.lc_origin[d];
+    }
+    return GDEM_OK;
+  });
+}
+
+int64_t gdem_num_particles(gdem_handle h) {
+  System* s = sys(h);
+  return s && s->have_state ? s->S.n : 0;
+}
+
+double gdem_last_step_ms(gdem_handle h) {
+  System* s = sys(h);
+  return s ? s->last_ms : 0.;
+}
+
+int gdem_use_graphs(gdem_handle h, int on) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s) throw std::runtime_error("invalid handle");
+    s->use_graphs = on != 0;
+    s->invalidateGraphs();
+    return GDEM_OK;
+  });
+}
+
+void gdem_destroy(gdem_handle h) { delete sys(h); }
+
+}  // extern "C"

@@ -1,0 +1,77 @@
+// gdem_types.h -- plain-old-data descriptors shared by the host runtime and
+// the sm_100a kernels of the Grains3D DEM step.
+#pragma once
+#include <stdint.h>
+
+namespace gdem {
+
+// Maximum number of candidate partners recorded per particle in the
+// per-particle segment of the pair list.
+constexpr int kPairCap = 32;
+// Material indices per instance (materials are bits in the reference,
+// ContactBuilderFactory.cpp:176-192; here they are indices 0..kMaxMat-1).
+constexpr int kMaxMat = 8;
+
+// Error bits reported through the device status word.  They replace the
+// reference's C++ exceptions (Base/include/Error.hh): ContactError,
+// MotionError, SimulationError; plus the capacity checks of this runtime.
+enum StatusBits : int {
+  kErrContactOverlap = 1 << 0,   // overlap >= sum of crusts (ContactError)
+  kErrMotion = 1 << 1,           // |dx| > crust over one step (MotionError)
+  kErrOutOfGrid = 1 << 2,        // particle outside the linked-cell grid (SimulationError)
+  kErrHashFull = 1 << 3,         // contact-history table has no free slot
+  kErrGjkMaxIter = 1 << 4,       // GJK hit its iteration cap
+  kErrTimeout = 1 << 5,          // a bounded device wait gave up
+  kErrPairsFull = 1 << 6,        // a particle has more than kPairCap candidates
+};
+
+// One independent simulation ("instance").  A single Grains3D system is a
+// batch of one.  Cell numbering follows LinkedCell::getCellNumber
+// (Base/src/LinkedCell.cpp:1165-1168): j * nbk * nbi + k * nbi + i.
+struct GridDesc {
+  double lc_origin[3];   // linked-cell origin (shifted by one cell where periodic)
+  double edge[3];        // cell edge lengths
+  double L[3];           // domain size: the periodic translation vector
+  int nb[3];             // cells per direction (incl. the 2 periodic layers)
+  int periodic[3];
+  int cell_offset;       // first global cell key of this instance
+  int wall_begin, wall_count;
+  int model_base;        // first entry of this instance in the model table
+  int pad0;
+  float edge_hi[3], edge_lo[3];   // edge as a float-float pair
+};
+
+// Particle class (a <Particle> node of the XML input).
+struct TypeDesc {
+  double radius;         // circumscribed radius
+  double crust;          // crust thickness
+  double mass;
+  double inertia[3];     // body-fixed principal inertia (inertia[0], [3], [5] of the reference)
+  double eqrad;          // Component::getEquivalentSphereRadius
+  double weight[3];      // m (1 - rho_f / rho) g
+  int mat;               // material index
+  int shape;             // 0 sphere, 1 box, 2 cylinder, 3 polyhedron
+  float r_hi, r_lo;      // radius as a float-float pair
+};
+
+// HookeMemory / Hooke parameters (HookeMemoryContactForceModel.cpp:12-27).
+struct ModelDesc {
+  double kn, en, etat, muc, kt, mur, etarpf, epst;
+  double beta;           // ln(en) / sqrt(pi^2 + ln^2(en))
+  int rolling;           // mur != 0
+  int memory;            // 1 HookeMemory, 0 Hooke (no tangential history)
+  int valid;
+  int pad;
+};
+
+// Axis-aligned box obstacle (SimpleObstacle with a Box convex).
+struct WallDesc {
+  double centre[3];
+  double extent[3];      // half lengths
+  double crust;
+  double eqrad;
+  int mat;
+  int id;                // obstacle index within its instance
+};
+
+}  // namespace gdem

@@ -1,0 +1,238 @@
+"""Seeded synthetic inputs for the Grains3D DEM step, written as Grains3D XML
+(the reference's input format) plus the initial particle state.
+
+The workloads follow the configurations the DEM step is measured on:
+
+* ``settling_box``   - monodisperse spheres settling in a closed box with six
+  planar walls (1,000 spheres, r = 1 mm, box 0.03 x 0.03 x 0.06 m, jittered
+  cubic lattice of spacing 2.4 mm, HookeMemory kn = 1e4, en = 0.7, etat = 0,
+  muc = 0.5, kt = 2/7 kn, dt = 1e-5 s).
+* ``periodic_gas``   - polydisperse spheres (r uniform in [0.8, 1.2] mm,
+  quantised to 256 radius classes) in a triply periodic cube at solid
+  fraction ~0.45, Maxwellian velocities (sigma = 0.1 m/s), no gravity,
+  HookeMemory kn = 1e5, en = 0.9, muc = 0.3, kt = 2/7 kn, dt = 5e-6 s.  Random
+  sequential insertion jams near 0.38, so the positions are an FCC lattice of
+  nearest-neighbour spacing 2.392 mm (n_fcc^3 * 4 sites) with radii redrawn
+  until every lattice-neighbour pair has a gap; n_fcc = 63 gives the
+  1,000,000-particle case (188 sites dropped at random).
+* ``batched_boxes``  - independent closed-box settling instances with their
+  own particle counts, radii and contact parameters.
+* ``adjoint_box``    - 4,096 spheres in a 0.02 x 0.02 x 0.08 m box on an FCC
+  lattice of 2.1 mm spacing with uniform +-0.2 m/s velocities.
+
+All are deterministic functions of their seed.  The crust thickness, which
+Grains3D requires, is 0.1 x radius.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+
+def _f(v) -> str:
+    """Shortest round-trip decimal form of a float."""
+    return repr(float(v))
+
+
+@dataclass
+class Scenario:
+    name: str
+    origin: tuple
+    maxc: tuple
+    periodic: tuple
+    gravity: tuple
+    dt: float
+    # particle classes: dicts with radius, crust, density, material
+    types: list
+    # walls: dicts with centre (3), size (LX, LY, LZ), crust, material
+    walls: list
+    # contact models: dicts with matA, matB, kn, en, etat (None = default), muc, kt
+    models: list
+    type: np.ndarray = field(repr=False)
+    x: np.ndarray = field(repr=False)
+    v: np.ndarray = field(repr=False)
+    w: np.ndarray = field(repr=False)
+    q: np.ndarray = field(repr=False)
+    cell_size_factor: float = 1.0
+
+    @property
+    def n(self) -> int:
+        return len(self.type)
+
+    def counts(self) -> np.ndarray:
+        return np.bincount(self.type, minlength=len(self.types))
+
+    def xml(self) -> str:
+        """Grains3D XML input (Grains3D/Construction/...; Grains.cpp:535-1030)."""
+        ox, oy, oz = self.origin
+        mx, my, mz = self.maxc
+        px, py, pz = (int(p) for p in self.periodic)
+        cnt = self.counts()
+        L = ['<Grains3D Type="Standard">', "  <Construction>",
+             f'    <LinkedCell MX="{_f(mx)}" MY="{_f(my)}" MZ="{_f(mz)}" '
+             f'CellSizeFactor="{_f(self.cell_size_factor)}"/>',
+             f'    <Origin OX="{_f(ox)}" OY="{_f(oy)}" OZ="{_f(oz)}"/>',
+             f'    <Periodicity PX="{px}" PY="{py}" PZ="{pz}"/>',
+             "    <Particles>"]
+        for k, t in enumerate(self.types):
+            L += [f'      <Particle Number="{int(cnt[k])}" Density="{_f(t["density"])}">',
+                  f'        <Convex CrustThickness="{_f(t["crust"])}">',
+                  f'          <Sphere Radius="{_f(t["radius"])}"/>',
+                  "        </Convex>",
+                  '        <AngularPosition Type="Identity"></AngularPosition>',
+                  f'        <Material>{t["material"]}</Material>',
+                  "      </Particle>"]
+        L.append("    </Particles>")
+        if self.walls:
+            L += ["    <Obstacles>", '      <Composite name="Box">']
+            for k, w in enumerate(self.walls):
+                c, s = w["centre"], w["size"]
+                L += [f'        <Obstacle name="Wall{k}">',
+                      f'          <Convex CrustThickness="{_f(w["crust"])}">',
+                      f'            <Box LX="{_f(s[0])}" LY="{_f(s[1])}" LZ="{_f(s[2])}"/>',
+                      "          </Convex>",
+                      f'          <Centre X="{_f(c[0])}" Y="{_f(c[1])}" Z="{_f(c[2])}"/>',
+                      '          <AngularPosition Type="Identity"></AngularPosition>',
+                      f'          <Material>{w["material"]}</Material>',
+                      "        </Obstacle>"]
+            L += ["      </Composite>", "    </Obstacles>"]
+        L.append("    <ContactForceModels>")
+        for m in self.models:
+            L += ["      <ContactForceModel>",
+                  f'        <Material materialA="{m["matA"]}" materialB="{m["matB"]}"/>',
+                  "        <HookeMemory>",
+                  f'          <kn>{_f(m["kn"])}</kn>',
+                  f'          <en>{_f(m["en"])}</en>']
+            if m.get("etat") is not None:
+                L.append(f'          <etat>{_f(m["etat"])}</etat>')
+            L += [f'          <muc>{_f(m["muc"])}</muc>',
+                  f'          <kt>{_f(m["kt"])}</kt>']
+            if m.get("mur"):
+                L.append(f'          <mur>{_f(m["mur"])}</mur>')
+            if m.get("epst") is not None:
+                L.append(f'          <epst>{_f(m["epst"])}</epst>')
+            L += ["        </HookeMemory>", "      </ContactForceModel>"]
+        gx, gy, gz = self.gravity
+        L += ["    </ContactForceModels>", "  </Construction>", "  <Forces>",
+              f'    <Gravity GX="{_f(gx)}" GY="{_f(gy)}" GZ="{_f(gz)}"/>', "  </Forces>",
+              "  <Simulation>",
+              f'    <TimeInterval Start="0." End="{_f(self.dt * 1000)}"/>',
+              f'    <TimeStep dt="{_f(self.dt)}"/>', "  </Simulation>", "</Grains3D>", ""]
+        return "\n".join(L)
+
+    def write_xml(self, path) -> Path:
+        p = Path(path)
+        p.write_text(self.xml())
+        return p
+
+
+def _box_walls(L, thickness, crust, material):
+    """Six axis-aligned walls just outside [0, L] on each face."""
+    Lx, Ly, Lz = L
+    t = thickness
+    walls = []
+    for d in range(3):
+        for side in (0, 1):
+            c = [Lx / 2, Ly / 2, Lz / 2]
+            s = [Lx + 2 * t, Ly + 2 * t, Lz + 2 * t]
+            c[d] = -t / 2 if side == 0 else L[d] + t / 2
+            s[d] = t
+            walls.append(dict(centre=tuple(c), size=tuple(s), crust=crust, material=material))
+    return walls
+
+
+def settling_box(n=1000, seed=1235, box=(0.03, 0.03, 0.06), radius=1.0e-3, spacing=2.4e-3,
+                 jitter=1.0e-4, vmax=0.05, kn=1.0e4, en=0.7, etat=0.0, muc=0.5,
+                 dt=1.0e-5, density=2500.0) -> Scenario:
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = (int(np.floor(b / spacing)) for b in box)
+    if n > nx * ny * nz:
+        raise ValueError("lattice too small")
+    k, j, i = np.unravel_index(np.arange(n), (nz, ny, nx))
+    x = np.stack([(i + 0.5) * spacing, (j + 0.5) * spacing, (k + 0.5) * spacing], axis=1)
+    x = x + rng.uniform(-jitter, jitter, size=x.shape)
+    v = rng.uniform(-vmax, vmax, size=(n, 3))
+    w = np.zeros((n, 3))
+    q = np.zeros((n, 4)); q[:, 3] = 1.0
+    crust = 0.1 * radius
+    types = [dict(radius=radius, crust=crust, density=density, material="matP")]
+    walls = _box_walls(box, 2.0e-3, crust, "matW")
+    kt = 2.0 / 7.0 * kn
+    models = [dict(matA="matP", matB="matP", kn=kn, en=en, etat=etat, muc=muc, kt=kt),
+              dict(matA="matP", matB="matW", kn=kn, en=en, etat=etat, muc=muc, kt=kt)]
+    return Scenario("settling_box", (0.0, 0.0, 0.0), tuple(box), (0, 0, 0), (0.0, 0.0, -9.81), dt,
+                    types, walls, models, np.zeros(n, np.int32), x, v, w, q)
+
+
+def fcc_sites(n_fcc, a):
+    base = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
+    g = np.stack(np.meshgrid(np.arange(n_fcc), np.arange(n_fcc), np.arange(n_fcc),
+                             indexing="ij"), axis=-1).reshape(-1, 3)
+    return ((g[:, None, :] + base[None, :, :]).reshape(-1, 3) + 0.25) * a
+
+
+def periodic_gas(n_fcc=63, n_target=None, seed=1236, spacing=2.392e-3, rmin=0.8e-3,
+                 rmax=1.2e-3, nclasses=256, sigma=0.1, kn=1.0e5, en=0.9, muc=0.3,
+                 dt=5.0e-6, density=2500.0) -> Scenario:
+    """FCC stand-in for the 1M-sphere granular gas (see module docstring)."""
+    rng = np.random.default_rng(seed)
+    a = spacing * np.sqrt(2.0)
+    side = n_fcc * a
+    x = fcc_sites(n_fcc, a)
+    nsite = len(x)
+    if n_target is None:
+        n_target = 1_000_000 if n_fcc == 63 else nsite
+    keep = np.sort(rng.permutation(nsite)[:n_target])
+    x = x[keep]
+    n = len(x)
+    # radius classes; redraw until every lattice-neighbour pair keeps a gap
+    width = (rmax - rmin) / nclasses
+    radii = rmin + (np.arange(nclasses) + 0.5) * width
+    cls = rng.integers(0, nclasses, size=n)
+    # lattice neighbours through a hash of integer half-lattice coordinates
+    half = np.rint((x / a - 0.25) * 2).astype(np.int64)
+    m = 2 * n_fcc
+    code = (half[:, 0] % m) * m * m + (half[:, 1] % m) * m + (half[:, 2] % m)
+    index = -np.ones(m ** 3, np.int64)
+    index[code] = np.arange(n)
+    nbr_off = np.array([[1, 1, 0], [1, -1, 0], [-1, 1, 0], [-1, -1, 0],
+                        [1, 0, 1], [1, 0, -1], [-1, 0, 1], [-1, 0, -1],
+                        [0, 1, 1], [0, 1, -1], [0, -1, 1], [0, -1, -1]])
+    nbrs = np.empty((n, 12), np.int64)
+    for k, o in enumerate(nbr_off):
+        h2 = (half + o) % m
+        nbrs[:, k] = index[h2[:, 0] * m * m + h2[:, 1] * m + h2[:, 2]]
+    limit = spacing * (1.0 - 1.0e-6)
+    for _ in range(200):
+        r = radii[cls]
+        rn = np.where(nbrs >= 0, r[np.maximum(nbrs, 0)], 0.0)
+        bad = np.any((rn + r[:, None] >= limit) & (nbrs >= 0), axis=1)
+        # redraw only the lower index of each offending pair to converge
+        idx = np.nonzero(bad)[0]
+        if len(idx) == 0:
+            break
+        cls[idx] = rng.integers(0, nclasses, size=len(idx))
+    else:
+        raise RuntimeError("radius redraw did not converge")
+    used = np.unique(cls)
+    remap = -np.ones(nclasses, np.int64)
+    remap[used] = np.arange(len(used))
+    type_ = remap[cls].astype(np.int32)
+    types = [dict(radius=float(radii[c]), crust=float(0.1 * radii[c]), density=density,
+                  material="matP") for c in used]
+    v = rng.normal(0.0, sigma, size=(n, 3))
+    v -= v.mean(axis=0)
+    w = np.zeros((n, 3))
+    q = np.zeros((n, 4)); q[:, 3] = 1.0
+    models = [dict(matA="matP", matB="matP", kn=kn, en=en, etat=None, muc=muc,
+                   kt=2.0 / 7.0 * kn)]
+    return Scenario("periodic_gas", (0.0, 0.0, 0.0), (side, side, side), (1, 1, 1),
+                    (0.0, 0.0, 0.0), dt, types, [], models, type_, x, v, w, q)
+
+
+def solid_fraction(sc: Scenario) -> float:
+    r = np.array([t["radius"] for t in sc.types])[sc.type]
+    vol = np.prod(np.array(sc.maxc) - np.array(sc.origin))
+    return float(np.sum(4.0 / 3.0 * np.pi * r ** 3) / vol)

@@ -1,0 +1,44 @@
+"""CPU-side checks of the C ABI library: it loads, exports every entry point
+that include/grains_b200.h declares, and refuses to run without a device."""
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def _declared():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        txt = h.read_text()
+        txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+        names |= set(re.findall(r"\b(gdem_[a-z0-9_]+)\s*\(", txt))
+    return names
+
+
+def test_exports_every_declared_symbol(lib):
+    declared = _declared()
+    assert "gdem_step" in declared and len(declared) >= 15
+    for name in sorted(declared):
+        assert hasattr(lib, name), name
+
+
+def test_create_without_device_fails_cleanly(lib, tmp_path):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    from pacific_b200 import Grains, GrainsError, scenarios
+    p = scenarios.settling_box(n=10).write_xml(tmp_path / "s.xml")
+    with pytest.raises(GrainsError, match="CUDA|device"):
+        Grains(p)
+
+
+def test_bad_xml_is_rejected_before_device(lib, tmp_path):
+    """XML errors surface as GDEM_ERR_INVALID / GDEM_ERR_CUDA, never a crash."""
+    from pacific_b200 import Grains, GrainsError
+    p = tmp_path / "bad.xml"
+    p.write_text("<Grains3D><Construction><LinkedCell MX='1'/></Construction>")
+    with pytest.raises(GrainsError):
+        Grains(p)

@@ -1,0 +1,167 @@
+"""Parity of the CUDA DEM step against the CPU FP64 restatement (oracle/).
+
+Tolerances (stated per the DEM step's accuracy targets):
+  * FP64 mode: cell indices and contact-pair sets equal exactly; per-particle
+    force and torque within 1e-10 of the particle's sum of contact-force
+    magnitudes (|dF_i| / sum_c |f_ic|); positions after one step equal to
+    1e-15 relative.
+  * FP32-split mode: per-particle force error within 1e-5 of the same
+    normaliser; contact sets equal except pairs whose FP64 overlap lies within
+    1e-12 m of zero (near ties).
+"""
+import numpy as np
+import pytest
+
+from pacific_b200 import FP32_SPLIT, FP64, Grains, scenarios
+from tests.helpers import (contact_scale, contact_set, force_errors, gpu_from_oracle, oracle_for,
+                           radii_of)
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-10
+FP32_TOL = 1e-5
+
+
+def _cases():
+    return {
+        "settling_box": (scenarios.settling_box(), [0, 1500, 3000]),
+        "periodic_gas": (scenarios.periodic_gas(n_fcc=6), [0, 100, 300]),
+        "periodic_dense": (scenarios.periodic_gas(n_fcc=8, seed=77, spacing=2.35e-3), [0, 200]),
+    }
+
+
+@pytest.fixture(scope="module")
+def cases(tmp_path_factory, lib, oracle_lib):
+    d = tmp_path_factory.mktemp("xml")
+    out = {}
+    for name, (sc, marks) in _cases().items():
+        p = sc.write_xml(d / f"{name}.xml")
+        out[name] = (sc, str(p), marks)
+    return out
+
+
+def _check_step(sc, xml, o, precision, tol):
+    """Both sides advance one step from the oracle's current state."""
+    g = gpu_from_oracle(xml, sc, o, precision)
+    g.set_diagnostics(True)
+    assert o.step(1) == 0
+    g.step(1)
+    os_, gs = o.state(), g.download_state()
+    id0, id1, dl, pt, f = o.contacts()
+    scale = contact_scale(sc.n, id0, id1, f)
+    fe, te = force_errors(os_, gs, scale, radii_of(sc))
+    oc = contact_set(id0, id1)
+    g0, g1, gdl = g.download_contacts()
+    gc = contact_set(g0, g1)
+    if precision == FP64:
+        assert np.array_equal(o.cells(), g.download_cells())
+        assert oc == gc
+        assert np.max(np.abs(os_["x"] - gs["x"])) <= 1e-15 * np.max(np.abs(os_["x"]))
+    else:
+        near = {(a, b) for a, b, d in zip(*[x.tolist() for x in (np.minimum(id0, id1), np.maximum(id0, id1), dl)])
+                if abs(d) < 1e-12}
+        assert (oc ^ gc) <= near | {(b, a) for a, b in near}
+    assert fe.max() <= tol, f"force error {fe.max():.3e}"
+    assert te.max() <= tol * 10, f"torque error {te.max():.3e}"
+    assert g.status() == 0
+    g.close()
+    return fe.max(), te.max(), len(oc)
+
+
+@pytest.mark.parametrize("name", ["settling_box", "periodic_gas", "periodic_dense"])
+def test_init_forces_fp64(cases, name):
+    sc, xml, _ = cases[name]
+    o = oracle_for(sc, xml)
+    assert o.init() == 0
+    g = Grains(xml, FP64)
+    g.upload_state(sc.type, sc.x, sc.v, sc.w, sc.q)
+    g.set_diagnostics(True)
+    g.do_before_time_stepping()
+    assert np.array_equal(o.cells(), g.download_cells())
+    id0, id1, dl, pt, f = o.contacts()
+    g0, g1, _ = g.download_contacts()
+    assert contact_set(id0, id1) == contact_set(g0, g1)
+    scale = contact_scale(sc.n, id0, id1, f)
+    fe, te = force_errors(o.state(), g.download_state(), scale, radii_of(sc))
+    assert fe.max() <= FP64_TOL and te.max() <= FP64_TOL
+
+
+@pytest.mark.parametrize("precision,tol", [(FP64, FP64_TOL), (FP32_SPLIT, FP32_TOL)],
+                         ids=["fp64", "fp32split"])
+@pytest.mark.parametrize("name", ["settling_box", "periodic_gas", "periodic_dense"])
+def test_one_step_from_oracle_state(cases, name, precision, tol):
+    sc, xml, marks = cases[name]
+    o = oracle_for(sc, xml)
+    assert o.init() == 0
+    done = 0
+    ncontacts = 0
+    for m in marks:
+        assert o.step(m - done) == 0
+        done = m
+        fe, te, nc = _check_step(sc, xml, o, precision, tol)
+        done += 1
+        ncontacts += nc
+    assert ncontacts > 0
+
+
+@pytest.mark.parametrize("name", ["settling_box", "periodic_gas"])
+def test_trajectory_fp64(cases, name):
+    """100 steps from the same start: FP64 trajectories stay together."""
+    sc, xml, _ = cases[name]
+    o = oracle_for(sc, xml)
+    o.init()
+    g = Grains(xml, FP64)
+    g.upload_state(sc.type, sc.x, sc.v, sc.w, sc.q)
+    g.do_before_time_stepping()
+    for _ in range(4):
+        o.step(25)
+        g.step(25)
+    os_, gs = o.state(), g.download_state()
+    assert np.max(np.abs(os_["x"] - gs["x"])) < 1e-12
+    assert np.max(np.abs(os_["v"] - gs["v"])) < 1e-9
+    assert np.array_equal(o.cells(), g.download_cells())
+
+
+@pytest.mark.parametrize("precision", [FP64, FP32_SPLIT], ids=["fp64", "fp32split"])
+def test_deterministic_and_graphs(cases, precision):
+    """Two runs give identical bytes; graph replay equals plain launches."""
+    sc, xml, _ = cases["periodic_dense"]
+    res = []
+    for graphs in (True, True, False):
+        g = Grains(xml, precision)
+        g.use_graphs(graphs)
+        g.upload_state(sc.type, sc.x, sc.v, sc.w, sc.q)
+        g.do_before_time_stepping()
+        g.step(37)
+        g.step(20)
+        res.append(g.download_state())
+        g.close()
+    for k in ("x", "v", "w", "q", "F", "T"):
+        assert np.array_equal(res[0][k], res[1][k])
+        assert np.array_equal(res[0][k], res[2][k])
+
+
+def test_error_status(cases):
+    sc, xml, _ = cases["settling_box"]
+    # MotionError: one particle moving faster than crust / dt
+    v = sc.v.copy()
+    v[5] = [50.0, 0.0, 0.0]
+    g = Grains(xml, FP64)
+    g.upload_state(sc.type, sc.x, v, sc.w, sc.q)
+    g.do_before_time_stepping()
+    g.step(1)
+    assert g.status() & 0x02
+    # ContactError: two spheres overlapping by more than both crusts
+    x = sc.x.copy()
+    x[1] = x[0] + np.array([1.5e-3, 0.0, 0.0])
+    g = Grains(xml, FP64)
+    g.upload_state(sc.type, x, sc.v, sc.w, sc.q)
+    g.do_before_time_stepping()
+    assert g.status() & 0x01
+    # SimulationError: a particle outside the linked-cell grid
+    x = sc.x.copy()
+    x[3] = [0.5, 0.5, 0.5]
+    g = Grains(xml, FP32_SPLIT)
+    g.upload_state(sc.type, x, sc.v, sc.w, sc.q)
+    g.do_before_time_stepping()
+    assert g.status() & 0x04
