@@ -1,0 +1,223 @@
+// ref_harness.cpp -- drives the unmodified Grains3D reference (serial,
+// Type="Standard") from a given particle state, one leapfrog step at a time.
+// TEST INFRASTRUCTURE ONLY: it is built into oracle/_ref/ by
+// oracle/build_ref.sh, from the reference sources and the MPI / Xerces
+// stand-ins under oracle/shim/, and is used to pin the CPU restatement
+// (grains_oracle.cpp) and to produce the golden vectors in tests/golden/.
+//
+// The sequence below is the one of Grains::do_before_time_stepping and
+// Grains::Simulation (Base/src/Grains.cpp:95-173, 286-364), minus file
+// output: Construction + Forces read the XML; particles are inserted with
+// the calls Grains::insertParticle makes (Grains.cpp:2070-2130:
+// getParticleToInsert, setPosition, setTranslationalVelocity,
+// setAngularVelocity, setQuaternionRotation, insertParticleSerial,
+// WaitToActive, InitializeForce); the leapfrog start is
+// computeParticlesForceAndTorque + setAllContactMapCumulativeFeaturesToZero;
+// a step is moveParticlesAndObstacles(dt/2, dt, dt),
+// computeParticlesForceAndTorque, advanceParticlesVelocity(dt/2).
+#include <map>
+#include <vector>
+
+#include "Cell.hh"
+#include "ContactBuilderFactory.hh"
+#include "Error.hh"
+#include "Grains.hh"
+#include "GrainsBuilderFactory.hh"
+#include "GrainsExec.hh"
+#include "LinkedCell.hh"
+#include "Obstacle.hh"
+#include "Particle.hh"
+#include "ReaderXML.hh"
+#include "SimpleObstacle.hh"
+
+namespace {
+
+class RefGrains : public Grains {
+ public:
+  std::map<int, int> id_to_index;     // reference component ID -> caller index
+  std::map<int, int> obstacle_index;  // obstacle ID -> wall index (XML order)
+  std::vector<Particle*> by_index;
+
+  void setup(DOMElement* root) {
+    Construction(root);
+    Forces(root);
+    DOMNode* simu = ReaderXML::getNode(root, "Simulation");
+    DOMNode* ts = ReaderXML::getNode(simu, "TimeStep");
+    m_dt = ReaderXML::getNodeAttr_Double(ts, "dt");
+    m_time = 0.;
+    // phase timers that the step functions start and stop (Grains.cpp:277-282)
+    SCT_insert_app("ParticlesInsertion");
+    SCT_insert_app("ComputeForces");
+    SCT_insert_app("Move");
+    SCT_insert_app("UpdateParticleActivity");
+    SCT_insert_app("LinkUpdate");
+    SCT_insert_app("OutputResults");
+    std::list<SimpleObstacle*> obs = m_allcomponents.getObstacles()->getObstacles();
+    int k = 0;
+    for (SimpleObstacle* o : obs) obstacle_index[o->getID()] = k++;
+  }
+
+  int insert(int n, const int* type, const double* x, const double* v, const double* w,
+             const double* q) {
+    by_index.assign(n, nullptr);
+    for (int i = 0; i < n; ++i) {
+      Particle* p = m_allcomponents.getParticleToInsert(type[i]);
+      p->setPosition(Point3(x[3 * i], x[3 * i + 1], x[3 * i + 2]));
+      p->setTranslationalVelocity(Vector3(v[3 * i], v[3 * i + 1], v[3 * i + 2]));
+      Quaternion qq(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]);
+      p->setQuaternionRotation(qq);
+      p->setAngularVelocity(Vector3(w[3 * i], w[3 * i + 1], w[3 * i + 2]));
+      p->initialize_transformWithCrust_to_notComputed();
+      bool ok = m_collision->insertParticleSerial(p, m_allcomponents.getActiveParticles(),
+                                                  m_allcomponents.getPeriodicCloneParticles(),
+                                                  m_allcomponents.getReferenceParticles(),
+                                                  m_periodic, true);
+      if (!ok) return 1;
+      m_allcomponents.WaitToActive();
+      p->InitializeForce(true);
+      id_to_index[p->getID()] = i;
+      by_index[i] = p;
+    }
+    m_allcomponents.computeNumberParticles(m_wrapper);
+    return 0;
+  }
+
+  int init() {
+    try {
+      computeParticlesForceAndTorque();
+      m_allcomponents.setAllContactMapCumulativeFeaturesToZero();
+    } catch (ContactError&) { return 1; }
+    catch (MotionError&) { return 2; }
+    catch (SimulationError&) { return 4; }
+    return 0;
+  }
+
+  int step(int nsteps) {
+    try {
+      for (int k = 0; k < nsteps; ++k) {
+        m_time += m_dt;
+        GrainsExec::m_time_counter++;
+        moveParticlesAndObstacles(0.5 * m_dt, m_dt, m_dt);
+        computeParticlesForceAndTorque();
+        m_allcomponents.advanceParticlesVelocity(m_time, 0.5 * m_dt);
+      }
+    } catch (ContactError&) { return 1; }
+    catch (MotionError&) { return 2; }
+    catch (SimulationError&) { return 4; }
+    return 0;
+  }
+
+  // The master of each ID (periodic clones carry their master's ID and tag 2).
+  std::vector<Particle*> masters() {
+    std::vector<Particle*> out(by_index.size(), nullptr);
+    for (Particle* p : *m_allcomponents.getActiveParticles()) {
+      if (p->getTag() == 2) continue;
+      auto it = id_to_index.find(p->getID());
+      if (it != id_to_index.end()) out[it->second] = p;
+    }
+    return out;
+  }
+
+  int partnerIndex(int id) {
+    auto it = id_to_index.find(id);
+    if (it != id_to_index.end()) return it->second;
+    auto jt = obstacle_index.find(id);
+    if (jt != obstacle_index.end()) return -(jt->second + 2);
+    return -1000000;
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+void* ref_create(const char* xml_path) {
+  static bool initialized = false;
+  if (!initialized) {
+    ReaderXML::initialize();
+    initialized = true;
+  }
+  DOMElement* root = ReaderXML::getRoot(xml_path);
+  if (!root) return nullptr;
+  delete GrainsBuilderFactory::create(root);   // sets the 3D context
+  RefGrains* g = new RefGrains();
+  g->setup(root);
+  return g;
+}
+
+int ref_set_particles(void* h, int n, const int* type, const double* x, const double* v,
+                      const double* w, const double* q) {
+  return static_cast<RefGrains*>(h)->insert(n, type, x, v, w, q);
+}
+
+int ref_init(void* h) { return static_cast<RefGrains*>(h)->init(); }
+int ref_step(void* h, int nsteps) { return static_cast<RefGrains*>(h)->step(nsteps); }
+
+void ref_get_state(void* h, double* x, double* v, double* w, double* q, double* F, double* T) {
+  RefGrains* g = static_cast<RefGrains*>(h);
+  std::vector<Particle*> m = g->masters();
+  for (size_t i = 0; i < m.size(); ++i) {
+    Particle* p = m[i];
+    if (!p) continue;
+    Point3 const* P = p->getPosition();
+    Vector3 const* V = p->getTranslationalVelocity();
+    Vector3 const* W = p->getAngularVelocity();
+    Vector3 const* f = p->getForce();
+    Vector3 const* t = p->getTorque();
+    Quaternion const* Q = p->getQuaternionRotation();
+    for (int d = 0; d < 3; ++d) {
+      if (x) x[3 * i + d] = (*P)[d];
+      if (v) v[3 * i + d] = (*V)[d];
+      if (w) w[3 * i + d] = (*W)[d];
+      if (F) F[3 * i + d] = (*f)[d];
+      if (T) T[3 * i + d] = (*t)[d];
+    }
+    if (q) {
+      Vector3 const* vq = Q->getVector3();
+      q[4 * i] = (*vq)[0]; q[4 * i + 1] = (*vq)[1]; q[4 * i + 2] = (*vq)[2];
+      q[4 * i + 3] = Q->getdouble();
+    }
+  }
+}
+
+void ref_get_cells(void* h, int* ijk) {
+  RefGrains* g = static_cast<RefGrains*>(h);
+  std::vector<Particle*> m = g->masters();
+  for (size_t i = 0; i < m.size(); ++i)
+    for (int d = 0; d < 3; ++d) ijk[3 * i + d] = m[i] ? (*m[i]->getCell())[d] : -1;
+}
+
+int ref_num_history(void* h) {
+  RefGrains* g = static_cast<RefGrains*>(h);
+  int n = 0;
+  for (Particle* p : g->masters())
+    if (p) n += (int)p->getContactMap()->size();
+  return n;
+}
+
+// Contact memory of the masters: owner index, partner index (walls as
+// -(k+2)), kdelta, previous normal, spring torque.
+void ref_get_history(void* h, int* owner, int* partner, double* kdelta, double* prevn,
+                     double* spring) {
+  RefGrains* g = static_cast<RefGrains*>(h);
+  std::vector<Particle*> m = g->masters();
+  int n = 0;
+  for (size_t i = 0; i < m.size(); ++i) {
+    if (!m[i]) continue;
+    for (auto const& kv : *m[i]->getContactMap()) {
+      owner[n] = (int)i;
+      partner[n] = g->partnerIndex(std::get<1>(kv.first));
+      Vector3 const& kd = std::get<1>(kv.second);
+      Vector3 const& pn = std::get<2>(kv.second);
+      Vector3 const& sp = std::get<3>(kv.second);
+      for (int d = 0; d < 3; ++d) {
+        kdelta[3 * n + d] = kd[d]; prevn[3 * n + d] = pn[d]; spring[3 * n + d] = sp[d];
+      }
+      ++n;
+    }
+  }
+}
+
+void ref_destroy(void* h) { delete static_cast<RefGrains*>(h); }
+
+}  // extern "C"

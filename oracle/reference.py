@@ -1,0 +1,109 @@
+"""ctypes front end of the Grains3D reference built by oracle/build_ref.sh.
+
+TEST INFRASTRUCTURE: available only where the reference tree was present at
+build time (oracle/_ref/ is not committed).  Used to pin the CPU
+restatement and to generate the golden vectors in tests/golden/.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_ref" / "libgrains_ref.so"
+_lib = None
+
+
+def available() -> bool:
+    return LIB.exists()
+
+
+def build() -> Path:
+    subprocess.run(["sh", str(HERE / "build_ref.sh")], check=True)
+    return LIB
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        lib = ctypes.CDLL(str(LIB))
+        V = ctypes.c_void_p
+        D = ctypes.POINTER(ctypes.c_double)
+        I = ctypes.POINTER(ctypes.c_int)
+        lib.ref_create.argtypes = [ctypes.c_char_p]
+        lib.ref_create.restype = V
+        lib.ref_set_particles.argtypes = [V, ctypes.c_int, I, D, D, D, D]
+        lib.ref_set_particles.restype = ctypes.c_int
+        lib.ref_init.argtypes = [V]
+        lib.ref_init.restype = ctypes.c_int
+        lib.ref_step.argtypes = [V, ctypes.c_int]
+        lib.ref_step.restype = ctypes.c_int
+        lib.ref_get_state.argtypes = [V, D, D, D, D, D, D]
+        lib.ref_get_cells.argtypes = [V, I]
+        lib.ref_num_history.argtypes = [V]
+        lib.ref_num_history.restype = ctypes.c_int
+        lib.ref_get_history.argtypes = [V, I, I, D, D, D]
+        lib.ref_destroy.argtypes = [V]
+        _lib = lib
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+class Reference:
+    """The unmodified Grains3D serial step driven from a given state."""
+
+    def __init__(self, xml_path, quiet=True):
+        lib = _load()
+        self._h = lib.ref_create(os.fsencode(str(xml_path)))
+        if not self._h:
+            raise RuntimeError(f"reference could not read {xml_path}")
+        self.n = 0
+
+    def set_particles(self, type, x, v, w, q):
+        n = len(type)
+        self._t = np.ascontiguousarray(type, np.int32)
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (x, v, w, q)]
+        rc = _load().ref_set_particles(self._h, n, _ip(self._t), *[_dp(a) for a in arrs])
+        self.n = n
+        return rc
+
+    def init(self):
+        return _load().ref_init(self._h)
+
+    def step(self, nsteps=1):
+        return _load().ref_step(self._h, nsteps)
+
+    def state(self):
+        n = self.n
+        out = {k: np.empty((n, 3)) for k in ("x", "v", "w", "F", "T")}
+        out["q"] = np.empty((n, 4))
+        _load().ref_get_state(self._h, _dp(out["x"]), _dp(out["v"]), _dp(out["w"]),
+                              _dp(out["q"]), _dp(out["F"]), _dp(out["T"]))
+        return out
+
+    def cells(self):
+        ijk = np.empty((self.n, 3), np.int32)
+        _load().ref_get_cells(self._h, _ip(ijk))
+        return ijk
+
+    def history(self):
+        lib = _load()
+        m = lib.ref_num_history(self._h)
+        own = np.empty(m, np.int32)
+        par = np.empty(m, np.int32)
+        kd = np.empty((m, 3))
+        pn = np.empty((m, 3))
+        sp = np.empty((m, 3))
+        lib.ref_get_history(self._h, _ip(own), _ip(par), _dp(kd), _dp(pn), _dp(sp))
+        return own, par, kd, pn, sp

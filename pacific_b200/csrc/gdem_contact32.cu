@@ -181,32 +181,26 @@ __global__ void __launch_bounds__(256) k_pairs32(DevState S) {
   const int4 cc = S.cellc[t];
   GridDesc const& g = S.grids[cc.w];
   const float4 ha = S.offh[t];
-  const int ida = S.id[t];
   int* out = S.pairs + (size_t)t * kPairCap;
   int cnt = 0;
-  for (int dj = -1; dj <= 1; ++dj)
-    for (int dk = -1; dk <= 1; ++dk)
-      for (int di = -1; di <= 1; ++di) {
-        int sh[3];
-        int key = neighbourKey(g, cc.x, cc.y, cc.z, di, dj, dk, sh);
-        if (key < 0) continue;
-        int b = S.cell_start[key], e = b + S.cell_count[key];
-        for (int u = b; u < e; ++u) {
-          if (u == t) continue;
-          const float4 hb = S.offh[u];
-          const int idb = S.id[u];
-          // evaluated in canonical orientation so both directions agree
-          float4 h0 = ida < idb ? ha : hb, h1 = ida < idb ? hb : ha;
-          int s = ida < idb ? 1 : -1;
-          float dx = fmaf((float)(s * di), g.edge_hi[0], h1.x - h0.x);
-          float dy = fmaf((float)(s * dj), g.edge_hi[1], h1.y - h0.y);
-          float dz = fmaf((float)(s * dk), g.edge_hi[2], h1.z - h0.z);
-          float R = (h0.w + h1.w) * (1.f + 4.e-6f);
-          if (dx * dx + dy * dy + dz * dz > R * R) continue;
-          if (cnt < kPairCap) out[cnt] = u | (offCode(di, dj, dk) << 27);
-          ++cnt;
-        }
-      }
+  const float4* __restrict__ offh = S.offh;
+  const float ex = g.edge_hi[0], ey = g.edge_hi[1], ez = g.edge_hi[2];
+  forEachCandidate(S.cell_start, g, cc, [&](int u, int dcx, int dj, int dk, int, int, int) {
+    if (u == t) return;
+    const float4 hb = offh[u];
+    // lower slot first, so both directions of a pair evaluate the same
+    // expression and agree on the (conservative) decision
+    const bool lo = t < u;
+    const float4 h0 = lo ? ha : hb, h1 = lo ? hb : ha;
+    const float s = lo ? 1.f : -1.f;
+    float dx = fmaf(s * (float)dcx, ex, h1.x - h0.x);
+    float dy = fmaf(s * (float)dj, ey, h1.y - h0.y);
+    float dz = fmaf(s * (float)dk, ez, h1.z - h0.z);
+    float R = (h0.w + h1.w) * (1.f + 4.e-6f);
+    if (dx * dx + dy * dy + dz * dz > R * R) return;
+    if (cnt < kPairCap) out[cnt] = u | (offCode(dcx, dj, dk) << 27);
+    ++cnt;
+  });
   if (cnt > kPairCap) { raise(S.status, kErrPairsFull); cnt = kPairCap; }
   S.npairs[t] = cnt;
 }
@@ -277,7 +271,7 @@ __global__ void __launch_bounds__(256) k_forces32(DevState S) {
     }
   }
   // walls: geometry from the FP64 master position, force law in FP32
-  d3 xt = ld3(S.x, cap, t);
+  const d3 xt = g.wall_count > 0 ? ld3(S.x, cap, t) : mk(0., 0., 0.);
   for (int k = 0; k < g.wall_count; ++k) {
     WallDesc const& wd = S.walls[g.wall_begin + k];
     Contact64 ct = sphereWall64(xt, ta.radius, ta.crust, wd);

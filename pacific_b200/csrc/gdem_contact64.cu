@@ -21,36 +21,30 @@ namespace gdem {
 
 namespace {
 
+// Keeps a candidate when ClosestPointSPHERESPHERE would report contact up to
+// a relative margin of 1e-12; k_forces64 then decides exactly (distance < 0)
+// in lower-ID-first orientation.  The margin only matters for periodic
+// images, where the two orientations round the image translation differently.
 __global__ void __launch_bounds__(256) k_pairs64(DevState S) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
   const int4 cc = S.cellc[t];
   GridDesc const& g = S.grids[cc.w];
   const double4 pa = S.pos64[t];
-  const int ida = S.id[t];
   int* out = S.pairs + (size_t)t * kPairCap;
   int cnt = 0;
-  for (int dj = -1; dj <= 1; ++dj)
-    for (int dk = -1; dk <= 1; ++dk)
-      for (int di = -1; di <= 1; ++di) {
-        int sh[3];
-        int key = neighbourKey(g, cc.x, cc.y, cc.z, di, dj, dk, sh);
-        if (key < 0) continue;
-        int b = S.cell_start[key], e = b + S.cell_count[key];
-        d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
-        for (int u = b; u < e; ++u) {
-          if (u == t) continue;
-          const double4 pb = S.pos64[u];
-          const int idb = S.id[u];
-          d3 xa, xb;
-          if (ida < idb) { xa = mk(pa.x, pa.y, pa.z); xb = mk(pb.x, pb.y, pb.z) + shift; }
-          else { xa = mk(pb.x, pb.y, pb.z); xb = mk(pa.x, pa.y, pa.z) + (-shift); }
-          double distance = norm(xb - xa) - (pa.w + pb.w);
-          if (distance > 0.) continue;
-          if (cnt < kPairCap) out[cnt] = u | (offCode(di, dj, dk) << 27);
-          ++cnt;
-        }
-      }
+  const double4* __restrict__ pos = S.pos64;
+  forEachCandidate(S.cell_start, g, cc, [&](int u, int dcx, int dj, int dk, int sx, int sy, int sz) {
+    if (u == t) return;
+    const double4 pb = pos[u];
+    d3 shift = mk(sx * g.L[0], sy * g.L[1], sz * g.L[2]);
+    d3 d = u > t ? (mk(pb.x, pb.y, pb.z) + shift) - mk(pa.x, pa.y, pa.z)
+                 : (mk(pa.x, pa.y, pa.z) + (-shift)) - mk(pb.x, pb.y, pb.z);
+    double R = pa.w + pb.w;
+    if (norm(d) - R > 1.0e-12 * R) return;
+    if (cnt < kPairCap) out[cnt] = u | (offCode(dcx, dj, dk) << 27);
+    ++cnt;
+  });
   if (cnt > kPairCap) { raise(S.status, kErrPairsFull); cnt = kPairCap; }
   S.npairs[t] = cnt;
 }

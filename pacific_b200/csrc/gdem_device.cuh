@@ -187,6 +187,56 @@ __device__ __forceinline__ int neighbourKey(GridDesc const& g, int i, int j, int
   return g.cell_offset + c[1] * g.nb[2] * g.nb[0] + c[2] * g.nb[0] + c[0];
 }
 
+// Enumerates the particles of the 27 cells around cell cc (i, j, k, inst),
+// row by row: for each of the 9 (dj, dk) rows the cells i-1, i, i+1 are
+// consecutive in the cell numbering, so their particles are one contiguous
+// slot range [cell_start[i-1], cell_start[i+2]); the cell of a candidate
+// within the row follows from two boundaries.  In a periodic x direction the
+// two extra layers are empty and the wrapped neighbour cell is visited
+// separately.  fn(u, dcx, dj, dk, shx, shy, shz) receives the candidate slot,
+// its cell offset and the periodic image shift (in periods); the centre
+// particle itself is included.
+template <typename Fn>
+__device__ __forceinline__ void forEachCandidate(const int* __restrict__ cs, GridDesc const& g,
+                                                 int4 cc, Fn&& fn) {
+  const int nbx = g.nb[0];
+  for (int dj = -1; dj <= 1; ++dj) {
+    int jj = cc.y + dj, shy = 0;
+    if (g.periodic[1]) {
+      int nin = g.nb[1] - 2;
+      if (jj < 1) { jj += nin; shy = -1; } else if (jj > nin) { jj -= nin; shy = 1; }
+    } else if (jj < 0 || jj >= g.nb[1]) {
+      continue;
+    }
+    for (int dk = -1; dk <= 1; ++dk) {
+      int kk = cc.z + dk, shz = 0;
+      if (g.periodic[2]) {
+        int nin = g.nb[2] - 2;
+        if (kk < 1) { kk += nin; shz = -1; } else if (kk > nin) { kk -= nin; shz = 1; }
+      } else if (kk < 0 || kk >= g.nb[2]) {
+        continue;
+      }
+      const int row = g.cell_offset + jj * g.nb[2] * nbx + kk * nbx;
+      int ilo = cc.x - 1, ihi = cc.x + 1;
+      if (!g.periodic[0]) { ilo = max(ilo, 0); ihi = min(ihi, nbx - 1); }
+      const int b0 = cs[row + ilo], b1 = cs[row + cc.x], b2 = cs[row + cc.x + 1],
+                b3 = cs[row + ihi + 1];
+      for (int u = b0; u < b3; ++u) fn(u, u < b1 ? -1 : (u < b2 ? 0 : 1), dj, dk, 0, shy, shz);
+      if (g.periodic[0]) {
+        const int nin = nbx - 2;
+        if (cc.x == 1) {
+          const int e0 = cs[row + nin], e1 = cs[row + nin + 1];
+          for (int u = e0; u < e1; ++u) fn(u, -1, dj, dk, -1, shy, shz);
+        }
+        if (cc.x == nin) {
+          const int e0 = cs[row + 1], e1 = cs[row + 2];
+          for (int u = e0; u < e1; ++u) fn(u, 1, dj, dk, 1, shy, shz);
+        }
+      }
+    }
+  }
+}
+
 // Code of a stencil offset in 0..26 and back.
 __device__ __forceinline__ int offCode(int di, int dj, int dk) { return (di + 1) + 3 * (dk + 1) + 9 * (dj + 1); }
 __device__ __forceinline__ void offDecode(int c, int* di, int* dj, int* dk) {

@@ -425,7 +425,7 @@ struct System {
     S.F = alloc<double>(3 * c); S.T = alloc<double>(3 * c);
     S.basis = nullptr; S.basis2 = nullptr;
     S.skey = alloc<int>(c); S.rank = alloc<int>(c); S.order = alloc<int>(c);
-    S.cell_count = alloc<int>(S.ncells); S.cell_start = alloc<int>(S.ncells);
+    S.cell_count = alloc<int>(S.ncells); S.cell_start = alloc<int>(S.ncells + 1);
     S.scan_tmp = alloc<int>((S.ncells + 1023) / 1024 + 1);
     S.cellc = alloc<int4>(c);
     if (precision == GDEM_FP64) {
@@ -482,12 +482,16 @@ struct System {
   void swapHist() { std::swap(S.hist_old, S.hist_new); }
   void swapBoth() { swapState(); swapHist(); ++parity; }
 
-  // Sort into cell order (after k_move or k_bin) and build the pair list.
-  void binAndPairs() {
+  // Sort into cell order (after k_key or k_bin), moving on the way when
+  // moving != 0, and build the pair list.
+  void binAndPairs(int moving, bool pre_kick) {
+    double dt = S.dt;
     timed("scan", [&] { launch_scan(S, stream); });
     timed("place", [&] { launch_place(S, stream); });
     timed("cellsort", [&] { launch_cellsort(S, stream); });
-    timed("gather", [&] { launch_gather(S, stream); });
+    timed("move_gather", [&] {
+      launch_move_gather(S, moving, 0.5 * dt, dt, pre_kick ? 1 : 0, 0.5 * dt, stream);
+    });
     swapState();
     ++parity;
     if (precision == GDEM_FP64) timed("pairs64", [&] { launch_pairs64(S, stream); });
@@ -508,14 +512,14 @@ struct System {
     timed("cell_clear", [&] {
       CK(cudaMemsetAsync(S.cell_count, 0, (size_t)S.ncells * sizeof(int), stream));
     });
-    timed("move", [&] { launch_move(S, 0.5 * dt, dt, pre_kick ? 1 : 0, 0.5 * dt, stream); });
-    binAndPairs();
+    timed("key", [&] { launch_key(S, 0.5 * dt, dt, pre_kick ? 1 : 0, 0.5 * dt, stream); });
+    binAndPairs(1, pre_kick);
     forces();
   }
   void init() {
     CK(cudaMemsetAsync(S.cell_count, 0, (size_t)S.ncells * sizeof(int), stream));
     launch_bin(S, stream);
-    binAndPairs();
+    binAndPairs(0, false);
     forces();
     launch_hist_zero_cumulative(S.hist_old, precision == GDEM_FP64, stream);
     CK(cudaStreamSynchronize(stream));

@@ -4,21 +4,24 @@
 // and follow the reference's expression order, so cell assignments are
 // bit-identical to Cell::GetCell on the same state.
 //
-//   k_move      SecondOrderLeapFrog::Move + ParticleKinematics::Move
-//               (TimeIntegration/src/SecondOrderLeapFrog.cpp:44-67,
-//                Component/src/ParticleKinematics.cpp:62-104), MotionError
-//               (Component/src/Particle.cpp:446-456), Cell::GetCell
-//               (Base/src/Cell.cpp:172-184), SimulationError when outside
-//               the grid (Base/src/LinkedCell.cpp:1506-1531), and the cell
-//               histogram of the counting-sort binning.
-//   k_kick      advanceVelocity (SecondOrderLeapFrog.cpp:74-94,
-//               ParticleKinematics.cpp:110-128).
-//   scan/place/cellsort/gather
+//   k_key       post-move cell of each particle (Cell::GetCell, Base/src/
+//               Cell.cpp:172-184; SimulationError when outside the grid,
+//               Base/src/LinkedCell.cpp:1506-1531) and the cell histogram of
+//               the counting-sort binning.
+//   scan/place/cellsort
 //               counting sort of particles on their cell key: a one-digit
 //               radix sort whose digit is the cell key, made stable by
 //               ordering each cell's entries by particle ID; it yields the
-//               cell start/end tables and permutes the particle state into
-//               cell order.
+//               cell start/end tables.
+//   k_move_gather
+//               SecondOrderLeapFrog::Move + ParticleKinematics::Move
+//               (TimeIntegration/src/SecondOrderLeapFrog.cpp:44-67,
+//                Component/src/ParticleKinematics.cpp:62-104) and MotionError
+//               (Component/src/Particle.cpp:446-456), applied while the state
+//               is permuted into cell order, so the state is read and written
+//               once per step.
+//   k_kick      advanceVelocity (SecondOrderLeapFrog.cpp:74-94,
+//               ParticleKinematics.cpp:110-128).
 #include "gdem_kernels.cuh"
 
 namespace gdem {
@@ -38,8 +41,15 @@ __device__ __forceinline__ d3 dOmega(TypeDesc const& t, d3 tbf, d3 om) {
             tbf.z / (c * I[2]) + om.x * om.y * (I[0] - I[1]) / I[2]);
 }
 
-// SSP-RK3 update of the body-fixed angular velocity over h.
+// SSP-RK3 update of the body-fixed angular velocity over h.  For a sphere
+// the acceleration does not depend on omega, so K1 = K2 = K3 and one
+// evaluation gives the same bits as three.
 __device__ __forceinline__ d3 rk3(TypeDesc const& t, d3 tbf, d3 wbf, double h) {
+  if (t.shape == 0) {
+    d3 K = dOmega(t, tbf, wbf);
+    K = K * h;
+    return wbf + ((K + K) + 4. * K) / 6.;
+  }
   d3 K1 = dOmega(t, tbf, wbf);
   K1 = K1 * h;
   d3 K2 = dOmega(t, tbf, wbf + K1);
@@ -59,60 +69,10 @@ __device__ __forceinline__ void kick(TypeDesc const& tp, d3 F, d3 T, d3& v, d3& 
   w = multToVector3(q, vecq(wbf, pc));
 }
 
-__global__ void k_move(DevState S, double h, double dt, int pre_kick, double pre_h) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= S.n) return;
-  const int cap = S.cap;
-  TypeDesc const tp = S.types[S.type[s]];
-  GridDesc const g = S.grids[S.inst[s]];
-  d3 F = ld3(S.F, cap, s), T = ld3(S.T, cap, s);
-  d3 v = ld3(S.v, cap, s), wbf = ld3(S.wbf, cap, s), w = ld3(S.w, cap, s);
-  d3 x = ld3(S.x, cap, s);
-  dq q = qmk(mk(S.q[s], S.q[cap + s], S.q[2 * cap + s]), S.q[3 * cap + s]);
-  if (pre_kick) kick(tp, F, T, v, wbf, w, q, pre_h);
-  // ParticleKinematics::Move
-  dq pc = conj(q);
-  d3 tbf = multToVector3(pc, vecq(T, q));
-  const double c = 1.;
-  v = v + (F / (tp.mass * c)) * h;
-  d3 dx = v * dt;
-  wbf = rk3(tp, tbf, wbf, h);
-  w = multToVector3(q, vecq(wbf, pc));
-  d3 meanw = multToVector3(q, vecq(wbf, pc));
-  x = x + dx;
-  double nOm = norm(meanw);
-  dq qdt;
-  if (nOm > 1.0e-10) {
-    double cc = cos(nOm * dt / 2.);
-    double ss = sin(nOm * dt / 2.);
-    qdt = qmk((ss * 1. / nOm) * meanw, cc);
-  } else {
-    qdt = qmk(mk(0., 0., 0.), 1.);
-  }
-  q = qmul(qdt, q);
-  if (S.basis && tp.shape != 0) {
-    // Transform::composeLeftByRotation (Geometry/src/Transform.cpp:140-159)
-    double mm[9], out[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) mm[k] = S.basis[k * cap + s];
-    double qx = qdt.v.x, qy = qdt.v.y, qz = qdt.v.z, qw = qdt.w;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-      double px = qy * mm[6 + i] - qz * mm[3 + i] + qw * mm[0 + i];
-      double py = qz * mm[0 + i] - qx * mm[6 + i] + qw * mm[3 + i];
-      double pz = qx * mm[3 + i] - qy * mm[0 + i] + qw * mm[6 + i];
-      double pw = -qx * mm[0 + i] - qy * mm[3 + i] - qz * mm[6 + i];
-      out[0 + i] = qy * pz - qz * py - pw * qx + qw * px;
-      out[3 + i] = qz * px - qx * pz - pw * qy + qw * py;
-      out[6 + i] = qx * py - qy * px - pw * qz + qw * pz;
-    }
-#pragma unroll
-    for (int k = 0; k < 9; ++k) S.basis[k * cap + s] = out[k];
-  }
-  if (norm(dx) > tp.crust) raise(S.status, kErrMotion);
-  // Periodic: a master leaving the inner cells is replaced by its image.
+// Cell of a position after the periodic wrap: a master leaving the inner
+// cells is replaced by its image (x is updated).  Cell::GetCell.
+__device__ __forceinline__ void cellOf(GridDesc const& g, d3& x, int* id) {
   double xs[3] = {x.x, x.y, x.z};
-  int id[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     id[d] = (int)floor((xs[d] - g.lc_origin[d]) / g.edge[d]);
@@ -123,17 +83,38 @@ __global__ void k_move(DevState S, double h, double dt, int pre_kick, double pre
     }
   }
   x = mk(xs[0], xs[1], xs[2]);
-  st3(S.x, cap, s, x); st3(S.v, cap, s, v); st3(S.w, cap, s, w); st3(S.wbf, cap, s, wbf);
-  S.q[s] = q.v.x; S.q[cap + s] = q.v.y; S.q[2 * cap + s] = q.v.z; S.q[3 * cap + s] = q.w;
+}
+
+__device__ __forceinline__ int keyOf(GridDesc const& g, int* id, int* status) {
   bool valid = id[0] >= 0 && id[0] < g.nb[0] && id[1] >= 0 && id[1] < g.nb[1] &&
                id[2] >= 0 && id[2] < g.nb[2];
   if (!valid) {
-    raise(S.status, kErrOutOfGrid);
+    raise(status, kErrOutOfGrid);
     id[0] = min(max(id[0], 0), g.nb[0] - 1);
     id[1] = min(max(id[1], 0), g.nb[1] - 1);
     id[2] = min(max(id[2], 0), g.nb[2] - 1);
   }
-  int key = g.cell_offset + id[1] * g.nb[2] * g.nb[0] + id[2] * g.nb[0] + id[0];
+  return g.cell_offset + id[1] * g.nb[2] * g.nb[0] + id[2] * g.nb[0] + id[0];
+}
+
+// First binning pass: the cell each particle will occupy after this step's
+// kick + drift.  Evaluates exactly the translational part of k_move_gather
+// (same expressions, same order), so both passes agree bit for bit.
+__global__ void k_key(DevState S, double h, double dt, int pre_kick, double pre_h) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= S.n) return;
+  const int cap = S.cap;
+  const double mass = S.types[S.type[s]].mass;
+  GridDesc const& g = S.grids[S.inst[s]];
+  const d3 F = ld3(S.F, cap, s);
+  d3 v = ld3(S.v, cap, s), x = ld3(S.x, cap, s);
+  const double c = 1.;
+  if (pre_kick) v = v + (F / (mass * c)) * pre_h;
+  v = v + (F / (mass * c)) * h;
+  x = x + v * dt;
+  int id[3];
+  cellOf(g, x, id);
+  int key = keyOf(g, id, S.status);
   S.skey[s] = key;
   S.rank[s] = atomicAdd(&S.cell_count[key], 1);
 }
@@ -142,19 +123,11 @@ __global__ void k_move(DevState S, double h, double dt, int pre_kick, double pre
 __global__ void k_bin(DevState S) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= S.n) return;
-  GridDesc const g = S.grids[S.inst[s]];
+  GridDesc const& g = S.grids[S.inst[s]];
   int id[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) id[d] = (int)floor((S.x[d * S.cap + s] - g.lc_origin[d]) / g.edge[d]);
-  bool valid = id[0] >= 0 && id[0] < g.nb[0] && id[1] >= 0 && id[1] < g.nb[1] &&
-               id[2] >= 0 && id[2] < g.nb[2];
-  if (!valid) {
-    raise(S.status, kErrOutOfGrid);
-    id[0] = min(max(id[0], 0), g.nb[0] - 1);
-    id[1] = min(max(id[1], 0), g.nb[1] - 1);
-    id[2] = min(max(id[2], 0), g.nb[2] - 1);
-  }
-  int key = g.cell_offset + id[1] * g.nb[2] * g.nb[0] + id[2] * g.nb[0] + id[0];
+  int key = keyOf(g, id, S.status);
   S.skey[s] = key;
   S.rank[s] = atomicAdd(&S.cell_count[key], 1);
 }
@@ -227,9 +200,15 @@ __global__ void k_scan_sums(int* sums, int ntiles) {
   }
 }
 
-__global__ void k_scan_add(int* out, const int* tile_sums, int n) {
+// Adds the tile offsets; out[n] receives the total so that cell c spans
+// [out[c], out[c + 1]).
+__global__ void k_scan_add(int* out, const int* tile_sums, const int* in, int n) {
   int i = blockIdx.x * kScanTile + threadIdx.x;
-  if (i < n) out[i] += tile_sums[blockIdx.x];
+  if (i < n) {
+    int v = out[i] + tile_sums[blockIdx.x];
+    out[i] = v;
+    if (i == n - 1) out[n] = v + in[i];
+  }
 }
 
 __global__ void k_place(DevState S) {
@@ -258,26 +237,77 @@ __global__ void k_cellsort(DevState S) {
   }
 }
 
-// Permutes the state into cell order and builds the compact contact arrays.
-__global__ void k_gather(DevState S) {
+// Second binning pass: permutes the state into cell order and, when moving,
+// applies the step's kick + drift on the way (ParticleKinematics::Move,
+// ParticleKinematics.cpp:62-104, with SecondOrderLeapFrog::Move,
+// SecondOrderLeapFrog.cpp:44-67), then builds the compact contact arrays.
+__global__ void k_move_gather(DevState S, int moving, double h, double dt, int pre_kick,
+                              double pre_h) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
   const int cap = S.cap;
-  int s = S.order[t];
-  int idv = S.id[s], ty = S.type[s], in = S.inst[s];
-  S.id2[t] = idv; S.type2[t] = ty; S.inst2[t] = in;
-  int key = S.skey[s];
-  S.key[t] = key;
-  d3 x = ld3(S.x, cap, s), v = ld3(S.v, cap, s), w = ld3(S.w, cap, s), wbf = ld3(S.wbf, cap, s);
-  st3(S.x2, cap, t, x); st3(S.v2, cap, t, v); st3(S.w2, cap, t, w); st3(S.wbf2, cap, t, wbf);
+  const int s = S.order[t];
+  const int idv = S.id[s], ty = S.type[s], in = S.inst[s];
+  const int key = S.skey[s];
+  TypeDesc const& tp = S.types[ty];
+  GridDesc const& g = S.grids[in];
+  d3 x = ld3(S.x, cap, s), v = ld3(S.v, cap, s), wbf = ld3(S.wbf, cap, s), w;
+  dq q = qmk(mk(S.q[s], S.q[cap + s], S.q[2 * cap + s]), S.q[3 * cap + s]);
+  if (moving) {
+    const d3 F = ld3(S.F, cap, s), T = ld3(S.T, cap, s);
+    if (pre_kick) kick(tp, F, T, v, wbf, w, q, pre_h);
+    dq pc = conj(q);
+    d3 tbf = multToVector3(pc, vecq(T, q));
+    const double c = 1.;
+    v = v + (F / (tp.mass * c)) * h;
+    d3 dx = v * dt;
+    wbf = rk3(tp, tbf, wbf, h);
+    w = multToVector3(q, vecq(wbf, pc));
+    const d3 meanw = w;     // same expression as w (ParticleKinematics.cpp:79-82)
+    x = x + dx;
+    double nOm = norm(meanw);
+    dq qdt;
+    if (nOm > 1.0e-10) {
+      double cc, ss;
+      sincos(nOm * dt / 2., &ss, &cc);
+      qdt = qmk((ss * 1. / nOm) * meanw, cc);
+    } else {
+      qdt = qmk(mk(0., 0., 0.), 1.);
+    }
+    q = qmul(qdt, q);
+    if (S.basis && tp.shape != 0) {
+      // Transform::composeLeftByRotation (Geometry/src/Transform.cpp:140-159)
+      double mm[9], out[9];
 #pragma unroll
-  for (int k = 0; k < 4; ++k) S.q2[k * cap + t] = S.q[k * cap + s];
-  if (S.basis) {
+      for (int k = 0; k < 9; ++k) mm[k] = S.basis[k * cap + s];
+      double qx = qdt.v.x, qy = qdt.v.y, qz = qdt.v.z, qw = qdt.w;
 #pragma unroll
-    for (int k = 0; k < 9; ++k) S.basis2[k * cap + t] = S.basis[k * cap + s];
+      for (int i = 0; i < 3; ++i) {
+        double px = qy * mm[6 + i] - qz * mm[3 + i] + qw * mm[0 + i];
+        double py = qz * mm[0 + i] - qx * mm[6 + i] + qw * mm[3 + i];
+        double pz = qx * mm[3 + i] - qy * mm[0 + i] + qw * mm[6 + i];
+        double pw = -qx * mm[0 + i] - qy * mm[3 + i] - qz * mm[6 + i];
+        out[0 + i] = qy * pz - qz * py - pw * qx + qw * px;
+        out[3 + i] = qz * px - qx * pz - pw * qy + qw * py;
+        out[6 + i] = qx * py - qy * px - pw * qz + qw * pz;
+      }
+#pragma unroll
+      for (int k = 0; k < 9; ++k) S.basis2[k * cap + t] = out[k];
+    }
+    if (norm(dx) > tp.crust) raise(S.status, kErrMotion);   // Particle.cpp:446-456
+    int id[3];
+    cellOf(g, x, id);
+  } else {
+    w = ld3(S.w, cap, s);
+    if (S.basis) {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) S.basis2[k * cap + t] = S.basis[k * cap + s];
+    }
   }
-  TypeDesc const tp = S.types[ty];
-  GridDesc const g = S.grids[in];
+  S.id2[t] = idv; S.type2[t] = ty; S.inst2[t] = in;
+  S.key[t] = key;
+  st3(S.x2, cap, t, x); st3(S.v2, cap, t, v); st3(S.w2, cap, t, w); st3(S.wbf2, cap, t, wbf);
+  S.q2[t] = q.v.x; S.q2[cap + t] = q.v.y; S.q2[2 * cap + t] = q.v.z; S.q2[3 * cap + t] = q.w;
   int c = key - g.cell_offset;
   int ci = c % g.nb[0];
   int ck = (c / g.nb[0]) % g.nb[2];
@@ -293,11 +323,11 @@ __global__ void k_gather(DevState S) {
     double o[3] = {x.x - (g.lc_origin[0] + ci * g.edge[0]),
                    x.y - (g.lc_origin[1] + cj * g.edge[1]),
                    x.z - (g.lc_origin[2] + ck * g.edge[2])};
-    float h[3], l[3];
+    float hh[3], ll[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) { h[d] = (float)o[d]; l[d] = (float)(o[d] - (double)h[d]); }
-    S.offh[t] = make_float4(h[0], h[1], h[2], tp.r_hi);
-    S.offl[t] = make_float4(l[0], l[1], l[2], tp.r_lo);
+    for (int d = 0; d < 3; ++d) { hh[d] = (float)o[d]; ll[d] = (float)(o[d] - (double)hh[d]); }
+    S.offh[t] = make_float4(hh[0], hh[1], hh[2], tp.r_hi);
+    S.offl[t] = make_float4(ll[0], ll[1], ll[2], tp.r_lo);
     S.velf[t] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)tp.mass);
     S.omgf[t] = make_float4((float)w.x, (float)w.y, (float)w.z, (float)tp.eqrad);
   }
@@ -448,8 +478,8 @@ void launch_vstats(DevState const& S, double* part, double* out, cudaStream_t st
   k_vstats_final<<<1, 256, 0, st>>>(part, nb, S.n, out);
 }
 
-void launch_move(DevState const& S, double h, double dt, int pre_kick, double pre_h, cudaStream_t st) {
-  if (S.n) k_move<<<blocks(S.n, 256), 256, 0, st>>>(S, h, dt, pre_kick, pre_h);
+void launch_key(DevState const& S, double h, double dt, int pre_kick, double pre_h, cudaStream_t st) {
+  if (S.n) k_key<<<blocks(S.n, 256), 256, 0, st>>>(S, h, dt, pre_kick, pre_h);
 }
 void launch_bin(DevState const& S, cudaStream_t st) {
   if (S.n) k_bin<<<blocks(S.n, 256), 256, 0, st>>>(S);
@@ -461,7 +491,7 @@ void launch_scan(DevState const& S, cudaStream_t st) {
   int ntiles = blocks(S.ncells, kScanTile);
   k_scan_tiles<<<ntiles, kScanTile, 0, st>>>(S.cell_count, S.cell_start, S.scan_tmp, S.ncells);
   k_scan_sums<<<1, kScanTile, 0, st>>>(S.scan_tmp, ntiles);
-  k_scan_add<<<ntiles, kScanTile, 0, st>>>(S.cell_start, S.scan_tmp, S.ncells);
+  k_scan_add<<<ntiles, kScanTile, 0, st>>>(S.cell_start, S.scan_tmp, S.cell_count, S.ncells);
 }
 void launch_place(DevState const& S, cudaStream_t st) {
   if (S.n) k_place<<<blocks(S.n, 256), 256, 0, st>>>(S);
@@ -469,8 +499,9 @@ void launch_place(DevState const& S, cudaStream_t st) {
 void launch_cellsort(DevState const& S, cudaStream_t st) {
   k_cellsort<<<blocks(S.ncells, 256), 256, 0, st>>>(S);
 }
-void launch_gather(DevState const& S, cudaStream_t st) {
-  if (S.n) k_gather<<<blocks(S.n, 256), 256, 0, st>>>(S);
+void launch_move_gather(DevState const& S, int moving, double h, double dt, int pre_kick,
+                        double pre_h, cudaStream_t st) {
+  if (S.n) k_move_gather<<<blocks(S.n, 256), 256, 0, st>>>(S, moving, h, dt, pre_kick, pre_h);
 }
 void launch_scatter_by_id(DevState const& S, double* x, double* v, double* w, double* wbf,
                           double* q, double* F, double* T, int id_base, cudaStream_t st) {

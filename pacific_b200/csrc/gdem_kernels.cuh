@@ -5,13 +5,14 @@
 namespace gdem {
 
 // gdem_integrate.cu
-void launch_move(DevState const& S, double h, double dt, int pre_kick, double pre_h, cudaStream_t st);
+void launch_key(DevState const& S, double h, double dt, int pre_kick, double pre_h, cudaStream_t st);
+void launch_move_gather(DevState const& S, int moving, double h, double dt, int pre_kick,
+                        double pre_h, cudaStream_t st);
 void launch_bin(DevState const& S, cudaStream_t st);
 void launch_kick(DevState const& S, double h, cudaStream_t st);
 void launch_scan(DevState const& S, cudaStream_t st);
 void launch_place(DevState const& S, cudaStream_t st);
 void launch_cellsort(DevState const& S, cudaStream_t st);
-void launch_gather(DevState const& S, cudaStream_t st);
 void launch_scatter_by_id(DevState const& S, double* x, double* v, double* w, double* wbf,
                           double* q, double* F, double* T, int id_base, cudaStream_t st);
 void launch_cells_by_id(DevState const& S, int* ijk, int id_base, cudaStream_t st);

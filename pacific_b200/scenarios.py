@@ -89,7 +89,7 @@ class Scenario:
             L += ["    <Obstacles>", '      <Composite name="Box">']
             for k, w in enumerate(self.walls):
                 c, s = w["centre"], w["size"]
-                L += [f'        <Obstacle name="Wall{k}">',
+                L += [f'        <Obstacle name="Wall{k}" Type="Standard">',
                       f'          <Convex CrustThickness="{_f(w["crust"])}">',
                       f'            <Box LX="{_f(s[0])}" LY="{_f(s[1])}" LZ="{_f(s[2])}"/>',
                       "          </Convex>",

@@ -1,0 +1,125 @@
+"""Golden vectors produced by the Grains3D reference itself (tests/golden/,
+made by tests/golden/make_golden.py from the unmodified reference sources).
+
+CPU: the FP64 restatement (oracle/) reproduces the reference bit for bit on
+the walled settling box (positions, velocities, angular velocities,
+quaternions, forces, torques, cells, contact memory) and to round-off on the
+periodic gas (the reference's periodic clones round the image translation in
+a different order than the minimum-image convention).
+
+GPU: starting from the reference's own state at step k (state + contact
+memory), one CUDA step reproduces the reference's step k+1: cells and contact
+sets exactly, forces and torques within 1e-10 (FP64) / 1e-5 (FP32-split) of
+each particle's sum of contact-force magnitudes.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def _load(name, tmp_path):
+    g = dict(np.load(GOLDEN / f"{name}.npz"))
+    xml = tmp_path / f"{name}.xml"
+    xml.write_text(str(g["xml"]))
+    return g, xml
+
+
+def _hist_dict(own, par, kd, pn):
+    return {(int(a), int(b)): (tuple(k), tuple(p)) for a, b, k, p in zip(own, par, kd, pn)}
+
+
+def test_restatement_bitexact_vs_reference_box(tmp_path, oracle_lib):
+    g, xml = _load("settling_box", tmp_path)
+    o = Oracle(xml)
+    assert o.set_particles(g["type"], g["x0"], g["v0"], g["w0"], g["q0"]) == 0
+    assert o.init() == 0
+    done = 0
+    for m in g["marks"]:
+        assert o.step(int(m) - done) == 0
+        done = int(m)
+        s = o.state()
+        for k in ("x", "v", "w", "q", "F", "T"):
+            assert np.array_equal(s[k], g[f"s{m}_{k}"]), (m, k)
+        assert np.array_equal(o.cells(), g[f"s{m}_cells"])
+        own, par, kd, pn, _ = o.history()
+        assert _hist_dict(own, par, kd, pn) == _hist_dict(
+            g[f"s{m}_hist_owner"], g[f"s{m}_hist_partner"], g[f"s{m}_hist_kdelta"],
+            g[f"s{m}_hist_prevn"])
+
+
+def test_restatement_vs_reference_periodic(tmp_path, oracle_lib):
+    g, xml = _load("periodic_gas", tmp_path)
+    o = Oracle(xml)
+    assert o.set_particles(g["type"], g["x0"], g["v0"], g["w0"], g["q0"]) == 0
+    assert o.init() == 0
+    done = 0
+    for m in g["marks"]:
+        assert o.step(int(m) - done) == 0
+        done = int(m)
+        s = o.state()
+        assert np.array_equal(o.cells(), g[f"s{m}_cells"])
+        assert np.max(np.abs(s["x"] - g[f"s{m}_x"])) <= 1e-15
+        scale = g[f"s{m}_scale"]
+        c = scale > 0
+        err = np.linalg.norm(s["F"] - g[f"s{m}_F"], axis=1)
+        assert np.all(err[c] <= 1e-10 * scale[c])
+        assert np.all(err[~c] == 0)
+        own, par, kd, pn, _ = o.history()
+        assert set(zip(own.tolist(), par.tolist())) == set(
+            zip(g[f"s{m}_hist_owner"].tolist(), g[f"s{m}_hist_partner"].tolist()))
+
+
+def _gpu_step_from_golden(g, xml, k, k1, precision, tol):
+    from pacific_b200 import Grains
+    from tests.helpers import contact_set
+    G = Grains(xml, precision)
+    G.upload_state(g["type"], g[f"s{k}_x"], g[f"s{k}_v"], g[f"s{k}_w"], g[f"s{k}_q"])
+    G.upload_forces(g[f"s{k}_F"], g[f"s{k}_T"])
+    own, par = g[f"s{k}_hist_owner"], g[f"s{k}_hist_partner"]
+    G.upload_history(own, par, g[f"s{k}_hist_kdelta"], g[f"s{k}_hist_prevn"])
+    G.set_diagnostics(True)
+    G.step(1)
+    s = G.download_state()
+    cells = G.download_cells()
+    id0, id1, _ = G.download_contacts()
+    G.close()
+    ref_pairs = {(min(a, b), max(a, b)) if b >= 0 else (a, b)
+                 for a, b in zip(g[f"s{k1}_hist_owner"].tolist(), g[f"s{k1}_hist_partner"].tolist())}
+    scale = g[f"s{k1}_scale"]
+    radius_scale = 1e-3
+    c = scale > 0
+    fe = np.linalg.norm(s["F"] - g[f"s{k1}_F"], axis=1)
+    te = np.linalg.norm(s["T"] - g[f"s{k1}_T"], axis=1)
+    return cells, contact_set(id0, id1), ref_pairs, fe[c] / scale[c], te[c] / (radius_scale * scale[c]), s
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["settling_box", "periodic_gas"])
+def test_gpu_fp64_step_matches_reference(tmp_path, lib, name):
+    from pacific_b200 import FP64
+    g, xml = _load(name, tmp_path)
+    marks = [int(m) for m in g["marks"]]
+    for k, k1 in zip(marks[0::2], marks[1::2]):
+        cells, gc, rc, fe, te, s = _gpu_step_from_golden(g, xml, k, k1, FP64, 1e-10)
+        assert np.array_equal(cells, g[f"s{k1}_cells"])
+        assert gc == rc
+        assert np.max(np.abs(s["x"] - g[f"s{k1}_x"])) <= 1e-15
+        assert fe.max(initial=0) <= 1e-10 and te.max(initial=0) <= 1e-10
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["settling_box", "periodic_gas"])
+def test_gpu_fp32split_step_matches_reference(tmp_path, lib, name):
+    from pacific_b200 import FP32_SPLIT
+    g, xml = _load(name, tmp_path)
+    marks = [int(m) for m in g["marks"]]
+    for k, k1 in zip(marks[0::2], marks[1::2]):
+        cells, gc, rc, fe, te, s = _gpu_step_from_golden(g, xml, k, k1, FP32_SPLIT, 1e-5)
+        assert np.array_equal(cells, g[f"s{k1}_cells"])
+        assert gc == rc
+        assert fe.max(initial=0) <= 1e-5 and te.max(initial=0) <= 1e-4
