@@ -234,22 +234,52 @@ def error_sample(n_fcc, steps_before, precision):
             "torque_max": float(te[m].max()), "particles_in_contact": int(m.sum())}
 
 
-def cpu_baseline(sc, xml, budget_s=15.0):
-    """Times the CPU FP64 restatement on a bounded sample of the same workload."""
+def _quiet(f, *a):
+    """Runs f with the process's stdout silenced (the reference prints its
+    construction log)."""
+    sys.stdout.flush()
+    fd = os.dup(1)
+    nul = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(nul, 1)
+    try:
+        return f(*a)
+    finally:
+        os.dup2(fd, 1)
+        os.close(fd)
+        os.close(nul)
+
+
+def cpu_system(sc, xml):
+    """The Grains3D reference itself (oracle/_ref, compiled from the reference
+    sources) when it was built, else the CPU FP64 restatement.  Returns
+    (kind, step function, label)."""
+    from oracle import reference
+    if reference.available():
+        r = _quiet(reference.Reference, xml)
+        assert _quiet(r.set_particles, sc.type, sc.x, sc.v, sc.w, sc.q) == 0
+        assert _quiet(r.init) == 0
+        return "reference", (lambda k: _quiet(r.step, k)), \
+            "Grains3D reference sources (serial Type=Standard step), g++ -O2"
     from tests.helpers import oracle_for
     o = oracle_for(sc, xml)
     o.init()
+    return "port", o.step, "CPU FP64 restatement oracle/grains_oracle.cpp"
+
+
+def cpu_baseline(sc, xml, budget_s=15.0):
+    """Times the reference CPU path on a bounded sample of the same workload
+    (single thread: the reference step has no threading inside an MPI rank)."""
+    kind, step, label = cpu_system(sc, xml)
     t0 = time.perf_counter()
-    o.step(1)
+    step(1)
     one = time.perf_counter() - t0
     k = max(1, min(50, int(budget_s / max(one, 1e-6))))
     t0 = time.perf_counter()
-    o.step(k)
+    step(k)
     dt = time.perf_counter() - t0
-    o.close()
-    return {"value": sc.n * k / dt, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"{k} steps of the full {sc.n}-sphere system after 1 warm-up step "
-                      "(oracle/grains_oracle.cpp, FP64, single thread)"}
+    return {"value": sc.n * k / dt, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": f"{k} steps of the full {sc.n}-sphere system after 1 warm-up step ({label}, "
+                      "FP64, 1 thread)"}
 
 
 # --------------------------------------------------------------- reference --
@@ -262,29 +292,27 @@ def run_reference(args, rank, world):
     sc = scenarios.periodic_gas(n_fcc=args.n_fcc, seed=1236)
     with tempfile.TemporaryDirectory() as d:
         xml = str(sc.write_xml(Path(d) / "gas.xml"))
-        from tests.helpers import oracle_for
-        o = oracle_for(sc, xml)
-        o.init()
+        kind, step, label = cpu_system(sc, xml)
         # each step is a bounded sample: the whole --steps/--warmup run stays
         # within a few minutes on one core
         t0 = time.perf_counter()
-        o.step(1)
+        step(1)
         one = time.perf_counter() - t0
         k = max(1, min(args.steps, int(60.0 / max(one, 1e-6))))
         w = min(args.warmup, 2)
-        o.step(w)
+        step(w)
         t0 = time.perf_counter()
-        o.step(k)
+        step(k)
         dt = time.perf_counter() - t0
     value = sc.n * k / dt
     sample = (f"{k} of the requested {args.steps} steps of the full {sc.n}-sphere system "
-              f"after {1 + w} warm-up steps, CPU FP64 restatement of the reference step, "
-              "1 thread (the reference step is single-threaded per MPI rank)")
+              f"after {1 + w} warm-up steps ({label}, FP64), 1 thread (the reference step "
+              "is single-threaded per MPI rank)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
             "n_gpus": world, "steps": k, "warmup": 1 + w, "ms_per_step": 1e3 * dt / k,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": {"workload": "periodic_gas_1M", "n": sc.n},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind,
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}

@@ -449,6 +449,7 @@ struct System {
     }
     S.status = alloc<int>(1);
     CK(cudaMemset(S.status, 0, sizeof(int)));
+    CK(cudaMemset(S.cell_count, 0, (size_t)S.ncells * sizeof(int)));
     CK(cudaMemset(S.F, 0, 3 * c * sizeof(double)));
     CK(cudaMemset(S.T, 0, 3 * c * sizeof(double)));
     d_stage = alloc<double>(22 * c);
@@ -509,9 +510,7 @@ struct System {
   // One full step; pre_kick applies the previous step's closing kick first.
   void stepBody(bool pre_kick) {
     double dt = S.dt;
-    timed("cell_clear", [&] {
-      CK(cudaMemsetAsync(S.cell_count, 0, (size_t)S.ncells * sizeof(int), stream));
-    });
+    // cell_count is zero here: k_cellsort of the previous binning reset it
     timed("key", [&] { launch_key(S, 0.5 * dt, dt, pre_kick ? 1 : 0, 0.5 * dt, stream); });
     binAndPairs(1, pre_kick);
     forces();

@@ -219,12 +219,15 @@ __global__ void k_place(DevState S) {
 
 // Orders each cell's entries by particle ID, so the permutation does not
 // depend on the arrival order of the atomic histogram.
+// It also resets the cell histogram for the next binning (every count has
+// been consumed by the scan at this point).
 __global__ void k_cellsort(DevState S) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= S.ncells) return;
-  int cnt = S.cell_count[c];
-  if (cnt < 2) return;
   int b = S.cell_start[c];
+  int cnt = S.cell_start[c + 1] - b;
+  S.cell_count[c] = 0;
+  if (cnt < 2) return;
   for (int i = 1; i < cnt; ++i) {
     int e = S.order[b + i];
     int ide = S.id[e];
