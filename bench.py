@@ -282,6 +282,41 @@ def cpu_baseline(sc, xml, budget_s=15.0):
                       "FP64, 1 thread)"}
 
 
+def batched_measure(n_inst, steps, warmup=3):
+    """The batched sweep: n_inst independent closed-box settling instances
+    (500-20,000 spheres each, their own kn/en/muc) stepped together in one
+    launch chain, against the same instances stepped one after another
+    (device time of each gdem_step, creation excluded on both sides)."""
+    from pacific_b200 import FP32_SPLIT, Grains, scenarios
+    inst = scenarios.batched_boxes(n_inst=n_inst)
+    with tempfile.TemporaryDirectory() as d:
+        xmls = [str(s.write_xml(Path(d) / f"i{k}.xml")) for k, s in enumerate(inst)]
+        ins, typ, x, v, w, q = scenarios.concat_state(inst)
+        g = Grains(xmls, FP32_SPLIT)
+        g.upload_state(typ, x, v, w, q, inst=ins)
+        g.do_before_time_stepping()
+        g.step(warmup)
+        g.step(steps)
+        t_batch = g.last_step_ms
+        st = g.status()
+        g.close()
+        t_seq = 0.0
+        for k, s in enumerate(inst):
+            gi = Grains(xmls[k], FP32_SPLIT)
+            gi.upload_state(s.type, s.x, s.v, s.w, s.q)
+            gi.do_before_time_stepping()
+            gi.step(warmup)
+            gi.step(steps)
+            t_seq += gi.last_step_ms
+            gi.close()
+    ntot = int(len(ins))
+    return {"instances": n_inst, "particles": ntot, "steps": steps,
+            "batched_value": ntot * steps / (t_batch * 1e-3),
+            "sequential_value": ntot * steps / (t_seq * 1e-3),
+            "speedup": t_seq / t_batch, "unit": UNIT, "precision": "fp32_split",
+            "status": st, "workload": "batched_boxes (seeded), FP32-split, device time"}
+
+
 # --------------------------------------------------------------- reference --
 def run_reference(args, rank, world):
     if rank != 0:
@@ -331,6 +366,8 @@ def main():
     ap.add_argument("--profile-steps", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-error", action="store_true")
+    ap.add_argument("--batched-instances", type=int, default=512)
+    ap.add_argument("--batched-steps", type=int, default=50)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -437,6 +474,8 @@ def main():
                                        "after 100 oracle steps, vs the CPU FP64 oracle",
                              "fp32_split": error_sample(20, 100, FP32_SPLIT),
                              "fp64": error_sample(20, 100, FP64)}
+        if args.batched_instances > 0:
+            line["batched"] = batched_measure(args.batched_instances, args.batched_steps)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(sc, xml)
         print(json.dumps(line), flush=True)

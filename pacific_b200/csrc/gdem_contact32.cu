@@ -72,8 +72,9 @@ __device__ __forceinline__ float3 crossf(float3 a, float3 b) {
 }
 __device__ __forceinline__ float normf3(float3 a) { return sqrtf(dotf(a, a)); }
 
-// Quaternion::setRotFromTwoVectors + rotateVector in FP32
-__device__ __forceinline__ float3 rotateTo(float3 u, float3 v, float3 x, bool& ok) {
+// Quaternion::setRotFromTwoVectors (the rotation taking u to v) in FP32.
+struct rot32 { float3 v; float w; };
+__device__ __forceinline__ rot32 rotFromTo(float3 u, float3 v) {
   float nn = sqrtf(dotf(u, u) * dotf(v, v));
   float real = nn + dotf(u, v);
   float3 vect;
@@ -84,24 +85,29 @@ __device__ __forceinline__ float3 rotateTo(float3 u, float3 v, float3 x, bool& o
     vect = crossf(u, v);
   }
   float nq = sqrtf(dotf(vect, vect) + real * real);
-  ok = nq > 0.f;
-  if (!ok) return x;
+  rot32 r;
+  if (!(nq > 0.f)) { r.v = f3(0.f, 0.f, 0.f); r.w = 1.f; return r; }
   float s = 1.f / nq;
-  vect = vect * s; real *= s;
-  float nv2 = dotf(vect, vect);
-  return ((real * real - nv2) * x + (2.f * dotf(x, vect)) * vect) + (2.f * real) * crossf(vect, x);
+  r.v = vect * s;
+  r.w = real * s;
+  return r;
+}
+// Quaternion::rotateVector in FP32
+__device__ __forceinline__ float3 rotate(rot32 const& q, float3 x) {
+  float nv2 = dotf(q.v, q.v);
+  return ((q.w * q.w - nv2) * x + (2.f * dotf(x, q.v)) * q.v) + (2.f * q.w) * crossf(q.v, x);
 }
 
-// HookeMemory force in FP32, seen from p0 (same structure as hodc64).
+// HookeMemory force in FP32, seen from p0 (same structure as hodc64).  relv
+// is the relative velocity of p0 with respect to p1 at the contact point and
+// wrel = w0 - w1; both are formed in FP64 by the caller, since they are small
+// differences of nearly equal velocities.
 __device__ __forceinline__ void hodc32(ModelDesc const& m, float kn, float beta, float dt,
-                                       float3 lev0, float3 lev1, float3 pen,
-                                       float3 v0, float3 w0, float m0, float rad0,
-                                       float3 v1, float3 w1, float m1, float rad1,
-                                       bool existed, float3& kd, float3& pn, float3& sp,
-                                       float3& f, float3& mr) {
+                                       float3 pen, float3 tmpV, float3 wrel, float m0, float rad0,
+                                       float m1, float rad1, bool existed, float3& kd,
+                                       float3& pn, float3& sp, float3& f, float3& mr) {
   float npen = normf3(pen);
   float3 normal = pen * (1.f / npen);
-  float3 tmpV = (v0 + crossf(w0, lev0)) - (v1 + crossf(w1, lev1));
   float3 v_n = normal * dotf(tmpV, normal);
   float3 v_t = tmpV - v_n;
   float avmass = 1.f / (1.f / m0 + 1.f / m1);
@@ -111,9 +117,12 @@ __device__ __forceinline__ void hodc32(ModelDesc const& m, float kn, float beta,
   float etat = m.etat == -1. ? -beta * sqrtf(kn / avmass) : (float)m.etat;
   float gammat = 2.f * etat * avmass;
   float3 viscousFT = -gammat * v_t;
-  bool rot_ok = false;
+  rot32 qrot;
   if (!existed) { kd = f3(0.f, 0.f, 0.f); sp = f3(0.f, 0.f, 0.f); }
-  else kd = rotateTo(pn, normal, kd, rot_ok);
+  else {
+    qrot = rotFromTo(pn, normal);
+    kd = rotate(qrot, kd);
+  }
   float kt = (float)m.kt;
   kd = kd + (dt * kt) * v_t;
   pn = normal;
@@ -144,8 +153,7 @@ __device__ __forceinline__ void hodc32(ModelDesc const& m, float kn, float beta,
     float kr = 3.f * kn * mur * mur * Req * Req;
     float etar = 3.f * gamman * mur * mur * Req * Req;
     float maxM = mur * Req * normFN;
-    float3 wrel = w0 - w1;
-    if (existed) { bool ok2; sp = rotateTo(pn, normal, sp, ok2); }
+    if (existed) sp = rotate(qrot, sp);
     sp = sp - (kr * dt) * wrel;
     float nM = normf3(sp);
     if (nM > maxM) sp = sp * (maxM / nM);
@@ -153,6 +161,13 @@ __device__ __forceinline__ void hodc32(ModelDesc const& m, float kn, float beta,
   }
   f = delFN + delFT;
 }
+
+// v + w x lever in FP64 from the master state (sorted order) and a float lever.
+__device__ __forceinline__ d3 pointVel(DevState const& S, int s, float3 lev) {
+  const d3 v = ld3(S.v, S.cap, s), w = ld3(S.w, S.cap, s);
+  return v + cross(w, mk((double)lev.x, (double)lev.y, (double)lev.z));
+}
+__device__ __forceinline__ float3 tof(d3 a) { return f3((float)a.x, (float)a.y, (float)a.z); }
 
 __device__ __forceinline__ void loadHistF(HistTable const& t, int slot, float3& kd, float3& pn, float3& sp) {
   const float* v = static_cast<const float*>(t.vals) + 9 * (size_t)slot;
@@ -213,7 +228,7 @@ __global__ void __launch_bounds__(256) k_forces32(DevState S) {
   GridDesc const& g = S.grids[cc.w];
   const int ida = S.id[t];
   TypeDesc const& ta = S.types[S.type[t]];
-  const float4 ha = S.offh[t], la = S.offl[t], va = S.velf[t], wa = S.omgf[t];
+  const float4 ha = S.offh[t], la = S.offl[t];
   float3 Fs = f3(0.f, 0.f, 0.f), Ts = f3(0.f, 0.f, 0.f);
   const float dt = (float)S.dt;
   const int np = S.npairs[t];
@@ -246,17 +261,17 @@ __global__ void __launch_bounds__(256) k_forces32(DevState S) {
     float3 lev0 = (h0.w + 0.5f * dd) * un;     // contact point - x0
     float3 lev1 = lev0 - dh;                    // contact point - x1 (image)
     float3 pen = dd * un;
-    const float4 vb = S.velf[u], wb = S.omgf[u];
-    float4 v0 = t0 ? va : vb, w0 = t0 ? wa : wb, v1 = t0 ? vb : va, w1 = t0 ? wb : wa;
     ModelDesc const& m = S.models[g.model_base + tp0.mat * kMaxMat + tp1.mat];
+    const int s0 = t0 ? t : u, s1 = t0 ? u : t;
+    const float3 relv = tof(pointVel(S, s0, lev0) - pointVel(S, s1, lev1));
+    const float3 wrel = m.rolling ? tof(ld3(S.w, cap, s0) - ld3(S.w, cap, s1)) : f3(0.f, 0.f, 0.f);
     const int id0 = t0 ? ida : idb, id1 = t0 ? idb : ida;
     const unsigned long long key = pairKey(id0, id1);
     int old = histFind(S.hist_old, key);
     float3 kd, pn, sp, f, mr;
     if (old >= 0) loadHistF(S.hist_old, old, kd, pn, sp);
-    hodc32(m, (float)m.kn, (float)m.beta, dt, lev0, lev1, pen, f3(v0.x, v0.y, v0.z),
-           f3(w0.x, w0.y, w0.z), v0.w, w0.w, f3(v1.x, v1.y, v1.z), f3(w1.x, w1.y, w1.z),
-           v1.w, w1.w, old >= 0, kd, pn, sp, f, mr);
+    hodc32(m, (float)m.kn, (float)m.beta, dt, pen, relv, wrel, (float)tp0.mass, (float)tp0.eqrad,
+           (float)tp1.mass, (float)tp1.eqrad, old >= 0, kd, pn, sp, f, mr);
     if (t0) {
       int slot = histInsert(S.hist_new, key);
       if (slot < 0) raise(S.status, kErrHashFull);
@@ -284,14 +299,12 @@ __global__ void __launch_bounds__(256) k_forces32(DevState S) {
     float3 kd, pn, sp, f, mr;
     if (old >= 0) loadHistF(S.hist_old, old, kd, pn, sp);
     d3 l0 = ct.point - xt;
-    d3 l1 = ct.point - mk(wd.centre[0], wd.centre[1], wd.centre[2]);
     float3 lev0 = f3((float)l0.x, (float)l0.y, (float)l0.z);
-    float3 lev1 = f3((float)l1.x, (float)l1.y, (float)l1.z);
     float3 pen = f3((float)ct.overlap.x, (float)ct.overlap.y, (float)ct.overlap.z);
-    float3 zero = f3(0.f, 0.f, 0.f);
-    hodc32(m, (float)m.kn, (float)m.beta, dt, lev0, lev1, pen, f3(va.x, va.y, va.z),
-           f3(wa.x, wa.y, wa.z), va.w, wa.w, zero, zero, 1.e20f, (float)wd.eqrad,
-           old >= 0, kd, pn, sp, f, mr);
+    const float3 relv = tof(pointVel(S, t, lev0));
+    const float3 wrel = tof(ld3(S.w, cap, t));
+    hodc32(m, (float)m.kn, (float)m.beta, dt, pen, relv, wrel, (float)ta.mass, (float)ta.eqrad,
+           1.e20f, (float)wd.eqrad, old >= 0, kd, pn, sp, f, mr);
     int slot = histInsert(S.hist_new, key);
     if (slot < 0) raise(S.status, kErrHashFull);
     else storeHistF(S.hist_new, slot, kd, pn, sp);

@@ -88,7 +88,7 @@ struct DevState {
   double4* omg64;         // w (space frame), equivalent radius
   float4* offh;           // cell-relative offset, hi part; radius hi
   float4* offl;           // lo parts; radius lo
-  float4* velf;           // v (float)
+  float4* velf;           // unused (FP32-split reads FP64 velocities per contact)
   float4* omgf;           // w (float)
   int4* cellc;            // cell i, j, k and instance
   // pair list: per-particle segments of kPairCap entries

@@ -433,7 +433,7 @@ struct System {
       S.offh = nullptr; S.offl = nullptr; S.velf = nullptr; S.omgf = nullptr;
     } else {
       S.offh = alloc<float4>(c); S.offl = alloc<float4>(c);
-      S.velf = alloc<float4>(c); S.omgf = alloc<float4>(c);
+      S.velf = nullptr; S.omgf = nullptr;   // contact velocities come from the FP64 state
       S.pos64 = nullptr; S.vel64 = nullptr; S.omg64 = nullptr;
     }
     S.pairs = alloc<int>(c * kPairCap); S.npairs = alloc<int>(c);

@@ -331,8 +331,6 @@ __global__ void k_move_gather(DevState S, int moving, double h, double dt, int p
     for (int d = 0; d < 3; ++d) { hh[d] = (float)o[d]; ll[d] = (float)(o[d] - (double)hh[d]); }
     S.offh[t] = make_float4(hh[0], hh[1], hh[2], tp.r_hi);
     S.offl[t] = make_float4(ll[0], ll[1], ll[2], tp.r_lo);
-    S.velf[t] = make_float4((float)v.x, (float)v.y, (float)v.z, (float)tp.mass);
-    S.omgf[t] = make_float4((float)w.x, (float)w.y, (float)w.z, (float)tp.eqrad);
   }
 }
 

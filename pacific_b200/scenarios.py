@@ -232,6 +232,72 @@ def periodic_gas(n_fcc=63, n_target=None, seed=1236, spacing=2.392e-3, rmin=0.8e
                     (0.0, 0.0, 0.0), dt, types, [], models, type_, x, v, w, q)
 
 
+def settling_instance(n, seed, rmin=0.8e-3, rmax=1.2e-3, nclasses=16, phi=0.3, kn=1.0e4,
+                      en=0.7, muc=0.5, dt=1.0e-5, vmax=0.05, density=2500.0) -> Scenario:
+    """One closed-box instance of the batched sweep: n polydisperse spheres
+    (radius uniform in [rmin, rmax], quantised to nclasses classes) on a
+    jittered cubic lattice in a cube whose side gives an initial solid
+    fraction phi, settling under gravity between six walls."""
+    rng = np.random.default_rng(seed)
+    width = (rmax - rmin) / nclasses
+    radii = rmin + (np.arange(nclasses) + 0.5) * width
+    cls = rng.integers(0, nclasses, size=n)
+    r = radii[cls]
+    side = float((np.sum(4.0 / 3.0 * np.pi * r ** 3) / phi) ** (1.0 / 3.0))
+    # FCC sites filling the cube from the bottom (a cubic lattice cannot hold
+    # phi = 0.3 with r up to 1.2 mm)
+    # (when n is just above 4 m^3 the lattice needs a slightly larger box:
+    # the side is then the smallest that keeps every lattice gap open and the
+    # achieved solid fraction is a little below phi)
+    m = int(np.ceil((n / 4.0) ** (1.0 / 3.0)))
+    off = 1.05 * rmax                                     # wall clearance
+    a = max((side - 2 * off) / (m - 0.5), 2 * rmax * 1.02 * np.sqrt(2.0))
+    side = (m - 0.5) * a + 2 * off
+    nn = a / np.sqrt(2.0)
+    sites = fcc_sites(m, a) - 0.25 * a + off
+    order = np.lexsort((sites[:, 0], sites[:, 1], sites[:, 2]))
+    x = sites[order[:n]]
+    jit = min(0.3 * (nn - 2 * rmax), 0.4 * (off - rmax))
+    x = x + rng.uniform(-jit, jit, size=x.shape)
+    v = rng.uniform(-vmax, vmax, size=(n, 3))
+    used = np.unique(cls)
+    remap = -np.ones(nclasses, np.int64)
+    remap[used] = np.arange(len(used))
+    types = [dict(radius=float(radii[c]), crust=float(0.1 * radii[c]), density=density,
+                  material="matP") for c in used]
+    kt = 2.0 / 7.0 * kn
+    models = [dict(matA="matP", matB="matP", kn=kn, en=en, etat=None, muc=muc, kt=kt),
+              dict(matA="matP", matB="matW", kn=kn, en=en, etat=None, muc=muc, kt=kt)]
+    walls = _box_walls((side, side, side), 2.0e-3, float(0.1 * rmin), "matW")
+    q = np.zeros((n, 4)); q[:, 3] = 1.0
+    return Scenario("settling_instance", (0.0, 0.0, 0.0), (side, side, side), (0, 0, 0),
+                    (0.0, 0.0, -9.81), dt, types, walls, models, remap[cls].astype(np.int32), x,
+                    v, np.zeros((n, 3)), q)
+
+
+def batched_boxes(n_inst=512, seed=1237, nmin=500, nmax=20000, dt=1.0e-5):
+    """Independent closed-box settling instances with their own particle
+    count (uniform in [nmin, nmax]), radii and contact parameters (kn
+    log-uniform in [1e3, 1e5], en uniform in [0.3, 0.95], muc uniform in
+    [0.1, 0.8]); instance k uses seed + k."""
+    out = []
+    for k in range(n_inst):
+        rng = np.random.default_rng(seed + k)
+        n = int(rng.integers(nmin, nmax + 1))
+        kn = float(10.0 ** rng.uniform(3.0, 5.0))
+        en = float(rng.uniform(0.3, 0.95))
+        muc = float(rng.uniform(0.1, 0.8))
+        out.append(settling_instance(n, seed + 100000 + k, kn=kn, en=en, muc=muc, dt=dt))
+    return out
+
+
+def concat_state(instances):
+    """Stacked (inst, type, x, v, w, q) of a batch, grouped by instance."""
+    inst = np.concatenate([np.full(s.n, k, np.int32) for k, s in enumerate(instances)])
+    cat = lambda a: np.concatenate([getattr(s, a) for s in instances])
+    return inst, cat("type").astype(np.int32), cat("x"), cat("v"), cat("w"), cat("q")
+
+
 def solid_fraction(sc: Scenario) -> float:
     r = np.array([t["radius"] for t in sc.types])[sc.type]
     vol = np.prod(np.array(sc.maxc) - np.array(sc.origin))
