@@ -139,9 +139,24 @@ struct Model {
   bool rolling;
 };
 
+// Convex shape of a particle class or a wall.
+struct Shape {
+  int kind = 0;                      // 0 sphere, 1 box, 2 polyhedron
+  double radius = 0.;                // circumscribed radius
+  V3 extent;                         // box half lengths
+  std::vector<V3> verts;             // polyhedron vertices (local frame)
+  std::vector<std::vector<int>> cob; // vertex neighbours (Polyhedron::BuildPolyhedron)
+  V3 scaling;                        // crust shrink factors (RigidBodyWithCrust ctor)
+  double volume = 0.;
+  double inertia[6] = {0, 0, 0, 0, 0, 0};
+};
+
 struct Particle {
   int id, type;
   double radius, crust, mass, inertia, density, eqrad;
+  double I[3] = {0, 0, 0};           // body-frame principal inertia (inertia[0], [3], [5])
+  const Shape* shape = nullptr;
+  int curv = 0;                      // Polyhedron::m_curr_vertex of this particle's clone
   int matbit;
   V3 weight;
   V3 x, v, w, wbf;
@@ -155,6 +170,7 @@ struct Particle {
 
 struct Wall {
   int id;
+  Shape shape;          // box with the wall's crust scaling
   V3 centre, extent;    // half lengths
   double crust;
   int matbit;
@@ -193,6 +209,12 @@ typedef struct {
   int n_models;
   const int* model_mask;
   const double* model_params;  // kn en etat muc kt mur etarpf epst
+  // convex particle classes (NULL: all spheres)
+  const int* type_shape;       // 0 sphere, 1 box, 2 polyhedron
+  const double* type_extent;   // box half lengths, 3 per class
+  const int* type_poly;        // 4 per class: first vertex, vertex count, first face int, face ints
+  const double* poly_verts;    // 3 per vertex
+  const int* poly_faces;       // per face: size, then vertex indices
 } or_config;
 
 enum { OR_OK = 0, OR_ERR_CONTACT = 1, OR_ERR_MOTION = 2, OR_ERR_OUT_OF_GRID = 4 };
@@ -215,6 +237,7 @@ struct System {
   std::vector<Wall> walls;
   std::map<int, Model> models;
   std::vector<double> type_radius, type_crust, type_density;
+  std::vector<Shape> shapes;       // per particle class
   std::vector<int> type_matbit;
   std::vector<ContactRec> contacts;
   int err = 0;
@@ -287,10 +310,25 @@ int neighbourCell(System const& s, int i, int j, int k, int* shift) {
 }
 
 // -------------------------------------------------------------- kinematics --
-// ParticleKinematicsSphere::computeAngularAccelerationBodyFixed
-inline V3 dOmega(Particle const& p, V3 const& tbf) {
+// ParticleKinematicsSphere / ParticleKinematics3D::computeAngularAccelerationBodyFixed
+// (ParticleKinematicsSphere.cpp:47-55, ParticleKinematics3D.cpp:56-77; the
+// predictor-mode gyroscopic term is on, Grains.cpp:18)
+inline V3 dOmega(Particle const& p, V3 const& tbf, V3 const& om) {
   double c = 1.;
-  return V3(tbf[0] / (c * p.inertia), tbf[1] / (c * p.inertia), tbf[2] / (c * p.inertia));
+  const double* I = p.I;
+  if (!p.shape || p.shape->kind == 0)
+    return V3(tbf[0] / (c * I[0]), tbf[1] / (c * I[1]), tbf[2] / (c * I[2]));
+  return V3(tbf[0] / (c * I[0]) + om[1] * om[2] * (I[1] - I[2]) / I[0],
+            tbf[1] / (c * I[1]) + om[2] * om[0] * (I[2] - I[0]) / I[1],
+            tbf[2] / (c * I[2]) + om[0] * om[1] * (I[0] - I[1]) / I[2]);
+}
+
+// SSP-RK3 of SecondOrderLeapFrog::Move / advanceVelocity (:53-62, :83-92)
+inline V3 rk3(Particle const& p, V3 const& tbf, V3 const& wbf, double h) {
+  V3 K1 = dOmega(p, tbf, wbf); K1 = K1 * h;
+  V3 K2 = dOmega(p, tbf, wbf + K1); K2 = K2 * h;
+  V3 K3 = dOmega(p, tbf, wbf + 0.25 * (K1 + K2)); K3 = K3 * h;
+  return wbf + ((K1 + K2) + 4. * K3) / 6.;
 }
 
 // ParticleKinematics::Move (ParticleKinematics.cpp:62-104); returns |dx|
@@ -300,10 +338,7 @@ double moveParticle(Particle& p, double h, double dt) {
   double c = 1.;
   p.v += (p.F / (p.mass * c)) * h;
   V3 dx = p.v * dt;
-  V3 K1 = dOmega(p, tbf); K1 = K1 * h;
-  V3 K2 = dOmega(p, tbf); K2 = K2 * h;
-  V3 K3 = dOmega(p, tbf); K3 = K3 * h;
-  p.wbf += ((K1 + K2) + 4. * K3) / 6.;
+  p.wbf = rk3(p, tbf, p.wbf, h);
   V3 meanw = p.wbf;
   p.w = multToVector3(p.q, vecq(p.wbf, pc));
   meanw = multToVector3(p.q, vecq(meanw, pc));
@@ -342,10 +377,7 @@ void advanceVelocity(Particle& p, double h) {
   V3 tbf = multToVector3(pc, vecq(p.T, p.q));
   double c = 1.;
   p.v += (p.F / (p.mass * c)) * h;
-  V3 K1 = dOmega(p, tbf); K1 = K1 * h;
-  V3 K2 = dOmega(p, tbf); K2 = K2 * h;
-  V3 K3 = dOmega(p, tbf); K3 = K3 * h;
-  p.wbf += ((K1 + K2) + 4. * K3) / 6.;
+  p.wbf = rk3(p, tbf, p.wbf, h);
   p.w = multToVector3(p.q, vecq(p.wbf, pc));
 }
 
@@ -513,6 +545,245 @@ PointContact sphereWall(Particle const& a, Wall const& w, int* err) {
   return pc;
 }
 
+// -------------------------------------------------------------------- GJK --
+// Transform with the crust shrink (RigidBodyWithCrust::getTransformWithCrust,
+// RigidBodyWithCrust.cpp:749-760): M = basis * diag(scaling) (Matrix::
+// multiplyByScalingMatrix scales columns), origin = centre.  Row-major M.
+struct XForm { double M[9]; V3 o; };
+
+XForm crustTransform(const double* basis, V3 const& s, V3 const& o) {
+  XForm t;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) t.M[3 * r + c] = basis[3 * r + c] * s[c];
+  t.o = o;
+  return t;
+}
+// Transform::operator() (Transform.cpp:312-317): m_basis[i] * p + m_origin[i]
+inline V3 apply(XForm const& t, V3 const& p) {
+  return V3((t.M[0] * p[0] + t.M[1] * p[1] + t.M[2] * p[2]) + t.o[0],
+            (t.M[3] * p[0] + t.M[4] * p[1] + t.M[5] * p[2]) + t.o[1],
+            (t.M[6] * p[0] + t.M[7] * p[1] + t.M[8] * p[2]) + t.o[2]);
+}
+// Vector3 * Matrix = (tdot(X, v), tdot(Y, v), tdot(Z, v)) (Matrix.cpp:238-241, 527-530)
+inline V3 tmul(V3 const& v, XForm const& t) {
+  return V3(t.M[0] * v[0] + t.M[3] * v[1] + t.M[6] * v[2],
+            t.M[1] * v[0] + t.M[4] * v[1] + t.M[7] * v[2],
+            t.M[2] * v[0] + t.M[5] * v[1] + t.M[8] * v[2]);
+}
+
+// Support functions in the shape's frame: Sphere.cpp:99-108, Box.cpp:307-316,
+// Polyhedron.cpp:265-293 (hill climbing over the vertex neighbours from the
+// clone's current vertex, moving only on a gain of at least 1e-16).
+V3 support(Shape const& s, int* curv, V3 const& v) {
+  if (s.kind == 0) {
+    double n = norm(v);
+    if (n > EPSILON) { double r = s.radius / n; return V3(v[0] * r, v[1] * r, v[2] * r); }
+    return V3();
+  }
+  if (s.kind == 1) {
+    if (norm(v) < EPSILON) return V3();
+    return V3(v[0] < 0. ? -s.extent[0] : s.extent[0], v[1] < 0. ? -s.extent[1] : s.extent[1],
+              v[2] < 0. ? -s.extent[2] : s.extent[2]);
+  }
+  if (!(norm(v) > EPSILON)) return V3();
+  int last = -1;
+  double h = dot(s.verts[*curv], v), d = 0.;
+  for (;;) {
+    std::vector<int> const& cb = s.cob[*curv];
+    size_t i = 0, n = cb.size();
+    while (i != n && (cb[i] == last || (d = dot(s.verts[cb[i]], v)) - h < 1.e-16)) ++i;
+    if (i == n) break;
+    last = *curv;
+    *curv = cb[i];
+    h = d;
+  }
+  return s.verts[*curv];
+}
+
+// Johnson's distance sub-algorithm as in Convex.cpp:219-430 (SOLID).
+struct Simplex {
+  V3 y[4], p[4], q[4];
+  double det[16][4];
+  double dp[4][4];
+  Simplex() {
+    for (auto& r : det) for (double& x : r) x = 0.;
+    for (auto& r : dp) for (double& x : r) x = 0.;
+  }
+};
+
+void computeDet(Simplex& S, unsigned bits, unsigned last, unsigned last_bit, unsigned all_bits) {
+  for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
+    if (bits & bit) S.dp[i][last] = S.dp[last][i] = dot(S.y[i], S.y[last]);
+  S.dp[last][last] = dot(S.y[last], S.y[last]);
+  S.det[last_bit][last] = 1.;
+  for (unsigned j = 0, sj = 1; j < 4; ++j, sj <<= 1) {
+    if (bits & sj) {
+      unsigned s2 = sj | last_bit;
+      S.det[s2][j] = S.dp[last][last] - S.dp[last][j];
+      S.det[s2][last] = S.dp[j][j] - S.dp[j][last];
+      for (unsigned k = 0, sk = 1; k < j; ++k, sk <<= 1) {
+        if (bits & sk) {
+          unsigned s3 = sk | s2;
+          S.det[s3][k] = S.det[s2][j] * (S.dp[j][j] - S.dp[j][k]) +
+                         S.det[s2][last] * (S.dp[last][j] - S.dp[last][k]);
+          S.det[s3][j] = S.det[sk | last_bit][k] * (S.dp[k][k] - S.dp[k][j]) +
+                         S.det[sk | last_bit][last] * (S.dp[last][k] - S.dp[last][j]);
+          S.det[s3][last] = S.det[sk | sj][k] * (S.dp[k][k] - S.dp[k][last]) +
+                            S.det[sk | sj][j] * (S.dp[j][k] - S.dp[j][last]);
+        }
+      }
+    }
+  }
+  if (all_bits == 15) {
+    S.det[15][0] = S.det[14][1] * (S.dp[1][1] - S.dp[1][0]) + S.det[14][2] * (S.dp[2][1] - S.dp[2][0]) +
+                   S.det[14][3] * (S.dp[3][1] - S.dp[3][0]);
+    S.det[15][1] = S.det[13][0] * (S.dp[0][0] - S.dp[0][1]) + S.det[13][2] * (S.dp[2][0] - S.dp[2][1]) +
+                   S.det[13][3] * (S.dp[3][0] - S.dp[3][1]);
+    S.det[15][2] = S.det[11][0] * (S.dp[0][0] - S.dp[0][2]) + S.det[11][1] * (S.dp[1][0] - S.dp[1][2]) +
+                   S.det[11][3] * (S.dp[3][0] - S.dp[3][2]);
+    S.det[15][3] = S.det[7][0] * (S.dp[0][0] - S.dp[0][3]) + S.det[7][1] * (S.dp[1][0] - S.dp[1][3]) +
+                   S.det[7][2] * (S.dp[2][0] - S.dp[2][3]);
+  }
+}
+
+bool validSet(Simplex const& S, unsigned s, unsigned all_bits) {
+  for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1) {
+    if (all_bits & bit) {
+      if (s & bit) { if (S.det[s][i] <= 1.0e-20) return false; }
+      else if (S.det[s | bit][i] > 0) return false;
+    }
+  }
+  return true;
+}
+
+V3 computeVector(Simplex const& S, unsigned bits) {
+  double sum = 0.;
+  V3 v(0., 0., 0.);
+  for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
+    if (bits & bit) { sum += S.det[bits][i]; v += S.det[bits][i] * S.y[i]; }
+  return v * (1. / sum);
+}
+
+void computePoints(Simplex const& S, unsigned bits, V3& p1, V3& p2) {
+  double sum = 0.;
+  p1 = V3(0., 0., 0.);
+  p2 = V3(0., 0., 0.);
+  for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
+    if (bits & bit) {
+      sum += S.det[bits][i];
+      p1 += S.det[bits][i] * S.p[i];
+      p2 += S.det[bits][i] * S.q[i];
+    }
+  double s = 1. / sum;
+  p1 = p1 * s;
+  p2 = p2 * s;
+}
+
+bool properSet(Simplex const& S, unsigned s) {
+  for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
+    if ((s & bit) && S.det[s][i] <= 1.0e-20) return false;
+  return true;
+}
+
+bool closestSub(Simplex& S, unsigned& bits, unsigned last, unsigned last_bit, unsigned all_bits,
+                V3& v) {
+  computeDet(S, bits, last, last_bit, all_bits);
+  for (unsigned s = bits; s; --s) {
+    if ((s & bits) == s && validSet(S, s | last_bit, all_bits)) {
+      bits = s | last_bit;
+      v = computeVector(S, bits);
+      return true;
+    }
+  }
+  if (validSet(S, last_bit, all_bits)) {
+    bits = last_bit;
+    v = S.y[last];
+    return true;
+  }
+  double min_dist2 = INFINITY;
+  for (unsigned s = all_bits; s; --s) {
+    if ((s & all_bits) == s && properSet(S, s)) {
+      V3 u = computeVector(S, s);
+      double d2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+      if (d2 < min_dist2) { min_dist2 = d2; bits = s; v = u; }
+    }
+  }
+  return false;
+}
+
+// closest_points (Convex.cpp:536-627), default settings: tolerance 1e-10,
+// no acceleration.  pa/pb are in the shapes' own frames.
+double closestPoints(Shape const& a, int* ca, XForm const& a2w, Shape const& b, int* cb,
+                     XForm const& b2w, V3& pa, V3& pb, int& nIter) {
+  unsigned bits = 0, last = 0, last_bit = 0, all_bits = 0;
+  Simplex S;
+  double mu = 0.;
+  int numIterations = 0;
+  const double relError = 1.e-10, absError = 1.e-4 * relError;
+  V3 v = apply(a2w, support(a, ca, V3())) - apply(b2w, support(b, cb, V3()));
+  V3 w = v;
+  double dist = norm(v);
+  while (bits < 15 && dist > 1.0e-15 && numIterations < 1000) {
+    ++numIterations;
+    last = 0;
+    last_bit = 1;
+    while (bits & last_bit) { ++last; last_bit <<= 1; }
+    V3 d = v;
+    S.p[last] = support(a, ca, tmul(-d, a2w));
+    S.q[last] = support(b, cb, tmul(d, b2w));
+    w = apply(a2w, S.p[last]) - apply(b2w, S.q[last]);
+    mu = dist - dot(v, w) / dist;
+    if (mu < dist * relError || mu < absError) break;
+    bool degen = false;
+    for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
+      if ((all_bits & bit) && S.y[i][0] == w[0] && S.y[i][1] == w[1] && S.y[i][2] == w[2]) degen = true;
+    if (degen) break;
+    S.y[last] = w;
+    all_bits = bits | last_bit;
+    if (!closestSub(S, bits, last, last_bit, all_bits, v)) break;
+    dist = norm(v);
+  }
+  computePoints(S, bits, pa, pb);
+  nIter = numIterations;
+  return dist;
+}
+
+// RigidBodyWithCrust::ClosestPoint, general branch (RigidBodyWithCrust.cpp:
+// 277-351): bounding-sphere test, GJK between the crust-shrunk bodies,
+// overlap = distance - crustA - crustB, contact at the witness midpoint.
+PointContact convexContact(Shape const& a, int* ca, const double* basisA, V3 const& xa,
+                           double crustA, Shape const& b, int* cb, const double* basisB,
+                           V3 const& xb, double crustB, int* err) {
+  PointContact pc;
+  pc.contact = false;
+  V3 gg = xa - xb;
+  if (!(norm(gg) < a.radius + b.radius)) { pc.dist = 1.; return pc; }
+  XForm a2w = crustTransform(basisA, a.scaling, xa);
+  XForm b2w = crustTransform(basisB, b.scaling, xb);
+  V3 pA, pB;
+  int it = 0;
+  double distance = closestPoints(a, ca, a2w, b, cb, b2w, pA, pB, it);
+  if (distance < EPSILON) {
+    // ContactError: the reference retries with a 10x crust shrink
+    *err |= OR_ERR_CONTACT;
+    pc.dist = 1.;
+    return pc;
+  }
+  pA = apply(a2w, pA);
+  pB = apply(b2w, pB);
+  V3 ba = pA - pB;
+  V3 contact = pA / 2.0 + pB / 2.0;
+  V3 ov = ba / distance;
+  round3(ov);
+  ov = ov * (crustA + crustB - distance);
+  distance -= crustA + crustB;
+  pc.point = contact;
+  pc.overlap = ov;
+  pc.dist = distance;
+  pc.contact = true;
+  return pc;
+}
+
 // ------------------------------------------------------------ force model --
 // HookeMemoryContactForceModel::computeTangentialVector (:54-65)
 V3 tangentVector(Model const& m, double n_t, V3 const& ut, V3 const& kdelta) {
@@ -612,7 +883,11 @@ void addForce(Particle& p, V3 const& point, V3 const& f) {   // Torsor::addForce
 // Particle::InterAction + HookeMemory::computeForces for a particle pair
 void interactPP(System& s, Particle& p0, Particle& p1, V3 const& shift) {
   V3 xb = p1.x + shift;
-  PointContact pc = sphereSphere(p0, xb, p1, &s.err);
+  PointContact pc;
+  if (p0.shape->kind == 0 && p1.shape->kind == 0) pc = sphereSphere(p0, xb, p1, &s.err);
+  else
+    pc = convexContact(*p0.shape, &p0.curv, p0.basis, p0.x, p0.crust, *p1.shape, &p1.curv,
+                       p1.basis, xb, p1.crust, &s.err);
   if (!pc.contact || !(pc.dist < 0.)) return;
   Model const& m = s.model(p0.matbit, p1.matbit);
   Body b0{p0.x, p0.v, p0.w, p0.mass, p0.eqrad, &p0.cmap, p0.id};
@@ -633,7 +908,17 @@ void interactPP(System& s, Particle& p0, Particle& p1, V3 const& shift) {
 
 // SimpleObstacle::InterAction: the particle is p0, the wall p1
 void interactPW(System& s, Particle& p, Wall& w, int k) {
-  PointContact pc = sphereWall(p, w, &s.err);
+  static const double I3[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  PointContact pc;
+  if (p.shape->kind == 0) {
+    pc = sphereWall(p, w, &s.err);
+  } else {
+    // SimpleObstacle::InterAction: bounding-box zone test, then the particle
+    // is A and the wall B of RigidBodyWithCrust::ClosestPoint
+    int wc = 0;
+    pc = convexContact(*p.shape, &p.curv, p.basis, p.x, p.crust, w.shape, &wc, I3, w.centre,
+                       w.crust, &s.err);
+  }
   if (!pc.contact || !(pc.dist < 0.)) return;
   Model const& m = s.model(p.matbit, w.matbit);
   Body b0{p.x, p.v, p.w, p.mass, p.eqrad, &p.cmap, p.id};
@@ -722,6 +1007,96 @@ void step(System& s) {
 
 extern "C" {
 
+// GrainsExec::computeVolumeInertiaContrib (Base/src/GrainsExec.cpp:746-797):
+// volume and inertia of the tetrahedron (origin, A2, A3, A4), Tonon (2004).
+void tetContrib(V3 const& A2, V3 const& A3, V3 const& A4, double& vol, double* I) {
+  double x1 = 0., x2 = A2[0], x3 = A3[0], x4 = A4[0];
+  double y1 = 0., y2 = A2[1], y3 = A3[1], y4 = A4[1];
+  double z1 = 0., z2 = A2[2], z3 = A3[2], z4 = A4[2];
+  double det = std::fabs((x2 - x1) * (y3 - y1) * (z4 - z1) + (y2 - y1) * (z3 - z1) * (x4 - x1) +
+                         (z2 - z1) * (x3 - x1) * (y4 - y1) - (z2 - z1) * (y3 - y1) * (x4 - x1) -
+                         (x2 - x1) * (z3 - z1) * (y4 - y1) - (y2 - y1) * (x3 - x1) * (z4 - z1));
+  vol += det / 6.;
+  I[0] += det * (y1 * y1 + y1 * y2 + y2 * y2 + y1 * y3 + y2 * y3 + y3 * y3 + y1 * y4 + y2 * y4 +
+                 y3 * y4 + y4 * y4 + z1 * z1 + z1 * z2 + z2 * z2 + z1 * z3 + z2 * z3 + z3 * z3 +
+                 z1 * z4 + z2 * z4 + z3 * z4 + z4 * z4) / 60.;
+  I[3] += det * (x1 * x1 + x1 * x2 + x2 * x2 + x1 * x3 + x2 * x3 + x3 * x3 + x1 * x4 + x2 * x4 +
+                 x3 * x4 + x4 * x4 + z1 * z1 + z1 * z2 + z2 * z2 + z1 * z3 + z2 * z3 + z3 * z3 +
+                 z1 * z4 + z2 * z4 + z3 * z4 + z4 * z4) / 60.;
+  I[5] += det * (x1 * x1 + x1 * x2 + x2 * x2 + x1 * x3 + x2 * x3 + x3 * x3 + x1 * x4 + x2 * x4 +
+                 x3 * x4 + x4 * x4 + y1 * y1 + y1 * y2 + y2 * y2 + y1 * y3 + y2 * y3 + y3 * y3 +
+                 y1 * y4 + y2 * y4 + y3 * y4 + y4 * y4) / 60.;
+}
+
+// Shape of particle class t: geometry, volume, inertia (Sphere / Box /
+// Polyhedron BuildInertia, getVolume, computeCircumscribedRadius) and the
+// crust scaling from the identity-frame bounding box (RigidBodyWithCrust ctor,
+// RigidBodyWithCrust.cpp:58-78; Convex::bbox, Convex.cpp:29-41).
+Shape makeShape(or_config const* c, int t) {
+  Shape sh;
+  sh.kind = c->type_shape ? c->type_shape[t] : 0;
+  double crust = c->type_crust[t];
+  if (sh.kind == 0) {
+    double r = c->type_radius[t];
+    sh.radius = r;
+    sh.volume = 4.0 * PI * std::pow(r, 3.) / 3.0;
+    double I = 8.0 * PI * std::pow(r, 5.) / 15.0;
+    sh.inertia[0] = sh.inertia[3] = sh.inertia[5] = I;
+    sh.extent = V3(r, r, r);
+  } else if (sh.kind == 1) {
+    V3 e(c->type_extent[3 * t], c->type_extent[3 * t + 1], c->type_extent[3 * t + 2]);
+    sh.extent = e;
+    sh.radius = norm(e);
+    sh.volume = 8.0 * e[0] * e[1] * e[2];
+    sh.inertia[0] = 8.0 * e[0] * e[1] * e[2] * (e[1] * e[1] + e[2] * e[2]) / 3.0;
+    sh.inertia[3] = 8.0 * e[0] * e[1] * e[2] * (e[0] * e[0] + e[2] * e[2]) / 3.0;
+    sh.inertia[5] = 8.0 * e[0] * e[1] * e[2] * (e[0] * e[0] + e[1] * e[1]) / 3.0;
+  } else {
+    const int* P = c->type_poly + 4 * t;
+    for (int k = 0; k < P[1]; ++k) {
+      const double* v = c->poly_verts + 3 * (P[0] + k);
+      sh.verts.push_back(V3(v[0], v[1], v[2]));
+    }
+    sh.cob.assign(sh.verts.size(), std::vector<int>());
+    const int* f = c->poly_faces + P[2];
+    const int* fend = f + P[3];
+    double vol = 0.;
+    double I[6] = {0, 0, 0, 0, 0, 0};
+    while (f < fend) {
+      int nf = *f++;
+      for (int j = 0, k = nf - 1; j < nf; k = j++) sh.cob[f[k]].push_back(f[j]);
+      if (nf == 3) {
+        tetContrib(sh.verts[f[0]], sh.verts[f[1]], sh.verts[f[2]], vol, I);
+      } else {
+        V3 G;
+        for (int j = 0; j < nf; ++j) G += sh.verts[f[j]];
+        G = G / double(nf);
+        for (int j = 0, k = nf - 1; j < nf; k = j++) tetContrib(G, sh.verts[f[k]], sh.verts[f[j]], vol, I);
+      }
+      f += nf;
+    }
+    sh.volume = vol;
+    for (int k = 0; k < 6; ++k) sh.inertia[k] = I[k];
+    double ray = dot(sh.verts[0], sh.verts[0]);
+    for (size_t k = 1; k < sh.verts.size(); ++k) {
+      double d = dot(sh.verts[k], sh.verts[k]);
+      if (d > ray) ray = d;
+    }
+    sh.radius = std::sqrt(ray);
+    int cv = 0;
+    V3 mn, mx;
+    for (int d = 0; d < 3; ++d) {
+      V3 e; e[d] = 1.;
+      mn[d] = support(sh, &cv, -e)[d];
+      mx[d] = support(sh, &cv, e)[d];
+    }
+    sh.extent = (mx - mn) / 2.;
+  }
+  for (int d = 0; d < 3; ++d)
+    sh.scaling[d] = sh.extent[d] < EPSILON ? 1. : (sh.extent[d] - crust) / sh.extent[d];
+  return sh;
+}
+
 void* or_create(or_config const* c) {
   System* s = new System();
   for (int d = 0; d < 3; ++d) {
@@ -732,7 +1107,8 @@ void* or_create(or_config const* c) {
   }
   s->dt = c->dt;
   for (int t = 0; t < c->n_types; ++t) {
-    s->type_radius.push_back(c->type_radius[t]);
+    s->shapes.push_back(makeShape(c, t));
+    s->type_radius.push_back(s->shapes.back().radius);
     s->type_crust.push_back(c->type_crust[t]);
     s->type_density.push_back(c->type_density[t]);
     s->type_matbit.push_back(c->type_matbit[t]);
@@ -744,6 +1120,11 @@ void* or_create(or_config const* c) {
     w.extent = V3(c->wall_extent[3*k], c->wall_extent[3*k+1], c->wall_extent[3*k+2]);
     w.crust = c->wall_crust[k];
     w.matbit = c->wall_matbit[k];
+    w.shape.kind = 1;
+    w.shape.extent = w.extent;
+    w.shape.radius = norm(w.extent);
+    for (int d = 0; d < 3; ++d)
+      w.shape.scaling[d] = w.extent[d] < EPSILON ? 1. : (w.extent[d] - w.crust) / w.extent[d];
     s->walls.push_back(w);
   }
   for (int k = 0; k < c->n_models; ++k) {
@@ -767,7 +1148,7 @@ void or_destroy(void* h) { delete static_cast<System*>(h); }
 // Particles are inserted in index order (ID = index) and linked to their
 // cell with push_front, as LinkedCell::Link does at insertion.
 int or_set_particles(void* h, int n, const int* type, const double* x, const double* v,
-                     const double* w, const double* q) {
+                     const double* w, const double* q, const double* basis) {
   System& s = *static_cast<System*>(h);
   s.parts.clear();
   for (auto& c : s.cells) c.clear();
@@ -776,15 +1157,18 @@ int or_set_particles(void* h, int n, const int* type, const double* x, const dou
     Particle& p = s.parts[i];
     int t = type[i];
     p.id = i; p.type = t;
+    p.shape = &s.shapes[t];
     p.radius = s.type_radius[t];
     p.crust = s.type_crust[t];
     p.density = s.type_density[t];
     p.matbit = s.type_matbit[t];
-    double vol = 4.0 * PI * std::pow(p.radius, 3.) / 3.0;          // Sphere::getVolume
-    p.mass = p.density * vol;
+    double vol = p.shape->volume;
+    p.mass = p.density * vol;                                       // Particle.cpp:150
     p.eqrad = std::pow((0.75 / PI) * vol, 1. / 3.);
-    double I = 8.0 * PI * std::pow(p.radius, 5.) / 15.0;           // Sphere::BuildInertia
-    p.inertia = I * p.density;
+    p.I[0] = p.shape->inertia[0] * p.density;                       // Particle.cpp:152-157
+    p.I[1] = p.shape->inertia[3] * p.density;
+    p.I[2] = p.shape->inertia[5] * p.density;
+    p.inertia = p.I[0];
     p.weight = V3(s.gravity[0], s.gravity[1], s.gravity[2]) * (p.mass * (1. - 0. / p.density));
     p.x = V3(x[3*i], x[3*i+1], x[3*i+2]);
     p.v = V3(v[3*i], v[3*i+1], v[3*i+2]);
@@ -792,7 +1176,7 @@ int or_set_particles(void* h, int n, const int* type, const double* x, const dou
     p.q = qmake(V3(q[4*i], q[4*i+1], q[4*i+2]), q[4*i+3]);
     // angular velocity in body frame: q* (w, q) (ParticleKinematics.cpp:220-221)
     p.wbf = multToVector3(conj(p.q), vecq(p.w, p.q));
-    for (int k = 0; k < 9; ++k) p.basis[k] = (k % 4 == 0) ? 1. : 0.;
+    for (int k = 0; k < 9; ++k) p.basis[k] = basis ? basis[9 * i + k] : ((k % 4 == 0) ? 1. : 0.);
     p.F = V3(); p.T = V3();
     int id[3];
     s.getCell(p.x, id);
@@ -839,6 +1223,12 @@ void or_get_state(void* h, double* x, double* v, double* w, double* wbf, double*
     }
     if (q) { q[4*i] = p.q.v[0]; q[4*i+1] = p.q.v[1]; q[4*i+2] = p.q.v[2]; q[4*i+3] = p.q.w; }
   }
+}
+
+void or_get_basis(void* h, double* basis) {
+  System& s = *static_cast<System*>(h);
+  for (size_t i = 0; i < s.parts.size(); ++i)
+    for (int k = 0; k < 9; ++k) basis[9 * i + k] = s.parts[i].basis[k];
 }
 
 void or_get_cells(void* h, int* ijk) {

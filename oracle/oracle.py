@@ -57,6 +57,11 @@ class _Config(ctypes.Structure):
         ("n_models", ctypes.c_int),
         ("model_mask", ctypes.POINTER(ctypes.c_int)),
         ("model_params", ctypes.POINTER(ctypes.c_double)),
+        ("type_shape", ctypes.POINTER(ctypes.c_int)),
+        ("type_extent", ctypes.POINTER(ctypes.c_double)),
+        ("type_poly", ctypes.POINTER(ctypes.c_int)),
+        ("poly_verts", ctypes.POINTER(ctypes.c_double)),
+        ("poly_faces", ctypes.POINTER(ctypes.c_int)),
     ]
 
 
@@ -73,7 +78,7 @@ def _load():
         lib.or_create.argtypes = [ctypes.POINTER(_Config)]
         lib.or_create.restype = V
         lib.or_destroy.argtypes = [V]
-        lib.or_set_particles.argtypes = [V, ctypes.c_int, I, D, D, D, D]
+        lib.or_set_particles.argtypes = [V, ctypes.c_int, I, D, D, D, D, D]
         lib.or_set_particles.restype = ctypes.c_int
         lib.or_init.argtypes = [V]
         lib.or_init.restype = ctypes.c_int
@@ -81,6 +86,7 @@ def _load():
         lib.or_step.restype = ctypes.c_int
         lib.or_get_state.argtypes = [V, D, D, D, D, D, D, D]
         lib.or_get_cells.argtypes = [V, I]
+        lib.or_get_basis.argtypes = [V, D]
         lib.or_get_grid.argtypes = [V, I, D, D]
         lib.or_num_contacts.argtypes = [V]
         lib.or_num_contacts.restype = ctypes.c_int
@@ -123,10 +129,21 @@ def read_xml(path):
     types = []
     for p in cons.find("Particles").findall("Particle"):
         cv = p.find("Convex")
-        sph = cv.find("Sphere")
-        types.append(dict(radius=float(sph.get("Radius")), crust=float(cv.get("CrustThickness")),
-                          density=float(p.get("Density")),
-                          matbit=matbit(p.find("Material").text.strip())))
+        t = dict(crust=float(cv.get("CrustThickness")), density=float(p.get("Density")),
+                 matbit=matbit(p.find("Material").text.strip()), shape=0, radius=0.0,
+                 extent=[0.0, 0.0, 0.0], verts=[], faces=[])
+        if cv.find("Sphere") is not None:
+            t["radius"] = float(cv.find("Sphere").get("Radius"))
+        elif cv.find("Box") is not None:
+            bx = cv.find("Box")
+            t["shape"] = 1
+            t["extent"] = [0.5 * float(bx.get(k)) for k in ("LX", "LY", "LZ")]
+        elif cv.find("Polyhedron") is not None:
+            t["shape"] = 2
+            t["verts"], t["faces"] = read_poly(cv.find("Polyhedron").get("Name"))
+        else:
+            raise ValueError("unsupported particle shape")
+        types.append(t)
     walls = []
     obs = cons.find("Obstacles")
     if obs is not None:
@@ -156,6 +173,19 @@ def read_xml(path):
                gravity=[float(g.get(k)) for k in ("GX", "GY", "GZ")],
                dt=float(root.find("Simulation").find("TimeStep").get("dt")))
     return cfg
+
+
+def read_poly(path):
+    """Polyhedron file (Polyhedron::create, Geometry/src/Polyhedron.cpp:127-160):
+    '<token> <nb_vertices>', one vertex per line, '<nb_faces>', then one line
+    of vertex indices per face."""
+    lines = Path(path).read_text().splitlines()
+    head = lines[0].split()
+    nv = int(head[1])
+    verts = [[float(x) for x in lines[1 + k].split()] for k in range(nv)]
+    nf = int(lines[1 + nv].split()[0])
+    faces = [[int(x) for x in lines[2 + nv + k].split()] for k in range(nf)]
+    return verts, faces
 
 
 class Oracle:
@@ -192,6 +222,18 @@ class Oracle:
         cf.wall_extent = _dp(arr([w["extent"] for w in W] or [[0, 0, 0]], np.float64))
         cf.wall_crust = _dp(arr([w["crust"] for w in W] or [0], np.float64))
         cf.wall_matbit = _ip(arr([w["matbit"] for w in W] or [0], np.int32))
+        cf.type_shape = _ip(arr([t["shape"] for t in T], np.int32))
+        cf.type_extent = _dp(arr([t["extent"] for t in T], np.float64))
+        tp, pv, pf = [], [], []
+        for t in T:
+            tp += [len(pv), len(t["verts"]), len(pf), 0]
+            pv += t["verts"]
+            for f in t["faces"]:
+                pf += [len(f)] + list(f)
+            tp[-1] = len(pf) - tp[-2]
+        cf.type_poly = _ip(arr(tp, np.int32))
+        cf.poly_verts = _dp(arr(pv or [[0.0, 0.0, 0.0]], np.float64))
+        cf.poly_faces = _ip(arr(pf or [0], np.int32))
         M = c["models"]
         cf.n_models = len(M)
         cf.model_mask = _ip(arr([m["mask"] for m in M], np.int32))
@@ -211,11 +253,13 @@ class Oracle:
         except Exception:
             pass
 
-    def set_particles(self, type, x, v, w, q):
+    def set_particles(self, type, x, v, w, q, basis=None):
         n = len(type)
         self._t = np.ascontiguousarray(type, np.int32)
         arrs = [np.ascontiguousarray(a, np.float64) for a in (x, v, w, q)]
-        rc = _load().or_set_particles(self._h, n, _ip(self._t), *[_dp(a) for a in arrs])
+        self._b = None if basis is None else np.ascontiguousarray(basis, np.float64).reshape(n, 9)
+        rc = _load().or_set_particles(self._h, n, _ip(self._t), *[_dp(a) for a in arrs],
+                                      None if self._b is None else _dp(self._b))
         self.n = n
         return rc
 
@@ -232,6 +276,11 @@ class Oracle:
         _load().or_get_state(self._h, _dp(out["x"]), _dp(out["v"]), _dp(out["w"]),
                              _dp(out["wbf"]), _dp(out["q"]), _dp(out["F"]), _dp(out["T"]))
         return out
+
+    def basis(self):
+        b = np.empty((self.n, 9))
+        _load().or_get_basis(self._h, _dp(b))
+        return b
 
     def cells(self):
         ijk = np.empty((self.n, 3), np.int32)

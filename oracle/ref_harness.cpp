@@ -63,8 +63,18 @@ class RefGrains : public Grains {
     for (int i = 0; i < n; ++i) {
       Particle* p = m_allcomponents.getParticleToInsert(type[i]);
       p->setPosition(Point3(x[3 * i], x[3 * i + 1], x[3 * i + 2]));
-      p->setTranslationalVelocity(Vector3(v[3 * i], v[3 * i + 1], v[3 * i + 2]));
+      // orientation as Grains::insertParticle applies a random rotation:
+      // basis = basis o R(q), then the quaternion is rebuilt from the basis
       Quaternion qq(q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]);
+      if (!(q[4 * i] == 0. && q[4 * i + 1] == 0. && q[4 * i + 2] == 0.)) {
+        Matrix R;
+        R.setRotation(qq);
+        Transform trot;
+        trot.setBasis(R);
+        p->composePositionRightByTransform(trot);
+        qq.setQuaternion(p->getRigidBody()->getTransform()->getBasis());
+      }
+      p->setTranslationalVelocity(Vector3(v[3 * i], v[3 * i + 1], v[3 * i + 2]));
       p->setQuaternionRotation(qq);
       p->setAngularVelocity(Vector3(w[3 * i], w[3 * i + 1], w[3 * i + 2]));
       p->initialize_transformWithCrust_to_notComputed();
@@ -177,6 +187,18 @@ void ref_get_state(void* h, double* x, double* v, double* w, double* q, double* 
       q[4 * i] = (*vq)[0]; q[4 * i + 1] = (*vq)[1]; q[4 * i + 2] = (*vq)[2];
       q[4 * i + 3] = Q->getdouble();
     }
+  }
+}
+
+// Rotation part of each master's transform, row-major 3x3.
+void ref_get_basis(void* h, double* basis) {
+  RefGrains* g = static_cast<RefGrains*>(h);
+  std::vector<Particle*> m = g->masters();
+  for (size_t i = 0; i < m.size(); ++i) {
+    if (!m[i]) continue;
+    Matrix const& B = m[i]->getRigidBody()->getTransform()->getBasis();
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) basis[9 * i + 3 * r + c] = B[r][c];
   }
 }
 

@@ -44,6 +44,7 @@ def _load():
         lib.ref_step.restype = ctypes.c_int
         lib.ref_get_state.argtypes = [V, D, D, D, D, D, D]
         lib.ref_get_cells.argtypes = [V, I]
+        lib.ref_get_basis.argtypes = [V, D]
         lib.ref_num_history.argtypes = [V]
         lib.ref_num_history.restype = ctypes.c_int
         lib.ref_get_history.argtypes = [V, I, I, D, D, D]
@@ -91,6 +92,11 @@ class Reference:
         _load().ref_get_state(self._h, _dp(out["x"]), _dp(out["v"]), _dp(out["w"]),
                               _dp(out["q"]), _dp(out["F"]), _dp(out["T"]))
         return out
+
+    def basis(self):
+        b = np.empty((self.n, 9))
+        _load().ref_get_basis(self._h, _dp(b))
+        return b
 
     def cells(self):
         ijk = np.empty((self.n, 3), np.int32)

@@ -6,10 +6,12 @@
 //     d = dc * edge + (off_b - off_a),      dc in {-1, 0, 1}
 // which is formed in float-float arithmetic (error-free two-sum / two-product
 // with fmaf), so the overlap  |d| - (ra + rb)  keeps ~44 bits although every
-// operation is an FP32 operation.  Everything after the overlap (normal,
-// contact point, relative velocity, HookeMemory force, tangential history,
-// reduction) is plain FP32.  Results are written to the FP64 force/torque
-// arrays that the FP64 leapfrog consumes.
+// operation is an FP32 operation.  For each active contact, the relative
+// velocity at the contact point and its split into normal and tangential
+// parts are formed from the FP64 state (they are differences of nearly equal
+// quantities); the HookeMemory force law, the tangential history, the torque
+// lever arms and the per-particle reduction are FP32.  Results are written to
+// the FP64 force/torque arrays that the FP64 leapfrog consumes.
 //
 // Reference functions restated: ClosestPointSPHERESPHERE
 // (Geometry/src/RigidBodyWithCrust.cpp:596-639), HookeMemoryContactForceModel
@@ -98,18 +100,31 @@ __device__ __forceinline__ float3 rotate(rot32 const& q, float3 x) {
   return ((q.w * q.w - nv2) * x + (2.f * dotf(x, q.v)) * q.v) + (2.f * q.w) * crossf(q.v, x);
 }
 
-// HookeMemory force in FP32, seen from p0 (same structure as hodc64).  relv
-// is the relative velocity of p0 with respect to p1 at the contact point and
-// wrel = w0 - w1; both are formed in FP64 by the caller, since they are small
-// differences of nearly equal velocities.
+// Normal and tangential parts of the relative contact velocity.  Both come
+// from FP64 inputs: the velocity difference cancels when two bodies move
+// together, and the tangential part cancels when the motion is mostly normal,
+// where a normal rounded to FP32 would tilt it by 6e-8 rad.
+struct RelVel { float3 normal, vn, vt; };
+__device__ __forceinline__ RelVel splitRelVel(d3 nD, d3 tmpV) {
+  d3 vn = nD * dot(tmpV, nD);
+  d3 vt = tmpV - vn;
+  RelVel r;
+  r.normal = f3((float)nD.x, (float)nD.y, (float)nD.z);
+  r.vn = f3((float)vn.x, (float)vn.y, (float)vn.z);
+  r.vt = f3((float)vt.x, (float)vt.y, (float)vt.z);
+  return r;
+}
+
+// HookeMemory force in FP32, seen from p0 (same structure as hodc64); rv is
+// the decomposed relative velocity of p0 with respect to p1 at the contact
+// point and wrel = w0 - w1.
 __device__ __forceinline__ void hodc32(ModelDesc const& m, float kn, float beta, float dt,
-                                       float3 pen, float3 tmpV, float3 wrel, float m0, float rad0,
+                                       float3 pen, RelVel const& rv, float3 wrel, float m0, float rad0,
                                        float m1, float rad1, bool existed, float3& kd,
                                        float3& pn, float3& sp, float3& f, float3& mr) {
-  float npen = normf3(pen);
-  float3 normal = pen * (1.f / npen);
-  float3 v_n = normal * dotf(tmpV, normal);
-  float3 v_t = tmpV - v_n;
+  const float3 normal = rv.normal;
+  const float3 v_n = rv.vn;
+  const float3 v_t = rv.vt;
   float avmass = 1.f / (1.f / m0 + 1.f / m1);
   float gamman = -2.f * beta * sqrtf(avmass * kn);
   float3 delFN = kn * pen - gamman * v_n;
@@ -263,7 +278,10 @@ __global__ void __launch_bounds__(256) k_forces32(DevState S) {
     float3 pen = dd * un;
     ModelDesc const& m = S.models[g.model_base + tp0.mat * kMaxMat + tp1.mat];
     const int s0 = t0 ? t : u, s1 = t0 ? u : t;
-    const float3 relv = tof(pointVel(S, s0, lev0) - pointVel(S, s1, lev1));
+    // unit normal p1 -> p0 from the float-float separation (pen = dd * un, dd < 0)
+    d3 dD = mk((double)r.d[0].hi + (double)r.d[0].lo, (double)r.d[1].hi + (double)r.d[1].lo,
+               (double)r.d[2].hi + (double)r.d[2].lo);
+    const RelVel relv = splitRelVel(dD * (-1. / norm(dD)), pointVel(S, s0, lev0) - pointVel(S, s1, lev1));
     const float3 wrel = m.rolling ? tof(ld3(S.w, cap, s0) - ld3(S.w, cap, s1)) : f3(0.f, 0.f, 0.f);
     const int id0 = t0 ? ida : idb, id1 = t0 ? idb : ida;
     const unsigned long long key = pairKey(id0, id1);
@@ -301,7 +319,7 @@ __global__ void __launch_bounds__(256) k_forces32(DevState S) {
     d3 l0 = ct.point - xt;
     float3 lev0 = f3((float)l0.x, (float)l0.y, (float)l0.z);
     float3 pen = f3((float)ct.overlap.x, (float)ct.overlap.y, (float)ct.overlap.z);
-    const float3 relv = tof(pointVel(S, t, lev0));
+    const RelVel relv = splitRelVel(ct.overlap / norm(ct.overlap), pointVel(S, t, lev0));
     const float3 wrel = tof(ld3(S.w, cap, t));
     hodc32(m, (float)m.kn, (float)m.beta, dt, pen, relv, wrel, (float)ta.mass, (float)ta.eqrad,
            1.e20f, (float)wd.eqrad, old >= 0, kd, pn, sp, f, mr);

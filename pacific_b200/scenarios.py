@@ -77,9 +77,17 @@ class Scenario:
              f'    <Periodicity PX="{px}" PY="{py}" PZ="{pz}"/>',
              "    <Particles>"]
         for k, t in enumerate(self.types):
+            shape = t.get("shape", "sphere")
+            if shape == "box":
+                s = t["size"]
+                geo = f'          <Box LX="{_f(s[0])}" LY="{_f(s[1])}" LZ="{_f(s[2])}"/>'
+            elif shape == "polyhedron":
+                geo = f'          <Polyhedron Name="{t["file"]}"/>'
+            else:
+                geo = f'          <Sphere Radius="{_f(t["radius"])}"/>'
             L += [f'      <Particle Number="{int(cnt[k])}" Density="{_f(t["density"])}">',
                   f'        <Convex CrustThickness="{_f(t["crust"])}">',
-                  f'          <Sphere Radius="{_f(t["radius"])}"/>',
+                  geo,
                   "        </Convex>",
                   '        <AngularPosition Type="Identity"></AngularPosition>',
                   f'        <Material>{t["material"]}</Material>',
@@ -296,6 +304,79 @@ def concat_state(instances):
     inst = np.concatenate([np.full(s.n, k, np.int32) for k, s in enumerate(instances)])
     cat = lambda a: np.concatenate([getattr(s, a) for s in instances])
     return inst, cat("type").astype(np.int32), cat("x"), cat("v"), cat("w"), cat("q")
+
+
+def write_tetrahedron(path, edge=3.0e-3) -> Path:
+    """Regular tetrahedron with its centroid at the origin, in the polyhedron
+    file layout Grains3D reads (Polyhedron::create): '3 <nv>', vertices,
+    '<nf>', one line of vertex indices per face."""
+    a = edge / (2.0 * np.sqrt(2.0))
+    verts = [(a, a, a), (a, -a, -a), (-a, a, -a), (-a, -a, a)]
+    faces = [(0, 1, 2), (0, 3, 1), (0, 2, 3), (1, 3, 2)]
+    lines = ["3 4"] + [" ".join(_f(c) for c in v) for v in verts] + ["4"] + \
+            [" ".join(str(i) for i in f) for f in faces]
+    p = Path(path)
+    p.write_text("\n".join(lines) + "\n")
+    return p
+
+
+def random_quaternions(rng, n):
+    """Uniform random unit quaternions (Shoemake), as (qx, qy, qz, qw)."""
+    u1, u2, u3 = rng.random(n), rng.random(n), rng.random(n)
+    q = np.stack([np.sqrt(1 - u1) * np.sin(2 * np.pi * u2), np.sqrt(1 - u1) * np.cos(2 * np.pi * u2),
+                  np.sqrt(u1) * np.sin(2 * np.pi * u3), np.sqrt(u1) * np.cos(2 * np.pi * u3)], axis=1)
+    return q
+
+
+def rotation_matrices(q):
+    """Row-major rotation matrices of unit quaternions (qx, qy, qz, qw), with
+    the expression order of Matrix::setRotation (Geometry/src/Matrix.cpp:114-127)."""
+    x, y, z, w = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
+    d = x * x + y * y + z * z + w * w
+    s = 2.0 / d
+    xs, ys, zs = x * s, y * s, z * s
+    wx, wy, wz = w * xs, w * ys, w * zs
+    xx, xy, xz = x * xs, x * ys, x * zs
+    yy, yz, zz = y * ys, y * zs, z * zs
+    return np.stack([1.0 - (yy + zz), xy - wz, xz + wy, xy + wz, 1.0 - (xx + zz), yz - wx,
+                     xz - wy, yz + wx, 1.0 - (xx + yy)], axis=1)
+
+
+def convex_pour(n=200_000, seed=1238, poly_path=None, box=(0.1, 0.1, 0.3), cube_edge=2.0e-3,
+                tet_edge=3.0e-3, density=2000.0, kn=5.0e4, en=0.5, muc=0.4, dt=2.0e-6,
+                vmax=0.0) -> Scenario:
+    """Half cubes, half regular tetrahedra with uniformly random orientations
+    on a jittered lattice of spacing 1.02 x the tetrahedron's circumscribed
+    diameter, poured under gravity into an open-top box of footprint
+    box[0] x box[1].  The lattice does not fit in a box[2]-high container, so
+    the side walls and the linked-cell domain extend up to the lattice top."""
+    rng = np.random.default_rng(seed)
+    r_tet = tet_edge * np.sqrt(6.0) / 4.0
+    spacing = 2.0 * r_tet * 1.02
+    nx, ny = int(box[0] // spacing), int(box[1] // spacing)
+    nz = int(np.ceil(n / (nx * ny)))
+    height = max(box[2], (nz + 0.5) * spacing)
+    k, j, i = np.unravel_index(np.arange(n), (nz, ny, nx))
+    x = np.stack([(i + 0.5) * spacing, (j + 0.5) * spacing, (k + 0.5) * spacing], axis=1)
+    x[:, 0] += 0.5 * (box[0] - nx * spacing)
+    x[:, 1] += 0.5 * (box[1] - ny * spacing)
+    jit = 0.2 * (spacing - 2.0 * r_tet)
+    x = x + rng.uniform(-jit, jit, size=x.shape)
+    v = rng.uniform(-vmax, vmax, size=(n, 3)) if vmax > 0 else np.zeros((n, 3))
+    q = random_quaternions(rng, n)
+    type_ = (rng.random(n) < 0.5).astype(np.int32)        # 0 cube, 1 tetrahedron
+    r_cube = cube_edge * np.sqrt(3.0) / 2.0
+    types = [dict(shape="box", size=(cube_edge,) * 3, radius=float(r_cube),
+                  crust=float(0.1 * r_cube), density=density, material="matP"),
+             dict(shape="polyhedron", file=str(poly_path), radius=float(r_tet),
+                  crust=float(0.1 * r_tet), density=density, material="matP")]
+    dom = (box[0], box[1], height)
+    walls = _box_walls(dom, 2.0e-3, float(0.1 * r_cube), "matW")
+    kt = 2.0 / 7.0 * kn
+    models = [dict(matA="matP", matB="matP", kn=kn, en=en, etat=None, muc=muc, kt=kt),
+              dict(matA="matP", matB="matW", kn=kn, en=en, etat=None, muc=muc, kt=kt)]
+    return Scenario("convex_pour", (0.0, 0.0, 0.0), dom, (0, 0, 0), (0.0, 0.0, -9.81), dt, types,
+                    walls, models, type_, x, v, np.zeros((n, 3)), q)
 
 
 def solid_fraction(sc: Scenario) -> float:

@@ -39,9 +39,19 @@ def _quiet(f, *a):
         os.close(nul)
 
 
+POLY_TOKEN = "@POLYHEDRON_FILE@"
+
+
+def _convex():
+    d = Path(tempfile.mkdtemp())
+    poly = scenarios.write_tetrahedron(d / "tet.poly")
+    return scenarios.convex_pour(n=400, seed=5, poly_path=poly, box=(0.03, 0.03, 0.02), vmax=0.2)
+
+
 SCENARIOS = {
     "settling_box": (lambda: scenarios.settling_box(n=500, seed=11), [0, 1, 800, 801, 1600, 1601]),
     "periodic_gas": (lambda: scenarios.periodic_gas(n_fcc=5, seed=12), [0, 1, 20, 21]),
+    "convex_pour": (_convex, [0, 1, 3000, 3001, 6000, 6001]),
 }
 
 
@@ -50,6 +60,7 @@ def snapshot(r, prefix, out):
     for k, v in s.items():
         out[f"{prefix}_{k}"] = v
     out[f"{prefix}_cells"] = r.cells()
+    out[f"{prefix}_basis"] = r.basis()
     own, par, kd, pn, sp = r.history()
     out[f"{prefix}_hist_owner"] = own
     out[f"{prefix}_hist_partner"] = par
@@ -68,15 +79,26 @@ def run(name):
             xml = sc.write_xml(Path(d) / f"{name}.xml")
             r = _quiet(reference.Reference, xml)
             assert _quiet(r.set_particles, sc.type, sc.x, sc.v, sc.w, sc.q) == 0
+            # initial state as the reference holds it after insertion (its
+            # quaternion is rebuilt from the rotated basis)
+            s0 = r.state()
+            b0 = r.basis()
             assert _quiet(r.init) == 0
-            out = {"xml": np.array(sc.xml()), "type": sc.type, "x0": sc.x, "v0": sc.v,
-                   "w0": sc.w, "q0": sc.q, "marks": np.array(marks)}
+            text = sc.xml()
+            polys = [t["file"] for t in sc.types if t.get("shape") == "polyhedron"]
+            if polys:
+                out_poly = Path(polys[0]).read_text()
+                text = text.replace(polys[0], POLY_TOKEN)
+            out = {"xml": np.array(text), "type": sc.type, "x0": s0["x"], "v0": s0["v"],
+                   "w0": s0["w"], "q0": s0["q"], "basis0": b0, "marks": np.array(marks)}
+            if polys:
+                out["poly"] = np.array(out_poly)
             # the CPU restatement runs alongside only to record, per particle,
             # the sum of its contact-force magnitudes (the error normaliser)
             from oracle.oracle import Oracle
             from tests.helpers import contact_scale
             o = Oracle(xml)
-            o.set_particles(sc.type, sc.x, sc.v, sc.w, sc.q)
+            o.set_particles(sc.type, s0["x"], s0["v"], s0["w"], s0["q"], b0)
             o.init()
             done = 0
             for m in marks:

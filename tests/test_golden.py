@@ -24,8 +24,13 @@ GOLDEN = Path(__file__).resolve().parent / "golden"
 
 def _load(name, tmp_path):
     g = dict(np.load(GOLDEN / f"{name}.npz"))
+    text = str(g["xml"])
+    if "poly" in g:
+        poly = tmp_path / f"{name}.poly"
+        poly.write_text(str(g["poly"]))
+        text = text.replace("@POLYHEDRON_FILE@", str(poly))
     xml = tmp_path / f"{name}.xml"
-    xml.write_text(str(g["xml"]))
+    xml.write_text(text)
     return g, xml
 
 
@@ -33,10 +38,11 @@ def _hist_dict(own, par, kd, pn):
     return {(int(a), int(b)): (tuple(k), tuple(p)) for a, b, k, p in zip(own, par, kd, pn)}
 
 
-def test_restatement_bitexact_vs_reference_box(tmp_path, oracle_lib):
-    g, xml = _load("settling_box", tmp_path)
+@pytest.mark.parametrize("name", ["settling_box", "convex_pour"])
+def test_restatement_bitexact_vs_reference(tmp_path, oracle_lib, name):
+    g, xml = _load(name, tmp_path)
     o = Oracle(xml)
-    assert o.set_particles(g["type"], g["x0"], g["v0"], g["w0"], g["q0"]) == 0
+    assert o.set_particles(g["type"], g["x0"], g["v0"], g["w0"], g["q0"], g.get("basis0")) == 0
     assert o.init() == 0
     done = 0
     for m in g["marks"]:
@@ -45,6 +51,7 @@ def test_restatement_bitexact_vs_reference_box(tmp_path, oracle_lib):
         s = o.state()
         for k in ("x", "v", "w", "q", "F", "T"):
             assert np.array_equal(s[k], g[f"s{m}_{k}"]), (m, k)
+        assert np.array_equal(o.basis(), g[f"s{m}_basis"])
         assert np.array_equal(o.cells(), g[f"s{m}_cells"])
         own, par, kd, pn, _ = o.history()
         assert _hist_dict(own, par, kd, pn) == _hist_dict(
