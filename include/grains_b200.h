@@ -81,6 +81,19 @@ int gdem_upload_forces(gdem_handle h, const double* F, const double* T);
 int gdem_set_state(gdem_handle h, const double* x, const double* v, const double* w,
                    const double* wbf, const double* q, const double* F, const double* T);
 
+/* Orientation matrices of non-spherical particles (the basis of
+ * RigidBody::m_transform, Geometry/src/Transform.cpp; Particle::
+ * setAngularPosition), row-major, 9 per particle, by particle ID.  Without
+ * this call they are built from q as Matrix::setRotation does
+ * (Geometry/src/Matrix.cpp:114-127); gdem_set_state rebuilds them the same
+ * way.  Allowed only right after gdem_upload_state or gdem_set_state.  For a
+ * spheres-only system it does nothing. */
+int gdem_upload_basis(gdem_handle h, const double* basis);
+
+/* Current orientation matrices by particle ID (9 each, row-major); the
+ * identity for a spheres-only system. */
+int gdem_download_basis(gdem_handle h, double* basis);
+
 /* Maximum and mean translational speed over the particles
  * (AllComponents::ComputeMaxMeanVelocity, Component/src/AllComponents.cpp:
  * 1781-1811), the quantity Grains3D writes to *_VelocityMaxMean.dat. */

@@ -235,6 +235,9 @@ __global__ void __launch_bounds__(256) k_pairs32(DevState S) {
   S.npairs[t] = cnt;
 }
 
+// kConvex: some class is not a sphere, so the GJK narrow phase is compiled in
+// (it is kept out of the sphere-only kernel, whose registers it would triple).
+template <bool kConvex>
 __global__ void __launch_bounds__(256) k_forces32(DevState S) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
@@ -256,32 +259,60 @@ __global__ void __launch_bounds__(256) k_forces32(DevState S) {
     const int idb = S.id[u];
     const float4 hb = S.offh[u], lb = S.offl[u];
     const bool t0 = ida < idb;
-    Rel r = t0 ? relVec(g, di, dj, dk, ha, la, hb, lb) : relVec(g, -di, -dj, -dk, hb, lb, ha, la);
-    ff d2 = ff_add(ff_add(ff_sqr(r.d[0]), ff_sqr(r.d[1])), ff_sqr(r.d[2]));
-    ff nd = ff_sqrt(d2);
-    float4 h0 = t0 ? ha : hb, l0 = t0 ? la : lb, h1 = t0 ? hb : ha, l1 = t0 ? lb : la;
-    ff rs = two_sum(h0.w, h1.w);
-    ff R = quick_two_sum(rs.hi, __fadd_rn(rs.lo, __fadd_rn(l0.w, l1.w)));
-    ff dist = ff_add(nd, ff{-R.hi, -R.lo});
-    float dd = dist.hi;
-    if (S.diag) S.pair_delta[(size_t)t * kPairCap + e] = dd < 0.f ? dd : __int_as_float(0x7f800000);
-    if (!(dd < 0.f)) continue;
     TypeDesc const& tb = S.types[S.type[u]];
     const TypeDesc& tp0 = t0 ? ta : tb;
     const TypeDesc& tp1 = t0 ? tb : ta;
-    if (-dd >= (float)(tp0.crust + tp1.crust)) raise(S.status, kErrContactOverlap);
-    float3 dh = f3(r.d[0].hi, r.d[1].hi, r.d[2].hi);
-    float inv = 1.f / nd.hi;
-    float3 un = dh * inv;
-    float3 lev0 = (h0.w + 0.5f * dd) * un;     // contact point - x0
-    float3 lev1 = lev0 - dh;                    // contact point - x1 (image)
-    float3 pen = dd * un;
-    ModelDesc const& m = S.models[g.model_base + tp0.mat * kMaxMat + tp1.mat];
     const int s0 = t0 ? t : u, s1 = t0 ? u : t;
-    // unit normal p1 -> p0 from the float-float separation (pen = dd * un, dd < 0)
-    d3 dD = mk((double)r.d[0].hi + (double)r.d[0].lo, (double)r.d[1].hi + (double)r.d[1].lo,
-               (double)r.d[2].hi + (double)r.d[2].lo);
-    const RelVel relv = splitRelVel(dD * (-1. / norm(dD)), pointVel(S, s0, lev0) - pointVel(S, s1, lev1));
+    float dd;
+    float3 lev0, lev1, pen;
+    d3 nD;
+    if (!kConvex || (ta.shape == 0 && tb.shape == 0)) {
+      Rel r = t0 ? relVec(g, di, dj, dk, ha, la, hb, lb) : relVec(g, -di, -dj, -dk, hb, lb, ha, la);
+      ff d2 = ff_add(ff_add(ff_sqr(r.d[0]), ff_sqr(r.d[1])), ff_sqr(r.d[2]));
+      ff nd = ff_sqrt(d2);
+      float4 h0 = t0 ? ha : hb, l0 = t0 ? la : lb, h1 = t0 ? hb : ha, l1 = t0 ? lb : la;
+      ff rs = two_sum(h0.w, h1.w);
+      ff R = quick_two_sum(rs.hi, __fadd_rn(rs.lo, __fadd_rn(l0.w, l1.w)));
+      ff dist = ff_add(nd, ff{-R.hi, -R.lo});
+      dd = dist.hi;
+      if (S.diag) S.pair_delta[(size_t)t * kPairCap + e] = dd < 0.f ? dd : __int_as_float(0x7f800000);
+      if (!(dd < 0.f)) continue;
+      if (-dd >= (float)(tp0.crust + tp1.crust)) raise(S.status, kErrContactOverlap);
+      float3 dh = f3(r.d[0].hi, r.d[1].hi, r.d[2].hi);
+      float inv = 1.f / nd.hi;
+      float3 un = dh * inv;
+      lev0 = (h0.w + 0.5f * dd) * un;     // contact point - x0
+      lev1 = lev0 - dh;                   // contact point - x1 (image)
+      pen = dd * un;
+      // unit normal p1 -> p0 from the float-float separation (pen = dd * un, dd < 0)
+      d3 dD = mk((double)r.d[0].hi + (double)r.d[0].lo, (double)r.d[1].hi + (double)r.d[1].lo,
+                 (double)r.d[2].hi + (double)r.d[2].lo);
+      nD = dD * (-1. / norm(dD));
+    } else {
+      // convex bodies: closest points by GJK on the FP64 state
+      int sh[3];
+      neighbourKey(g, cc.x, cc.y, cc.z, di, dj, dk, sh);
+      const d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
+      // lower ID at its own position, the other at its image seen from it
+      const d3 xt = ld3(S.x, cap, t), xu = ld3(S.x, cap, u);
+      const d3 x0 = t0 ? xt : xu;
+      const d3 x1 = t0 ? xu + shift : xt + (-shift);
+      Contact64 ct = convexContact64(convexOf(tp0, S.poly_verts),
+                                     crustXForm(S.basis, cap, s0, tp0.scaling, x0), tp0.radius,
+                                     tp0.crust, convexOf(tp1, S.poly_verts),
+                                     crustXForm(S.basis, cap, s1, tp1.scaling, x1), tp1.radius,
+                                     tp1.crust);
+      if (ct.error) raise(S.status, kErrContactOverlap);
+      if (S.diag) S.pair_delta[(size_t)t * kPairCap + e] = ct.contact && ct.dist < 0. ? (float)ct.dist : __int_as_float(0x7f800000);
+      if (!ct.contact || !(ct.dist < 0.)) continue;
+      dd = (float)ct.dist;
+      lev0 = tof(ct.point - x0);
+      lev1 = tof(ct.point - x1);
+      pen = tof(ct.overlap);
+      nD = ct.overlap / norm(ct.overlap);
+    }
+    ModelDesc const& m = S.models[g.model_base + tp0.mat * kMaxMat + tp1.mat];
+    const RelVel relv = splitRelVel(nD, pointVel(S, s0, lev0) - pointVel(S, s1, lev1));
     const float3 wrel = m.rolling ? tof(ld3(S.w, cap, s0) - ld3(S.w, cap, s1)) : f3(0.f, 0.f, 0.f);
     const int id0 = t0 ? ida : idb, id1 = t0 ? idb : ida;
     const unsigned long long key = pairKey(id0, id1);
@@ -307,7 +338,12 @@ __global__ void __launch_bounds__(256) k_forces32(DevState S) {
   const d3 xt = g.wall_count > 0 ? ld3(S.x, cap, t) : mk(0., 0., 0.);
   for (int k = 0; k < g.wall_count; ++k) {
     WallDesc const& wd = S.walls[g.wall_begin + k];
-    Contact64 ct = sphereWall64(xt, ta.radius, ta.crust, wd);
+    Contact64 ct = (!kConvex || ta.shape == 0)
+        ? sphereWall64(xt, ta.radius, ta.crust, wd)
+        : convexContact64(convexOf(ta, S.poly_verts), crustXForm(S.basis, cap, t, ta.scaling, xt),
+                          ta.radius, ta.crust, convexOf(wd),
+                          identityXForm(wd.scaling, mk(wd.centre[0], wd.centre[1], wd.centre[2])),
+                          wd.radius, wd.crust);
     if (S.diag) S.wall_delta[(size_t)t * S.max_walls + k] = ct.contact ? ct.dist : __longlong_as_double(0x7ff0000000000000ll);
     if (ct.error) raise(S.status, kErrContactOverlap);
     if (!ct.contact || !(ct.dist < 0.)) continue;
@@ -342,7 +378,9 @@ void launch_pairs32(DevState const& S, cudaStream_t st) {
   if (S.n) k_pairs32<<<(S.n + 255) / 256, 256, 0, st>>>(S);
 }
 void launch_forces32(DevState const& S, cudaStream_t st) {
-  if (S.n) k_forces32<<<(S.n + 255) / 256, 256, 0, st>>>(S);
+  if (!S.n) return;
+  if (S.any_convex) k_forces32<true><<<(S.n + 255) / 256, 256, 0, st>>>(S);
+  else k_forces32<false><<<(S.n + 255) / 256, 256, 0, st>>>(S);
 }
 
 }  // namespace gdem

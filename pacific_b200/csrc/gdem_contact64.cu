@@ -59,6 +59,9 @@ __device__ __forceinline__ void storeHist(HistTable const& t, int slot, d3 kd, d
   v[6] = sp.x; v[7] = sp.y; v[8] = sp.z;
 }
 
+// kConvex: some class is not a sphere, so the GJK narrow phase is compiled in
+// (it is kept out of the sphere-only kernel, whose registers it would triple).
+template <bool kConvex>
 __global__ void __launch_bounds__(256) k_forces64(DevState S) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
@@ -99,7 +102,17 @@ __global__ void __launch_bounds__(256) k_forces64(DevState S) {
       x1 = xt + (-shift); v1 = vt; w1 = wt; r1 = pa.w; m1 = va.w; q1 = wa.w; c1 = ta.crust;
       mat1 = ta.mat; id1 = ida;
     }
-    Contact64 ct = sphereSphere64(x0, r0, c0, x1, r1, c1);
+    Contact64 ct;
+    if (!kConvex || (ta.shape == 0 && tb.shape == 0)) {
+      ct = sphereSphere64(x0, r0, c0, x1, r1, c1);
+    } else {
+      TypeDesc const& tp0 = t0 ? ta : tb;
+      TypeDesc const& tp1 = t0 ? tb : ta;
+      const int s0 = t0 ? t : u, s1 = t0 ? u : t;
+      ct = convexContact64(convexOf(tp0, S.poly_verts), crustXForm(S.basis, cap, s0, tp0.scaling, x0),
+                           r0, c0, convexOf(tp1, S.poly_verts),
+                           crustXForm(S.basis, cap, s1, tp1.scaling, x1), r1, c1);
+    }
     if (S.diag) S.pair_delta[(size_t)t * kPairCap + e] = ct.contact ? (float)ct.dist : __int_as_float(0x7f800000);
     if (!ct.contact || !(ct.dist < 0.)) continue;
     if (ct.error) raise(S.status, kErrContactOverlap);
@@ -128,7 +141,12 @@ __global__ void __launch_bounds__(256) k_forces64(DevState S) {
   // walls: the particle is p0, the obstacle p1 (mass Component::m_massObstacle)
   for (int k = 0; k < g.wall_count; ++k) {
     WallDesc const& wd = S.walls[g.wall_begin + k];
-    Contact64 ct = sphereWall64(xt, pa.w, ta.crust, wd);
+    Contact64 ct = (!kConvex || ta.shape == 0)
+        ? sphereWall64(xt, pa.w, ta.crust, wd)
+        : convexContact64(convexOf(ta, S.poly_verts), crustXForm(S.basis, cap, t, ta.scaling, xt),
+                          ta.radius, ta.crust, convexOf(wd),
+                          identityXForm(wd.scaling, mk(wd.centre[0], wd.centre[1], wd.centre[2])),
+                          wd.radius, wd.crust);
     if (S.diag) S.wall_delta[(size_t)t * S.max_walls + k] = ct.contact ? ct.dist : __longlong_as_double(0x7ff0000000000000ll);
     if (ct.error) raise(S.status, kErrContactOverlap);
     if (!ct.contact || !(ct.dist < 0.)) continue;
@@ -159,7 +177,9 @@ void launch_pairs64(DevState const& S, cudaStream_t st) {
   if (S.n) k_pairs64<<<(S.n + 255) / 256, 256, 0, st>>>(S);
 }
 void launch_forces64(DevState const& S, cudaStream_t st) {
-  if (S.n) k_forces64<<<(S.n + 255) / 256, 256, 0, st>>>(S);
+  if (!S.n) return;
+  if (S.any_convex) k_forces64<true><<<(S.n + 255) / 256, 256, 0, st>>>(S);
+  else k_forces64<false><<<(S.n + 255) / 256, 256, 0, st>>>(S);
 }
 
 }  // namespace gdem

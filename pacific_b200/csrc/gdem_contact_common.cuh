@@ -4,6 +4,7 @@
 // reference functions cited beside it.
 #pragma once
 #include "gdem_device.cuh"
+#include "gdem_gjk.cuh"
 
 namespace gdem {
 
@@ -146,6 +147,59 @@ __device__ __forceinline__ Contact64 sphereWall64(d3 xa, double ra, double ca, W
     c.contact = true;
   }
   return c;
+}
+
+// RigidBodyWithCrust::ClosestPoint, general branch (RigidBodyWithCrust.cpp:
+// 277-351): bounding-sphere test on the circumscribed radii, GJK between the
+// crust-shrunk bodies, overlap = distance - crustA - crustB along the
+// witness direction, contact at the witness midpoint.  A GJK distance below
+// 1e-10 is the reference's ContactError (it then retries with a 10x crust
+// shrink); here it raises the overlap status and no force is applied.
+__device__ inline Contact64 convexContact64(ConvexRef const& a, XForm64 const& a2w, double Ra,
+                                            double ca, ConvexRef const& b, XForm64 const& b2w,
+                                            double Rb, double cb) {
+  Contact64 c;
+  c.contact = false;
+  c.error = false;
+  c.dist = 1.;
+  d3 gg = a2w.o - b2w.o;
+  if (!(norm(gg) < Ra + Rb)) return c;
+  d3 pA, pB;
+  int it = 0;
+  double distance = closestPoints64(a, a2w, b, b2w, pA, pB, &it);
+  if (distance < 1.0e-10) { c.error = true; return c; }
+  d3 ba = pA - pB;
+  d3 contact = pA / 2.0 + pB / 2.0;
+  d3 ov = ba / distance;
+  ov.x = fabs(ov.x) < 1.0e-10 ? 0. : ov.x;
+  ov.y = fabs(ov.y) < 1.0e-10 ? 0. : ov.y;
+  ov.z = fabs(ov.z) < 1.0e-10 ? 0. : ov.z;
+  ov = ov * (ca + cb - distance);
+  distance = distance - (ca + cb);
+  c.point = contact;
+  c.overlap = ov;
+  c.dist = distance;
+  c.contact = true;
+  return c;
+}
+
+__device__ __forceinline__ ConvexRef convexOf(TypeDesc const& t, const double* verts) {
+  ConvexRef r;
+  r.kind = t.shape;
+  r.radius = t.radius;
+  r.extent = mk(t.extent[0], t.extent[1], t.extent[2]);
+  r.verts = verts ? verts + 3 * t.poly_begin : nullptr;
+  r.nverts = t.poly_count;
+  return r;
+}
+__device__ __forceinline__ ConvexRef convexOf(WallDesc const& w) {
+  ConvexRef r;
+  r.kind = 1;
+  r.radius = w.radius;
+  r.extent = mk(w.extent[0], w.extent[1], w.extent[2]);
+  r.verts = nullptr;
+  r.nverts = 0;
+  return r;
 }
 
 // HookeMemoryContactForceModel::computeTangentialVector (:54-65)

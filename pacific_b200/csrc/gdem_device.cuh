@@ -100,7 +100,9 @@ struct DevState {
   int* status;
   GridDesc const* grids; TypeDesc const* types; ModelDesc const* models;
   WallDesc const* walls;
+  const double* poly_verts;   // polyhedron vertices of all classes (x, y, z)
   int max_walls;          // walls of the largest instance
+  int any_convex;         // some class is not a sphere (GJK narrow phase)
 };
 
 // ----------------------------------------------------------- FP64 helpers --

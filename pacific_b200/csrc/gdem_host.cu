@@ -16,11 +16,14 @@
 // Steps after the first of a gdem_step call are replayed from two captured
 // CUDA graphs (the double-buffered state and history tables alternate with
 // period two).
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
 #include <map>
 #include <memory>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -66,6 +69,7 @@ struct InstanceDesc {
   GridDesc grid;
   std::vector<TypeDesc> types;
   std::vector<WallDesc> walls;
+  std::vector<double> poly_verts;   // polyhedron vertices of this instance (x, y, z)
   ModelDesc models[kMaxMat * kMaxMat];
   double gravity[3];
   double dt;
@@ -119,6 +123,87 @@ void collectObstacles(XmlNode const* n, std::vector<XmlNode const*>& out) {
   }
 }
 
+// Polyhedron description file (Polyhedron::create and Polyhedron::readface,
+// Geometry/src/Polyhedron.cpp:143-180, 580-620): "<token> <nb_vertices>", one
+// vertex per line, "<nb_faces>", then one line of vertex indices per face.
+struct PolyFile {
+  std::vector<std::array<double, 3>> verts;
+  std::vector<std::vector<int>> faces;
+};
+
+PolyFile readPolyFile(std::string const& path) {
+  std::ifstream in(path);
+  if (!in) throw std::runtime_error("cannot open polyhedron file " + path);
+  PolyFile P;
+  int tok = 0, nv = 0, nf = 0;
+  if (!(in >> tok >> nv) || nv < 4) throw std::runtime_error("bad polyhedron header in " + path);
+  P.verts.resize(nv);
+  for (auto& v : P.verts)
+    if (!(in >> v[0] >> v[1] >> v[2])) throw std::runtime_error("bad polyhedron vertex in " + path);
+  if (!(in >> nf) || nf < 4) throw std::runtime_error("bad polyhedron face count in " + path);
+  std::string line;
+  std::getline(in, line);
+  for (int f = 0; f < nf; ++f) {
+    if (!std::getline(in, line)) throw std::runtime_error("missing polyhedron face in " + path);
+    std::istringstream ls(line);
+    std::vector<int> face;
+    int k;
+    while (ls >> k) {
+      if (k < 0 || k >= nv) throw std::runtime_error("polyhedron face index out of range in " + path);
+      face.push_back(k);
+    }
+    if (face.size() < 3) throw std::runtime_error("polyhedron face with fewer than 3 vertices in " + path);
+    P.faces.push_back(face);
+  }
+  return P;
+}
+
+// Volume and principal inertia (unit density) of the tetrahedron (origin, a,
+// b, c), by Tonon's closed form (F. Tonon, J. Math. Stat. 1 (2004) 8-11), as
+// used by GrainsExec::computeVolumeInertiaContrib (Base/src/GrainsExec.cpp:
+// 746-797).  The sums run in the same order as there so that the masses agree
+// to the last bit.
+void tetMass(std::array<double, 3> const& a, std::array<double, 3> const& b,
+             std::array<double, 3> const& c, double& vol, double* I) {
+  const double o = 0.;
+  double x2 = a[0], x3 = b[0], x4 = c[0], y2 = a[1], y3 = b[1], y4 = c[1];
+  double z2 = a[2], z3 = b[2], z4 = c[2];
+  double det = std::fabs((x2 - o) * (y3 - o) * (z4 - o) + (y2 - o) * (z3 - o) * (x4 - o) +
+                         (z2 - o) * (x3 - o) * (y4 - o) - (z2 - o) * (y3 - o) * (x4 - o) -
+                         (x2 - o) * (z3 - o) * (y4 - o) - (y2 - o) * (x3 - o) * (z4 - o));
+  vol += det / 6.;
+  // sum over i <= j of u_i u_j for the four vertices (u_1 = 0), continued
+  auto chain = [](double s, double u2, double u3, double u4) {
+    const double u1 = 0.;
+    s = s + u1 * u1; s = s + u1 * u2; s = s + u2 * u2; s = s + u1 * u3; s = s + u2 * u3;
+    s = s + u3 * u3; s = s + u1 * u4; s = s + u2 * u4; s = s + u3 * u4; s = s + u4 * u4;
+    return s;
+  };
+  I[0] += det * chain(chain(0., y2, y3, y4), z2, z3, z4) / 60.;
+  I[1] += det * chain(chain(0., x2, x3, x4), z2, z3, z4) / 60.;
+  I[2] += det * chain(chain(0., x2, x3, x4), y2, y3, y4) / 60.;
+}
+
+// Polyhedron volume and inertia: triangles form tetrahedra with the origin,
+// larger faces are fanned around their vertex centroid (Polyhedron::
+// BuildInertia / computeVolumeInertia, Geometry/src/Polyhedron.cpp).
+void polyMassProperties(PolyFile const& P, double& vol, double* Iv) {
+  vol = 0.;
+  Iv[0] = Iv[1] = Iv[2] = 0.;
+  for (auto const& f : P.faces) {
+    int nf = (int)f.size();
+    if (nf == 3) {
+      tetMass(P.verts[f[0]], P.verts[f[1]], P.verts[f[2]], vol, Iv);
+    } else {
+      std::array<double, 3> G = {0., 0., 0.};
+      for (int j = 0; j < nf; ++j)
+        for (int d = 0; d < 3; ++d) G[d] += P.verts[f[j]][d];
+      for (int d = 0; d < 3; ++d) G[d] = G[d] / double(nf);
+      for (int j = 0, k = nf - 1; j < nf; k = j++) tetMass(G, P.verts[f[k]], P.verts[f[j]], vol, Iv);
+    }
+  }
+}
+
 InstanceDesc readInstance(std::string const& path) {
   auto doc = parseXmlFile(path);
   XmlNode const* root = doc.get();
@@ -155,18 +240,52 @@ InstanceDesc readInstance(std::string const& path) {
     if (!cv) throw std::runtime_error("<Particle> without <Convex>");
     t.crust = cv->attrD("CrustThickness");
     if (!(t.crust > 0.)) throw std::runtime_error("crust thickness must be > 0");
+    double vol = 0., Iv[3] = {0., 0., 0.};
     if (XmlNode const* sp = cv->child("Sphere")) {
       double r = sp->attrD("Radius");
       t.shape = 0;
       t.radius = r;
-      double vol = 4.0 * PI * std::pow(r, 3.) / 3.0;                  // Sphere::getVolume
-      t.mass = density * vol;
+      vol = 4.0 * PI * std::pow(r, 3.) / 3.0;                         // Sphere::getVolume
       double I0 = 8.0 * PI * std::pow(r, 5.) / 15.0;                  // Sphere::BuildInertia
-      t.inertia[0] = t.inertia[1] = t.inertia[2] = I0 * density;
-      t.eqrad = std::pow((0.75 / PI) * vol, 1. / 3.);                 // getEquivalentSphereRadius
+      Iv[0] = Iv[1] = Iv[2] = I0;
+      t.extent[0] = t.extent[1] = t.extent[2] = r;
+    } else if (XmlNode const* bx = cv->child("Box")) {
+      // Box::getVolume, Box::BuildInertia, Box::computeCircumscribedRadius
+      // (Geometry/src/Box.cpp); the XML gives full lengths
+      t.shape = 1;
+      double e[3] = {0.5 * bx->attrD("LX"), 0.5 * bx->attrD("LY"), 0.5 * bx->attrD("LZ")};
+      for (int d = 0; d < 3; ++d) t.extent[d] = e[d];
+      t.radius = std::sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+      vol = 8.0 * e[0] * e[1] * e[2];
+      Iv[0] = 8.0 * e[0] * e[1] * e[2] * (e[1] * e[1] + e[2] * e[2]) / 3.0;
+      Iv[1] = 8.0 * e[0] * e[1] * e[2] * (e[0] * e[0] + e[2] * e[2]) / 3.0;
+      Iv[2] = 8.0 * e[0] * e[1] * e[2] * (e[0] * e[0] + e[1] * e[1]) / 3.0;
+    } else if (XmlNode const* ph = cv->child("Polyhedron")) {
+      t.shape = 2;
+      PolyFile P = readPolyFile(ph->attr("Name"));
+      polyMassProperties(P, vol, Iv);
+      double ray = 0.;
+      for (auto const& v : P.verts) ray = std::max(ray, v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+      t.radius = std::sqrt(ray);                 // Polyhedron::computeCircumscribedRadius
+      // identity-frame bounding box (Convex::bbox, Convex.cpp:29-41)
+      for (int d = 0; d < 3; ++d) {
+        double lo = P.verts[0][d], hi = P.verts[0][d];
+        for (auto const& v : P.verts) { lo = std::min(lo, v[d]); hi = std::max(hi, v[d]); }
+        t.extent[d] = (hi - lo) / 2.;
+      }
+      t.poly_begin = (int)I.poly_verts.size() / 3;
+      t.poly_count = (int)P.verts.size();
+      for (auto const& v : P.verts)
+        for (int d = 0; d < 3; ++d) I.poly_verts.push_back(v[d]);
     } else {
       throw std::runtime_error("unsupported particle shape in <Convex>");
     }
+    t.mass = density * vol;
+    for (int d = 0; d < 3; ++d) t.inertia[d] = Iv[d] * density;
+    t.eqrad = std::pow((0.75 / PI) * vol, 1. / 3.);                   // getEquivalentSphereRadius
+    // crust shrink factors (RigidBodyWithCrust ctor, RigidBodyWithCrust.cpp:58-78)
+    for (int d = 0; d < 3; ++d)
+      t.scaling[d] = t.extent[d] < 1.e-10 ? 1. : (t.extent[d] - t.crust) / t.extent[d];
     XmlNode const* mat = pn->child("Material");
     if (!mat) throw std::runtime_error("<Particle> without <Material>");
     t.mat = materialIndex(mats, morder, mat->valueS());
@@ -201,6 +320,10 @@ InstanceDesc readInstance(std::string const& path) {
       w.mat = materialIndex(mats, morder, mat->valueS());
       double vol = 8. * w.extent[0] * w.extent[1] * w.extent[2];
       w.eqrad = std::pow((0.75 / PI) * vol, 1. / 3.);
+      w.radius = std::sqrt(w.extent[0] * w.extent[0] + w.extent[1] * w.extent[1] +
+                           w.extent[2] * w.extent[2]);
+      for (int d = 0; d < 3; ++d)
+        w.scaling[d] = w.extent[d] < 1.e-10 ? 1. : (w.extent[d] - w.crust) / w.extent[d];
       w.id = (int)I.walls.size();
       I.walls.push_back(w);
     }
@@ -295,9 +418,11 @@ struct System {
   DevState S{};
   GridDesc* d_grids = nullptr; TypeDesc* d_types = nullptr; ModelDesc* d_models = nullptr;
   WallDesc* d_walls = nullptr;
+  double* d_poly = nullptr;        // polyhedron vertex table of all instances
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool have_state = false, started = false, diag = false, use_graphs = true;
+  bool id_order = false;           // state arrays are in particle-ID order (not yet binned)
   double last_ms = 0.;
   int status_host = 0;
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -326,7 +451,8 @@ struct System {
     if (d_types) cudaFree(d_types);
     if (d_models) cudaFree(d_models);
     if (d_walls) cudaFree(d_walls);
-    d_grids = nullptr; d_types = nullptr; d_models = nullptr; d_walls = nullptr;
+    if (d_poly) cudaFree(d_poly);
+    d_grids = nullptr; d_types = nullptr; d_models = nullptr; d_walls = nullptr; d_poly = nullptr;
     for (auto& e : evpool) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
     evpool.clear();
     if (ev0) cudaEventDestroy(ev0);
@@ -382,7 +508,9 @@ struct System {
     std::vector<TypeDesc> types;
     std::vector<ModelDesc> models;
     std::vector<WallDesc> walls;
+    std::vector<double> poly;
     int cell_offset = 0, max_walls = 1;
+    S.any_convex = 0;
     for (auto& I : inst) {
       GridDesc g = I.grid;
       g.cell_offset = cell_offset;
@@ -391,7 +519,13 @@ struct System {
       g.wall_count = (int)I.walls.size();
       g.model_base = (int)models.size();
       type_base.push_back((int)types.size());
-      for (auto const& t : I.types) types.push_back(t);
+      const int vbase = (int)poly.size() / 3;
+      for (auto const& t : I.types) {
+        types.push_back(t);
+        if (t.shape == 2) types.back().poly_begin += vbase;
+        if (t.shape != 0) S.any_convex = 1;
+      }
+      poly.insert(poly.end(), I.poly_verts.begin(), I.poly_verts.end());
       for (auto const& w : I.walls) walls.push_back(w);
       for (int k = 0; k < kMaxMat * kMaxMat; ++k) models.push_back(I.models[k]);
       max_walls = std::max(max_walls, (int)I.walls.size());
@@ -409,7 +543,9 @@ struct System {
       if (!vec.empty()) CK(cudaMemcpy(dst, vec.data(), vec.size() * sizeof(T), cudaMemcpyHostToDevice));
     };
     up(d_grids, grids); up(d_types, types); up(d_models, models); up(d_walls, walls);
+    up(d_poly, poly);
     S.grids = d_grids; S.types = d_types; S.models = d_models; S.walls = d_walls;
+    S.poly_verts = d_poly;
   }
 
   void allocateParticles(int n) {
@@ -423,7 +559,9 @@ struct System {
     S.x2 = alloc<double>(3 * c); S.v2 = alloc<double>(3 * c); S.w2 = alloc<double>(3 * c);
     S.wbf2 = alloc<double>(3 * c); S.q2 = alloc<double>(4 * c);
     S.F = alloc<double>(3 * c); S.T = alloc<double>(3 * c);
-    S.basis = nullptr; S.basis2 = nullptr;
+    // orientation matrices, SoA (9 x cap), only when some class is not a sphere
+    S.basis = S.any_convex ? alloc<double>(9 * c) : nullptr;
+    S.basis2 = S.any_convex ? alloc<double>(9 * c) : nullptr;
     S.skey = alloc<int>(c); S.rank = alloc<int>(c); S.order = alloc<int>(c);
     S.cell_count = alloc<int>(S.ncells); S.cell_start = alloc<int>(S.ncells + 1);
     S.scan_tmp = alloc<int>((S.ncells + 1023) / 1024 + 1);
@@ -473,6 +611,7 @@ struct System {
                       d_type_id, d_inst_id, stream);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(stream));
+    id_order = true;
   }
 
   void swapState() {
@@ -487,6 +626,7 @@ struct System {
   // moving != 0, and build the pair list.
   void binAndPairs(int moving, bool pre_kick) {
     double dt = S.dt;
+    id_order = false;
     timed("scan", [&] { launch_scan(S, stream); });
     timed("place", [&] { launch_place(S, stream); });
     timed("cellsort", [&] { launch_cellsort(S, stream); });
@@ -827,6 +967,44 @@ int gdem_download_state(gdem_handle h, double* x, double* v, double* w, double* 
         {x, dx, 3}, {v, dv, 3}, {w, dw, 3}, {wbf, dwb, 3}, {q, dq, 4}, {F, dF, 3}, {T, dT, 3}};
     for (auto& it : items)
       if (it.h) CK(cudaMemcpyAsync(it.h, it.d, it.k * n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return GDEM_OK;
+  });
+}
+
+int gdem_upload_basis(gdem_handle h, const double* basis) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state || !basis) throw std::runtime_error("upload the state first");
+    if (!s->id_order)
+      throw std::runtime_error("orientations can only be set right after gdem_upload_state or gdem_set_state");
+    DevState& S = s->S;
+    if (!S.basis) return GDEM_OK;   // spheres only: orientation matrices are not used
+    size_t n = (size_t)S.n, c = (size_t)S.cap;
+    std::vector<double> hb(9 * c, 0.);
+    for (size_t i = 0; i < n; ++i)
+      for (int k = 0; k < 9; ++k) hb[k * c + i] = basis[9 * i + k];
+    CK(cudaMemcpy(S.basis, hb.data(), hb.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return GDEM_OK;
+  });
+}
+
+int gdem_download_basis(gdem_handle h, double* basis) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state || !basis) throw std::runtime_error("no state");
+    DevState& S = s->S;
+    size_t n = (size_t)S.n;
+    if (!S.basis) {
+      // spheres carry no orientation matrix: report the identity
+      for (size_t i = 0; i < n; ++i)
+        for (int k = 0; k < 9; ++k) basis[9 * i + k] = (k % 4 == 0) ? 1. : 0.;
+      return GDEM_OK;
+    }
+    double* d = s->d_stage;   // 22 doubles per particle: room for 9
+    launch_basis_by_id(S, d, 0, s->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(basis, d, 9 * n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
     return GDEM_OK;
   });

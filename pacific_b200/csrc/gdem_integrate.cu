@@ -278,7 +278,7 @@ __global__ void k_move_gather(DevState S, int moving, double h, double dt, int p
       qdt = qmk(mk(0., 0., 0.), 1.);
     }
     q = qmul(qdt, q);
-    if (S.basis && tp.shape != 0) {
+    if (S.basis) {
       // Transform::composeLeftByRotation (Geometry/src/Transform.cpp:140-159)
       double mm[9], out[9];
 #pragma unroll
@@ -358,6 +358,16 @@ __global__ void k_scatter_by_id(DevState S, double* out_x, double* out_v, double
   }
 }
 
+// Orientation matrices (row-major, 9 per particle) into ID order.
+__global__ void k_basis_by_id(DevState S, double* out, int id_base) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= S.n) return;
+  int i = S.id[t] - id_base;
+  if (i < 0 || i >= S.n) return;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) out[9 * (size_t)i + k] = S.basis[k * S.cap + t];
+}
+
 __global__ void k_cells_by_id(DevState S, int* ijk, int id_base) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
@@ -401,6 +411,19 @@ __global__ void k_load_state(DevState S, const double* x, const double* v, const
   }
 #pragma unroll
   for (int k = 0; k < 4; ++k) S.q[k * cap + i] = q[4 * i + k];
+  if (S.basis) {
+    // orientation matrix of q with the expression order of Matrix::setRotation
+    // (Geometry/src/Matrix.cpp:114-127); gdem_upload_basis may replace it
+    double x = q[4 * i], y = q[4 * i + 1], z = q[4 * i + 2], w4 = q[4 * i + 3];
+    double s = 2.0 / (x * x + y * y + z * z + w4 * w4);
+    double xs = x * s, ys = y * s, zs = z * s;
+    double wx = w4 * xs, wy = w4 * ys, wz = w4 * zs;
+    double xx = x * xs, xy = x * ys, xz = x * zs, yy = y * ys, yz = y * zs, zz = z * zs;
+    double m[9] = {1.0 - (yy + zz), xy - wz, xz + wy, xy + wz, 1.0 - (xx + zz), yz - wx,
+                   xz - wy, yz + wx, 1.0 - (xx + yy)};
+#pragma unroll
+    for (int k = 0; k < 9; ++k) S.basis[k * cap + i] = m[k];
+  }
   if (!wbf) {
     // q* (w, q) (ParticleKinematics.cpp:220-221)
     dq qq = qmk(mk(q[4 * i], q[4 * i + 1], q[4 * i + 2]), q[4 * i + 3]);
@@ -507,6 +530,9 @@ void launch_move_gather(DevState const& S, int moving, double h, double dt, int 
 void launch_scatter_by_id(DevState const& S, double* x, double* v, double* w, double* wbf,
                           double* q, double* F, double* T, int id_base, cudaStream_t st) {
   if (S.n) k_scatter_by_id<<<blocks(S.n, 256), 256, 0, st>>>(S, x, v, w, wbf, q, F, T, id_base);
+}
+void launch_basis_by_id(DevState const& S, double* out, int id_base, cudaStream_t st) {
+  if (S.n && S.basis) k_basis_by_id<<<blocks(S.n, 256), 256, 0, st>>>(S, out, id_base);
 }
 void launch_cells_by_id(DevState const& S, int* ijk, int id_base, cudaStream_t st) {
   if (S.n) k_cells_by_id<<<blocks(S.n, 256), 256, 0, st>>>(S, ijk, id_base);

@@ -15,6 +15,7 @@ void launch_place(DevState const& S, cudaStream_t st);
 void launch_cellsort(DevState const& S, cudaStream_t st);
 void launch_scatter_by_id(DevState const& S, double* x, double* v, double* w, double* wbf,
                           double* q, double* F, double* T, int id_base, cudaStream_t st);
+void launch_basis_by_id(DevState const& S, double* out, int id_base, cudaStream_t st);
 void launch_cells_by_id(DevState const& S, int* ijk, int id_base, cudaStream_t st);
 void launch_hist_zero_cumulative(HistTable const& t, int fp64, cudaStream_t st);
 void launch_load_state(DevState const& S, const double* x, const double* v, const double* w,

@@ -50,8 +50,12 @@ struct TypeDesc {
   double eqrad;          // Component::getEquivalentSphereRadius
   double weight[3];      // m (1 - rho_f / rho) g
   int mat;               // material index
-  int shape;             // 0 sphere, 1 box, 2 cylinder, 3 polyhedron
+  int shape;             // 0 sphere, 1 box, 2 polyhedron
   float r_hi, r_lo;      // radius as a float-float pair
+  double extent[3];      // box half lengths / bounding-box half extent
+  double scaling[3];     // crust shrink factors (extent - crust) / extent
+  int poly_begin;        // first vertex of a polyhedron in the vertex table
+  int poly_count;        // its vertex count
 };
 
 // HookeMemory / Hooke parameters (HookeMemoryContactForceModel.cpp:12-27).
@@ -70,6 +74,8 @@ struct WallDesc {
   double extent[3];      // half lengths
   double crust;
   double eqrad;
+  double radius;         // circumscribed radius |extent|
+  double scaling[3];     // crust shrink factors
   int mat;
   int id;                // obstacle index within its instance
 };

@@ -81,6 +81,8 @@ def library() -> ctypes.CDLL:
         "gdem_step": ([_P, ctypes.c_int], ctypes.c_int),
         "gdem_download_state": ([_P, _DP, _DP, _DP, _DP, _DP, _DP, _DP], ctypes.c_int),
         "gdem_download_cells": ([_P, _IP], ctypes.c_int),
+        "gdem_upload_basis": ([_P, _DP], ctypes.c_int),
+        "gdem_download_basis": ([_P, _DP], ctypes.c_int),
         "gdem_set_diagnostics": ([_P, ctypes.c_int], ctypes.c_int),
         "gdem_download_contacts": ([_P, i64, ctypes.POINTER(i64), _IP, _IP, _DP], ctypes.c_int),
         "gdem_status": ([_P, _IP, ctypes.c_int], ctypes.c_int),
@@ -170,6 +172,17 @@ class Grains:
                                                  _dp(arrs[1]), _dp(arrs[2]), _dp(arrs[3]),
                                                  _dp(arrs[4])))
         self.n = n
+
+    def upload_basis(self, basis):
+        """Orientation matrices (n, 3, 3) or (n, 9), row-major, by particle ID;
+        only right after upload_state / set_state.  Without it they follow q."""
+        b = _f64(basis, (self.n, 9))
+        self._check(library().gdem_upload_basis(self._h, _dp(b)))
+
+    def download_basis(self):
+        out = np.empty((self.n, 9))
+        self._check(library().gdem_download_basis(self._h, _dp(out)))
+        return out
 
     def upload_forces(self, F, T):
         F = _f64(F, (self.n, 3))

@@ -7,10 +7,11 @@ quaternions, forces, torques, cells, contact memory) and to round-off on the
 periodic gas (the reference's periodic clones round the image translation in
 a different order than the minimum-image convention).
 
-GPU: starting from the reference's own state at step k (state + contact
-memory), one CUDA step reproduces the reference's step k+1: cells and contact
-sets exactly, forces and torques within 1e-10 (FP64) / 1e-5 (FP32-split) of
-each particle's sum of contact-force magnitudes.
+GPU: starting from the reference's own state at step k (state, orientation
+matrices of the cubes and tetrahedra, contact memory), one CUDA step
+reproduces the reference's step k+1: cells and contact sets exactly, forces
+and torques within 1e-10 (FP64) / 1e-5 (FP32-split) of each particle's sum of
+contact-force magnitudes, orientation matrices within 1e-14.
 """
 from pathlib import Path
 
@@ -86,6 +87,8 @@ def _gpu_step_from_golden(g, xml, k, k1, precision, tol):
     from tests.helpers import contact_set
     G = Grains(xml, precision)
     G.upload_state(g["type"], g[f"s{k}_x"], g[f"s{k}_v"], g[f"s{k}_w"], g[f"s{k}_q"])
+    if f"s{k}_basis" in g:
+        G.upload_basis(g[f"s{k}_basis"])
     G.upload_forces(g[f"s{k}_F"], g[f"s{k}_T"])
     own, par = g[f"s{k}_hist_owner"], g[f"s{k}_hist_partner"]
     G.upload_history(own, par, g[f"s{k}_hist_kdelta"], g[f"s{k}_hist_prevn"])
@@ -94,6 +97,7 @@ def _gpu_step_from_golden(g, xml, k, k1, precision, tol):
     s = G.download_state()
     cells = G.download_cells()
     id0, id1, _ = G.download_contacts()
+    s["basis"] = G.download_basis()
     G.close()
     ref_pairs = {(min(a, b), max(a, b)) if b >= 0 else (a, b)
                  for a, b in zip(g[f"s{k1}_hist_owner"].tolist(), g[f"s{k1}_hist_partner"].tolist())}
@@ -106,7 +110,7 @@ def _gpu_step_from_golden(g, xml, k, k1, precision, tol):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["settling_box", "periodic_gas"])
+@pytest.mark.parametrize("name", ["settling_box", "periodic_gas", "convex_pour"])
 def test_gpu_fp64_step_matches_reference(tmp_path, lib, name):
     from pacific_b200 import FP64
     g, xml = _load(name, tmp_path)
@@ -116,11 +120,13 @@ def test_gpu_fp64_step_matches_reference(tmp_path, lib, name):
         assert np.array_equal(cells, g[f"s{k1}_cells"])
         assert gc == rc
         assert np.max(np.abs(s["x"] - g[f"s{k1}_x"])) <= 1e-15
+        if f"s{k1}_basis" in g:
+            assert np.max(np.abs(s["basis"] - g[f"s{k1}_basis"])) <= 1e-14
         assert fe.max(initial=0) <= 1e-10 and te.max(initial=0) <= 1e-10
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["settling_box", "periodic_gas"])
+@pytest.mark.parametrize("name", ["settling_box", "periodic_gas", "convex_pour"])
 def test_gpu_fp32split_step_matches_reference(tmp_path, lib, name):
     from pacific_b200 import FP32_SPLIT
     g, xml = _load(name, tmp_path)
