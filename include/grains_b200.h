@@ -134,9 +134,12 @@ int gdem_set_diagnostics(gdem_handle h, int on);
 
 /* Contacts (overlap < 0) of the last force evaluation: *count receives the
  * number of contacts; when capacity >= *count the arrays are filled with
- * (id0 < id1) pairs and their overlap distance; walls appear as id1 = -(k+2). */
+ * (id0 < id1) pairs, their overlap distance and (force may be NULL) the
+ * contact force exerted on id0, 3 per contact (the per-contact record of
+ * AppCollision / PostProcessingWriter force output); walls appear as
+ * id1 = -(k+2), with the force on the particle. */
 int gdem_download_contacts(gdem_handle h, int64_t capacity, int64_t* count, int* id0,
-                           int* id1, double* delta);
+                           int* id1, double* delta, double* force);
 
 /* OR of the status bits raised since creation (or the last reset). */
 int gdem_status(gdem_handle h, int* bits, int reset);

@@ -135,8 +135,10 @@ typedef std::tuple<int, int, int> Key;
 
 struct Model {
   double kn, en, etat, muc, kt, mur, etarpf, epst;
+  double kr;       // Hooke rolling coefficient
   double beta;
-  bool rolling;
+  bool memory;     // HookeMemory (true) or Hooke (false)
+  bool rolling;    // HookeMemory: mur != 0; Hooke: kr != 0
 };
 
 // Convex shape of a particle class or a wall.
@@ -208,7 +210,7 @@ typedef struct {
   const int* wall_matbit;
   int n_models;
   const int* model_mask;
-  const double* model_params;  // kn en etat muc kt mur etarpf epst
+  const double* model_params;  // kn en etat muc kt mur etarpf epst kr memory (10 per model)
   // convex particle classes (NULL: all spheres)
   const int* type_shape;       // 0 sphere, 1 box, 2 polyhedron
   const double* type_extent;   // box half lengths, 3 per class
@@ -874,6 +876,58 @@ void hookeMemory(Model const& m, Body& p0, Body& p1, double dt, PointContact con
   mOn0 = delM;
 }
 
+// HookeContactForceModel::performForcesCalculus (HookeContactForceModel.cpp:
+// 44-121): the same normal law without tangential memory; the viscous
+// tangential force is capped at muc |Fn|, and the optional rolling moment is
+// kr Req |Fn| |w x r|_rel / |w_rel| against w_rel.
+void hooke(Model const& m, Body const& p0, Body const& p1, PointContact const& ci, V3& fOn0,
+           V3& mOn0) {
+  V3 pcp = ci.point;
+  V3 pen = ci.overlap;
+  V3 normal = pen;
+  normal = normal / norm(normal);
+  round3(normal);
+  V3 v0 = p0.v + cross(p0.w, pcp - p0.x);
+  V3 v1 = p1.v + cross(p1.w, pcp - p1.x);
+  V3 tmpV = v0 - v1;
+  V3 v_n = normal * dot(tmpV, normal);
+  V3 v_t = tmpV - v_n;
+  V3 delFN = m.kn * pen;
+  double avmass = 1. / (1. / p0.mass + 1. / p1.mass);
+  double gamman = -2. * m.beta * std::sqrt(avmass * m.kn);
+  delFN -= gamman * v_n;
+  double normFN = norm(delFN);
+  double etat = m.etat == -1. ? -m.beta * std::sqrt(m.kn / avmass) : m.etat;
+  double gammat = 2. * etat * avmass;
+  V3 delFT = -gammat * v_t;
+  double fn = m.muc * normFN;
+  double ft = norm(delFT);
+  if (fn < ft) {
+    double normv_t = norm(v_t);
+    V3 tangent(0., 0., 0.);
+    if (normv_t > EPSILON) tangent = (-v_t) / normv_t;
+    delFT = tangent * fn;
+  }
+  V3 delM(0., 0., 0.);
+  if (m.kr != 0.) {
+    V3 wrel = p0.w - p1.w;
+    double normwrel = norm(wrel);
+    double normwtrel = norm(cross(p0.w, p0.x - pcp) - cross(p1.w, p1.x - pcp));
+    if (normwrel > EPSILON) {
+      double Req = 1. / (1. / p0.rad + 1. / p1.rad);
+      delM = -(m.kr * Req * normFN * normwtrel / normwrel) * wrel;
+    }
+  }
+  fOn0 = 1. * (delFN + delFT);
+  mOn0 = delM * 1.;
+}
+
+void contactLaw(Model const& m, Body& b0, Body& b1, double dt, PointContact const& pc, V3& f,
+                V3& mm) {
+  if (m.memory) hookeMemory(m, b0, b1, dt, pc, f, mm);
+  else hooke(m, b0, b1, pc, f, mm);
+}
+
 void addForce(Particle& p, V3 const& point, V3 const& f) {   // Torsor::addForce
   p.F += f;
   V3 a = point - p.ref;
@@ -893,7 +947,7 @@ void interactPP(System& s, Particle& p0, Particle& p1, V3 const& shift) {
   Body b0{p0.x, p0.v, p0.w, p0.mass, p0.eqrad, &p0.cmap, p0.id};
   Body b1{xb, p1.v, p1.w, p1.mass, p1.eqrad, &p1.cmap, p1.id};
   V3 f, mm;
-  hookeMemory(m, b0, b1, s.dt, pc, f, mm);
+  contactLaw(m, b0, b1, s.dt, pc, f, mm);
   addForce(p0, pc.point, f);
   if (m.rolling) p0.T += mm;
   // p1 torque lever arm uses its own (image) reference point
@@ -927,7 +981,7 @@ void interactPW(System& s, Particle& p, Wall& w, int k) {
   b1.x = w.centre;
   b1.rad = std::pow((0.75 / PI) * (8. * w.extent[0] * w.extent[1] * w.extent[2]), 1. / 3.);
   V3 f, mm;
-  hookeMemory(m, b0, b1, s.dt, pc, f, mm);
+  contactLaw(m, b0, b1, s.dt, pc, f, mm);
   addForce(p, pc.point, f);
   if (m.rolling) p.T += mm;
   ContactRec r{p.id, w.id, pc.dist, pc.point, pc.overlap, f};
@@ -1128,11 +1182,13 @@ void* or_create(or_config const* c) {
     s->walls.push_back(w);
   }
   for (int k = 0; k < c->n_models; ++k) {
-    const double* q = c->model_params + 8 * k;
+    const double* q = c->model_params + 10 * k;
     Model m;
     m.kn = q[0]; m.en = q[1]; m.etat = q[2]; m.muc = q[3];
     m.kt = q[4]; m.mur = q[5]; m.etarpf = q[6]; m.epst = q[7];
-    m.rolling = m.mur != 0.;
+    m.kr = q[8];
+    m.memory = q[9] != 0.;
+    m.rolling = m.memory ? m.mur != 0. : m.kr != 0.;
     m.beta = std::log(m.en) / std::sqrt(PI * PI + std::log(m.en) * std::log(m.en));
     s->models[c->model_mask[k]] = m;
   }

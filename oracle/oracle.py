@@ -160,14 +160,20 @@ def read_xml(path):
         m = cf.find("Material")
         mask = matbit(m.get("materialA")) | matbit(m.get("materialB"))
         law = cf.find("HookeMemory")
+        memory = law is not None
+        if not memory:
+            law = cf.find("Hooke")
+        if law is None:
+            raise ValueError("only Hooke and HookeMemory contact laws are restated")
 
         def val(tag, dflt=None):
             e = law.find(tag)
             return float(e.text) if e is not None else dflt
 
         models.append(dict(mask=mask, params=[val("kn"), val("en"), val("etat", -1.0), val("muc"),
-                                              val("kt"), val("mur", 0.0), val("etarpf", 0.0),
-                                              val("epst", 0.0)]))
+                                              val("kt", 0.0), val("mur", 0.0), val("etarpf", 0.0),
+                                              val("epst", 0.0), val("kr", 0.0),
+                                              1.0 if memory else 0.0]))
     g = root.find("Forces").find("Gravity")
     cfg.update(types=types, walls=walls, models=models,
                gravity=[float(g.get(k)) for k in ("GX", "GY", "GZ")],

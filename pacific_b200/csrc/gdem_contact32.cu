@@ -1,17 +1,21 @@
 // gdem_contact32.cu -- FP32-split mode contact kernels.
 //
-// Positions enter as the particle's cell (integer) plus its offset from the
-// cell's lower corner, held as an unevaluated float pair (hi + lo).  The
-// vector between two particles in neighbouring cells is then
-//     d = dc * edge + (off_b - off_a),      dc in {-1, 0, 1}
-// which is formed in float-float arithmetic (error-free two-sum / two-product
-// with fmaf), so the overlap  |d| - (ra + rb)  keeps ~44 bits although every
-// operation is an FP32 operation.  For each active contact, the relative
-// velocity at the contact point and its split into normal and tangential
-// parts are formed from the FP64 state (they are differences of nearly equal
-// quantities); the HookeMemory force law, the tangential history, the torque
-// lever arms and the per-particle reduction are FP32.  Results are written to
-// the FP64 force/torque arrays that the FP64 leapfrog consumes.
+// Broad phase: positions enter as the particle's cell (integer) plus its FP32
+// offset from the cell's lower corner, so the vector between two particles in
+// neighbouring cells,  d = dc * edge + (off_b - off_a)  with dc in {-1, 0, 1},
+// is formed from small FP32 numbers whatever the domain size; candidates are
+// kept with a relative margin of 4e-6 on the sum of radii.
+//
+// Narrow phase: each kept candidate (a near contact: a few per particle) is
+// decided on the FP64 master positions with the reference's expressions, so
+// contact sets equal the FP64 mode's and the overlap keeps FP64 accuracy even
+// for a contact that has only just formed (an FP32 or float-float overlap
+// would carry a relative error of 1e-5 when the overlap is 1e-11 m).  The
+// relative velocity at the contact point and its normal/tangential split are
+// formed in FP64 too (differences of nearly equal quantities).  The Hooke /
+// HookeMemory force law, the tangential history, the torque lever arms and
+// the per-particle reduction are FP32.  Results are written to the FP64
+// force/torque arrays that the FP64 leapfrog consumes.
 //
 // Reference functions restated: ClosestPointSPHERESPHERE
 // (Geometry/src/RigidBodyWithCrust.cpp:596-639), HookeMemoryContactForceModel
@@ -23,43 +27,6 @@
 namespace gdem {
 
 namespace {
-
-// ------------------------------------------------------ float-float ops --
-struct ff { float hi, lo; };
-__device__ __forceinline__ ff two_sum(float a, float b) {
-  float s = __fadd_rn(a, b);
-  float bb = __fadd_rn(s, -a);
-  float e = __fadd_rn(__fadd_rn(a, -__fadd_rn(s, -bb)), __fadd_rn(b, -bb));
-  return {s, e};
-}
-__device__ __forceinline__ ff quick_two_sum(float a, float b) {
-  float s = __fadd_rn(a, b);
-  return {s, __fadd_rn(b, -__fadd_rn(s, -a))};
-}
-__device__ __forceinline__ ff ff_add(ff a, ff b) {
-  ff s = two_sum(a.hi, b.hi);
-  return quick_two_sum(s.hi, __fadd_rn(s.lo, __fadd_rn(a.lo, b.lo)));
-}
-__device__ __forceinline__ ff ff_sqr(ff a) {
-  float p = __fmul_rn(a.hi, a.hi);
-  float e = fmaf(a.hi, a.hi, -p);
-  return quick_two_sum(p, __fadd_rn(e, __fmul_rn(__fmul_rn(2.f, a.hi), a.lo)));
-}
-__device__ __forceinline__ ff ff_sqrt(ff a) {
-  float x = __fsqrt_rn(a.hi);
-  float p = __fmul_rn(x, x);
-  float e = fmaf(x, x, -p);
-  float r = __fadd_rn(__fadd_rn(__fadd_rn(a.hi, -p), -e), a.lo);
-  return quick_two_sum(x, __fdiv_rn(r, __fmul_rn(2.f, x)));
-}
-// One component of d = dc * edge + (ob - oa)
-__device__ __forceinline__ ff relComp(int dc, float eh, float el, float oah, float oal,
-                                      float obh, float obl) {
-  ff s = two_sum(obh, -oah);
-  ff t = two_sum((float)dc * eh, s.hi);
-  float lo = __fadd_rn(__fadd_rn(__fadd_rn(s.lo, t.lo), __fadd_rn(obl, -oal)), (float)dc * el);
-  return quick_two_sum(t.hi, lo);
-}
 
 // ------------------------------------------------------------ float3 ops --
 __device__ __forceinline__ float3 f3(float a, float b, float c) { return make_float3(a, b, c); }
@@ -194,15 +161,39 @@ __device__ __forceinline__ void storeHistF(HistTable const& t, int slot, float3 
   v[6] = sp.x; v[7] = sp.y; v[8] = sp.z;
 }
 
-// Canonical relative vector (p0 = lower ID) from the split positions.
-struct Rel { ff d[3]; };
-__device__ __forceinline__ Rel relVec(GridDesc const& g, int dcx, int dcy, int dcz,
-                                      float4 h0, float4 l0, float4 h1, float4 l1) {
-  Rel r;
-  r.d[0] = relComp(dcx, g.edge_hi[0], g.edge_lo[0], h0.x, l0.x, h1.x, l1.x);
-  r.d[1] = relComp(dcy, g.edge_hi[1], g.edge_lo[1], h0.y, l0.y, h1.y, l1.y);
-  r.d[2] = relComp(dcz, g.edge_hi[2], g.edge_lo[2], h0.z, l0.z, h1.z, l1.z);
-  return r;
+// Hooke law (no tangential memory) in FP32, seen from p0 (same structure as
+// hooke64).  lev0 / lev1 are the contact point relative to p0 / p1; w0, w1
+// the space-fixed angular velocities.
+__device__ __forceinline__ void hooke32(ModelDesc const& m, float kn, float beta, float3 pen,
+                                        RelVel const& rv, float3 w0, float3 w1, float3 lev0,
+                                        float3 lev1, float m0, float rad0, float m1, float rad1,
+                                        float3& f, float3& mr) {
+  const float3 v_n = rv.vn;
+  const float3 v_t = rv.vt;
+  float avmass = 1.f / (1.f / m0 + 1.f / m1);
+  float gamman = -2.f * beta * sqrtf(avmass * kn);
+  float3 delFN = kn * pen - gamman * v_n;
+  float normFN = normf3(delFN);
+  float etat = m.etat == -1. ? -beta * sqrtf(kn / avmass) : (float)m.etat;
+  float gammat = 2.f * etat * avmass;
+  float3 delFT = -gammat * v_t;
+  float fn = (float)m.muc * normFN;
+  if (fn < normf3(delFT)) {
+    float nvt = normf3(v_t);
+    delFT = nvt > 1.e-10f ? (-fn / nvt) * v_t : f3(0.f, 0.f, 0.f);
+  }
+  mr = f3(0.f, 0.f, 0.f);
+  if (m.kr != 0.) {
+    float3 wrel = w0 - w1;
+    float nwr = normf3(wrel);
+    // w0 x (x0 - pc) - w1 x (x1 - pc) = w1 x lev1 - w0 x lev0
+    float nwt = normf3(crossf(w1, lev1) - crossf(w0, lev0));
+    if (nwr > 1.e-10f) {
+      float Req = 1.f / (1.f / rad0 + 1.f / rad1);
+      mr = (-((float)m.kr * Req * normFN * nwt / nwr)) * wrel;
+    }
+  }
+  f = delFN + delFT;
 }
 
 __global__ void __launch_bounds__(256) k_pairs32(DevState S) {
@@ -214,7 +205,7 @@ __global__ void __launch_bounds__(256) k_pairs32(DevState S) {
   int* out = S.pairs + (size_t)t * kPairCap;
   int cnt = 0;
   const float4* __restrict__ offh = S.offh;
-  const float ex = g.edge_hi[0], ey = g.edge_hi[1], ez = g.edge_hi[2];
+  const float ex = g.edge_f[0], ey = g.edge_f[1], ez = g.edge_f[2];
   forEachCandidate(S.cell_start, g, cc, [&](int u, int dcx, int dj, int dk, int, int, int) {
     if (u == t) return;
     const float4 hb = offh[u];
@@ -246,7 +237,7 @@ __global__ void __launch_bounds__(256) k_forces32(DevState S) {
   GridDesc const& g = S.grids[cc.w];
   const int ida = S.id[t];
   TypeDesc const& ta = S.types[S.type[t]];
-  const float4 ha = S.offh[t], la = S.offl[t];
+  const d3 xt = ld3(S.x, cap, t);
   float3 Fs = f3(0.f, 0.f, 0.f), Ts = f3(0.f, 0.f, 0.f);
   const float dt = (float)S.dt;
   const int np = S.npairs[t];
@@ -257,74 +248,63 @@ __global__ void __launch_bounds__(256) k_forces32(DevState S) {
     int di, dj, dk;
     offDecode((int)(ent >> 27), &di, &dj, &dk);
     const int idb = S.id[u];
-    const float4 hb = S.offh[u], lb = S.offl[u];
     const bool t0 = ida < idb;
     TypeDesc const& tb = S.types[S.type[u]];
     const TypeDesc& tp0 = t0 ? ta : tb;
     const TypeDesc& tp1 = t0 ? tb : ta;
     const int s0 = t0 ? t : u, s1 = t0 ? u : t;
-    float dd;
-    float3 lev0, lev1, pen;
-    d3 nD;
+    // exact narrow phase on the FP64 master positions: lower ID at its own
+    // position, the other at its periodic image seen from it
+    int sh[3];
+    neighbourKey(g, cc.x, cc.y, cc.z, di, dj, dk, sh);
+    const d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
+    const d3 xu = ld3(S.x, cap, u);
+    const d3 x0 = t0 ? xt : xu;
+    const d3 x1 = t0 ? xu + shift : xt + (-shift);
+    Contact64 ct;
     if (!kConvex || (ta.shape == 0 && tb.shape == 0)) {
-      Rel r = t0 ? relVec(g, di, dj, dk, ha, la, hb, lb) : relVec(g, -di, -dj, -dk, hb, lb, ha, la);
-      ff d2 = ff_add(ff_add(ff_sqr(r.d[0]), ff_sqr(r.d[1])), ff_sqr(r.d[2]));
-      ff nd = ff_sqrt(d2);
-      float4 h0 = t0 ? ha : hb, l0 = t0 ? la : lb, h1 = t0 ? hb : ha, l1 = t0 ? lb : la;
-      ff rs = two_sum(h0.w, h1.w);
-      ff R = quick_two_sum(rs.hi, __fadd_rn(rs.lo, __fadd_rn(l0.w, l1.w)));
-      ff dist = ff_add(nd, ff{-R.hi, -R.lo});
-      dd = dist.hi;
-      if (S.diag) S.pair_delta[(size_t)t * kPairCap + e] = dd < 0.f ? dd : __int_as_float(0x7f800000);
-      if (!(dd < 0.f)) continue;
-      if (-dd >= (float)(tp0.crust + tp1.crust)) raise(S.status, kErrContactOverlap);
-      float3 dh = f3(r.d[0].hi, r.d[1].hi, r.d[2].hi);
-      float inv = 1.f / nd.hi;
-      float3 un = dh * inv;
-      lev0 = (h0.w + 0.5f * dd) * un;     // contact point - x0
-      lev1 = lev0 - dh;                   // contact point - x1 (image)
-      pen = dd * un;
-      // unit normal p1 -> p0 from the float-float separation (pen = dd * un, dd < 0)
-      d3 dD = mk((double)r.d[0].hi + (double)r.d[0].lo, (double)r.d[1].hi + (double)r.d[1].lo,
-                 (double)r.d[2].hi + (double)r.d[2].lo);
-      nD = dD * (-1. / norm(dD));
+      ct = sphereSphere64(x0, tp0.radius, tp0.crust, x1, tp1.radius, tp1.crust);
     } else {
-      // convex bodies: closest points by GJK on the FP64 state
-      int sh[3];
-      neighbourKey(g, cc.x, cc.y, cc.z, di, dj, dk, sh);
-      const d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
-      // lower ID at its own position, the other at its image seen from it
-      const d3 xt = ld3(S.x, cap, t), xu = ld3(S.x, cap, u);
-      const d3 x0 = t0 ? xt : xu;
-      const d3 x1 = t0 ? xu + shift : xt + (-shift);
-      Contact64 ct = convexContact64(convexOf(tp0, S.poly_verts),
-                                     crustXForm(S.basis, cap, s0, tp0.scaling, x0), tp0.radius,
-                                     tp0.crust, convexOf(tp1, S.poly_verts),
-                                     crustXForm(S.basis, cap, s1, tp1.scaling, x1), tp1.radius,
-                                     tp1.crust);
-      if (ct.error) raise(S.status, kErrContactOverlap);
-      if (S.diag) S.pair_delta[(size_t)t * kPairCap + e] = ct.contact && ct.dist < 0. ? (float)ct.dist : __int_as_float(0x7f800000);
-      if (!ct.contact || !(ct.dist < 0.)) continue;
-      dd = (float)ct.dist;
-      lev0 = tof(ct.point - x0);
-      lev1 = tof(ct.point - x1);
-      pen = tof(ct.overlap);
-      nD = ct.overlap / norm(ct.overlap);
+      ct = convexContact64(convexOf(tp0, S.poly_verts),
+                           crustXForm(S.basis, cap, s0, tp0.scaling, x0), tp0.radius, tp0.crust,
+                           convexOf(tp1, S.poly_verts),
+                           crustXForm(S.basis, cap, s1, tp1.scaling, x1), tp1.radius, tp1.crust);
     }
+    if (S.diag) S.pair_delta[(size_t)t * kPairCap + e] = ct.contact && ct.dist < 0. ? ct.dist : __longlong_as_double(0x7ff0000000000000ll);
+    if (!ct.contact || !(ct.dist < 0.)) continue;
+    if (ct.error) raise(S.status, kErrContactOverlap);
+    // the force law from here on is FP32
+    const float3 lev0 = tof(ct.point - x0);
+    const float3 lev1 = tof(ct.point - x1);
+    const float3 pen = tof(ct.overlap);
+    const d3 nD = ct.overlap / norm(ct.overlap);
     ModelDesc const& m = S.models[g.model_base + tp0.mat * kMaxMat + tp1.mat];
     const RelVel relv = splitRelVel(nD, pointVel(S, s0, lev0) - pointVel(S, s1, lev1));
-    const float3 wrel = m.rolling ? tof(ld3(S.w, cap, s0) - ld3(S.w, cap, s1)) : f3(0.f, 0.f, 0.f);
-    const int id0 = t0 ? ida : idb, id1 = t0 ? idb : ida;
-    const unsigned long long key = pairKey(id0, id1);
-    int old = histFind(S.hist_old, key);
-    float3 kd, pn, sp, f, mr;
-    if (old >= 0) loadHistF(S.hist_old, old, kd, pn, sp);
-    hodc32(m, (float)m.kn, (float)m.beta, dt, pen, relv, wrel, (float)tp0.mass, (float)tp0.eqrad,
-           (float)tp1.mass, (float)tp1.eqrad, old >= 0, kd, pn, sp, f, mr);
+    float3 f, mr;
+    if (m.memory) {
+      const float3 wrel = m.rolling ? tof(ld3(S.w, cap, s0) - ld3(S.w, cap, s1)) : f3(0.f, 0.f, 0.f);
+      const int id0 = t0 ? ida : idb, id1 = t0 ? idb : ida;
+      const unsigned long long key = pairKey(id0, id1);
+      int old = histFind(S.hist_old, key);
+      float3 kd, pn, sp;
+      if (old >= 0) loadHistF(S.hist_old, old, kd, pn, sp);
+      hodc32(m, (float)m.kn, (float)m.beta, dt, pen, relv, wrel, (float)tp0.mass,
+             (float)tp0.eqrad, (float)tp1.mass, (float)tp1.eqrad, old >= 0, kd, pn, sp, f, mr);
+      if (t0) {
+        int slot = histInsert(S.hist_new, key);
+        if (slot < 0) raise(S.status, kErrHashFull);
+        else storeHistF(S.hist_new, slot, kd, pn, sp);
+      }
+    } else {
+      hooke32(m, (float)m.kn, (float)m.beta, pen, relv, tof(ld3(S.w, cap, s0)),
+              tof(ld3(S.w, cap, s1)), lev0, lev1, (float)tp0.mass, (float)tp0.eqrad,
+              (float)tp1.mass, (float)tp1.eqrad, f, mr);
+    }
+    if (S.diag) {
+      double* fd = S.pair_force + 3 * ((size_t)t * kPairCap + e);
+      fd[0] = f.x; fd[1] = f.y; fd[2] = f.z;
+    }
     if (t0) {
-      int slot = histInsert(S.hist_new, key);
-      if (slot < 0) raise(S.status, kErrHashFull);
-      else storeHistF(S.hist_new, slot, kd, pn, sp);
       Fs = Fs + f;
       Ts = Ts + crossf(lev0, f);
       if (m.rolling) Ts = Ts + mr;
@@ -335,7 +315,6 @@ __global__ void __launch_bounds__(256) k_forces32(DevState S) {
     }
   }
   // walls: geometry from the FP64 master position, force law in FP32
-  const d3 xt = g.wall_count > 0 ? ld3(S.x, cap, t) : mk(0., 0., 0.);
   for (int k = 0; k < g.wall_count; ++k) {
     WallDesc const& wd = S.walls[g.wall_begin + k];
     Contact64 ct = (!kConvex || ta.shape == 0)
@@ -348,20 +327,31 @@ __global__ void __launch_bounds__(256) k_forces32(DevState S) {
     if (ct.error) raise(S.status, kErrContactOverlap);
     if (!ct.contact || !(ct.dist < 0.)) continue;
     ModelDesc const& m = S.models[g.model_base + ta.mat * kMaxMat + wd.mat];
-    const unsigned long long key = wallKey(ida, k);
-    int old = histFind(S.hist_old, key);
-    float3 kd, pn, sp, f, mr;
-    if (old >= 0) loadHistF(S.hist_old, old, kd, pn, sp);
+    float3 f, mr;
     d3 l0 = ct.point - xt;
     float3 lev0 = f3((float)l0.x, (float)l0.y, (float)l0.z);
     float3 pen = f3((float)ct.overlap.x, (float)ct.overlap.y, (float)ct.overlap.z);
     const RelVel relv = splitRelVel(ct.overlap / norm(ct.overlap), pointVel(S, t, lev0));
     const float3 wrel = tof(ld3(S.w, cap, t));
-    hodc32(m, (float)m.kn, (float)m.beta, dt, pen, relv, wrel, (float)ta.mass, (float)ta.eqrad,
-           1.e20f, (float)wd.eqrad, old >= 0, kd, pn, sp, f, mr);
-    int slot = histInsert(S.hist_new, key);
-    if (slot < 0) raise(S.status, kErrHashFull);
-    else storeHistF(S.hist_new, slot, kd, pn, sp);
+    if (m.memory) {
+      const unsigned long long key = wallKey(ida, k);
+      int old = histFind(S.hist_old, key);
+      float3 kd, pn, sp;
+      if (old >= 0) loadHistF(S.hist_old, old, kd, pn, sp);
+      hodc32(m, (float)m.kn, (float)m.beta, dt, pen, relv, wrel, (float)ta.mass,
+             (float)ta.eqrad, 1.e20f, (float)wd.eqrad, old >= 0, kd, pn, sp, f, mr);
+      int slot = histInsert(S.hist_new, key);
+      if (slot < 0) raise(S.status, kErrHashFull);
+      else storeHistF(S.hist_new, slot, kd, pn, sp);
+    } else {
+      d3 l1 = ct.point - mk(wd.centre[0], wd.centre[1], wd.centre[2]);
+      hooke32(m, (float)m.kn, (float)m.beta, pen, relv, wrel, f3(0.f, 0.f, 0.f), lev0, tof(l1),
+              (float)ta.mass, (float)ta.eqrad, 1.e20f, (float)wd.eqrad, f, mr);
+    }
+    if (S.diag) {
+      double* fd = S.wall_force + 3 * ((size_t)t * S.max_walls + k);
+      fd[0] = f.x; fd[1] = f.y; fd[2] = f.z;
+    }
     Fs = Fs + f;
     Ts = Ts + crossf(lev0, f);
     if (m.rolling) Ts = Ts + mr;

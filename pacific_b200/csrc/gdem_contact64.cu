@@ -113,21 +113,31 @@ __global__ void __launch_bounds__(256) k_forces64(DevState S) {
                            r0, c0, convexOf(tp1, S.poly_verts),
                            crustXForm(S.basis, cap, s1, tp1.scaling, x1), r1, c1);
     }
-    if (S.diag) S.pair_delta[(size_t)t * kPairCap + e] = ct.contact ? (float)ct.dist : __int_as_float(0x7f800000);
+    if (S.diag) S.pair_delta[(size_t)t * kPairCap + e] = ct.contact ? ct.dist : __longlong_as_double(0x7ff0000000000000ll);
     if (!ct.contact || !(ct.dist < 0.)) continue;
     if (ct.error) raise(S.status, kErrContactOverlap);
     ModelDesc const& m = S.models[g.model_base + mat0 * kMaxMat + mat1];
-    const unsigned long long key = pairKey(id0, id1);
-    int old = histFind(S.hist_old, key);
-    d3 kd, pn, sp;
-    if (old >= 0) loadHist(S.hist_old, old, kd, pn, sp);
     d3 f, mr;
-    hodc64(m, dt, ct.point, ct.overlap, x0, v0, w0, m0, q0, x1, v1, w1, m1, q1, old >= 0,
-           kd, pn, sp, f, mr);
+    if (m.memory) {
+      const unsigned long long key = pairKey(id0, id1);
+      int old = histFind(S.hist_old, key);
+      d3 kd, pn, sp;
+      if (old >= 0) loadHist(S.hist_old, old, kd, pn, sp);
+      hodc64(m, dt, ct.point, ct.overlap, x0, v0, w0, m0, q0, x1, v1, w1, m1, q1, old >= 0,
+             kd, pn, sp, f, mr);
+      if (t0) {
+        int slot = histInsert(S.hist_new, key);
+        if (slot < 0) raise(S.status, kErrHashFull);
+        else storeHist(S.hist_new, slot, kd, pn, sp);
+      }
+    } else {
+      hooke64(m, ct.point, ct.overlap, x0, v0, w0, m0, q0, x1, v1, w1, m1, q1, f, mr);
+    }
+    if (S.diag) {
+      double* fd = S.pair_force + 3 * ((size_t)t * kPairCap + e);
+      fd[0] = f.x; fd[1] = f.y; fd[2] = f.z;
+    }
     if (t0) {
-      int slot = histInsert(S.hist_new, key);
-      if (slot < 0) raise(S.status, kErrHashFull);
-      else storeHist(S.hist_new, slot, kd, pn, sp);
       F = F + f;
       T = T + cross(ct.point - x0, f);
       if (m.rolling) T = T + mr;
@@ -151,18 +161,27 @@ __global__ void __launch_bounds__(256) k_forces64(DevState S) {
     if (ct.error) raise(S.status, kErrContactOverlap);
     if (!ct.contact || !(ct.dist < 0.)) continue;
     ModelDesc const& m = S.models[g.model_base + ta.mat * kMaxMat + wd.mat];
-    const unsigned long long key = wallKey(ida, k);
-    int old = histFind(S.hist_old, key);
-    d3 kd, pn, sp;
-    if (old >= 0) loadHist(S.hist_old, old, kd, pn, sp);
     d3 f, mr;
-    d3 zero = mk(0., 0., 0.);
-    hodc64(m, dt, ct.point, ct.overlap, xt, vt, wt, va.w, wa.w,
-           mk(wd.centre[0], wd.centre[1], wd.centre[2]), zero, zero, 1.e20, wd.eqrad,
-           old >= 0, kd, pn, sp, f, mr);
-    int slot = histInsert(S.hist_new, key);
-    if (slot < 0) raise(S.status, kErrHashFull);
-    else storeHist(S.hist_new, slot, kd, pn, sp);
+    const d3 zero = mk(0., 0., 0.);
+    const d3 wc = mk(wd.centre[0], wd.centre[1], wd.centre[2]);
+    if (m.memory) {
+      const unsigned long long key = wallKey(ida, k);
+      int old = histFind(S.hist_old, key);
+      d3 kd, pn, sp;
+      if (old >= 0) loadHist(S.hist_old, old, kd, pn, sp);
+      hodc64(m, dt, ct.point, ct.overlap, xt, vt, wt, va.w, wa.w, wc, zero, zero, 1.e20,
+             wd.eqrad, old >= 0, kd, pn, sp, f, mr);
+      int slot = histInsert(S.hist_new, key);
+      if (slot < 0) raise(S.status, kErrHashFull);
+      else storeHist(S.hist_new, slot, kd, pn, sp);
+    } else {
+      hooke64(m, ct.point, ct.overlap, xt, vt, wt, va.w, wa.w, wc, zero, zero, 1.e20, wd.eqrad,
+              f, mr);
+    }
+    if (S.diag) {
+      double* fd = S.wall_force + 3 * ((size_t)t * S.max_walls + k);
+      fd[0] = f.x; fd[1] = f.y; fd[2] = f.z;
+    }
     F = F + f;
     T = T + cross(ct.point - xt, f);
     if (m.rolling) T = T + mr;

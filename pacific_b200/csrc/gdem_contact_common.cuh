@@ -268,4 +268,50 @@ __device__ inline void hodc64(ModelDesc const& m, double dt, d3 pcp, d3 pen,
   f = 1. * (delFN + delFT);
 }
 
+// HookeContactForceModel::performForcesCalculus (HookeContactForceModel.cpp:
+// 44-121): the normal law of hodc64 without tangential memory; the viscous
+// tangential force is capped at muc |Fn|; with kr != 0 a rolling-resistance
+// moment -kr Req |Fn| |w0 x (x0 - pc) - w1 x (x1 - pc)| / |w0 - w1| (w0 - w1).
+__device__ inline void hooke64(ModelDesc const& m, d3 pcp, d3 pen, d3 x0, d3 v0, d3 w0,
+                               double m0, double rad0, d3 x1, d3 v1, d3 w1, double m1,
+                               double rad1, d3& f, d3& mr) {
+  d3 normal = pen;
+  normal = normal / norm(normal);
+  normal.x = fabs(normal.x) < 1.0e-10 ? 0. : normal.x;     // Group3::round
+  normal.y = fabs(normal.y) < 1.0e-10 ? 0. : normal.y;
+  normal.z = fabs(normal.z) < 1.0e-10 ? 0. : normal.z;
+  d3 va = v0 + cross(w0, pcp - x0);
+  d3 vb = v1 + cross(w1, pcp - x1);
+  d3 tmpV = va - vb;
+  d3 v_n = normal * dot(tmpV, normal);
+  d3 v_t = tmpV - v_n;
+  d3 delFN = m.kn * pen;
+  double avmass = 1. / (1. / m0 + 1. / m1);
+  double gamman = -2. * m.beta * sqrt(avmass * m.kn);
+  delFN = delFN - gamman * v_n;
+  double normFN = norm(delFN);
+  double etat = m.etat == -1. ? -m.beta * sqrt(m.kn / avmass) : m.etat;
+  double gammat = 2. * etat * avmass;
+  d3 delFT = -gammat * v_t;
+  double fn = m.muc * normFN;
+  double ft = norm(delFT);
+  if (fn < ft) {
+    double normv_t = norm(v_t);
+    d3 tangent = mk(0., 0., 0.);
+    if (normv_t > 1.0e-10) tangent = (-v_t) / normv_t;
+    delFT = tangent * fn;
+  }
+  mr = mk(0., 0., 0.);
+  if (m.kr != 0.) {
+    d3 wrel = w0 - w1;
+    double normwrel = norm(wrel);
+    double normwtrel = norm(cross(w0, x0 - pcp) - cross(w1, x1 - pcp));
+    if (normwrel > 1.0e-10) {
+      double Req = 1. / (1. / rad0 + 1. / rad1);
+      mr = -(m.kr * Req * normFN * normwtrel / normwrel) * wrel;
+    }
+  }
+  f = 1. * (delFN + delFT);
+}
+
 }  // namespace gdem

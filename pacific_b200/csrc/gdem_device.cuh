@@ -86,15 +86,14 @@ struct DevState {
   double4* pos64;         // x, y, z, radius
   double4* vel64;         // v, mass
   double4* omg64;         // w (space frame), equivalent radius
-  float4* offh;           // cell-relative offset, hi part; radius hi
-  float4* offl;           // lo parts; radius lo
-  float4* velf;           // unused (FP32-split reads FP64 velocities per contact)
-  float4* omgf;           // w (float)
+  float4* offh;           // FP32 cell-relative offset; FP32 radius
   int4* cellc;            // cell i, j, k and instance
   // pair list: per-particle segments of kPairCap entries
   int* pairs; int* npairs;
-  float* pair_delta;      // diagnostics: overlap of each entry (+inf: no contact)
+  double* pair_delta;     // diagnostics: overlap of each entry (+inf: no contact)
   double* wall_delta;     // diagnostics: overlap with each wall slot
+  double* pair_force;     // diagnostics: contact force on the lower ID (3 per entry)
+  double* wall_force;     // diagnostics: wall contact force on the particle (3 per slot)
   int diag;
   HistTable hist_old, hist_new;
   int* status;

@@ -97,8 +97,9 @@ double childD(XmlNode const* n, const char* name, bool required, double dflt) {
 }
 
 // HookeMemoryContactForceModel::defineParameters (:256-310) and
-// HookeContactForceModel::defineParameters.  A missing <epst> leaves epst at
-// zero in the reference (the default is stored under the key "eps").
+// HookeContactForceModel::defineParameters (HookeContactForceModel.cpp:
+// 170-200, where <kr> is required).  A missing <epst> leaves epst at zero in
+// the reference (the default is stored under the key "eps").
 ModelDesc readModel(XmlNode const* law, std::string const& kind) {
   ModelDesc m{};
   m.kn = childD(law, "kn", true, 0.);
@@ -109,8 +110,9 @@ ModelDesc readModel(XmlNode const* law, std::string const& kind) {
   m.etarpf = childD(law, "etarpf", false, 0.);
   m.kt = childD(law, "kt", kind == "HookeMemory", 0.);
   m.epst = childD(law, "epst", false, 0.);
-  m.rolling = m.mur != 0. ? 1 : 0;
+  m.kr = childD(law, "kr", kind == "Hooke", 0.);
   m.memory = kind == "HookeMemory" ? 1 : 0;
+  m.rolling = (m.memory ? m.mur != 0. : m.kr != 0.) ? 1 : 0;
   m.beta = std::log(m.en) / std::sqrt(PI * PI + std::log(m.en) * std::log(m.en));
   m.valid = 1;
   return m;
@@ -289,8 +291,7 @@ InstanceDesc readInstance(std::string const& path) {
     XmlNode const* mat = pn->child("Material");
     if (!mat) throw std::runtime_error("<Particle> without <Material>");
     t.mat = materialIndex(mats, morder, mat->valueS());
-    t.r_hi = (float)t.radius;
-    t.r_lo = (float)(t.radius - (double)t.r_hi);
+    t.r_f = (float)t.radius;
     maxR = std::max(maxR, t.radius);
     I.types.push_back(t);
   }
@@ -371,9 +372,6 @@ InstanceDesc readInstance(std::string const& path) {
       if (!I.models[t.mat * kMaxMat + w.mat].valid)
         throw std::runtime_error("no contact force model for a particle/obstacle material pair");
   }
-  for (auto const& t : I.types)
-    if (!I.models[t.mat * kMaxMat + t.mat].memory)
-      throw std::runtime_error("only HookeMemory is implemented on the device");
   // gravity and time step
   I.gravity[0] = I.gravity[1] = I.gravity[2] = 0.;
   if (XmlNode const* fo = root->find("Forces"))
@@ -402,8 +400,7 @@ InstanceDesc readInstance(std::string const& path) {
       g.lc_origin[d] += -g.edge[d];
       g.nb[d] += 2;
     }
-    g.edge_hi[d] = (float)g.edge[d];
-    g.edge_lo[d] = (float)(g.edge[d] - (double)g.edge_hi[d]);
+    g.edge_f[d] = (float)g.edge[d];
   }
   return I;
 }
@@ -568,14 +565,14 @@ struct System {
     S.cellc = alloc<int4>(c);
     if (precision == GDEM_FP64) {
       S.pos64 = alloc<double4>(c); S.vel64 = alloc<double4>(c); S.omg64 = alloc<double4>(c);
-      S.offh = nullptr; S.offl = nullptr; S.velf = nullptr; S.omgf = nullptr;
+      S.offh = nullptr;
     } else {
-      S.offh = alloc<float4>(c); S.offl = alloc<float4>(c);
-      S.velf = nullptr; S.omgf = nullptr;   // contact velocities come from the FP64 state
+      S.offh = alloc<float4>(c);
       S.pos64 = nullptr; S.vel64 = nullptr; S.omg64 = nullptr;
     }
     S.pairs = alloc<int>(c * kPairCap); S.npairs = alloc<int>(c);
     S.pair_delta = nullptr; S.wall_delta = nullptr; S.diag = 0;
+    S.pair_force = nullptr; S.wall_force = nullptr;
     int l2 = nextPow2Log((size_t)8 * c + 64);
     size_t hc = size_t(1) << l2;
     size_t vsz = precision == GDEM_FP64 ? sizeof(double) : sizeof(float);
@@ -1029,8 +1026,10 @@ int gdem_set_diagnostics(gdem_handle h, int on) {
     if (!s || !s->have_state) throw std::runtime_error("upload the state first");
     DevState& S = s->S;
     if (on && !S.pair_delta) {
-      S.pair_delta = s->alloc<float>((size_t)S.cap * kPairCap);
+      S.pair_delta = s->alloc<double>((size_t)S.cap * kPairCap);
       S.wall_delta = s->alloc<double>((size_t)S.cap * S.max_walls);
+      S.pair_force = s->alloc<double>((size_t)S.cap * kPairCap * 3);
+      S.wall_force = s->alloc<double>((size_t)S.cap * S.max_walls * 3);
     }
     S.diag = on ? 1 : 0;
     s->diag = on != 0;
@@ -1040,7 +1039,7 @@ int gdem_set_diagnostics(gdem_handle h, int on) {
 }
 
 int gdem_download_contacts(gdem_handle h, int64_t capacity, int64_t* count, int* id0, int* id1,
-                           double* delta) {
+                           double* delta, double* force) {
   return guarded([&] {
     System* s = sys(h);
     if (!s || !s->started || !count) throw std::runtime_error("invalid arguments");
@@ -1048,29 +1047,41 @@ int gdem_download_contacts(gdem_handle h, int64_t capacity, int64_t* count, int*
     if (!S.pair_delta) throw std::runtime_error("enable diagnostics before the step");
     size_t n = (size_t)S.n;
     std::vector<int> ids(n), np(n), pairs(n * kPairCap);
-    std::vector<float> pd(n * kPairCap);
-    std::vector<double> wd(n * S.max_walls);
+    std::vector<double> pd(n * kPairCap), pf(3 * n * kPairCap);
+    std::vector<double> wd(n * S.max_walls), wf(3 * n * S.max_walls);
     std::vector<int4> cells(n);
     CK(cudaMemcpy(ids.data(), S.id, n * sizeof(int), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(np.data(), S.npairs, n * sizeof(int), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(pairs.data(), S.pairs, n * kPairCap * sizeof(int), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(pd.data(), S.pair_delta, n * kPairCap * sizeof(float), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(wd.data(), S.wall_delta, n * S.max_walls * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(pd.data(), S.pair_delta, pd.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(wd.data(), S.wall_delta, wd.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    if (force) {
+      CK(cudaMemcpy(pf.data(), S.pair_force, pf.size() * sizeof(double), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(wf.data(), S.wall_force, wf.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    }
     CK(cudaMemcpy(cells.data(), S.cellc, n * sizeof(int4), cudaMemcpyDeviceToHost));
     int64_t c = 0;
     for (size_t t = 0; t < n; ++t) {
       for (int e = 0; e < np[t]; ++e) {
         int u = pairs[t * kPairCap + e] & ((1 << 27) - 1);
-        float dl = pd[t * kPairCap + e];
-        if (!(dl < 0.f) || !(ids[t] < ids[u])) continue;
-        if (c < capacity && id0) { id0[c] = ids[t]; id1[c] = ids[u]; delta[c] = dl; }
+        size_t slot = t * kPairCap + e;
+        double dl = pd[slot];
+        if (!(dl < 0.) || !(ids[t] < ids[u])) continue;
+        if (c < capacity && id0) {
+          id0[c] = ids[t]; id1[c] = ids[u]; delta[c] = dl;
+          if (force) for (int d = 0; d < 3; ++d) force[3 * c + d] = pf[3 * slot + d];
+        }
         ++c;
       }
       int nw = s->inst[cells[t].w].walls.size();
       for (int k = 0; k < nw; ++k) {
-        double dl = wd[t * S.max_walls + k];
+        size_t slot = t * S.max_walls + k;
+        double dl = wd[slot];
         if (!(dl < 0.)) continue;
-        if (c < capacity && id0) { id0[c] = ids[t]; id1[c] = -(k + 2); delta[c] = dl; }
+        if (c < capacity && id0) {
+          id0[c] = ids[t]; id1[c] = -(k + 2); delta[c] = dl;
+          if (force) for (int d = 0; d < 3; ++d) force[3 * c + d] = wf[3 * slot + d];
+        }
         ++c;
       }
     }

@@ -322,15 +322,10 @@ __global__ void k_move_gather(DevState S, int moving, double h, double dt, int p
     S.omg64[t] = make_double4(w.x, w.y, w.z, tp.eqrad);
   }
   if (S.offh) {
-    // offset from the cell's lower corner, split into a float pair
-    double o[3] = {x.x - (g.lc_origin[0] + ci * g.edge[0]),
-                   x.y - (g.lc_origin[1] + cj * g.edge[1]),
-                   x.z - (g.lc_origin[2] + ck * g.edge[2])};
-    float hh[3], ll[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) { hh[d] = (float)o[d]; ll[d] = (float)(o[d] - (double)hh[d]); }
-    S.offh[t] = make_float4(hh[0], hh[1], hh[2], tp.r_hi);
-    S.offl[t] = make_float4(ll[0], ll[1], ll[2], tp.r_lo);
+    // FP32 offset from the cell's lower corner (broad phase of FP32-split)
+    S.offh[t] = make_float4((float)(x.x - (g.lc_origin[0] + ci * g.edge[0])),
+                            (float)(x.y - (g.lc_origin[1] + cj * g.edge[1])),
+                            (float)(x.z - (g.lc_origin[2] + ck * g.edge[2])), tp.r_f);
   }
 }
 

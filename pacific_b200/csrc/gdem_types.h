@@ -38,7 +38,7 @@ struct GridDesc {
   int wall_begin, wall_count;
   int model_base;        // first entry of this instance in the model table
   int pad0;
-  float edge_hi[3], edge_lo[3];   // edge as a float-float pair
+  float edge_f[3];       // edge in FP32 (FP32-split broad phase)
 };
 
 // Particle class (a <Particle> node of the XML input).
@@ -51,7 +51,8 @@ struct TypeDesc {
   double weight[3];      // m (1 - rho_f / rho) g
   int mat;               // material index
   int shape;             // 0 sphere, 1 box, 2 polyhedron
-  float r_hi, r_lo;      // radius as a float-float pair
+  float r_f;             // radius in FP32 (FP32-split broad phase)
+  int pad_r;
   double extent[3];      // box half lengths / bounding-box half extent
   double scaling[3];     // crust shrink factors (extent - crust) / extent
   int poly_begin;        // first vertex of a polyhedron in the vertex table
@@ -62,7 +63,8 @@ struct TypeDesc {
 struct ModelDesc {
   double kn, en, etat, muc, kt, mur, etarpf, epst;
   double beta;           // ln(en) / sqrt(pi^2 + ln^2(en))
-  int rolling;           // mur != 0
+  double kr;             // Hooke rolling-resistance coefficient
+  int rolling;           // HookeMemory: mur != 0; Hooke: kr != 0
   int memory;            // 1 HookeMemory, 0 Hooke (no tangential history)
   int valid;
   int pad;

@@ -84,7 +84,8 @@ def library() -> ctypes.CDLL:
         "gdem_upload_basis": ([_P, _DP], ctypes.c_int),
         "gdem_download_basis": ([_P, _DP], ctypes.c_int),
         "gdem_set_diagnostics": ([_P, ctypes.c_int], ctypes.c_int),
-        "gdem_download_contacts": ([_P, i64, ctypes.POINTER(i64), _IP, _IP, _DP], ctypes.c_int),
+        "gdem_download_contacts": ([_P, i64, ctypes.POINTER(i64), _IP, _IP, _DP, _DP],
+                                   ctypes.c_int),
         "gdem_status": ([_P, _IP, ctypes.c_int], ctypes.c_int),
         "gdem_grid": ([_P, ctypes.c_int, _IP, _DP, _DP], ctypes.c_int),
         "gdem_num_particles": ([_P], i64),
@@ -257,17 +258,21 @@ class Grains:
     def set_diagnostics(self, on=True):
         self._check(library().gdem_set_diagnostics(self._h, 1 if on else 0))
 
-    def download_contacts(self):
+    def download_contacts(self, forces=False):
+        """(id0, id1, overlap) of the last force evaluation's contacts, plus
+        the force on id0 (m, 3) when forces=True."""
         lib = library()
         cnt = ctypes.c_int64(0)
-        self._check(lib.gdem_download_contacts(self._h, 0, ctypes.byref(cnt), None, None, None))
+        self._check(lib.gdem_download_contacts(self._h, 0, ctypes.byref(cnt), None, None, None,
+                                               None))
         m = cnt.value
         id0 = np.empty(m, np.int32)
         id1 = np.empty(m, np.int32)
         dl = np.empty(m)
+        f = np.empty((m, 3)) if forces else None
         self._check(lib.gdem_download_contacts(self._h, m, ctypes.byref(cnt), _ip(id0), _ip(id1),
-                                               _dp(dl)))
-        return id0, id1, dl
+                                               _dp(dl), _dp(f)))
+        return (id0, id1, dl, f) if forces else (id0, id1, dl)
 
     def grid(self, k=0):
         nb = np.empty(3, np.int32)

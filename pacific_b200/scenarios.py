@@ -108,15 +108,21 @@ class Scenario:
             L += ["      </Composite>", "    </Obstacles>"]
         L.append("    <ContactForceModels>")
         for m in self.models:
+            law = m.get("law", "HookeMemory")
             L += ["      <ContactForceModel>",
                   f'        <Material materialA="{m["matA"]}" materialB="{m["matB"]}"/>',
-                  "        <HookeMemory>",
+                  f"        <{law}>",
                   f'          <kn>{_f(m["kn"])}</kn>',
                   f'          <en>{_f(m["en"])}</en>']
             if m.get("etat") is not None:
                 L.append(f'          <etat>{_f(m["etat"])}</etat>')
-            L += [f'          <muc>{_f(m["muc"])}</muc>',
-                  f'          <kt>{_f(m["kt"])}</kt>']
+            L.append(f'          <muc>{_f(m["muc"])}</muc>')
+            if law == "Hooke":
+                # HookeContactForceModel::defineParameters requires <kr>
+                L += [f'          <kr>{_f(m.get("kr", 0.0))}</kr>', "        </Hooke>",
+                      "      </ContactForceModel>"]
+                continue
+            L.append(f'          <kt>{_f(m["kt"])}</kt>')
             if m.get("mur"):
                 L.append(f'          <mur>{_f(m["mur"])}</mur>')
             if m.get("epst") is not None:
@@ -153,7 +159,7 @@ def _box_walls(L, thickness, crust, material):
 
 def settling_box(n=1000, seed=1235, box=(0.03, 0.03, 0.06), radius=1.0e-3, spacing=2.4e-3,
                  jitter=1.0e-4, vmax=0.05, kn=1.0e4, en=0.7, etat=0.0, muc=0.5,
-                 dt=1.0e-5, density=2500.0) -> Scenario:
+                 dt=1.0e-5, density=2500.0, law="HookeMemory", kr=0.0) -> Scenario:
     rng = np.random.default_rng(seed)
     nx, ny, nz = (int(np.floor(b / spacing)) for b in box)
     if n > nx * ny * nz:
@@ -168,8 +174,10 @@ def settling_box(n=1000, seed=1235, box=(0.03, 0.03, 0.06), radius=1.0e-3, spaci
     types = [dict(radius=radius, crust=crust, density=density, material="matP")]
     walls = _box_walls(box, 2.0e-3, crust, "matW")
     kt = 2.0 / 7.0 * kn
-    models = [dict(matA="matP", matB="matP", kn=kn, en=en, etat=etat, muc=muc, kt=kt),
-              dict(matA="matP", matB="matW", kn=kn, en=en, etat=etat, muc=muc, kt=kt)]
+    models = [dict(matA="matP", matB="matP", kn=kn, en=en, etat=etat, muc=muc, kt=kt, law=law,
+                   kr=kr),
+              dict(matA="matP", matB="matW", kn=kn, en=en, etat=etat, muc=muc, kt=kt, law=law,
+                   kr=kr)]
     return Scenario("settling_box", (0.0, 0.0, 0.0), tuple(box), (0, 0, 0), (0.0, 0.0, -9.81), dt,
                     types, walls, models, np.zeros(n, np.int32), x, v, w, q)
 

@@ -52,6 +52,10 @@ SCENARIOS = {
     "settling_box": (lambda: scenarios.settling_box(n=500, seed=11), [0, 1, 800, 801, 1600, 1601]),
     "periodic_gas": (lambda: scenarios.periodic_gas(n_fcc=5, seed=12), [0, 1, 20, 21]),
     "convex_pour": (_convex, [0, 1, 3000, 3001, 6000, 6001]),
+    # Hooke law (no tangential memory) with a rolling-resistance moment
+    "settling_hooke": (lambda: scenarios.settling_box(n=500, seed=17, etat=None, law="Hooke",
+                                                      kr=0.05, vmax=0.2),
+                       [0, 1, 800, 801, 1600, 1601]),
 }
 
 

@@ -16,6 +16,23 @@ def contact_set(id0, id1):
     return set(zip(first.tolist(), second.tolist()))
 
 
+def contact_forces(id0, id1, f):
+    """{(lower ID, higher ID) or (particle, wall): force on the first body}."""
+    out = {}
+    for a, b, v in zip(id0.tolist(), id1.tolist(), np.asarray(f)):
+        if b >= 0 and a > b:
+            out[(b, a)] = -v
+        else:
+            out[(a, b)] = v
+    return out
+
+
+def per_contact_errors(ref, got):
+    """|f_got - f_ref| / |f_ref| per contact present in both dicts."""
+    return np.array([np.linalg.norm(got[k] - ref[k]) / np.linalg.norm(ref[k])
+                     for k in ref if k in got and np.linalg.norm(ref[k]) > 0])
+
+
 def contact_scale(n, id0, id1, f):
     """Sum over each particle's contacts of |f_ic| (the per-particle error
     normaliser: |dF_i| / sum_c |f_ic|)."""

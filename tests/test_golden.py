@@ -21,6 +21,7 @@ import pytest
 from oracle.oracle import Oracle
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
+CONVEX = {"convex_pour"}
 
 
 def _load(name, tmp_path):
@@ -39,7 +40,7 @@ def _hist_dict(own, par, kd, pn):
     return {(int(a), int(b)): (tuple(k), tuple(p)) for a, b, k, p in zip(own, par, kd, pn)}
 
 
-@pytest.mark.parametrize("name", ["settling_box", "convex_pour"])
+@pytest.mark.parametrize("name", ["settling_box", "convex_pour", "settling_hooke"])
 def test_restatement_bitexact_vs_reference(tmp_path, oracle_lib, name):
     g, xml = _load(name, tmp_path)
     o = Oracle(xml)
@@ -87,8 +88,7 @@ def _gpu_step_from_golden(g, xml, k, k1, precision, tol):
     from tests.helpers import contact_set
     G = Grains(xml, precision)
     G.upload_state(g["type"], g[f"s{k}_x"], g[f"s{k}_v"], g[f"s{k}_w"], g[f"s{k}_q"])
-    if f"s{k}_basis" in g:
-        G.upload_basis(g[f"s{k}_basis"])
+    G.upload_basis(g[f"s{k}_basis"])
     G.upload_forces(g[f"s{k}_F"], g[f"s{k}_T"])
     own, par = g[f"s{k}_hist_owner"], g[f"s{k}_hist_partner"]
     G.upload_history(own, par, g[f"s{k}_hist_kdelta"], g[f"s{k}_hist_prevn"])
@@ -110,7 +110,8 @@ def _gpu_step_from_golden(g, xml, k, k1, precision, tol):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["settling_box", "periodic_gas", "convex_pour"])
+@pytest.mark.parametrize("name", ["settling_box", "periodic_gas", "convex_pour",
+                                  "settling_hooke"])
 def test_gpu_fp64_step_matches_reference(tmp_path, lib, name):
     from pacific_b200 import FP64
     g, xml = _load(name, tmp_path)
@@ -120,13 +121,15 @@ def test_gpu_fp64_step_matches_reference(tmp_path, lib, name):
         assert np.array_equal(cells, g[f"s{k1}_cells"])
         assert gc == rc
         assert np.max(np.abs(s["x"] - g[f"s{k1}_x"])) <= 1e-15
-        if f"s{k1}_basis" in g:
+        if name in CONVEX:
+            # orientation matrices are state for non-spherical classes only
             assert np.max(np.abs(s["basis"] - g[f"s{k1}_basis"])) <= 1e-14
         assert fe.max(initial=0) <= 1e-10 and te.max(initial=0) <= 1e-10
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["settling_box", "periodic_gas", "convex_pour"])
+@pytest.mark.parametrize("name", ["settling_box", "periodic_gas", "convex_pour",
+                                  "settling_hooke"])
 def test_gpu_fp32split_step_matches_reference(tmp_path, lib, name):
     from pacific_b200 import FP32_SPLIT
     g, xml = _load(name, tmp_path)
