@@ -214,8 +214,8 @@ def error_sample(n_fcc, steps_before, precision):
     """Per-particle force error of one GPU step against the FP64 oracle from
     the same state (normaliser: the particle's sum of contact-force magnitudes)."""
     from pacific_b200 import scenarios
-    from tests.helpers import (contact_scale, force_errors, gpu_from_oracle, oracle_for,
-                               radii_of)
+    from tests.helpers import (contact_forces, contact_scale, force_errors, gpu_from_oracle,
+                               oracle_for, per_contact_errors, radii_of)
     sc = scenarios.periodic_gas(n_fcc=n_fcc, seed=1236)
     with tempfile.TemporaryDirectory() as d:
         xml = str(sc.write_xml(Path(d) / "err.xml"))
@@ -223,15 +223,25 @@ def error_sample(n_fcc, steps_before, precision):
         o.init()
         o.step(steps_before)
         g = gpu_from_oracle(xml, sc, o, precision)
+        g.set_diagnostics(True)
         o.step(1)
         g.step(1)
         id0, id1, dl, pt, f = o.contacts()
         scale = contact_scale(sc.n, id0, id1, f)
         fe, te = force_errors(o.state(), g.download_state(), scale, radii_of(sc))
+        g0, g1, _, gf = g.download_contacts(forces=True)
+        pe = per_contact_errors(contact_forces(id0, id1, f), contact_forces(g0, g1, gf))
+        nlaw, nre = g.law_counts()
         m = scale > 0
         g.close()
-    return {"force_max": float(fe[m].max()), "force_p99": float(np.percentile(fe[m], 99)),
-            "torque_max": float(te[m].max()), "particles_in_contact": int(m.sum())}
+    out = {"force_max": float(fe[m].max()), "force_p99": float(np.percentile(fe[m], 99)),
+           "torque_max": float(te[m].max()), "per_contact_max": float(pe.max(initial=0.0)),
+           "particles_in_contact": int(m.sum()), "contacts": int(len(id0))}
+    from pacific_b200 import FP32_SPLIT
+    if precision == FP32_SPLIT:
+        out["fp64_reevaluated"] = int(nre)
+        out["law_evaluations"] = int(nlaw)
+    return out
 
 
 def _quiet(f, *a):

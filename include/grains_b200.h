@@ -99,6 +99,11 @@ int gdem_download_basis(gdem_handle h, double* basis);
  * 1781-1811), the quantity Grains3D writes to *_VelocityMaxMean.dat. */
 int gdem_velocity_stats(gdem_handle h, double* vmax, double* vmean);
 
+/* FP32-split mode: contact-law evaluations since the last reset, and how
+ * many of them were re-evaluated in FP64 because the FP32 force was
+ * ill-conditioned (a small difference of large terms).  Zero in FP64 mode. */
+int gdem_law_counts(gdem_handle h, int64_t* evaluated, int64_t* reevaluated, int reset);
+
 /* Per-kernel device timing with CUDA events (replaces the SCT_* phase timers,
  * Base/include/solvercomputingtime.hh:46-75).  While on, gdem_step uses plain
  * launches instead of graph replay.  gdem_kernel_times returns, per timed

@@ -88,7 +88,8 @@ __device__ __forceinline__ RelVel splitRelVel(d3 nD, d3 tmpV) {
 __device__ __forceinline__ void hodc32(ModelDesc const& m, float kn, float beta, float dt,
                                        float3 pen, RelVel const& rv, float3 wrel, float m0, float rad0,
                                        float m1, float rad1, bool existed, float3& kd,
-                                       float3& pn, float3& sp, float3& f, float3& mr) {
+                                       float3& pn, float3& sp, float3& f, float3& mr,
+                                       float& cond) {
   const float3 normal = rv.normal;
   const float3 v_n = rv.vn;
   const float3 v_t = rv.vt;
@@ -142,13 +143,12 @@ __device__ __forceinline__ void hodc32(ModelDesc const& m, float kn, float beta,
     mr = sp - ((float)m.etarpf * etar) * wrel;
   }
   f = delFN + delFT;
+  // size of the terms against the result: FP32 rounding of the terms is
+  // amplified by this factor in f
+  cond = (kn * normf3(pen) + fabsf(gamman) * normf3(v_n) + normf3(kd) + normf3(viscousFT)) /
+         normf3(f);
 }
 
-// v + w x lever in FP64 from the master state (sorted order) and a float lever.
-__device__ __forceinline__ d3 pointVel(DevState const& S, int s, float3 lev) {
-  const d3 v = ld3(S.v, S.cap, s), w = ld3(S.w, S.cap, s);
-  return v + cross(w, mk((double)lev.x, (double)lev.y, (double)lev.z));
-}
 __device__ __forceinline__ float3 tof(d3 a) { return f3((float)a.x, (float)a.y, (float)a.z); }
 
 __device__ __forceinline__ void loadHistF(HistTable const& t, int slot, float3& kd, float3& pn, float3& sp) {
@@ -167,7 +167,7 @@ __device__ __forceinline__ void storeHistF(HistTable const& t, int slot, float3 
 __device__ __forceinline__ void hooke32(ModelDesc const& m, float kn, float beta, float3 pen,
                                         RelVel const& rv, float3 w0, float3 w1, float3 lev0,
                                         float3 lev1, float m0, float rad0, float m1, float rad1,
-                                        float3& f, float3& mr) {
+                                        float3& f, float3& mr, float& cond) {
   const float3 v_n = rv.vn;
   const float3 v_t = rv.vt;
   float avmass = 1.f / (1.f / m0 + 1.f / m1);
@@ -194,6 +194,68 @@ __device__ __forceinline__ void hooke32(ModelDesc const& m, float kn, float beta
     }
   }
   f = delFN + delFT;
+  cond = (kn * normf3(pen) + fabsf(gamman) * normf3(v_n) + fabsf(gammat) * normf3(v_t)) /
+         normf3(f);
+}
+
+// A contact whose FP32 force carries more than this amplification of FP32
+// rounding (about 6e-8 times it, relative to |f|) is re-evaluated in FP64:
+// the result then stays within ~1e-6 of the FP64 force per contact.
+constexpr float kReevalCond = 16.f;
+
+struct Body64 { d3 x, v, w; double m, rad; };
+__device__ __forceinline__ float3 tof3(d3 a) { return make_float3((float)a.x, (float)a.y, (float)a.z); }
+__device__ __forceinline__ d3 tod3(float3 a) { return mk((double)a.x, (double)a.y, (double)a.z); }
+
+// FP64 evaluation of one contact from the loaded FP32 history (kd0, pn0,
+// sp0).
+__device__ __forceinline__ void contactLaw64(ModelDesc const& m, double dt, Contact64 const& ct,
+                                          Body64 const& b0, Body64 const& b1, bool existed,
+                                          float3 kd0, float3 pn0, float3 sp0, float3& kd,
+                                          float3& pn, float3& sp, float3& f, float3& mr) {
+  d3 f64, mr64;
+  if (m.memory) {
+    d3 kdd = tod3(kd0), pnd = tod3(pn0), spd = tod3(sp0);
+    hodc64(m, dt, ct.point, ct.overlap, b0.x, b0.v, b0.w, b0.m, b0.rad, b1.x, b1.v, b1.w, b1.m,
+           b1.rad, existed, kdd, pnd, spd, f64, mr64);
+    kd = tof3(kdd); pn = tof3(pnd); sp = tof3(spd);
+  } else {
+    hooke64(m, ct.point, ct.overlap, b0.x, b0.v, b0.w, b0.m, b0.rad, b1.x, b1.v, b1.w, b1.m,
+            b1.rad, f64, mr64);
+  }
+  f = tof3(f64);
+  mr = tof3(mr64);
+}
+
+// One contact's force law seen from b0 (force on b0 returned in f, rolling
+// moment in mr), evaluated in FP32 from FP64 geometry and velocities, and
+// again in FP64 from the same inputs when the FP32 result is ill-conditioned
+// (a force that is a small difference of large terms: a contact that is
+// about to open, a rebound).  kd/pn/sp hold the loaded history on entry and
+// the updated history on exit.
+__device__ __forceinline__ void contactLaw32(ModelDesc const& m, double dt, Contact64 const& ct,
+                                             Body64 const& b0, Body64 const& b1, bool existed,
+                                             float3& kd, float3& pn, float3& sp, float3& f,
+                                             float3& mr, int& reeval) {
+  const d3 lev0 = ct.point - b0.x, lev1 = ct.point - b1.x;
+  const d3 nD = ct.overlap / norm(ct.overlap);
+  // relative velocity at the contact point (Particle::getVelocityAtPoint)
+  const d3 tmpV = (b0.v + cross(b0.w, lev0)) - (b1.v + cross(b1.w, lev1));
+  const RelVel rv = splitRelVel(nD, tmpV);
+  const float3 pen = tof3(ct.overlap);
+  const float3 kd0 = kd, pn0 = pn, sp0 = sp;
+  float cond;
+  if (m.memory)
+    hodc32(m, (float)m.kn, (float)m.beta, (float)dt, pen, rv, tof3(b0.w - b1.w), (float)b0.m,
+           (float)b0.rad, (float)b1.m, (float)b1.rad, existed, kd, pn, sp, f, mr, cond);
+  else
+    hooke32(m, (float)m.kn, (float)m.beta, pen, rv, tof3(b0.w), tof3(b1.w), tof3(lev0),
+            tof3(lev1), (float)b0.m, (float)b0.rad, (float)b1.m, (float)b1.rad, f, mr, cond);
+  reeval = 0;
+  if (!(cond <= kReevalCond)) {
+    contactLaw64(m, dt, ct, b0, b1, existed, kd0, pn0, sp0, kd, pn, sp, f, mr);
+    reeval = 1;
+  }
 }
 
 __global__ void __launch_bounds__(256) k_pairs32(DevState S) {
@@ -229,7 +291,7 @@ __global__ void __launch_bounds__(256) k_pairs32(DevState S) {
 // kConvex: some class is not a sphere, so the GJK narrow phase is compiled in
 // (it is kept out of the sphere-only kernel, whose registers it would triple).
 template <bool kConvex>
-__global__ void __launch_bounds__(256) k_forces32(DevState S) {
+__global__ void __launch_bounds__(256, 2) k_forces32(DevState S) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
   const int cap = S.cap;
@@ -239,7 +301,7 @@ __global__ void __launch_bounds__(256) k_forces32(DevState S) {
   TypeDesc const& ta = S.types[S.type[t]];
   const d3 xt = ld3(S.x, cap, t);
   float3 Fs = f3(0.f, 0.f, 0.f), Ts = f3(0.f, 0.f, 0.f);
-  const float dt = (float)S.dt;
+  int nlaw = 0, nre = 0;   // contacts evaluated / re-evaluated in FP64
   const int np = S.npairs[t];
   const int* seg = S.pairs + (size_t)t * kPairCap;
   for (int e = 0; e < np; ++e) {
@@ -273,33 +335,30 @@ __global__ void __launch_bounds__(256) k_forces32(DevState S) {
     if (S.diag) S.pair_delta[(size_t)t * kPairCap + e] = ct.contact && ct.dist < 0. ? ct.dist : __longlong_as_double(0x7ff0000000000000ll);
     if (!ct.contact || !(ct.dist < 0.)) continue;
     if (ct.error) raise(S.status, kErrContactOverlap);
-    // the force law from here on is FP32
+    // the force law from here on is FP32 (FP64 when ill-conditioned)
     const float3 lev0 = tof(ct.point - x0);
     const float3 lev1 = tof(ct.point - x1);
-    const float3 pen = tof(ct.overlap);
-    const d3 nD = ct.overlap / norm(ct.overlap);
     ModelDesc const& m = S.models[g.model_base + tp0.mat * kMaxMat + tp1.mat];
-    const RelVel relv = splitRelVel(nD, pointVel(S, s0, lev0) - pointVel(S, s1, lev1));
-    float3 f, mr;
+    const Body64 b0{x0, ld3(S.v, cap, s0), ld3(S.w, cap, s0), tp0.mass, tp0.eqrad};
+    const Body64 b1{x1, ld3(S.v, cap, s1), ld3(S.w, cap, s1), tp1.mass, tp1.eqrad};
+    float3 f, mr, kd = f3(0.f, 0.f, 0.f), pn = kd, sp = kd;
+    int re;
+    ++nlaw;
     if (m.memory) {
-      const float3 wrel = m.rolling ? tof(ld3(S.w, cap, s0) - ld3(S.w, cap, s1)) : f3(0.f, 0.f, 0.f);
       const int id0 = t0 ? ida : idb, id1 = t0 ? idb : ida;
       const unsigned long long key = pairKey(id0, id1);
       int old = histFind(S.hist_old, key);
-      float3 kd, pn, sp;
       if (old >= 0) loadHistF(S.hist_old, old, kd, pn, sp);
-      hodc32(m, (float)m.kn, (float)m.beta, dt, pen, relv, wrel, (float)tp0.mass,
-             (float)tp0.eqrad, (float)tp1.mass, (float)tp1.eqrad, old >= 0, kd, pn, sp, f, mr);
+      contactLaw32(m, S.dt, ct, b0, b1, old >= 0, kd, pn, sp, f, mr, re);
       if (t0) {
         int slot = histInsert(S.hist_new, key);
         if (slot < 0) raise(S.status, kErrHashFull);
         else storeHistF(S.hist_new, slot, kd, pn, sp);
       }
     } else {
-      hooke32(m, (float)m.kn, (float)m.beta, pen, relv, tof(ld3(S.w, cap, s0)),
-              tof(ld3(S.w, cap, s1)), lev0, lev1, (float)tp0.mass, (float)tp0.eqrad,
-              (float)tp1.mass, (float)tp1.eqrad, f, mr);
+      contactLaw32(m, S.dt, ct, b0, b1, false, kd, pn, sp, f, mr, re);
     }
+    nre += re;
     if (S.diag) {
       double* fd = S.pair_force + 3 * ((size_t)t * kPairCap + e);
       fd[0] = f.x; fd[1] = f.y; fd[2] = f.z;
@@ -327,27 +386,25 @@ __global__ void __launch_bounds__(256) k_forces32(DevState S) {
     if (ct.error) raise(S.status, kErrContactOverlap);
     if (!ct.contact || !(ct.dist < 0.)) continue;
     ModelDesc const& m = S.models[g.model_base + ta.mat * kMaxMat + wd.mat];
-    float3 f, mr;
-    d3 l0 = ct.point - xt;
-    float3 lev0 = f3((float)l0.x, (float)l0.y, (float)l0.z);
-    float3 pen = f3((float)ct.overlap.x, (float)ct.overlap.y, (float)ct.overlap.z);
-    const RelVel relv = splitRelVel(ct.overlap / norm(ct.overlap), pointVel(S, t, lev0));
-    const float3 wrel = tof(ld3(S.w, cap, t));
+    const float3 lev0 = tof(ct.point - xt);
+    const d3 zero = mk(0., 0., 0.);
+    const Body64 b0{xt, ld3(S.v, cap, t), ld3(S.w, cap, t), ta.mass, ta.eqrad};
+    const Body64 b1{mk(wd.centre[0], wd.centre[1], wd.centre[2]), zero, zero, 1.e20, wd.eqrad};
+    float3 f, mr, kd = f3(0.f, 0.f, 0.f), pn = kd, sp = kd;
+    int re;
+    ++nlaw;
     if (m.memory) {
       const unsigned long long key = wallKey(ida, k);
       int old = histFind(S.hist_old, key);
-      float3 kd, pn, sp;
       if (old >= 0) loadHistF(S.hist_old, old, kd, pn, sp);
-      hodc32(m, (float)m.kn, (float)m.beta, dt, pen, relv, wrel, (float)ta.mass,
-             (float)ta.eqrad, 1.e20f, (float)wd.eqrad, old >= 0, kd, pn, sp, f, mr);
+      contactLaw32(m, S.dt, ct, b0, b1, old >= 0, kd, pn, sp, f, mr, re);
       int slot = histInsert(S.hist_new, key);
       if (slot < 0) raise(S.status, kErrHashFull);
       else storeHistF(S.hist_new, slot, kd, pn, sp);
     } else {
-      d3 l1 = ct.point - mk(wd.centre[0], wd.centre[1], wd.centre[2]);
-      hooke32(m, (float)m.kn, (float)m.beta, pen, relv, wrel, f3(0.f, 0.f, 0.f), lev0, tof(l1),
-              (float)ta.mass, (float)ta.eqrad, 1.e20f, (float)wd.eqrad, f, mr);
+      contactLaw32(m, S.dt, ct, b0, b1, false, kd, pn, sp, f, mr, re);
     }
+    nre += re;
     if (S.diag) {
       double* fd = S.wall_force + 3 * ((size_t)t * S.max_walls + k);
       fd[0] = f.x; fd[1] = f.y; fd[2] = f.z;
@@ -360,6 +417,13 @@ __global__ void __launch_bounds__(256) k_forces32(DevState S) {
   S.F[cap + t] = ta.weight[1] + (double)Fs.y;
   S.F[2 * cap + t] = ta.weight[2] + (double)Fs.z;
   S.T[t] = (double)Ts.x; S.T[cap + t] = (double)Ts.y; S.T[2 * cap + t] = (double)Ts.z;
+  // warp-aggregated counters of the FP64 re-evaluations
+  const unsigned mask = __activemask();
+  const int wl = __reduce_add_sync(mask, nlaw), wr = __reduce_add_sync(mask, nre);
+  if ((threadIdx.x & 31) == __ffs(mask) - 1 && wl) {
+    atomicAdd(S.law_counts, (unsigned long long)wl);
+    if (wr) atomicAdd(S.law_counts + 1, (unsigned long long)wr);
+  }
 }
 
 }  // namespace

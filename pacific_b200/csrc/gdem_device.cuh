@@ -93,6 +93,7 @@ struct DevState {
   double* pair_delta;     // diagnostics: overlap of each entry (+inf: no contact)
   double* wall_delta;     // diagnostics: overlap with each wall slot
   double* pair_force;     // diagnostics: contact force on the lower ID (3 per entry)
+  unsigned long long* law_counts;   // FP32-split: contacts evaluated, re-evaluated in FP64
   double* wall_force;     // diagnostics: wall contact force on the particle (3 per slot)
   int diag;
   HistTable hist_old, hist_new;

@@ -584,6 +584,8 @@ struct System {
     }
     S.status = alloc<int>(1);
     CK(cudaMemset(S.status, 0, sizeof(int)));
+    S.law_counts = alloc<unsigned long long>(2);
+    CK(cudaMemset(S.law_counts, 0, 2 * sizeof(unsigned long long)));
     CK(cudaMemset(S.cell_count, 0, (size_t)S.ncells * sizeof(int)));
     CK(cudaMemset(S.F, 0, 3 * c * sizeof(double)));
     CK(cudaMemset(S.T, 0, 3 * c * sizeof(double)));
@@ -852,6 +854,20 @@ int gdem_pair_counts(gdem_handle h, int64_t* entries, int64_t* contacts) {
     CK(cudaStreamSynchronize(s->stream));
     if (entries) *entries = (int64_t)r[0];
     if (contacts) *contacts = (int64_t)r[1];
+    return GDEM_OK;
+  });
+}
+
+int gdem_law_counts(gdem_handle h, int64_t* evaluated, int64_t* reevaluated, int reset) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state) throw std::runtime_error("no state");
+    unsigned long long r[2];
+    CK(cudaStreamSynchronize(s->stream));
+    CK(cudaMemcpy(r, s->S.law_counts, sizeof(r), cudaMemcpyDeviceToHost));
+    if (reset) CK(cudaMemset(s->S.law_counts, 0, sizeof(r)));
+    if (evaluated) *evaluated = (int64_t)r[0];
+    if (reevaluated) *reevaluated = (int64_t)r[1];
     return GDEM_OK;
   });
 }

@@ -94,6 +94,8 @@ def library() -> ctypes.CDLL:
         "gdem_set_state": ([_P, _DP, _DP, _DP, _DP, _DP, _DP, _DP], ctypes.c_int),
         "gdem_velocity_stats": ([_P, _DP, _DP], ctypes.c_int),
         "gdem_set_profiling": ([_P, ctypes.c_int], ctypes.c_int),
+        "gdem_law_counts": ([_P, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.c_int],
+                            ctypes.c_int),
         "gdem_pair_counts": ([_P, ctypes.POINTER(i64), ctypes.POINTER(i64)], ctypes.c_int),
         "gdem_kernel_times": ([_P, ctypes.c_int, _IP, ctypes.c_char_p, _DP,
                                ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
@@ -221,6 +223,14 @@ class Grains:
         a = ctypes.c_int64(0)
         b = ctypes.c_int64(0)
         self._check(library().gdem_pair_counts(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def law_counts(self, reset=False):
+        """(contact-law evaluations, FP64 re-evaluations) of FP32-split mode."""
+        a = ctypes.c_int64(0)
+        b = ctypes.c_int64(0)
+        self._check(library().gdem_law_counts(self._h, ctypes.byref(a), ctypes.byref(b),
+                                              1 if reset else 0))
         return a.value, b.value
 
     def set_profiling(self, on=True):
