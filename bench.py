@@ -98,26 +98,32 @@ class ClockSampler:
 
 # --------------------------------------------------------------- roofline --
 def algorithmic_bytes(kernel, n, entries, contacts, ncells, fp64):
-    """Compulsory DRAM bytes of one launch of each phase (each input read
-    once, each output written once; neighbour re-reads assumed cache hits)."""
-    if kernel == "move":       # F T v w wbf x q + type inst | x v w wbf q + key rank + count
-        return n * (176 + 8 + 128 + 8 + 4)
-    if kernel == "gather":     # order id type inst key + state | state + ids + cell + compact
-        return n * (148 + 16 + 128 + 16 + (96 if fp64 else 64))
-    if kernel in ("pairs64", "pairs32"):
-        return n * ((32 if fp64 else 16) + 4 + 16 + 4) + 4 * entries + 8 * ncells
+    """Compulsory DRAM bytes of one launch of each phase of a spheres-only
+    step: each input read once, each output written once, neighbour re-reads
+    counted as cache hits.  Per particle unless noted."""
+    if kernel == "key":          # F v x type inst | skey rank; cell-count RMW
+        return n * (24 * 3 + 8 + 8 + 8)
+    if kernel == "scan":         # counts | starts (per cell)
+        return ncells * 8
+    if kernel == "place":        # skey rank start[skey] | order
+        return n * 16
+    if kernel == "cellsort":     # starts, count reset (per cell); order, id of shared cells
+        return ncells * 8 + n * 8
+    if kernel == "move_gather":  # order id type inst skey x v wbf q F T | same + w key cellc
+        #                          + pos/vel/omg (FP64) or offsets (FP32-split)
+        return n * (172 + 160 + (96 if fp64 else 16))
+    if kernel in ("pairs64", "pairs32"):   # cellc + own position | npairs; entries; starts
+        return n * (16 + (32 if fp64 else 16) + 4) + 4 * entries + 4 * ncells
     if kernel in ("forces64", "forces32"):
-        per_p = (96 if fp64 else 64) + 8 + 16 + 4 + 48 + (0 if fp64 else 24)
+        # cellc id type npairs + own position (FP64 packed or SoA x) | F T;
+        # per entry the entry word; per contact the history key + values, read and written
+        per_p = 16 + 4 + 4 + 4 + (96 if fp64 else 24) + 48
         per_c = 2 * (8 + (72 if fp64 else 36))
         return n * per_p + 4 * entries + contacts * per_c
-    if kernel == "kick":
-        return n * (128 + 4 + 72)
-    if kernel == "place":
-        return n * 16
-    if kernel == "scan":
-        return ncells * 8
-    if kernel == "cellsort":
-        return ncells * 8 + n * 8
+    if kernel == "kick":         # F T v wbf q type | v wbf w
+        return n * (48 + 48 + 32 + 4 + 72)
+    if kernel == "hist_clear":   # the new table's keys are reset
+        return None
     return None
 
 
