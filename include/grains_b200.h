@@ -167,6 +167,18 @@ int gdem_use_graphs(gdem_handle h, int on);
 const char* gdem_last_error(void);
 void gdem_destroy(gdem_handle h);
 
+/* No counterpart in the reference.  Maximum and mean |v| (as
+ * gdem_velocity_stats, AllComponents::ComputeMaxMeanVelocity) of n particle
+ * velocities v (device memory, 3 doubles per particle), written to out
+ * (device memory, 2 doubles: max, mean) in stream order on stream (a
+ * cudaStream_t; NULL for the default stream).  Needs no handle and allocates
+ * nothing: the reduction's scratch is a fixed device array of the library,
+ * so n is limited to 1,048,576 (larger n returns GDEM_ERR_INVALID).  Calls
+ * that overlap in time on one device race on that scratch.  The first call on
+ * a device sets up the scratch address and should come before any stream
+ * capture. */
+int gdem_speed_stats_static(const double* v, int64_t n, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

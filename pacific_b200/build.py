@@ -27,6 +27,7 @@ UNITS = [
     ("gdem_contact64.cu", ["-fmad=false"]),
     ("gdem_contact32.cu", ["-fmad=true"]),
     ("gdem_host.cu", ["-fmad=false"]),
+    ("gdem_noalloc.cu", ["-fmad=false"]),
     ("xml_reader.cpp", []),
 ]
 

@@ -726,6 +726,9 @@ int guarded(F&& f) {
 }
 
 }  // namespace
+
+void setLastError(std::string const& msg) { g_last_error = msg; }
+
 }  // namespace gdem
 
 using namespace gdem;
