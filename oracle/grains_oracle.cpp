@@ -143,9 +143,9 @@ struct Model {
 
 // Convex shape of a particle class or a wall.
 struct Shape {
-  int kind = 0;                      // 0 sphere, 1 box, 2 polyhedron
+  int kind = 0;                      // 0 sphere, 1 box, 2 polyhedron, 3 cylinder
   double radius = 0.;                // circumscribed radius
-  V3 extent;                         // box half lengths
+  V3 extent;                         // box half lengths; cylinder (radius, half height, radius)
   std::vector<V3> verts;             // polyhedron vertices (local frame)
   std::vector<std::vector<int>> cob; // vertex neighbours (Polyhedron::BuildPolyhedron)
   V3 scaling;                        // crust shrink factors (RigidBodyWithCrust ctor)
@@ -581,6 +581,17 @@ V3 support(Shape const& s, int* curv, V3 const& v) {
     double n = norm(v);
     if (n > EPSILON) { double r = s.radius / n; return V3(v[0] * r, v[1] * r, v[2] * r); }
     return V3();
+  }
+  if (s.kind == 3) {   // Cylinder::support (Cylinder.cpp:112-133), axis along local Y
+    if (!(norm(v) > EPSILON)) return V3();
+    double r = s.extent[0], hh = s.extent[1];
+    double sxz = std::sqrt(v[0] * v[0] + v[2] * v[2]);
+    if (sxz > EPSILON) {
+      double d = r / sxz;
+      if (std::fabs(v[1]) < EPSILON) return V3(v[0] * d, 0., v[2] * d);
+      return V3(v[0] * d, v[1] < 0. ? -hh : hh, v[2] * d);
+    }
+    return V3(0., v[1] < 0. ? -hh : hh, 0.);
   }
   if (s.kind == 1) {
     if (norm(v) < EPSILON) return V3();
@@ -1105,6 +1116,16 @@ Shape makeShape(or_config const* c, int t) {
     sh.inertia[0] = 8.0 * e[0] * e[1] * e[2] * (e[1] * e[1] + e[2] * e[2]) / 3.0;
     sh.inertia[3] = 8.0 * e[0] * e[1] * e[2] * (e[0] * e[0] + e[2] * e[2]) / 3.0;
     sh.inertia[5] = 8.0 * e[0] * e[1] * e[2] * (e[0] * e[0] + e[1] * e[1]) / 3.0;
+  } else if (sh.kind == 3) {
+    // Cylinder (Geometry/src/Cylinder.cpp): radius r, half height hh; the
+    // class extent holds (r, hh, r)
+    double r = c->type_extent[3 * t], hh = c->type_extent[3 * t + 1];
+    sh.extent = V3(r, hh, r);
+    sh.radius = std::sqrt(r * r + hh * hh);                    // computeCircumscribedRadius
+    sh.volume = 2 * hh * PI * r * r;                           // getVolume
+    double constant = 0.5 * hh * r * r * PI;                   // BuildInertia
+    sh.inertia[0] = sh.inertia[5] = constant * (4.0 * hh * hh / 3.0 + r * r);
+    sh.inertia[3] = 2.0 * constant * r * r;
   } else {
     const int* P = c->type_poly + 4 * t;
     for (int k = 0; k < P[1]; ++k) {

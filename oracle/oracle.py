@@ -141,6 +141,11 @@ def read_xml(path):
         elif cv.find("Polyhedron") is not None:
             t["shape"] = 2
             t["verts"], t["faces"] = read_poly(cv.find("Polyhedron").get("Name"))
+        elif cv.find("Cylinder") is not None:
+            cy = cv.find("Cylinder")
+            t["shape"] = 3
+            r = float(cy.get("Radius"))
+            t["extent"] = [r, float(cy.get("Height")) / 2.0, r]
         else:
             raise ValueError("unsupported particle shape")
         types.append(t)

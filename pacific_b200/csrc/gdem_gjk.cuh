@@ -16,7 +16,7 @@
 namespace gdem {
 
 struct ConvexRef {
-  int kind;              // 0 sphere, 1 box, 2 polyhedron
+  int kind;              // 0 sphere, 1 box, 2 polyhedron, 3 cylinder
   double radius;         // sphere radius
   d3 extent;             // box half lengths
   const double* verts;   // polyhedron vertices (x, y, z), local frame
@@ -60,6 +60,18 @@ __device__ __forceinline__ d3 support(ConvexRef const& s, d3 v) {
     double n = norm(v);
     if (n > 1.0e-10) { double r = s.radius / n; return mk(v.x * r, v.y * r, v.z * r); }
     return mk(0., 0., 0.);
+  }
+  if (s.kind == 3) {
+    // Cylinder::support (Geometry/src/Cylinder.cpp:112-133): axis along local
+    // Y, extent = (radius, half height, radius)
+    if (!(norm(v) > 1.0e-10)) return mk(0., 0., 0.);
+    const double sxz = sqrt(v.x * v.x + v.z * v.z);
+    const double hh = v.y < 0. ? -s.extent.y : s.extent.y;
+    if (sxz > 1.0e-10) {
+      const double d = s.extent.x / sxz;
+      return mk(v.x * d, fabs(v.y) < 1.0e-10 ? 0. : hh, v.z * d);
+    }
+    return mk(0., hh, 0.);
   }
   if (s.kind == 1) {
     if (norm(v) < 1.0e-10) return mk(0., 0., 0.);

@@ -262,6 +262,17 @@ InstanceDesc readInstance(std::string const& path) {
       Iv[0] = 8.0 * e[0] * e[1] * e[2] * (e[1] * e[1] + e[2] * e[2]) / 3.0;
       Iv[1] = 8.0 * e[0] * e[1] * e[2] * (e[0] * e[0] + e[2] * e[2]) / 3.0;
       Iv[2] = 8.0 * e[0] * e[1] * e[2] * (e[0] * e[0] + e[1] * e[1]) / 3.0;
+    } else if (XmlNode const* cy = cv->child("Cylinder")) {
+      // Cylinder::getVolume, BuildInertia, computeCircumscribedRadius
+      // (Geometry/src/Cylinder.cpp:32-106); axis along the local Y
+      t.shape = 3;
+      double r = cy->attrD("Radius"), hh = cy->attrD("Height") / 2.;
+      t.extent[0] = r; t.extent[1] = hh; t.extent[2] = r;
+      t.radius = std::sqrt(r * r + hh * hh);
+      vol = 2 * hh * PI * r * r;
+      double constant = 0.5 * hh * r * r * PI;
+      Iv[0] = Iv[2] = constant * (4.0 * hh * hh / 3.0 + r * r);
+      Iv[1] = 2.0 * constant * r * r;
     } else if (XmlNode const* ph = cv->child("Polyhedron")) {
       t.shape = 2;
       PolyFile P = readPolyFile(ph->attr("Name"));

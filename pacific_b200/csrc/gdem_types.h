@@ -50,10 +50,11 @@ struct TypeDesc {
   double eqrad;          // Component::getEquivalentSphereRadius
   double weight[3];      // m (1 - rho_f / rho) g
   int mat;               // material index
-  int shape;             // 0 sphere, 1 box, 2 polyhedron
+  int shape;             // 0 sphere, 1 box, 2 polyhedron, 3 cylinder
   float r_f;             // radius in FP32 (FP32-split broad phase)
   int pad_r;
-  double extent[3];      // box half lengths / bounding-box half extent
+  double extent[3];      // box half lengths / bounding-box half extent;
+                         // cylinder (radius, half height, radius)
   double scaling[3];     // crust shrink factors (extent - crust) / extent
   int poly_begin;        // first vertex of a polyhedron in the vertex table
   int poly_count;        // its vertex count

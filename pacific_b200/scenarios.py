@@ -83,6 +83,9 @@ class Scenario:
                 geo = f'          <Box LX="{_f(s[0])}" LY="{_f(s[1])}" LZ="{_f(s[2])}"/>'
             elif shape == "polyhedron":
                 geo = f'          <Polyhedron Name="{t["file"]}"/>'
+            elif shape == "cylinder":
+                geo = (f'          <Cylinder Radius="{_f(t["cyl_radius"])}" '
+                       f'Height="{_f(t["height"])}"/>')
             else:
                 geo = f'          <Sphere Radius="{_f(t["radius"])}"/>'
             L += [f'      <Particle Number="{int(cnt[k])}" Density="{_f(t["density"])}">',
@@ -352,12 +355,14 @@ def rotation_matrices(q):
 
 def convex_pour(n=200_000, seed=1238, poly_path=None, box=(0.1, 0.1, 0.3), cube_edge=2.0e-3,
                 tet_edge=3.0e-3, density=2000.0, kn=5.0e4, en=0.5, muc=0.4, dt=2.0e-6,
-                vmax=0.0) -> Scenario:
+                vmax=0.0, cylinders=False) -> Scenario:
     """Half cubes, half regular tetrahedra with uniformly random orientations
     on a jittered lattice of spacing 1.02 x the tetrahedron's circumscribed
     diameter, poured under gravity into an open-top box of footprint
     box[0] x box[1].  The lattice does not fit in a box[2]-high container, so
-    the side walls and the linked-cell domain extend up to the lattice top."""
+    the side walls and the linked-cell domain extend up to the lattice top.
+    With cylinders=True a third class, cylinders of radius 0.8 mm and height
+    2 mm, takes a third of the sites."""
     rng = np.random.default_rng(seed)
     r_tet = tet_edge * np.sqrt(6.0) / 4.0
     spacing = 2.0 * r_tet * 1.02
@@ -373,11 +378,18 @@ def convex_pour(n=200_000, seed=1238, poly_path=None, box=(0.1, 0.1, 0.3), cube_
     v = rng.uniform(-vmax, vmax, size=(n, 3)) if vmax > 0 else np.zeros((n, 3))
     q = random_quaternions(rng, n)
     type_ = (rng.random(n) < 0.5).astype(np.int32)        # 0 cube, 1 tetrahedron
+    if cylinders:
+        type_ = rng.integers(0, 3, n).astype(np.int32)    # 2 cylinder
     r_cube = cube_edge * np.sqrt(3.0) / 2.0
     types = [dict(shape="box", size=(cube_edge,) * 3, radius=float(r_cube),
                   crust=float(0.1 * r_cube), density=density, material="matP"),
              dict(shape="polyhedron", file=str(poly_path), radius=float(r_tet),
                   crust=float(0.1 * r_tet), density=density, material="matP")]
+    if cylinders:
+        rc, hc = 0.8e-3, 2.0e-3
+        r_cyl = float(np.hypot(rc, 0.5 * hc))
+        types.append(dict(shape="cylinder", cyl_radius=rc, height=hc, radius=r_cyl,
+                          crust=float(0.1 * r_cyl), density=density, material="matP"))
     dom = (box[0], box[1], height)
     walls = _box_walls(dom, 2.0e-3, float(0.1 * r_cube), "matW")
     kt = 2.0 / 7.0 * kn

@@ -42,16 +42,20 @@ def _quiet(f, *a):
 POLY_TOKEN = "@POLYHEDRON_FILE@"
 
 
-def _convex():
+def _convex(cylinders=False, seed=5, vmax=0.2):
     d = Path(tempfile.mkdtemp())
     poly = scenarios.write_tetrahedron(d / "tet.poly")
-    return scenarios.convex_pour(n=400, seed=5, poly_path=poly, box=(0.03, 0.03, 0.02), vmax=0.2)
+    return scenarios.convex_pour(n=400, seed=seed, poly_path=poly, box=(0.03, 0.03, 0.02),
+                                 vmax=vmax, cylinders=cylinders)
 
 
 SCENARIOS = {
     "settling_box": (lambda: scenarios.settling_box(n=500, seed=11), [0, 1, 800, 801, 1600, 1601]),
     "periodic_gas": (lambda: scenarios.periodic_gas(n_fcc=5, seed=12), [0, 1, 20, 21]),
     "convex_pour": (_convex, [0, 1, 3000, 3001, 6000, 6001]),
+    # cubes, tetrahedra and cylinders (GJK with the cylinder support function)
+    "convex_cylinders": (lambda: _convex(cylinders=True, seed=6, vmax=1.0),
+                         [0, 1, 3000, 3001, 6000, 6001]),
     # Hooke law (no tangential memory) with a rolling-resistance moment
     "settling_hooke": (lambda: scenarios.settling_box(n=500, seed=17, etat=None, law="Hooke",
                                                       kr=0.05, vmax=0.2),

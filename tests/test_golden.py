@@ -21,7 +21,7 @@ import pytest
 from oracle.oracle import Oracle
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
-CONVEX = {"convex_pour"}
+CONVEX = {"convex_pour", "convex_cylinders"}
 # fixtures whose law keeps no contact memory, so the reference's contact set is
 # not recorded (its restatement is pinned bit for bit above instead)
 NO_MEMORY = {"settling_hooke"}
@@ -43,7 +43,8 @@ def _hist_dict(own, par, kd, pn):
     return {(int(a), int(b)): (tuple(k), tuple(p)) for a, b, k, p in zip(own, par, kd, pn)}
 
 
-@pytest.mark.parametrize("name", ["settling_box", "convex_pour", "settling_hooke"])
+@pytest.mark.parametrize("name", ["settling_box", "convex_pour", "convex_cylinders",
+                                  "settling_hooke"])
 def test_restatement_bitexact_vs_reference(tmp_path, oracle_lib, name):
     g, xml = _load(name, tmp_path)
     o = Oracle(xml)
@@ -114,7 +115,7 @@ def _gpu_step_from_golden(g, xml, k, k1, precision, tol):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["settling_box", "periodic_gas", "convex_pour",
-                                  "settling_hooke"])
+                                  "convex_cylinders", "settling_hooke"])
 def test_gpu_fp64_step_matches_reference(tmp_path, lib, name):
     from pacific_b200 import FP64
     g, xml = _load(name, tmp_path)
@@ -132,7 +133,7 @@ def test_gpu_fp64_step_matches_reference(tmp_path, lib, name):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["settling_box", "periodic_gas", "convex_pour",
-                                  "settling_hooke"])
+                                  "convex_cylinders", "settling_hooke"])
 def test_gpu_fp32split_step_matches_reference(tmp_path, lib, name):
     from pacific_b200 import FP32_SPLIT
     g, xml = _load(name, tmp_path)
