@@ -101,29 +101,29 @@ def algorithmic_bytes(kernel, n, entries, contacts, ncells, fp64):
     """Compulsory DRAM bytes of one launch of each phase of a spheres-only
     step: each input read once, each output written once, neighbour re-reads
     counted as cache hits.  Per particle unless noted."""
-    if kernel == "key":          # F v x type inst | skey rank; cell-count RMW
-        return n * (24 * 3 + 8 + 8 + 8)
+    if kernel in ("step64", "step32"):
+        # fused force + leapfrog: cellc id type inst npairs wrap disp x v w w_bf q |
+        # x v w w_bf q wrap disp (second buffers); per entry its word; per
+        # contact the history key + values, read and written
+        per_p = (16 + 4 + 4 + 4 + 4 + 4 + 12 + 72 + 24 + 32) + (72 + 24 + 32 + 4 + 12)
+        per_c = 2 * (8 + (72 if fp64 else 36))
+        return n * per_p + 4 * entries + contacts * per_c
+    if kernel == "move_only":    # F T x v w w_bf q type inst disp wrap | x v w w_bf q disp wrap
+        return n * (48 + 104 + 8 + 12 + 4 + 104 + 12 + 4)
+    if kernel == "bin":          # x inst | skey rank; cell-count RMW
+        return n * (24 + 4 + 8 + 8)
     if kernel == "scan":         # counts | starts (per cell)
         return ncells * 8
     if kernel == "place":        # skey rank start[skey] | order
         return n * 16
     if kernel == "cellsort":     # starts, count reset (per cell); order, id of shared cells
         return ncells * 8 + n * 8
-    if kernel == "move_gather":  # order id type inst skey x v wbf q F T | same + w key cellc
-        #                          + pos/vel/omg (FP64) or offsets (FP32-split)
-        return n * (172 + 160 + (96 if fp64 else 16))
+    if kernel == "permute":      # order skey ids state F T | ids state F T cellc + pos / offset
+        return n * (4 + 4 + 12 + 176 + 12 + 176 + 16 + (32 if fp64 else 16))
+    if kernel == "copyback":     # ids state F T | ids state F T disp wrap
+        return n * (12 + 176 + 12 + 176 + 12 + 4)
     if kernel in ("pairs64", "pairs32"):   # cellc + own position | npairs; entries; starts
         return n * (16 + (32 if fp64 else 16) + 4) + 4 * entries + 4 * ncells
-    if kernel in ("forces64", "forces32"):
-        # cellc id type npairs + own position (FP64 packed or SoA x) | F T;
-        # per entry the entry word; per contact the history key + values, read and written
-        per_p = 16 + 4 + 4 + 4 + (96 if fp64 else 24) + 48
-        per_c = 2 * (8 + (72 if fp64 else 36))
-        return n * per_p + 4 * entries + contacts * per_c
-    if kernel == "kick":         # F T v wbf q type | v wbf w
-        return n * (48 + 48 + 32 + 4 + 72)
-    if kernel == "hist_clear":   # the new table's keys are reset
-        return None
     return None
 
 
@@ -449,12 +449,14 @@ def main():
     for name, prec in (("fp64", FP64), ("fp32_split", FP32_SPLIT)):
         g = make_system(xml, sc, prec)
         g.step(args.warmup)
+        e0, r0 = g.step_counts()
         if name == "fp32_split":
             with ClockSampler(local) as clk:
                 ms = timed_steps(g, dist, args.steps)
             clocks = clk.summary()
         else:
             ms = timed_steps(g, dist, args.steps)
+        e1, r1 = g.step_counts()
         st = g.status()
         entries, contacts = g.pair_counts()
         # per-phase device times with CUDA events (plain launches)
@@ -463,7 +465,7 @@ def main():
         kt = g.kernel_times()
         g.set_profiling(False)
         res[name] = dict(ms=ms, status=st, entries=entries, contacts=contacts, kt=kt, g=g,
-                         ncells=int(np.prod(g.grid()[0])))
+                         ncells=int(np.prod(g.grid()[0])), evals=(e0, e1), rebuilds=r1 - r0)
         if name == "fp64":
             g.close()
 
@@ -478,7 +480,7 @@ def main():
         v64 = world * n * args.steps / (fp64["ms"] * 1e-3)
         # roofline of the dominant kernel of the FP32-split step
         kt = fp32["kt"]
-        dom = max((k for k in kt if k not in ("cell_clear", "hist_clear")), key=lambda k: kt[k][0])
+        dom = max((k for k in kt if k not in ("decide", "hist_fill")), key=lambda k: kt[k][0])
         avg_ms = kt[dom][0] / kt[dom][1]
         ncells = fp32["ncells"]
         ab = algorithmic_bytes(dom, n, fp32["entries"], fp32["contacts"], ncells, False)
@@ -522,9 +524,15 @@ def main():
                     "steps": args.e2e_steps},
             "gpu_launches": None,
         }
-        # kernels launched in the timed region: per step move, scan(3), place,
-        # cellsort, gather, pairs, forces; plus the closing kick
-        line["gpu_launches"] = args.steps * 9 + 1
+        # kernels launched in the timed region: the opening move, per step
+        # k_decide + the fused step kernel, per pair-list rebuild its 9
+        # kernels (bin, scan x3, place, cellsort, permute, copyback, pairs),
+        # and the history-table refills (every 512 evaluations per table)
+        e0, e1 = fp32["evals"]
+        fills = sum(1 for e in range(e0 + 1, e1 + 1) if e % 512 < 2)
+        line["gpu_launches"] = 1 + 2 * args.steps + 9 * fp32["rebuilds"] + fills
+        line["pair_list"] = {"rebuilds_fp32_split": fp32["rebuilds"],
+                             "rebuilds_fp64": fp64["rebuilds"], "steps": args.steps}
         if not args.no_error:
             line["error"] = {"sample": "periodic_gas n_fcc=20 (32,000 spheres), one step "
                                        "after 100 oracle steps, vs the CPU FP64 oracle",

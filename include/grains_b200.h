@@ -32,7 +32,8 @@ typedef struct gdem_system* gdem_handle;
 
 /* precision modes */
 #define GDEM_FP64 0        /* all contact arithmetic in FP64 (reference order) */
-#define GDEM_FP32_SPLIT 1  /* cell + float-pair offsets, FP32 force law, FP64 leapfrog */
+#define GDEM_FP32_SPLIT 1  /* FP32 cell-relative pair search, FP64 contact geometry,
+                              FP32 force law (FP64 when ill-conditioned), FP64 leapfrog */
 
 /* return codes */
 #define GDEM_OK 0
@@ -99,6 +100,13 @@ int gdem_download_basis(gdem_handle h, double* basis);
  * 1781-1811), the quantity Grains3D writes to *_VelocityMaxMean.dat. */
 int gdem_velocity_stats(gdem_handle h, double* vmax, double* vmean);
 
+/* Force evaluations and pair-list rebuilds since the state was created.
+ * The pair list holds every pair whose bounding spheres are closer than the
+ * skin; it is rebuilt (counting sort into cell order + 27-cell search) only
+ * before an evaluation at which some particle has moved more than half the
+ * skin since the last rebuild. */
+int gdem_step_counts(gdem_handle h, int64_t* evaluations, int64_t* rebuilds);
+
 /* FP32-split mode: contact-law evaluations since the last reset, and how
  * many of them were re-evaluated in FP64 because the FP32 force was
  * ill-conditioned (a small difference of large terms).  Zero in FP64 mode. */
@@ -123,7 +131,10 @@ int gdem_upload_history(gdem_handle h, int64_t n, const int* owner, const int* p
 int gdem_init(gdem_handle h);
 
 /* Advances nsteps kick-drift-kick leapfrog steps of size dt (from the XML).
- * Equivalent to the loop body of Grains::Simulation (Grains.cpp:286-364). */
+ * Equivalent to the loop body of Grains::Simulation (Grains.cpp:286-364).
+ * Per step one fused kernel evaluates the contact forces and applies the
+ * closing and the next opening kick and drift; the pair list is rebuilt
+ * only when needed (gdem_step_counts), inside a CUDA-graph conditional node. */
 int gdem_step(gdem_handle h, int nsteps);
 
 /* State by particle ID; any pointer may be NULL. */

@@ -25,7 +25,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", str(CSR
 UNITS = [
     ("gdem_integrate.cu", ["-fmad=false"]),
     ("gdem_contact64.cu", ["-fmad=false"]),
-    ("gdem_contact32.cu", ["-fmad=true"]),
+    ("gdem_contact32.cu", ["-fmad=false"]),
     ("gdem_host.cu", ["-fmad=false"]),
     ("gdem_noalloc.cu", ["-fmad=false"]),
     ("xml_reader.cpp", []),

@@ -23,6 +23,7 @@
 // (Component/src/Torsor.cpp:184-189).
 #include "gdem_contact_common.cuh"
 #include "gdem_kernels.cuh"
+#include "gdem_motion.cuh"
 
 namespace gdem {
 
@@ -258,11 +259,14 @@ __device__ __forceinline__ void contactLaw32(ModelDesc const& m, double dt, Cont
   }
 }
 
-__global__ void __launch_bounds__(256) k_pairs32(DevState S) {
+// Lists a candidate when its bounding spheres are closer than the skin, with
+// a relative margin of 4e-6 that covers the FP32 rounding of the test.
+__global__ void __launch_bounds__(256) k_pairs32(DevState S, const int* gate) {
+  if (gate && !*gate) return;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
   const int4 cc = S.cellc[t];
-  GridDesc const& g = S.grids[cc.w];
+  GridDesc const& g = S.bgrids[cc.w];
   const float4 ha = S.offh[t];
   int* out = S.pairs + (size_t)t * kPairCap;
   int cnt = 0;
@@ -279,7 +283,7 @@ __global__ void __launch_bounds__(256) k_pairs32(DevState S) {
     float dx = fmaf(s * (float)dcx, ex, h1.x - h0.x);
     float dy = fmaf(s * (float)dj, ey, h1.y - h0.y);
     float dz = fmaf(s * (float)dk, ez, h1.z - h0.z);
-    float R = (h0.w + h1.w) * (1.f + 4.e-6f);
+    float R = (h0.w + h1.w + g.skin_f) * (1.f + 4.e-6f);
     if (dx * dx + dy * dy + dz * dz > R * R) return;
     if (cnt < kPairCap) out[cnt] = u | (offCode(dcx, dj, dk) << 27);
     ++cnt;
@@ -291,12 +295,14 @@ __global__ void __launch_bounds__(256) k_pairs32(DevState S) {
 // kConvex: some class is not a sphere, so the GJK narrow phase is compiled in
 // (it is kept out of the sphere-only kernel, whose registers it would triple).
 template <bool kConvex>
-__global__ void __launch_bounds__(256, 2) k_forces32(DevState S) {
+__global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_step32(DevState S, int flags) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
   const int cap = S.cap;
   const int4 cc = S.cellc[t];
   GridDesc const& g = S.grids[cc.w];
+  GridDesc const& bg = S.bgrids[cc.w];
+  const unsigned tag = (unsigned)S.ctl[kCtlEpoch], tag_old = tag - 1u;
   const int ida = S.id[t];
   TypeDesc const& ta = S.types[S.type[t]];
   const d3 xt = ld3(S.x, cap, t);
@@ -318,7 +324,7 @@ __global__ void __launch_bounds__(256, 2) k_forces32(DevState S) {
     // exact narrow phase on the FP64 master positions: lower ID at its own
     // position, the other at its periodic image seen from it
     int sh[3];
-    neighbourKey(g, cc.x, cc.y, cc.z, di, dj, dk, sh);
+    entryShift(S, bg, cc, t, u, di, dj, dk, sh);
     const d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
     const d3 xu = ld3(S.x, cap, u);
     const d3 x0 = t0 ? xt : xu;
@@ -347,11 +353,11 @@ __global__ void __launch_bounds__(256, 2) k_forces32(DevState S) {
     if (m.memory) {
       const int id0 = t0 ? ida : idb, id1 = t0 ? idb : ida;
       const unsigned long long key = pairKey(id0, id1);
-      int old = histFind(S.hist_old, key);
+      int old = histFind(S.hist_old, key, tag_old);
       if (old >= 0) loadHistF(S.hist_old, old, kd, pn, sp);
       contactLaw32(m, S.dt, ct, b0, b1, old >= 0, kd, pn, sp, f, mr, re);
       if (t0) {
-        int slot = histInsert(S.hist_new, key);
+        int slot = histInsert(S.hist_new, key, tag);
         if (slot < 0) raise(S.status, kErrHashFull);
         else storeHistF(S.hist_new, slot, kd, pn, sp);
       }
@@ -395,10 +401,10 @@ __global__ void __launch_bounds__(256, 2) k_forces32(DevState S) {
     ++nlaw;
     if (m.memory) {
       const unsigned long long key = wallKey(ida, k);
-      int old = histFind(S.hist_old, key);
+      int old = histFind(S.hist_old, key, tag_old);
       if (old >= 0) loadHistF(S.hist_old, old, kd, pn, sp);
       contactLaw32(m, S.dt, ct, b0, b1, old >= 0, kd, pn, sp, f, mr, re);
-      int slot = histInsert(S.hist_new, key);
+      int slot = histInsert(S.hist_new, key, tag);
       if (slot < 0) raise(S.status, kErrHashFull);
       else storeHistF(S.hist_new, slot, kd, pn, sp);
     } else {
@@ -413,10 +419,13 @@ __global__ void __launch_bounds__(256, 2) k_forces32(DevState S) {
     Ts = Ts + crossf(lev0, f);
     if (m.rolling) Ts = Ts + mr;
   }
-  S.F[t] = ta.weight[0] + (double)Fs.x;
-  S.F[cap + t] = ta.weight[1] + (double)Fs.y;
-  S.F[2 * cap + t] = ta.weight[2] + (double)Fs.z;
-  S.T[t] = (double)Ts.x; S.T[cap + t] = (double)Ts.y; S.T[2 * cap + t] = (double)Ts.z;
+  const d3 F = mk(ta.weight[0] + (double)Fs.x, ta.weight[1] + (double)Fs.y,
+                  ta.weight[2] + (double)Fs.z);
+  const d3 T = mk((double)Ts.x, (double)Ts.y, (double)Ts.z);
+  if (flags & kStepStoreFT) {
+    st3(S.F, cap, t, F);
+    st3(S.T, cap, t, T);
+  }
   // warp-aggregated counters of the FP64 re-evaluations
   const unsigned mask = __activemask();
   const int wl = __reduce_add_sync(mask, nlaw), wr = __reduce_add_sync(mask, nre);
@@ -424,17 +433,18 @@ __global__ void __launch_bounds__(256, 2) k_forces32(DevState S) {
     atomicAdd(S.law_counts, (unsigned long long)wl);
     if (wr) atomicAdd(S.law_counts + 1, (unsigned long long)wr);
   }
+  advanceParticle(S, t, ta, F, T, (flags & kStepClose) != 0, (flags & kStepMove) != 0);
 }
 
 }  // namespace
 
-void launch_pairs32(DevState const& S, cudaStream_t st) {
-  if (S.n) k_pairs32<<<(S.n + 255) / 256, 256, 0, st>>>(S);
+void launch_pairs32(DevState const& S, const int* gate, cudaStream_t st) {
+  if (S.n) k_pairs32<<<(S.n + 255) / 256, 256, 0, st>>>(S, gate);
 }
-void launch_forces32(DevState const& S, cudaStream_t st) {
+void launch_step32(DevState const& S, int flags, cudaStream_t st) {
   if (!S.n) return;
-  if (S.any_convex) k_forces32<true><<<(S.n + 255) / 256, 256, 0, st>>>(S);
-  else k_forces32<false><<<(S.n + 255) / 256, 256, 0, st>>>(S);
+  if (S.any_convex) k_step32<true><<<(S.n + 255) / 256, 256, 0, st>>>(S, flags);
+  else k_step32<false><<<(S.n + 255) / 256, 256, 0, st>>>(S, flags);
 }
 
 }  // namespace gdem

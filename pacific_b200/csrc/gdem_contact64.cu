@@ -1,35 +1,40 @@
-// gdem_contact64.cu -- FP64-mode broad phase, narrow phase, HODC force and
-// per-particle reduction.  Compiled with -fmad=false so that every FP64
-// expression rounds like the reference's scalar CPU code.
+// gdem_contact64.cu -- FP64 mode: pair-list search and the fused force +
+// leapfrog step.  Compiled with -fmad=false so that every FP64 expression
+// rounds like the reference's scalar CPU code.
 //
-//   k_pairs64   27-cell stencil enumeration (the reference uses the 13-cell
-//               half stencil of LinkedCell::setCellContactNeighborhood,
-//               Base/src/LinkedCell.cpp:958-984; here each particle lists
-//               all its partners so that its forces can be reduced without
-//               atomics).  A candidate is kept when ClosestPointSPHERESPHERE
-//               reports contact (distance <= 0), evaluated with the lower-ID
-//               body first so both directions of a pair agree bit for bit.
-//   k_forces64  narrow phase + HookeMemory force + tangential history through
-//               the hashed pair table + deterministic segmented reduction of
-//               each particle's force and torque over its own pair segment,
-//               in list order, then its wall contacts (SimpleObstacle::
-//               InterAction, Component/src/SimpleObstacle.cpp:222-271).
+//   k_pairs64   27-cell stencil enumeration over the pair-list grid (the
+//               reference uses the 13-cell half stencil of LinkedCell::
+//               setCellContactNeighborhood, Base/src/LinkedCell.cpp:958-984;
+//               here each particle lists all its partners so that its forces
+//               can be reduced without atomics).  A candidate is listed when
+//               its bounding spheres are closer than the skin, evaluated with
+//               the lower-ID body first so both directions of a pair agree.
+//   k_step64    for each particle: narrow phase on every listed partner
+//               (ClosestPointSPHERESPHERE or GJK), Hooke / HookeMemory force
+//               with the tangential history in the hashed pair table, the
+//               deterministic reduction of its force and torque over its own
+//               list in list order, then its wall contacts (SimpleObstacle::
+//               InterAction, Component/src/SimpleObstacle.cpp:222-271); then
+//               its leapfrog (closing kick, opening kick, drift) into the
+//               second buffers.
 #include "gdem_contact_common.cuh"
 #include "gdem_kernels.cuh"
+#include "gdem_motion.cuh"
 
 namespace gdem {
 
 namespace {
 
-// Keeps a candidate when ClosestPointSPHERESPHERE would report contact up to
-// a relative margin of 1e-12; k_forces64 then decides exactly (distance < 0)
-// in lower-ID-first orientation.  The margin only matters for periodic
-// images, where the two orientations round the image translation differently.
-__global__ void __launch_bounds__(256) k_pairs64(DevState S) {
+// Lists a candidate when its bounding spheres are closer than the skin (with
+// a relative margin of 1e-12, for periodic images whose two orientations
+// round the image translation differently); k_step64 then decides contact
+// exactly (distance < 0) in lower-ID-first orientation.
+__global__ void __launch_bounds__(256) k_pairs64(DevState S, const int* gate) {
+  if (gate && !*gate) return;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
   const int4 cc = S.cellc[t];
-  GridDesc const& g = S.grids[cc.w];
+  GridDesc const& g = S.bgrids[cc.w];
   const double4 pa = S.pos64[t];
   int* out = S.pairs + (size_t)t * kPairCap;
   int cnt = 0;
@@ -41,7 +46,7 @@ __global__ void __launch_bounds__(256) k_pairs64(DevState S) {
     d3 d = u > t ? (mk(pb.x, pb.y, pb.z) + shift) - mk(pa.x, pa.y, pa.z)
                  : (mk(pa.x, pa.y, pa.z) + (-shift)) - mk(pb.x, pb.y, pb.z);
     double R = pa.w + pb.w;
-    if (norm(d) - R > 1.0e-12 * R) return;
+    if (norm(d) - R > g.skin + 1.0e-12 * R) return;
     if (cnt < kPairCap) out[cnt] = u | (offCode(dcx, dj, dk) << 27);
     ++cnt;
   });
@@ -62,19 +67,20 @@ __device__ __forceinline__ void storeHist(HistTable const& t, int slot, d3 kd, d
 // kConvex: some class is not a sphere, so the GJK narrow phase is compiled in
 // (it is kept out of the sphere-only kernel, whose registers it would triple).
 template <bool kConvex>
-__global__ void __launch_bounds__(256) k_forces64(DevState S) {
+__global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_step64(DevState S, int flags) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
   const int cap = S.cap;
   const int4 cc = S.cellc[t];
   GridDesc const& g = S.grids[cc.w];
+  GridDesc const& bg = S.bgrids[cc.w];
   const int ida = S.id[t];
   TypeDesc const& ta = S.types[S.type[t]];
-  const double4 pa = S.pos64[t], va = S.vel64[t], wa = S.omg64[t];
-  const d3 xt = mk(pa.x, pa.y, pa.z), vt = mk(va.x, va.y, va.z), wt = mk(wa.x, wa.y, wa.z);
+  const d3 xt = ld3(S.x, cap, t), vt = ld3(S.v, cap, t), wt = ld3(S.w, cap, t);
   d3 F = mk(ta.weight[0], ta.weight[1], ta.weight[2]);
   d3 T = mk(0., 0., 0.);
   const double dt = S.dt;
+  const unsigned tag = (unsigned)S.ctl[kCtlEpoch], tag_old = tag - 1u;
   const int np = S.npairs[t];
   const int* seg = S.pairs + (size_t)t * kPairCap;
   for (int e = 0; e < np; ++e) {
@@ -82,25 +88,26 @@ __global__ void __launch_bounds__(256) k_forces64(DevState S) {
     const int u = (int)(ent & ((1u << 27) - 1));
     int di, dj, dk, sh[3];
     offDecode((int)(ent >> 27), &di, &dj, &dk);
-    neighbourKey(g, cc.x, cc.y, cc.z, di, dj, dk, sh);
+    entryShift(S, bg, cc, t, u, di, dj, dk, sh);
     d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
     const int idb = S.id[u];
     TypeDesc const& tb = S.types[S.type[u]];
-    const double4 pb = S.pos64[u], vb = S.vel64[u], wb = S.omg64[u];
+    const d3 xu = ld3(S.x, cap, u), vu = ld3(S.v, cap, u), wu = ld3(S.w, cap, u);
     const bool t0 = ida < idb;
     // canonical bodies: p0 = lower ID at its own position, p1 at its image
     d3 x0, x1, v0, v1, w0, w1;
     double r0, r1, c0, c1, m0, m1, q0, q1;
     int mat0, mat1, id0, id1;
     if (t0) {
-      x0 = xt; v0 = vt; w0 = wt; r0 = pa.w; m0 = va.w; q0 = wa.w; c0 = ta.crust; mat0 = ta.mat; id0 = ida;
-      x1 = mk(pb.x, pb.y, pb.z) + shift; v1 = mk(vb.x, vb.y, vb.z); w1 = mk(wb.x, wb.y, wb.z);
-      r1 = pb.w; m1 = vb.w; q1 = wb.w; c1 = tb.crust; mat1 = tb.mat; id1 = idb;
+      x0 = xt; v0 = vt; w0 = wt; r0 = ta.radius; m0 = ta.mass; q0 = ta.eqrad; c0 = ta.crust;
+      mat0 = ta.mat; id0 = ida;
+      x1 = xu + shift; v1 = vu; w1 = wu; r1 = tb.radius; m1 = tb.mass; q1 = tb.eqrad;
+      c1 = tb.crust; mat1 = tb.mat; id1 = idb;
     } else {
-      x0 = mk(pb.x, pb.y, pb.z); v0 = mk(vb.x, vb.y, vb.z); w0 = mk(wb.x, wb.y, wb.z);
-      r0 = pb.w; m0 = vb.w; q0 = wb.w; c0 = tb.crust; mat0 = tb.mat; id0 = idb;
-      x1 = xt + (-shift); v1 = vt; w1 = wt; r1 = pa.w; m1 = va.w; q1 = wa.w; c1 = ta.crust;
-      mat1 = ta.mat; id1 = ida;
+      x0 = xu; v0 = vu; w0 = wu; r0 = tb.radius; m0 = tb.mass; q0 = tb.eqrad; c0 = tb.crust;
+      mat0 = tb.mat; id0 = idb;
+      x1 = xt + (-shift); v1 = vt; w1 = wt; r1 = ta.radius; m1 = ta.mass; q1 = ta.eqrad;
+      c1 = ta.crust; mat1 = ta.mat; id1 = ida;
     }
     Contact64 ct;
     if (!kConvex || (ta.shape == 0 && tb.shape == 0)) {
@@ -120,13 +127,13 @@ __global__ void __launch_bounds__(256) k_forces64(DevState S) {
     d3 f, mr;
     if (m.memory) {
       const unsigned long long key = pairKey(id0, id1);
-      int old = histFind(S.hist_old, key);
+      int old = histFind(S.hist_old, key, tag_old);
       d3 kd, pn, sp;
       if (old >= 0) loadHist(S.hist_old, old, kd, pn, sp);
       hodc64(m, dt, ct.point, ct.overlap, x0, v0, w0, m0, q0, x1, v1, w1, m1, q1, old >= 0,
              kd, pn, sp, f, mr);
       if (t0) {
-        int slot = histInsert(S.hist_new, key);
+        int slot = histInsert(S.hist_new, key, tag);
         if (slot < 0) raise(S.status, kErrHashFull);
         else storeHist(S.hist_new, slot, kd, pn, sp);
       }
@@ -152,7 +159,7 @@ __global__ void __launch_bounds__(256) k_forces64(DevState S) {
   for (int k = 0; k < g.wall_count; ++k) {
     WallDesc const& wd = S.walls[g.wall_begin + k];
     Contact64 ct = (!kConvex || ta.shape == 0)
-        ? sphereWall64(xt, pa.w, ta.crust, wd)
+        ? sphereWall64(xt, ta.radius, ta.crust, wd)
         : convexContact64(convexOf(ta, S.poly_verts), crustXForm(S.basis, cap, t, ta.scaling, xt),
                           ta.radius, ta.crust, convexOf(wd),
                           identityXForm(wd.scaling, mk(wd.centre[0], wd.centre[1], wd.centre[2])),
@@ -166,17 +173,17 @@ __global__ void __launch_bounds__(256) k_forces64(DevState S) {
     const d3 wc = mk(wd.centre[0], wd.centre[1], wd.centre[2]);
     if (m.memory) {
       const unsigned long long key = wallKey(ida, k);
-      int old = histFind(S.hist_old, key);
+      int old = histFind(S.hist_old, key, tag_old);
       d3 kd, pn, sp;
       if (old >= 0) loadHist(S.hist_old, old, kd, pn, sp);
-      hodc64(m, dt, ct.point, ct.overlap, xt, vt, wt, va.w, wa.w, wc, zero, zero, 1.e20,
+      hodc64(m, dt, ct.point, ct.overlap, xt, vt, wt, ta.mass, ta.eqrad, wc, zero, zero, 1.e20,
              wd.eqrad, old >= 0, kd, pn, sp, f, mr);
-      int slot = histInsert(S.hist_new, key);
+      int slot = histInsert(S.hist_new, key, tag);
       if (slot < 0) raise(S.status, kErrHashFull);
       else storeHist(S.hist_new, slot, kd, pn, sp);
     } else {
-      hooke64(m, ct.point, ct.overlap, xt, vt, wt, va.w, wa.w, wc, zero, zero, 1.e20, wd.eqrad,
-              f, mr);
+      hooke64(m, ct.point, ct.overlap, xt, vt, wt, ta.mass, ta.eqrad, wc, zero, zero, 1.e20,
+              wd.eqrad, f, mr);
     }
     if (S.diag) {
       double* fd = S.wall_force + 3 * ((size_t)t * S.max_walls + k);
@@ -186,19 +193,22 @@ __global__ void __launch_bounds__(256) k_forces64(DevState S) {
     T = T + cross(ct.point - xt, f);
     if (m.rolling) T = T + mr;
   }
-  st3(S.F, cap, t, F);
-  st3(S.T, cap, t, T);
+  if (flags & kStepStoreFT) {
+    st3(S.F, cap, t, F);
+    st3(S.T, cap, t, T);
+  }
+  advanceParticle(S, t, ta, F, T, (flags & kStepClose) != 0, (flags & kStepMove) != 0);
 }
 
 }  // namespace
 
-void launch_pairs64(DevState const& S, cudaStream_t st) {
-  if (S.n) k_pairs64<<<(S.n + 255) / 256, 256, 0, st>>>(S);
+void launch_pairs64(DevState const& S, const int* gate, cudaStream_t st) {
+  if (S.n) k_pairs64<<<(S.n + 255) / 256, 256, 0, st>>>(S, gate);
 }
-void launch_forces64(DevState const& S, cudaStream_t st) {
+void launch_step64(DevState const& S, int flags, cudaStream_t st) {
   if (!S.n) return;
-  if (S.any_convex) k_forces64<true><<<(S.n + 255) / 256, 256, 0, st>>>(S);
-  else k_forces64<false><<<(S.n + 255) / 256, 256, 0, st>>>(S);
+  if (S.any_convex) k_step64<true><<<(S.n + 255) / 256, 256, 0, st>>>(S, flags);
+  else k_step64<false><<<(S.n + 255) / 256, 256, 0, st>>>(S, flags);
 }
 
 }  // namespace gdem

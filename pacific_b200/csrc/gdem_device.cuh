@@ -7,17 +7,25 @@
 
 namespace gdem {
 
-constexpr unsigned long long kEmptyKey = 0xFFFFFFFFFFFFFFFFull;
-constexpr uint32_t kWallBit = 0x80000000u;
-
 // Contact-history table: open addressing with linear probing, keyed on the
-// unordered particle pair (lower ID in the high word) or on (particle, wall).
-// Values are stored as seen from the lower-ID body (or the particle, for a
-// wall); the other body's view is the negation, as in the reference where p1
-// holds (-kdelta, -normal, -spring) (HookeMemoryContactForceModel.cpp:191-192).
-// Two tables alternate: the one written during step n is read during step
-// n+1, so entries not touched in a step disappear, which is what
+// unordered particle pair or on (particle, wall).  Values are stored as seen
+// from the lower-ID body (or the particle, for a wall); the other body's view
+// is the negation, as in the reference where p1 holds (-kdelta, -normal,
+// -spring) (HookeMemoryContactForceModel.cpp:191-192).  Two tables
+// alternate: the one written by force evaluation e is read by evaluation
+// e + 1, so entries not touched in a step disappear, which is what
 // Component::updateContactMap (Component.cpp:583-595) does.
+//
+// Key layout: bits 54-63 the evaluation tag (e mod 1024), bits 27-53 the
+// lower particle ID, bits 0-26 the higher particle ID or, for a wall,
+// 2^27 - 1 - wall index.  A slot whose tag is not the current evaluation's is
+// free, so a table needs no clearing between uses; the host clears each
+// table once every 512 of its uses, before a tag value can come round again.
+constexpr int kTagShift = 54;
+constexpr unsigned kTagMask = 1023u;
+constexpr int kMaxIdBits = 27;
+constexpr unsigned long long kEmptyKey = 0xFFFFFFFFFFFFFFFFull;
+
 struct HistTable {
   unsigned long long* keys;
   void* vals;            // 9 values per slot (kdelta, prev normal, spring torque)
@@ -25,10 +33,17 @@ struct HistTable {
 };
 
 __host__ __device__ inline unsigned long long pairKey(int ida, int idb) {
-  return ((unsigned long long)(uint32_t)ida << 32) | (uint32_t)idb;
+  return ((unsigned long long)(uint32_t)ida << kMaxIdBits) | (uint32_t)idb;
 }
 __host__ __device__ inline unsigned long long wallKey(int id, int wall) {
-  return ((unsigned long long)(uint32_t)id << 32) | (kWallBit | (uint32_t)wall);
+  return ((unsigned long long)(uint32_t)id << kMaxIdBits) |
+         (uint32_t)((1 << kMaxIdBits) - 1 - wall);
+}
+__host__ __device__ inline unsigned long long tagged(unsigned long long base, unsigned tag) {
+  return ((unsigned long long)(tag & kTagMask) << kTagShift) | base;
+}
+__host__ __device__ inline unsigned tagOf(unsigned long long key) {
+  return (unsigned)(key >> kTagShift);
 }
 __host__ __device__ inline uint32_t hashSlot(unsigned long long k, int log2cap) {
   k ^= k >> 33;
@@ -38,25 +53,36 @@ __host__ __device__ inline uint32_t hashSlot(unsigned long long k, int log2cap) 
   k ^= k >> 33;
   return (uint32_t)(k & ((1ull << log2cap) - 1));
 }
-// Returns the slot holding key, or -1.
-__device__ inline int histFind(HistTable const& t, unsigned long long key) {
-  uint32_t mask = (1u << t.log2cap) - 1;
-  uint32_t s = hashSlot(key, t.log2cap);
+// Slot holding base with tag, or -1.
+__device__ inline int histFind(HistTable const& t, unsigned long long base, unsigned tag) {
+  const uint32_t mask = (1u << t.log2cap) - 1;
+  const unsigned long long key = tagged(base, tag);
+  uint32_t s = hashSlot(base, t.log2cap);
   for (uint32_t probe = 0; probe <= mask; ++probe) {
-    unsigned long long k = t.keys[s];
+    const unsigned long long k = t.keys[s];
     if (k == key) return (int)s;
-    if (k == kEmptyKey) return -1;
+    if (tagOf(k) != (tag & kTagMask)) return -1;
     s = (s + 1) & mask;
   }
   return -1;
 }
-// Claims a slot for key (one writer per key); -1 when the table is full.
-__device__ inline int histInsert(HistTable const& t, unsigned long long key) {
-  uint32_t mask = (1u << t.log2cap) - 1;
-  uint32_t s = hashSlot(key, t.log2cap);
+// Claims a slot for base with tag (one writer per key and evaluation); -1
+// when every slot carries the tag already (table full).
+__device__ inline int histInsert(HistTable const& t, unsigned long long base, unsigned tag) {
+  const uint32_t mask = (1u << t.log2cap) - 1;
+  const unsigned long long key = tagged(base, tag);
+  uint32_t s = hashSlot(base, t.log2cap);
   for (uint32_t probe = 0; probe <= mask; ++probe) {
-    unsigned long long prev = atomicCAS(&t.keys[s], kEmptyKey, key);
-    if (prev == kEmptyKey || prev == key) return (int)s;
+    unsigned long long cur = t.keys[s];
+    for (;;) {
+      if (tagOf(cur) == (tag & kTagMask)) {
+        if (cur == key) return (int)s;
+        break;                                   // taken this evaluation
+      }
+      const unsigned long long prev = atomicCAS(&t.keys[s], cur, key);
+      if (prev == cur) return (int)s;
+      cur = prev;                                // raced: look again
+    }
     s = (s + 1) & mask;
   }
   return -1;
@@ -68,15 +94,21 @@ __device__ inline int histInsert(HistTable const& t, unsigned long long key) {
 struct DevState {
   int n;                  // particles
   int cap;                // allocated particles (component stride)
-  int ncells;             // total cell keys of all instances
+  int ncells;             // total cell keys of all instances (pair-list grids)
   int ninst;
   double dt;
-  int* id; int* type; int* inst; int* key;
+  int* id; int* type; int* inst;
   double* x; double* v; double* w; double* wbf; double* q; double* F; double* T;
   double* basis;          // 9 per particle, non-spherical shapes only
-  // permutation targets (swapped with the above after each binning)
+  // second buffers: a step reads x, v, w, w_bf, q, basis and writes x2 ...;
+  // a pair-list rebuild permutes everything into them and copies back
   int* id2; int* type2; int* inst2;
   double* x2; double* v2; double* w2; double* wbf2; double* q2; double* basis2;
+  double* F2; double* T2;
+  // pair-list validity: displacement since the last rebuild (FP32, SoA) and
+  // periodic wraps since then (signed bytes x, y, z)
+  float* disp; int* wrap; int* wrap2;
+  int* ctl;               // control words (CtlWords)
   // binning
   int* skey;              // cell key in the old order
   int* rank;              // arrival rank within the cell
@@ -87,7 +119,7 @@ struct DevState {
   double4* vel64;         // v, mass
   double4* omg64;         // w (space frame), equivalent radius
   float4* offh;           // FP32 cell-relative offset; FP32 radius
-  int4* cellc;            // cell i, j, k and instance
+  int4* cellc;            // pair-list cell i, j, k and instance at the last rebuild
   // pair list: per-particle segments of kPairCap entries
   int* pairs; int* npairs;
   double* pair_delta;     // diagnostics: overlap of each entry (+inf: no contact)
@@ -98,7 +130,9 @@ struct DevState {
   int diag;
   HistTable hist_old, hist_new;
   int* status;
-  GridDesc const* grids; TypeDesc const* types; ModelDesc const* models;
+  GridDesc const* grids;  // reference linked-cell grids (cell reports, periodic wrap)
+  GridDesc const* bgrids; // pair-list grids: cells at least 2 rmax + skin wide
+  TypeDesc const* types; ModelDesc const* models;
   WallDesc const* walls;
   const double* poly_verts;   // polyhedron vertices of all classes (x, y, z)
   int max_walls;          // walls of the largest instance

@@ -66,7 +66,8 @@ int nextPow2Log(size_t n) {
 
 // ----------------------------------------------------------- XML import --
 struct InstanceDesc {
-  GridDesc grid;
+  GridDesc grid;        // the reference linked-cell grid
+  GridDesc bgrid;       // the pair-list grid: cells of at least 2 rmax f + skin
   std::vector<TypeDesc> types;
   std::vector<WallDesc> walls;
   std::vector<double> poly_verts;   // polyhedron vertices of this instance (x, y, z)
@@ -413,6 +414,35 @@ InstanceDesc readInstance(std::string const& path) {
     }
     g.edge_f[d] = (float)g.edge[d];
   }
+  // Pair-list grid.  The list holds the pairs whose bounding spheres are
+  // closer than the skin and stays valid while no particle has moved more
+  // than skin / 2, so its cells must be at least 2 rmax f + skin wide.  The
+  // skin defaults to a quarter of the largest circumscribed radius (the
+  // LinkedCell attribute Skin, a length, overrides it; 0 rebuilds the list
+  // every step); it shrinks when a periodic direction would get fewer than 3
+  // cells.
+  double skin = lc->has("Skin") ? lc->attrD("Skin") : 0.25 * maxR;
+  if (!(skin >= 0.)) throw std::runtime_error("LinkedCell Skin must be >= 0");
+  for (int d = 0; d < 3; ++d)
+    if (per[d]) skin = std::min(skin, std::max(0., (maxc[d] - org[d]) / 3. - cellsize) * 0.999999);
+  GridDesc& b = I.bgrid;
+  b = g;
+  for (int d = 0; d < 3; ++d) {
+    double size = maxc[d] - org[d];
+    int n = (int)((size + 1.0e-10) / (cellsize + skin));
+    if (!n) n = 1;
+    if (per[d] && n < 3) n = 3;
+    b.nb[d] = n;
+    b.edge[d] = size / n;
+    b.lc_origin[d] = org[d];
+    if (per[d]) {
+      b.lc_origin[d] += -b.edge[d];
+      b.nb[d] += 2;
+    }
+    b.edge_f[d] = (float)b.edge[d];
+  }
+  b.skin = skin;
+  b.skin_f = (float)skin;
   return I;
 }
 
@@ -427,15 +457,17 @@ struct System {
   GridDesc* d_grids = nullptr; TypeDesc* d_types = nullptr; ModelDesc* d_models = nullptr;
   WallDesc* d_walls = nullptr;
   double* d_poly = nullptr;        // polyhedron vertex table of all instances
+  GridDesc* d_bgrids = nullptr;    // pair-list grids
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool have_state = false, started = false, diag = false, use_graphs = true;
   bool id_order = false;           // state arrays are in particle-ID order (not yet binned)
   double last_ms = 0.;
   int status_host = 0;
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};
-  long parity = 0;                 // buffer swaps so far (state and history swap together)
-  long graph_parity = 0;           // parity at which graph[0] was captured
+  cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  long parity = 0;                 // force evaluations so far (state and history swap together)
+  long epoch = 0;                  // host copy of the evaluation counter (history tags)
+  bool graph_conditional = false;  // the graphs rebuild through a conditional node
   std::vector<void*> allocs;
   double* d_stage = nullptr;       // AoS staging, ID order (x v w wbf q F T: 22 doubles/particle)
   int* d_type_id = nullptr;        // particle class by ID
@@ -452,7 +484,8 @@ struct System {
 
   ~System() { release(); }
   void release() {
-    for (auto& gx : graph) if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
+    for (auto& row : graph)
+      for (auto& gx : row) if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
     for (void* p : allocs) cudaFree(p);
     allocs.clear();
     if (d_grids) cudaFree(d_grids);
@@ -460,6 +493,8 @@ struct System {
     if (d_models) cudaFree(d_models);
     if (d_walls) cudaFree(d_walls);
     if (d_poly) cudaFree(d_poly);
+    if (d_bgrids) cudaFree(d_bgrids);
+    d_bgrids = nullptr;
     d_grids = nullptr; d_types = nullptr; d_models = nullptr; d_walls = nullptr; d_poly = nullptr;
     for (auto& e : evpool) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
     evpool.clear();
@@ -476,7 +511,8 @@ struct System {
     return p;
   }
   void invalidateGraphs() {
-    for (auto& gx : graph) if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
+    for (auto& row : graph)
+      for (auto& gx : row) if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
   }
 
   // Runs f between two events when profiling (plain launches only).
@@ -519,13 +555,22 @@ struct System {
     std::vector<double> poly;
     int cell_offset = 0, max_walls = 1;
     S.any_convex = 0;
+    std::vector<GridDesc> bgrids;
+    int ref_cells = 0;
     for (auto& I : inst) {
       GridDesc g = I.grid;
-      g.cell_offset = cell_offset;
-      cell_offset += g.nb[0] * g.nb[1] * g.nb[2];
+      g.cell_offset = ref_cells;
+      ref_cells += g.nb[0] * g.nb[1] * g.nb[2];
       g.wall_begin = (int)walls.size();
       g.wall_count = (int)I.walls.size();
       g.model_base = (int)models.size();
+      GridDesc b = I.bgrid;
+      b.cell_offset = cell_offset;
+      cell_offset += b.nb[0] * b.nb[1] * b.nb[2];
+      b.wall_begin = g.wall_begin;
+      b.wall_count = g.wall_count;
+      b.model_base = g.model_base;
+      bgrids.push_back(b);
       type_base.push_back((int)types.size());
       const int vbase = (int)poly.size() / 3;
       for (auto const& t : I.types) {
@@ -551,8 +596,9 @@ struct System {
       if (!vec.empty()) CK(cudaMemcpy(dst, vec.data(), vec.size() * sizeof(T), cudaMemcpyHostToDevice));
     };
     up(d_grids, grids); up(d_types, types); up(d_models, models); up(d_walls, walls);
-    up(d_poly, poly);
+    up(d_poly, poly); up(d_bgrids, bgrids);
     S.grids = d_grids; S.types = d_types; S.models = d_models; S.walls = d_walls;
+    S.bgrids = d_bgrids;
     S.poly_verts = d_poly;
   }
 
@@ -560,13 +606,18 @@ struct System {
     S.n = n;
     S.cap = std::max(n, 1);
     size_t c = (size_t)S.cap;
-    S.id = alloc<int>(c); S.type = alloc<int>(c); S.inst = alloc<int>(c); S.key = alloc<int>(c);
+    S.id = alloc<int>(c); S.type = alloc<int>(c); S.inst = alloc<int>(c);
     S.id2 = alloc<int>(c); S.type2 = alloc<int>(c); S.inst2 = alloc<int>(c);
     S.x = alloc<double>(3 * c); S.v = alloc<double>(3 * c); S.w = alloc<double>(3 * c);
     S.wbf = alloc<double>(3 * c); S.q = alloc<double>(4 * c);
     S.x2 = alloc<double>(3 * c); S.v2 = alloc<double>(3 * c); S.w2 = alloc<double>(3 * c);
     S.wbf2 = alloc<double>(3 * c); S.q2 = alloc<double>(4 * c);
     S.F = alloc<double>(3 * c); S.T = alloc<double>(3 * c);
+    S.F2 = alloc<double>(3 * c); S.T2 = alloc<double>(3 * c);
+    S.disp = alloc<float>(3 * c); S.wrap = alloc<int>(c); S.wrap2 = alloc<int>(c);
+    S.ctl = alloc<int>(kCtlWords);
+    CK(cudaMemset(S.ctl, 0, kCtlWords * sizeof(int)));
+    epoch = 0;
     // orientation matrices, SoA (9 x cap), only when some class is not a sphere
     S.basis = S.any_convex ? alloc<double>(9 * c) : nullptr;
     S.basis2 = S.any_convex ? alloc<double>(9 * c) : nullptr;
@@ -575,11 +626,11 @@ struct System {
     S.scan_tmp = alloc<int>((S.ncells + 1023) / 1024 + 1);
     S.cellc = alloc<int4>(c);
     if (precision == GDEM_FP64) {
-      S.pos64 = alloc<double4>(c); S.vel64 = alloc<double4>(c); S.omg64 = alloc<double4>(c);
+      S.pos64 = alloc<double4>(c);
       S.offh = nullptr;
     } else {
       S.offh = alloc<float4>(c);
-      S.pos64 = nullptr; S.vel64 = nullptr; S.omg64 = nullptr;
+      S.pos64 = nullptr;
     }
     S.pairs = alloc<int>(c * kPairCap); S.npairs = alloc<int>(c);
     S.pair_delta = nullptr; S.wall_delta = nullptr; S.diag = 0;
@@ -591,6 +642,7 @@ struct System {
       t->log2cap = l2;
       t->keys = alloc<unsigned long long>(hc);
       t->vals = alloc<char>(hc * 9 * vsz);
+      // all-ones keys: tag 1023, which the first 512 uses of a table never carry
       CK(cudaMemset(t->keys, 0xFF, hc * sizeof(unsigned long long)));
     }
     S.status = alloc<int>(1);
@@ -620,91 +672,155 @@ struct System {
     launch_load_state(S, dx, dv, dw, wbf ? dwb : nullptr, dq, F ? dF : nullptr, T ? dT : nullptr,
                       d_type_id, d_inst_id, stream);
     CK(cudaGetLastError());
+    // the pair list no longer describes this state: rebuild before the next
+    // force evaluation
+    const int one = 1;
+    CK(cudaMemcpyAsync(S.ctl + kCtlNeed, &one, sizeof(int), cudaMemcpyHostToDevice, stream));
     CK(cudaStreamSynchronize(stream));
     id_order = true;
   }
 
-  void swapState() {
-    std::swap(S.id, S.id2); std::swap(S.type, S.type2); std::swap(S.inst, S.inst2);
+  // A force evaluation reads x, v, w, w_bf, q, basis, wraps and writes the
+  // second buffers; the contact-history tables alternate with it, so both
+  // parities advance together.
+  void swapDyn() {
     std::swap(S.x, S.x2); std::swap(S.v, S.v2); std::swap(S.w, S.w2);
     std::swap(S.wbf, S.wbf2); std::swap(S.q, S.q2); std::swap(S.basis, S.basis2);
+    std::swap(S.wrap, S.wrap2);
   }
   void swapHist() { std::swap(S.hist_old, S.hist_new); }
-  void swapBoth() { swapState(); swapHist(); ++parity; }
 
-  // Sort into cell order (after k_key or k_bin), moving on the way when
-  // moving != 0, and build the pair list.
-  void binAndPairs(int moving, bool pre_kick) {
-    double dt = S.dt;
-    id_order = false;
-    timed("scan", [&] { launch_scan(S, stream); });
-    timed("place", [&] { launch_place(S, stream); });
-    timed("cellsort", [&] { launch_cellsort(S, stream); });
-    timed("move_gather", [&] {
-      launch_move_gather(S, moving, 0.5 * dt, dt, pre_kick ? 1 : 0, 0.5 * dt, stream);
-    });
-    swapState();
-    ++parity;
-    if (precision == GDEM_FP64) timed("pairs64", [&] { launch_pairs64(S, stream); });
-    else timed("pairs32", [&] { launch_pairs32(S, stream); });
-  }
-  void forces() {
+  // The table that evaluation e (1-based) writes is refilled every 512 of its
+  // uses with the tag e - 1, which none of its next 512 uses carries.
+  void maybeClearHistory(long e) {
+    if ((e % 512) >= 2) return;
     size_t hc = size_t(1) << S.hist_new.log2cap;
-    timed("hist_clear", [&] {
-      CK(cudaMemsetAsync(S.hist_new.keys, 0xFF, hc * sizeof(unsigned long long), stream));
-    });
-    if (precision == GDEM_FP64) timed("forces64", [&] { launch_forces64(S, stream); });
-    else timed("forces32", [&] { launch_forces32(S, stream); });
+    unsigned long long v = tagged((1ull << kTagShift) - 1, (unsigned)(e - 1));
+    timed("hist_fill", [&] { launch_fill64(S.hist_new.keys, hc, v, stream); });
+  }
+
+  // Pair-list rebuild: cells, counting sort, permutation into cell order,
+  // pair search.  gate: the control word that tells gated kernels whether
+  // this step rebuilds (plain launches), or null inside the graph's
+  // conditional node.
+  void rebuild(const int* gate) {
+    id_order = false;
+    timed("bin", [&] { launch_bin(S, gate, stream); });
+    timed("scan", [&] { launch_scan(S, gate, stream); });
+    timed("place", [&] { launch_place(S, gate, stream); });
+    timed("cellsort", [&] { launch_cellsort(S, gate, stream); });
+    timed("permute", [&] { launch_permute(S, gate, stream); });
+    timed("copyback", [&] { launch_copyback(S, gate, stream); });
+    if (precision == GDEM_FP64) timed("pairs64", [&] { launch_pairs64(S, gate, stream); });
+    else timed("pairs32", [&] { launch_pairs32(S, gate, stream); });
+  }
+  void stepKernel(int flags) {
+    if (precision == GDEM_FP64) timed("step64", [&] { launch_step64(S, flags, stream); });
+    else timed("step32", [&] { launch_step32(S, flags, stream); });
+  }
+  // One force evaluation with plain launches: decide, gated rebuild, step.
+  void evaluate(int flags) {
+    maybeClearHistory(epoch + 1);
+    timed("decide", [&] { launch_decide(S, cudaGraphConditionalHandle(), 0, stream); });
+    rebuild(S.ctl + kCtlActive);
+    stepKernel(flags);
+    ++epoch;
+    swapDyn();
     swapHist();
   }
-  // One full step; pre_kick applies the previous step's closing kick first.
-  void stepBody(bool pre_kick) {
-    double dt = S.dt;
-    // cell_count is zero here: k_cellsort of the previous binning reset it
-    timed("key", [&] { launch_key(S, 0.5 * dt, dt, pre_kick ? 1 : 0, 0.5 * dt, stream); });
-    binAndPairs(1, pre_kick);
-    forces();
+
+  // The same evaluation as one graph: decide -> conditional node holding the
+  // rebuild -> step kernel.  If the conditional node cannot be built, the
+  // graph holds the gated rebuild instead.
+  cudaGraphExec_t captureEvaluation(int flags) {
+    cudaGraph_t g = nullptr;
+    CK(cudaGraphCreate(&g, 0));
+    bool conditional = true;
+    cudaGraphConditionalHandle h{};
+    if (cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) {
+      cudaGetLastError();
+      conditional = false;
+    }
+    CK(cudaStreamBeginCaptureToGraph(stream, g, nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal));
+    launch_decide(S, h, conditional ? 1 : 0, stream);
+    CK(cudaStreamEndCapture(stream, &g));
+    cudaGraphNode_t decide_node = nullptr;
+    size_t nn = 1;
+    CK(cudaGraphGetNodes(g, &decide_node, &nn));
+    cudaGraphNode_t tail = decide_node;
+    if (conditional) {
+      cudaGraphNodeParams cp{};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeIf;
+      cp.conditional.size = 1;
+      cudaGraphNode_t cond = nullptr;
+      if (cudaGraphAddNode(&cond, g, &decide_node, 1, &cp) == cudaSuccess) {
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        CK(cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeThreadLocal));
+        rebuild(nullptr);
+        CK(cudaStreamEndCapture(stream, &body));
+        tail = cond;
+      } else {
+        cudaGetLastError();
+        conditional = false;
+      }
+    }
+    CK(cudaStreamBeginCaptureToGraph(stream, g, &tail, nullptr, 1,
+                                     cudaStreamCaptureModeThreadLocal));
+    if (!conditional) rebuild(S.ctl + kCtlActive);
+    stepKernel(flags);
+    CK(cudaStreamEndCapture(stream, &g));
+    cudaGraphExec_t ex = nullptr;
+    CK(cudaGraphInstantiate(&ex, g, 0));
+    CK(cudaGraphDestroy(g));
+    graph_conditional = conditional;
+    return ex;
   }
+  // Graph of evaluation kind k (0: inside a call, 1: last of a call) for the
+  // current buffer parity; built on first use.
+  void launchEvaluation(int k, int flags) {
+    maybeClearHistory(epoch + 1);
+    const int par = (int)(parity & 1);
+    if (!graph[k][par]) graph[k][par] = captureEvaluation(flags);
+    CK(cudaGraphLaunch(graph[k][par], stream));
+    ++epoch;
+    ++parity;
+    swapDyn();
+    swapHist();
+  }
+
   void init() {
-    CK(cudaMemsetAsync(S.cell_count, 0, (size_t)S.ncells * sizeof(int), stream));
-    launch_bin(S, stream);
-    binAndPairs(0, false);
-    forces();
-    launch_hist_zero_cumulative(S.hist_old, precision == GDEM_FP64, stream);
+    id_order = false;
+    evaluate(kStepForces | kStepStoreFT);
+    ++parity;
+    launch_hist_zero_cumulative(S.hist_old, S.ctl, precision == GDEM_FP64, stream);
     CK(cudaStreamSynchronize(stream));
     collectTimes();
     started = true;
   }
-  void captureGraphs() {
-    invalidateGraphs();
-    for (int k = 0; k < 2; ++k) {
-      cudaGraph_t gph;
-      CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-      stepBody(true);
-      CK(cudaStreamEndCapture(stream, &gph));
-      CK(cudaGraphInstantiate(&graph[k], gph, 0));
-      CK(cudaGraphDestroy(gph));
-    }
-    // capturing advanced the host-side buffer parity by two: back where it was
-    graph_parity = parity - 2;
-  }
+  // nsteps leapfrog steps: the opening kick and drift of the first (with the
+  // stored forces), then per step a force evaluation followed by the closing
+  // kick and -- except after the last -- the next opening kick and drift.
   void step(int nsteps) {
     if (nsteps <= 0) return;
+    id_order = false;
     CK(cudaEventRecord(ev0, stream));
-    stepBody(false);
-    int rest = nsteps - 1;
-    if (rest > 0) {
-      if (use_graphs && !diag && !profiling) {
-        if (!graph[0]) captureGraphs();
-        int g = (int)((parity - graph_parity) & 1);
-        for (int k = 0; k < rest; ++k) { CK(cudaGraphLaunch(graph[g], stream)); g ^= 1; }
-        if (rest & 1) { swapBoth(); parity += rest - 1; }
-        else parity += rest;
+    timed("move_only", [&] { launch_move_only(S, stream); });
+    const int mid = kStepForces | kStepClose | kStepMove;
+    const int last = kStepForces | kStepClose | kStepStoreFT;
+    const bool graphs = use_graphs && !diag && !profiling;
+    for (int k = 0; k < nsteps; ++k) {
+      const bool is_last = k == nsteps - 1;
+      if (graphs) {
+        launchEvaluation(is_last ? 1 : 0, is_last ? last : mid);
       } else {
-        for (int k = 0; k < rest; ++k) stepBody(true);
+        evaluate(is_last ? last : mid);
+        ++parity;
       }
     }
-    timed("kick", [&] { launch_kick(S, 0.5 * S.dt, stream); });
     CK(cudaEventRecord(ev1, stream));
     CK(cudaGetLastError());
     CK(cudaEventSynchronize(ev1));
@@ -778,8 +894,9 @@ int gdem_upload_state(gdem_handle h, int64_t n, const int* inst, const int* type
                       const double* q) {
   return guarded([&] {
     System* s = sys(h);
-    if (!s || n <= 0 || n >= (int64_t(1) << 27) || !type || !x || !v || !w || !q)
-      throw std::runtime_error("invalid arguments");
+    if (!s || n <= 0 || !type || !x || !v || !w || !q) throw std::runtime_error("invalid arguments");
+    if (n > (int64_t(1) << kMaxIdBits) - 64)
+      throw std::runtime_error("too many particles for the 27-bit particle IDs of the contact keys");
     if (s->have_state) throw std::runtime_error("state already uploaded");
     int N = (int)n;
     std::vector<int> hinst(N, 0), htype(N), hid(N);
@@ -872,6 +989,19 @@ int gdem_pair_counts(gdem_handle h, int64_t* entries, int64_t* contacts) {
   });
 }
 
+int gdem_step_counts(gdem_handle h, int64_t* evaluations, int64_t* rebuilds) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state) throw std::runtime_error("no state");
+    int r[kCtlWords];
+    CK(cudaStreamSynchronize(s->stream));
+    CK(cudaMemcpy(r, s->S.ctl, sizeof(r), cudaMemcpyDeviceToHost));
+    if (evaluations) *evaluations = r[kCtlEpoch];
+    if (rebuilds) *rebuilds = r[kCtlRebuilds];
+    return GDEM_OK;
+  });
+}
+
 int gdem_law_counts(gdem_handle h, int64_t* evaluated, int64_t* reevaluated, int reset) {
   return guarded([&] {
     System* s = sys(h);
@@ -922,7 +1052,12 @@ int gdem_upload_history(gdem_handle h, int64_t n, const int* owner, const int* p
     DevState& S = s->S;
     HistTable& t = S.hist_old;   // read by the next force evaluation
     size_t hc = size_t(1) << t.log2cap;
-    std::vector<unsigned long long> keys(hc, kEmptyKey);
+    // the next evaluation (epoch + 1) looks up tag epoch; the free slots get
+    // tag epoch - 1, which this table's next uses (tags epoch + 2, + 4, ...)
+    // never carry
+    const unsigned tag = (unsigned)s->epoch;
+    const unsigned long long empty = tagged((1ull << kTagShift) - 1, tag - 1u);
+    std::vector<unsigned long long> keys(hc, empty);
     bool fp64 = s->precision == GDEM_FP64;
     std::vector<double> vd(fp64 ? 9 * hc : 0);
     std::vector<float> vf(fp64 ? 0 : 9 * hc);
@@ -936,8 +1071,8 @@ int gdem_upload_history(gdem_handle h, int64_t n, const int* owner, const int* p
         key = wallKey(a, -b - 2);
       }
       uint32_t slot = hashSlot(key, t.log2cap);
-      while (keys[slot] != kEmptyKey) slot = (slot + 1) & (uint32_t)(hc - 1);
-      keys[slot] = key;
+      while (keys[slot] != empty) slot = (slot + 1) & (uint32_t)(hc - 1);
+      keys[slot] = tagged(key, tag);
       double vals[9] = {kdelta[3 * e], kdelta[3 * e + 1], kdelta[3 * e + 2],
                         prevn[3 * e], prevn[3 * e + 1], prevn[3 * e + 2],
                         spring ? spring[3 * e] : 0., spring ? spring[3 * e + 1] : 0.,

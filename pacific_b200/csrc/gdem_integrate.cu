@@ -1,147 +1,75 @@
-// gdem_integrate.cu -- leapfrog kick/drift and linked-cell binning kernels.
+// gdem_integrate.cu -- leapfrog move and pair-list rebuild kernels.
 //
 // Compiled with -fmad=false: positions, velocities and cell indices are FP64
 // and follow the reference's expression order, so cell assignments are
 // bit-identical to Cell::GetCell on the same state.
 //
-//   k_key       post-move cell of each particle (Cell::GetCell, Base/src/
-//               Cell.cpp:172-184; SimulationError when outside the grid,
-//               Base/src/LinkedCell.cpp:1506-1531) and the cell histogram of
-//               the counting-sort binning.
+// A step is (host side, gdem_host.cu): k_decide, then -- only when some
+// particle has moved more than half the pair-list skin since the last
+// rebuild -- the rebuild below, then one fused force + leapfrog kernel
+// (gdem_contact64.cu / gdem_contact32.cu).
+//
+//   k_decide    turns the rebuild request of the previous step into this
+//               step's decision (and the CUDA-graph condition), and counts
+//               the force evaluation (contact-history tag).
+//   k_bin       pair-list cell of each particle and the cell histogram.
 //   scan/place/cellsort
 //               counting sort of particles on their cell key: a one-digit
 //               radix sort whose digit is the cell key, made stable by
 //               ordering each cell's entries by particle ID; it yields the
 //               cell start/end tables.
-//   k_move_gather
-//               SecondOrderLeapFrog::Move + ParticleKinematics::Move
-//               (TimeIntegration/src/SecondOrderLeapFrog.cpp:44-67,
-//                Component/src/ParticleKinematics.cpp:62-104) and MotionError
-//               (Component/src/Particle.cpp:446-456), applied while the state
-//               is permuted into cell order, so the state is read and written
-//               once per step.
-//   k_kick      advanceVelocity (SecondOrderLeapFrog.cpp:74-94,
-//               ParticleKinematics.cpp:110-128).
+//   k_permute / k_copyback
+//               the whole state into cell order (through the second
+//               buffers), with the compact copies the pair search reads.
+//   k_move_only the opening kick and drift of the first step of a call
+//               (SecondOrderLeapFrog::Move, ParticleKinematics::Move).
+// Rebuild kernels take a gate: with a non-null gate they return at once
+// unless this step rebuilds (plain launches); inside the graph's conditional
+// node they run ungated.
 #include "gdem_kernels.cuh"
+#include "gdem_motion.cuh"
 
 namespace gdem {
 
 namespace {
 
-// ParticleKinematicsSphere / ParticleKinematics3D angular acceleration
-// (ParticleKinematicsSphere.cpp:47-55, ParticleKinematics3D.cpp:56-77, with
-// the predictor-mode gyroscopic term).
-__device__ __forceinline__ d3 dOmega(TypeDesc const& t, d3 tbf, d3 om) {
-  const double c = 1.;
-  if (t.shape == 0)
-    return mk(tbf.x / (c * t.inertia[0]), tbf.y / (c * t.inertia[1]), tbf.z / (c * t.inertia[2]));
-  const double* I = t.inertia;
-  return mk(tbf.x / (c * I[0]) + om.y * om.z * (I[1] - I[2]) / I[0],
-            tbf.y / (c * I[1]) + om.z * om.x * (I[2] - I[0]) / I[1],
-            tbf.z / (c * I[2]) + om.x * om.y * (I[0] - I[1]) / I[2]);
+__device__ __forceinline__ bool gatedOff(const int* gate) { return gate && !*gate; }
+
+__global__ void k_decide(DevState S, cudaGraphConditionalHandle h, int use_handle) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int need = S.ctl[kCtlNeed];
+  S.ctl[kCtlActive] = need;
+  S.ctl[kCtlNeed] = 0;
+  S.ctl[kCtlEpoch] += 1;
+  S.ctl[kCtlRebuilds] += need ? 1 : 0;
+  if (use_handle) cudaGraphSetConditional(h, need ? 1u : 0u);
 }
 
-// SSP-RK3 update of the body-fixed angular velocity over h.  For a sphere
-// the acceleration does not depend on omega, so K1 = K2 = K3 and one
-// evaluation gives the same bits as three.
-__device__ __forceinline__ d3 rk3(TypeDesc const& t, d3 tbf, d3 wbf, double h) {
-  if (t.shape == 0) {
-    d3 K = dOmega(t, tbf, wbf);
-    K = K * h;
-    return wbf + ((K + K) + 4. * K) / 6.;
-  }
-  d3 K1 = dOmega(t, tbf, wbf);
-  K1 = K1 * h;
-  d3 K2 = dOmega(t, tbf, wbf + K1);
-  K2 = K2 * h;
-  d3 K3 = dOmega(t, tbf, wbf + 0.25 * (K1 + K2));
-  K3 = K3 * h;
-  return wbf + ((K1 + K2) + 4. * K3) / 6.;
-}
-
-__device__ __forceinline__ void kick(TypeDesc const& tp, d3 F, d3 T, d3& v, d3& wbf, d3& w,
-                                     dq q, double h) {
-  dq pc = conj(q);
-  d3 tbf = multToVector3(pc, vecq(T, q));
-  const double c = 1.;
-  v = v + (F / (tp.mass * c)) * h;
-  wbf = rk3(tp, tbf, wbf, h);
-  w = multToVector3(q, vecq(wbf, pc));
-}
-
-// Cell of a position after the periodic wrap: a master leaving the inner
-// cells is replaced by its image (x is updated).  Cell::GetCell.
-__device__ __forceinline__ void cellOf(GridDesc const& g, d3& x, int* id) {
-  double xs[3] = {x.x, x.y, x.z};
+// Pair-list cell key of x (clamped into the grid; outside it raises
+// kErrOutOfGrid like the reference's SimulationError).
+__device__ __forceinline__ int buildKey(GridDesc const& bg, d3 x, int* status) {
+  const double xs[3] = {x.x, x.y, x.z};
+  int id[3];
+  bool valid = true;
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    id[d] = (int)floor((xs[d] - g.lc_origin[d]) / g.edge[d]);
-    if (g.periodic[d]) {
-      if (id[d] < 1) xs[d] = xs[d] + g.L[d];
-      else if (id[d] > g.nb[d] - 2) xs[d] = xs[d] + (-g.L[d]);
-      id[d] = (int)floor((xs[d] - g.lc_origin[d]) / g.edge[d]);
+    id[d] = (int)floor((xs[d] - bg.lc_origin[d]) / bg.edge[d]);
+    if (id[d] < 0 || id[d] >= bg.nb[d]) {
+      valid = false;
+      id[d] = min(max(id[d], 0), bg.nb[d] - 1);
     }
   }
-  x = mk(xs[0], xs[1], xs[2]);
+  if (!valid) raise(status, kErrOutOfGrid);
+  return bg.cell_offset + id[1] * bg.nb[2] * bg.nb[0] + id[2] * bg.nb[0] + id[0];
 }
 
-__device__ __forceinline__ int keyOf(GridDesc const& g, int* id, int* status) {
-  bool valid = id[0] >= 0 && id[0] < g.nb[0] && id[1] >= 0 && id[1] < g.nb[1] &&
-               id[2] >= 0 && id[2] < g.nb[2];
-  if (!valid) {
-    raise(status, kErrOutOfGrid);
-    id[0] = min(max(id[0], 0), g.nb[0] - 1);
-    id[1] = min(max(id[1], 0), g.nb[1] - 1);
-    id[2] = min(max(id[2], 0), g.nb[2] - 1);
-  }
-  return g.cell_offset + id[1] * g.nb[2] * g.nb[0] + id[2] * g.nb[0] + id[0];
-}
-
-// First binning pass: the cell each particle will occupy after this step's
-// kick + drift.  Evaluates exactly the translational part of k_move_gather
-// (same expressions, same order), so both passes agree bit for bit.
-__global__ void k_key(DevState S, double h, double dt, int pre_kick, double pre_h) {
+__global__ void k_bin(DevState S, const int* gate) {
+  if (gatedOff(gate)) return;
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= S.n) return;
-  const int cap = S.cap;
-  const double mass = S.types[S.type[s]].mass;
-  GridDesc const& g = S.grids[S.inst[s]];
-  const d3 F = ld3(S.F, cap, s);
-  d3 v = ld3(S.v, cap, s), x = ld3(S.x, cap, s);
-  const double c = 1.;
-  if (pre_kick) v = v + (F / (mass * c)) * pre_h;
-  v = v + (F / (mass * c)) * h;
-  x = x + v * dt;
-  int id[3];
-  cellOf(g, x, id);
-  int key = keyOf(g, id, S.status);
+  const int key = buildKey(S.bgrids[S.inst[s]], ld3(S.x, S.cap, s), S.status);
   S.skey[s] = key;
   S.rank[s] = atomicAdd(&S.cell_count[key], 1);
-}
-
-// Binning without motion (initial linking, LinkedCell::Link).
-__global__ void k_bin(DevState S) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= S.n) return;
-  GridDesc const& g = S.grids[S.inst[s]];
-  int id[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) id[d] = (int)floor((S.x[d * S.cap + s] - g.lc_origin[d]) / g.edge[d]);
-  int key = keyOf(g, id, S.status);
-  S.skey[s] = key;
-  S.rank[s] = atomicAdd(&S.cell_count[key], 1);
-}
-
-__global__ void k_kick(DevState S, double h) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= S.n) return;
-  const int cap = S.cap;
-  TypeDesc const tp = S.types[S.type[s]];
-  d3 F = ld3(S.F, cap, s), T = ld3(S.T, cap, s);
-  d3 v = ld3(S.v, cap, s), wbf = ld3(S.wbf, cap, s), w;
-  dq q = qmk(mk(S.q[s], S.q[cap + s], S.q[2 * cap + s]), S.q[3 * cap + s]);
-  kick(tp, F, T, v, wbf, w, q, h);
-  st3(S.v, cap, s, v); st3(S.wbf, cap, s, wbf); st3(S.w, cap, s, w);
 }
 
 // ------------------------------------------------------------------ scan --
@@ -175,7 +103,8 @@ __device__ __forceinline__ int blockExclusiveScan(int v, int* smem, int& total) 
   return before + x - v;
 }
 
-__global__ void k_scan_tiles(const int* in, int* out, int* tile_sums, int n) {
+__global__ void k_scan_tiles(const int* in, int* out, int* tile_sums, int n, const int* gate) {
+  if (gatedOff(gate)) return;
   __shared__ int smem[32];
   int i = blockIdx.x * kScanTile + threadIdx.x;
   int v = i < n ? in[i] : 0;
@@ -186,7 +115,8 @@ __global__ void k_scan_tiles(const int* in, int* out, int* tile_sums, int n) {
 }
 
 // Scans the tile sums in place with one block, looping over chunks.
-__global__ void k_scan_sums(int* sums, int ntiles) {
+__global__ void k_scan_sums(int* sums, int ntiles, const int* gate) {
+  if (gatedOff(gate)) return;
   __shared__ int smem[32];
   int carry = 0;
   for (int base = 0; base < ntiles; base += kScanTile) {
@@ -202,7 +132,9 @@ __global__ void k_scan_sums(int* sums, int ntiles) {
 
 // Adds the tile offsets; out[n] receives the total so that cell c spans
 // [out[c], out[c + 1]).
-__global__ void k_scan_add(int* out, const int* tile_sums, const int* in, int n) {
+__global__ void k_scan_add(int* out, const int* tile_sums, const int* in, int n,
+                           const int* gate) {
+  if (gatedOff(gate)) return;
   int i = blockIdx.x * kScanTile + threadIdx.x;
   if (i < n) {
     int v = out[i] + tile_sums[blockIdx.x];
@@ -211,17 +143,19 @@ __global__ void k_scan_add(int* out, const int* tile_sums, const int* in, int n)
   }
 }
 
-__global__ void k_place(DevState S) {
+__global__ void k_place(DevState S, const int* gate) {
+  if (gatedOff(gate)) return;
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= S.n) return;
   S.order[S.cell_start[S.skey[s]] + S.rank[s]] = s;
 }
 
 // Orders each cell's entries by particle ID, so the permutation does not
-// depend on the arrival order of the atomic histogram.
-// It also resets the cell histogram for the next binning (every count has
-// been consumed by the scan at this point).
-__global__ void k_cellsort(DevState S) {
+// depend on the arrival order of the atomic histogram.  It also resets the
+// cell histogram for the next rebuild (every count has been consumed by the
+// scan at this point).
+__global__ void k_cellsort(DevState S, const int* gate) {
+  if (gatedOff(gate)) return;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= S.ncells) return;
   int b = S.cell_start[c];
@@ -240,93 +174,77 @@ __global__ void k_cellsort(DevState S) {
   }
 }
 
-// Second binning pass: permutes the state into cell order and, when moving,
-// applies the step's kick + drift on the way (ParticleKinematics::Move,
-// ParticleKinematics.cpp:62-104, with SecondOrderLeapFrog::Move,
-// SecondOrderLeapFrog.cpp:44-67), then builds the compact contact arrays.
-__global__ void k_move_gather(DevState S, int moving, double h, double dt, int pre_kick,
-                              double pre_h) {
+// Gathers the state into cell order (second buffers) and writes the compact
+// arrays of the pair search: the cell, the FP64 position + radius (FP64
+// mode) or the FP32 offset from the cell's lower corner + radius (FP32-split).
+__global__ void k_permute(DevState S, const int* gate) {
+  if (gatedOff(gate)) return;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
   const int cap = S.cap;
   const int s = S.order[t];
-  const int idv = S.id[s], ty = S.type[s], in = S.inst[s];
-  const int key = S.skey[s];
-  TypeDesc const& tp = S.types[ty];
-  GridDesc const& g = S.grids[in];
-  d3 x = ld3(S.x, cap, s), v = ld3(S.v, cap, s), wbf = ld3(S.wbf, cap, s), w;
-  dq q = qmk(mk(S.q[s], S.q[cap + s], S.q[2 * cap + s]), S.q[3 * cap + s]);
-  if (moving) {
-    const d3 F = ld3(S.F, cap, s), T = ld3(S.T, cap, s);
-    if (pre_kick) kick(tp, F, T, v, wbf, w, q, pre_h);
-    dq pc = conj(q);
-    d3 tbf = multToVector3(pc, vecq(T, q));
-    const double c = 1.;
-    v = v + (F / (tp.mass * c)) * h;
-    d3 dx = v * dt;
-    wbf = rk3(tp, tbf, wbf, h);
-    w = multToVector3(q, vecq(wbf, pc));
-    const d3 meanw = w;     // same expression as w (ParticleKinematics.cpp:79-82)
-    x = x + dx;
-    double nOm = norm(meanw);
-    dq qdt;
-    if (nOm > 1.0e-10) {
-      double cc, ss;
-      sincos(nOm * dt / 2., &ss, &cc);
-      qdt = qmk((ss * 1. / nOm) * meanw, cc);
-    } else {
-      qdt = qmk(mk(0., 0., 0.), 1.);
-    }
-    q = qmul(qdt, q);
-    if (S.basis) {
-      // Transform::composeLeftByRotation (Geometry/src/Transform.cpp:140-159)
-      double mm[9], out[9];
+  const int ty = S.type[s], in = S.inst[s];
+  S.id2[t] = S.id[s]; S.type2[t] = ty; S.inst2[t] = in;
+  const d3 x = ld3(S.x, cap, s);
+  st3(S.x2, cap, t, x);
+  st3(S.v2, cap, t, ld3(S.v, cap, s));
+  st3(S.w2, cap, t, ld3(S.w, cap, s));
+  st3(S.wbf2, cap, t, ld3(S.wbf, cap, s));
+  st3(S.F2, cap, t, ld3(S.F, cap, s));
+  st3(S.T2, cap, t, ld3(S.T, cap, s));
 #pragma unroll
-      for (int k = 0; k < 9; ++k) mm[k] = S.basis[k * cap + s];
-      double qx = qdt.v.x, qy = qdt.v.y, qz = qdt.v.z, qw = qdt.w;
+  for (int k = 0; k < 4; ++k) S.q2[k * cap + t] = S.q[k * cap + s];
+  if (S.basis) {
 #pragma unroll
-      for (int i = 0; i < 3; ++i) {
-        double px = qy * mm[6 + i] - qz * mm[3 + i] + qw * mm[0 + i];
-        double py = qz * mm[0 + i] - qx * mm[6 + i] + qw * mm[3 + i];
-        double pz = qx * mm[3 + i] - qy * mm[0 + i] + qw * mm[6 + i];
-        double pw = -qx * mm[0 + i] - qy * mm[3 + i] - qz * mm[6 + i];
-        out[0 + i] = qy * pz - qz * py - pw * qx + qw * px;
-        out[3 + i] = qz * px - qx * pz - pw * qy + qw * py;
-        out[6 + i] = qx * py - qy * px - pw * qz + qw * pz;
-      }
-#pragma unroll
-      for (int k = 0; k < 9; ++k) S.basis2[k * cap + t] = out[k];
-    }
-    if (norm(dx) > tp.crust) raise(S.status, kErrMotion);   // Particle.cpp:446-456
-    int id[3];
-    cellOf(g, x, id);
-  } else {
-    w = ld3(S.w, cap, s);
-    if (S.basis) {
-#pragma unroll
-      for (int k = 0; k < 9; ++k) S.basis2[k * cap + t] = S.basis[k * cap + s];
-    }
+    for (int k = 0; k < 9; ++k) S.basis2[k * cap + t] = S.basis[k * cap + s];
   }
-  S.id2[t] = idv; S.type2[t] = ty; S.inst2[t] = in;
-  S.key[t] = key;
-  st3(S.x2, cap, t, x); st3(S.v2, cap, t, v); st3(S.w2, cap, t, w); st3(S.wbf2, cap, t, wbf);
-  S.q2[t] = q.v.x; S.q2[cap + t] = q.v.y; S.q2[2 * cap + t] = q.v.z; S.q2[3 * cap + t] = q.w;
-  int c = key - g.cell_offset;
-  int ci = c % g.nb[0];
-  int ck = (c / g.nb[0]) % g.nb[2];
-  int cj = c / (g.nb[0] * g.nb[2]);
+  GridDesc const& bg = S.bgrids[in];
+  const int c = S.skey[s] - bg.cell_offset;
+  const int ci = c % bg.nb[0];
+  const int ck = (c / bg.nb[0]) % bg.nb[2];
+  const int cj = c / (bg.nb[0] * bg.nb[2]);
   S.cellc[t] = make_int4(ci, cj, ck, in);
-  if (S.pos64) {
-    S.pos64[t] = make_double4(x.x, x.y, x.z, tp.radius);
-    S.vel64[t] = make_double4(v.x, v.y, v.z, tp.mass);
-    S.omg64[t] = make_double4(w.x, w.y, w.z, tp.eqrad);
-  }
+  TypeDesc const& tp = S.types[ty];
+  if (S.pos64) S.pos64[t] = make_double4(x.x, x.y, x.z, tp.radius);
   if (S.offh) {
-    // FP32 offset from the cell's lower corner (broad phase of FP32-split)
-    S.offh[t] = make_float4((float)(x.x - (g.lc_origin[0] + ci * g.edge[0])),
-                            (float)(x.y - (g.lc_origin[1] + cj * g.edge[1])),
-                            (float)(x.z - (g.lc_origin[2] + ck * g.edge[2])), tp.r_f);
+    S.offh[t] = make_float4((float)(x.x - (bg.lc_origin[0] + ci * bg.edge[0])),
+                            (float)(x.y - (bg.lc_origin[1] + cj * bg.edge[1])),
+                            (float)(x.z - (bg.lc_origin[2] + ck * bg.edge[2])), tp.r_f);
   }
+}
+
+// Second buffers back into the current ones; the displacement and the wraps
+// since the rebuild start again from zero.
+__global__ void k_copyback(DevState S, const int* gate) {
+  if (gatedOff(gate)) return;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= S.n) return;
+  const int cap = S.cap;
+  S.id[t] = S.id2[t]; S.type[t] = S.type2[t]; S.inst[t] = S.inst2[t];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const size_t k = (size_t)d * cap + t;
+    S.x[k] = S.x2[k]; S.v[k] = S.v2[k]; S.w[k] = S.w2[k]; S.wbf[k] = S.wbf2[k];
+    S.F[k] = S.F2[k]; S.T[k] = S.T2[k];
+    S.disp[k] = 0.f;
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) S.q[k * cap + t] = S.q2[k * cap + t];
+  if (S.basis) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) S.basis[k * cap + t] = S.basis2[k * cap + t];
+  }
+  S.wrap[t] = 0;
+}
+
+// Opening kick + drift with the stored F, T (the first step of a call).
+// Per particle only, so it runs in place (the launcher aliases the second
+// buffers to the current ones).
+__global__ void k_move_only(DevState S) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= S.n) return;
+  TypeDesc const& tp = S.types[S.type[t]];
+  advanceParticle(S, t, tp, ld3(S.F, S.cap, t), ld3(S.T, S.cap, t), false, true);
 }
 
 // Scatter of sorted-order state into ID order (for download).
@@ -363,25 +281,35 @@ __global__ void k_basis_by_id(DevState S, double* out, int id_base) {
   for (int k = 0; k < 9; ++k) out[9 * (size_t)i + k] = S.basis[k * S.cap + t];
 }
 
+// Reference-grid cell (Cell::GetCell) of each particle, by ID.
 __global__ void k_cells_by_id(DevState S, int* ijk, int id_base) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
   int i = S.id[t] - id_base;
   if (i < 0 || i >= S.n) return;
-  int4 c = S.cellc[t];
-  ijk[3 * i] = c.x; ijk[3 * i + 1] = c.y; ijk[3 * i + 2] = c.z;
+  GridDesc const& g = S.grids[S.inst[t]];
+  const d3 x = ld3(S.x, S.cap, t);
+  const double xs[3] = {x.x, x.y, x.z};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) ijk[3 * i + d] = (int)floor((xs[d] - g.lc_origin[d]) / g.edge[d]);
 }
 
-// Zeroes the cumulative tangential and rolling memories of every live entry
-// (Component::setContactMapCumulativeFeaturesToZero, Component.cpp:842-851).
+// Zeroes the cumulative tangential and rolling memories of every entry of
+// the given evaluation (Component::setContactMapCumulativeFeaturesToZero,
+// Component.cpp:842-851).
 template <typename V>
-__global__ void k_hist_zero_cumulative(HistTable t) {
+__global__ void k_hist_zero_cumulative(HistTable t, const int* ctl) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= (1 << t.log2cap)) return;
-  if (t.keys[s] == kEmptyKey) return;
+  if (tagOf(t.keys[s]) != ((unsigned)ctl[kCtlEpoch] & kTagMask)) return;
   V* v = static_cast<V*>(t.vals) + 9 * (size_t)s;
   v[0] = v[1] = v[2] = 0;
   v[6] = v[7] = v[8] = 0;
+}
+
+__global__ void k_fill64(unsigned long long* p, size_t n, unsigned long long value) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = value;
 }
 
 // Loads host-layout state (AoS, by particle ID, staged in device memory)
@@ -419,6 +347,8 @@ __global__ void k_load_state(DevState S, const double* x, const double* v, const
 #pragma unroll
     for (int k = 0; k < 9; ++k) S.basis[k * cap + i] = m[k];
   }
+  S.disp[i] = 0.f; S.disp[cap + i] = 0.f; S.disp[2 * cap + i] = 0.f;
+  S.wrap[i] = 0;
   if (!wbf) {
     // q* (w, q) (ParticleKinematics.cpp:220-221)
     dq qq = qmk(mk(q[4 * i], q[4 * i + 1], q[4 * i + 2]), q[4 * i + 3]);
@@ -463,13 +393,15 @@ __global__ void k_vstats_final(const double* part, int nparts, int n, double* ou
   if (threadIdx.x == 0) { out[0] = smax[0]; out[1] = n > 0 ? ssum[0] / n : 0.; }
 }
 
-// Sum of the pair-list segment lengths and count of live history keys.
+// Sum of the pair-list segment lengths and count of the history keys of
+// the last force evaluation.
 __global__ void k_pair_counts(DevState S, unsigned long long* out) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long e = 0, c = 0;
   if (i < S.n) e = (unsigned long long)S.npairs[i];
+  const unsigned tag = (unsigned)S.ctl[kCtlEpoch] & kTagMask;
   int cap = 1 << S.hist_old.log2cap;
-  for (int k = i; k < cap; k += gridDim.x * blockDim.x) c += S.hist_old.keys[k] != kEmptyKey;
+  for (int k = i; k < cap; k += gridDim.x * blockDim.x) c += tagOf(S.hist_old.keys[k]) == tag;
   for (int o = 16; o > 0; o >>= 1) {
     e += __shfl_down_sync(0xffffffffu, e, o);
     c += __shfl_down_sync(0xffffffffu, c, o);
@@ -481,11 +413,45 @@ __global__ void k_pair_counts(DevState S, unsigned long long* out) {
 
 inline int blocks(int n, int b) { return (n + b - 1) / b; }
 
+void launch_decide(DevState const& S, cudaGraphConditionalHandle h, int use_handle,
+                   cudaStream_t st) {
+  k_decide<<<1, 32, 0, st>>>(S, h, use_handle);
+}
+void launch_bin(DevState const& S, const int* gate, cudaStream_t st) {
+  if (S.n) k_bin<<<blocks(S.n, 256), 256, 0, st>>>(S, gate);
+}
+void launch_scan(DevState const& S, const int* gate, cudaStream_t st) {
+  int ntiles = blocks(S.ncells, kScanTile);
+  k_scan_tiles<<<ntiles, kScanTile, 0, st>>>(S.cell_count, S.cell_start, S.scan_tmp, S.ncells, gate);
+  k_scan_sums<<<1, kScanTile, 0, st>>>(S.scan_tmp, ntiles, gate);
+  k_scan_add<<<ntiles, kScanTile, 0, st>>>(S.cell_start, S.scan_tmp, S.cell_count, S.ncells, gate);
+}
+void launch_place(DevState const& S, const int* gate, cudaStream_t st) {
+  if (S.n) k_place<<<blocks(S.n, 256), 256, 0, st>>>(S, gate);
+}
+void launch_cellsort(DevState const& S, const int* gate, cudaStream_t st) {
+  k_cellsort<<<blocks(S.ncells, 256), 256, 0, st>>>(S, gate);
+}
+void launch_permute(DevState const& S, const int* gate, cudaStream_t st) {
+  if (S.n) k_permute<<<blocks(S.n, 256), 256, 0, st>>>(S, gate);
+}
+void launch_copyback(DevState const& S, const int* gate, cudaStream_t st) {
+  if (S.n) k_copyback<<<blocks(S.n, 256), 256, 0, st>>>(S, gate);
+}
+void launch_move_only(DevState const& S, cudaStream_t st) {
+  if (!S.n) return;
+  DevState M = S;   // in place: the "next" buffers are the current ones
+  M.x2 = S.x; M.v2 = S.v; M.w2 = S.w; M.wbf2 = S.wbf; M.q2 = S.q; M.basis2 = S.basis;
+  M.wrap2 = S.wrap;
+  k_move_only<<<blocks(S.n, 256), 256, 0, st>>>(M);
+}
+void launch_fill64(unsigned long long* p, size_t n, unsigned long long value, cudaStream_t st) {
+  if (n) k_fill64<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p, n, value);
+}
 void launch_pair_counts(DevState const& S, unsigned long long* out, cudaStream_t st) {
   cudaMemsetAsync(out, 0, 2 * sizeof(unsigned long long), st);
   k_pair_counts<<<blocks(std::max(S.n, 1), 256), 256, 0, st>>>(S, out);
 }
-
 void launch_load_state(DevState const& S, const double* x, const double* v, const double* w,
                        const double* wbf, const double* q, const double* F, const double* T,
                        const int* type_by_id, const int* inst_by_id, cudaStream_t st) {
@@ -495,32 +461,6 @@ void launch_vstats(DevState const& S, double* part, double* out, cudaStream_t st
   int nb = blocks(S.n, 256);
   k_vstats_partial<<<nb, 256, 0, st>>>(S, part);
   k_vstats_final<<<1, 256, 0, st>>>(part, nb, S.n, out);
-}
-
-void launch_key(DevState const& S, double h, double dt, int pre_kick, double pre_h, cudaStream_t st) {
-  if (S.n) k_key<<<blocks(S.n, 256), 256, 0, st>>>(S, h, dt, pre_kick, pre_h);
-}
-void launch_bin(DevState const& S, cudaStream_t st) {
-  if (S.n) k_bin<<<blocks(S.n, 256), 256, 0, st>>>(S);
-}
-void launch_kick(DevState const& S, double h, cudaStream_t st) {
-  if (S.n) k_kick<<<blocks(S.n, 256), 256, 0, st>>>(S, h);
-}
-void launch_scan(DevState const& S, cudaStream_t st) {
-  int ntiles = blocks(S.ncells, kScanTile);
-  k_scan_tiles<<<ntiles, kScanTile, 0, st>>>(S.cell_count, S.cell_start, S.scan_tmp, S.ncells);
-  k_scan_sums<<<1, kScanTile, 0, st>>>(S.scan_tmp, ntiles);
-  k_scan_add<<<ntiles, kScanTile, 0, st>>>(S.cell_start, S.scan_tmp, S.cell_count, S.ncells);
-}
-void launch_place(DevState const& S, cudaStream_t st) {
-  if (S.n) k_place<<<blocks(S.n, 256), 256, 0, st>>>(S);
-}
-void launch_cellsort(DevState const& S, cudaStream_t st) {
-  k_cellsort<<<blocks(S.ncells, 256), 256, 0, st>>>(S);
-}
-void launch_move_gather(DevState const& S, int moving, double h, double dt, int pre_kick,
-                        double pre_h, cudaStream_t st) {
-  if (S.n) k_move_gather<<<blocks(S.n, 256), 256, 0, st>>>(S, moving, h, dt, pre_kick, pre_h);
 }
 void launch_scatter_by_id(DevState const& S, double* x, double* v, double* w, double* wbf,
                           double* q, double* F, double* T, int id_base, cudaStream_t st) {
@@ -532,10 +472,10 @@ void launch_basis_by_id(DevState const& S, double* out, int id_base, cudaStream_
 void launch_cells_by_id(DevState const& S, int* ijk, int id_base, cudaStream_t st) {
   if (S.n) k_cells_by_id<<<blocks(S.n, 256), 256, 0, st>>>(S, ijk, id_base);
 }
-void launch_hist_zero_cumulative(HistTable const& t, int fp64, cudaStream_t st) {
+void launch_hist_zero_cumulative(HistTable const& t, const int* ctl, int fp64, cudaStream_t st) {
   int cap = 1 << t.log2cap;
-  if (fp64) k_hist_zero_cumulative<double><<<blocks(cap, 256), 256, 0, st>>>(t);
-  else k_hist_zero_cumulative<float><<<blocks(cap, 256), 256, 0, st>>>(t);
+  if (fp64) k_hist_zero_cumulative<double><<<blocks(cap, 256), 256, 0, st>>>(t, ctl);
+  else k_hist_zero_cumulative<float><<<blocks(cap, 256), 256, 0, st>>>(t, ctl);
 }
 
 }  // namespace gdem

@@ -1,0 +1,197 @@
+// gdem_motion.cuh -- second-order leapfrog of one particle, shared by the
+// move-only kernel and the fused force + move step kernels.
+//
+// The expressions follow the reference operation by operation (the files
+// that include this header are compiled with -fmad=false):
+//   SecondOrderLeapFrog::Move / advanceVelocity
+//     (TimeIntegration/src/SecondOrderLeapFrog.cpp:44-94),
+//   ParticleKinematics::Move (Component/src/ParticleKinematics.cpp:62-128),
+//   ParticleKinematicsSphere / ParticleKinematics3D angular acceleration
+//     (ParticleKinematicsSphere.cpp:47-55, ParticleKinematics3D.cpp:56-77),
+//   Transform::composeLeftByRotation (Geometry/src/Transform.cpp:140-159),
+//   MotionError (Component/src/Particle.cpp:446-456),
+//   Cell::GetCell and the periodic master/clone swap
+//     (Base/src/Cell.cpp:172-184, Base/src/LinkedCell.cpp:1502-1547).
+#pragma once
+#include "gdem_device.cuh"
+
+namespace gdem {
+
+// Angular acceleration in the body frame; the gyroscopic term for
+// non-spherical classes (predictor mode).
+__device__ __forceinline__ d3 dOmega(TypeDesc const& t, d3 tbf, d3 om) {
+  const double c = 1.;
+  if (t.shape == 0)
+    return mk(tbf.x / (c * t.inertia[0]), tbf.y / (c * t.inertia[1]), tbf.z / (c * t.inertia[2]));
+  const double* I = t.inertia;
+  return mk(tbf.x / (c * I[0]) + om.y * om.z * (I[1] - I[2]) / I[0],
+            tbf.y / (c * I[1]) + om.z * om.x * (I[2] - I[0]) / I[1],
+            tbf.z / (c * I[2]) + om.x * om.y * (I[0] - I[1]) / I[2]);
+}
+
+// SSP-RK3 update of the body-fixed angular velocity over h.  For a sphere
+// the acceleration does not depend on omega, so K1 = K2 = K3 and one
+// evaluation gives the same bits as three.
+__device__ __forceinline__ d3 rk3(TypeDesc const& t, d3 tbf, d3 wbf, double h) {
+  if (t.shape == 0) {
+    d3 K = dOmega(t, tbf, wbf);
+    K = K * h;
+    return wbf + ((K + K) + 4. * K) / 6.;
+  }
+  d3 K1 = dOmega(t, tbf, wbf);
+  K1 = K1 * h;
+  d3 K2 = dOmega(t, tbf, wbf + K1);
+  K2 = K2 * h;
+  d3 K3 = dOmega(t, tbf, wbf + 0.25 * (K1 + K2));
+  K3 = K3 * h;
+  return wbf + ((K1 + K2) + 4. * K3) / 6.;
+}
+
+// advanceVelocity: v, w_bf (and the space-frame w) over h.
+__device__ __forceinline__ void kick(TypeDesc const& tp, d3 F, d3 T, d3& v, d3& wbf, d3& w,
+                                     dq q, double h) {
+  dq pc = conj(q);
+  d3 tbf = multToVector3(pc, vecq(T, q));
+  const double c = 1.;
+  v = v + (F / (tp.mass * c)) * h;
+  wbf = rk3(tp, tbf, wbf, h);
+  w = multToVector3(q, vecq(wbf, pc));
+}
+
+// Signed periodic wrap counts, one byte per axis.
+__device__ __forceinline__ int wrapGet(int w, int d) {
+  return (int)(signed char)((unsigned)w >> (8 * d) & 0xFFu);
+}
+__device__ __forceinline__ int wrapSet(int w, int d, int val) {
+  const unsigned m = 0xFFu << (8 * d);
+  return (int)(((unsigned)w & ~m) | (((unsigned)val & 0xFFu) << (8 * d)));
+}
+
+// Cell of x in the reference grid after the periodic wrap (a particle that
+// left the inner cells is replaced by its image; x is updated).  wrapd[d]
+// counts the wrap: the continuous position is x + wrapd * L.  Out-of-grid
+// particles raise kErrOutOfGrid.
+__device__ __forceinline__ void wrapToGrid(GridDesc const& g, d3& x, int* wrapd, int* status) {
+  double xs[3] = {x.x, x.y, x.z};
+  bool outside = false;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    wrapd[d] = 0;
+    int id = (int)floor((xs[d] - g.lc_origin[d]) / g.edge[d]);
+    if (g.periodic[d]) {
+      if (id < 1) { xs[d] = xs[d] + g.L[d]; wrapd[d] = -1; }
+      else if (id > g.nb[d] - 2) { xs[d] = xs[d] + (-g.L[d]); wrapd[d] = 1; }
+      id = (int)floor((xs[d] - g.lc_origin[d]) / g.edge[d]);
+    }
+    outside |= id < 0 || id >= g.nb[d];
+  }
+  if (outside) raise(status, kErrOutOfGrid);
+  x = mk(xs[0], xs[1], xs[2]);
+}
+
+// One particle's leapfrog: optionally the closing kick of the previous step
+// (with this step's F, T over hc), then optionally the opening kick over h
+// and the drift over dt with the quaternion and orientation update.
+// basis: 9 entries (row-major) or null.  dx receives the translation.
+__device__ __forceinline__ void leapfrog(TypeDesc const& tp, d3 F, d3 T, bool close, double hc,
+                                         bool move, double h, double dt, d3& x, d3& v,
+                                         d3& wbf, d3& w, dq& q, double* basis, d3& dx,
+                                         int* status) {
+  if (close) kick(tp, F, T, v, wbf, w, q, hc);
+  dx = mk(0., 0., 0.);
+  if (!move) return;
+  dq pc = conj(q);
+  d3 tbf = multToVector3(pc, vecq(T, q));
+  const double c = 1.;
+  v = v + (F / (tp.mass * c)) * h;
+  dx = v * dt;
+  wbf = rk3(tp, tbf, wbf, h);
+  w = multToVector3(q, vecq(wbf, pc));
+  const d3 meanw = w;     // same expression as w (ParticleKinematics.cpp:79-82)
+  x = x + dx;
+  double nOm = norm(meanw);
+  dq qdt;
+  if (nOm > 1.0e-10) {
+    double cc, ss;
+    sincos(nOm * dt / 2., &ss, &cc);
+    qdt = qmk((ss * 1. / nOm) * meanw, cc);
+  } else {
+    qdt = qmk(mk(0., 0., 0.), 1.);
+  }
+  q = qmul(qdt, q);
+  if (basis) {
+    double out[9];
+    const double qx = qdt.v.x, qy = qdt.v.y, qz = qdt.v.z, qw = qdt.w;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      double px = qy * basis[6 + i] - qz * basis[3 + i] + qw * basis[0 + i];
+      double py = qz * basis[0 + i] - qx * basis[6 + i] + qw * basis[3 + i];
+      double pz = qx * basis[3 + i] - qy * basis[0 + i] + qw * basis[6 + i];
+      double pw = -qx * basis[0 + i] - qy * basis[3 + i] - qz * basis[6 + i];
+      out[0 + i] = qy * pz - qz * py - pw * qx + qw * px;
+      out[3 + i] = qz * px - qx * pz - pw * qy + qw * py;
+      out[6 + i] = qx * py - qy * px - pw * qz + qw * pz;
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) basis[k] = out[k];
+  }
+  if (norm(dx) > tp.crust) raise(status, kErrMotion);
+}
+
+// Moves particle t of the current buffers (F, T as given) and writes the
+// result to the second buffers; updates the pair-list displacement and wraps
+// and flags a rebuild when the particle has moved more than half the skin.
+// close/move select the kicks as in leapfrog().
+__device__ __forceinline__ void advanceParticle(DevState const& S, int t, TypeDesc const& tp,
+                                                d3 F, d3 T, bool close, bool move) {
+  const int cap = S.cap;
+  const double dt = S.dt;
+  GridDesc const& g = S.grids[S.inst[t]];
+  d3 x = ld3(S.x, cap, t), v = ld3(S.v, cap, t), w = ld3(S.w, cap, t);
+  d3 wbf = ld3(S.wbf, cap, t);
+  dq q = qmk(mk(S.q[t], S.q[cap + t], S.q[2 * cap + t]), S.q[3 * cap + t]);
+  double bas[9];
+  double* bp = nullptr;
+  if (S.basis) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) bas[k] = S.basis[k * cap + t];
+    bp = bas;
+  }
+  d3 dx;
+  leapfrog(tp, F, T, close, 0.5 * dt, move, 0.5 * dt, dt, x, v, wbf, w, q, bp, dx, S.status);
+  int wr = S.wrap[t];
+  if (move) {
+    int wd[3];
+    wrapToGrid(g, x, wd, S.status);
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      if (wd[d]) wr = wrapSet(wr, d, wrapGet(wr, d) + wd[d]);
+    float3 ds = make_float3(S.disp[t] + (float)dx.x, S.disp[cap + t] + (float)dx.y,
+                            S.disp[2 * cap + t] + (float)dx.z);
+    S.disp[t] = ds.x; S.disp[cap + t] = ds.y; S.disp[2 * cap + t] = ds.z;
+    const float half = 0.5f * S.bgrids[S.inst[t]].skin_f;
+    if (ds.x * ds.x + ds.y * ds.y + ds.z * ds.z > half * half) S.ctl[kCtlNeed] = 1;
+  }
+  st3(S.x2, cap, t, x); st3(S.v2, cap, t, v); st3(S.w2, cap, t, w); st3(S.wbf2, cap, t, wbf);
+  S.q2[t] = q.v.x; S.q2[cap + t] = q.v.y; S.q2[2 * cap + t] = q.v.z; S.q2[3 * cap + t] = q.w;
+  if (bp) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) S.basis2[k * cap + t] = bas[k];
+  }
+  S.wrap2[t] = wr;
+}
+
+// Image shift (in periods) between slot t and its list entry u found through
+// pair-list cell offset (di, dj, dk) of t's rebuild-time cell cc, corrected by
+// the wraps of both particles since the rebuild.
+__device__ __forceinline__ void entryShift(DevState const& S, GridDesc const& bg, int4 cc, int t,
+                                           int u, int di, int dj, int dk, int* sh) {
+  neighbourKey(bg, cc.x, cc.y, cc.z, di, dj, dk, sh);
+  const int wt = S.wrap[t], wu = S.wrap[u];
+  if (wt | wu) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) sh[d] += wrapGet(wu, d) - wrapGet(wt, d);
+  }
+}
+
+}  // namespace gdem

@@ -25,6 +25,15 @@ enum StatusBits : int {
   kErrPairsFull = 1 << 6,        // a particle has more than kPairCap candidates
 };
 
+// Words of the device control block (DevState::ctl).
+enum CtlWords : int {
+  kCtlNeed = 0,     // set by the step kernels: a particle moved more than skin / 2
+  kCtlActive = 1,   // this step rebuilds the pair list (set by k_decide)
+  kCtlEpoch = 2,    // force evaluations so far (tags the contact-history keys)
+  kCtlRebuilds = 3, // pair-list rebuilds so far
+  kCtlWords = 4
+};
+
 // One independent simulation ("instance").  A single Grains3D system is a
 // batch of one.  Cell numbering follows LinkedCell::getCellNumber
 // (Base/src/LinkedCell.cpp:1165-1168): j * nbk * nbi + k * nbi + i.
@@ -39,6 +48,8 @@ struct GridDesc {
   int model_base;        // first entry of this instance in the model table
   int pad0;
   float edge_f[3];       // edge in FP32 (FP32-split broad phase)
+  float skin_f;          // pair-list skin in FP32
+  double skin;           // pair-list skin: pairs closer than the sum of radii + skin are listed
 };
 
 // Particle class (a <Particle> node of the XML input).

@@ -96,6 +96,7 @@ def library() -> ctypes.CDLL:
         "gdem_set_profiling": ([_P, ctypes.c_int], ctypes.c_int),
         "gdem_law_counts": ([_P, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.c_int],
                             ctypes.c_int),
+        "gdem_step_counts": ([_P, ctypes.POINTER(i64), ctypes.POINTER(i64)], ctypes.c_int),
         "gdem_pair_counts": ([_P, ctypes.POINTER(i64), ctypes.POINTER(i64)], ctypes.c_int),
         "gdem_kernel_times": ([_P, ctypes.c_int, _IP, ctypes.c_char_p, _DP,
                                ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
@@ -223,6 +224,13 @@ class Grains:
         a = ctypes.c_int64(0)
         b = ctypes.c_int64(0)
         self._check(library().gdem_pair_counts(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def step_counts(self):
+        """(force evaluations, pair-list rebuilds) since the state was created."""
+        a = ctypes.c_int64(0)
+        b = ctypes.c_int64(0)
+        self._check(library().gdem_step_counts(self._h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
 
     def law_counts(self, reset=False):
