@@ -2,19 +2,27 @@
 """Grains3D DEM time step on B200: particle-steps/s for 1,000,000 polydisperse
 spheres in a triply periodic box (granular-gas cooling), FP32-split vs FP64.
 
-One step = one kick-drift-kick leapfrog step of the whole system: move,
-linked-cell binning (counting sort on the cell key), 27-cell pair search,
-narrow phase, HookeMemory contact force with hashed tangential history,
-per-particle force/torque reduction.  Inputs: the seeded FCC stand-in of the
+One step = one kick-drift-kick leapfrog step of the whole system: the force
+evaluation (narrow phase over the skin pair list, Hooke / HookeMemory contact
+force with hashed tangential history, per-particle force/torque reduction)
+fused with the closing kick, the next opening kick and the drift; the pair
+list (counting sort on the cell key + 27-cell search) is rebuilt when a
+particle has moved half the skin.  Inputs: the seeded FCC stand-in of the
 1M-sphere configuration (pacific_b200.scenarios.periodic_gas), synthetic.
+
+Other legs on the same line: per-particle and per-contact force error against
+the CPU FP64 oracle, the batched sweep against sequential runs, the convex
+(cube + tetrahedron) pour, the end-to-end run through the public API with host
+buffers, and the CPU baseline (the Grains3D reference sources compiled here,
+single thread, on a bounded sample).
 
 Multi-GPU: the workload does not shard without a halo exchange, so each rank
 runs an independent replica (weak scaling, no data-path collective); the
 timed region is bracketed by barriers and the max over ranks is reported.
 
-`--impl reference` times the CPU FP64 restatement of the reference's step
-(oracle/) on the host: the reference itself cannot be built here (it needs
-Xerces-C and MPI, neither present).
+`--impl reference` times the Grains3D reference's own CPU step (compiled from
+its sources by oracle/build_ref.sh; the CPU FP64 restatement when that build
+is absent) on the host, on a bounded sample of the same workload.
 """
 from __future__ import annotations
 

@@ -289,6 +289,7 @@ __global__ void __launch_bounds__(256) k_pairs32(DevState S, const int* gate) {
     ++cnt;
   });
   if (cnt > kPairCap) { raise(S.status, kErrPairsFull); cnt = kPairCap; }
+  sortEntriesById(out, cnt, S.id);
   S.npairs[t] = cnt;
 }
 

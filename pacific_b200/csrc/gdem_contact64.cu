@@ -51,6 +51,7 @@ __global__ void __launch_bounds__(256) k_pairs64(DevState S, const int* gate) {
     ++cnt;
   });
   if (cnt > kPairCap) { raise(S.status, kErrPairsFull); cnt = kPairCap; }
+  sortEntriesById(out, cnt, S.id);
   S.npairs[t] = cnt;
 }
 

@@ -273,6 +273,22 @@ __device__ __forceinline__ void forEachCandidate(const int* __restrict__ cs, Gri
   }
 }
 
+// Orders a particle's list entries by partner ID, so that the reduction
+// order of its forces does not depend on the cells at the last rebuild (nor
+// on when the list was rebuilt).
+__device__ __forceinline__ void sortEntriesById(int* seg, int cnt, const int* id) {
+  for (int i = 1; i < cnt; ++i) {
+    const int e = seg[i];
+    const int ide = id[e & ((1 << 27) - 1)];
+    int j = i - 1;
+    while (j >= 0 && id[seg[j] & ((1 << 27) - 1)] > ide) {
+      seg[j + 1] = seg[j];
+      --j;
+    }
+    seg[j + 1] = e;
+  }
+}
+
 // Code of a stencil offset in 0..26 and back.
 __device__ __forceinline__ int offCode(int di, int dj, int dk) { return (di + 1) + 3 * (dk + 1) + 9 * (dj + 1); }
 __device__ __forceinline__ void offDecode(int c, int* di, int* dj, int* dk) {
