@@ -109,15 +109,15 @@ def algorithmic_bytes(kernel, n, entries, contacts, ncells, fp64):
     """Compulsory DRAM bytes of one launch of each phase of a spheres-only
     step: each input read once, each output written once, neighbour re-reads
     counted as cache hits.  Per particle unless noted."""
-    if kernel in ("step64", "step32"):
-        # fused force + leapfrog: cellc id type inst npairs wrap disp x v w w_bf q |
-        # x v w w_bf q wrap disp (second buffers); per entry its word; per
-        # contact the history key + values, read and written
-        per_p = (16 + 4 + 4 + 4 + 4 + 4 + 12 + 72 + 24 + 32) + (72 + 24 + 32 + 4 + 12)
-        per_c = 2 * (8 + (72 if fp64 else 36))
-        return n * per_p + 4 * entries + contacts * per_c
-    if kernel == "move_only":    # F T x v w w_bf q type inst disp wrap | x v w w_bf q disp wrap
-        return n * (48 + 104 + 8 + 12 + 4 + 104 + 12 + 4)
+    if kernel == "filter":       # cellc posf npairs wrap + entry words | kept entries + count
+        return n * (16 + 16 + 4 + 4 + 4) + 4 * entries + 4 * contacts
+    if kernel in ("forces64", "forces32"):
+        # cellc id type x v w nact | F T; per contact the entry word and the
+        # history key + values, read and written
+        per_c = 4 + 2 * (8 + (72 if fp64 else 36))
+        return n * (16 + 4 + 4 + 72 + 4 + 48) + contacts * per_c
+    if kernel == "move":         # F T x v w w_bf q type inst disp wrap | x v w w_bf q disp wrap posf
+        return n * (48 + 104 + 8 + 12 + 4 + 104 + 12 + 4 + 16)
     if kernel == "bin":          # x inst | skey rank; cell-count RMW
         return n * (24 + 4 + 8 + 8)
     if kernel == "scan":         # counts | starts (per cell)
@@ -533,12 +533,13 @@ def main():
             "gpu_launches": None,
         }
         # kernels launched in the timed region: the opening move, per step
-        # k_decide + the fused step kernel, per pair-list rebuild its 9
-        # kernels (bin, scan x3, place, cellsort, permute, copyback, pairs),
-        # and the history-table refills (every 512 evaluations per table)
+        # k_decide, the contact filter, the force kernel and the move, per
+        # pair-list rebuild its 9 kernels (bin, scan x3, place, cellsort,
+        # permute, copyback, pairs), and the history-table refills (every 512
+        # evaluations per table)
         e0, e1 = fp32["evals"]
         fills = sum(1 for e in range(e0 + 1, e1 + 1) if e % 512 < 2)
-        line["gpu_launches"] = 1 + 2 * args.steps + 9 * fp32["rebuilds"] + fills
+        line["gpu_launches"] = 1 + 4 * args.steps + 9 * fp32["rebuilds"] + fills
         line["pair_list"] = {"rebuilds_fp32_split": fp32["rebuilds"],
                              "rebuilds_fp64": fp64["rebuilds"], "steps": args.steps}
         if not args.no_error:

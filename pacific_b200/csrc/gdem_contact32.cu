@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(256) k_pairs32(DevState S, const int* gate) {
 // kConvex: some class is not a sphere, so the GJK narrow phase is compiled in
 // (it is kept out of the sphere-only kernel, whose registers it would triple).
 template <bool kConvex>
-__global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_step32(DevState S, int flags) {
+__global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_forces32(DevState S) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
   const int cap = S.cap;
@@ -309,8 +309,8 @@ __global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_step32(DevState S, int
   const d3 xt = ld3(S.x, cap, t);
   float3 Fs = f3(0.f, 0.f, 0.f), Ts = f3(0.f, 0.f, 0.f);
   int nlaw = 0, nre = 0;   // contacts evaluated / re-evaluated in FP64
-  const int np = S.npairs[t];
-  const int* seg = S.pairs + (size_t)t * kPairCap;
+  const int np = S.nact[t];
+  const int* seg = S.act + (size_t)t * kPairCap;
   for (int e = 0; e < np; ++e) {
     const uint32_t ent = (uint32_t)seg[e];
     const int u = (int)(ent & ((1u << 27) - 1));
@@ -423,10 +423,8 @@ __global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_step32(DevState S, int
   const d3 F = mk(ta.weight[0] + (double)Fs.x, ta.weight[1] + (double)Fs.y,
                   ta.weight[2] + (double)Fs.z);
   const d3 T = mk((double)Ts.x, (double)Ts.y, (double)Ts.z);
-  if (flags & kStepStoreFT) {
-    st3(S.F, cap, t, F);
-    st3(S.T, cap, t, T);
-  }
+  st3(S.F, cap, t, F);
+  st3(S.T, cap, t, T);
   // warp-aggregated counters of the FP64 re-evaluations
   const unsigned mask = __activemask();
   const int wl = __reduce_add_sync(mask, nlaw), wr = __reduce_add_sync(mask, nre);
@@ -434,7 +432,6 @@ __global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_step32(DevState S, int
     atomicAdd(S.law_counts, (unsigned long long)wl);
     if (wr) atomicAdd(S.law_counts + 1, (unsigned long long)wr);
   }
-  advanceParticle(S, t, ta, F, T, (flags & kStepClose) != 0, (flags & kStepMove) != 0);
 }
 
 }  // namespace
@@ -442,10 +439,10 @@ __global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_step32(DevState S, int
 void launch_pairs32(DevState const& S, const int* gate, cudaStream_t st) {
   if (S.n) k_pairs32<<<(S.n + 255) / 256, 256, 0, st>>>(S, gate);
 }
-void launch_step32(DevState const& S, int flags, cudaStream_t st) {
+void launch_forces32(DevState const& S, cudaStream_t st) {
   if (!S.n) return;
-  if (S.any_convex) k_step32<true><<<(S.n + 255) / 256, 256, 0, st>>>(S, flags);
-  else k_step32<false><<<(S.n + 255) / 256, 256, 0, st>>>(S, flags);
+  if (S.any_convex) k_forces32<true><<<(S.n + 255) / 256, 256, 0, st>>>(S);
+  else k_forces32<false><<<(S.n + 255) / 256, 256, 0, st>>>(S);
 }
 
 }  // namespace gdem

@@ -9,14 +9,13 @@
 //               can be reduced without atomics).  A candidate is listed when
 //               its bounding spheres are closer than the skin, evaluated with
 //               the lower-ID body first so both directions of a pair agree.
-//   k_step64    for each particle: narrow phase on every listed partner
-//               (ClosestPointSPHERESPHERE or GJK), Hooke / HookeMemory force
-//               with the tangential history in the hashed pair table, the
-//               deterministic reduction of its force and torque over its own
-//               list in list order, then its wall contacts (SimpleObstacle::
-//               InterAction, Component/src/SimpleObstacle.cpp:222-271); then
-//               its leapfrog (closing kick, opening kick, drift) into the
-//               second buffers.
+//   k_forces64  for each particle: narrow phase on every entry that the
+//               contact filter kept (ClosestPointSPHERESPHERE or GJK), Hooke /
+//               HookeMemory force with the tangential history in the hashed
+//               pair table, the deterministic reduction of its force and
+//               torque over those entries in list (partner-ID) order, then its
+//               wall contacts (SimpleObstacle::InterAction, Component/src/
+//               SimpleObstacle.cpp:222-271).
 #include "gdem_contact_common.cuh"
 #include "gdem_kernels.cuh"
 #include "gdem_motion.cuh"
@@ -27,7 +26,7 @@ namespace {
 
 // Lists a candidate when its bounding spheres are closer than the skin (with
 // a relative margin of 1e-12, for periodic images whose two orientations
-// round the image translation differently); k_step64 then decides contact
+// round the image translation differently); k_forces64 then decides contact
 // exactly (distance < 0) in lower-ID-first orientation.
 __global__ void __launch_bounds__(256) k_pairs64(DevState S, const int* gate) {
   if (gate && !*gate) return;
@@ -68,7 +67,7 @@ __device__ __forceinline__ void storeHist(HistTable const& t, int slot, d3 kd, d
 // kConvex: some class is not a sphere, so the GJK narrow phase is compiled in
 // (it is kept out of the sphere-only kernel, whose registers it would triple).
 template <bool kConvex>
-__global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_step64(DevState S, int flags) {
+__global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_forces64(DevState S) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
   const int cap = S.cap;
@@ -82,8 +81,8 @@ __global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_step64(DevState S, int
   d3 T = mk(0., 0., 0.);
   const double dt = S.dt;
   const unsigned tag = (unsigned)S.ctl[kCtlEpoch], tag_old = tag - 1u;
-  const int np = S.npairs[t];
-  const int* seg = S.pairs + (size_t)t * kPairCap;
+  const int np = S.nact[t];
+  const int* seg = S.act + (size_t)t * kPairCap;
   for (int e = 0; e < np; ++e) {
     const uint32_t ent = (uint32_t)seg[e];
     const int u = (int)(ent & ((1u << 27) - 1));
@@ -194,11 +193,8 @@ __global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_step64(DevState S, int
     T = T + cross(ct.point - xt, f);
     if (m.rolling) T = T + mr;
   }
-  if (flags & kStepStoreFT) {
-    st3(S.F, cap, t, F);
-    st3(S.T, cap, t, T);
-  }
-  advanceParticle(S, t, ta, F, T, (flags & kStepClose) != 0, (flags & kStepMove) != 0);
+  st3(S.F, cap, t, F);
+  st3(S.T, cap, t, T);
 }
 
 }  // namespace
@@ -206,10 +202,10 @@ __global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_step64(DevState S, int
 void launch_pairs64(DevState const& S, const int* gate, cudaStream_t st) {
   if (S.n) k_pairs64<<<(S.n + 255) / 256, 256, 0, st>>>(S, gate);
 }
-void launch_step64(DevState const& S, int flags, cudaStream_t st) {
+void launch_forces64(DevState const& S, cudaStream_t st) {
   if (!S.n) return;
-  if (S.any_convex) k_step64<true><<<(S.n + 255) / 256, 256, 0, st>>>(S, flags);
-  else k_step64<false><<<(S.n + 255) / 256, 256, 0, st>>>(S, flags);
+  if (S.any_convex) k_forces64<true><<<(S.n + 255) / 256, 256, 0, st>>>(S);
+  else k_forces64<false><<<(S.n + 255) / 256, 256, 0, st>>>(S);
 }
 
 }  // namespace gdem

@@ -121,7 +121,9 @@ struct DevState {
   float4* offh;           // FP32 cell-relative offset; FP32 radius
   int4* cellc;            // pair-list cell i, j, k and instance at the last rebuild
   // pair list: per-particle segments of kPairCap entries
-  int* pairs; int* npairs;
+  int* pairs; int* npairs;   // skin list (rebuilt on demand)
+  int* act; int* nact;       // entries of the skin list in contact this step (same layout)
+  float4* posf;           // FP32 position + circumscribed radius (contact filter)
   double* pair_delta;     // diagnostics: overlap of each entry (+inf: no contact)
   double* wall_delta;     // diagnostics: overlap with each wall slot
   double* pair_force;     // diagnostics: contact force on the lower ID (3 per entry)

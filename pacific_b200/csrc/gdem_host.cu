@@ -443,6 +443,17 @@ InstanceDesc readInstance(std::string const& path) {
   }
   b.skin = skin;
   b.skin_f = (float)skin;
+  // FP32 contact filter: positions rounded to float carry at most half an ulp
+  // of the largest coordinate each (2^-24 relative); 5e-7 of it bounds the
+  // error of a difference plus an image shift with room to spare
+  double maxabs = 0.;
+  for (int d = 0; d < 3; ++d) {
+    maxabs = std::max(maxabs, std::fabs(org[d]) + (maxc[d] - org[d]));
+    b.Lf[d] = (float)(maxc[d] - org[d]);
+    g.Lf[d] = b.Lf[d];
+  }
+  b.filt_margin = (float)(5.e-7 * maxabs);
+  g.filt_margin = b.filt_margin;
   return I;
 }
 
@@ -633,6 +644,8 @@ struct System {
       S.pos64 = nullptr;
     }
     S.pairs = alloc<int>(c * kPairCap); S.npairs = alloc<int>(c);
+    S.act = alloc<int>(c * kPairCap); S.nact = alloc<int>(c);
+    S.posf = alloc<float4>(c);
     S.pair_delta = nullptr; S.wall_delta = nullptr; S.diag = 0;
     S.pair_force = nullptr; S.wall_force = nullptr;
     int l2 = nextPow2Log((size_t)8 * c + 64);
@@ -680,14 +693,7 @@ struct System {
     id_order = true;
   }
 
-  // A force evaluation reads x, v, w, w_bf, q, basis, wraps and writes the
-  // second buffers; the contact-history tables alternate with it, so both
-  // parities advance together.
-  void swapDyn() {
-    std::swap(S.x, S.x2); std::swap(S.v, S.v2); std::swap(S.w, S.w2);
-    std::swap(S.wbf, S.wbf2); std::swap(S.q, S.q2); std::swap(S.basis, S.basis2);
-    std::swap(S.wrap, S.wrap2);
-  }
+  // The contact-history tables alternate with every force evaluation.
   void swapHist() { std::swap(S.hist_old, S.hist_new); }
 
   // The table that evaluation e (1-based) writes is refilled every 512 of its
@@ -714,18 +720,22 @@ struct System {
     if (precision == GDEM_FP64) timed("pairs64", [&] { launch_pairs64(S, gate, stream); });
     else timed("pairs32", [&] { launch_pairs32(S, gate, stream); });
   }
-  void stepKernel(int flags) {
-    if (precision == GDEM_FP64) timed("step64", [&] { launch_step64(S, flags, stream); });
-    else timed("step32", [&] { launch_step32(S, flags, stream); });
+  // Contact filter, forces, then the leapfrog parts in flags (none at the
+  // leapfrog start).
+  void forcesAndMove(int flags) {
+    timed("filter", [&] { launch_filter(S, stream); });
+    if (precision == GDEM_FP64) timed("forces64", [&] { launch_forces64(S, stream); });
+    else timed("forces32", [&] { launch_forces32(S, stream); });
+    if (flags) timed("move", [&] { launch_move(S, flags, stream); });
   }
-  // One force evaluation with plain launches: decide, gated rebuild, step.
+  // One force evaluation with plain launches: decide, gated rebuild, filter,
+  // forces, move.
   void evaluate(int flags) {
     maybeClearHistory(epoch + 1);
     timed("decide", [&] { launch_decide(S, cudaGraphConditionalHandle(), 0, stream); });
     rebuild(S.ctl + kCtlActive);
-    stepKernel(flags);
+    forcesAndMove(flags);
     ++epoch;
-    swapDyn();
     swapHist();
   }
 
@@ -771,7 +781,7 @@ struct System {
     CK(cudaStreamBeginCaptureToGraph(stream, g, &tail, nullptr, 1,
                                      cudaStreamCaptureModeThreadLocal));
     if (!conditional) rebuild(S.ctl + kCtlActive);
-    stepKernel(flags);
+    forcesAndMove(flags);
     CK(cudaStreamEndCapture(stream, &g));
     cudaGraphExec_t ex = nullptr;
     CK(cudaGraphInstantiate(&ex, g, 0));
@@ -780,7 +790,7 @@ struct System {
     return ex;
   }
   // Graph of evaluation kind k (0: inside a call, 1: last of a call) for the
-  // current buffer parity; built on first use.
+  // current history-table parity; built on first use.
   void launchEvaluation(int k, int flags) {
     maybeClearHistory(epoch + 1);
     const int par = (int)(parity & 1);
@@ -788,13 +798,12 @@ struct System {
     CK(cudaGraphLaunch(graph[k][par], stream));
     ++epoch;
     ++parity;
-    swapDyn();
     swapHist();
   }
 
   void init() {
     id_order = false;
-    evaluate(kStepForces | kStepStoreFT);
+    evaluate(0);
     ++parity;
     launch_hist_zero_cumulative(S.hist_old, S.ctl, precision == GDEM_FP64, stream);
     CK(cudaStreamSynchronize(stream));
@@ -808,9 +817,9 @@ struct System {
     if (nsteps <= 0) return;
     id_order = false;
     CK(cudaEventRecord(ev0, stream));
-    timed("move_only", [&] { launch_move_only(S, stream); });
-    const int mid = kStepForces | kStepClose | kStepMove;
-    const int last = kStepForces | kStepClose | kStepStoreFT;
+    timed("move", [&] { launch_move(S, kStepMove, stream); });
+    const int mid = kStepClose | kStepMove;
+    const int last = kStepClose;
     const bool graphs = use_graphs && !diag && !profiling;
     for (int k = 0; k < nsteps; ++k) {
       const bool is_last = k == nsteps - 1;
@@ -1216,8 +1225,8 @@ int gdem_download_contacts(gdem_handle h, int64_t capacity, int64_t* count, int*
     std::vector<double> wd(n * S.max_walls), wf(3 * n * S.max_walls);
     std::vector<int4> cells(n);
     CK(cudaMemcpy(ids.data(), S.id, n * sizeof(int), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(np.data(), S.npairs, n * sizeof(int), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(pairs.data(), S.pairs, n * kPairCap * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(np.data(), S.nact, n * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(pairs.data(), S.act, n * kPairCap * sizeof(int), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(pd.data(), S.pair_delta, pd.size() * sizeof(double), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(wd.data(), S.wall_delta, wd.size() * sizeof(double), cudaMemcpyDeviceToHost));
     if (force) {

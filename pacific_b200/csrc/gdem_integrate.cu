@@ -6,8 +6,8 @@
 //
 // A step is (host side, gdem_host.cu): k_decide, then -- only when some
 // particle has moved more than half the pair-list skin since the last
-// rebuild -- the rebuild below, then one fused force + leapfrog kernel
-// (gdem_contact64.cu / gdem_contact32.cu).
+// rebuild -- the rebuild below, then k_filter, the force kernel
+// (gdem_contact64.cu / gdem_contact32.cu) and k_move.
 //
 //   k_decide    turns the rebuild request of the previous step into this
 //               step's decision (and the CUDA-graph condition), and counts
@@ -21,8 +21,11 @@
 //   k_permute / k_copyback
 //               the whole state into cell order (through the second
 //               buffers), with the compact copies the pair search reads.
-//   k_move_only the opening kick and drift of the first step of a call
-//               (SecondOrderLeapFrog::Move, ParticleKinematics::Move).
+//   k_filter    the skin-list entries whose bounding spheres overlap now.
+//   k_move      the leapfrog of each particle in place: closing kick of the
+//               step that ends and opening kick + drift of the next
+//               (SecondOrderLeapFrog::Move / advanceVelocity,
+//               ParticleKinematics::Move).
 // Rebuild kernels take a gate: with a non-null gate they return at once
 // unless this step rebuilds (plain launches); inside the graph's conditional
 // node they run ungated.
@@ -235,16 +238,51 @@ __global__ void k_copyback(DevState S, const int* gate) {
     for (int k = 0; k < 9; ++k) S.basis[k * cap + t] = S.basis2[k * cap + t];
   }
   S.wrap[t] = 0;
+  const d3 x = ld3(S.x, cap, t);
+  S.posf[t] = make_float4((float)x.x, (float)x.y, (float)x.z,
+                          (float)S.types[S.type[t]].radius);
 }
 
-// Opening kick + drift with the stored F, T (the first step of a call).
-// Per particle only, so it runs in place (the launcher aliases the second
-// buffers to the current ones).
-__global__ void k_move_only(DevState S) {
+// Leapfrog of each particle with the stored F, T: the closing kick of the
+// step that ends (flags & kStepClose) and the opening kick + drift of the
+// next (flags & kStepMove).  Per particle only, so it runs in place (the
+// launcher aliases the second buffers to the current ones).
+__global__ void __launch_bounds__(256, 3) k_move(DevState S, int flags) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
   TypeDesc const& tp = S.types[S.type[t]];
-  advanceParticle(S, t, tp, ld3(S.F, S.cap, t), ld3(S.T, S.cap, t), false, true);
+  advanceParticle(S, t, tp, ld3(S.F, S.cap, t), ld3(S.T, S.cap, t),
+                  (flags & kStepClose) != 0, (flags & kStepMove) != 0);
+}
+
+// Contact filter: the entries of each particle's skin list whose bounding
+// spheres overlap now, tested on FP32 positions with an absolute margin that
+// covers their rounding (a superset of the contacts; the force kernels
+// decide each one exactly in FP64).
+__global__ void __launch_bounds__(256) k_filter(DevState S) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= S.n) return;
+  const int4 cc = S.cellc[t];
+  GridDesc const& bg = S.bgrids[cc.w];
+  const float4 pt = S.posf[t];
+  const int np = S.npairs[t];
+  const int* seg = S.pairs + (size_t)t * kPairCap;
+  int* out = S.act + (size_t)t * kPairCap;
+  int k = 0;
+  for (int e = 0; e < np; ++e) {
+    const int ent = seg[e];
+    const int u = ent & ((1 << 27) - 1);
+    int di, dj, dk, sh[3];
+    offDecode((unsigned)ent >> 27, &di, &dj, &dk);
+    entryShift(S, bg, cc, t, u, di, dj, dk, sh);
+    const float4 pu = S.posf[u];
+    const float dx = (pu.x - pt.x) + (float)sh[0] * bg.Lf[0];
+    const float dy = (pu.y - pt.y) + (float)sh[1] * bg.Lf[1];
+    const float dz = (pu.z - pt.z) + (float)sh[2] * bg.Lf[2];
+    const float R = pt.w + pu.w + bg.filt_margin;
+    if (dx * dx + dy * dy + dz * dz <= R * R) out[k++] = ent;
+  }
+  S.nact[t] = k;
 }
 
 // Scatter of sorted-order state into ID order (for download).
@@ -438,12 +476,15 @@ void launch_permute(DevState const& S, const int* gate, cudaStream_t st) {
 void launch_copyback(DevState const& S, const int* gate, cudaStream_t st) {
   if (S.n) k_copyback<<<blocks(S.n, 256), 256, 0, st>>>(S, gate);
 }
-void launch_move_only(DevState const& S, cudaStream_t st) {
+void launch_move(DevState const& S, int flags, cudaStream_t st) {
   if (!S.n) return;
   DevState M = S;   // in place: the "next" buffers are the current ones
   M.x2 = S.x; M.v2 = S.v; M.w2 = S.w; M.wbf2 = S.wbf; M.q2 = S.q; M.basis2 = S.basis;
   M.wrap2 = S.wrap;
-  k_move_only<<<blocks(S.n, 256), 256, 0, st>>>(M);
+  k_move<<<blocks(S.n, 256), 256, 0, st>>>(M, flags);
+}
+void launch_filter(DevState const& S, cudaStream_t st) {
+  if (S.n) k_filter<<<blocks(S.n, 256), 256, 0, st>>>(S);
 }
 void launch_fill64(unsigned long long* p, size_t n, unsigned long long value, cudaStream_t st) {
   if (n) k_fill64<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p, n, value);

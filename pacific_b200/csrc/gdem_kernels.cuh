@@ -4,12 +4,10 @@
 
 namespace gdem {
 
-// Step variants of the fused force + leapfrog kernels.
+// Parts of the leapfrog applied by k_move.
 enum StepFlags : int {
-  kStepForces = 1,    // evaluate contact forces (always set by the step kernels)
   kStepClose = 2,     // closing kick of the step that ends here (dt / 2)
   kStepMove = 4,      // opening kick (dt / 2) and drift (dt) of the next step
-  kStepStoreFT = 8,   // keep F and T (needed after the last evaluation of a call)
 };
 
 // gdem_integrate.cu
@@ -21,7 +19,8 @@ void launch_place(DevState const& S, const int* gate, cudaStream_t st);
 void launch_cellsort(DevState const& S, const int* gate, cudaStream_t st);
 void launch_permute(DevState const& S, const int* gate, cudaStream_t st);
 void launch_copyback(DevState const& S, const int* gate, cudaStream_t st);
-void launch_move_only(DevState const& S, cudaStream_t st);
+void launch_move(DevState const& S, int flags, cudaStream_t st);
+void launch_filter(DevState const& S, cudaStream_t st);
 void launch_fill64(unsigned long long* p, size_t n, unsigned long long value, cudaStream_t st);
 void launch_scatter_by_id(DevState const& S, double* x, double* v, double* w, double* wbf,
                           double* q, double* F, double* T, int id_base, cudaStream_t st);
@@ -36,10 +35,10 @@ void launch_pair_counts(DevState const& S, unsigned long long* out, cudaStream_t
 
 // gdem_contact64.cu (FP64 mode)
 void launch_pairs64(DevState const& S, const int* gate, cudaStream_t st);
-void launch_step64(DevState const& S, int flags, cudaStream_t st);
+void launch_forces64(DevState const& S, cudaStream_t st);
 
 // gdem_contact32.cu (FP32-split mode)
 void launch_pairs32(DevState const& S, const int* gate, cudaStream_t st);
-void launch_step32(DevState const& S, int flags, cudaStream_t st);
+void launch_forces32(DevState const& S, cudaStream_t st);
 
 }  // namespace gdem

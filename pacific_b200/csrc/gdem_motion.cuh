@@ -179,6 +179,7 @@ __device__ __forceinline__ void advanceParticle(DevState const& S, int t, TypeDe
     for (int k = 0; k < 9; ++k) S.basis2[k * cap + t] = bas[k];
   }
   S.wrap2[t] = wr;
+  S.posf[t] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)tp.radius);
 }
 
 // Image shift (in periods) between slot t and its list entry u found through

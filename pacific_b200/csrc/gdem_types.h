@@ -49,6 +49,9 @@ struct GridDesc {
   int pad0;
   float edge_f[3];       // edge in FP32 (FP32-split broad phase)
   float skin_f;          // pair-list skin in FP32
+  float filt_margin;     // absolute margin of the FP32 contact filter (covers rounding)
+  float Lf[3];           // domain size in FP32
+  float pad_f;
   double skin;           // pair-list skin: pairs closer than the sum of radii + skin are listed
 };
 
