@@ -174,9 +174,10 @@ def max_over_ranks(dist, value):
     return float(t.item())
 
 
-def make_system(xml, sc, precision):
+def make_system(xml, sc, precision, graphs=True):
     from pacific_b200 import Grains
     g = Grains(xml, precision)
+    g.use_graphs(graphs)
     g.upload_state(sc.type, sc.x, sc.v, sc.w, sc.q)
     g.do_before_time_stepping()
     return g
@@ -431,6 +432,8 @@ def main():
     ap.add_argument("--batched-instances", type=int, default=512)
     ap.add_argument("--batched-steps", type=int, default=50)
     ap.add_argument("--convex-n", type=int, default=200_000)
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="plain kernel launches instead of graph replay (for per-kernel profilers)")
     ap.add_argument("--convex-steps", type=int, default=200)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
@@ -455,7 +458,7 @@ def main():
 
     res = {}
     for name, prec in (("fp64", FP64), ("fp32_split", FP32_SPLIT)):
-        g = make_system(xml, sc, prec)
+        g = make_system(xml, sc, prec, graphs=not args.no_graphs)
         g.step(args.warmup)
         e0, r0 = g.step_counts()
         if name == "fp32_split":

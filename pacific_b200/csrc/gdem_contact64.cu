@@ -67,9 +67,13 @@ __device__ __forceinline__ void storeHist(HistTable const& t, int slot, d3 kd, d
 // kConvex: some class is not a sphere, so the GJK narrow phase is compiled in
 // (it is kept out of the sphere-only kernel, whose registers it would triple).
 template <bool kConvex>
-__global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_forces64(DevState S) {
+__global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_forces64(DevState S, int sparse) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
+  // sparse: a particle without listed contact and away from the walls keeps
+  // its weight, which k_move applies without reading F, T
+  const int na = S.nact[t];
+  if (sparse && na == 0) return;
   const int cap = S.cap;
   const int4 cc = S.cellc[t];
   GridDesc const& g = S.grids[cc.w];
@@ -81,7 +85,7 @@ __global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_forces64(DevState S) {
   d3 T = mk(0., 0., 0.);
   const double dt = S.dt;
   const unsigned tag = (unsigned)S.ctl[kCtlEpoch], tag_old = tag - 1u;
-  const int np = S.nact[t];
+  const int np = na & kActMask;
   const int* seg = S.act + (size_t)t * kPairCap;
   for (int e = 0; e < np; ++e) {
     const uint32_t ent = (uint32_t)seg[e];
@@ -156,7 +160,8 @@ __global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_forces64(DevState S) {
     }
   }
   // walls: the particle is p0, the obstacle p1 (mass Component::m_massObstacle)
-  for (int k = 0; k < g.wall_count; ++k) {
+  const int nwalls = (!sparse || (na & kNearWall)) ? g.wall_count : 0;
+  for (int k = 0; k < nwalls; ++k) {
     WallDesc const& wd = S.walls[g.wall_begin + k];
     Contact64 ct = (!kConvex || ta.shape == 0)
         ? sphereWall64(xt, ta.radius, ta.crust, wd)
@@ -202,10 +207,10 @@ __global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_forces64(DevState S) {
 void launch_pairs64(DevState const& S, const int* gate, cudaStream_t st) {
   if (S.n) k_pairs64<<<(S.n + 255) / 256, 256, 0, st>>>(S, gate);
 }
-void launch_forces64(DevState const& S, cudaStream_t st) {
+void launch_forces64(DevState const& S, int sparse, cudaStream_t st) {
   if (!S.n) return;
-  if (S.any_convex) k_forces64<true><<<(S.n + 255) / 256, 256, 0, st>>>(S);
-  else k_forces64<false><<<(S.n + 255) / 256, 256, 0, st>>>(S);
+  if (S.any_convex) k_forces64<true><<<(S.n + 255) / 256, 256, 0, st>>>(S, sparse);
+  else k_forces64<false><<<(S.n + 255) / 256, 256, 0, st>>>(S, sparse);
 }
 
 }  // namespace gdem

@@ -724,8 +724,12 @@ struct System {
   // leapfrog start).
   void forcesAndMove(int flags) {
     timed("filter", [&] { launch_filter(S, stream); });
-    if (precision == GDEM_FP64) timed("forces64", [&] { launch_forces64(S, stream); });
-    else timed("forces32", [&] { launch_forces32(S, stream); });
+    // the leapfrog start evaluates every particle; later evaluations skip the
+    // particles without contact (k_move applies their weight), except with
+    // diagnostics on, which record every particle's wall overlaps
+    const int sparse = (flags && !diag) ? 1 : 0;
+    if (precision == GDEM_FP64) timed("forces64", [&] { launch_forces64(S, sparse, stream); });
+    else timed("forces32", [&] { launch_forces32(S, sparse, stream); });
     if (flags) timed("move", [&] { launch_move(S, flags, stream); });
   }
   // One force evaluation with plain launches: decide, gated rebuild, filter,
@@ -819,7 +823,7 @@ struct System {
     CK(cudaEventRecord(ev0, stream));
     timed("move", [&] { launch_move(S, kStepMove, stream); });
     const int mid = kStepClose | kStepMove;
-    const int last = kStepClose;
+    const int last = kStepClose | kStepStoreFT;
     const bool graphs = use_graphs && !diag && !profiling;
     for (int k = 0; k < nsteps; ++k) {
       const bool is_last = k == nsteps - 1;
@@ -1236,8 +1240,8 @@ int gdem_download_contacts(gdem_handle h, int64_t capacity, int64_t* count, int*
     CK(cudaMemcpy(cells.data(), S.cellc, n * sizeof(int4), cudaMemcpyDeviceToHost));
     int64_t c = 0;
     for (size_t t = 0; t < n; ++t) {
-      for (int e = 0; e < np[t]; ++e) {
-        int u = pairs[t * kPairCap + e] & ((1 << 27) - 1);
+      for (int e = 0; e < (np[t] & kActMask); ++e) {
+        int u = pairs[t * kPairCap + e] & ((1 << 27) - 1);   // entries of act
         size_t slot = t * kPairCap + e;
         double dl = pd[slot];
         if (!(dl < 0.) || !(ids[t] < ids[u])) continue;

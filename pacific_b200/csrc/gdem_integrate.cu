@@ -247,12 +247,23 @@ __global__ void k_copyback(DevState S, const int* gate) {
 // step that ends (flags & kStepClose) and the opening kick + drift of the
 // next (flags & kStepMove).  Per particle only, so it runs in place (the
 // launcher aliases the second buffers to the current ones).
+// A particle that the contact filter left without contact carries only its
+// weight: the force kernel skipped it and its F, T are taken as such here
+// (and written back at the end of a call, kStepStoreFT).
 __global__ void __launch_bounds__(256, 3) k_move(DevState S, int flags) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
   TypeDesc const& tp = S.types[S.type[t]];
-  advanceParticle(S, t, tp, ld3(S.F, S.cap, t), ld3(S.T, S.cap, t),
-                  (flags & kStepClose) != 0, (flags & kStepMove) != 0);
+  d3 F, T;
+  if ((flags & kStepClose) && S.nact[t] == 0) {
+    F = mk(tp.weight[0], tp.weight[1], tp.weight[2]);
+    T = mk(0., 0., 0.);
+    if (flags & kStepStoreFT) { st3(S.F, S.cap, t, F); st3(S.T, S.cap, t, T); }
+  } else {
+    F = ld3(S.F, S.cap, t);
+    T = ld3(S.T, S.cap, t);
+  }
+  advanceParticle(S, t, tp, F, T, (flags & kStepClose) != 0, (flags & kStepMove) != 0);
 }
 
 // Contact filter: the entries of each particle's skin list whose bounding
@@ -282,7 +293,23 @@ __global__ void __launch_bounds__(256) k_filter(DevState S) {
     const float R = pt.w + pu.w + bg.filt_margin;
     if (dx * dx + dy * dy + dz * dz <= R * R) out[k++] = ent;
   }
-  S.nact[t] = k;
+  // walls (axis-aligned boxes): distance from the centre to the box against
+  // the bounding radius
+  GridDesc const& g = S.grids[cc.w];
+  bool near = false;
+  for (int w = 0; w < g.wall_count && !near; ++w) {
+    WallDesc const& wd = S.walls[g.wall_begin + w];
+    const float p[3] = {pt.x, pt.y, pt.z};
+    float d2 = 0.f;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const float o = fabsf(p[d] - (float)wd.centre[d]) - (float)wd.extent[d];
+      if (o > 0.f) d2 += o * o;
+    }
+    const float R = pt.w + bg.filt_margin;
+    near = d2 <= R * R;
+  }
+  S.nact[t] = k | (near ? kNearWall : 0);
 }
 
 // Scatter of sorted-order state into ID order (for download).

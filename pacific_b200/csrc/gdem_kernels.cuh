@@ -8,7 +8,11 @@ namespace gdem {
 enum StepFlags : int {
   kStepClose = 2,     // closing kick of the step that ends here (dt / 2)
   kStepMove = 4,      // opening kick (dt / 2) and drift (dt) of the next step
+  kStepStoreFT = 8,   // write F, T of particles without contact (last step of a call)
 };
+// nact[t] = number of entries kept | kNearWall when a wall may touch t.
+constexpr int kNearWall = 1 << 16;
+constexpr int kActMask = kNearWall - 1;
 
 // gdem_integrate.cu
 void launch_decide(DevState const& S, cudaGraphConditionalHandle h, int use_handle,
@@ -35,10 +39,10 @@ void launch_pair_counts(DevState const& S, unsigned long long* out, cudaStream_t
 
 // gdem_contact64.cu (FP64 mode)
 void launch_pairs64(DevState const& S, const int* gate, cudaStream_t st);
-void launch_forces64(DevState const& S, cudaStream_t st);
+void launch_forces64(DevState const& S, int sparse, cudaStream_t st);
 
 // gdem_contact32.cu (FP32-split mode)
 void launch_pairs32(DevState const& S, const int* gate, cudaStream_t st);
-void launch_forces32(DevState const& S, cudaStream_t st);
+void launch_forces32(DevState const& S, int sparse, cudaStream_t st);
 
 }  // namespace gdem

@@ -137,8 +137,9 @@ def test_gpu_fp64_step_matches_reference(tmp_path, lib, name):
             # call to call in its serial order), the device search starts at
             # vertex 0.  Such contacts agree in overlap and normal but their
             # contact point can move within the contact face.
-            assert np.mean(fe <= 1e-10) >= 0.8 and fe.max(initial=0) <= 1e-5
-            assert np.mean(te <= 1e-10) >= 0.8 and te.max(initial=0) <= 1e-4
+            if fe.size:
+                assert np.mean(fe <= 1e-10) >= 0.8 and fe.max() <= 1e-5
+                assert np.mean(te <= 1e-10) >= 0.8 and te.max() <= 1e-4
         else:
             assert fe.max(initial=0) <= 1e-10 and te.max(initial=0) <= 1e-10
 
