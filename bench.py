@@ -346,14 +346,14 @@ def convex_measure(n, steps, warmup=3):
     """Cubes (2 mm) and regular tetrahedra (3 mm edge) poured into a
     0.1 x 0.1 x 0.3 m box (GJK narrow phase, 3D rotation).  Two starts: the
     pour as specified (at rest on the lattice: no contact for the first ~9,800
-    steps) and the same lattice launched at up to 0.5 m/s per component so
-    that the timed steps are collisional.  Device time per step in FP64 and
+    steps) and the same lattice launched at up to 2 m/s per component so that
+    the timed steps are collisional.  Device time per step in FP64 and
     FP32-split, with the FP64 re-evaluation count of FP32-split."""
     from pacific_b200 import FP32_SPLIT, FP64, Grains, scenarios
     out = {"workload": f"convex_pour n={n} (cubes + tetrahedra), dt=2e-6", "steps": steps}
     with tempfile.TemporaryDirectory() as d:
         poly = scenarios.write_tetrahedron(Path(d) / "tet.poly")
-        for label, vmax in (("at_rest", 0.0), ("collisional", 0.5)):
+        for label, vmax in (("at_rest", 0.0), ("collisional", 2.0)):
             sc = scenarios.convex_pour(n=n, seed=1238, poly_path=poly, vmax=vmax)
             xml = str(sc.write_xml(Path(d) / f"convex_{label}.xml"))
             row = {}
@@ -434,7 +434,7 @@ def main():
     ap.add_argument("--convex-n", type=int, default=200_000)
     ap.add_argument("--no-graphs", action="store_true",
                     help="plain kernel launches instead of graph replay (for per-kernel profilers)")
-    ap.add_argument("--convex-steps", type=int, default=200)
+    ap.add_argument("--convex-steps", type=int, default=500)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

@@ -21,6 +21,8 @@
 // (Geometry/src/RigidBodyWithCrust.cpp:596-639), HookeMemoryContactForceModel
 // (Component/src/HookeMemoryContactForceModel.cpp:54-249), Torsor::addForce
 // (Component/src/Torsor.cpp:184-189).
+#include <algorithm>
+
 #include "gdem_contact_common.cuh"
 #include "gdem_kernels.cuh"
 #include "gdem_motion.cuh"
@@ -272,7 +274,7 @@ __global__ void __launch_bounds__(256) k_pairs32(DevState S, const int* gate) {
   int cnt = 0;
   const float4* __restrict__ offh = S.offh;
   const float ex = g.edge_f[0], ey = g.edge_f[1], ez = g.edge_f[2];
-  forEachCandidate(S.cell_start, g, cc, [&](int u, int dcx, int dj, int dk, int, int, int) {
+  forEachCandidate(S.cell_start, g, cc, [&](int u, int dcx, int dj, int dk, int sx, int sy, int sz) {
     if (u == t) return;
     const float4 hb = offh[u];
     // lower slot first, so both directions of a pair evaluate the same
@@ -285,7 +287,7 @@ __global__ void __launch_bounds__(256) k_pairs32(DevState S, const int* gate) {
     float dz = fmaf(s * (float)dk, ez, h1.z - h0.z);
     float R = (h0.w + h1.w + g.skin_f) * (1.f + 4.e-6f);
     if (dx * dx + dy * dy + dz * dz > R * R) return;
-    if (cnt < kPairCap) out[cnt] = u | (offCode(dcx, dj, dk) << 27);
+    if (cnt < kPairCap) out[cnt] = u | (shiftCode(sx, sy, sz) << 27);
     ++cnt;
   });
   if (cnt > kPairCap) { raise(S.status, kErrPairsFull); cnt = kPairCap; }
@@ -296,30 +298,21 @@ __global__ void __launch_bounds__(256) k_pairs32(DevState S, const int* gate) {
 // kConvex: some class is not a sphere, so the GJK narrow phase is compiled in
 // (it is kept out of the sphere-only kernel, whose registers it would triple).
 template <bool kConvex>
-__global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_forces32(DevState S, int sparse) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= S.n) return;
-  // sparse: a particle without listed contact and away from the walls keeps
-  // its weight, which k_move applies without reading F, T
-  const int na = S.nact[t];
-  if (sparse && na == 0) return;
+__device__ __forceinline__ void forcesOn32(DevState const& S, int t, int na, int sparse,
+                                           int& nlaw, int& nre) {
   const int cap = S.cap;
   const int4 cc = S.cellc[t];
   GridDesc const& g = S.grids[cc.w];
-  GridDesc const& bg = S.bgrids[cc.w];
   const unsigned tag = (unsigned)S.ctl[kCtlEpoch], tag_old = tag - 1u;
   const int ida = S.id[t];
   TypeDesc const& ta = S.types[S.type[t]];
   const d3 xt = ld3(S.x, cap, t);
   float3 Fs = f3(0.f, 0.f, 0.f), Ts = f3(0.f, 0.f, 0.f);
-  int nlaw = 0, nre = 0;   // contacts evaluated / re-evaluated in FP64
   const int np = na & kActMask;
   const int* seg = S.act + (size_t)t * kPairCap;
   for (int e = 0; e < np; ++e) {
     const uint32_t ent = (uint32_t)seg[e];
     const int u = (int)(ent & ((1u << 27) - 1));
-    int di, dj, dk;
-    offDecode((int)(ent >> 27), &di, &dj, &dk);
     const int idb = S.id[u];
     const bool t0 = ida < idb;
     TypeDesc const& tb = S.types[S.type[u]];
@@ -329,7 +322,7 @@ __global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_forces32(DevState S, i
     // exact narrow phase on the FP64 master positions: lower ID at its own
     // position, the other at its periodic image seen from it
     int sh[3];
-    entryShift(S, bg, cc, t, u, di, dj, dk, sh);
+    entryShift(S, ent, t, u, sh);
     const d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
     const d3 xu = ld3(S.x, cap, u);
     const d3 x0 = t0 ? xt : xu;
@@ -430,10 +423,24 @@ __global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_forces32(DevState S, i
   const d3 T = mk((double)Ts.x, (double)Ts.y, (double)Ts.z);
   st3(S.F, cap, t, F);
   st3(S.T, cap, t, T);
-  // warp-aggregated counters of the FP64 re-evaluations
-  const unsigned mask = __activemask();
-  const int wl = __reduce_add_sync(mask, nlaw), wr = __reduce_add_sync(mask, nre);
-  if ((threadIdx.x & 31) == __ffs(mask) - 1 && wl) {
+}
+
+// Persistent grid.  sparse: only the particles of the work list (those with
+// a listed contact or near a wall); the others keep their weight, which
+// k_move applies without reading F, T.  Otherwise every particle.
+template <bool kConvex>
+__global__ void __launch_bounds__(256) k_forces32(DevState S, int sparse) {
+  const int stride = gridDim.x * blockDim.x;
+  const int nw = sparse ? S.ctl[kCtlWork] : S.n;
+  int nlaw = 0, nre = 0;   // contacts evaluated / re-evaluated in FP64
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += stride) {
+    const int t = sparse ? S.work[i] : i;
+    forcesOn32<kConvex>(S, t, S.nact[t], sparse, nlaw, nre);
+  }
+  // warp-aggregated counters of the FP64 re-evaluations (every lane of the
+  // warp reaches this point: no thread leaves the loop early)
+  const int wl = __reduce_add_sync(0xffffffffu, nlaw), wr = __reduce_add_sync(0xffffffffu, nre);
+  if ((threadIdx.x & 31) == 0 && wl) {
     atomicAdd(S.law_counts, (unsigned long long)wl);
     if (wr) atomicAdd(S.law_counts + 1, (unsigned long long)wr);
   }
@@ -446,8 +453,9 @@ void launch_pairs32(DevState const& S, const int* gate, cudaStream_t st) {
 }
 void launch_forces32(DevState const& S, int sparse, cudaStream_t st) {
   if (!S.n) return;
-  if (S.any_convex) k_forces32<true><<<(S.n + 255) / 256, 256, 0, st>>>(S, sparse);
-  else k_forces32<false><<<(S.n + 255) / 256, 256, 0, st>>>(S, sparse);
+  const int grid = std::min((S.n + 255) / 256, 4 * S.nsm);
+  if (S.any_convex) k_forces32<true><<<grid, 256, 0, st>>>(S, sparse);
+  else k_forces32<false><<<grid, 256, 0, st>>>(S, sparse);
 }
 
 }  // namespace gdem

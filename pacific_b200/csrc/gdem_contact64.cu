@@ -16,6 +16,8 @@
 //               torque over those entries in list (partner-ID) order, then its
 //               wall contacts (SimpleObstacle::InterAction, Component/src/
 //               SimpleObstacle.cpp:222-271).
+#include <algorithm>
+
 #include "gdem_contact_common.cuh"
 #include "gdem_kernels.cuh"
 #include "gdem_motion.cuh"
@@ -46,7 +48,7 @@ __global__ void __launch_bounds__(256) k_pairs64(DevState S, const int* gate) {
                  : (mk(pa.x, pa.y, pa.z) + (-shift)) - mk(pb.x, pb.y, pb.z);
     double R = pa.w + pb.w;
     if (norm(d) - R > g.skin + 1.0e-12 * R) return;
-    if (cnt < kPairCap) out[cnt] = u | (offCode(dcx, dj, dk) << 27);
+    if (cnt < kPairCap) out[cnt] = u | (shiftCode(sx, sy, sz) << 27);
     ++cnt;
   });
   if (cnt > kPairCap) { raise(S.status, kErrPairsFull); cnt = kPairCap; }
@@ -67,17 +69,10 @@ __device__ __forceinline__ void storeHist(HistTable const& t, int slot, d3 kd, d
 // kConvex: some class is not a sphere, so the GJK narrow phase is compiled in
 // (it is kept out of the sphere-only kernel, whose registers it would triple).
 template <bool kConvex>
-__global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_forces64(DevState S, int sparse) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= S.n) return;
-  // sparse: a particle without listed contact and away from the walls keeps
-  // its weight, which k_move applies without reading F, T
-  const int na = S.nact[t];
-  if (sparse && na == 0) return;
+__device__ __forceinline__ void forcesOn64(DevState const& S, int t, int na, int sparse) {
   const int cap = S.cap;
   const int4 cc = S.cellc[t];
   GridDesc const& g = S.grids[cc.w];
-  GridDesc const& bg = S.bgrids[cc.w];
   const int ida = S.id[t];
   TypeDesc const& ta = S.types[S.type[t]];
   const d3 xt = ld3(S.x, cap, t), vt = ld3(S.v, cap, t), wt = ld3(S.w, cap, t);
@@ -90,9 +85,8 @@ __global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_forces64(DevState S, i
   for (int e = 0; e < np; ++e) {
     const uint32_t ent = (uint32_t)seg[e];
     const int u = (int)(ent & ((1u << 27) - 1));
-    int di, dj, dk, sh[3];
-    offDecode((int)(ent >> 27), &di, &dj, &dk);
-    entryShift(S, bg, cc, t, u, di, dj, dk, sh);
+    int sh[3];
+    entryShift(S, ent, t, u, sh);
     d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
     const int idb = S.id[u];
     TypeDesc const& tb = S.types[S.type[u]];
@@ -202,6 +196,19 @@ __global__ void __launch_bounds__(256, kConvex ? 1 : 2) k_forces64(DevState S, i
   st3(S.T, cap, t, T);
 }
 
+// Persistent grid.  sparse: only the particles of the work list (those with
+// a listed contact or near a wall); the others keep their weight, which
+// k_move applies without reading F, T.  Otherwise every particle.
+template <bool kConvex>
+__global__ void __launch_bounds__(256) k_forces64(DevState S, int sparse) {
+  const int stride = gridDim.x * blockDim.x;
+  const int nw = sparse ? S.ctl[kCtlWork] : S.n;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += stride) {
+    const int t = sparse ? S.work[i] : i;
+    forcesOn64<kConvex>(S, t, S.nact[t], sparse);
+  }
+}
+
 }  // namespace
 
 void launch_pairs64(DevState const& S, const int* gate, cudaStream_t st) {
@@ -209,8 +216,9 @@ void launch_pairs64(DevState const& S, const int* gate, cudaStream_t st) {
 }
 void launch_forces64(DevState const& S, int sparse, cudaStream_t st) {
   if (!S.n) return;
-  if (S.any_convex) k_forces64<true><<<(S.n + 255) / 256, 256, 0, st>>>(S, sparse);
-  else k_forces64<false><<<(S.n + 255) / 256, 256, 0, st>>>(S, sparse);
+  const int grid = std::min((S.n + 255) / 256, 4 * S.nsm);
+  if (S.any_convex) k_forces64<true><<<grid, 256, 0, st>>>(S, sparse);
+  else k_forces64<false><<<grid, 256, 0, st>>>(S, sparse);
 }
 
 }  // namespace gdem

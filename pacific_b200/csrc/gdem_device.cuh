@@ -124,6 +124,8 @@ struct DevState {
   int* pairs; int* npairs;   // skin list (rebuilt on demand)
   int* act; int* nact;       // entries of the skin list in contact this step (same layout)
   float4* posf;           // FP32 position + circumscribed radius (contact filter)
+  int* work;              // particles with a listed contact or near a wall (this step)
+  int nsm;                // multiprocessors of the device (persistent grids)
   double* pair_delta;     // diagnostics: overlap of each entry (+inf: no contact)
   double* wall_delta;     // diagnostics: overlap with each wall slot
   double* pair_force;     // diagnostics: contact force on the lower ID (3 per entry)
@@ -289,6 +291,11 @@ __device__ __forceinline__ void sortEntriesById(int* seg, int cnt, const int* id
     }
     seg[j + 1] = e;
   }
+}
+
+// Code of a periodic image shift (in periods, each -1, 0 or 1) in 0..26.
+__device__ __forceinline__ int shiftCode(int sx, int sy, int sz) {
+  return (sx + 1) + 3 * (sy + 1) + 9 * (sz + 1);
 }
 
 // Code of a stencil offset in 0..26 and back.

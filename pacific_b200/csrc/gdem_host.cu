@@ -454,6 +454,16 @@ InstanceDesc readInstance(std::string const& path) {
   }
   b.filt_margin = (float)(5.e-7 * maxabs);
   g.filt_margin = b.filt_margin;
+  // band in which a particle stays in the reference grid's inner cells
+  // (periodic: cells 1 .. nb-2; otherwise 0 .. nb-1), with a relative margin
+  // of 1e-6 of a cell that dwarfs the rounding of the cell computation
+  for (int d = 0; d < 3; ++d) {
+    const double lo_cell = per[d] ? 1. : 0., hi_cell = per[d] ? g.nb[d] - 1. : (double)g.nb[d];
+    g.safe_lo[d] = g.lc_origin[d] + (lo_cell + 1.e-6) * g.edge[d];
+    g.safe_hi[d] = g.lc_origin[d] + (hi_cell - 1.e-6) * g.edge[d];
+    b.safe_lo[d] = g.safe_lo[d];
+    b.safe_hi[d] = g.safe_hi[d];
+  }
   return I;
 }
 
@@ -645,6 +655,12 @@ struct System {
     }
     S.pairs = alloc<int>(c * kPairCap); S.npairs = alloc<int>(c);
     S.act = alloc<int>(c * kPairCap); S.nact = alloc<int>(c);
+    S.work = alloc<int>(c);
+    {
+      int dev = 0;
+      CK(cudaGetDevice(&dev));
+      CK(cudaDeviceGetAttribute(&S.nsm, cudaDevAttrMultiProcessorCount, dev));
+    }
     S.posf = alloc<float4>(c);
     S.pair_delta = nullptr; S.wall_delta = nullptr; S.diag = 0;
     S.pair_force = nullptr; S.wall_force = nullptr;

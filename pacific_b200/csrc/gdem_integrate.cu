@@ -45,6 +45,7 @@ __global__ void k_decide(DevState S, cudaGraphConditionalHandle h, int use_handl
   S.ctl[kCtlNeed] = 0;
   S.ctl[kCtlEpoch] += 1;
   S.ctl[kCtlRebuilds] += need ? 1 : 0;
+  S.ctl[kCtlWork] = 0;
   if (use_handle) cudaGraphSetConditional(h, need ? 1u : 0u);
 }
 
@@ -271,45 +272,56 @@ __global__ void __launch_bounds__(256, 3) k_move(DevState S, int flags) {
 // covers their rounding (a superset of the contacts; the force kernels
 // decide each one exactly in FP64).
 __global__ void __launch_bounds__(256) k_filter(DevState S) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= S.n) return;
-  const int4 cc = S.cellc[t];
-  GridDesc const& bg = S.bgrids[cc.w];
-  const float4 pt = S.posf[t];
-  const int np = S.npairs[t];
-  const int* seg = S.pairs + (size_t)t * kPairCap;
-  int* out = S.act + (size_t)t * kPairCap;
-  int k = 0;
-  for (int e = 0; e < np; ++e) {
-    const int ent = seg[e];
-    const int u = ent & ((1 << 27) - 1);
-    int di, dj, dk, sh[3];
-    offDecode((unsigned)ent >> 27, &di, &dj, &dk);
-    entryShift(S, bg, cc, t, u, di, dj, dk, sh);
-    const float4 pu = S.posf[u];
-    const float dx = (pu.x - pt.x) + (float)sh[0] * bg.Lf[0];
-    const float dy = (pu.y - pt.y) + (float)sh[1] * bg.Lf[1];
-    const float dz = (pu.z - pt.z) + (float)sh[2] * bg.Lf[2];
-    const float R = pt.w + pu.w + bg.filt_margin;
-    if (dx * dx + dy * dy + dz * dz <= R * R) out[k++] = ent;
-  }
-  // walls (axis-aligned boxes): distance from the centre to the box against
-  // the bounding radius
-  GridDesc const& g = S.grids[cc.w];
-  bool near = false;
-  for (int w = 0; w < g.wall_count && !near; ++w) {
-    WallDesc const& wd = S.walls[g.wall_begin + w];
-    const float p[3] = {pt.x, pt.y, pt.z};
-    float d2 = 0.f;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const float o = fabsf(p[d] - (float)wd.centre[d]) - (float)wd.extent[d];
-      if (o > 0.f) d2 += o * o;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int flag = 0;
+  if (t < S.n) {
+    const int4 cc = S.cellc[t];
+    GridDesc const& bg = S.bgrids[cc.w];
+    const float4 pt = S.posf[t];
+    const int np = S.npairs[t];
+    const int* seg = S.pairs + (size_t)t * kPairCap;
+    int* out = S.act + (size_t)t * kPairCap;
+    int k = 0;
+    for (int e = 0; e < np; ++e) {
+      const int ent = seg[e];
+      const int u = ent & ((1 << 27) - 1);
+      int sh[3];
+      entryShift(S, (unsigned)ent, t, u, sh);
+      const float4 pu = S.posf[u];
+      const float dx = (pu.x - pt.x) + (float)sh[0] * bg.Lf[0];
+      const float dy = (pu.y - pt.y) + (float)sh[1] * bg.Lf[1];
+      const float dz = (pu.z - pt.z) + (float)sh[2] * bg.Lf[2];
+      const float R = pt.w + pu.w + bg.filt_margin;
+      if (dx * dx + dy * dy + dz * dz <= R * R) out[k++] = ent;
     }
-    const float R = pt.w + bg.filt_margin;
-    near = d2 <= R * R;
+    // walls (axis-aligned boxes): distance from the centre to the box against
+    // the bounding radius
+    GridDesc const& g = S.grids[cc.w];
+    bool near = false;
+    for (int w = 0; w < g.wall_count && !near; ++w) {
+      WallDesc const& wd = S.walls[g.wall_begin + w];
+      const float p[3] = {pt.x, pt.y, pt.z};
+      float d2 = 0.f;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const float o = fabsf(p[d] - (float)wd.centre[d]) - (float)wd.extent[d];
+        if (o > 0.f) d2 += o * o;
+      }
+      const float R = pt.w + bg.filt_margin;
+      near = d2 <= R * R;
+    }
+    flag = k | (near ? kNearWall : 0);
+    S.nact[t] = flag;
   }
-  S.nact[t] = k | (near ? kNearWall : 0);
+  // work list of the force kernel, appended once per warp
+  const unsigned ballot = __ballot_sync(0xffffffffu, flag != 0);
+  if (ballot) {
+    const int lane = threadIdx.x & 31;
+    int base = 0;
+    if (lane == 0) base = atomicAdd(&S.ctl[kCtlWork], __popc(ballot));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (flag) S.work[base + __popc(ballot & ((1u << lane) - 1))] = t;
+  }
 }
 
 // Scatter of sorted-order state into ID order (for download).

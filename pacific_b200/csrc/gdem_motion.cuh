@@ -77,6 +77,8 @@ __device__ __forceinline__ void wrapToGrid(GridDesc const& g, d3& x, int* wrapd,
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     wrapd[d] = 0;
+    // well inside the inner cells: the cell test below cannot trigger
+    if (xs[d] > g.safe_lo[d] && xs[d] < g.safe_hi[d]) continue;
     int id = (int)floor((xs[d] - g.lc_origin[d]) / g.edge[d]);
     if (g.periodic[d]) {
       if (id < 1) { xs[d] = xs[d] + g.L[d]; wrapd[d] = -1; }
@@ -182,12 +184,13 @@ __device__ __forceinline__ void advanceParticle(DevState const& S, int t, TypeDe
   S.posf[t] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)tp.radius);
 }
 
-// Image shift (in periods) between slot t and its list entry u found through
-// pair-list cell offset (di, dj, dk) of t's rebuild-time cell cc, corrected by
-// the wraps of both particles since the rebuild.
-__device__ __forceinline__ void entryShift(DevState const& S, GridDesc const& bg, int4 cc, int t,
-                                           int u, int di, int dj, int dk, int* sh) {
-  neighbourKey(bg, cc.x, cc.y, cc.z, di, dj, dk, sh);
+// Image shift (in periods) of list entry ent (partner u) of slot t: the
+// shift recorded at the rebuild (bits 27-31 of the entry, shiftCode),
+// corrected by the wraps of both particles since the rebuild.
+__device__ __forceinline__ void entryShift(DevState const& S, unsigned ent, int t, int u,
+                                           int* sh) {
+  const int c = (int)(ent >> 27);
+  sh[0] = c % 3 - 1; sh[1] = (c / 3) % 3 - 1; sh[2] = c / 9 - 1;
   const int wt = S.wrap[t], wu = S.wrap[u];
   if (wt | wu) {
 #pragma unroll

@@ -31,7 +31,8 @@ enum CtlWords : int {
   kCtlActive = 1,   // this step rebuilds the pair list (set by k_decide)
   kCtlEpoch = 2,    // force evaluations so far (tags the contact-history keys)
   kCtlRebuilds = 3, // pair-list rebuilds so far
-  kCtlWords = 4
+  kCtlWork = 4,     // particles the force kernel must evaluate this step (work list length)
+  kCtlWords = 8
 };
 
 // One independent simulation ("instance").  A single Grains3D system is a
@@ -53,6 +54,7 @@ struct GridDesc {
   float Lf[3];           // domain size in FP32
   float pad_f;
   double skin;           // pair-list skin: pairs closer than the sum of radii + skin are listed
+  double safe_lo[3], safe_hi[3];  // coordinates strictly inside these need no wrap or grid check
 };
 
 // Particle class (a <Particle> node of the XML input).
