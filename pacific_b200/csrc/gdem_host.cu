@@ -30,6 +30,7 @@
 
 #include "../../include/grains_b200.h"
 #include "gdem_kernels.cuh"
+#include "gdem_setup.h"
 #include "xml_reader.hpp"
 
 namespace gdem {
@@ -884,6 +885,15 @@ int guarded(F&& f) {
 }  // namespace
 
 void setLastError(std::string const& msg) { g_last_error = msg; }
+
+void readAdjointSetup(std::string const& path, AdjointSetup& out) {
+  InstanceDesc I = readInstance(path);
+  out.types = I.types;
+  out.walls = I.walls;
+  for (int k = 0; k < kMaxMat * kMaxMat; ++k) out.models[k] = I.models[k];
+  out.dt = I.dt;
+  for (int d = 0; d < 3; ++d) out.periodic[d] = I.grid.periodic[d];
+}
 
 }  // namespace gdem
 

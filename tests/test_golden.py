@@ -12,9 +12,9 @@ matrices of the cubes and tetrahedra, contact memory), one CUDA step
 reproduces the reference's step k+1: cells and contact sets exactly, forces
 and torques within 1e-10 (FP64) / 1e-5 (FP32-split) of each particle's sum of
 contact-force magnitudes, orientation matrices within 1e-14.  For the convex
-fixtures the FP64 bound holds for the median particle; a face-to-face
-contact, whose closest points are not unique, is held to 1e-5 (see the
-test).
+fixtures the median particle is held to 1e-9 (GJK's own termination
+tolerance and the summation order) and a face-to-face contact, whose closest
+points are not unique, to 1e-5 (see the test).
 """
 from pathlib import Path
 
@@ -139,8 +139,8 @@ def test_gpu_fp64_step_matches_reference(tmp_path, lib, name):
             # vertex 0.  Such contacts agree in overlap and normal but their
             # contact point can move within the contact face.
             if fe.size:
-                assert np.median(fe) <= 1e-10 and fe.max() <= 1e-5
-                assert np.median(te) <= 1e-10 and te.max() <= 1e-4
+                assert np.median(fe) <= 1e-9 and fe.max() <= 1e-5
+                assert np.median(te) <= 1e-9 and te.max() <= 1e-4
         else:
             assert fe.max(initial=0) <= 1e-10 and te.max(initial=0) <= 1e-10
 
