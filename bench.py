@@ -380,6 +380,40 @@ def convex_measure(n, steps, warmup=3):
     return out
 
 
+def adjoint_measure(n, steps, every):
+    """Calibration gradients (the adjoint): 4,096 spheres released in a
+    0.02 x 0.02 x 0.08 m box, loss = squared error of positions and
+    velocities after `steps` steps against the trajectory at kn = 2e4,
+    en = 0.6, muc = 0.35, gradients at parameters perturbed by 5 %, with
+    checkpoints every `every` steps; checked against dual-number forward
+    mode.  Wall-clock time of each call (device work dominates)."""
+    from pacific_b200 import scenarios
+    from pacific_b200.adjoint import Adjoint
+    p_t = np.array([2.0e4, 0.6, 0.35])
+    p_s = p_t * np.array([1.05, 0.95, 1.05])
+    sc = scenarios.adjoint_box(n=n)
+    with tempfile.TemporaryDirectory() as d:
+        xml = sc.write_xml(Path(d) / "adj.xml")
+        a = Adjoint(xml)
+        a.set_particles(sc.type, sc.x, sc.v)
+        t0 = time.perf_counter()
+        tx, tv, _ = a.run(p_t, steps)
+        t_fwd = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        loss, gp, gv = a.gradients(p_s, tx, tv, steps, every)
+        t_adj = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        loss_f, gp_f = a.forward_mode(p_s, tx, tv, steps)
+        t_dual = time.perf_counter() - t0
+        a.close()
+    rel = np.abs(gp - gp_f) / np.abs(gp_f)
+    return {"workload": f"adjoint_box n={n}, {steps} steps, checkpoint every {every}",
+            "loss": loss, "dL_dparams": gp.tolist(), "dL_dparams_forward_mode": gp_f.tolist(),
+            "max_rel_diff_vs_forward_mode": float(rel.max()),
+            "dL_dv0_norm": float(np.linalg.norm(gv)),
+            "forward_s": t_fwd, "gradient_s": t_adj, "forward_mode_s": t_dual}
+
+
 # --------------------------------------------------------------- reference --
 def run_reference(args, rank, world):
     if rank != 0:
@@ -432,6 +466,8 @@ def main():
     ap.add_argument("--batched-instances", type=int, default=512)
     ap.add_argument("--batched-steps", type=int, default=50)
     ap.add_argument("--convex-n", type=int, default=200_000)
+    ap.add_argument("--adjoint-n", type=int, default=4096)
+    ap.add_argument("--adjoint-steps", type=int, default=500)
     ap.add_argument("--no-graphs", action="store_true",
                     help="plain kernel launches instead of graph replay (for per-kernel profilers)")
     ap.add_argument("--convex-steps", type=int, default=500)
@@ -554,6 +590,8 @@ def main():
             line["batched"] = batched_measure(args.batched_instances, args.batched_steps)
         if args.convex_n > 0:
             line["convex"] = convex_measure(args.convex_n, args.convex_steps)
+        if args.adjoint_n > 0:
+            line["adjoint"] = adjoint_measure(args.adjoint_n, args.adjoint_steps, 50)
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(sc, xml)
         print(json.dumps(line), flush=True)

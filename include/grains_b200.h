@@ -132,9 +132,10 @@ int gdem_init(gdem_handle h);
 
 /* Advances nsteps kick-drift-kick leapfrog steps of size dt (from the XML).
  * Equivalent to the loop body of Grains::Simulation (Grains.cpp:286-364).
- * Per step one fused kernel evaluates the contact forces and applies the
- * closing and the next opening kick and drift; the pair list is rebuilt
- * only when needed (gdem_step_counts), inside a CUDA-graph conditional node. */
+ * Per step: a contact filter over the pair list, the force kernel over the
+ * particles in contact, and the leapfrog kernel (closing kick, next opening
+ * kick and drift); the pair list is rebuilt only when needed
+ * (gdem_step_counts), inside a CUDA-graph conditional node. */
 int gdem_step(gdem_handle h, int nsteps);
 
 /* State by particle ID; any pointer may be NULL. */
@@ -177,6 +178,34 @@ int gdem_use_graphs(gdem_handle h, int on);
 
 const char* gdem_last_error(void);
 void gdem_destroy(gdem_handle h);
+
+/* ---------------------------------------------------------------- adjoint
+ * Calibration gradients (the reference has no differentiation).  The
+ * adjoint engine integrates spheres in a walled box with the same leapfrog
+ * and Hooke / HookeMemory law as gdem_step (FP64, no rolling resistance, no
+ * periodic directions) and differentiates the loss
+ *     L = sum_i |x_i(nsteps) - target_x_i|^2 + |v_i(nsteps) - target_v_i|^2
+ * with respect to params = (kn, en, muc) (replacing those of every contact
+ * model of the XML) and the initial velocities, by a reverse sweep over the
+ * steps with the transposed leapfrog and contact-force Jacobians, recomputing
+ * states from checkpoints taken every checkpoint_every steps. */
+typedef struct gdem_adjoint* gdem_adjoint_handle;
+int gdem_adjoint_create(const char* xml_path, gdem_adjoint_handle* out);
+/* Particles by index: class, x0, v0 (3 each), w0 (3 each; NULL: zero). */
+int gdem_adjoint_set_particles(gdem_adjoint_handle h, int64_t n, const int* type,
+                               const double* x0, const double* v0, const double* w0);
+/* Forward run, loss and gradients; every output pointer may be NULL (no
+ * gradient pointer: forward only; no target: no loss). */
+int gdem_adjoint_run(gdem_adjoint_handle h, int nsteps, int checkpoint_every,
+                     const double* params, const double* target_x, const double* target_v,
+                     double* loss, double* x_out, double* v_out, double* dL_dparams,
+                     double* dL_dv0);
+/* The same loss differentiated in forward mode (dual numbers seeded on kn,
+ * en, muc), to check the adjoint. */
+int gdem_adjoint_forward_dual(gdem_adjoint_handle h, int nsteps, const double* params,
+                              const double* target_x, const double* target_v, double* loss,
+                              double* dL_dparams);
+void gdem_adjoint_destroy(gdem_adjoint_handle h);
 
 /* No counterpart in the reference.  Maximum and mean |v| (as
  * gdem_velocity_stats, AllComponents::ComputeMaxMeanVelocity) of n particle

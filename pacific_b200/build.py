@@ -28,6 +28,7 @@ UNITS = [
     ("gdem_contact32.cu", ["-fmad=false"]),
     ("gdem_host.cu", ["-fmad=false"]),
     ("gdem_noalloc.cu", ["-fmad=false"]),
+    ("gdem_adjoint.cu", ["-fmad=false"]),
     ("xml_reader.cpp", []),
 ]
 

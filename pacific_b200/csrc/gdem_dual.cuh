@@ -15,6 +15,7 @@ namespace gdem {
 
 template <int N>
 struct Dual {
+  static constexpr int kN = N;
   double v;
   double d[N];
 };
@@ -110,13 +111,31 @@ __host__ __device__ __forceinline__ Dual<N> dsqrt(Dual<N> a) {
   return r;
 }
 __host__ __device__ __forceinline__ double dsqrt(double a) { return sqrt(a); }
+template <int N>
+__host__ __device__ __forceinline__ Dual<N> dlog(Dual<N> a) {
+  Dual<N> r;
+  r.v = log(a.v);
+  const double ia = 1. / a.v;
+#pragma unroll
+  for (int k = 0; k < N; ++k) r.d[k] = a.d[k] * ia;
+  return r;
+}
+__host__ __device__ __forceinline__ double dlog(double a) { return log(a); }
+template <int N>
+__host__ __device__ __forceinline__ Dual<N> dfabs(Dual<N> a) { return a.v < 0. ? -a : a; }
+__host__ __device__ __forceinline__ double dfabs(double a) { return fabs(a); }
 __host__ __device__ __forceinline__ double val(double a) { return a; }
 template <int N>
 __host__ __device__ __forceinline__ double val(Dual<N> a) { return a.v; }
+// A constant of scalar type T.
 template <typename T>
-__host__ __device__ __forceinline__ T scal(double a);
+struct Scal {
+  __host__ __device__ static T make(double a) { return dconst<T::kN>(a); }
+};
 template <>
-__host__ __device__ __forceinline__ double scal<double>(double a) { return a; }
+struct Scal<double> {
+  __host__ __device__ static double make(double a) { return a; }
+};
 
 // Generic 3-vector.
 template <typename T>

@@ -399,6 +399,41 @@ def convex_pour(n=200_000, seed=1238, poly_path=None, box=(0.1, 0.1, 0.3), cube_
                     walls, models, type_, x, v, np.zeros((n, 3)), q)
 
 
+def adjoint_box(n=4096, seed=1239, box=(0.02, 0.02, 0.08), radius=1.0e-3, spacing=2.1e-3,
+                jitter=2.5e-5, vmax=0.2, kn=2.0e4, en=0.6, muc=0.35, dt=1.0e-5,
+                density=2500.0, gravity=(0.0, 0.0, -9.81)) -> Scenario:
+    """The calibration case: spheres of radius 1 mm on an FCC lattice of
+    nearest-neighbour spacing 2.1 mm (a cubic lattice of 2.4 mm holds only
+    2,112 in the 0.02 x 0.02 x 0.08 m box), centres at least r from the walls,
+    the first n sites in (z, y, x) order, jitter up to +-0.025 mm per axis
+    (sites closer than r + jitter to a wall are dropped),
+    velocities uniform in +-0.2 m/s, HookeMemory with kt = 2/7 kn."""
+    rng = np.random.default_rng(seed)
+    a = spacing * np.sqrt(2.0)
+    base = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]]) * a
+    ncell = [int(np.ceil(b / a)) + 1 for b in box]
+    g = np.stack(np.meshgrid(*[np.arange(k) for k in ncell], indexing="ij"), axis=-1).reshape(-1, 3)
+    sites = (g[:, None, :] * a + base[None, :, :]).reshape(-1, 3) + (radius + jitter)
+    inside = np.all((sites >= radius + jitter) & (sites <= np.array(box) - radius - jitter), axis=1)
+    sites = sites[inside]
+    order = np.lexsort((sites[:, 0], sites[:, 1], sites[:, 2]))
+    sites = sites[order]
+    if n > len(sites):
+        raise ValueError("lattice too small")
+    x = sites[:n] + rng.uniform(-jitter, jitter, size=(n, 3))
+    v = rng.uniform(-vmax, vmax, size=(n, 3))
+    w = np.zeros((n, 3))
+    q = np.zeros((n, 4)); q[:, 3] = 1.0
+    crust = 0.1 * radius
+    types = [dict(radius=radius, crust=crust, density=density, material="matP")]
+    walls = _box_walls(box, 2.0e-3, crust, "matW")
+    kt = 2.0 / 7.0 * kn
+    models = [dict(matA="matP", matB="matP", kn=kn, en=en, etat=None, muc=muc, kt=kt),
+              dict(matA="matP", matB="matW", kn=kn, en=en, etat=None, muc=muc, kt=kt)]
+    return Scenario("adjoint_box", (0.0, 0.0, 0.0), tuple(box), (0, 0, 0), tuple(gravity), dt,
+                    types, walls, models, np.zeros(n, np.int32), x, v, w, q)
+
+
 def solid_fraction(sc: Scenario) -> float:
     r = np.array([t["radius"] for t in sc.types])[sc.type]
     vol = np.prod(np.array(sc.maxc) - np.array(sc.origin))
