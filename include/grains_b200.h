@@ -200,11 +200,14 @@ int gdem_adjoint_run(gdem_adjoint_handle h, int nsteps, int checkpoint_every,
                      const double* params, const double* target_x, const double* target_v,
                      double* loss, double* x_out, double* v_out, double* dL_dparams,
                      double* dL_dv0);
-/* The same loss differentiated in forward mode (dual numbers seeded on kn,
- * en, muc), to check the adjoint. */
+/* The same loss differentiated in forward mode, to check the adjoint: with
+ * seed_particle < 0 the dual numbers are seeded on (kn, en, muc) and
+ * dL_dseed receives 3 values; otherwise on the initial velocity component
+ * (seed_particle, seed_component) and dL_dseed receives 1 value. */
 int gdem_adjoint_forward_dual(gdem_adjoint_handle h, int nsteps, const double* params,
-                              const double* target_x, const double* target_v, double* loss,
-                              double* dL_dparams);
+                              const double* target_x, const double* target_v,
+                              int seed_particle, int seed_component, double* loss,
+                              double* dL_dseed);
 void gdem_adjoint_destroy(gdem_adjoint_handle h);
 
 /* No counterpart in the reference.  Maximum and mean |v| (as

@@ -33,8 +33,8 @@ def _lib():
             "gdem_adjoint_set_particles": ([_P, ctypes.c_int64, _IP, _DP, _DP, _DP], ctypes.c_int),
             "gdem_adjoint_run": ([_P, ctypes.c_int, ctypes.c_int, _DP, _DP, _DP, _DP, _DP, _DP,
                                   _DP, _DP], ctypes.c_int),
-            "gdem_adjoint_forward_dual": ([_P, ctypes.c_int, _DP, _DP, _DP, _DP, _DP],
-                                          ctypes.c_int),
+            "gdem_adjoint_forward_dual": ([_P, ctypes.c_int, _DP, _DP, _DP, ctypes.c_int,
+                                           ctypes.c_int, _DP, _DP], ctypes.c_int),
             "gdem_adjoint_destroy": ([_P], None),
         }
         for name, (args, res) in sig.items():
@@ -110,15 +110,18 @@ class Adjoint:
                                             ctypes.byref(loss), None, None, _dp(gp), _dp(gv)))
         return loss.value, gp, gv
 
-    def forward_mode(self, params, target_x, target_v, nsteps):
-        """(loss, dL/d(kn, en, muc)) by dual numbers through the whole run."""
+    def forward_mode(self, params, target_x, target_v, nsteps, v0_component=None):
+        """(loss, dL/d(kn, en, muc)) by dual numbers through the whole run; with
+        v0_component = (particle, axis): (loss, dL/dv0[particle, axis])."""
         p = _f64(params, (3,))
         tx, tv = _f64(target_x, (self.n, 3)), _f64(target_v, (self.n, 3))
         loss = ctypes.c_double(0.0)
         gp = np.zeros(3)
+        i, d = v0_component if v0_component is not None else (-1, 0)
         self._check(_lib().gdem_adjoint_forward_dual(self._h, nsteps, _dp(p), _dp(tx), _dp(tv),
-                                                     ctypes.byref(loss), _dp(gp)))
-        return loss.value, gp
+                                                     int(i), int(d), ctypes.byref(loss),
+                                                     _dp(gp)))
+        return (loss.value, gp) if v0_component is None else (loss.value, gp[0])
 
 
 def trajectory_loss_function():

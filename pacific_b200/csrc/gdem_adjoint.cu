@@ -479,6 +479,14 @@ __global__ void k_promote(int n3, const double* a, T* out) {
 
 inline int nblk(int n) { return (n + 127) / 128; }
 
+// Sets the first derivative slot of one element to 1 (forward-mode seed).
+template <typename T>
+__global__ void k_seed(T* a, int i) {
+  a[i].d[0] = 1.;
+}
+template <>
+__global__ void k_seed<double>(double*, int) {}
+
 struct AdjointSystem {
   AdjointSetup setup;
   AdjTables A{};
@@ -611,10 +619,11 @@ struct AdjointSystem {
 
   // Leapfrog start: forces at (x0, v0, w0) with no history, spring zeroed.
   template <typename T>
-  void start(State<T>& S, ListsT<T>& L, T kn, T en, T muc) {
+  void start(State<T>& S, ListsT<T>& L, T kn, T en, T muc, int seed_v0 = -1) {
     const int n3 = 3 * n;
     k_promote<T><<<nblk(n3), 128, 0, st>>>(n3, d_x0, S.x);
     k_promote<T><<<nblk(n3), 128, 0, st>>>(n3, d_v0, S.v);
+    if (seed_v0 >= 0) k_seed<T><<<1, 1, 0, st>>>(S.v, seed_v0);
     k_promote<T><<<nblk(n3), 128, 0, st>>>(n3, d_w0, S.w);
     k_fwd_forces<T><<<nblk(n), 128, 0, st>>>(n, A, d_type, S.x, S.v, S.w, L, 0, L, S.F, S.Tq,
                                              kn, en, muc, 1, d_overflow);
@@ -764,10 +773,11 @@ struct AdjointSystem {
     }
   }
 
-  // Forward-mode gradient of the loss in (kn, en, muc): the whole forward run
-  // on Dual<3> numbers.
+  // Forward-mode derivative of the loss: the whole forward run on Dual<3>
+  // numbers seeded on (kn, en, muc), or, with seed_particle >= 0, on the one
+  // initial velocity component (seed_particle, seed_component) in slot 0.
   void forwardDual(int nsteps, const double* p, const double* tx, const double* tv,
-                   double* loss, double* dLdp) {
+                   double* loss, double* dLdp, int seed_particle, int seed_component) {
     using D = Dual<3>;
     if (nsteps < 1) throw std::runtime_error("nsteps must be >= 1");
     if (!tx || !tv) throw std::runtime_error("the loss needs target x and v");
@@ -775,14 +785,17 @@ struct AdjointSystem {
     Scope scope(this);
     ACK(cudaMemsetAsync(d_overflow, 0, sizeof(int), st));
     D kn = dconst<3>(p[0]), en = dconst<3>(p[1]), muc = dconst<3>(p[2]);
-    kn.d[0] = 1.; en.d[1] = 1.; muc.d[2] = 1.;
+    const bool seed_v = seed_particle >= 0;
+    if (seed_v && (seed_particle >= n || seed_component < 0 || seed_component > 2))
+      throw std::runtime_error("seed out of range");
+    if (!seed_v) { kn.d[0] = 1.; en.d[1] = 1.; muc.d[2] = 1.; }
     const size_t n3 = 3 * (size_t)n;
     State<D> S = allocState<D>();
     D* xs = alloc<D>(n3);
     D* vh = alloc<D>(n3);
     D* wh = alloc<D>(n3);
     ListsT<D> L[2] = {allocLists<D>(), allocLists<D>()};
-    start(S, L[0], kn, en, muc);
+    start(S, L[0], kn, en, muc, seed_v ? 3 * seed_particle + seed_component : -1);
     for (int s = 1; s <= nsteps; ++s) advance(S, xs, vh, wh, L[(s - 1) & 1], L[s & 1], kn, en, muc);
     checkOverflow();
     std::vector<D> per;
@@ -793,7 +806,10 @@ struct AdjointSystem {
       for (int d = 0; d < 3; ++d) g[d] += a.d[d];
     }
     if (loss) *loss = Lv;
-    if (dLdp) for (int d = 0; d < 3; ++d) dLdp[d] = g[d];
+    if (dLdp) {
+      if (seed_v) dLdp[0] = g[0];
+      else for (int d = 0; d < 3; ++d) dLdp[d] = g[d];
+    }
   }
 };
 
@@ -854,11 +870,13 @@ int gdem_adjoint_run(gdem_adjoint_handle h, int nsteps, int checkpoint_every,
 }
 
 int gdem_adjoint_forward_dual(gdem_adjoint_handle h, int nsteps, const double* params,
-                              const double* target_x, const double* target_v, double* loss,
-                              double* dL_dparams) {
+                              const double* target_x, const double* target_v,
+                              int seed_particle, int seed_component, double* loss,
+                              double* dL_dseed) {
   return adjGuarded([&] {
     if (!h || !params) throw std::runtime_error("invalid arguments");
-    adj(h)->forwardDual(nsteps, params, target_x, target_v, loss, dL_dparams);
+    adj(h)->forwardDual(nsteps, params, target_x, target_v, loss, dL_dseed, seed_particle,
+                        seed_component);
   });
 }
 

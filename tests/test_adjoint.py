@@ -3,9 +3,11 @@ numbers and central finite differences.
 
 Both the reverse sweep and the dual-number forward run differentiate the same
 discrete FP64 trajectory exactly, so they agree to round-off (1e-8 relative
-here).  Central differences (h = 1e-6 relative) agree to 1e-4 relative when
-no contact opens, closes or switches between stick and slip inside the
-perturbation, which holds on these seeded cases."""
+here), for the parameters and for single initial-velocity components.
+Central differences (h = 1e-6 relative) agree with the parameter gradient to
+1e-4; for initial velocities, where one particle's perturbation can move a
+stick/slip switch of its own contacts inside the difference interval, they
+are a coarse check (5 %)."""
 import numpy as np
 import pytest
 
@@ -47,9 +49,17 @@ def test_adjoint_matches_forward_mode_and_differences(tmp_path, lib):
         fd = (lp - lm) / (2 * h)
         assert abs(fd - gp[k]) <= 1e-4 * abs(gp[k]), (k, fd, gp[k])
     adj.close()
-    # initial velocities: central differences on a few components
+    # initial velocities: forward mode seeded on single components (exact),
+    # and central differences as a coarse check (a contact that switches
+    # between stick and slip inside the perturbation makes the loss kinked
+    # there, which a difference quotient averages)
+    adj = Adjoint(xml)
+    adj.set_particles(sc.type, sc.x, sc.v)
     rng = np.random.default_rng(3)
-    for i, d in zip(rng.integers(0, sc.n, 3), rng.integers(0, 3, 3)):
+    scale = np.abs(gv).max()
+    for i, d in zip(rng.integers(0, sc.n, 4), rng.integers(0, 3, 4)):
+        _, gfm = adj.forward_mode(P_START, tx, tv, steps, v0_component=(i, d))
+        assert abs(gfm - gv[i, d]) <= 1e-8 * abs(gfm) + 1e-12 * scale, (i, d, gfm, gv[i, d])
         h = 1e-6
         out = []
         for sgn in (1, -1):
@@ -60,7 +70,8 @@ def test_adjoint_matches_forward_mode_and_differences(tmp_path, lib):
             out.append(a.run(P_START, steps, tx, tv)[2])
             a.close()
         fd = (out[0] - out[1]) / (2 * h)
-        assert abs(fd - gv[i, d]) <= 1e-4 * abs(gv[i, d]) + 1e-9 * np.abs(gv).max(), (i, d)
+        assert abs(fd - gv[i, d]) <= 5e-2 * abs(gv[i, d]) + 1e-6 * scale, (i, d, fd, gv[i, d])
+    adj.close()
 
 
 def test_checkpoint_interval_does_not_change_gradients(tmp_path, lib):
