@@ -297,6 +297,8 @@ InstanceDesc readInstance(std::string const& path) {
     }
     t.mass = density * vol;
     for (int d = 0; d < 3; ++d) t.inertia[d] = Iv[d] * density;
+    t.inv_mass = 1. / t.mass;
+    for (int d = 0; d < 3; ++d) t.inv_inertia[d] = 1. / t.inertia[d];
     t.eqrad = std::pow((0.75 / PI) * vol, 1. / 3.);                   // getEquivalentSphereRadius
     // crust shrink factors (RigidBodyWithCrust ctor, RigidBodyWithCrust.cpp:58-78)
     for (int d = 0; d < 3; ++d)
@@ -747,7 +749,7 @@ struct System {
     const int sparse = (flags && !diag) ? 1 : 0;
     if (precision == GDEM_FP64) timed("forces64", [&] { launch_forces64(S, sparse, stream); });
     else timed("forces32", [&] { launch_forces32(S, sparse, stream); });
-    if (flags) timed("move", [&] { launch_move(S, flags, stream); });
+    if (flags) timed("move", [&] { launch_move(S, flags, precision == GDEM_FP32_SPLIT, stream); });
   }
   // One force evaluation with plain launches: decide, gated rebuild, filter,
   // forces, move.
@@ -838,7 +840,7 @@ struct System {
     if (nsteps <= 0) return;
     id_order = false;
     CK(cudaEventRecord(ev0, stream));
-    timed("move", [&] { launch_move(S, kStepMove, stream); });
+    timed("move", [&] { launch_move(S, kStepMove, precision == GDEM_FP32_SPLIT, stream); });
     const int mid = kStepClose | kStepMove;
     const int last = kStepClose | kStepStoreFT;
     const bool graphs = use_graphs && !diag && !profiling;

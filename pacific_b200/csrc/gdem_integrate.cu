@@ -251,6 +251,7 @@ __global__ void k_copyback(DevState S, const int* gate) {
 // A particle that the contact filter left without contact carries only its
 // weight: the force kernel skipped it and its F, T are taken as such here
 // (and written back at the end of a call, kStepStoreFT).
+template <bool kFast>
 __global__ void __launch_bounds__(256, 3) k_move(DevState S, int flags) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
@@ -264,7 +265,7 @@ __global__ void __launch_bounds__(256, 3) k_move(DevState S, int flags) {
     F = ld3(S.F, S.cap, t);
     T = ld3(S.T, S.cap, t);
   }
-  advanceParticle(S, t, tp, F, T, (flags & kStepClose) != 0, (flags & kStepMove) != 0);
+  advanceParticle<kFast>(S, t, tp, F, T, (flags & kStepClose) != 0, (flags & kStepMove) != 0);
 }
 
 // Contact filter: the entries of each particle's skin list whose bounding
@@ -515,12 +516,13 @@ void launch_permute(DevState const& S, const int* gate, cudaStream_t st) {
 void launch_copyback(DevState const& S, const int* gate, cudaStream_t st) {
   if (S.n) k_copyback<<<blocks(S.n, 256), 256, 0, st>>>(S, gate);
 }
-void launch_move(DevState const& S, int flags, cudaStream_t st) {
+void launch_move(DevState const& S, int flags, int fast, cudaStream_t st) {
   if (!S.n) return;
   DevState M = S;   // in place: the "next" buffers are the current ones
   M.x2 = S.x; M.v2 = S.v; M.w2 = S.w; M.wbf2 = S.wbf; M.q2 = S.q; M.basis2 = S.basis;
   M.wrap2 = S.wrap;
-  k_move<<<blocks(S.n, 256), 256, 0, st>>>(M, flags);
+  if (fast) k_move<true><<<blocks(S.n, 256), 256, 0, st>>>(M, flags);
+  else k_move<false><<<blocks(S.n, 256), 256, 0, st>>>(M, flags);
 }
 void launch_filter(DevState const& S, cudaStream_t st) {
   if (S.n) k_filter<<<blocks(S.n, 256), 256, 0, st>>>(S);

@@ -23,7 +23,9 @@ void launch_place(DevState const& S, const int* gate, cudaStream_t st);
 void launch_cellsort(DevState const& S, const int* gate, cudaStream_t st);
 void launch_permute(DevState const& S, const int* gate, cudaStream_t st);
 void launch_copyback(DevState const& S, const int* gate, cudaStream_t st);
-void launch_move(DevState const& S, int flags, cudaStream_t st);
+// fast: the FP32-split leapfrog (reciprocals, series; not the reference's
+// operation order)
+void launch_move(DevState const& S, int flags, int fast, cudaStream_t st);
 void launch_filter(DevState const& S, cudaStream_t st);
 void launch_fill64(unsigned long long* p, size_t n, unsigned long long value, cudaStream_t st);
 void launch_scatter_by_id(DevState const& S, double* x, double* v, double* w, double* wbf,

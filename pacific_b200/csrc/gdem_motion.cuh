@@ -91,23 +91,74 @@ __device__ __forceinline__ void wrapToGrid(GridDesc const& g, d3& x, int* wrapd,
   x = mk(xs[0], xs[1], xs[2]);
 }
 
+// ------------------------------------------------- FP32-split leapfrog --
+// The same integration with the FP64 arithmetic reorganised: products by
+// precomputed reciprocals instead of divisions, the sphere's SSP-RK3 taken as
+// the single evaluation it equals in exact arithmetic, the sine and cosine of
+// the small rotation angle from their series.  Every quantity stays FP64;
+// the results differ from the reference's operation order by a few ulps per
+// step, far below the FP32 force law of this mode.
+__device__ __forceinline__ d3 dOmegaFast(TypeDesc const& t, d3 tbf, d3 om) {
+  const double* iI = t.inv_inertia;
+  if (t.shape == 0) return mk(tbf.x * iI[0], tbf.y * iI[1], tbf.z * iI[2]);
+  const double* I = t.inertia;
+  return mk((tbf.x + om.y * om.z * (I[1] - I[2])) * iI[0],
+            (tbf.y + om.z * om.x * (I[2] - I[0])) * iI[1],
+            (tbf.z + om.x * om.y * (I[0] - I[1])) * iI[2]);
+}
+__device__ __forceinline__ d3 rk3Fast(TypeDesc const& t, d3 tbf, d3 wbf, double h) {
+  if (t.shape == 0) return wbf + dOmegaFast(t, tbf, wbf) * h;
+  const double sixth = 1. / 6.;
+  d3 K1 = dOmegaFast(t, tbf, wbf) * h;
+  d3 K2 = dOmegaFast(t, tbf, wbf + K1) * h;
+  d3 K3 = dOmegaFast(t, tbf, wbf + 0.25 * (K1 + K2)) * h;
+  return wbf + ((K1 + K2) + 4. * K3) * sixth;
+}
+__device__ __forceinline__ void kickFast(TypeDesc const& tp, d3 F, d3 T, d3& v, d3& wbf, d3& w,
+                                         dq q, double h) {
+  dq pc = conj(q);
+  d3 tbf = multToVector3(pc, vecq(T, q));
+  v = v + F * (h * tp.inv_mass);
+  wbf = rk3Fast(tp, tbf, wbf, h);
+  w = multToVector3(q, vecq(wbf, pc));
+}
+// sin and cos of a; series below 1e-2 (truncation below 1e-19 relative)
+__device__ __forceinline__ void sinCosSmall(double a, double* s, double* c) {
+  if (fabs(a) < 1.e-2) {
+    const double a2 = a * a;
+    *s = a * (1. - a2 * (1. / 6. - a2 * (1. / 120. - a2 * (1. / 5040.))));
+    *c = 1. - a2 * (0.5 - a2 * (1. / 24. - a2 * (1. / 720.)));
+  } else {
+    sincos(a, s, c);
+  }
+}
+
 // One particle's leapfrog: optionally the closing kick of the previous step
 // (with this step's F, T over hc), then optionally the opening kick over h
 // and the drift over dt with the quaternion and orientation update.
 // basis: 9 entries (row-major) or null.  dx receives the translation.
+template <bool kFast>
 __device__ __forceinline__ void leapfrog(TypeDesc const& tp, d3 F, d3 T, bool close, double hc,
                                          bool move, double h, double dt, d3& x, d3& v,
                                          d3& wbf, d3& w, dq& q, double* basis, d3& dx,
                                          int* status) {
-  if (close) kick(tp, F, T, v, wbf, w, q, hc);
+  if (close) {
+    if (kFast) kickFast(tp, F, T, v, wbf, w, q, hc);
+    else kick(tp, F, T, v, wbf, w, q, hc);
+  }
   dx = mk(0., 0., 0.);
   if (!move) return;
   dq pc = conj(q);
   d3 tbf = multToVector3(pc, vecq(T, q));
   const double c = 1.;
-  v = v + (F / (tp.mass * c)) * h;
+  if (kFast) {
+    v = v + F * (h * tp.inv_mass);
+    wbf = rk3Fast(tp, tbf, wbf, h);
+  } else {
+    v = v + (F / (tp.mass * c)) * h;
+  }
   dx = v * dt;
-  wbf = rk3(tp, tbf, wbf, h);
+  if (!kFast) wbf = rk3(tp, tbf, wbf, h);
   w = multToVector3(q, vecq(wbf, pc));
   const d3 meanw = w;     // same expression as w (ParticleKinematics.cpp:79-82)
   x = x + dx;
@@ -115,8 +166,13 @@ __device__ __forceinline__ void leapfrog(TypeDesc const& tp, d3 F, d3 T, bool cl
   dq qdt;
   if (nOm > 1.0e-10) {
     double cc, ss;
-    sincos(nOm * dt / 2., &ss, &cc);
-    qdt = qmk((ss * 1. / nOm) * meanw, cc);
+    if (kFast) {
+      sinCosSmall(nOm * dt * 0.5, &ss, &cc);
+      qdt = qmk((ss / nOm) * meanw, cc);
+    } else {
+      sincos(nOm * dt / 2., &ss, &cc);
+      qdt = qmk((ss * 1. / nOm) * meanw, cc);
+    }
   } else {
     qdt = qmk(mk(0., 0., 0.), 1.);
   }
@@ -137,13 +193,14 @@ __device__ __forceinline__ void leapfrog(TypeDesc const& tp, d3 F, d3 T, bool cl
 #pragma unroll
     for (int k = 0; k < 9; ++k) basis[k] = out[k];
   }
-  if (norm(dx) > tp.crust) raise(status, kErrMotion);
+  if (kFast ? dot(dx, dx) > tp.crust * tp.crust : norm(dx) > tp.crust) raise(status, kErrMotion);
 }
 
 // Moves particle t of the current buffers (F, T as given) and writes the
 // result to the second buffers; updates the pair-list displacement and wraps
 // and flags a rebuild when the particle has moved more than half the skin.
 // close/move select the kicks as in leapfrog().
+template <bool kFast>
 __device__ __forceinline__ void advanceParticle(DevState const& S, int t, TypeDesc const& tp,
                                                 d3 F, d3 T, bool close, bool move) {
   const int cap = S.cap;
@@ -160,7 +217,7 @@ __device__ __forceinline__ void advanceParticle(DevState const& S, int t, TypeDe
     bp = bas;
   }
   d3 dx;
-  leapfrog(tp, F, T, close, 0.5 * dt, move, 0.5 * dt, dt, x, v, wbf, w, q, bp, dx, S.status);
+  leapfrog<kFast>(tp, F, T, close, 0.5 * dt, move, 0.5 * dt, dt, x, v, wbf, w, q, bp, dx, S.status);
   int wr = S.wrap[t];
   if (move) {
     int wd[3];

@@ -74,6 +74,8 @@ struct TypeDesc {
   double scaling[3];     // crust shrink factors (extent - crust) / extent
   int poly_begin;        // first vertex of a polyhedron in the vertex table
   int poly_count;        // its vertex count
+  double inv_mass;       // 1 / mass and 1 / inertia (FP32-split leapfrog)
+  double inv_inertia[3];
 };
 
 // HookeMemory / Hooke parameters (HookeMemoryContactForceModel.cpp:12-27).

@@ -98,5 +98,5 @@ def test_torch_function(tmp_path, lib):
     adj = Adjoint(xml)
     adj.set_particles(sc.type, sc.x, sc.v)
     l2, gp, gv = adj.gradients(P_START, tx, tv, steps, 50)
-    assert float(loss) == l2
+    assert float(loss.detach()) == l2
     assert np.array_equal(p.grad.numpy(), gp) and np.array_equal(v0.grad.numpy(), gv)
