@@ -108,16 +108,28 @@ class ClockSampler:
 def algorithmic_bytes(kernel, n, entries, contacts, ncells, fp64):
     """Compulsory DRAM bytes of one launch of each phase of a spheres-only
     step: each input read once, each output written once, neighbour re-reads
-    counted as cache hits.  Per particle unless noted."""
-    if kernel == "filter":       # cellc posf npairs wrap + entry words | kept entries + count
-        return n * (16 + 16 + 4 + 4 + 4) + 4 * entries + 4 * contacts
+    counted as cache hits.  Per particle unless noted.  The particle state is
+    x, v, w, w_bf, q in FP64; FP32-split spheres keep no w_bf (w is their
+    angular state)."""
+    vel = 24
+    state = 24 + (3 if fp64 else 2) * vel + 32
+    touched = min(n, 2 * contacts)    # particles with a contact (the force work list)
+    if kernel == "filter":
+        # instance, posf, upper count | next flags; per pair (half the
+        # directed entries) the entry word and the partner's posf; per
+        # contact the two flags and the work-list entries
+        return n * (4 + 16 + 4 + 4) + (entries // 2) * (4 + 16) + contacts * 16
     if kernel in ("forces64", "forces32"):
-        # cellc id type x v w nact | F T; per contact the entry word and the
-        # history key + values, read and written
-        per_c = 4 + 2 * (8 + (72 if fp64 else 36))
-        return n * (16 + 4 + 4 + 72 + 4 + 48) + contacts * per_c
-    if kernel == "move":         # F T x v w w_bf q type inst disp wrap | x v w w_bf q disp wrap posf
-        return n * (48 + 104 + 8 + 12 + 4 + 104 + 12 + 4 + 16)
+        # per particle of the work list: cellc id type x v w nact | F T; per
+        # contact the entry word, the partner's id type x v w and the history
+        # key + values, read and written
+        per_p = 16 + 4 + 4 + 24 + 2 * vel + 4 + 48
+        per_c = 4 + (4 + 4 + 24 + 2 * vel) + 2 * (8 + (72 if fp64 else 36))
+        return touched * per_p + contacts * per_c
+    if kernel == "move":
+        # state type inst disp wrap nact (+ F T of the particles in contact)
+        # | state disp wrap posf
+        return n * (state + 8 + 12 + 4 + 4 + state + 12 + 4 + 16) + touched * 48
     if kernel == "bin":          # x inst | skey rank; cell-count RMW
         return n * (24 + 4 + 8 + 8)
     if kernel == "scan":         # counts | starts (per cell)
@@ -127,9 +139,9 @@ def algorithmic_bytes(kernel, n, entries, contacts, ncells, fp64):
     if kernel == "cellsort":     # starts, count reset (per cell); order, id of shared cells
         return ncells * 8 + n * 8
     if kernel == "permute":      # order skey ids state F T | ids state F T cellc + pos / offset
-        return n * (4 + 4 + 12 + 176 + 12 + 176 + 16 + (32 if fp64 else 16))
+        return n * (4 + 4 + 12 + 2 * (state + 48) + 16 + (32 if fp64 else 16))
     if kernel == "copyback":     # ids state F T | ids state F T disp wrap
-        return n * (12 + 176 + 12 + 176 + 12 + 4)
+        return n * (12 + 2 * (state + 48) + 12 + 12 + 4)
     if kernel in ("pairs64", "pairs32"):   # cellc + own position | npairs; entries; starts
         return n * (16 + (32 if fp64 else 16) + 4) + 4 * entries + 4 * ncells
     return None
@@ -310,21 +322,28 @@ def cpu_baseline(sc, xml, budget_s=15.0):
 def batched_measure(n_inst, steps, warmup=3):
     """The batched sweep: n_inst independent closed-box settling instances
     (500-20,000 spheres each, their own kn/en/muc) stepped together in one
-    launch chain, against the same instances stepped one after another
-    (device time of each gdem_step, creation excluded on both sides)."""
+    launch chain, with the launch settings the autotuner picks (and, beside
+    it, with the default ones), against the same instances stepped one after
+    another with the default settings (device time of each gdem_step,
+    creation and tuning excluded on both sides)."""
     from pacific_b200 import FP32_SPLIT, Grains, scenarios
     inst = scenarios.batched_boxes(n_inst=n_inst)
     with tempfile.TemporaryDirectory() as d:
         xmls = [str(s.write_xml(Path(d) / f"i{k}.xml")) for k, s in enumerate(inst)]
         ins, typ, x, v, w, q = scenarios.concat_state(inst)
-        g = Grains(xmls, FP32_SPLIT)
-        g.upload_state(typ, x, v, w, q, inst=ins)
-        g.do_before_time_stepping()
-        g.step(warmup)
-        g.step(steps)
-        t_batch = g.last_step_ms
-        st = g.status()
-        g.close()
+        times = {}
+        for label in ("default", "autotuned"):
+            g = Grains(xmls, FP32_SPLIT)
+            g.upload_state(typ, x, v, w, q, inst=ins)
+            if label == "autotuned":
+                tuned = g.autotune(trial_steps=20)
+            g.do_before_time_stepping()
+            g.step(warmup)
+            g.step(steps)
+            times[label] = g.last_step_ms
+            st = g.status()
+            g.close()
+        t_batch = times["autotuned"]
         t_seq = 0.0
         for k, s in enumerate(inst):
             gi = Grains(xmls[k], FP32_SPLIT)
@@ -337,6 +356,8 @@ def batched_measure(n_inst, steps, warmup=3):
     ntot = int(len(ins))
     return {"instances": n_inst, "particles": ntot, "steps": steps,
             "batched_value": ntot * steps / (t_batch * 1e-3),
+            "autotune": tuned,
+            "batched_default_value": ntot * steps / (times["default"] * 1e-3),
             "sequential_value": ntot * steps / (t_seq * 1e-3),
             "speedup": t_seq / t_batch, "unit": UNIT, "precision": "fp32_split",
             "status": st, "workload": "batched_boxes (seeded), FP32-split, device time"}
@@ -363,15 +384,27 @@ def convex_measure(n, steps, warmup=3):
                 g.do_before_time_stepping()
                 g.step(warmup)
                 g.law_counts(reset=True)
+                g.gjk_counts(reset=True)
                 g.step(steps)
                 ms = g.last_step_ms
                 entries, contacts = g.pair_counts()
+                calls, iters, most = g.gjk_counts()
                 r = {"value": n * steps / (ms * 1e-3), "ms_per_step": ms / steps,
-                     "status": g.status(), "contacts_last_step": contacts}
+                     "status": g.status(), "contacts_last_step": contacts,
+                     "gjk": {"calls_per_step": calls / steps,
+                             "mean_iterations": iters / calls if calls else 0.0,
+                             "max_iterations": most}}
                 if prec == FP32_SPLIT:
                     nlaw, nre = g.law_counts()
                     r["law_evaluations"] = nlaw
                     r["fp64_reevaluated"] = nre
+                if vmax > 0:
+                    # per-kernel device times over a few more steps (plain launches)
+                    g.set_profiling(True)
+                    g.step(10)
+                    r["phases"] = {k: {"total_ms": round(v[0], 4), "launches": v[1]}
+                                   for k, v in g.kernel_times().items()}
+                    g.set_profiling(False)
                 row[name] = r
                 g.close()
             row["fp32_split_speedup"] = row["fp32_split"]["value"] / row["fp64"]["value"]
@@ -540,8 +573,18 @@ def main():
         hbm = hbm or 6650.0
         achieved = ab / (avg_ms * 1e-3) / 1e9 if ab else None
         traffic = read_ncu_traffic(dom)
-        phases = {k: {"total_ms": round(v[0], 4), "launches": v[1],
-                      "avg_us": round(1e3 * v[0] / v[1], 2)} for k, v in kt.items()}
+        def phase_table(kts, res_, fp64):
+            out = {}
+            for k, v in kts.items():
+                avg = v[0] / v[1]
+                row = {"total_ms": round(v[0], 4), "launches": v[1],
+                       "avg_us": round(1e3 * avg, 2)}
+                b = algorithmic_bytes(k, n, res_["entries"], res_["contacts"], ncells, fp64)
+                if b:
+                    row["algorithmic_GBs"] = round(b / (avg * 1e-3) / 1e9, 1)
+                out[k] = row
+            return out
+        phases = phase_table(kt, fp32, False)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
@@ -562,9 +605,7 @@ def main():
                          "algorithmic_bytes_per_launch": ab, "avg_launch_us": 1e3 * avg_ms,
                          "traffic": traffic},
             "phases_fp32_split": phases,
-            "phases_fp64": {k: {"total_ms": round(v[0], 4), "launches": v[1],
-                                "avg_us": round(1e3 * v[0] / v[1], 2)}
-                            for k, v in fp64["kt"].items()},
+            "phases_fp64": phase_table(fp64["kt"], fp64, True),
             "clocks": clocks,
             "e2e": {"value": world * n * args.e2e_steps / e2e_dt, "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

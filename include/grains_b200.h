@@ -112,6 +112,13 @@ int gdem_step_counts(gdem_handle h, int64_t* evaluations, int64_t* rebuilds);
  * ill-conditioned (a small difference of large terms).  Zero in FP64 mode. */
 int gdem_law_counts(gdem_handle h, int64_t* evaluated, int64_t* reevaluated, int reset);
 
+/* Systems with convex bodies: GJK closest-point calls of the force kernels
+ * since the last reset (pairs and walls whose bounding spheres overlap), their
+ * iterations, and the most iterations of one call (the reference stops at
+ * 1000, Convex.cpp:536-627).  No counterpart in the reference. */
+int gdem_gjk_counts(gdem_handle h, int64_t* calls, int64_t* iterations, int64_t* max_iterations,
+                    int reset);
+
 /* Per-kernel device timing with CUDA events (replaces the SCT_* phase timers,
  * Base/include/solvercomputingtime.hh:46-75).  While on, gdem_step uses plain
  * launches instead of graph replay.  gdem_kernel_times returns, per timed
@@ -125,6 +132,23 @@ int gdem_kernel_times(gdem_handle h, int capacity, int* count, char* names, doub
  * owner's instance), kdelta, previous normal, spring torque (3 each). */
 int gdem_upload_history(gdem_handle h, int64_t n, const int* owner, const int* partner,
                         const double* kdelta, const double* prevn, const double* spring);
+
+/* Launch tuning, before gdem_init.  No counterpart in the reference (its
+ * LinkedCell has a cell size only, Grains.cpp:1005-1022).  skin_factor is
+ * the pair-list skin as a multiple of each instance's largest circumscribed
+ * radius (it sets the pair-list cell size, 2 rmax f + skin, and how often the
+ * list is rebuilt; < 0 restores the LinkedCell Skin attribute or 0.25);
+ * blocks_per_sm is the force kernels' persistent grid, in blocks per
+ * multiprocessor (<= 0: 4).  Results do not depend on either. */
+int gdem_set_tuning(gdem_handle h, double skin_factor, int blocks_per_sm);
+
+/* Autotuner, before gdem_init: steps copies of the uploaded system for
+ * trial_steps steps per candidate (skin factors 0.1, 0.175, 0.25, 0.4, 0.6,
+ * then 2, 4 or 8 blocks per multiprocessor at the best skin), applies the
+ * fastest with gdem_set_tuning and returns it with its device time per step.
+ * Needs device memory for one more copy of the system. */
+int gdem_autotune(gdem_handle h, int trial_steps, double* skin_factor, int* blocks_per_sm,
+                  double* ms_per_step);
 
 /* Leapfrog start (Grains.cpp:168-173): forces at t0, then zero the
  * cumulative tangential and rolling memories. */

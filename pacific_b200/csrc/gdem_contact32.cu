@@ -291,7 +291,7 @@ __global__ void __launch_bounds__(256) k_pairs32(DevState S, const int* gate) {
     ++cnt;
   });
   if (cnt > kPairCap) { raise(S.status, kErrPairsFull); cnt = kPairCap; }
-  sortEntriesById(out, cnt, S.id);
+  S.nupper[t] = sortEntriesUpperFirst(out, cnt, S.id, S.id[t]);
   S.npairs[t] = cnt;
 }
 
@@ -299,82 +299,99 @@ __global__ void __launch_bounds__(256) k_pairs32(DevState S, const int* gate) {
 // (it is kept out of the sphere-only kernel, whose registers it would triple).
 template <bool kConvex>
 __device__ __forceinline__ void forcesOn32(DevState const& S, int t, int na, int sparse,
-                                           int& nlaw, int& nre) {
+                                           int& nlaw, int& nre, GjkTally& gjk) {
   const int cap = S.cap;
   const int4 cc = S.cellc[t];
   GridDesc const& g = S.grids[cc.w];
   const unsigned tag = (unsigned)S.ctl[kCtlEpoch], tag_old = tag - 1u;
   const int ida = S.id[t];
   TypeDesc const& ta = S.types[S.type[t]];
-  const d3 xt = ld3(S.x, cap, t);
+  const d3 xt = ld3(S.x, cap, t), vt = ld3(S.v, cap, t), wt = ld3(S.w, cap, t);
   float3 Fs = f3(0.f, 0.f, 0.f), Ts = f3(0.f, 0.f, 0.f);
-  const int np = na & kActMask;
-  const int* seg = S.act + (size_t)t * kPairCap;
-  for (int e = 0; e < np; ++e) {
-    const uint32_t ent = (uint32_t)seg[e];
-    const int u = (int)(ent & ((1u << 27) - 1));
-    const int idb = S.id[u];
-    const bool t0 = ida < idb;
-    TypeDesc const& tb = S.types[S.type[u]];
-    const TypeDesc& tp0 = t0 ? ta : tb;
-    const TypeDesc& tp1 = t0 ? tb : ta;
-    const int s0 = t0 ? t : u, s1 = t0 ? u : t;
-    // exact narrow phase on the FP64 master positions: lower ID at its own
-    // position, the other at its periodic image seen from it
-    int sh[3];
-    entryShift(S, ent, t, u, sh);
-    const d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
-    const d3 xu = ld3(S.x, cap, u);
-    const d3 x0 = t0 ? xt : xu;
-    const d3 x1 = t0 ? xu + shift : xt + (-shift);
-    Contact64 ct;
-    if (!kConvex || (ta.shape == 0 && tb.shape == 0)) {
-      ct = sphereSphere64(x0, tp0.radius, tp0.crust, x1, tp1.radius, tp1.crust);
-    } else {
-      ct = convexContact64(convexOf(tp0, S.poly_verts),
-                           crustXForm(S.basis, cap, s0, tp0.scaling, x0), tp0.radius, tp0.crust,
-                           convexOf(tp1, S.poly_verts),
-                           crustXForm(S.basis, cap, s1, tp1.scaling, x1), tp1.radius, tp1.crust);
-    }
-    if (S.diag) S.pair_delta[(size_t)t * kPairCap + e] = ct.contact && ct.dist < 0. ? ct.dist : __longlong_as_double(0x7ff0000000000000ll);
-    if (!ct.contact || !(ct.dist < 0.)) continue;
-    if (ct.error) raise(S.status, kErrContactOverlap);
-    // the force law from here on is FP32 (FP64 when ill-conditioned)
-    const float3 lev0 = tof(ct.point - x0);
-    const float3 lev1 = tof(ct.point - x1);
-    ModelDesc const& m = S.models[g.model_base + tp0.mat * kMaxMat + tp1.mat];
-    const Body64 b0{x0, ld3(S.v, cap, s0), ld3(S.w, cap, s0), tp0.mass, tp0.eqrad};
-    const Body64 b1{x1, ld3(S.v, cap, s1), ld3(S.w, cap, s1), tp1.mass, tp1.eqrad};
-    float3 f, mr, kd = f3(0.f, 0.f, 0.f), pn = kd, sp = kd;
-    int re;
-    ++nlaw;
-    if (m.memory) {
-      const int id0 = t0 ? ida : idb, id1 = t0 ? idb : ida;
-      const unsigned long long key = pairKey(id0, id1);
-      int old = histFind(S.hist_old, key, tag_old);
-      if (old >= 0) loadHistF(S.hist_old, old, kd, pn, sp);
-      contactLaw32(m, S.dt, ct, b0, b1, old >= 0, kd, pn, sp, f, mr, re);
-      if (t0) {
-        int slot = histInsert(S.hist_new, key, tag);
-        if (slot < 0) raise(S.status, kErrHashFull);
-        else storeHistF(S.hist_new, slot, kd, pn, sp);
+  // the pair-list entries that pass the contact filter's test
+  const int np = (!sparse || (na & kHasPair)) ? S.npairs[t] : 0;
+  const int* seg = S.pairs + (size_t)t * kPairCap;
+  GridDesc const& bg = S.bgrids[cc.w];
+  const float4 pt = S.posf[t];
+  for (int e0 = 0; e0 < np; e0 += kProbe) {
+    unsigned keep = probeEntries(S, bg, pt, seg, e0, np);
+    if (S.diag)
+      for (int e = e0; e < min(e0 + kProbe, np); ++e)
+        if (!(keep >> (e - e0) & 1u))
+          S.pair_delta[(size_t)t * kPairCap + e] = __longlong_as_double(0x7ff0000000000000ll);
+    // the kept entries in list order; lane by lane the k-th kept entries run
+    // together, as the warp's lanes hold different particles
+    while (keep) {
+      const int e = e0 + __ffs(keep) - 1;
+      keep &= keep - 1u;
+      const uint32_t ent = (uint32_t)seg[e];
+      const int u = (int)(ent & ((1u << 27) - 1));
+      const int idb = S.id[u];
+      const bool t0 = ida < idb;
+      TypeDesc const& tb = S.types[S.type[u]];
+      const TypeDesc& tp0 = t0 ? ta : tb;
+      const TypeDesc& tp1 = t0 ? tb : ta;
+      const int s0 = t0 ? t : u, s1 = t0 ? u : t;
+      // exact narrow phase on the FP64 master positions: lower ID at its own
+      // position, the other at its periodic image seen from it
+      int sh[3];
+      entryShift(S, ent, t, u, sh);
+      const d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
+      // (the partner's velocities are loaded with its position: a kept entry
+      // is nearly always a contact, and the loads then overlap)
+      const d3 xu = ld3(S.x, cap, u), vu = ld3(S.v, cap, u), wu = ld3(S.w, cap, u);
+      const d3 x0 = t0 ? xt : xu;
+      const d3 x1 = t0 ? xu + shift : xt + (-shift);
+      Contact64 ct;
+      if (!kConvex || (ta.shape == 0 && tb.shape == 0)) {
+        ct = sphereSphere64(x0, tp0.radius, tp0.crust, x1, tp1.radius, tp1.crust);
+      } else {
+        ct = convexContact64(convexOf(tp0, S.poly_verts),
+                             crustXForm(S.basis, cap, s0, tp0.scaling, x0), tp0.radius, tp0.crust,
+                             convexOf(tp1, S.poly_verts),
+                             crustXForm(S.basis, cap, s1, tp1.scaling, x1), tp1.radius, tp1.crust);
+        gjk.add(ct.gjk_iters);
       }
-    } else {
-      contactLaw32(m, S.dt, ct, b0, b1, false, kd, pn, sp, f, mr, re);
-    }
-    nre += re;
-    if (S.diag) {
-      double* fd = S.pair_force + 3 * ((size_t)t * kPairCap + e);
-      fd[0] = f.x; fd[1] = f.y; fd[2] = f.z;
-    }
-    if (t0) {
-      Fs = Fs + f;
-      Ts = Ts + crossf(lev0, f);
-      if (m.rolling) Ts = Ts + mr;
-    } else {
-      Fs = Fs - f;
-      Ts = Ts - crossf(lev1, f);
-      if (m.rolling) Ts = Ts - mr;
+      if (S.diag) S.pair_delta[(size_t)t * kPairCap + e] = ct.contact && ct.dist < 0. ? ct.dist : __longlong_as_double(0x7ff0000000000000ll);
+      if (!ct.contact || !(ct.dist < 0.)) continue;
+      if (ct.error) raise(S.status, kErrContactOverlap);
+      // the force law from here on is FP32 (FP64 when ill-conditioned)
+      const float3 lev0 = tof(ct.point - x0);
+      const float3 lev1 = tof(ct.point - x1);
+      ModelDesc const& m = S.models[g.model_base + tp0.mat * kMaxMat + tp1.mat];
+      const Body64 b0{x0, t0 ? vt : vu, t0 ? wt : wu, tp0.mass, tp0.eqrad};
+      const Body64 b1{x1, t0 ? vu : vt, t0 ? wu : wt, tp1.mass, tp1.eqrad};
+      float3 f, mr, kd = f3(0.f, 0.f, 0.f), pn = kd, sp = kd;
+      int re;
+      ++nlaw;
+      if (m.memory) {
+        const int id0 = t0 ? ida : idb, id1 = t0 ? idb : ida;
+        const unsigned long long key = pairKey(id0, id1);
+        int old = histFind(S.hist_old, key, tag_old);
+        if (old >= 0) loadHistF(S.hist_old, old, kd, pn, sp);
+        contactLaw32(m, S.dt, ct, b0, b1, old >= 0, kd, pn, sp, f, mr, re);
+        if (t0) {
+          int slot = histInsert(S.hist_new, key, tag);
+          if (slot < 0) raise(S.status, kErrHashFull);
+          else storeHistF(S.hist_new, slot, kd, pn, sp);
+        }
+      } else {
+        contactLaw32(m, S.dt, ct, b0, b1, false, kd, pn, sp, f, mr, re);
+      }
+      nre += re;
+      if (S.diag) {
+        double* fd = S.pair_force + 3 * ((size_t)t * kPairCap + e);
+        fd[0] = f.x; fd[1] = f.y; fd[2] = f.z;
+      }
+      if (t0) {
+        Fs = Fs + f;
+        Ts = Ts + crossf(lev0, f);
+        if (m.rolling) Ts = Ts + mr;
+      } else {
+        Fs = Fs - f;
+        Ts = Ts - crossf(lev1, f);
+        if (m.rolling) Ts = Ts - mr;
+      }
     }
   }
   // walls: geometry from the FP64 master position, force law in FP32
@@ -387,13 +404,14 @@ __device__ __forceinline__ void forcesOn32(DevState const& S, int t, int na, int
                           ta.radius, ta.crust, convexOf(wd),
                           identityXForm(wd.scaling, mk(wd.centre[0], wd.centre[1], wd.centre[2])),
                           wd.radius, wd.crust);
+    if (kConvex) gjk.add(ct.gjk_iters);
     if (S.diag) S.wall_delta[(size_t)t * S.max_walls + k] = ct.contact ? ct.dist : __longlong_as_double(0x7ff0000000000000ll);
     if (ct.error) raise(S.status, kErrContactOverlap);
     if (!ct.contact || !(ct.dist < 0.)) continue;
     ModelDesc const& m = S.models[g.model_base + ta.mat * kMaxMat + wd.mat];
     const float3 lev0 = tof(ct.point - xt);
     const d3 zero = mk(0., 0., 0.);
-    const Body64 b0{xt, ld3(S.v, cap, t), ld3(S.w, cap, t), ta.mass, ta.eqrad};
+    const Body64 b0{xt, vt, wt, ta.mass, ta.eqrad};
     const Body64 b1{mk(wd.centre[0], wd.centre[1], wd.centre[2]), zero, zero, 1.e20, wd.eqrad};
     float3 f, mr, kd = f3(0.f, 0.f, 0.f), pn = kd, sp = kd;
     int re;
@@ -432,11 +450,14 @@ template <bool kConvex>
 __global__ void __launch_bounds__(256) k_forces32(DevState S, int sparse) {
   const int stride = gridDim.x * blockDim.x;
   const int nw = sparse ? S.ctl[kCtlWork] : S.n;
+  const int* flags = contactFlags(S);
   int nlaw = 0, nre = 0;   // contacts evaluated / re-evaluated in FP64
+  GjkTally gjk;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += stride) {
     const int t = sparse ? S.work[i] : i;
-    forcesOn32<kConvex>(S, t, S.nact[t], sparse, nlaw, nre);
+    forcesOn32<kConvex>(S, t, flags[t], sparse, nlaw, nre, gjk);
   }
+  if constexpr (kConvex) gjk.flush(S.gjk_counts);
   // warp-aggregated counters of the FP64 re-evaluations (every lane of the
   // warp reaches this point: no thread leaves the loop early)
   const int wl = __reduce_add_sync(0xffffffffu, nlaw), wr = __reduce_add_sync(0xffffffffu, nre);
@@ -453,7 +474,7 @@ void launch_pairs32(DevState const& S, const int* gate, cudaStream_t st) {
 }
 void launch_forces32(DevState const& S, int sparse, cudaStream_t st) {
   if (!S.n) return;
-  const int grid = std::min((S.n + 255) / 256, 4 * S.nsm);
+  const int grid = std::min((S.n + 255) / 256, (S.forces_bps > 0 ? S.forces_bps : 4) * S.nsm);
   if (S.any_convex) k_forces32<true><<<grid, 256, 0, st>>>(S, sparse);
   else k_forces32<false><<<grid, 256, 0, st>>>(S, sparse);
 }

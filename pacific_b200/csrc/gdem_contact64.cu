@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(256) k_pairs64(DevState S, const int* gate) {
     ++cnt;
   });
   if (cnt > kPairCap) { raise(S.status, kErrPairsFull); cnt = kPairCap; }
-  sortEntriesById(out, cnt, S.id);
+  S.nupper[t] = sortEntriesUpperFirst(out, cnt, S.id, S.id[t]);
   S.npairs[t] = cnt;
 }
 
@@ -69,7 +69,8 @@ __device__ __forceinline__ void storeHist(HistTable const& t, int slot, d3 kd, d
 // kConvex: some class is not a sphere, so the GJK narrow phase is compiled in
 // (it is kept out of the sphere-only kernel, whose registers it would triple).
 template <bool kConvex>
-__device__ __forceinline__ void forcesOn64(DevState const& S, int t, int na, int sparse) {
+__device__ __forceinline__ void forcesOn64(DevState const& S, int t, int na, int sparse,
+                                           GjkTally& gjk) {
   const int cap = S.cap;
   const int4 cc = S.cellc[t];
   GridDesc const& g = S.grids[cc.w];
@@ -80,77 +81,92 @@ __device__ __forceinline__ void forcesOn64(DevState const& S, int t, int na, int
   d3 T = mk(0., 0., 0.);
   const double dt = S.dt;
   const unsigned tag = (unsigned)S.ctl[kCtlEpoch], tag_old = tag - 1u;
-  const int np = na & kActMask;
-  const int* seg = S.act + (size_t)t * kPairCap;
-  for (int e = 0; e < np; ++e) {
-    const uint32_t ent = (uint32_t)seg[e];
-    const int u = (int)(ent & ((1u << 27) - 1));
-    int sh[3];
-    entryShift(S, ent, t, u, sh);
-    d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
-    const int idb = S.id[u];
-    TypeDesc const& tb = S.types[S.type[u]];
-    const d3 xu = ld3(S.x, cap, u), vu = ld3(S.v, cap, u), wu = ld3(S.w, cap, u);
-    const bool t0 = ida < idb;
-    // canonical bodies: p0 = lower ID at its own position, p1 at its image
-    d3 x0, x1, v0, v1, w0, w1;
-    double r0, r1, c0, c1, m0, m1, q0, q1;
-    int mat0, mat1, id0, id1;
-    if (t0) {
-      x0 = xt; v0 = vt; w0 = wt; r0 = ta.radius; m0 = ta.mass; q0 = ta.eqrad; c0 = ta.crust;
-      mat0 = ta.mat; id0 = ida;
-      x1 = xu + shift; v1 = vu; w1 = wu; r1 = tb.radius; m1 = tb.mass; q1 = tb.eqrad;
-      c1 = tb.crust; mat1 = tb.mat; id1 = idb;
-    } else {
-      x0 = xu; v0 = vu; w0 = wu; r0 = tb.radius; m0 = tb.mass; q0 = tb.eqrad; c0 = tb.crust;
-      mat0 = tb.mat; id0 = idb;
-      x1 = xt + (-shift); v1 = vt; w1 = wt; r1 = ta.radius; m1 = ta.mass; q1 = ta.eqrad;
-      c1 = ta.crust; mat1 = ta.mat; id1 = ida;
-    }
-    Contact64 ct;
-    if (!kConvex || (ta.shape == 0 && tb.shape == 0)) {
-      ct = sphereSphere64(x0, r0, c0, x1, r1, c1);
-    } else {
-      TypeDesc const& tp0 = t0 ? ta : tb;
-      TypeDesc const& tp1 = t0 ? tb : ta;
-      const int s0 = t0 ? t : u, s1 = t0 ? u : t;
-      ct = convexContact64(convexOf(tp0, S.poly_verts), crustXForm(S.basis, cap, s0, tp0.scaling, x0),
-                           r0, c0, convexOf(tp1, S.poly_verts),
-                           crustXForm(S.basis, cap, s1, tp1.scaling, x1), r1, c1);
-    }
-    if (S.diag) S.pair_delta[(size_t)t * kPairCap + e] = ct.contact ? ct.dist : __longlong_as_double(0x7ff0000000000000ll);
-    if (!ct.contact || !(ct.dist < 0.)) continue;
-    if (ct.error) raise(S.status, kErrContactOverlap);
-    ModelDesc const& m = S.models[g.model_base + mat0 * kMaxMat + mat1];
-    d3 f, mr;
-    if (m.memory) {
-      const unsigned long long key = pairKey(id0, id1);
-      int old = histFind(S.hist_old, key, tag_old);
-      d3 kd, pn, sp;
-      if (old >= 0) loadHist(S.hist_old, old, kd, pn, sp);
-      hodc64(m, dt, ct.point, ct.overlap, x0, v0, w0, m0, q0, x1, v1, w1, m1, q1, old >= 0,
-             kd, pn, sp, f, mr);
+  // the pair-list entries that pass the contact filter's test
+  const int np = (!sparse || (na & kHasPair)) ? S.npairs[t] : 0;
+  const int* seg = S.pairs + (size_t)t * kPairCap;
+  GridDesc const& bg = S.bgrids[cc.w];
+  const float4 pt = S.posf[t];
+  for (int e0 = 0; e0 < np; e0 += kProbe) {
+    unsigned keep = probeEntries(S, bg, pt, seg, e0, np);
+    if (S.diag)
+      for (int e = e0; e < min(e0 + kProbe, np); ++e)
+        if (!(keep >> (e - e0) & 1u))
+          S.pair_delta[(size_t)t * kPairCap + e] = __longlong_as_double(0x7ff0000000000000ll);
+    // the kept entries in list order; lane by lane the k-th kept entries run
+    // together, as the warp's lanes hold different particles
+    while (keep) {
+      const int e = e0 + __ffs(keep) - 1;
+      keep &= keep - 1u;
+      const uint32_t ent = (uint32_t)seg[e];
+      const int u = (int)(ent & ((1u << 27) - 1));
+      int sh[3];
+      entryShift(S, ent, t, u, sh);
+      d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
+      const int idb = S.id[u];
+      TypeDesc const& tb = S.types[S.type[u]];
+      const d3 xu = ld3(S.x, cap, u), vu = ld3(S.v, cap, u), wu = ld3(S.w, cap, u);
+      const bool t0 = ida < idb;
+      // canonical bodies: p0 = lower ID at its own position, p1 at its image
+      d3 x0, x1, v0, v1, w0, w1;
+      double r0, r1, c0, c1, m0, m1, q0, q1;
+      int mat0, mat1, id0, id1;
       if (t0) {
-        int slot = histInsert(S.hist_new, key, tag);
-        if (slot < 0) raise(S.status, kErrHashFull);
-        else storeHist(S.hist_new, slot, kd, pn, sp);
+        x0 = xt; v0 = vt; w0 = wt; r0 = ta.radius; m0 = ta.mass; q0 = ta.eqrad; c0 = ta.crust;
+        mat0 = ta.mat; id0 = ida;
+        x1 = xu + shift; v1 = vu; w1 = wu; r1 = tb.radius; m1 = tb.mass; q1 = tb.eqrad;
+        c1 = tb.crust; mat1 = tb.mat; id1 = idb;
+      } else {
+        x0 = xu; v0 = vu; w0 = wu; r0 = tb.radius; m0 = tb.mass; q0 = tb.eqrad; c0 = tb.crust;
+        mat0 = tb.mat; id0 = idb;
+        x1 = xt + (-shift); v1 = vt; w1 = wt; r1 = ta.radius; m1 = ta.mass; q1 = ta.eqrad;
+        c1 = ta.crust; mat1 = ta.mat; id1 = ida;
       }
-    } else {
-      hooke64(m, ct.point, ct.overlap, x0, v0, w0, m0, q0, x1, v1, w1, m1, q1, f, mr);
-    }
-    if (S.diag) {
-      double* fd = S.pair_force + 3 * ((size_t)t * kPairCap + e);
-      fd[0] = f.x; fd[1] = f.y; fd[2] = f.z;
-    }
-    if (t0) {
-      F = F + f;
-      T = T + cross(ct.point - x0, f);
-      if (m.rolling) T = T + mr;
-    } else {
-      d3 fm = -f;
-      F = F + fm;
-      T = T + cross(ct.point - x1, fm);
-      if (m.rolling) T = T + (-mr);
+      Contact64 ct;
+      if (!kConvex || (ta.shape == 0 && tb.shape == 0)) {
+        ct = sphereSphere64(x0, r0, c0, x1, r1, c1);
+      } else {
+        TypeDesc const& tp0 = t0 ? ta : tb;
+        TypeDesc const& tp1 = t0 ? tb : ta;
+        const int s0 = t0 ? t : u, s1 = t0 ? u : t;
+        ct = convexContact64(convexOf(tp0, S.poly_verts), crustXForm(S.basis, cap, s0, tp0.scaling, x0),
+                             r0, c0, convexOf(tp1, S.poly_verts),
+                             crustXForm(S.basis, cap, s1, tp1.scaling, x1), r1, c1);
+        gjk.add(ct.gjk_iters);
+      }
+      if (S.diag) S.pair_delta[(size_t)t * kPairCap + e] = ct.contact ? ct.dist : __longlong_as_double(0x7ff0000000000000ll);
+      if (!ct.contact || !(ct.dist < 0.)) continue;
+      if (ct.error) raise(S.status, kErrContactOverlap);
+      ModelDesc const& m = S.models[g.model_base + mat0 * kMaxMat + mat1];
+      d3 f, mr;
+      if (m.memory) {
+        const unsigned long long key = pairKey(id0, id1);
+        int old = histFind(S.hist_old, key, tag_old);
+        d3 kd, pn, sp;
+        if (old >= 0) loadHist(S.hist_old, old, kd, pn, sp);
+        hodc64(m, dt, ct.point, ct.overlap, x0, v0, w0, m0, q0, x1, v1, w1, m1, q1, old >= 0,
+               kd, pn, sp, f, mr);
+        if (t0) {
+          int slot = histInsert(S.hist_new, key, tag);
+          if (slot < 0) raise(S.status, kErrHashFull);
+          else storeHist(S.hist_new, slot, kd, pn, sp);
+        }
+      } else {
+        hooke64(m, ct.point, ct.overlap, x0, v0, w0, m0, q0, x1, v1, w1, m1, q1, f, mr);
+      }
+      if (S.diag) {
+        double* fd = S.pair_force + 3 * ((size_t)t * kPairCap + e);
+        fd[0] = f.x; fd[1] = f.y; fd[2] = f.z;
+      }
+      if (t0) {
+        F = F + f;
+        T = T + cross(ct.point - x0, f);
+        if (m.rolling) T = T + mr;
+      } else {
+        d3 fm = -f;
+        F = F + fm;
+        T = T + cross(ct.point - x1, fm);
+        if (m.rolling) T = T + (-mr);
+      }
     }
   }
   // walls: the particle is p0, the obstacle p1 (mass Component::m_massObstacle)
@@ -163,6 +179,7 @@ __device__ __forceinline__ void forcesOn64(DevState const& S, int t, int na, int
                           ta.radius, ta.crust, convexOf(wd),
                           identityXForm(wd.scaling, mk(wd.centre[0], wd.centre[1], wd.centre[2])),
                           wd.radius, wd.crust);
+    if (kConvex) gjk.add(ct.gjk_iters);
     if (S.diag) S.wall_delta[(size_t)t * S.max_walls + k] = ct.contact ? ct.dist : __longlong_as_double(0x7ff0000000000000ll);
     if (ct.error) raise(S.status, kErrContactOverlap);
     if (!ct.contact || !(ct.dist < 0.)) continue;
@@ -203,10 +220,14 @@ template <bool kConvex>
 __global__ void __launch_bounds__(256) k_forces64(DevState S, int sparse) {
   const int stride = gridDim.x * blockDim.x;
   const int nw = sparse ? S.ctl[kCtlWork] : S.n;
+  const int* flags = contactFlags(S);
+  GjkTally gjk;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += stride) {
     const int t = sparse ? S.work[i] : i;
-    forcesOn64<kConvex>(S, t, S.nact[t], sparse);
+    forcesOn64<kConvex>(S, t, flags[t], sparse, gjk);
   }
+  // (every lane of the warp reaches this point: no thread leaves the loop early)
+  if constexpr (kConvex) gjk.flush(S.gjk_counts);
 }
 
 }  // namespace
@@ -216,7 +237,7 @@ void launch_pairs64(DevState const& S, const int* gate, cudaStream_t st) {
 }
 void launch_forces64(DevState const& S, int sparse, cudaStream_t st) {
   if (!S.n) return;
-  const int grid = std::min((S.n + 255) / 256, 4 * S.nsm);
+  const int grid = std::min((S.n + 255) / 256, (S.forces_bps > 0 ? S.forces_bps : 4) * S.nsm);
   if (S.any_convex) k_forces64<true><<<grid, 256, 0, st>>>(S, sparse);
   else k_forces64<false><<<grid, 256, 0, st>>>(S, sparse);
 }

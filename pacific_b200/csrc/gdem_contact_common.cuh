@@ -13,6 +13,27 @@ struct Contact64 {
   double dist;
   bool contact;
   bool error;
+  int gjk_iters = 0;     // GJK iterations spent on this pair (0: no GJK call)
+};
+
+// GJK work of one thread of a force kernel (convex systems): calls,
+// iterations and the most iterations of one call; flushed once per warp.
+struct GjkTally {
+  int calls = 0, iters = 0, maxit = 0;
+  __device__ __forceinline__ void add(int it) {
+    if (it > 0) { ++calls; iters += it; maxit = max(maxit, it); }
+  }
+  // every lane of the warp calls this
+  __device__ __forceinline__ void flush(unsigned long long* out) const {
+    const unsigned full = 0xffffffffu;
+    const int c = __reduce_add_sync(full, calls), i = __reduce_add_sync(full, iters);
+    const int m = __reduce_max_sync(full, (unsigned)maxit);
+    if ((threadIdx.x & 31) == 0 && c) {
+      atomicAdd(out, (unsigned long long)c);
+      atomicAdd(out + 1, (unsigned long long)i);
+      atomicMax(out + 2, (unsigned long long)m);
+    }
+  }
 };
 
 // ClosestPointSPHERESPHERE (Geometry/src/RigidBodyWithCrust.cpp:596-639).
@@ -167,6 +188,7 @@ __device__ inline Contact64 convexContact64(ConvexRef const& a, XForm64 const& a
   d3 pA, pB;
   int it = 0;
   double distance = closestPoints64(a, a2w, b, b2w, pA, pB, &it);
+  c.gjk_iters = it;
   if (distance < 1.0e-10) { c.error = true; return c; }
   d3 ba = pA - pB;
   d3 contact = pA / 2.0 + pB / 2.0;

@@ -99,6 +99,10 @@ struct DevState {
   double dt;
   int* id; int* type; int* inst;
   double* x; double* v; double* w; double* wbf; double* q; double* F; double* T;
+  // wbf_state: w_bf is integrated (FP64 mode, or convex bodies present);
+  // otherwise (FP32-split, spheres only) w is the angular state and w_bf is
+  // derived on output as q* w q
+  int wbf_state;
   double* basis;          // 9 per particle, non-spherical shapes only
   // second buffers: a step reads x, v, w, w_bf, q, basis and writes x2 ...;
   // a pair-list rebuild permutes everything into them and copies back
@@ -122,13 +126,16 @@ struct DevState {
   int4* cellc;            // pair-list cell i, j, k and instance at the last rebuild
   // pair list: per-particle segments of kPairCap entries
   int* pairs; int* npairs;   // skin list (rebuilt on demand)
-  int* act; int* nact;       // entries of the skin list in contact this step (same layout)
-  float4* posf;           // FP32 position + circumscribed radius (contact filter)
+  int* nupper;            // entries of each list whose partner has a higher ID (listed first)
+  int* nact;              // contact-filter flags, two buffers of cap (contactFlags)
+  float4* posf;           // FP32 continuous position since the last rebuild + circumscribed radius
   int* work;              // particles with a listed contact or near a wall (this step)
   int nsm;                // multiprocessors of the device (persistent grids)
+  int forces_bps;         // blocks per multiprocessor of the force kernels' persistent grid (0: 4)
   double* pair_delta;     // diagnostics: overlap of each entry (+inf: no contact)
   double* wall_delta;     // diagnostics: overlap with each wall slot
   double* pair_force;     // diagnostics: contact force on the lower ID (3 per entry)
+  unsigned long long* gjk_counts;   // convex: GJK calls, iterations, most iterations of a call
   unsigned long long* law_counts;   // FP32-split: contacts evaluated, re-evaluated in FP64
   double* wall_force;     // diagnostics: wall contact force on the particle (3 per slot)
   int diag;
@@ -277,20 +284,36 @@ __device__ __forceinline__ void forEachCandidate(const int* __restrict__ cs, Gri
   }
 }
 
-// Orders a particle's list entries by partner ID, so that the reduction
-// order of its forces does not depend on the cells at the last rebuild (nor
-// on when the list was rebuilt).
-__device__ __forceinline__ void sortEntriesById(int* seg, int cnt, const int* id) {
-  for (int i = 1; i < cnt; ++i) {
+// Orders a particle's list entries by partner ID, the partners with a
+// higher ID than the particle's own (idt) first, and returns how many those
+// are.  The reduction order of its forces then does not depend on the cells
+// at the last rebuild (nor on when the list was rebuilt), and the contact
+// filter tests each pair once, from the lower ID's "upper" entries.
+__device__ __forceinline__ int sortEntriesUpperFirst(int* seg, int cnt, const int* id, int idt) {
+  auto key = [&](int e) {
+    const int idu = id[e & ((1 << 27) - 1)];
+    return idu > idt ? idu : (1 << 30) | idu;
+  };
+  int nup = 0;
+  for (int i = 0; i < cnt; ++i) {
     const int e = seg[i];
-    const int ide = id[e & ((1 << 27) - 1)];
+    const int ke = key(e);
+    if (ke < (1 << 30)) ++nup;
     int j = i - 1;
-    while (j >= 0 && id[seg[j] & ((1 << 27) - 1)] > ide) {
+    while (j >= 0 && key(seg[j]) > ke) {
       seg[j + 1] = seg[j];
       --j;
     }
     seg[j + 1] = e;
   }
+  return nup;
+}
+
+// Contact-filter flags of the current force evaluation: two buffers used
+// alternately, the filter of one evaluation clearing the other's, so that no
+// kernel needs to clear flags that other warps may still be setting.
+__device__ __forceinline__ int* contactFlags(DevState const& S, int which = 0) {
+  return S.nact + (size_t)(((unsigned)S.ctl[kCtlEpoch] + (unsigned)which) & 1u) * S.cap;
 }
 
 // Code of a periodic image shift (in periods, each -1, 0 or 1) in 0..26.

@@ -76,7 +76,43 @@ struct InstanceDesc {
   double gravity[3];
   double dt;
   int nmat;
+  // what the pair-list grid is made from (it is remade when the skin changes)
+  double box_org[3], box_max[3];
+  int box_per[3];
+  double cellsize;      // 2 rmax f: the reference cell size
+  double max_radius;    // largest circumscribed radius
+  double xml_skin;      // LinkedCell Skin attribute, or < 0 when absent
 };
+
+// Pair-list grid of one instance for a skin (a length).  The list holds the
+// pairs whose bounding spheres are closer than the skin and stays valid while
+// no particle has moved more than skin / 2, so its cells must be at least
+// 2 rmax f + skin wide; the skin shrinks when a periodic direction would get
+// fewer than 3 cells.  Only the cell layout and the skin change; the fields
+// shared with the reference grid (safe bands, periods, filter margin) stay.
+void makePairGrid(InstanceDesc& I, double skin) {
+  if (!(skin >= 0.)) throw std::runtime_error("LinkedCell Skin must be >= 0");
+  for (int d = 0; d < 3; ++d)
+    if (I.box_per[d])
+      skin = std::min(skin, std::max(0., (I.box_max[d] - I.box_org[d]) / 3. - I.cellsize) * 0.999999);
+  GridDesc& b = I.bgrid;
+  for (int d = 0; d < 3; ++d) {
+    double size = I.box_max[d] - I.box_org[d];
+    int n = (int)((size + 1.0e-10) / (I.cellsize + skin));
+    if (!n) n = 1;
+    if (I.box_per[d] && n < 3) n = 3;
+    b.nb[d] = n;
+    b.edge[d] = size / n;
+    b.lc_origin[d] = I.box_org[d];
+    if (I.box_per[d]) {
+      b.lc_origin[d] += -b.edge[d];
+      b.nb[d] += 2;
+    }
+    b.edge_f[d] = (float)b.edge[d];
+  }
+  b.skin = skin;
+  b.skin_f = (float)skin;
+}
 
 int materialIndex(std::map<std::string, int>& mats, std::vector<std::string>& order,
                   std::string const& name) {
@@ -417,35 +453,20 @@ InstanceDesc readInstance(std::string const& path) {
     }
     g.edge_f[d] = (float)g.edge[d];
   }
-  // Pair-list grid.  The list holds the pairs whose bounding spheres are
-  // closer than the skin and stays valid while no particle has moved more
-  // than skin / 2, so its cells must be at least 2 rmax f + skin wide.  The
-  // skin defaults to a quarter of the largest circumscribed radius (the
-  // LinkedCell attribute Skin, a length, overrides it; 0 rebuilds the list
-  // every step); it shrinks when a periodic direction would get fewer than 3
-  // cells.
-  double skin = lc->has("Skin") ? lc->attrD("Skin") : 0.25 * maxR;
-  if (!(skin >= 0.)) throw std::runtime_error("LinkedCell Skin must be >= 0");
-  for (int d = 0; d < 3; ++d)
-    if (per[d]) skin = std::min(skin, std::max(0., (maxc[d] - org[d]) / 3. - cellsize) * 0.999999);
+  // Pair-list grid.  The skin defaults to a quarter of the largest
+  // circumscribed radius (the LinkedCell attribute Skin, a length, overrides
+  // it; 0 rebuilds the list every step).
+  for (int d = 0; d < 3; ++d) {
+    I.box_org[d] = org[d];
+    I.box_max[d] = maxc[d];
+    I.box_per[d] = per[d];
+  }
+  I.cellsize = cellsize;
+  I.max_radius = maxR;
+  I.xml_skin = lc->has("Skin") ? lc->attrD("Skin") : -1.;
   GridDesc& b = I.bgrid;
   b = g;
-  for (int d = 0; d < 3; ++d) {
-    double size = maxc[d] - org[d];
-    int n = (int)((size + 1.0e-10) / (cellsize + skin));
-    if (!n) n = 1;
-    if (per[d] && n < 3) n = 3;
-    b.nb[d] = n;
-    b.edge[d] = size / n;
-    b.lc_origin[d] = org[d];
-    if (per[d]) {
-      b.lc_origin[d] += -b.edge[d];
-      b.nb[d] += 2;
-    }
-    b.edge_f[d] = (float)b.edge[d];
-  }
-  b.skin = skin;
-  b.skin_f = (float)skin;
+  makePairGrid(I, I.xml_skin >= 0. ? I.xml_skin : 0.25 * maxR);
   // FP32 contact filter: positions rounded to float carry at most half an ulp
   // of the largest coordinate each (2^-24 relative); 5e-7 of it bounds the
   // error of a difference plus an image shift with room to spare
@@ -455,7 +476,11 @@ InstanceDesc readInstance(std::string const& path) {
     b.Lf[d] = (float)(maxc[d] - org[d]);
     g.Lf[d] = b.Lf[d];
   }
-  b.filt_margin = (float)(5.e-7 * maxabs);
+  // (the filter's positions are continuous since the last rebuild, so they
+  // may leave the box by less than a period: the margin allows a period more)
+  double maxL = 0.;
+  for (int d = 0; d < 3; ++d) maxL = std::max(maxL, maxc[d] - org[d]);
+  b.filt_margin = (float)(5.e-7 * (maxabs + maxL));
   g.filt_margin = b.filt_margin;
   // band in which a particle stays in the reference grid's inner cells
   // (periodic: cells 1 .. nb-2; otherwise 0 .. nb-1), with a relative margin
@@ -474,6 +499,11 @@ InstanceDesc readInstance(std::string const& path) {
 struct System {
   int precision = GDEM_FP64;
   std::vector<InstanceDesc> inst;
+  std::vector<std::string> xml_paths;
+  std::vector<GridDesc> h_bgrids;  // host copy of the pair-list grids
+  std::vector<int> h_type, h_inst; // uploaded classes (instance-local) and instances, by ID
+  double tune_skin = -1.;          // skin as a multiple of rmax (< 0: the XML's or 0.25)
+  int tune_bps = 0;                // force-kernel blocks per multiprocessor (0: 4)
   std::vector<int> type_base;     // first global type of each instance
   std::vector<int> id_base;       // first particle ID of each instance
   std::vector<int> inst_n;
@@ -537,6 +567,44 @@ struct System {
   void invalidateGraphs() {
     for (auto& row : graph)
       for (auto& gx : row) if (gx) { cudaGraphExecDestroy(gx); gx = nullptr; }
+  }
+  void freeAlloc(void* p) {
+    for (auto& a : allocs)
+      if (a == p) { CK(cudaFree(a)); a = allocs.back(); allocs.pop_back(); return; }
+  }
+
+  // Pair-list skin (a multiple of each instance's largest circumscribed
+  // radius; < 0 restores the XML's) and the force kernels' blocks per
+  // multiprocessor (<= 0: the default).  Neither changes a result: the
+  // contact set is exact for any skin and the sums run in partner-ID order.
+  void applyTuning(double skin_factor, int bps) {
+    if (started) throw std::runtime_error("tuning is set before gdem_init");
+    tune_skin = skin_factor;
+    tune_bps = bps > 0 ? bps : 0;
+    int offset = 0;
+    for (size_t k = 0; k < inst.size(); ++k) {
+      InstanceDesc& I = inst[k];
+      makePairGrid(I, skin_factor >= 0. ? skin_factor * I.max_radius
+                                        : (I.xml_skin >= 0. ? I.xml_skin : 0.25 * I.max_radius));
+      GridDesc b = I.bgrid;
+      b.cell_offset = offset;
+      b.wall_begin = h_bgrids[k].wall_begin;
+      b.wall_count = h_bgrids[k].wall_count;
+      b.model_base = h_bgrids[k].model_base;
+      offset += b.nb[0] * b.nb[1] * b.nb[2];
+      h_bgrids[k] = b;
+    }
+    CK(cudaMemcpy(d_bgrids, h_bgrids.data(), h_bgrids.size() * sizeof(GridDesc), cudaMemcpyHostToDevice));
+    S.forces_bps = tune_bps;
+    if (S.cell_count && offset != S.ncells) {
+      freeAlloc(S.cell_count); freeAlloc(S.cell_start); freeAlloc(S.scan_tmp);
+      S.ncells = offset;
+      S.cell_count = alloc<int>(S.ncells); S.cell_start = alloc<int>(S.ncells + 1);
+      S.scan_tmp = alloc<int>((S.ncells + 1023) / 1024 + 1);
+      CK(cudaMemset(S.cell_count, 0, (size_t)S.ncells * sizeof(int)));
+    }
+    S.ncells = offset;
+    invalidateGraphs();
   }
 
   // Runs f between two events when profiling (plain launches only).
@@ -621,6 +689,7 @@ struct System {
     };
     up(d_grids, grids); up(d_types, types); up(d_models, models); up(d_walls, walls);
     up(d_poly, poly); up(d_bgrids, bgrids);
+    h_bgrids = bgrids;
     S.grids = d_grids; S.types = d_types; S.models = d_models; S.walls = d_walls;
     S.bgrids = d_bgrids;
     S.poly_verts = d_poly;
@@ -649,6 +718,7 @@ struct System {
     S.cell_count = alloc<int>(S.ncells); S.cell_start = alloc<int>(S.ncells + 1);
     S.scan_tmp = alloc<int>((S.ncells + 1023) / 1024 + 1);
     S.cellc = alloc<int4>(c);
+    S.wbf_state = (precision == GDEM_FP64 || S.any_convex) ? 1 : 0;
     if (precision == GDEM_FP64) {
       S.pos64 = alloc<double4>(c);
       S.offh = nullptr;
@@ -656,8 +726,9 @@ struct System {
       S.offh = alloc<float4>(c);
       S.pos64 = nullptr;
     }
-    S.pairs = alloc<int>(c * kPairCap); S.npairs = alloc<int>(c);
-    S.act = alloc<int>(c * kPairCap); S.nact = alloc<int>(c);
+    S.pairs = alloc<int>(c * kPairCap); S.npairs = alloc<int>(c); S.nupper = alloc<int>(c);
+    S.nact = alloc<int>(2 * c);
+    CK(cudaMemset(S.nact, 0, 2 * c * sizeof(int)));
     S.work = alloc<int>(c);
     {
       int dev = 0;
@@ -681,6 +752,8 @@ struct System {
     CK(cudaMemset(S.status, 0, sizeof(int)));
     S.law_counts = alloc<unsigned long long>(2);
     CK(cudaMemset(S.law_counts, 0, 2 * sizeof(unsigned long long)));
+    S.gjk_counts = alloc<unsigned long long>(3);
+    CK(cudaMemset(S.gjk_counts, 0, 3 * sizeof(unsigned long long)));
     CK(cudaMemset(S.cell_count, 0, (size_t)S.ncells * sizeof(int)));
     CK(cudaMemset(S.F, 0, 3 * c * sizeof(double)));
     CK(cudaMemset(S.T, 0, 3 * c * sizeof(double)));
@@ -915,7 +988,10 @@ int gdem_create_batch(int n, const char* const* xml_paths, int precision, gdem_h
       throw CudaError("no CUDA device: the Grains3D B200 step has no CPU fallback");
     auto s = std::make_unique<System>();
     s->precision = precision;
-    for (int k = 0; k < n; ++k) s->inst.push_back(readInstance(xml_paths[k]));
+    for (int k = 0; k < n; ++k) {
+      s->inst.push_back(readInstance(xml_paths[k]));
+      s->xml_paths.push_back(xml_paths[k]);
+    }
     s->setupTables();
     CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     CK(cudaEventCreate(&s->ev0));
@@ -953,6 +1029,8 @@ int gdem_upload_state(gdem_handle h, int64_t n, const int* inst, const int* type
       hid[i] = i;
       s->inst_n[k]++;
     }
+    s->h_inst = hinst;
+    s->h_type.assign(type, type + N);
     s->id_base.assign(s->inst.size(), 0);
     for (size_t k = 1; k < s->inst.size(); ++k) s->id_base[k] = s->id_base[k - 1] + s->inst_n[k - 1];
     s->allocateParticles(N);
@@ -1057,6 +1135,22 @@ int gdem_law_counts(gdem_handle h, int64_t* evaluated, int64_t* reevaluated, int
   });
 }
 
+int gdem_gjk_counts(gdem_handle h, int64_t* calls, int64_t* iterations, int64_t* max_iterations,
+                    int reset) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state) throw std::runtime_error("no state");
+    unsigned long long r[3];
+    CK(cudaStreamSynchronize(s->stream));
+    CK(cudaMemcpy(r, s->S.gjk_counts, sizeof(r), cudaMemcpyDeviceToHost));
+    if (reset) CK(cudaMemset(s->S.gjk_counts, 0, sizeof(r)));
+    if (calls) *calls = (int64_t)r[0];
+    if (iterations) *iterations = (int64_t)r[1];
+    if (max_iterations) *max_iterations = (int64_t)r[2];
+    return GDEM_OK;
+  });
+}
+
 int gdem_set_profiling(gdem_handle h, int on) {
   return guarded([&] {
     System* s = sys(h);
@@ -1137,6 +1231,79 @@ int gdem_init(gdem_handle h) {
     s->invalidateGraphs();
     s->init();
     s->readStatus();
+    return GDEM_OK;
+  });
+}
+
+int gdem_set_tuning(gdem_handle h, double skin_factor, int blocks_per_sm) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s) throw std::runtime_error("invalid handle");
+    if (!(skin_factor < 0.) && !(skin_factor <= 4.)) throw std::runtime_error("skin factor out of range");
+    if (blocks_per_sm > 64) throw std::runtime_error("blocks per multiprocessor out of range");
+    s->applyTuning(skin_factor, blocks_per_sm);
+    return GDEM_OK;
+  });
+}
+
+// Autotuner: times trial_steps steps (after 3 warm-up steps) of a copy of
+// the uploaded system for each candidate skin (as a multiple of rmax: it sets
+// the pair-list cell size and how often the list is rebuilt), then for each
+// candidate number of force-kernel blocks per multiprocessor at the best
+// skin, and keeps the fastest pair.  The copies start from the same state, so
+// the choice reflects this workload; the results of the system do not depend
+// on it.
+int gdem_autotune(gdem_handle h, int trial_steps, double* skin_factor, int* blocks_per_sm,
+                  double* ms_per_step) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state) throw std::runtime_error("upload the state first");
+    if (s->started) throw std::runtime_error("gdem_autotune runs before gdem_init");
+    if (trial_steps < 1) throw std::runtime_error("trial_steps must be >= 1");
+    const int n = s->S.n;
+    std::vector<double> x(3 * (size_t)n), v(3 * (size_t)n), w(3 * (size_t)n),
+        wb(3 * (size_t)n), q(4 * (size_t)n), basis;
+    auto rc = [](int code) {
+      if (code != GDEM_OK) throw std::runtime_error("autotune trial: " + g_last_error);
+    };
+    rc(gdem_download_state(h, x.data(), v.data(), w.data(), wb.data(), q.data(), nullptr, nullptr));
+    if (s->S.basis) {
+      basis.resize(9 * (size_t)n);
+      rc(gdem_download_basis(h, basis.data()));
+    }
+    std::vector<const char*> paths;
+    for (auto const& p : s->xml_paths) paths.push_back(p.c_str());
+    auto trial = [&](double sf, int bps) {
+      gdem_handle c = nullptr;
+      rc(gdem_create_batch((int)paths.size(), paths.data(), s->precision, &c));
+      std::unique_ptr<System> guard(sys(c));
+      rc(gdem_set_tuning(c, sf, bps));
+      rc(gdem_upload_state(c, n, s->h_inst.data(), s->h_type.data(), x.data(), v.data(),
+                           w.data(), wb.data(), q.data()));
+      if (!basis.empty()) rc(gdem_upload_basis(c, basis.data()));
+      rc(gdem_init(c));
+      rc(gdem_step(c, 3));
+      rc(gdem_step(c, trial_steps));
+      if (guard->status_host) return 1.e300;   // a failing candidate is never chosen
+      return guard->last_ms / trial_steps;
+    };
+    const double skins[] = {0.1, 0.175, 0.25, 0.4, 0.6};
+    const int bpss[] = {2, 4, 8};
+    double best = 1.e300, best_sf = 0.25;
+    int best_bps = 4;
+    for (double sf : skins) {
+      const double ms = trial(sf, 4);
+      if (ms < best) { best = ms; best_sf = sf; }
+    }
+    for (int bps : bpss) {
+      if (bps == 4) continue;
+      const double ms = trial(best_sf, bps);
+      if (ms < best) { best = ms; best_bps = bps; }
+    }
+    s->applyTuning(best_sf, best_bps);
+    if (skin_factor) *skin_factor = best_sf;
+    if (blocks_per_sm) *blocks_per_sm = best_bps;
+    if (ms_per_step) *ms_per_step = best;
     return GDEM_OK;
   });
 }
@@ -1257,8 +1424,8 @@ int gdem_download_contacts(gdem_handle h, int64_t capacity, int64_t* count, int*
     std::vector<double> wd(n * S.max_walls), wf(3 * n * S.max_walls);
     std::vector<int4> cells(n);
     CK(cudaMemcpy(ids.data(), S.id, n * sizeof(int), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(np.data(), S.nact, n * sizeof(int), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(pairs.data(), S.act, n * kPairCap * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(np.data(), S.npairs, n * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(pairs.data(), S.pairs, n * kPairCap * sizeof(int), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(pd.data(), S.pair_delta, pd.size() * sizeof(double), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(wd.data(), S.wall_delta, wd.size() * sizeof(double), cudaMemcpyDeviceToHost));
     if (force) {
@@ -1268,8 +1435,8 @@ int gdem_download_contacts(gdem_handle h, int64_t capacity, int64_t* count, int*
     CK(cudaMemcpy(cells.data(), S.cellc, n * sizeof(int4), cudaMemcpyDeviceToHost));
     int64_t c = 0;
     for (size_t t = 0; t < n; ++t) {
-      for (int e = 0; e < (np[t] & kActMask); ++e) {
-        int u = pairs[t * kPairCap + e] & ((1 << 27) - 1);   // entries of act
+      for (int e = 0; e < np[t]; ++e) {
+        int u = pairs[t * kPairCap + e] & ((1 << 27) - 1);   // pair-list entries
         size_t slot = t * kPairCap + e;
         double dl = pd[slot];
         if (!(dl < 0.) || !(ids[t] < ids[u])) continue;

@@ -21,7 +21,9 @@
 //   k_permute / k_copyback
 //               the whole state into cell order (through the second
 //               buffers), with the compact copies the pair search reads.
-//   k_filter    the skin-list entries whose bounding spheres overlap now.
+//   k_filter    flags the particles with a pair of the skin list whose
+//               bounding spheres overlap now, or near a wall, and lists them
+//               for the force kernel.
 //   k_move      the leapfrog of each particle in place: closing kick of the
 //               step that ends and opening kick + drift of the next
 //               (SecondOrderLeapFrog::Move / advanceVelocity,
@@ -193,7 +195,7 @@ __global__ void k_permute(DevState S, const int* gate) {
   st3(S.x2, cap, t, x);
   st3(S.v2, cap, t, ld3(S.v, cap, s));
   st3(S.w2, cap, t, ld3(S.w, cap, s));
-  st3(S.wbf2, cap, t, ld3(S.wbf, cap, s));
+  if (S.wbf_state) st3(S.wbf2, cap, t, ld3(S.wbf, cap, s));
   st3(S.F2, cap, t, ld3(S.F, cap, s));
   st3(S.T2, cap, t, ld3(S.T, cap, s));
 #pragma unroll
@@ -228,7 +230,8 @@ __global__ void k_copyback(DevState S, const int* gate) {
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     const size_t k = (size_t)d * cap + t;
-    S.x[k] = S.x2[k]; S.v[k] = S.v2[k]; S.w[k] = S.w2[k]; S.wbf[k] = S.wbf2[k];
+    S.x[k] = S.x2[k]; S.v[k] = S.v2[k]; S.w[k] = S.w2[k];
+    if (S.wbf_state) S.wbf[k] = S.wbf2[k];
     S.F[k] = S.F2[k]; S.T[k] = S.T2[k];
     S.disp[k] = 0.f;
   }
@@ -251,13 +254,14 @@ __global__ void k_copyback(DevState S, const int* gate) {
 // A particle that the contact filter left without contact carries only its
 // weight: the force kernel skipped it and its F, T are taken as such here
 // (and written back at the end of a call, kStepStoreFT).
-template <bool kFast>
-__global__ void __launch_bounds__(256, 3) k_move(DevState S, int flags) {
+template <bool kFast, bool kBasis>
+__global__ void __launch_bounds__(256, (kFast && kBasis) ? 2 : 3) k_move(DevState S, int flags) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
   TypeDesc const& tp = S.types[S.type[t]];
   d3 F, T;
-  if ((flags & kStepClose) && S.nact[t] == 0) {
+  const int na = contactFlags(S)[t];
+  if ((flags & kStepClose) && na == 0) {
     F = mk(tp.weight[0], tp.weight[1], tp.weight[2]);
     T = mk(0., 0., 0.);
     if (flags & kStepStoreFT) { st3(S.F, S.cap, t, F); st3(S.T, S.cap, t, T); }
@@ -265,64 +269,135 @@ __global__ void __launch_bounds__(256, 3) k_move(DevState S, int flags) {
     F = ld3(S.F, S.cap, t);
     T = ld3(S.T, S.cap, t);
   }
-  advanceParticle<kFast>(S, t, tp, F, T, (flags & kStepClose) != 0, (flags & kStepMove) != 0);
+  advanceParticle<kFast, kBasis>(S, t, tp, F, T, (flags & kStepClose) != 0, (flags & kStepMove) != 0);
 }
 
-// Contact filter: the entries of each particle's skin list whose bounding
-// spheres overlap now, tested on FP32 positions with an absolute margin that
-// covers their rounding (a superset of the contacts; the force kernels
-// decide each one exactly in FP64).
-__global__ void __launch_bounds__(256) k_filter(DevState S) {
+// Contact filter.  Tests each pair of the skin list once, from the "upper"
+// entries of its lower-ID particle (boundingOverlap: FP32, a superset of the
+// contacts; the force kernels test both entries of the pair again with the
+// same arithmetic and decide each kept one exactly in FP64), flags both
+// particles of a kept pair, flags the particles near a wall, and appends
+// every flagged particle once to the force kernels' work list.  A warp
+// filters the upper entries of its 32 particles together: the lists are laid
+// end to end and lane l takes the entries l, l + 32, ... of the
+// concatenation, so the lanes stay busy whatever the list lengths; up to
+// kFilterBatch rounds of 32 entries are loaded before any is tested, so that
+// their loads overlap.
+constexpr int kFilterBatch = 6;
+
+// Appends idx for every lane whose pred holds (one atomic per warp); every
+// lane of the warp calls it.
+__device__ __forceinline__ void appendWork(DevState const& S, bool pred, int idx) {
+  const unsigned m = __ballot_sync(0xffffffffu, pred);
+  if (!m) return;
+  const int lane = threadIdx.x & 31;
+  int base = 0;
+  if (lane == 0) base = atomicAdd(&S.ctl[kCtlWork], __popc(m));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (pred) S.work[base + __popc(m & ((1u << lane) - 1u))] = idx;
+}
+
+// Sets flag bits of particle i; true for the caller that lists it first.
+__device__ __forceinline__ bool flagParticle(int* flags, int i, int bits) {
+  return !(atomicOr(&flags[i], bits | kListed) & kListed);
+}
+
+__global__ void __launch_bounds__(256, 3) k_filter(DevState S) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  int flag = 0;
-  if (t < S.n) {
-    const int4 cc = S.cellc[t];
-    GridDesc const& bg = S.bgrids[cc.w];
-    const float4 pt = S.posf[t];
-    const int np = S.npairs[t];
-    const int* seg = S.pairs + (size_t)t * kPairCap;
-    int* out = S.act + (size_t)t * kPairCap;
-    int k = 0;
-    for (int e = 0; e < np; ++e) {
-      const int ent = seg[e];
-      const int u = ent & ((1 << 27) - 1);
-      int sh[3];
-      entryShift(S, (unsigned)ent, t, u, sh);
-      const float4 pu = S.posf[u];
-      const float dx = (pu.x - pt.x) + (float)sh[0] * bg.Lf[0];
-      const float dy = (pu.y - pt.y) + (float)sh[1] * bg.Lf[1];
-      const float dz = (pu.z - pt.z) + (float)sh[2] * bg.Lf[2];
-      const float R = pt.w + pu.w + bg.filt_margin;
-      if (dx * dx + dy * dy + dz * dz <= R * R) out[k++] = ent;
-    }
-    // walls (axis-aligned boxes): distance from the centre to the box against
-    // the bounding radius
-    GridDesc const& g = S.grids[cc.w];
-    bool near = false;
-    for (int w = 0; w < g.wall_count && !near; ++w) {
-      WallDesc const& wd = S.walls[g.wall_begin + w];
-      const float p[3] = {pt.x, pt.y, pt.z};
-      float d2 = 0.f;
+  const int first = t - lane;
+  const bool valid = t < S.n;
+  int inst = 0;
+  float4 pt = make_float4(0.f, 0.f, 0.f, 0.f);
+  int nu = 0;
+  int* flags = contactFlags(S);
+  if (valid) {
+    inst = S.cellc[t].w;
+    pt = S.posf[t];
+    nu = S.nupper[t];
+    contactFlags(S, 1)[t] = 0;   // the next evaluation's flags start clear
+  }
+  int incl = nu;
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const float o = fabsf(p[d] - (float)wd.centre[d]) - (float)wd.extent[d];
-        if (o > 0.f) d2 += o * o;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(full, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const int total = __shfl_sync(full, incl, 31);
+  const int excl = incl - nu;
+  for (int base = 0; base < total; base += 32 * kFilterBatch) {
+    unsigned ent[kFilterBatch];
+    int own[kFilterBatch];
+    float4 pu[kFilterBatch];
+    // round 1: owners and entry words
+#pragma unroll
+    for (int c = 0; c < kFilterBatch; ++c) {
+      const int f = base + 32 * c + lane;
+      int p = 0;                          // the last lane whose list starts at or before f
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const int ex = __shfl_sync(full, excl, p + step);
+        if (ex <= f) p += step;
       }
-      const float R = pt.w + bg.filt_margin;
-      near = d2 <= R * R;
+      own[c] = p;
+      const int e = f - __shfl_sync(full, excl, p);
+      ent[c] = 0u;
+      if (f < total) ent[c] = (unsigned)S.pairs[(size_t)(first + p) * kPairCap + e];
     }
-    flag = k | (near ? kNearWall : 0);
-    S.nact[t] = flag;
+    // round 2: the partners' positions
+#pragma unroll
+    for (int c = 0; c < kFilterBatch; ++c) {
+      pu[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (base + 32 * c + lane < total) pu[c] = S.posf[ent[c] & ((1u << 27) - 1u)];
+    }
+    // round 3: the tests; both particles of a kept pair are flagged
+#pragma unroll
+    for (int c = 0; c < kFilterBatch; ++c) {
+      const int cb = base + 32 * c;
+      if (cb >= total) break;             // warp-uniform
+      const int p = own[c];
+      const float4 po = make_float4(__shfl_sync(full, pt.x, p), __shfl_sync(full, pt.y, p),
+                                    __shfl_sync(full, pt.z, p), __shfl_sync(full, pt.w, p));
+      const int ip = __shfl_sync(full, inst, p);
+      const bool keep = cb + lane < total && boundingOverlap(S.bgrids[ip], po, pu[c], ent[c]);
+      bool newT = false, newU = false;
+      const int tp = first + p, u = (int)(ent[c] & ((1u << 27) - 1u));
+      if (keep) {
+        newT = flagParticle(flags, tp, kHasPair);
+        newU = flagParticle(flags, u, kHasPair);
+      }
+      appendWork(S, newT, tp);
+      appendWork(S, newU, u);
+    }
   }
-  // work list of the force kernel, appended once per warp
-  const unsigned ballot = __ballot_sync(0xffffffffu, flag != 0);
-  if (ballot) {
-    const int lane = threadIdx.x & 31;
-    int base = 0;
-    if (lane == 0) base = atomicAdd(&S.ctl[kCtlWork], __popc(ballot));
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (flag) S.work[base + __popc(ballot & ((1u << lane) - 1))] = t;
+  bool newW = false;
+  if (valid) {
+    // walls (axis-aligned boxes): distance from the centre (wrapped back into
+    // the box) to the box against the bounding radius
+    GridDesc const& g = S.grids[inst];
+    GridDesc const& bg = S.bgrids[inst];
+    bool near = false;
+    if (g.wall_count) {
+      const int wt = S.wrap[t];
+      const float q[3] = {pt.x - (float)wrapGet(wt, 0) * bg.Lf[0],
+                          pt.y - (float)wrapGet(wt, 1) * bg.Lf[1],
+                          pt.z - (float)wrapGet(wt, 2) * bg.Lf[2]};
+      for (int w = 0; w < g.wall_count && !near; ++w) {
+        WallDesc const& wd = S.walls[g.wall_begin + w];
+        float d2 = 0.f;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const float o = fabsf(q[d] - (float)wd.centre[d]) - (float)wd.extent[d];
+          if (o > 0.f) d2 += o * o;
+        }
+        const float R = pt.w + bg.filt_margin;
+        near = d2 <= R * R;
+      }
+    }
+    if (near) newW = flagParticle(flags, t, kNearWall);
   }
+  appendWork(S, newW, t);
 }
 
 // Scatter of sorted-order state into ID order (for download).
@@ -334,6 +409,13 @@ __global__ void k_scatter_by_id(DevState S, double* out_x, double* out_v, double
   const int cap = S.cap, n = S.n;
   int i = S.id[t] - id_base;
   if (i < 0 || i >= n) return;
+  if (out_wbf && !S.wbf_state) {
+    // q* w q (ParticleKinematics.cpp:220-221), the body-frame image of the state w
+    const dq qq = qmk(mk(S.q[t], S.q[cap + t], S.q[2 * cap + t]), S.q[3 * cap + t]);
+    const d3 wb = multToVector3(conj(qq), vecq(ld3(S.w, cap, t), qq));
+    out_wbf[3 * i] = wb.x; out_wbf[3 * i + 1] = wb.y; out_wbf[3 * i + 2] = wb.z;
+    out_wbf = nullptr;
+  }
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     if (out_x) out_x[3 * i + d] = S.x[d * cap + t];
@@ -521,8 +603,10 @@ void launch_move(DevState const& S, int flags, int fast, cudaStream_t st) {
   DevState M = S;   // in place: the "next" buffers are the current ones
   M.x2 = S.x; M.v2 = S.v; M.w2 = S.w; M.wbf2 = S.wbf; M.q2 = S.q; M.basis2 = S.basis;
   M.wrap2 = S.wrap;
-  if (fast) k_move<true><<<blocks(S.n, 256), 256, 0, st>>>(M, flags);
-  else k_move<false><<<blocks(S.n, 256), 256, 0, st>>>(M, flags);
+  const int nb = blocks(S.n, 256);
+  if (!fast) k_move<false, false><<<nb, 256, 0, st>>>(M, flags);   // basis tested at run time
+  else if (S.basis) k_move<true, true><<<nb, 256, 0, st>>>(M, flags);
+  else k_move<true, false><<<nb, 256, 0, st>>>(M, flags);
 }
 void launch_filter(DevState const& S, cudaStream_t st) {
   if (S.n) k_filter<<<blocks(S.n, 256), 256, 0, st>>>(S);

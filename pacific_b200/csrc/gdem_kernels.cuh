@@ -10,9 +10,13 @@ enum StepFlags : int {
   kStepMove = 4,      // opening kick (dt / 2) and drift (dt) of the next step
   kStepStoreFT = 8,   // write F, T of particles without contact (last step of a call)
 };
-// nact[t] = number of entries kept | kNearWall when a wall may touch t.
-constexpr int kNearWall = 1 << 16;
-constexpr int kActMask = kNearWall - 1;
+// nact[t], set by the contact filter (atomically: both particles of a kept
+// pair are flagged) and cleared by k_move: kHasPair when a pair-list entry
+// of t passed the bounding-sphere test, kNearWall when a wall may touch t,
+// kListed once t is on the force kernels' work list (0: no contact possible).
+constexpr int kHasPair = 1;
+constexpr int kNearWall = 2;
+constexpr int kListed = 4;
 
 // gdem_integrate.cu
 void launch_decide(DevState const& S, cudaGraphConditionalHandle h, int use_handle,

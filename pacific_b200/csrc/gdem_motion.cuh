@@ -133,6 +133,39 @@ __device__ __forceinline__ void sinCosSmall(double a, double* s, double* c) {
   }
 }
 
+// FP32-split leapfrog of a sphere in a spheres-only system.  With an
+// isotropic inertia the body-frame kick followed by the rotation back to the
+// space frame (kick: w = q (w_bf + q* T q / I h) q*) equals the space-frame
+// kick w + T / I h in exact arithmetic, and the drift's rotation about w
+// leaves w unchanged, so the space-frame angular velocity is the state and
+// the body-frame one is derived on output (q* w q).  Same leapfrog otherwise.
+__device__ __forceinline__ void leapfrogSphere(TypeDesc const& tp, d3 F, d3 T, bool close,
+                                               double hc, bool move, double h, double dt,
+                                               d3& x, d3& v, d3& w, dq& q, d3& dx, int* status) {
+  const double iI = tp.inv_inertia[0];
+  if (close) {
+    v = v + F * (hc * tp.inv_mass);
+    w = w + T * (hc * iI);
+  }
+  dx = mk(0., 0., 0.);
+  if (!move) return;
+  v = v + F * (h * tp.inv_mass);
+  w = w + T * (h * iI);
+  dx = v * dt;
+  x = x + dx;
+  const double nOm = norm(w);
+  dq qdt;
+  if (nOm > 1.0e-10) {
+    double cc, ss;
+    sinCosSmall(nOm * dt * 0.5, &ss, &cc);
+    qdt = qmk((ss / nOm) * w, cc);
+  } else {
+    qdt = qmk(mk(0., 0., 0.), 1.);
+  }
+  q = qmul(qdt, q);
+  if (dot(dx, dx) > tp.crust * tp.crust) raise(status, kErrMotion);
+}
+
 // One particle's leapfrog: optionally the closing kick of the previous step
 // (with this step's F, T over hc), then optionally the opening kick over h
 // and the drift over dt with the quaternion and orientation update.
@@ -200,24 +233,33 @@ __device__ __forceinline__ void leapfrog(TypeDesc const& tp, d3 F, d3 T, bool cl
 // result to the second buffers; updates the pair-list displacement and wraps
 // and flags a rebuild when the particle has moved more than half the skin.
 // close/move select the kicks as in leapfrog().
-template <bool kFast>
+template <bool kFast, bool kBasis>
 __device__ __forceinline__ void advanceParticle(DevState const& S, int t, TypeDesc const& tp,
                                                 d3 F, d3 T, bool close, bool move) {
   const int cap = S.cap;
   const double dt = S.dt;
   GridDesc const& g = S.grids[S.inst[t]];
+  // FP32-split, spheres only: w is the angular state (leapfrogSphere)
+  constexpr bool kSphereW = kFast && !kBasis;
   d3 x = ld3(S.x, cap, t), v = ld3(S.v, cap, t), w = ld3(S.w, cap, t);
-  d3 wbf = ld3(S.wbf, cap, t);
+  d3 wbf = kSphereW ? mk(0., 0., 0.) : ld3(S.wbf, cap, t);
   dq q = qmk(mk(S.q[t], S.q[cap + t], S.q[2 * cap + t]), S.q[3 * cap + t]);
+  // FP32-split: the basis array exists only in the instantiation for
+  // systems that carry one (convex bodies), a compile-time choice that keeps
+  // it in registers.  FP64: one instantiation tests for it at run time (the
+  // faster of the two on B200 for that path, measured).
   double bas[9];
   double* bp = nullptr;
-  if (S.basis) {
+  if (kFast ? kBasis : S.basis != nullptr) {
 #pragma unroll
     for (int k = 0; k < 9; ++k) bas[k] = S.basis[k * cap + t];
     bp = bas;
   }
   d3 dx;
-  leapfrog<kFast>(tp, F, T, close, 0.5 * dt, move, 0.5 * dt, dt, x, v, wbf, w, q, bp, dx, S.status);
+  if constexpr (kSphereW)
+    leapfrogSphere(tp, F, T, close, 0.5 * dt, move, 0.5 * dt, dt, x, v, w, q, dx, S.status);
+  else
+    leapfrog<kFast>(tp, F, T, close, 0.5 * dt, move, 0.5 * dt, dt, x, v, wbf, w, q, bp, dx, S.status);
   int wr = S.wrap[t];
   if (move) {
     int wd[3];
@@ -231,14 +273,57 @@ __device__ __forceinline__ void advanceParticle(DevState const& S, int t, TypeDe
     const float half = 0.5f * S.bgrids[S.inst[t]].skin_f;
     if (ds.x * ds.x + ds.y * ds.y + ds.z * ds.z > half * half) S.ctl[kCtlNeed] = 1;
   }
-  st3(S.x2, cap, t, x); st3(S.v2, cap, t, v); st3(S.w2, cap, t, w); st3(S.wbf2, cap, t, wbf);
+  st3(S.x2, cap, t, x); st3(S.v2, cap, t, v); st3(S.w2, cap, t, w);
+  if (!kSphereW) st3(S.wbf2, cap, t, wbf);
   S.q2[t] = q.v.x; S.q2[cap + t] = q.v.y; S.q2[2 * cap + t] = q.v.z; S.q2[3 * cap + t] = q.w;
   if (bp) {
 #pragma unroll
     for (int k = 0; k < 9; ++k) S.basis2[k * cap + t] = bas[k];
   }
   S.wrap2[t] = wr;
-  S.posf[t] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)tp.radius);
+  // FP32 copy for the contact filter: the continuous position since the
+  // last rebuild (the wrapped one plus the wraps), so that the image shift
+  // recorded in a list entry at the rebuild stays valid
+  // (in FP32: its rounding is covered by the filter's margin)
+  GridDesc const& bg = S.bgrids[S.inst[t]];
+  S.posf[t] = make_float4((float)x.x + (float)wrapGet(wr, 0) * bg.Lf[0],
+                          (float)x.y + (float)wrapGet(wr, 1) * bg.Lf[1],
+                          (float)x.z + (float)wrapGet(wr, 2) * bg.Lf[2], (float)tp.radius);
+}
+
+// The FP32 bounding-sphere test of a pair-list entry: the centres of the two
+// bounding spheres (FP32 continuous positions, entry image shift) are closer
+// than the sum of the radii plus the margin that covers the FP32 rounding, so
+// the kept entries are a superset of the contacts.  The contact filter and the
+// force kernels call this same function and so take the same decisions.
+__device__ __forceinline__ bool boundingOverlap(GridDesc const& bg, float4 pt, float4 pu,
+                                                unsigned ent) {
+  const int code = (int)(ent >> 27);
+  const float dx = (pu.x - pt.x) + (float)(code % 3 - 1) * bg.Lf[0];
+  const float dy = (pu.y - pt.y) + (float)((code / 3) % 3 - 1) * bg.Lf[1];
+  const float dz = (pu.z - pt.z) + (float)(code / 9 - 1) * bg.Lf[2];
+  const float R = pt.w + pu.w + bg.filt_margin;
+  return dx * dx + dy * dy + dz * dz <= R * R;
+}
+
+// Bounding-sphere tests of the entries e0 .. e0 + kProbe - 1 of a pair list
+// of np entries (seg), with all their loads issued before the first test;
+// bit j of the result is set when entry e0 + j is kept.
+constexpr int kProbe = 8;
+__device__ __forceinline__ unsigned probeEntries(DevState const& S, GridDesc const& bg, float4 pt,
+                                                 const int* seg, int e0, int np) {
+  unsigned en[kProbe];
+  float4 pu[kProbe];
+#pragma unroll
+  for (int j = 0; j < kProbe; ++j) en[j] = e0 + j < np ? (unsigned)seg[e0 + j] : 0u;
+#pragma unroll
+  for (int j = 0; j < kProbe; ++j)
+    pu[j] = e0 + j < np ? S.posf[en[j] & ((1u << 27) - 1u)] : make_float4(0.f, 0.f, 0.f, 0.f);
+  unsigned keep = 0u;
+#pragma unroll
+  for (int j = 0; j < kProbe; ++j)
+    if (e0 + j < np && boundingOverlap(bg, pt, pu[j], en[j])) keep |= 1u << j;
+  return keep;
 }
 
 // Image shift (in periods) of list entry ent (partner u) of slot t: the

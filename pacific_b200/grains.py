@@ -78,6 +78,10 @@ def library() -> ctypes.CDLL:
         "gdem_upload_forces": ([_P, _DP, _DP], ctypes.c_int),
         "gdem_upload_history": ([_P, i64, _IP, _IP, _DP, _DP, _DP], ctypes.c_int),
         "gdem_init": ([_P], ctypes.c_int),
+        "gdem_set_tuning": ([_P, ctypes.c_double, ctypes.c_int], ctypes.c_int),
+        "gdem_autotune": ([_P, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                           ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)],
+                          ctypes.c_int),
         "gdem_step": ([_P, ctypes.c_int], ctypes.c_int),
         "gdem_download_state": ([_P, _DP, _DP, _DP, _DP, _DP, _DP, _DP], ctypes.c_int),
         "gdem_download_cells": ([_P, _IP], ctypes.c_int),
@@ -96,6 +100,8 @@ def library() -> ctypes.CDLL:
         "gdem_set_profiling": ([_P, ctypes.c_int], ctypes.c_int),
         "gdem_law_counts": ([_P, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.c_int],
                             ctypes.c_int),
+        "gdem_gjk_counts": ([_P, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64),
+                             ctypes.c_int], ctypes.c_int),
         "gdem_step_counts": ([_P, ctypes.POINTER(i64), ctypes.POINTER(i64)], ctypes.c_int),
         "gdem_pair_counts": ([_P, ctypes.POINTER(i64), ctypes.POINTER(i64)], ctypes.c_int),
         "gdem_kernel_times": ([_P, ctypes.c_int, _IP, ctypes.c_char_p, _DP,
@@ -226,6 +232,14 @@ class Grains:
         self._check(library().gdem_pair_counts(self._h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
 
+    def gjk_counts(self, reset=False):
+        """(calls, iterations, most iterations of one call) of the GJK narrow
+        phase since the last reset (convex bodies)."""
+        c, it, mx = ctypes.c_int64(0), ctypes.c_int64(0), ctypes.c_int64(0)
+        self._check(library().gdem_gjk_counts(self._h, ctypes.byref(c), ctypes.byref(it),
+                                              ctypes.byref(mx), 1 if reset else 0))
+        return c.value, it.value, mx.value
+
     def step_counts(self):
         """(force evaluations, pair-list rebuilds) since the state was created."""
         a = ctypes.c_int64(0)
@@ -312,6 +326,24 @@ class Grains:
         return library().gdem_last_step_ms(self._h)
 
     # ------------------------------------------------------------- stepping
+    def set_tuning(self, skin_factor=None, blocks_per_sm=None):
+        """Pair-list skin (multiple of rmax) and force-kernel blocks per
+        multiprocessor, before do_before_time_stepping; None keeps the default."""
+        self._check(library().gdem_set_tuning(
+            self._h, -1.0 if skin_factor is None else float(skin_factor),
+            0 if blocks_per_sm is None else int(blocks_per_sm)))
+
+    def autotune(self, trial_steps=50):
+        """Times copies of the uploaded system over the candidate launch
+        settings and applies the fastest; returns
+        {"skin_factor", "blocks_per_sm", "ms_per_step"}."""
+        sf = ctypes.c_double(0.0)
+        bps = ctypes.c_int(0)
+        ms = ctypes.c_double(0.0)
+        self._check(library().gdem_autotune(self._h, int(trial_steps), ctypes.byref(sf),
+                                            ctypes.byref(bps), ctypes.byref(ms)))
+        return {"skin_factor": sf.value, "blocks_per_sm": bps.value, "ms_per_step": ms.value}
+
     def do_before_time_stepping(self):
         """Leapfrog start: forces at t0, zeroed cumulative contact memory."""
         self._check(library().gdem_init(self._h))

@@ -229,3 +229,37 @@ def test_convex_trajectory(tmp_path, lib, oracle_lib, precision):
     assert g.status() == 0
     assert ncontact > 20
     g.close()
+
+
+def _q_conj_w_q(q, w):
+    """Body-frame image q* w q of space-frame vectors w (rows), q = (x, y, z, w)."""
+    qv, qw = q[:, :3], q[:, 3:4]
+    # rotate by the inverse quaternion: w' = w + 2 qw (w x -qv) + 2 (-qv) x ((-qv) x w) ... written
+    # as the sandwich conj(q) (0, w) q
+    t = 2.0 * np.cross(-qv, w)
+    return w + qw * t + np.cross(-qv, t)
+
+
+def test_fp32split_sphere_angular_state(tmp_path, lib):
+    """FP32-split spheres integrate the space-frame angular velocity (the
+    body-frame one is derived as q* w q on output): it tracks the FP64 mode,
+    which integrates the body-frame one, and the derived w_bf is q* w q."""
+    sc = scenarios.periodic_gas(n_fcc=6, seed=31, spacing=3.0e-3)
+    rng = np.random.default_rng(4)
+    w0 = rng.normal(0.0, 200.0, (sc.n, 3))
+    xml = str(sc.write_xml(tmp_path / "spin.xml"))
+    out = {}
+    for prec in (FP64, FP32_SPLIT):
+        g = Grains(xml, prec)
+        g.upload_state(sc.type, sc.x, sc.v, w0, sc.q)
+        g.do_before_time_stepping()
+        g.step(200)
+        out[prec] = g.download_state()
+        assert g.status() == 0
+        g.close()
+    a, b = out[FP64], out[FP32_SPLIT]
+    scale = np.abs(a["w"]).max()
+    assert np.max(np.abs(a["w"] - b["w"])) <= 1e-6 * scale
+    assert np.max(np.abs(a["q"] - b["q"])) <= 1e-9
+    assert np.max(np.abs(b["wbf"] - _q_conj_w_q(b["q"], b["w"]))) <= 1e-12 * scale
+    assert np.max(np.abs(a["wbf"] - b["wbf"])) <= 1e-6 * scale
