@@ -115,10 +115,10 @@ def algorithmic_bytes(kernel, n, entries, contacts, ncells, fp64):
     state = 24 + (3 if fp64 else 2) * vel + 32
     touched = min(n, 2 * contacts)    # particles with a contact (the force work list)
     if kernel == "filter":
-        # instance, posf, upper count | next flags; per pair (half the
-        # directed entries) the entry word and the partner's posf; per
-        # contact the two flags and the work-list entries
-        return n * (4 + 16 + 4 + 4) + (entries // 2) * (4 + 16) + contacts * 16
+        # posf, instance | next flags; per pair (half the directed entries)
+        # its compact-list word pair; per contact the two flags and the
+        # work-list entries
+        return n * (16 + 4 + 4) + (entries // 2) * 8 + contacts * 16
     if kernel in ("forces64", "forces32"):
         # per particle of the work list: cellc id type x v w nact | F T; per
         # contact the entry word, the partner's id type x v w and the history

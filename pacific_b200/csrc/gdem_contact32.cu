@@ -263,10 +263,8 @@ __device__ __forceinline__ void contactLaw32(ModelDesc const& m, double dt, Cont
 
 // Lists a candidate when its bounding spheres are closer than the skin, with
 // a relative margin of 4e-6 that covers the FP32 rounding of the test.
-__global__ void __launch_bounds__(256) k_pairs32(DevState S, const int* gate) {
-  if (gate && !*gate) return;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= S.n) return;
+// The list of slot t; returns its number of upper entries.
+__device__ __forceinline__ int listPairs32(DevState const& S, int t) {
   const int4 cc = S.cellc[t];
   GridDesc const& g = S.bgrids[cc.w];
   const float4 ha = S.offh[t];
@@ -291,8 +289,18 @@ __global__ void __launch_bounds__(256) k_pairs32(DevState S, const int* gate) {
     ++cnt;
   });
   if (cnt > kPairCap) { raise(S.status, kErrPairsFull); cnt = kPairCap; }
-  S.nupper[t] = sortEntriesUpperFirst(out, cnt, S.id, S.id[t]);
+  const int nu = sortEntriesUpperFirst(out, cnt, S.id, S.id[t]);
   S.npairs[t] = cnt;
+  return nu;
+}
+
+__global__ void __launch_bounds__(256) k_pairs32(DevState S, const int* gate) {
+  if (gate && !*gate) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = t < S.n;
+  const int nu = valid ? listPairs32(S, t) : 0;
+  // each pair once, from its lower ID, into the compact list of the filter
+  appendUpperPairs(S, t, valid ? S.pairs + (size_t)t * kPairCap : S.pairs, nu, S.status);
 }
 
 // kConvex: some class is not a sphere, so the GJK narrow phase is compiled in
@@ -449,6 +457,8 @@ __device__ __forceinline__ void forcesOn32(DevState const& S, int t, int na, int
 template <bool kConvex>
 __global__ void __launch_bounds__(256) k_forces32(DevState S, int sparse) {
   const int stride = gridDim.x * blockDim.x;
+  pdlWait();      // the contact filter's work list and flags
+  pdlTrigger();   // the move kernel may be scheduled; it waits for this one
   const int nw = sparse ? S.ctl[kCtlWork] : S.n;
   const int* flags = contactFlags(S);
   int nlaw = 0, nre = 0;   // contacts evaluated / re-evaluated in FP64
@@ -475,8 +485,8 @@ void launch_pairs32(DevState const& S, const int* gate, cudaStream_t st) {
 void launch_forces32(DevState const& S, int sparse, cudaStream_t st) {
   if (!S.n) return;
   const int grid = std::min((S.n + 255) / 256, (S.forces_bps > 0 ? S.forces_bps : 4) * S.nsm);
-  if (S.any_convex) k_forces32<true><<<grid, 256, 0, st>>>(S, sparse);
-  else k_forces32<false><<<grid, 256, 0, st>>>(S, sparse);
+  if (S.any_convex) launchAfterPrevious(k_forces32<true>, grid, 256, st, S, sparse);
+  else launchAfterPrevious(k_forces32<false>, grid, 256, st, S, sparse);
 }
 
 }  // namespace gdem

@@ -30,10 +30,8 @@ namespace {
 // a relative margin of 1e-12, for periodic images whose two orientations
 // round the image translation differently); k_forces64 then decides contact
 // exactly (distance < 0) in lower-ID-first orientation.
-__global__ void __launch_bounds__(256) k_pairs64(DevState S, const int* gate) {
-  if (gate && !*gate) return;
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= S.n) return;
+// The list of slot t; returns its number of upper entries.
+__device__ __forceinline__ int listPairs64(DevState const& S, int t) {
   const int4 cc = S.cellc[t];
   GridDesc const& g = S.bgrids[cc.w];
   const double4 pa = S.pos64[t];
@@ -52,8 +50,18 @@ __global__ void __launch_bounds__(256) k_pairs64(DevState S, const int* gate) {
     ++cnt;
   });
   if (cnt > kPairCap) { raise(S.status, kErrPairsFull); cnt = kPairCap; }
-  S.nupper[t] = sortEntriesUpperFirst(out, cnt, S.id, S.id[t]);
+  const int nu = sortEntriesUpperFirst(out, cnt, S.id, S.id[t]);
   S.npairs[t] = cnt;
+  return nu;
+}
+
+__global__ void __launch_bounds__(256) k_pairs64(DevState S, const int* gate) {
+  if (gate && !*gate) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = t < S.n;
+  const int nu = valid ? listPairs64(S, t) : 0;
+  // each pair once, from its lower ID, into the compact list of the filter
+  appendUpperPairs(S, t, valid ? S.pairs + (size_t)t * kPairCap : S.pairs, nu, S.status);
 }
 
 __device__ __forceinline__ void loadHist(HistTable const& t, int slot, d3& kd, d3& pn, d3& sp) {
@@ -219,6 +227,8 @@ __device__ __forceinline__ void forcesOn64(DevState const& S, int t, int na, int
 template <bool kConvex>
 __global__ void __launch_bounds__(256) k_forces64(DevState S, int sparse) {
   const int stride = gridDim.x * blockDim.x;
+  pdlWait();      // the contact filter's work list and flags
+  pdlTrigger();   // the move kernel may be scheduled; it waits for this one
   const int nw = sparse ? S.ctl[kCtlWork] : S.n;
   const int* flags = contactFlags(S);
   GjkTally gjk;
@@ -238,8 +248,8 @@ void launch_pairs64(DevState const& S, const int* gate, cudaStream_t st) {
 void launch_forces64(DevState const& S, int sparse, cudaStream_t st) {
   if (!S.n) return;
   const int grid = std::min((S.n + 255) / 256, (S.forces_bps > 0 ? S.forces_bps : 4) * S.nsm);
-  if (S.any_convex) k_forces64<true><<<grid, 256, 0, st>>>(S, sparse);
-  else k_forces64<false><<<grid, 256, 0, st>>>(S, sparse);
+  if (S.any_convex) launchAfterPrevious(k_forces64<true>, grid, 256, st, S, sparse);
+  else launchAfterPrevious(k_forces64<false>, grid, 256, st, S, sparse);
 }
 
 }  // namespace gdem

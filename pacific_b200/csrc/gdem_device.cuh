@@ -126,7 +126,7 @@ struct DevState {
   int4* cellc;            // pair-list cell i, j, k and instance at the last rebuild
   // pair list: per-particle segments of kPairCap entries
   int* pairs; int* npairs;   // skin list (rebuilt on demand)
-  int* nupper;            // entries of each list whose partner has a higher ID (listed first)
+  int2* upairs;           // compact pair list: (slot, entry) of every upper entry, ctl[kCtlPairs] of them
   int* nact;              // contact-filter flags, two buffers of cap (contactFlags)
   float4* posf;           // FP32 continuous position since the last rebuild + circumscribed radius
   int* work;              // particles with a listed contact or near a wall (this step)
@@ -148,6 +148,9 @@ struct DevState {
   const double* poly_verts;   // polyhedron vertices of all classes (x, y, z)
   int max_walls;          // walls of the largest instance
   int any_convex;         // some class is not a sphere (GJK narrow phase)
+  int any_walls;          // some instance has walls
+  float filt_margin_max;  // largest contact-filter margin of the instances
+  int filter_qblocks;     // contact filter: blocks for the pairs (0: from the particle count)
 };
 
 // ----------------------------------------------------------- FP64 helpers --
@@ -308,6 +311,43 @@ __device__ __forceinline__ int sortEntriesUpperFirst(int* seg, int cnt, const in
   }
   return nup;
 }
+
+// Appends the first nu entries of slot t's list to the compact pair list
+// (one atomic per warp).  Every lane of the warp calls it; valid lanes only
+// contribute.
+__device__ __forceinline__ void appendUpperPairs(DevState const& S, int t, const int* seg, int nu,
+                                                 int* status) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  int incl = nu;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(full, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const int total = __shfl_sync(full, incl, 31);
+  if (!total) return;
+  int base = 0;
+  if (lane == 31) base = atomicAdd(&S.ctl[kCtlPairs], total);
+  base = __shfl_sync(full, base, 31);
+  const long long cap = (long long)S.cap * kUpperCap;
+  if (base + (long long)total > cap) {
+    if (lane == 0) raise(status, kErrPairsFull);
+    return;
+  }
+  const int first = base + incl - nu;
+  for (int e = 0; e < nu; ++e) S.upairs[first + e] = make_int2(t, seg[e]);
+}
+
+// Programmatic dependent launch (sm_90 and later): a kernel launched with
+// the programmatic-serialization attribute (launchAfterPrevious) may start
+// while the previous kernel of its stream still runs.  pdlWait() returns once
+// that kernel has completed and its writes are visible (at once for a kernel
+// launched without the attribute); pdlTrigger() lets the next kernel start
+// early.  Everything a kernel reads that its predecessor writes, and all its
+// writes, come after its pdlWait().
+__device__ __forceinline__ void pdlWait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdlTrigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 // Contact-filter flags of the current force evaluation: two buffers used
 // alternately, the filter of one evaluation clearing the other's, so that no

@@ -679,6 +679,12 @@ struct System {
     S.ncells = cell_offset;
     S.ninst = (int)inst.size();
     S.max_walls = max_walls;
+    S.any_walls = 0;
+    S.filt_margin_max = 0.f;
+    for (auto const& b : bgrids) {
+      if (b.wall_count) S.any_walls = 1;
+      S.filt_margin_max = std::max(S.filt_margin_max, b.filt_margin);
+    }
     S.dt = inst[0].dt;
     for (auto& I : inst)
       if (I.dt != S.dt) throw std::runtime_error("all instances of a batch must share dt");
@@ -726,7 +732,8 @@ struct System {
       S.offh = alloc<float4>(c);
       S.pos64 = nullptr;
     }
-    S.pairs = alloc<int>(c * kPairCap); S.npairs = alloc<int>(c); S.nupper = alloc<int>(c);
+    S.pairs = alloc<int>(c * kPairCap); S.npairs = alloc<int>(c);
+    S.upairs = alloc<int2>(c * kUpperCap);
     S.nact = alloc<int>(2 * c);
     CK(cudaMemset(S.nact, 0, 2 * c * sizeof(int)));
     S.work = alloc<int>(c);
@@ -903,6 +910,12 @@ struct System {
     ++parity;
     launch_hist_zero_cumulative(S.hist_old, S.ctl, precision == GDEM_FP64, stream);
     CK(cudaStreamSynchronize(stream));
+    // size the contact filter's grid for the pair list just built (a quarter
+    // more for growth; the kernel loops over any excess)
+    int np = 0;
+    CK(cudaMemcpy(&np, S.ctl + kCtlPairs, sizeof(int), cudaMemcpyDeviceToHost));
+    S.filter_qblocks = std::max(1, (int)((1.25 * np + 1023.) / 1024.));
+    invalidateGraphs();
     collectTimes();
     started = true;
   }

@@ -31,6 +31,8 @@
 // Rebuild kernels take a gate: with a non-null gate they return at once
 // unless this step rebuilds (plain launches); inside the graph's conditional
 // node they run ungated.
+#include <algorithm>
+
 #include "gdem_kernels.cuh"
 #include "gdem_motion.cuh"
 
@@ -48,6 +50,7 @@ __global__ void k_decide(DevState S, cudaGraphConditionalHandle h, int use_handl
   S.ctl[kCtlEpoch] += 1;
   S.ctl[kCtlRebuilds] += need ? 1 : 0;
   S.ctl[kCtlWork] = 0;
+  if (need) S.ctl[kCtlPairs] = 0;
   if (use_handle) cudaGraphSetConditional(h, need ? 1u : 0u);
 }
 
@@ -259,6 +262,9 @@ __global__ void __launch_bounds__(256, (kFast && kBasis) ? 2 : 3) k_move(DevStat
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
   TypeDesc const& tp = S.types[S.type[t]];
+  MoveIn m;
+  loadMoveIn<kFast, kBasis>(S, t, m);   // nothing the force kernel writes
+  pdlWait();
   d3 F, T;
   const int na = contactFlags(S)[t];
   if ((flags & kStepClose) && na == 0) {
@@ -269,21 +275,26 @@ __global__ void __launch_bounds__(256, (kFast && kBasis) ? 2 : 3) k_move(DevStat
     F = ld3(S.F, S.cap, t);
     T = ld3(S.T, S.cap, t);
   }
-  advanceParticle<kFast, kBasis>(S, t, tp, F, T, (flags & kStepClose) != 0, (flags & kStepMove) != 0);
+  advanceParticle<kFast, kBasis>(S, t, tp, F, T, (flags & kStepClose) != 0, (flags & kStepMove) != 0,
+                                 m);
+  // the next evaluation's contact flags start clear (no other kernel touches
+  // that buffer until the next contact filter)
+  contactFlags(S, 1)[t] = 0;
 }
 
-// Contact filter.  Tests each pair of the skin list once, from the "upper"
-// entries of its lower-ID particle (boundingOverlap: FP32, a superset of the
-// contacts; the force kernels test both entries of the pair again with the
-// same arithmetic and decide each kept one exactly in FP64), flags both
-// particles of a kept pair, flags the particles near a wall, and appends
-// every flagged particle once to the force kernels' work list.  A warp
-// filters the upper entries of its 32 particles together: the lists are laid
-// end to end and lane l takes the entries l, l + 32, ... of the
-// concatenation, so the lanes stay busy whatever the list lengths; up to
-// kFilterBatch rounds of 32 entries are loaded before any is tested, so that
-// their loads overlap.
-constexpr int kFilterBatch = 6;
+// Contact filter.  One lane per pair of the compact pair list (each pair
+// once, from its lower ID): the FP32 bounding-sphere test (a superset of the
+// contacts; the force kernels test both entries of the pair again with
+// boundingOverlap and decide each kept one exactly in FP64); both particles
+// of a kept pair are flagged and each flagged particle is appended once to
+// the force kernels' work list.  One lane per particle: the next
+// evaluation's flags are cleared by k_move.  With walls, the first pblocks
+// blocks take the particles and flag those near a wall; the others take the
+// pairs, in chunks
+// of kFilterUnroll rounds of 32 per warp with their loads issued together
+// (a grid-stride loop over chunks: the grid is sized for the pair count at
+// the leapfrog start, the count itself is known on the device only).
+constexpr int kFilterUnroll = 4;
 
 // Appends idx for every lane whose pred holds (one atomic per warp); every
 // lane of the warp calls it.
@@ -302,102 +313,97 @@ __device__ __forceinline__ bool flagParticle(int* flags, int i, int bits) {
   return !(atomicOr(&flags[i], bits | kListed) & kListed);
 }
 
-__global__ void __launch_bounds__(256, 3) k_filter(DevState S) {
-  const unsigned full = 0xffffffffu;
+__global__ void __launch_bounds__(256) k_filter(DevState S, int pblocks) {
+  pdlTrigger();   // the force kernel may be scheduled; it waits for this one
   const int lane = threadIdx.x & 31;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int first = t - lane;
-  const bool valid = t < S.n;
-  int inst = 0;
-  float4 pt = make_float4(0.f, 0.f, 0.f, 0.f);
-  int nu = 0;
   int* flags = contactFlags(S);
-  if (valid) {
-    inst = S.cellc[t].w;
-    pt = S.posf[t];
-    nu = S.nupper[t];
-    contactFlags(S, 1)[t] = 0;   // the next evaluation's flags start clear
-  }
-  int incl = nu;
+  if ((int)blockIdx.x < pblocks) {
+    // particles near a wall
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    bool newW = false;
+    if (t < S.n) {
+      const int inst = S.inst[t];
+      GridDesc const& g = S.grids[inst];
+      if (g.wall_count) {
+        // distance from the centre (wrapped back into the box) to each wall
+        // box against the bounding radius
+        GridDesc const& bg = S.bgrids[inst];
+        const float4 pt = S.posf[t];
+        const int wt = S.wrap[t];
+        const float q[3] = {pt.x - (float)wrapGet(wt, 0) * bg.Lf[0],
+                            pt.y - (float)wrapGet(wt, 1) * bg.Lf[1],
+                            pt.z - (float)wrapGet(wt, 2) * bg.Lf[2]};
+        bool near = false;
+        for (int w = 0; w < g.wall_count && !near; ++w) {
+          WallDesc const& wd = S.walls[g.wall_begin + w];
+          float d2 = 0.f;
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(full, incl, o);
-    if (lane >= o) incl += y;
-  }
-  const int total = __shfl_sync(full, incl, 31);
-  const int excl = incl - nu;
-  for (int base = 0; base < total; base += 32 * kFilterBatch) {
-    unsigned ent[kFilterBatch];
-    int own[kFilterBatch];
-    float4 pu[kFilterBatch];
-    // round 1: owners and entry words
-#pragma unroll
-    for (int c = 0; c < kFilterBatch; ++c) {
-      const int f = base + 32 * c + lane;
-      int p = 0;                          // the last lane whose list starts at or before f
-#pragma unroll
-      for (int step = 16; step > 0; step >>= 1) {
-        const int ex = __shfl_sync(full, excl, p + step);
-        if (ex <= f) p += step;
+          for (int d = 0; d < 3; ++d) {
+            const float o = fabsf(q[d] - (float)wd.centre[d]) - (float)wd.extent[d];
+            if (o > 0.f) d2 += o * o;
+          }
+          const float R = pt.w + bg.filt_margin;
+          near = d2 <= R * R;
+        }
+        if (near) newW = flagParticle(flags, t, kNearWall);
       }
-      own[c] = p;
-      const int e = f - __shfl_sync(full, excl, p);
-      ent[c] = 0u;
-      if (f < total) ent[c] = (unsigned)S.pairs[(size_t)(first + p) * kPairCap + e];
     }
-    // round 2: the partners' positions
+    appendWork(S, newW, t);
+    return;
+  }
+  // pairs
+  const int np = S.ctl[kCtlPairs];
+  constexpr int chunk = 32 * kFilterUnroll;
+  const long long wq = ((long long)((int)blockIdx.x - pblocks) * blockDim.x + threadIdx.x) >> 5;
+  const long long nwq = ((long long)(gridDim.x - pblocks) * blockDim.x) >> 5;
+  for (long long c0l = wq * chunk; c0l < np; c0l += nwq * chunk) {   // warp-uniform
+    const int c0 = (int)c0l;
+    int2 pr[kFilterUnroll];
+    float4 pa[kFilterUnroll], pb[kFilterUnroll];
 #pragma unroll
-    for (int c = 0; c < kFilterBatch; ++c) {
-      pu[c] = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (base + 32 * c + lane < total) pu[c] = S.posf[ent[c] & ((1u << 27) - 1u)];
+    for (int j = 0; j < kFilterUnroll; ++j) {
+      const int i = c0 + 32 * j + lane;
+      pr[j] = i < np ? S.upairs[i] : make_int2(0, 0);
     }
-    // round 3: the tests; both particles of a kept pair are flagged
 #pragma unroll
-    for (int c = 0; c < kFilterBatch; ++c) {
-      const int cb = base + 32 * c;
-      if (cb >= total) break;             // warp-uniform
-      const int p = own[c];
-      const float4 po = make_float4(__shfl_sync(full, pt.x, p), __shfl_sync(full, pt.y, p),
-                                    __shfl_sync(full, pt.z, p), __shfl_sync(full, pt.w, p));
-      const int ip = __shfl_sync(full, inst, p);
-      const bool keep = cb + lane < total && boundingOverlap(S.bgrids[ip], po, pu[c], ent[c]);
+    for (int j = 0; j < kFilterUnroll; ++j) {
+      pa[j] = pb[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (c0 + 32 * j + lane < np) {
+        pa[j] = S.posf[pr[j].x];
+        pb[j] = S.posf[(unsigned)pr[j].y & ((1u << 27) - 1u)];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kFilterUnroll; ++j) {
+      const int t = pr[j].x, u = (int)((unsigned)pr[j].y & ((1u << 27) - 1u));
+      bool keep = false;
+      if (c0 + 32 * j + lane < np) {
+        // the largest margin of the instances (a superset of the force
+        // kernels' decisions); the period only for an entry with an image
+        // shift (code 13 is none), which needs the instance's grid
+        const unsigned code = (unsigned)pr[j].y >> 27;
+        float sx = 0.f, sy = 0.f, sz = 0.f;
+        if (code != 13u) {
+          GridDesc const& bg = S.bgrids[S.inst[t]];
+          sx = (float)((int)(code % 3u) - 1) * bg.Lf[0];
+          sy = (float)((int)((code / 3u) % 3u) - 1) * bg.Lf[1];
+          sz = (float)((int)(code / 9u) - 1) * bg.Lf[2];
+        }
+        const float dx = (pb[j].x - pa[j].x) + sx;
+        const float dy = (pb[j].y - pa[j].y) + sy;
+        const float dz = (pb[j].z - pa[j].z) + sz;
+        const float R = pa[j].w + pb[j].w + S.filt_margin_max;
+        keep = dx * dx + dy * dy + dz * dz <= R * R;
+      }
       bool newT = false, newU = false;
-      const int tp = first + p, u = (int)(ent[c] & ((1u << 27) - 1u));
       if (keep) {
-        newT = flagParticle(flags, tp, kHasPair);
+        newT = flagParticle(flags, t, kHasPair);
         newU = flagParticle(flags, u, kHasPair);
       }
-      appendWork(S, newT, tp);
+      appendWork(S, newT, t);
       appendWork(S, newU, u);
     }
   }
-  bool newW = false;
-  if (valid) {
-    // walls (axis-aligned boxes): distance from the centre (wrapped back into
-    // the box) to the box against the bounding radius
-    GridDesc const& g = S.grids[inst];
-    GridDesc const& bg = S.bgrids[inst];
-    bool near = false;
-    if (g.wall_count) {
-      const int wt = S.wrap[t];
-      const float q[3] = {pt.x - (float)wrapGet(wt, 0) * bg.Lf[0],
-                          pt.y - (float)wrapGet(wt, 1) * bg.Lf[1],
-                          pt.z - (float)wrapGet(wt, 2) * bg.Lf[2]};
-      for (int w = 0; w < g.wall_count && !near; ++w) {
-        WallDesc const& wd = S.walls[g.wall_begin + w];
-        float d2 = 0.f;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-          const float o = fabsf(q[d] - (float)wd.centre[d]) - (float)wd.extent[d];
-          if (o > 0.f) d2 += o * o;
-        }
-        const float R = pt.w + bg.filt_margin;
-        near = d2 <= R * R;
-      }
-    }
-    if (near) newW = flagParticle(flags, t, kNearWall);
-  }
-  appendWork(S, newW, t);
 }
 
 // Scatter of sorted-order state into ID order (for download).
@@ -604,12 +610,17 @@ void launch_move(DevState const& S, int flags, int fast, cudaStream_t st) {
   M.x2 = S.x; M.v2 = S.v; M.w2 = S.w; M.wbf2 = S.wbf; M.q2 = S.q; M.basis2 = S.basis;
   M.wrap2 = S.wrap;
   const int nb = blocks(S.n, 256);
-  if (!fast) k_move<false, false><<<nb, 256, 0, st>>>(M, flags);   // basis tested at run time
-  else if (S.basis) k_move<true, true><<<nb, 256, 0, st>>>(M, flags);
-  else k_move<true, false><<<nb, 256, 0, st>>>(M, flags);
+  if (!fast) launchAfterPrevious(k_move<false, false>, nb, 256, st, M, flags);   // basis tested at run time
+  else if (S.basis) launchAfterPrevious(k_move<true, true>, nb, 256, st, M, flags);
+  else launchAfterPrevious(k_move<true, false>, nb, 256, st, M, flags);
 }
 void launch_filter(DevState const& S, cudaStream_t st) {
-  if (S.n) k_filter<<<blocks(S.n, 256), 256, 0, st>>>(S);
+  if (!S.n) return;
+  const int pblocks = S.any_walls ? blocks(S.n, 256) : 0;
+  // about 4 pairs per particle until the leapfrog start has counted them
+  const int qblocks =
+      S.filter_qblocks > 0 ? S.filter_qblocks : (S.n + 64 * kFilterUnroll - 1) / (64 * kFilterUnroll);
+  k_filter<<<pblocks + qblocks, 256, 0, st>>>(S, pblocks);
 }
 void launch_fill64(unsigned long long* p, size_t n, unsigned long long value, cudaStream_t st) {
   if (n) k_fill64<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p, n, value);

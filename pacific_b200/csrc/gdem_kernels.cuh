@@ -4,6 +4,25 @@
 
 namespace gdem {
 
+// Launches kernel k so that it may start while the previous kernel of the
+// stream still runs (programmatic stream serialization; k calls pdlWait()
+// before it touches that kernel's results).
+template <typename... KArgs, typename... Args>
+inline void launchAfterPrevious(void (*k)(KArgs...), unsigned grid, unsigned block,
+                                cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  (void)cudaLaunchKernelEx(&cfg, k, args...);   // a failure shows in cudaGetLastError
+}
+
 // Parts of the leapfrog applied by k_move.
 enum StepFlags : int {
   kStepClose = 2,     // closing kick of the step that ends here (dt / 2)

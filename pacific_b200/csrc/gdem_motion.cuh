@@ -229,28 +229,54 @@ __device__ __forceinline__ void leapfrog(TypeDesc const& tp, d3 F, d3 T, bool cl
   if (kFast ? dot(dx, dx) > tp.crust * tp.crust : norm(dx) > tp.crust) raise(status, kErrMotion);
 }
 
-// Moves particle t of the current buffers (F, T as given) and writes the
-// result to the second buffers; updates the pair-list displacement and wraps
-// and flags a rebuild when the particle has moved more than half the skin.
-// close/move select the kicks as in leapfrog().
+// The state of particle t that the leapfrog reads besides F and T; loaded
+// before the move kernel waits for the force kernel (nothing between them
+// writes it).
+struct MoveIn {
+  d3 x, v, w, wbf;
+  dq q;
+  double bas[9];
+  int wrap;
+  float3 disp;
+};
+template <bool kFast, bool kBasis>
+__device__ __forceinline__ void loadMoveIn(DevState const& S, int t, MoveIn& m) {
+  const int cap = S.cap;
+  // FP32-split, spheres only: w is the angular state (leapfrogSphere)
+  constexpr bool kSphereW = kFast && !kBasis;
+  m.x = ld3(S.x, cap, t); m.v = ld3(S.v, cap, t); m.w = ld3(S.w, cap, t);
+  m.wbf = kSphereW ? mk(0., 0., 0.) : ld3(S.wbf, cap, t);
+  m.q = qmk(mk(S.q[t], S.q[cap + t], S.q[2 * cap + t]), S.q[3 * cap + t]);
+  // FP32-split: the basis array exists only in the instantiation for
+  // systems that carry one (convex bodies), a compile-time choice that keeps
+  // it in registers.  FP64: one instantiation tests for it at run time, in
+  // advanceParticle (the faster of the two on B200 for that path, measured).
+  if constexpr (kFast && kBasis) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) m.bas[k] = S.basis[k * cap + t];
+  }
+  m.wrap = S.wrap[t];
+  m.disp = make_float3(S.disp[t], S.disp[cap + t], S.disp[2 * cap + t]);
+}
+
+// Moves particle t (state m, F, T as given) and writes the result to the
+// second buffers; updates the pair-list displacement and wraps and flags a
+// rebuild when the particle has moved more than half the skin.  close/move
+// select the kicks as in leapfrog().
 template <bool kFast, bool kBasis>
 __device__ __forceinline__ void advanceParticle(DevState const& S, int t, TypeDesc const& tp,
-                                                d3 F, d3 T, bool close, bool move) {
+                                                d3 F, d3 T, bool close, bool move, MoveIn& m) {
   const int cap = S.cap;
   const double dt = S.dt;
   GridDesc const& g = S.grids[S.inst[t]];
-  // FP32-split, spheres only: w is the angular state (leapfrogSphere)
   constexpr bool kSphereW = kFast && !kBasis;
-  d3 x = ld3(S.x, cap, t), v = ld3(S.v, cap, t), w = ld3(S.w, cap, t);
-  d3 wbf = kSphereW ? mk(0., 0., 0.) : ld3(S.wbf, cap, t);
-  dq q = qmk(mk(S.q[t], S.q[cap + t], S.q[2 * cap + t]), S.q[3 * cap + t]);
-  // FP32-split: the basis array exists only in the instantiation for
-  // systems that carry one (convex bodies), a compile-time choice that keeps
-  // it in registers.  FP64: one instantiation tests for it at run time (the
-  // faster of the two on B200 for that path, measured).
-  double bas[9];
+  d3 x = m.x, v = m.v, w = m.w, wbf = m.wbf;
+  dq q = m.q;
+  double* bas = m.bas;
   double* bp = nullptr;
-  if (kFast ? kBasis : S.basis != nullptr) {
+  if constexpr (kFast) {
+    if constexpr (kBasis) bp = bas;
+  } else if (S.basis) {
 #pragma unroll
     for (int k = 0; k < 9; ++k) bas[k] = S.basis[k * cap + t];
     bp = bas;
@@ -260,15 +286,15 @@ __device__ __forceinline__ void advanceParticle(DevState const& S, int t, TypeDe
     leapfrogSphere(tp, F, T, close, 0.5 * dt, move, 0.5 * dt, dt, x, v, w, q, dx, S.status);
   else
     leapfrog<kFast>(tp, F, T, close, 0.5 * dt, move, 0.5 * dt, dt, x, v, wbf, w, q, bp, dx, S.status);
-  int wr = S.wrap[t];
+  int wr = m.wrap;
   if (move) {
     int wd[3];
     wrapToGrid(g, x, wd, S.status);
 #pragma unroll
     for (int d = 0; d < 3; ++d)
       if (wd[d]) wr = wrapSet(wr, d, wrapGet(wr, d) + wd[d]);
-    float3 ds = make_float3(S.disp[t] + (float)dx.x, S.disp[cap + t] + (float)dx.y,
-                            S.disp[2 * cap + t] + (float)dx.z);
+    float3 ds = make_float3(m.disp.x + (float)dx.x, m.disp.y + (float)dx.y,
+                            m.disp.z + (float)dx.z);
     S.disp[t] = ds.x; S.disp[cap + t] = ds.y; S.disp[2 * cap + t] = ds.z;
     const float half = 0.5f * S.bgrids[S.inst[t]].skin_f;
     if (ds.x * ds.x + ds.y * ds.y + ds.z * ds.z > half * half) S.ctl[kCtlNeed] = 1;

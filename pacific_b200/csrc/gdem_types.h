@@ -8,6 +8,8 @@ namespace gdem {
 // Maximum number of candidate partners recorded per particle in the
 // per-particle segment of the pair list.
 constexpr int kPairCap = 32;
+// compact pair list (each pair once, from its lower ID): entries per particle
+constexpr int kUpperCap = 16;
 // Material indices per instance (materials are bits in the reference,
 // ContactBuilderFactory.cpp:176-192; here they are indices 0..kMaxMat-1).
 constexpr int kMaxMat = 8;
@@ -32,6 +34,7 @@ enum CtlWords : int {
   kCtlEpoch = 2,    // force evaluations so far (tags the contact-history keys)
   kCtlRebuilds = 3, // pair-list rebuilds so far
   kCtlWork = 4,     // particles the force kernel must evaluate this step (work list length)
+  kCtlPairs = 5,    // pairs of the compact pair list (set by the rebuild)
   kCtlWords = 8
 };
 
