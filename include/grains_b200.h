@@ -107,13 +107,15 @@ int gdem_velocity_stats(gdem_handle h, double* vmax, double* vmean);
  * skin since the last rebuild. */
 int gdem_step_counts(gdem_handle h, int64_t* evaluations, int64_t* rebuilds);
 
-/* FP32-split mode: contact-law evaluations since the last reset, and how
+/* FP32-split mode: contact-law evaluations since the last reset (each pair
+ * in contact once per force evaluation, walls once per particle), and how
  * many of them were re-evaluated in FP64 because the FP32 force was
  * ill-conditioned (a small difference of large terms).  Zero in FP64 mode. */
 int gdem_law_counts(gdem_handle h, int64_t* evaluated, int64_t* reevaluated, int reset);
 
 /* Systems with convex bodies: GJK closest-point calls of the force kernels
- * since the last reset (pairs and walls whose bounding spheres overlap), their
+ * since the last reset (each pair and each particle-wall pair whose bounding
+ * spheres overlap, once per force evaluation), their
  * iterations, and the most iterations of one call (the reference stops at
  * 1000, Convex.cpp:536-627).  No counterpart in the reference. */
 int gdem_gjk_counts(gdem_handle h, int64_t* calls, int64_t* iterations, int64_t* max_iterations,

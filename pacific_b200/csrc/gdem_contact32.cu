@@ -303,9 +303,87 @@ __global__ void __launch_bounds__(256) k_pairs32(DevState S, const int* gate) {
   appendUpperPairs(S, t, valid ? S.pairs + (size_t)t * kPairCap : S.pairs, nu, S.status);
 }
 
-// kConvex: some class is not a sphere, so the GJK narrow phase is compiled in
-// (it is kept out of the sphere-only kernel, whose registers it would triple).
+// One pair in the canonical orientation -- p0 (slot s0, the lower ID) at its
+// own position, p1 at its periodic image seen from p0 -- with the exact
+// narrow phase on the FP64 master positions, the FP32 law (FP64 when
+// ill-conditioned) and the contact history (the new entry written when
+// insert).  Returns true for a contact, with the force f on p0, the torques
+// c0 = lev0 x f and c1 = lev1 x f of the lever arms from p0 and p1, and the
+// rolling torque mr (rolling: the model has rolling resistance); delta gets
+// the overlap (+inf without contact).  kConvex: some class is not a sphere,
+// so the GJK narrow phase is compiled in (it is kept out of the sphere-only
+// kernel, whose registers it would triple).
 template <bool kConvex>
+__device__ __forceinline__ bool evalPair32(DevState const& S, GridDesc const& g, int s0, int s1,
+                                           int id0, int id1, TypeDesc const& tp0,
+                                           TypeDesc const& tp1, d3 x0, d3 x1, d3 v0, d3 v1,
+                                           d3 w0, d3 w1, bool insert, int& nlaw, int& nre,
+                                           GjkTally& gjk, double& delta, float3& f, float3& c0,
+                                           float3& c1, float3& mr, bool& rolling) {
+  const int cap = S.cap;
+  const unsigned tag = (unsigned)S.ctl[kCtlEpoch], tag_old = tag - 1u;
+  Contact64 ct;
+  if (!kConvex || (tp0.shape == 0 && tp1.shape == 0)) {
+    ct = sphereSphere64(x0, tp0.radius, tp0.crust, x1, tp1.radius, tp1.crust);
+  } else {
+    ct = convexContact64(convexOf(tp0, S.poly_verts),
+                         crustXForm(S.basis, cap, s0, tp0.scaling, x0), tp0.radius, tp0.crust,
+                         convexOf(tp1, S.poly_verts),
+                         crustXForm(S.basis, cap, s1, tp1.scaling, x1), tp1.radius, tp1.crust);
+    if (insert) gjk.add(ct.gjk_iters);   // each pair counted once
+  }
+  delta = ct.contact && ct.dist < 0. ? ct.dist : __longlong_as_double(0x7ff0000000000000ll);
+  if (!ct.contact || !(ct.dist < 0.)) return false;
+  if (ct.error) raise(S.status, kErrContactOverlap);
+  // the force law from here on is FP32 (FP64 when ill-conditioned)
+  const float3 lev0 = tof(ct.point - x0);
+  const float3 lev1 = tof(ct.point - x1);
+  ModelDesc const& m = S.models[g.model_base + tp0.mat * kMaxMat + tp1.mat];
+  const Body64 b0{x0, v0, w0, tp0.mass, tp0.eqrad};
+  const Body64 b1{x1, v1, w1, tp1.mass, tp1.eqrad};
+  float3 kd = f3(0.f, 0.f, 0.f), pn = kd, sp = kd;
+  int re;
+  if (insert) ++nlaw;   // each pair counted once, by its lower ID
+  if (m.memory) {
+    const unsigned long long key = pairKey(id0, id1);
+    int old = histFind(S.hist_old, key, tag_old);
+    if (old >= 0) loadHistF(S.hist_old, old, kd, pn, sp);
+    contactLaw32(m, S.dt, ct, b0, b1, old >= 0, kd, pn, sp, f, mr, re);
+    if (insert) {
+      int slot = histInsert(S.hist_new, key, tag);
+      if (slot < 0) raise(S.status, kErrHashFull);
+      else storeHistF(S.hist_new, slot, kd, pn, sp);
+    }
+  } else {
+    contactLaw32(m, S.dt, ct, b0, b1, false, kd, pn, sp, f, mr, re);
+  }
+  if (insert) nre += re;
+  c0 = crossf(lev0, f);
+  c1 = crossf(lev1, f);
+  rolling = m.rolling != 0;
+  if (!rolling) mr = f3(0.f, 0.f, 0.f);
+  return true;
+}
+
+// Position in slot t's list of the entry whose partner is slot u.
+__device__ __forceinline__ int findEntry(DevState const& S, int t, int u) {
+  const int n = S.npairs[t];
+  const int* seg = S.pairs + (size_t)t * kPairCap;
+  for (int e = 0; e < n; ++e)
+    if ((int)((unsigned)seg[e] & ((1u << 27) - 1u)) == u) return e;
+  return -1;
+}
+
+// One side's share of a pair (two-phase path): force and torque terms in the
+// order the per-particle sum adds them.
+struct PairShare32 { float f[3], c[3], mr[3]; };
+
+// Forces and torques on particle t.  kSums (two-phase path, systems with
+// convex bodies): the pairs were evaluated once each by k_pairforces32, and
+// each kept entry's share is read back; otherwise both partners of a pair
+// evaluate it, with identical operands, and the lower ID writes the history.
+// Either way the shares are added in list order, then the walls.
+template <bool kConvex, bool kSums>
 __device__ __forceinline__ void forcesOn32(DevState const& S, int t, int na, int sparse,
                                            int& nlaw, int& nre, GjkTally& gjk) {
   const int cap = S.cap;
@@ -332,73 +410,50 @@ __device__ __forceinline__ void forcesOn32(DevState const& S, int t, int na, int
     while (keep) {
       const int e = e0 + __ffs(keep) - 1;
       keep &= keep - 1u;
+      if constexpr (kSums) {
+        const PairShare32 r = reinterpret_cast<const PairShare32*>(S.pshare)[S.eslot[(size_t)t * kPairCap + e]];
+        Fs = Fs + f3(r.f[0], r.f[1], r.f[2]);
+        Ts = Ts + f3(r.c[0], r.c[1], r.c[2]);
+        Ts = Ts + f3(r.mr[0], r.mr[1], r.mr[2]);
+        continue;
+      }
       const uint32_t ent = (uint32_t)seg[e];
       const int u = (int)(ent & ((1u << 27) - 1));
       const int idb = S.id[u];
       const bool t0 = ida < idb;
       TypeDesc const& tb = S.types[S.type[u]];
-      const TypeDesc& tp0 = t0 ? ta : tb;
-      const TypeDesc& tp1 = t0 ? tb : ta;
-      const int s0 = t0 ? t : u, s1 = t0 ? u : t;
-      // exact narrow phase on the FP64 master positions: lower ID at its own
-      // position, the other at its periodic image seen from it
+      // lower ID at its own position, the other at its periodic image seen
+      // from it
       int sh[3];
       entryShift(S, ent, t, u, sh);
       const d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
       // (the partner's velocities are loaded with its position: a kept entry
       // is nearly always a contact, and the loads then overlap)
       const d3 xu = ld3(S.x, cap, u), vu = ld3(S.v, cap, u), wu = ld3(S.w, cap, u);
-      const d3 x0 = t0 ? xt : xu;
-      const d3 x1 = t0 ? xu + shift : xt + (-shift);
-      Contact64 ct;
-      if (!kConvex || (ta.shape == 0 && tb.shape == 0)) {
-        ct = sphereSphere64(x0, tp0.radius, tp0.crust, x1, tp1.radius, tp1.crust);
-      } else {
-        ct = convexContact64(convexOf(tp0, S.poly_verts),
-                             crustXForm(S.basis, cap, s0, tp0.scaling, x0), tp0.radius, tp0.crust,
-                             convexOf(tp1, S.poly_verts),
-                             crustXForm(S.basis, cap, s1, tp1.scaling, x1), tp1.radius, tp1.crust);
-        gjk.add(ct.gjk_iters);
-      }
-      if (S.diag) S.pair_delta[(size_t)t * kPairCap + e] = ct.contact && ct.dist < 0. ? ct.dist : __longlong_as_double(0x7ff0000000000000ll);
-      if (!ct.contact || !(ct.dist < 0.)) continue;
-      if (ct.error) raise(S.status, kErrContactOverlap);
-      // the force law from here on is FP32 (FP64 when ill-conditioned)
-      const float3 lev0 = tof(ct.point - x0);
-      const float3 lev1 = tof(ct.point - x1);
-      ModelDesc const& m = S.models[g.model_base + tp0.mat * kMaxMat + tp1.mat];
-      const Body64 b0{x0, t0 ? vt : vu, t0 ? wt : wu, tp0.mass, tp0.eqrad};
-      const Body64 b1{x1, t0 ? vu : vt, t0 ? wu : wt, tp1.mass, tp1.eqrad};
-      float3 f, mr, kd = f3(0.f, 0.f, 0.f), pn = kd, sp = kd;
-      int re;
-      ++nlaw;
-      if (m.memory) {
-        const int id0 = t0 ? ida : idb, id1 = t0 ? idb : ida;
-        const unsigned long long key = pairKey(id0, id1);
-        int old = histFind(S.hist_old, key, tag_old);
-        if (old >= 0) loadHistF(S.hist_old, old, kd, pn, sp);
-        contactLaw32(m, S.dt, ct, b0, b1, old >= 0, kd, pn, sp, f, mr, re);
-        if (t0) {
-          int slot = histInsert(S.hist_new, key, tag);
-          if (slot < 0) raise(S.status, kErrHashFull);
-          else storeHistF(S.hist_new, slot, kd, pn, sp);
-        }
-      } else {
-        contactLaw32(m, S.dt, ct, b0, b1, false, kd, pn, sp, f, mr, re);
-      }
-      nre += re;
+      float3 f, c0, c1, mr;
+      double dl;
+      bool rolling;
+      const bool hit = evalPair32<kConvex>(
+          S, g, t0 ? t : u, t0 ? u : t, t0 ? ida : idb, t0 ? idb : ida, t0 ? ta : tb,
+          t0 ? tb : ta, t0 ? xt : xu, t0 ? xu + shift : xt + (-shift), t0 ? vt : vu,
+          t0 ? vu : vt, t0 ? wt : wu, t0 ? wu : wt, t0, nlaw, nre, gjk, dl, f, c0, c1, mr,
+          rolling);
       if (S.diag) {
-        double* fd = S.pair_force + 3 * ((size_t)t * kPairCap + e);
-        fd[0] = f.x; fd[1] = f.y; fd[2] = f.z;
+        S.pair_delta[(size_t)t * kPairCap + e] = dl;
+        if (hit) {
+          double* fd = S.pair_force + 3 * ((size_t)t * kPairCap + e);
+          fd[0] = f.x; fd[1] = f.y; fd[2] = f.z;
+        }
       }
+      if (!hit) continue;
       if (t0) {
         Fs = Fs + f;
-        Ts = Ts + crossf(lev0, f);
-        if (m.rolling) Ts = Ts + mr;
+        Ts = Ts + c0;
+        if (rolling) Ts = Ts + mr;
       } else {
         Fs = Fs - f;
-        Ts = Ts - crossf(lev1, f);
-        if (m.rolling) Ts = Ts - mr;
+        Ts = Ts - c1;
+        if (rolling) Ts = Ts - mr;
       }
     }
   }
@@ -454,7 +509,7 @@ __device__ __forceinline__ void forcesOn32(DevState const& S, int t, int na, int
 // Persistent grid.  sparse: only the particles of the work list (those with
 // a listed contact or near a wall); the others keep their weight, which
 // k_move applies without reading F, T.  Otherwise every particle.
-template <bool kConvex>
+template <bool kConvex, bool kSums>
 __global__ void __launch_bounds__(256) k_forces32(DevState S, int sparse) {
   const int stride = gridDim.x * blockDim.x;
   pdlWait();      // the contact filter's work list and flags
@@ -465,7 +520,7 @@ __global__ void __launch_bounds__(256) k_forces32(DevState S, int sparse) {
   GjkTally gjk;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += stride) {
     const int t = sparse ? S.work[i] : i;
-    forcesOn32<kConvex>(S, t, flags[t], sparse, nlaw, nre, gjk);
+    forcesOn32<kConvex, kSums>(S, t, flags[t], sparse, nlaw, nre, gjk);
   }
   if constexpr (kConvex) gjk.flush(S.gjk_counts);
   // warp-aggregated counters of the FP64 re-evaluations (every lane of the
@@ -477,6 +532,73 @@ __global__ void __launch_bounds__(256) k_forces32(DevState S, int sparse) {
   }
 }
 
+// First phase of the two-phase force path (systems with convex bodies):
+// each pair kept by the contact filter is evaluated once, by one thread -- a
+// GJK pair is far more work than the sum that follows -- and its two shares
+// are written for the partners' sums (forcesOn32 with kSums).  The pair is
+// seen from its lower ID (an upper entry), which writes the history, as in
+// the one-phase path, so both paths give the same forces.
+template <bool kConvex>
+__global__ void __launch_bounds__(128) k_pairforces32(DevState S) {
+  pdlWait();      // the contact filter's kept pairs
+  pdlTrigger();   // the force sums may be scheduled; they wait for this kernel
+  const int nk = S.ctl[kCtlKept];
+  const int stride = gridDim.x * blockDim.x;
+  const int cap = S.cap;
+  int nlaw = 0, nre = 0;
+  GjkTally gjk;
+  PairShare32* share = static_cast<PairShare32*>(S.pshare);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nk; k += stride) {
+    const int2 pr = S.upairs[S.kept[k]];
+    const int t = pr.x;
+    const unsigned ent = (unsigned)pr.y;
+    const int u = (int)(ent & ((1u << 27) - 1u));
+    const int et = findEntry(S, t, u), eu = findEntry(S, u, t);
+    GridDesc const& g = S.grids[S.inst[t]];
+    int sh[3];
+    entryShift(S, ent, t, u, sh);
+    const d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
+    const d3 xt = ld3(S.x, cap, t), xu = ld3(S.x, cap, u);
+    float3 f, c0, c1, mr;
+    double dl;
+    bool rolling;
+    const bool hit = evalPair32<kConvex>(
+        S, g, t, u, S.id[t], S.id[u], S.types[S.type[t]], S.types[S.type[u]], xt, xu + shift,
+        ld3(S.v, cap, t), ld3(S.v, cap, u), ld3(S.w, cap, t), ld3(S.w, cap, u), true, nlaw, nre,
+        gjk, dl, f, c0, c1, mr, rolling);
+    PairShare32 a, b;
+    const float3 zero = f3(0.f, 0.f, 0.f);
+    const float3 fa = hit ? f : zero, ca = hit ? c0 : zero, ma = hit ? mr : zero;
+    const float3 fb = hit ? -f : zero, cb = hit ? -c1 : zero, mb = hit ? -mr : zero;
+    a.f[0] = fa.x; a.f[1] = fa.y; a.f[2] = fa.z; a.c[0] = ca.x; a.c[1] = ca.y; a.c[2] = ca.z;
+    a.mr[0] = ma.x; a.mr[1] = ma.y; a.mr[2] = ma.z;
+    b.f[0] = fb.x; b.f[1] = fb.y; b.f[2] = fb.z; b.c[0] = cb.x; b.c[1] = cb.y; b.c[2] = cb.z;
+    b.mr[0] = mb.x; b.mr[1] = mb.y; b.mr[2] = mb.z;
+    share[2 * k] = a;
+    share[2 * k + 1] = b;
+    if (et >= 0) S.eslot[(size_t)t * kPairCap + et] = 2 * k;
+    if (eu >= 0) S.eslot[(size_t)u * kPairCap + eu] = 2 * k + 1;
+    if (S.diag) {
+      for (int side = 0; side < 2; ++side) {
+        const int s = side ? u : t, e = side ? eu : et;
+        if (e < 0) continue;
+        S.pair_delta[(size_t)s * kPairCap + e] = dl;
+        if (hit) {
+          double* fd = S.pair_force + 3 * ((size_t)s * kPairCap + e);
+          fd[0] = f.x; fd[1] = f.y; fd[2] = f.z;
+        }
+      }
+    }
+  }
+  // warp-aggregated counters (every lane of the warp reaches this point)
+  const int wl = __reduce_add_sync(0xffffffffu, nlaw), wr = __reduce_add_sync(0xffffffffu, nre);
+  if ((threadIdx.x & 31) == 0 && wl) {
+    atomicAdd(S.law_counts, (unsigned long long)wl);
+    if (wr) atomicAdd(S.law_counts + 1, (unsigned long long)wr);
+  }
+  if constexpr (kConvex) gjk.flush(S.gjk_counts);
+}
+
 }  // namespace
 
 void launch_pairs32(DevState const& S, const int* gate, cudaStream_t st) {
@@ -485,8 +607,13 @@ void launch_pairs32(DevState const& S, const int* gate, cudaStream_t st) {
 void launch_forces32(DevState const& S, int sparse, cudaStream_t st) {
   if (!S.n) return;
   const int grid = std::min((S.n + 255) / 256, (S.forces_bps > 0 ? S.forces_bps : 4) * S.nsm);
-  if (S.any_convex) launchAfterPrevious(k_forces32<true>, grid, 256, st, S, sparse);
-  else launchAfterPrevious(k_forces32<false>, grid, 256, st, S, sparse);
+  if (S.any_convex) {
+    // two phases: each kept pair once, then the sums
+    launchAfterPrevious(k_pairforces32<true>, 4 * S.nsm, 128, st, S);
+    launchAfterPrevious(k_forces32<true, true>, grid, 256, st, S, sparse);
+  } else {
+    launchAfterPrevious(k_forces32<false, false>, grid, 256, st, S, sparse);
+  }
 }
 
 }  // namespace gdem

@@ -74,9 +74,79 @@ __device__ __forceinline__ void storeHist(HistTable const& t, int slot, d3 kd, d
   v[6] = sp.x; v[7] = sp.y; v[8] = sp.z;
 }
 
-// kConvex: some class is not a sphere, so the GJK narrow phase is compiled in
-// (it is kept out of the sphere-only kernel, whose registers it would triple).
+// One pair in the canonical orientation -- p0 (slot s0, the lower ID) at its
+// own position, p1 at its periodic image seen from p0 -- with the
+// reference's expressions (closest points, Hooke / HookeMemory) and the
+// contact history (the new entry written when insert).  Returns true for a
+// contact, with the force f on p0, the torques c0 = (point - x0) x f and
+// c1m = (point - x1) x (-f) of p0 and p1, and the rolling torque mr
+// (rolling: the model has rolling resistance); delta gets the distance
+// (+inf without contact).  kConvex: some class is not a sphere, so the GJK
+// narrow phase is compiled in.
 template <bool kConvex>
+__device__ __forceinline__ bool evalPair64(DevState const& S, GridDesc const& g, int s0, int s1,
+                                           int id0, int id1, TypeDesc const& tp0,
+                                           TypeDesc const& tp1, d3 x0, d3 x1, d3 v0, d3 v1,
+                                           d3 w0, d3 w1, bool insert, GjkTally& gjk,
+                                           double& delta, d3& f, d3& c0, d3& c1m, d3& mr,
+                                           bool& rolling) {
+  const int cap = S.cap;
+  const unsigned tag = (unsigned)S.ctl[kCtlEpoch], tag_old = tag - 1u;
+  Contact64 ct;
+  if (!kConvex || (tp0.shape == 0 && tp1.shape == 0)) {
+    ct = sphereSphere64(x0, tp0.radius, tp0.crust, x1, tp1.radius, tp1.crust);
+  } else {
+    ct = convexContact64(convexOf(tp0, S.poly_verts), crustXForm(S.basis, cap, s0, tp0.scaling, x0),
+                         tp0.radius, tp0.crust, convexOf(tp1, S.poly_verts),
+                         crustXForm(S.basis, cap, s1, tp1.scaling, x1), tp1.radius, tp1.crust);
+    if (insert) gjk.add(ct.gjk_iters);   // each pair counted once
+  }
+  delta = ct.contact ? ct.dist : __longlong_as_double(0x7ff0000000000000ll);
+  if (!ct.contact || !(ct.dist < 0.)) return false;
+  if (ct.error) raise(S.status, kErrContactOverlap);
+  ModelDesc const& m = S.models[g.model_base + tp0.mat * kMaxMat + tp1.mat];
+  if (m.memory) {
+    const unsigned long long key = pairKey(id0, id1);
+    int old = histFind(S.hist_old, key, tag_old);
+    d3 kd, pn, sp;
+    if (old >= 0) loadHist(S.hist_old, old, kd, pn, sp);
+    hodc64(m, S.dt, ct.point, ct.overlap, x0, v0, w0, tp0.mass, tp0.eqrad, x1, v1, w1, tp1.mass,
+           tp1.eqrad, old >= 0, kd, pn, sp, f, mr);
+    if (insert) {
+      int slot = histInsert(S.hist_new, key, tag);
+      if (slot < 0) raise(S.status, kErrHashFull);
+      else storeHist(S.hist_new, slot, kd, pn, sp);
+    }
+  } else {
+    hooke64(m, ct.point, ct.overlap, x0, v0, w0, tp0.mass, tp0.eqrad, x1, v1, w1, tp1.mass,
+            tp1.eqrad, f, mr);
+  }
+  c0 = cross(ct.point - x0, f);
+  c1m = cross(ct.point - x1, -f);
+  rolling = m.rolling != 0;
+  if (!rolling) mr = mk(0., 0., 0.);
+  return true;
+}
+
+// Position in slot t's list of the entry whose partner is slot u.
+__device__ __forceinline__ int findEntry(DevState const& S, int t, int u) {
+  const int n = S.npairs[t];
+  const int* seg = S.pairs + (size_t)t * kPairCap;
+  for (int e = 0; e < n; ++e)
+    if ((int)((unsigned)seg[e] & ((1u << 27) - 1u)) == u) return e;
+  return -1;
+}
+
+// One side's share of a pair (two-phase path): force and torque terms in the
+// order the per-particle sum adds them.
+struct PairShare64 { double f[3], c[3], mr[3]; };
+
+// Forces and torques on particle t.  kSums (two-phase path, systems with
+// convex bodies): the pairs were evaluated once each by k_pairforces64, and
+// each kept entry's share is read back; otherwise both partners of a pair
+// evaluate it, with identical operands, and the lower ID writes the history.
+// Either way the shares are added in list order, then the walls.
+template <bool kConvex, bool kSums>
 __device__ __forceinline__ void forcesOn64(DevState const& S, int t, int na, int sparse,
                                            GjkTally& gjk) {
   const int cap = S.cap;
@@ -105,6 +175,13 @@ __device__ __forceinline__ void forcesOn64(DevState const& S, int t, int na, int
     while (keep) {
       const int e = e0 + __ffs(keep) - 1;
       keep &= keep - 1u;
+      if constexpr (kSums) {
+        const PairShare64 r = static_cast<const PairShare64*>(S.pshare)[S.eslot[(size_t)t * kPairCap + e]];
+        F = F + mk(r.f[0], r.f[1], r.f[2]);
+        T = T + mk(r.c[0], r.c[1], r.c[2]);
+        T = T + mk(r.mr[0], r.mr[1], r.mr[2]);
+        continue;
+      }
       const uint32_t ent = (uint32_t)seg[e];
       const int u = (int)(ent & ((1u << 27) - 1));
       int sh[3];
@@ -115,65 +192,29 @@ __device__ __forceinline__ void forcesOn64(DevState const& S, int t, int na, int
       const d3 xu = ld3(S.x, cap, u), vu = ld3(S.v, cap, u), wu = ld3(S.w, cap, u);
       const bool t0 = ida < idb;
       // canonical bodies: p0 = lower ID at its own position, p1 at its image
-      d3 x0, x1, v0, v1, w0, w1;
-      double r0, r1, c0, c1, m0, m1, q0, q1;
-      int mat0, mat1, id0, id1;
-      if (t0) {
-        x0 = xt; v0 = vt; w0 = wt; r0 = ta.radius; m0 = ta.mass; q0 = ta.eqrad; c0 = ta.crust;
-        mat0 = ta.mat; id0 = ida;
-        x1 = xu + shift; v1 = vu; w1 = wu; r1 = tb.radius; m1 = tb.mass; q1 = tb.eqrad;
-        c1 = tb.crust; mat1 = tb.mat; id1 = idb;
-      } else {
-        x0 = xu; v0 = vu; w0 = wu; r0 = tb.radius; m0 = tb.mass; q0 = tb.eqrad; c0 = tb.crust;
-        mat0 = tb.mat; id0 = idb;
-        x1 = xt + (-shift); v1 = vt; w1 = wt; r1 = ta.radius; m1 = ta.mass; q1 = ta.eqrad;
-        c1 = ta.crust; mat1 = ta.mat; id1 = ida;
-      }
-      Contact64 ct;
-      if (!kConvex || (ta.shape == 0 && tb.shape == 0)) {
-        ct = sphereSphere64(x0, r0, c0, x1, r1, c1);
-      } else {
-        TypeDesc const& tp0 = t0 ? ta : tb;
-        TypeDesc const& tp1 = t0 ? tb : ta;
-        const int s0 = t0 ? t : u, s1 = t0 ? u : t;
-        ct = convexContact64(convexOf(tp0, S.poly_verts), crustXForm(S.basis, cap, s0, tp0.scaling, x0),
-                             r0, c0, convexOf(tp1, S.poly_verts),
-                             crustXForm(S.basis, cap, s1, tp1.scaling, x1), r1, c1);
-        gjk.add(ct.gjk_iters);
-      }
-      if (S.diag) S.pair_delta[(size_t)t * kPairCap + e] = ct.contact ? ct.dist : __longlong_as_double(0x7ff0000000000000ll);
-      if (!ct.contact || !(ct.dist < 0.)) continue;
-      if (ct.error) raise(S.status, kErrContactOverlap);
-      ModelDesc const& m = S.models[g.model_base + mat0 * kMaxMat + mat1];
-      d3 f, mr;
-      if (m.memory) {
-        const unsigned long long key = pairKey(id0, id1);
-        int old = histFind(S.hist_old, key, tag_old);
-        d3 kd, pn, sp;
-        if (old >= 0) loadHist(S.hist_old, old, kd, pn, sp);
-        hodc64(m, dt, ct.point, ct.overlap, x0, v0, w0, m0, q0, x1, v1, w1, m1, q1, old >= 0,
-               kd, pn, sp, f, mr);
-        if (t0) {
-          int slot = histInsert(S.hist_new, key, tag);
-          if (slot < 0) raise(S.status, kErrHashFull);
-          else storeHist(S.hist_new, slot, kd, pn, sp);
-        }
-      } else {
-        hooke64(m, ct.point, ct.overlap, x0, v0, w0, m0, q0, x1, v1, w1, m1, q1, f, mr);
-      }
+      d3 f, c0, c1m, mr;
+      double dl;
+      bool rolling;
+      const bool hit = evalPair64<kConvex>(
+          S, g, t0 ? t : u, t0 ? u : t, t0 ? ida : idb, t0 ? idb : ida, t0 ? ta : tb,
+          t0 ? tb : ta, t0 ? xt : xu, t0 ? xu + shift : xt + (-shift), t0 ? vt : vu,
+          t0 ? vu : vt, t0 ? wt : wu, t0 ? wu : wt, t0, gjk, dl, f, c0, c1m, mr, rolling);
       if (S.diag) {
-        double* fd = S.pair_force + 3 * ((size_t)t * kPairCap + e);
-        fd[0] = f.x; fd[1] = f.y; fd[2] = f.z;
+        S.pair_delta[(size_t)t * kPairCap + e] = dl;
+        if (hit) {
+          double* fd = S.pair_force + 3 * ((size_t)t * kPairCap + e);
+          fd[0] = f.x; fd[1] = f.y; fd[2] = f.z;
+        }
       }
+      if (!hit) continue;
       if (t0) {
         F = F + f;
-        T = T + cross(ct.point - x0, f);
-        if (m.rolling) T = T + mr;
+        T = T + c0;
+        if (rolling) T = T + mr;
       } else {
-        d3 fm = -f;
-        F = F + fm;
-        T = T + cross(ct.point - x1, fm);
-        if (m.rolling) T = T + (-mr);
+        F = F + (-f);
+        T = T + c1m;
+        if (rolling) T = T + (-mr);
       }
     }
   }
@@ -224,7 +265,7 @@ __device__ __forceinline__ void forcesOn64(DevState const& S, int t, int na, int
 // Persistent grid.  sparse: only the particles of the work list (those with
 // a listed contact or near a wall); the others keep their weight, which
 // k_move applies without reading F, T.  Otherwise every particle.
-template <bool kConvex>
+template <bool kConvex, bool kSums>
 __global__ void __launch_bounds__(256) k_forces64(DevState S, int sparse) {
   const int stride = gridDim.x * blockDim.x;
   pdlWait();      // the contact filter's work list and flags
@@ -234,9 +275,69 @@ __global__ void __launch_bounds__(256) k_forces64(DevState S, int sparse) {
   GjkTally gjk;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += stride) {
     const int t = sparse ? S.work[i] : i;
-    forcesOn64<kConvex>(S, t, flags[t], sparse, gjk);
+    forcesOn64<kConvex, kSums>(S, t, flags[t], sparse, gjk);
   }
   // (every lane of the warp reaches this point: no thread leaves the loop early)
+  if constexpr (kConvex) gjk.flush(S.gjk_counts);
+}
+
+// First phase of the two-phase force path (systems with convex bodies):
+// each pair kept by the contact filter is evaluated once, by one thread, and
+// its two shares are written for the partners' sums (forcesOn64 with
+// kSums).  The pair is seen from its lower ID (an upper entry), which writes
+// the history, as in the one-phase path, so both paths give the same forces.
+template <bool kConvex>
+__global__ void __launch_bounds__(128) k_pairforces64(DevState S) {
+  pdlWait();      // the contact filter's kept pairs
+  pdlTrigger();   // the force sums may be scheduled; they wait for this kernel
+  const int nk = S.ctl[kCtlKept];
+  const int stride = gridDim.x * blockDim.x;
+  const int cap = S.cap;
+  GjkTally gjk;
+  PairShare64* share = static_cast<PairShare64*>(S.pshare);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nk; k += stride) {
+    const int2 pr = S.upairs[S.kept[k]];
+    const int t = pr.x;
+    const unsigned ent = (unsigned)pr.y;
+    const int u = (int)(ent & ((1u << 27) - 1u));
+    const int et = findEntry(S, t, u), eu = findEntry(S, u, t);
+    GridDesc const& g = S.grids[S.inst[t]];
+    int sh[3];
+    entryShift(S, ent, t, u, sh);
+    const d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
+    const d3 xt = ld3(S.x, cap, t), xu = ld3(S.x, cap, u);
+    d3 f, c0, c1m, mr;
+    double dl;
+    bool rolling;
+    const bool hit = evalPair64<kConvex>(
+        S, g, t, u, S.id[t], S.id[u], S.types[S.type[t]], S.types[S.type[u]], xt, xu + shift,
+        ld3(S.v, cap, t), ld3(S.v, cap, u), ld3(S.w, cap, t), ld3(S.w, cap, u), true, gjk, dl,
+        f, c0, c1m, mr, rolling);
+    const d3 zero = mk(0., 0., 0.);
+    const d3 fa = hit ? f : zero, ca = hit ? c0 : zero, ma = hit ? mr : zero;
+    const d3 fb = hit ? -f : zero, cb = hit ? c1m : zero, mb = hit ? -mr : zero;
+    PairShare64 a, b;
+    a.f[0] = fa.x; a.f[1] = fa.y; a.f[2] = fa.z; a.c[0] = ca.x; a.c[1] = ca.y; a.c[2] = ca.z;
+    a.mr[0] = ma.x; a.mr[1] = ma.y; a.mr[2] = ma.z;
+    b.f[0] = fb.x; b.f[1] = fb.y; b.f[2] = fb.z; b.c[0] = cb.x; b.c[1] = cb.y; b.c[2] = cb.z;
+    b.mr[0] = mb.x; b.mr[1] = mb.y; b.mr[2] = mb.z;
+    share[2 * k] = a;
+    share[2 * k + 1] = b;
+    if (et >= 0) S.eslot[(size_t)t * kPairCap + et] = 2 * k;
+    if (eu >= 0) S.eslot[(size_t)u * kPairCap + eu] = 2 * k + 1;
+    if (S.diag) {
+      for (int side = 0; side < 2; ++side) {
+        const int s = side ? u : t, e = side ? eu : et;
+        if (e < 0) continue;
+        S.pair_delta[(size_t)s * kPairCap + e] = dl;
+        if (hit) {
+          double* fd = S.pair_force + 3 * ((size_t)s * kPairCap + e);
+          fd[0] = f.x; fd[1] = f.y; fd[2] = f.z;
+        }
+      }
+    }
+  }
+  // (every lane of the warp reaches this point)
   if constexpr (kConvex) gjk.flush(S.gjk_counts);
 }
 
@@ -248,8 +349,13 @@ void launch_pairs64(DevState const& S, const int* gate, cudaStream_t st) {
 void launch_forces64(DevState const& S, int sparse, cudaStream_t st) {
   if (!S.n) return;
   const int grid = std::min((S.n + 255) / 256, (S.forces_bps > 0 ? S.forces_bps : 4) * S.nsm);
-  if (S.any_convex) launchAfterPrevious(k_forces64<true>, grid, 256, st, S, sparse);
-  else launchAfterPrevious(k_forces64<false>, grid, 256, st, S, sparse);
+  if (S.any_convex) {
+    // two phases: each kept pair once, then the sums
+    launchAfterPrevious(k_pairforces64<true>, 4 * S.nsm, 128, st, S);
+    launchAfterPrevious(k_forces64<true, true>, grid, 256, st, S, sparse);
+  } else {
+    launchAfterPrevious(k_forces64<false, false>, grid, 256, st, S, sparse);
+  }
 }
 
 }  // namespace gdem

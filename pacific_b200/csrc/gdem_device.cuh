@@ -127,6 +127,10 @@ struct DevState {
   // pair list: per-particle segments of kPairCap entries
   int* pairs; int* npairs;   // skin list (rebuilt on demand)
   int2* upairs;           // compact pair list: (slot, entry) of every upper entry, ctl[kCtlPairs] of them
+  // two-phase force path (systems with convex bodies; null otherwise)
+  int* kept;              // compact-list indices of the pairs kept by the filter, ctl[kCtlKept]
+  int* eslot;             // per list entry: index of its share in pshare (this step)
+  void* pshare;           // per kept pair: the two partners' force and torque shares
   int* nact;              // contact-filter flags, two buffers of cap (contactFlags)
   float4* posf;           // FP32 continuous position since the last rebuild + circumscribed radius
   int* work;              // particles with a listed contact or near a wall (this step)

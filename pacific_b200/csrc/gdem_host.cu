@@ -734,6 +734,13 @@ struct System {
     }
     S.pairs = alloc<int>(c * kPairCap); S.npairs = alloc<int>(c);
     S.upairs = alloc<int2>(c * kUpperCap);
+    if (S.any_convex) {
+      S.kept = alloc<int>(c * kUpperCap);
+      S.eslot = alloc<int>(c * kPairCap);
+      S.pshare = alloc<char>(c * kUpperCap * 2 * (precision == GDEM_FP64 ? 72 : 36));
+    } else {
+      S.kept = nullptr; S.eslot = nullptr; S.pshare = nullptr;
+    }
     S.nact = alloc<int>(2 * c);
     CK(cudaMemset(S.nact, 0, 2 * c * sizeof(int)));
     S.work = alloc<int>(c);

@@ -50,6 +50,7 @@ __global__ void k_decide(DevState S, cudaGraphConditionalHandle h, int use_handl
   S.ctl[kCtlEpoch] += 1;
   S.ctl[kCtlRebuilds] += need ? 1 : 0;
   S.ctl[kCtlWork] = 0;
+  S.ctl[kCtlKept] = 0;
   if (need) S.ctl[kCtlPairs] = 0;
   if (use_handle) cudaGraphSetConditional(h, need ? 1u : 0u);
 }
@@ -308,6 +309,18 @@ __device__ __forceinline__ void appendWork(DevState const& S, bool pred, int idx
   if (pred) S.work[base + __popc(m & ((1u << lane) - 1u))] = idx;
 }
 
+// Appends idx to list (length *count) for every lane whose pred holds (one
+// atomic per warp); every lane of the warp calls it.
+__device__ __forceinline__ void appendList(int* list, int* count, bool pred, int idx) {
+  const unsigned m = __ballot_sync(0xffffffffu, pred);
+  if (!m) return;
+  const int lane = threadIdx.x & 31;
+  int base = 0;
+  if (lane == 0) base = atomicAdd(count, __popc(m));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (pred) list[base + __popc(m & ((1u << lane) - 1u))] = idx;
+}
+
 // Sets flag bits of particle i; true for the caller that lists it first.
 __device__ __forceinline__ bool flagParticle(int* flags, int i, int bits) {
   return !(atomicOr(&flags[i], bits | kListed) & kListed);
@@ -402,6 +415,7 @@ __global__ void __launch_bounds__(256) k_filter(DevState S, int pblocks) {
       }
       appendWork(S, newT, t);
       appendWork(S, newU, u);
+      if (S.kept) appendList(S.kept, S.ctl + kCtlKept, keep, c0 + 32 * j + lane);
     }
   }
 }

@@ -35,6 +35,7 @@ enum CtlWords : int {
   kCtlRebuilds = 3, // pair-list rebuilds so far
   kCtlWork = 4,     // particles the force kernel must evaluate this step (work list length)
   kCtlPairs = 5,    // pairs of the compact pair list (set by the rebuild)
+  kCtlKept = 6,     // pairs kept by this step's contact filter (two-phase force path)
   kCtlWords = 8
 };
 
