@@ -168,6 +168,25 @@ int gdem_step(gdem_handle h, int nsteps);
 int gdem_download_state(gdem_handle h, double* x, double* v, double* w, double* wbf,
                         double* q, double* F, double* T);
 
+/* Format2024 reload, particle file: the "<reload>_Particles" text file that
+ * AllComponents::write writes and AllComponents::read_particles reads
+ * (Component/src/AllComponents.cpp:1299-1420, 1136-1290), one line per
+ * particle as Particle::write2014 (Particle.cpp:1167-1176): class, ID, tag,
+ * activity, position and orientation matrix (Transform::writeTransform2014),
+ * velocity, quaternion (w, x, y, z), angular velocity, force, torque
+ * (SecondOrderLeapFrog.cpp:102-109) and the contact memory
+ * (Component::writeContactMemory2014, Component.cpp:776-801).  IDs are the
+ * reference's (1-based); an obstacle partner is -(k + 1) for wall k.  One
+ * system (not a batch).  gdem_write_reload_particles writes the state after
+ * the last step (tags written 0, activity 1); gdem_read_reload_particles
+ * loads such a file into a created system without particles (it replaces
+ * gdem_upload_state + gdem_upload_basis + gdem_upload_forces +
+ * gdem_upload_history: the leapfrog continues from the stored forces,
+ * without gdem_init); periodic clones (tag 2) and inactive particles are
+ * skipped. */
+int gdem_write_reload_particles(gdem_handle h, const char* path);
+int gdem_read_reload_particles(gdem_handle h, const char* path);
+
 /* Cell (i, j, k) of every particle, in Cell::GetCell numbering
  * (Base/src/Cell.cpp:172-184), by particle ID. */
 int gdem_download_cells(gdem_handle h, int* ijk);

@@ -15,6 +15,7 @@
 // computeParticlesForceAndTorque + setAllContactMapCumulativeFeaturesToZero;
 // a step is moveParticlesAndObstacles(dt/2, dt, dt),
 // computeParticlesForceAndTorque, advanceParticlesVelocity(dt/2).
+#include <fstream>
 #include <map>
 #include <vector>
 
@@ -238,6 +239,18 @@ void ref_get_history(void* h, int* owner, int* partner, double* kdelta, double* 
       ++n;
     }
   }
+}
+
+// The particle file of a Format2024 reload, written by the reference's own
+// Particle::write2014 (Component/src/Particle.cpp:1167-1176) for every
+// master in particle-index order.
+int ref_write_particles(void* h, const char* path) {
+  RefGrains* g = static_cast<RefGrains*>(h);
+  std::ofstream out(path);
+  if (!out) return 1;
+  for (Particle* p : g->masters())
+    if (p) p->write2014(out);
+  return out ? 0 : 1;
 }
 
 void ref_destroy(void* h) { delete static_cast<RefGrains*>(h); }

@@ -48,6 +48,8 @@ def _load():
         lib.ref_num_history.argtypes = [V]
         lib.ref_num_history.restype = ctypes.c_int
         lib.ref_get_history.argtypes = [V, I, I, D, D, D]
+        lib.ref_write_particles.argtypes = [V, ctypes.c_char_p]
+        lib.ref_write_particles.restype = ctypes.c_int
         lib.ref_destroy.argtypes = [V]
         _lib = lib
     return _lib
@@ -102,6 +104,10 @@ class Reference:
         ijk = np.empty((self.n, 3), np.int32)
         _load().ref_get_cells(self._h, _ip(ijk))
         return ijk
+
+    def write_particles(self, path):
+        """The particle file of a Format2024 reload, by Particle::write2014."""
+        return _load().ref_write_particles(self._h, os.fsencode(str(path)))
 
     def history(self):
         lib = _load()

@@ -16,6 +16,7 @@
 // Steps after the first of a gdem_step call are replayed from two captured
 // CUDA graphs (the double-buffered state and history tables alternate with
 // period two).
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <cstdio>
@@ -502,6 +503,7 @@ struct System {
   std::vector<std::string> xml_paths;
   std::vector<GridDesc> h_bgrids;  // host copy of the pair-list grids
   std::vector<int> h_type, h_inst; // uploaded classes (instance-local) and instances, by ID
+  std::vector<int> ref_ids;        // reload particle IDs by particle index (empty: index + 1)
   double tune_skin = -1.;          // skin as a multiple of rmax (< 0: the XML's or 0.25)
   int tune_bps = 0;                // force-kernel blocks per multiprocessor (0: 4)
   std::vector<int> type_base;     // first global type of each instance
@@ -1396,6 +1398,231 @@ int gdem_download_basis(gdem_handle h, double* basis) {
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(basis, d, 9 * n * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
     CK(cudaStreamSynchronize(s->stream));
+    return GDEM_OK;
+  });
+}
+
+// ------------------------------------------------------ Format2024 reload --
+// The particle file of a Format2024 reload (the "<reload>_Particles" text
+// file that AllComponents::write and AllComponents::read_particles exchange,
+// Component/src/AllComponents.cpp:1299-1420, 1136-1290), one line per
+// particle (Particle::write2014, Particle.cpp:1167-1176):
+//   class ID tag active | origin(3) basis(9, by rows) transform-type |
+//   v(3) q(w, x, y, z) w(3) | F(3) T(3) (SecondOrderLeapFrog.cpp:102-109) |
+//   n, then n x (1 partner-ID 1 active kdelta(3) normal(3) spring(3)): the
+//   key's elementary IDs are 1 for simple bodies (HookeMemoryContactForce
+//   Model.cpp:218-221), (Component::writeContactMemory2014, Component.cpp:
+//   776-801).
+// Numbers as GrainsExec::doubleToString(ios::scientific, 16 digits) (d16).
+// Particle IDs are the reference's (1-based insertion numbers, Particle.cpp:
+// 45-50); an obstacle partner is -(k + 1) for wall k (obstacle IDs count
+// down from -1, Obstacle.cpp:28-32).  Both partners of a pair carry it, the
+// higher ID with the signs reversed (HookeMemoryContactForceModel.cpp:
+// 191-192).  The transform type is written 3 (translation | rotation), what
+// the reference's particles carry after their first step.
+namespace {
+
+// GrainsExec::doubleToString(ios::scientific, 16, v) (Base/src/GrainsExec.cpp:
+// 212-224): an exact zero in the stream's default format
+std::string d16(double v) {
+  if (v == 0.) return std::signbit(v) ? "-0" : "0";
+  char buf[40];
+  std::snprintf(buf, sizeof(buf), "%.16e", v);
+  return buf;
+}
+
+// Matrix::setRotation (Geometry/src/Matrix.cpp:114-127) of q = (x, y, z, w).
+void rotationOf(const double* q, double* m) {
+  const double x = q[0], y = q[1], z = q[2], w = q[3];
+  const double s = 2.0 / (x * x + y * y + z * z + w * w);
+  const double xs = x * s, ys = y * s, zs = z * s;
+  const double wx = w * xs, wy = w * ys, wz = w * zs;
+  const double xx = x * xs, xy = x * ys, xz = x * zs, yy = y * ys, yz = y * zs, zz = z * zs;
+  const double r[9] = {1.0 - (yy + zz), xy - wz, xz + wy, xy + wz, 1.0 - (xx + zz), yz - wx,
+                       xz - wy, yz + wx, 1.0 - (xx + yy)};
+  for (int k = 0; k < 9; ++k) m[k] = r[k];
+}
+
+struct MapEntry {
+  int partner;          // reload ID
+  double v[9];          // kdelta, normal, spring
+};
+
+}  // namespace
+
+int gdem_write_reload_particles(gdem_handle h, const char* path) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->started || !path) throw std::runtime_error("no stepped state to write");
+    if (s->inst.size() != 1) throw std::runtime_error("a reload file holds one system, not a batch");
+    DevState& S = s->S;
+    const size_t n = (size_t)S.n;
+    std::vector<double> x(3 * n), v(3 * n), w(3 * n), q(4 * n), F(3 * n), T(3 * n), B(9 * n);
+    CK(cudaStreamSynchronize(s->stream));
+    int rc = gdem_download_state(h, x.data(), v.data(), w.data(), nullptr, q.data(), F.data(),
+                                 T.data());
+    if (rc != GDEM_OK) throw std::runtime_error(g_last_error);
+    if (S.basis) {
+      rc = gdem_download_basis(h, B.data());
+      if (rc != GDEM_OK) throw std::runtime_error(g_last_error);
+    } else {
+      for (size_t i = 0; i < n; ++i) rotationOf(&q[4 * i], &B[9 * i]);
+    }
+    auto refId = [&](size_t i) { return s->ref_ids.empty() ? (int)i + 1 : s->ref_ids[i]; };
+    // contact memory of the last evaluation: the table the next one reads
+    HistTable const& t = S.hist_old;
+    const size_t hc = size_t(1) << t.log2cap;
+    std::vector<unsigned long long> keys(hc);
+    CK(cudaMemcpy(keys.data(), t.keys, hc * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    const bool fp64 = s->precision == GDEM_FP64;
+    std::vector<double> vd(fp64 ? 9 * hc : 0);
+    std::vector<float> vf(fp64 ? 0 : 9 * hc);
+    if (fp64) CK(cudaMemcpy(vd.data(), t.vals, vd.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    else CK(cudaMemcpy(vf.data(), t.vals, vf.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    std::vector<std::vector<MapEntry>> maps(n);
+    const unsigned tag = (unsigned)s->epoch & kTagMask;
+    const unsigned idmask = (1u << kMaxIdBits) - 1u;
+    for (size_t k = 0; k < hc; ++k) {
+      if (tagOf(keys[k]) != tag) continue;
+      const unsigned base_hi = (unsigned)((keys[k] >> kMaxIdBits) & idmask);
+      const unsigned base_lo = (unsigned)(keys[k] & idmask);
+      double val[9];
+      for (int c = 0; c < 9; ++c) val[c] = fp64 ? vd[9 * k + c] : (double)vf[9 * k + c];
+      const size_t a = base_hi;
+      if (a >= n) continue;
+      if (base_lo < n) {
+        const size_t b = base_lo;
+        MapEntry ea{refId(b), {}}, eb{refId(a), {}};
+        for (int c = 0; c < 9; ++c) { ea.v[c] = val[c]; eb.v[c] = -val[c]; }
+        maps[a].push_back(ea);
+        maps[b].push_back(eb);
+      } else {
+        const int wall = (int)(idmask - base_lo);
+        MapEntry ea{-(wall + 1), {}};
+        for (int c = 0; c < 9; ++c) ea.v[c] = val[c];
+        maps[a].push_back(ea);
+      }
+    }
+    std::ofstream out(path);
+    if (!out) throw std::runtime_error(std::string("cannot write ") + path);
+    for (size_t i = 0; i < n; ++i) {
+      auto& m = maps[i];
+      std::sort(m.begin(), m.end(), [](MapEntry const& p, MapEntry const& r) { return p.partner < r.partner; });
+      const double* b = &B[9 * i];
+      out << s->h_type[i] << " " << refId(i) << " 0 1 ";
+      out << d16(x[3 * i]) << " " << d16(x[3 * i + 1]) << " " << d16(x[3 * i + 2]);
+      for (int k = 0; k < 9; ++k) out << " " << d16(b[k]);
+      out << " 3 ";
+      out << d16(v[3 * i]) << " " << d16(v[3 * i + 1]) << " " << d16(v[3 * i + 2]) << " ";
+      out << d16(q[4 * i + 3]) << " " << d16(q[4 * i]) << " " << d16(q[4 * i + 1]) << " "
+          << d16(q[4 * i + 2]) << " ";
+      out << d16(w[3 * i]) << " " << d16(w[3 * i + 1]) << " " << d16(w[3 * i + 2]) << " ";
+      out << d16(F[3 * i]) << " " << d16(F[3 * i + 1]) << " " << d16(F[3 * i + 2]) << " ";
+      out << d16(T[3 * i]) << " " << d16(T[3 * i + 1]) << " " << d16(T[3 * i + 2]);
+      out << " " << m.size();
+      for (auto const& e : m) {
+        out << " 1 " << e.partner << " 1 1";
+        for (int c = 0; c < 9; ++c) out << " " << d16(e.v[c]);
+      }
+      out << "\n";
+    }
+    if (!out) throw std::runtime_error(std::string("write failed: ") + path);
+    return GDEM_OK;
+  });
+}
+
+int gdem_read_reload_particles(gdem_handle h, const char* path) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !path) throw std::runtime_error("invalid arguments");
+    if (s->have_state) throw std::runtime_error("the system already has particles");
+    if (s->inst.size() != 1) throw std::runtime_error("a reload file holds one system, not a batch");
+    std::ifstream in(path);
+    if (!in) throw std::runtime_error(std::string("cannot read ") + path);
+    struct Rec {
+      int cls, id;
+      double x[3], B[9], v[3], q[4], w[3], F[3], T[3];
+      std::vector<MapEntry> map;
+    };
+    std::vector<Rec> recs;
+    std::string line;
+    while (std::getline(in, line)) {
+      std::istringstream is(line);
+      Rec r;
+      int tag = 0, ttype = 0;
+      unsigned active = 0;
+      if (!(is >> r.cls >> r.id >> tag >> active)) continue;   // blank line
+      for (double& d : r.x) is >> d;
+      for (double& d : r.B) is >> d;
+      is >> ttype;
+      for (double& d : r.v) is >> d;
+      is >> r.q[3] >> r.q[0] >> r.q[1] >> r.q[2];
+      for (double& d : r.w) is >> d;
+      for (double& d : r.F) is >> d;
+      for (double& d : r.T) is >> d;
+      int nm = 0;
+      is >> nm;
+      for (int k = 0; k < nm; ++k) {
+        int e0 = 0, e1 = 0;
+        unsigned act = 0;
+        MapEntry e;
+        is >> e0 >> e.partner >> e1 >> act;
+        for (double& d : e.v) is >> d;
+        if (act) r.map.push_back(e);
+      }
+      if (!is) throw std::runtime_error("malformed particle line in " + std::string(path));
+      if (tag > 1 || !active) continue;   // periodic clones and waiting particles
+      if (r.cls < 0 || r.cls >= (int)s->inst[0].types.size())
+        throw std::runtime_error("particle class out of range in " + std::string(path));
+      recs.push_back(std::move(r));
+    }
+    if (recs.empty()) throw std::runtime_error(std::string("no particle in ") + path);
+    std::sort(recs.begin(), recs.end(), [](Rec const& a, Rec const& b) { return a.id < b.id; });
+    const size_t n = recs.size();
+    std::map<int, int> index;
+    std::vector<int> type(n), ids(n);
+    std::vector<double> x(3 * n), v(3 * n), w(3 * n), q(4 * n), F(3 * n), T(3 * n), B(9 * n);
+    for (size_t i = 0; i < n; ++i) {
+      Rec const& r = recs[i];
+      if (!index.emplace(r.id, (int)i).second) throw std::runtime_error("duplicate particle ID");
+      type[i] = r.cls;
+      ids[i] = r.id;
+      for (int d = 0; d < 3; ++d) {
+        x[3 * i + d] = r.x[d]; v[3 * i + d] = r.v[d]; w[3 * i + d] = r.w[d];
+        F[3 * i + d] = r.F[d]; T[3 * i + d] = r.T[d];
+      }
+      for (int d = 0; d < 4; ++d) q[4 * i + d] = r.q[d];
+      for (int k = 0; k < 9; ++k) B[9 * i + k] = r.B[k];
+    }
+    auto check = [](int code) {
+      if (code != GDEM_OK) throw std::runtime_error(g_last_error);
+    };
+    check(gdem_upload_state(h, (int64_t)n, nullptr, type.data(), x.data(), v.data(), w.data(),
+                            nullptr, q.data()));
+    check(gdem_upload_basis(h, B.data()));
+    s->ref_ids = ids;
+    // contact memory: owner index, partner index (walls -(k+2))
+    std::vector<int> owner, partner;
+    std::vector<double> kd, pn, sp;
+    for (size_t i = 0; i < n; ++i)
+      for (auto const& e : recs[i].map) {
+        int p;
+        if (e.partner >= 0) {
+          auto it = index.find(e.partner);
+          if (it == index.end()) continue;   // a partner not in the file
+          p = it->second;
+        } else {
+          p = e.partner - 1;   // obstacle -(k + 1) is wall k, -(k + 2) here
+        }
+        owner.push_back((int)i);
+        partner.push_back(p);
+        for (int c = 0; c < 3; ++c) {
+          kd.push_back(e.v[c]); pn.push_back(e.v[3 + c]); sp.push_back(e.v[6 + c]);
+        }
+      }
+    check(gdem_upload_forces(h, F.data(), T.data()));
+    check(gdem_upload_history(h, (int64_t)owner.size(), owner.data(), partner.data(), kd.data(),
+                              pn.data(), sp.data()));
     return GDEM_OK;
   });
 }

@@ -77,6 +77,8 @@ def library() -> ctypes.CDLL:
         "gdem_upload_state": ([_P, i64, _IP, _IP, _DP, _DP, _DP, _DP, _DP], ctypes.c_int),
         "gdem_upload_forces": ([_P, _DP, _DP], ctypes.c_int),
         "gdem_upload_history": ([_P, i64, _IP, _IP, _DP, _DP, _DP], ctypes.c_int),
+        "gdem_write_reload_particles": ([_P, ctypes.c_char_p], ctypes.c_int),
+        "gdem_read_reload_particles": ([_P, ctypes.c_char_p], ctypes.c_int),
         "gdem_init": ([_P], ctypes.c_int),
         "gdem_set_tuning": ([_P, ctypes.c_double, ctypes.c_int], ctypes.c_int),
         "gdem_autotune": ([_P, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
@@ -182,6 +184,17 @@ class Grains:
                                                  _dp(arrs[1]), _dp(arrs[2]), _dp(arrs[3]),
                                                  _dp(arrs[4])))
         self.n = n
+
+    def read_reload_particles(self, path):
+        """Loads a Format2024 reload particle file (state, forces, contact
+        memory); stepping then continues without do_before_time_stepping."""
+        self._check(library().gdem_read_reload_particles(self._h, os.fsencode(str(path))))
+        self.n = library().gdem_num_particles(self._h)
+
+    def write_reload_particles(self, path):
+        """Writes the state after the last step as a Format2024 reload
+        particle file."""
+        self._check(library().gdem_write_reload_particles(self._h, os.fsencode(str(path))))
 
     def upload_basis(self, basis):
         """Orientation matrices (n, 3, 3) or (n, 9), row-major, by particle ID;

@@ -7,7 +7,9 @@ from the unmodified reference sources).
 Each fixture holds the scenario parameters, the initial state, and the
 reference's state, cells and contact memory at a few step counts.  The
 "settling_box" fixture records consecutive snapshots (k, k+1) so that a
-single step can be checked from the reference's own state.
+single step can be checked from the reference's own state.  The
+"reload_settling" fixture holds a Format2024 reload particle file written by
+the reference itself and the reference's state after it.
 """
 from __future__ import annotations
 
@@ -120,16 +122,52 @@ def run(name):
         print(f"wrote {name}.npz ({len(sc.type)} particles, steps {marks})")
 
 
+def run_reload():
+    """The reload fixture: 200 spheres settling in the walled box, stepped
+    600 times by the reference, which then writes the particle file of a
+    Format2024 reload with its own Particle::write2014; then the reference's
+    state after 1 and 50 more steps."""
+    sc = scenarios.settling_box(n=200, seed=23)
+    with tempfile.TemporaryDirectory() as d:
+        xml = sc.write_xml(Path(d) / "reload.xml")
+        r = _quiet(reference.Reference, xml)
+        assert _quiet(r.set_particles, sc.type, sc.x, sc.v, sc.w, sc.q) == 0
+        assert _quiet(r.init) == 0
+        assert _quiet(r.step, 600) == 0
+        pfile = Path(d) / "reload_Particles"
+        assert r.write_particles(pfile) == 0
+        out = {"xml": np.array(sc.xml()), "particles": np.array(pfile.read_text()),
+               "marks": np.array([1, 50])}
+        from oracle.oracle import Oracle
+        from tests.helpers import contact_scale
+        done = 0
+        for m in (1, 50):
+            assert _quiet(r.step, m - done) == 0
+            done = m
+            snapshot(r, f"s{m}", out)
+            # the error normaliser (each particle's sum of contact-force
+            # magnitudes) from the CPU restatement at the reference's state
+            st = r.state()
+            o = Oracle(xml)
+            o.set_particles(sc.type, st["x"], st["v"], st["w"], st["q"], r.basis())
+            o.init()
+            id0, id1, dl, pt, f = o.contacts()
+            out[f"s{m}_scale"] = contact_scale(len(sc.type), id0, id1, f)
+    np.savez_compressed(HERE / "reload_settling.npz", **out)
+    print("wrote reload_settling.npz (200 particles, particle file after 600 steps)")
+
+
 def main():
     import subprocess
     if not reference.available():
         reference.build()
     for name in SCENARIOS:
         subprocess.run([sys.executable, __file__, name], check=True)
+    subprocess.run([sys.executable, __file__, "reload"], check=True)
 
 
 if __name__ == "__main__":
     if len(sys.argv) > 1:
-        run(sys.argv[1])
+        run_reload() if sys.argv[1] == "reload" else run(sys.argv[1])
     else:
         main()
