@@ -156,6 +156,44 @@ int gdem_autotune(gdem_handle h, int trial_steps, double* skin_factor, int* bloc
  * cumulative tangential and rolling memories. */
 int gdem_init(gdem_handle h);
 
+/* ---- fluid coupling (GrainsCoupledWithFluid, Fluid/src/
+ * GrainsCoupledWithFluid.cpp; the Basilisk C ABI of
+ * libgrains_b200_basilisk.so is built on these) ---- */
+
+/* Fluid density: the weight becomes m (1 - rho_f / rho) g
+ * (Particle::computeWeight, Particle.cpp:413-418) and, with
+ * corrected_acceleration, the kicks divide by m c and c I with the coupling
+ * factor c = 1 - rho_f / rho (ParticleKinematics::setCouplingFactor,
+ * ParticleKinematics.cpp:483-488). */
+int gdem_set_fluid(gdem_handle h, double fluid_density, int corrected_acceleration);
+
+/* Time step of the next steps (the coupled run's sub-step,
+ * GrainsCoupledWithFluid::Simulation, :123-133). */
+int gdem_set_time_step(gdem_handle h, double dt);
+
+/* TimeStep mindt, maxdt, ndt of a coupled run's XML (a plain run's dt for
+ * both bounds and 1). */
+int gdem_time_step_bounds(gdem_handle h, double* min_dt, double* max_dt, int* ndt);
+
+/* The Construction/Reload Filename attribute ("" without one). */
+int gdem_reload_filename(gdem_handle h, char* buf, int capacity);
+
+/* Class cls (of the first instance): props = mass, density, principal
+ * inertia (3), circumscribed radius, crust thickness; shape 0 sphere, 1 box,
+ * 2 polyhedron, 3 cylinder. */
+int gdem_particle_class(gdem_handle h, int cls, double* props, int* shape);
+
+/* Velocities and space-frame angular velocities from the fluid solver, by
+ * particle ID, 3 each (GrainsCoupledWithFluid::updateParticlesVelocity,
+ * :1126-1180; the body-frame angular velocity follows as q* w q). */
+int gdem_set_velocities(gdem_handle h, const double* v, const double* w);
+
+/* Hydrodynamic force and torque by particle ID (3 each), added to every
+ * particle's force and torque at each step until replaced (the PRSHydroFT
+ * application, GrainsCoupledWithFluid::updateParticlesHydroFT, :1187-1193);
+ * both NULL clears them. */
+int gdem_set_hydro_forces(gdem_handle h, const double* F, const double* T);
+
 /* Advances nsteps kick-drift-kick leapfrog steps of size dt (from the XML).
  * Equivalent to the loop body of Grains::Simulation (Grains.cpp:286-364).
  * Per step: a contact filter over the pair list, the force kernel over the

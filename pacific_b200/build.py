@@ -1,4 +1,5 @@
-"""Builds libgrains_b200.so (sm_100a) in the package directory.
+"""Builds libgrains_b200.so (sm_100a) and the Basilisk coupling library
+libgrains_b200_basilisk.so over it, in the package directory.
 
 Each CUDA translation unit is compiled separately so that the FP64 units can
 be built with -fmad=false (no contraction of a*b+c into FMA, which keeps the
@@ -15,6 +16,8 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 OUT = PKG / "libgrains_b200.so"
+# the Basilisk coupling C ABI (host code over libgrains_b200.so)
+OUT_BASILISK = PKG / "libgrains_b200_basilisk.so"
 BUILD = PKG / "_build"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -64,6 +67,15 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> Path:
         subprocess.run(cmd, check=True)
     if _stale(OUT, objs):
         cmd = [_nvcc(), *ARCH, "-shared", "-o", str(OUT), *map(str, objs), "-lcudart"]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    src = CSRC / "gdem_basilisk.cpp"
+    if _stale(OUT_BASILISK, [src, OUT, *headers]):
+        # the system g++ (shared libstdc++, the one the host process loads)
+        cmd = [os.environ.get("GRAINS_B200_CXX", "g++"), "-std=c++17", "-O2", "-fPIC", "-shared",
+               "-I", str(PKG.parent / "include"), str(src), "-o", str(OUT_BASILISK),
+               "-L", str(PKG), "-l:libgrains_b200.so", "-Wl,-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

@@ -1,0 +1,268 @@
+// gdem_basilisk.cpp -- the Basilisk coupling C ABI of Grains3D
+// (GRAINS_V1/Grains/InterfaceCBasilisk/include/InterfaceGrains3DBasilisk.h,
+// src/InterfaceGrains3DBasilisk.cpp) on the B200 DEM step.  Built as
+// libgrains_b200_basilisk.so over libgrains_b200.so; it exports the same
+// symbols with the same signatures, so a Basilisk DLMFD build links it in
+// place of the reference's interface library.
+//
+// Like the reference (InterfaceGrains3DBasilisk.cpp:15) it keeps one system
+// in a file-static handle, has no error returns (errors are printed and
+// recorded, and later calls then do nothing) and is meant for one process.
+// What each entry does:
+//   Init_Grains       the XML's system (FP64; GRAINS_B200_PRECISION=fp32split
+//                     selects the FP32-split mode) with the particles of its
+//                     Construction/Reload file (the "<stem>_Particles" file of
+//                     the Format2024 reload, AllComponents::read_particles),
+//                     the fluid density in the weight and, with
+//                     b_fluidcorrectedacc, in the coupling factor
+//                     (GrainsCoupledWithFluid::do_before_time_stepping, :54-97).
+//   Simu_Grains       sub-steps over the fluid step as
+//                     GrainsCoupledWithFluid::Simulation (:123-133): ndt from
+//                     the XML's TimeStep, dt = dt_fluid / ndt within
+//                     [mindt, maxdt].
+//   GrainsToBasilisk  the rigid-body stream of GrainsCoupledWithFluid::
+//                     GrainsToFluid (:912-1120), tokens separated by one
+//                     space (InterfaceGrains3DBasilisk.cpp:62-82); spheres
+//                     (a class that is not a sphere is reported as an error:
+//                     its envelope and faces are not written).
+//   UpdateVelocityGrains  velocities from the fluid (updateParticlesVelocity).
+// Contact memory: the reference's coupled step never prunes a contact map
+// entry whose contact has ended (it skips Grains::computeParticlesForceAnd
+// Torque's setContactMapToFalse / updateContactMap), so a pair that touches
+// again resumes an old tangential spring; here an ended contact's memory is
+// dropped, as in the uncoupled step.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/grains_b200.h"
+
+namespace {
+
+gdem_handle g_sys = nullptr;
+bool g_error = false;
+double g_time = 0.;
+int g_cycle = 0;
+int g_ndt = 1;
+double g_min_dt = 0., g_max_dt = 0.;
+int64_t g_n = 0;
+std::vector<int> g_class;      // particle class by particle index
+std::vector<int> g_ids;        // reload IDs by particle index
+
+void fail(const char* where) {
+  std::fprintf(stderr, "Grains3D B200 coupling: %s: %s\n", where, gdem_last_error());
+  g_error = true;
+}
+
+// GrainsExec::doubleToString(ios::scientific, 16, v)
+std::string d16(double v) {
+  if (v == 0.) return std::signbit(v) ? "-0" : "0";
+  char buf[40];
+  std::snprintf(buf, sizeof(buf), "%.16e", v);
+  return buf;
+}
+
+// The reference particle file's IDs (1-based, in particle-index order).
+bool readIds(const std::string& pfile) {
+  FILE* f = std::fopen(pfile.c_str(), "r");
+  if (!f) return false;
+  std::vector<std::pair<int, int>> rec;   // (ID, class)
+  char line[1 << 16];
+  while (std::fgets(line, sizeof(line), f)) {
+    int cls, id, tag;
+    unsigned act;
+    if (std::sscanf(line, "%d %d %d %u", &cls, &id, &tag, &act) != 4) continue;
+    if (tag > 1 || !act) continue;
+    rec.push_back({id, cls});
+  }
+  std::fclose(f);
+  std::sort(rec.begin(), rec.end());
+  g_ids.clear();
+  g_class.clear();
+  for (auto const& r : rec) { g_ids.push_back(r.first); g_class.push_back(r.second); }
+  return true;
+}
+
+// Matrix::setRotation (Geometry/src/Matrix.cpp:114-127) of q = (x, y, z, w):
+// a sphere's orientation, which the reference carries in its transform.
+void rotationOf(const double* q, double* m) {
+  const double x = q[0], y = q[1], z = q[2], w = q[3];
+  const double s = 2.0 / (x * x + y * y + z * z + w * w);
+  const double xs = x * s, ys = y * s, zs = z * s;
+  const double wx = w * xs, wy = w * ys, wz = w * zs;
+  const double xx = x * xs, xy = x * ys, xz = x * zs, yy = y * ys, yz = y * zs, zz = z * zs;
+  const double r[9] = {1.0 - (yy + zz), xy - wz, xz + wy, xy + wz, 1.0 - (xx + zz), yz - wx,
+                       xz - wy, yz + wx, 1.0 - (xx + yy)};
+  for (int k = 0; k < 9; ++k) m[k] = r[k];
+}
+
+// Row-major 3x3 product as Matrix::operator* (Geometry/src/Matrix.cpp).
+void matmul(const double* a, const double* b, double* c) {
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      c[3 * i + j] = a[3 * i] * b[j] + a[3 * i + 1] * b[3 + j] + a[3 * i + 2] * b[6 + j];
+}
+
+}  // namespace
+
+extern "C" {
+
+void Init_Grains(char const* inputfile, double fluid_rho, const bool b_restart,
+                 const bool b_fluidcorrectedacc) {
+  (void)b_restart;   // the particles always come from the XML's reload file
+  if (g_sys) { gdem_destroy(g_sys); g_sys = nullptr; }
+  g_error = false;
+  const char* prec = std::getenv("GRAINS_B200_PRECISION");
+  const int mode = (prec && std::strcmp(prec, "fp32split") == 0) ? GDEM_FP32_SPLIT : GDEM_FP64;
+  if (gdem_create(inputfile, mode, &g_sys) != GDEM_OK) { fail("Init_Grains"); return; }
+  char reload[4096];
+  if (gdem_reload_filename(g_sys, reload, sizeof(reload)) != GDEM_OK) { fail("Init_Grains"); return; }
+  if (!reload[0]) {
+    std::fprintf(stderr, "Grains3D B200 coupling: Init_Grains: the XML has no Construction/Reload"
+                         " file (particle insertion is not part of this library)\n");
+    g_error = true;
+    return;
+  }
+  // AllComponents::read_particles: the reload name up to its first '.',
+  // then "_Particles"
+  std::string pfile(reload);
+  const size_t dot = pfile.find_first_of('.');
+  if (dot != std::string::npos) pfile.erase(dot);
+  pfile += "_Particles";
+  if (gdem_read_reload_particles(g_sys, pfile.c_str()) != GDEM_OK) { fail("Init_Grains"); return; }
+  if (!readIds(pfile)) { fail("Init_Grains"); return; }
+  g_n = gdem_num_particles(g_sys);
+  if (gdem_set_fluid(g_sys, fluid_rho, b_fluidcorrectedacc ? 1 : 0) != GDEM_OK) {
+    fail("Init_Grains");
+    return;
+  }
+  if (gdem_time_step_bounds(g_sys, &g_min_dt, &g_max_dt, &g_ndt) != GDEM_OK) {
+    fail("Init_Grains");
+    return;
+  }
+  std::printf("Construction of Grains completed\n");
+}
+
+void Simu_Grains(const double dt_fluid) {
+  if (!g_sys || g_error) return;
+  // GrainsCoupledWithFluid::Simulation (:127-132)
+  const double dteff = std::max(std::min(g_max_dt, dt_fluid / double(g_ndt)), g_min_dt);
+  g_ndt = (int)(size_t)(dt_fluid / dteff);
+  if (g_ndt < 1) g_ndt = 1;
+  const double dt = dt_fluid / double(g_ndt);
+  if (gdem_set_time_step(g_sys, dt) != GDEM_OK || gdem_step(g_sys, g_ndt) != GDEM_OK) {
+    fail("Simu_Grains");
+    return;
+  }
+  g_time += dt_fluid;
+  int bits = 0;
+  gdem_status(g_sys, &bits, 0);
+  if (bits) {
+    std::fprintf(stderr, "Grains3D B200 coupling: Simu_Grains: simulation status %#x\n", bits);
+    g_error = true;
+  }
+}
+
+char* GrainsToBasilisk(int* pstrsize) {
+  // the stream is built with snprintf: tokens joined by one space, as the
+  // reference's interface re-joins them (InterfaceGrains3DBasilisk.cpp:62-82)
+  std::string out;
+  auto tok = [&](const std::string& t) { out += t; out += ' '; };
+  char buf[64];
+  const int64_t n = g_sys && !g_error ? g_n : 0;
+  std::vector<double> x(3 * n), v(3 * n), w(3 * n), q(4 * n), B(9 * n);
+  if (n) {
+    if (gdem_download_state(g_sys, x.data(), v.data(), w.data(), nullptr, q.data(), nullptr,
+                            nullptr) != GDEM_OK)
+      fail("GrainsToBasilisk");
+    for (int64_t i = 0; i < n; ++i) rotationOf(&q[4 * i], &B[9 * i]);
+  }
+  std::snprintf(buf, sizeof(buf), "%lld", (long long)n);
+  tok(buf);
+  for (int64_t i = 0; i < n && !g_error; ++i) {
+    double props[7];
+    int shape = 0;
+    if (gdem_particle_class(g_sys, g_class[i], props, &shape) != GDEM_OK) { fail("GrainsToBasilisk"); break; }
+    if (shape != 0) {
+      std::fprintf(stderr, "Grains3D B200 coupling: GrainsToBasilisk: only spheres are written\n");
+      g_error = true;
+      break;
+    }
+    const double* mr = &B[9 * i];
+    // Particle::computeInertiaTensorSpaceFixed (Particle.cpp:1797-1821):
+    // Mr (I_body Mr^t), I_body diagonal in the body frame
+    const double ib[9] = {props[2], 0., 0., 0., props[3], 0., 0., 0., props[4]};
+    const double mrt[9] = {mr[0], mr[3], mr[6], mr[1], mr[4], mr[7], mr[2], mr[5], mr[8]};
+    double tmp[9], is[9];
+    matmul(ib, mrt, tmp);
+    matmul(mr, tmp, is);
+    const double inertia[6] = {is[0], is[1], is[2], is[4], is[5], is[8]};
+    // GrainsToFluid (:950-1030): ID - 1, corners (1 for a sphere), "P",
+    // v, w, density, mass, space-fixed inertia, orientation, centre
+    std::snprintf(buf, sizeof(buf), "%d", g_ids[i] - 1);
+    tok(buf);
+    tok("1");
+    tok("P");
+    for (int d = 0; d < 3; ++d) tok(d16(v[3 * i + d]));
+    for (int d = 0; d < 3; ++d) tok(d16(w[3 * i + d]));
+    tok(d16(props[1]));
+    tok(d16(props[0]));
+    for (double c : inertia) tok(d16(c));
+    for (int k = 0; k < 9; ++k) tok(d16(mr[k]));
+    for (int d = 0; d < 3; ++d) tok(d16(x[3 * i + d]));
+    // radius in the stream's default format (%g), then RigidBody::
+    // writePositionInFluid (RigidBody.cpp:445-500): one envelope point (the
+    // centre) and no face
+    std::snprintf(buf, sizeof(buf), "%g", props[5]);
+    tok(buf);
+    tok("1");
+    for (int d = 0; d < 3; ++d) tok(d16(x[3 * i + d]));
+    tok("0");
+  }
+  *pstrsize = (int)out.size() + 1;
+  char* res = new char[*pstrsize];
+  std::memcpy(res, out.c_str(), out.size() + 1);
+  return res;
+}
+
+void SetInitialTime(double tinit) { g_time = tinit; }
+
+void SaveResults_Grains() {
+  // the reference's post-processing writers are not part of this library;
+  // a Format2024 particle file of the current state stands in for them
+  if (!g_sys || g_error) return;
+  char name[64];
+  std::snprintf(name, sizeof(name), "grains_b200_%06d_Particles", g_cycle++);
+  if (gdem_write_reload_particles(g_sys, name) != GDEM_OK) fail("SaveResults_Grains");
+}
+
+void checkParaviewPostProcessing_Grains(char* solid_resDir) { (void)solid_resDir; }
+
+void UpdateVelocityGrains(double** arrayv, const int m) {
+  if (!g_sys || g_error) return;
+  if (m != g_n) {
+    std::fprintf(stderr, "WARNING: numbers of particles in Grains and in the fluid solver are "
+                         "different in UpdateVelocityGrains\n");
+    if (m < g_n) return;
+  }
+  std::vector<double> v(3 * g_n), w(3 * g_n);
+  for (int64_t i = 0; i < g_n; ++i) {
+    // row i belongs to the particle of ID i + 1 (GrainsCoupledWithFluid.cpp:1150)
+    const double* row = arrayv[g_ids[i] - 1];
+    for (int d = 0; d < 3; ++d) { v[3 * i + d] = row[d]; w[3 * i + d] = row[3 + d]; }
+  }
+  if (gdem_set_velocities(g_sys, v.data(), w.data()) != GDEM_OK) fail("UpdateVelocityGrains");
+}
+
+void SetInitialCycleNumber(int cycle0) { g_cycle = cycle0; }
+
+void NumberOfRigidBodiesInBasilisk(size_t* nparticles, size_t* nobstacles) {
+  *nparticles = (size_t)(g_sys && !g_error ? g_n : 0);
+  *nobstacles = 0;   // no obstacle of these XMLs is sent to the fluid
+}
+
+}  // extern "C"

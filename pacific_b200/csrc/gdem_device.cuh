@@ -126,6 +126,7 @@ struct DevState {
   int4* cellc;            // pair-list cell i, j, k and instance at the last rebuild
   // pair list: per-particle segments of kPairCap entries
   int* pairs; int* npairs;   // skin list (rebuilt on demand)
+  double* hydro;          // coupled runs: hydrodynamic force and torque by particle ID (6 each), or null
   int2* upairs;           // compact pair list: (slot, entry) of every upper entry, ctl[kCtlPairs] of them
   // two-phase force path (systems with convex bodies; null otherwise)
   int* kept;              // compact-list indices of the pairs kept by the filter, ctl[kCtlKept]

@@ -76,6 +76,12 @@ struct InstanceDesc {
   ModelDesc models[kMaxMat * kMaxMat];
   double gravity[3];
   double dt;
+  // coupled runs (GrainsCoupledWithFluid::AdditionalFeatures,
+  // Fluid/src/GrainsCoupledWithFluid.cpp:510-530): TimeStep mindt, maxdt,
+  // ndt; a plain run's dt is all three
+  double min_dt, max_dt;
+  int ndt;
+  std::string reload_file;   // Construction/Reload Filename, if any
   int nmat;
   // what the pair-list grid is made from (it is remade when the skin changes)
   double box_org[3], box_max[3];
@@ -334,8 +340,13 @@ InstanceDesc readInstance(std::string const& path) {
     }
     t.mass = density * vol;
     for (int d = 0; d < 3; ++d) t.inertia[d] = Iv[d] * density;
+    t.density = density;
+    t.coupling = 1.;
     t.inv_mass = 1. / t.mass;
-    for (int d = 0; d < 3; ++d) t.inv_inertia[d] = 1. / t.inertia[d];
+    for (int d = 0; d < 3; ++d) {
+      t.inv_inertia[d] = 1. / t.inertia[d];
+      t.inv_inertia_c[d] = t.inv_inertia[d];
+    }
     t.eqrad = std::pow((0.75 / PI) * vol, 1. / 3.);                   // getEquivalentSphereRadius
     // crust shrink factors (RigidBodyWithCrust ctor, RigidBodyWithCrust.cpp:58-78)
     for (int d = 0; d < 3; ++d)
@@ -432,7 +443,15 @@ InstanceDesc readInstance(std::string const& path) {
     }
   XmlNode const* ts = root->find("TimeStep");
   if (!ts) throw std::runtime_error("no <TimeStep>");
-  I.dt = ts->attrD("dt");
+  if (ts->has("dt")) I.dt = ts->attrD("dt");
+  else if (ts->has("mindt")) I.dt = ts->attrD("mindt");   // the coupled run's start
+  else throw std::runtime_error("<TimeStep> needs dt (or mindt, maxdt, ndt)");
+  I.min_dt = ts->has("mindt") ? ts->attrD("mindt") : I.dt;
+  I.max_dt = ts->has("maxdt") ? ts->attrD("maxdt") : I.dt;
+  I.ndt = ts->has("ndt") ? ts->attrI("ndt") : 1;
+  I.reload_file.clear();
+  if (XmlNode const* rl = root->find("Reload"))
+    if (rl->has("Filename")) I.reload_file = rl->attr("Filename");
   for (auto& t : I.types)
     for (int d = 0; d < 3; ++d) t.weight[d] = I.gravity[d] * (t.mass * (1. - 0. / 1.));
   // linked cell grid (LinkedCell::set, Base/src/LinkedCell.cpp:47-160)
@@ -502,6 +521,7 @@ struct System {
   std::vector<InstanceDesc> inst;
   std::vector<std::string> xml_paths;
   std::vector<GridDesc> h_bgrids;  // host copy of the pair-list grids
+  std::vector<TypeDesc> h_types;   // host copy of the particle classes (all instances)
   std::vector<int> h_type, h_inst; // uploaded classes (instance-local) and instances, by ID
   std::vector<int> ref_ids;        // reload particle IDs by particle index (empty: index + 1)
   double tune_skin = -1.;          // skin as a multiple of rmax (< 0: the XML's or 0.25)
@@ -698,6 +718,7 @@ struct System {
     up(d_grids, grids); up(d_types, types); up(d_models, models); up(d_walls, walls);
     up(d_poly, poly); up(d_bgrids, bgrids);
     h_bgrids = bgrids;
+    h_types = types;
     S.grids = d_grids; S.types = d_types; S.models = d_models; S.walls = d_walls;
     S.bgrids = d_bgrids;
     S.poly_verts = d_poly;
@@ -1326,6 +1347,124 @@ int gdem_autotune(gdem_handle h, int trial_steps, double* skin_factor, int* bloc
     if (skin_factor) *skin_factor = best_sf;
     if (blocks_per_sm) *blocks_per_sm = best_bps;
     if (ms_per_step) *ms_per_step = best;
+    return GDEM_OK;
+  });
+}
+
+// ----------------------------------------------------- fluid coupling --
+int gdem_set_fluid(gdem_handle h, double fluid_density, int corrected_acceleration) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s) throw std::runtime_error("invalid handle");
+    if (!(fluid_density >= 0.)) throw std::runtime_error("fluid density must be >= 0");
+    size_t k = 0;
+    for (auto const& I : s->inst)
+      for (size_t c = 0; c < I.types.size(); ++c, ++k) {
+        TypeDesc& t = s->h_types[k];
+        if (!(fluid_density < t.density)) throw std::runtime_error("fluid denser than a particle class");
+        // Particle::computeWeight (Particle.cpp:413-418) and
+        // ParticleKinematics::setCouplingFactor (ParticleKinematics.cpp:483-488)
+        for (int d = 0; d < 3; ++d)
+          t.weight[d] = I.gravity[d] * (t.mass * (1. - fluid_density / t.density));
+        t.coupling = 1.;
+        if (corrected_acceleration) t.coupling -= fluid_density / t.density;
+        t.inv_mass = 1. / (t.mass * t.coupling);
+        for (int d = 0; d < 3; ++d) t.inv_inertia_c[d] = 1. / (t.coupling * t.inertia[d]);
+      }
+    // the kernels read the class table when they run: no graph to recapture
+    CK(cudaMemcpy(s->d_types, s->h_types.data(), s->h_types.size() * sizeof(TypeDesc),
+                  cudaMemcpyHostToDevice));
+    return GDEM_OK;
+  });
+}
+
+int gdem_set_time_step(gdem_handle h, double dt) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !(dt > 0.)) throw std::runtime_error("invalid time step");
+    if (dt != s->S.dt) {
+      s->S.dt = dt;
+      for (auto& I : s->inst) I.dt = dt;
+      s->invalidateGraphs();   // the kernels take dt by value
+    }
+    return GDEM_OK;
+  });
+}
+
+int gdem_time_step_bounds(gdem_handle h, double* min_dt, double* max_dt, int* ndt) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s) throw std::runtime_error("invalid handle");
+    InstanceDesc const& I = s->inst[0];
+    if (min_dt) *min_dt = I.min_dt;
+    if (max_dt) *max_dt = I.max_dt;
+    if (ndt) *ndt = I.ndt;
+    return GDEM_OK;
+  });
+}
+
+int gdem_reload_filename(gdem_handle h, char* buf, int capacity) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !buf || capacity <= 0) throw std::runtime_error("invalid arguments");
+    std::string const& f = s->inst[0].reload_file;
+    if ((int)f.size() >= capacity) throw std::runtime_error("buffer too small");
+    std::memcpy(buf, f.c_str(), f.size() + 1);
+    return GDEM_OK;
+  });
+}
+
+int gdem_particle_class(gdem_handle h, int cls, double* props, int* shape) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || cls < 0 || cls >= (int)s->inst[0].types.size()) throw std::runtime_error("no such class");
+    TypeDesc const& t = s->h_types[cls];
+    if (props) {
+      props[0] = t.mass; props[1] = t.density;
+      props[2] = t.inertia[0]; props[3] = t.inertia[1]; props[4] = t.inertia[2];
+      props[5] = t.radius; props[6] = t.crust;
+    }
+    if (shape) *shape = t.shape;
+    return GDEM_OK;
+  });
+}
+
+int gdem_set_velocities(gdem_handle h, const double* v, const double* w) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state || !v || !w) throw std::runtime_error("invalid arguments");
+    DevState& S = s->S;
+    const size_t n = (size_t)S.n;
+    double* dv = s->d_stage;
+    double* dw = s->d_stage + 3 * n;
+    CK(cudaMemcpyAsync(dv, v, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaMemcpyAsync(dw, w, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    launch_set_velocities(S, dv, dw, s->stream);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(s->stream));
+    return GDEM_OK;
+  });
+}
+
+int gdem_set_hydro_forces(gdem_handle h, const double* F, const double* T) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state) throw std::runtime_error("upload the state first");
+    DevState& S = s->S;
+    const size_t n = (size_t)S.n;
+    if (!F && !T) {
+      if (S.hydro) { CK(cudaMemset(S.hydro, 0, 6 * n * sizeof(double))); }
+      return GDEM_OK;
+    }
+    if (!F || !T) throw std::runtime_error("give both F and T, or neither");
+    if (!S.hydro) {
+      S.hydro = s->alloc<double>(6 * (size_t)S.cap);
+      s->invalidateGraphs();   // the move kernel now adds them
+    }
+    std::vector<double> hv(6 * n);
+    for (size_t i = 0; i < n; ++i)
+      for (int d = 0; d < 3; ++d) { hv[6 * i + d] = F[3 * i + d]; hv[6 * i + 3 + d] = T[3 * i + d]; }
+    CK(cudaMemcpy(S.hydro, hv.data(), hv.size() * sizeof(double), cudaMemcpyHostToDevice));
     return GDEM_OK;
   });
 }

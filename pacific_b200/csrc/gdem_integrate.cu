@@ -276,6 +276,13 @@ __global__ void __launch_bounds__(256, (kFast && kBasis) ? 2 : 3) k_move(DevStat
     F = ld3(S.F, S.cap, t);
     T = ld3(S.T, S.cap, t);
   }
+  if (S.hydro) {
+    // coupled run: the fluid's force and torque, added after the contacts as
+    // the PRSHydroFT application does (it runs after the collision one)
+    const double* hy = S.hydro + 6 * (size_t)S.id[t];
+    F = F + mk(hy[0], hy[1], hy[2]);
+    T = T + mk(hy[3], hy[4], hy[5]);
+  }
   advanceParticle<kFast, kBasis>(S, t, tp, F, T, (flags & kStepClose) != 0, (flags & kStepMove) != 0,
                                  m);
   // the next evaluation's contact flags start clear (no other kernel touches
@@ -537,6 +544,23 @@ __global__ void k_load_state(DevState S, const double* x, const double* v, const
   }
 }
 
+// GrainsCoupledWithFluid::updateParticlesVelocity (Fluid/src/
+// GrainsCoupledWithFluid.cpp:1126-1180): velocities and space-frame angular
+// velocities by particle ID (AoS), the body-frame one rebuilt as q* w q.
+__global__ void k_set_velocities(DevState S, const double* v, const double* w) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= S.n) return;
+  const int cap = S.cap, i = S.id[t];
+  const d3 vi = mk(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+  const d3 wi = mk(w[3 * i], w[3 * i + 1], w[3 * i + 2]);
+  st3(S.v, cap, t, vi);
+  st3(S.w, cap, t, wi);
+  if (S.wbf_state) {
+    const dq qq = qmk(mk(S.q[t], S.q[cap + t], S.q[2 * cap + t]), S.q[3 * cap + t]);
+    st3(S.wbf, cap, t, multToVector3(conj(qq), vecq(wi, qq)));
+  }
+}
+
 // AllComponents::ComputeMaxMeanVelocity (Component/src/AllComponents.cpp:
 // 1781-1811): block partial max and sum of |v|, reduced in a fixed order.
 __global__ void k_vstats_partial(DevState S, double* part) {
@@ -647,6 +671,9 @@ void launch_load_state(DevState const& S, const double* x, const double* v, cons
                        const double* wbf, const double* q, const double* F, const double* T,
                        const int* type_by_id, const int* inst_by_id, cudaStream_t st) {
   if (S.n) k_load_state<<<blocks(S.n, 256), 256, 0, st>>>(S, x, v, w, wbf, q, F, T, type_by_id, inst_by_id);
+}
+void launch_set_velocities(DevState const& S, const double* v, const double* w, cudaStream_t st) {
+  if (S.n) k_set_velocities<<<blocks(S.n, 256), 256, 0, st>>>(S, v, w);
 }
 void launch_vstats(DevState const& S, double* part, double* out, cudaStream_t st) {
   int nb = blocks(S.n, 256);

@@ -60,6 +60,7 @@ void launch_load_state(DevState const& S, const double* x, const double* v, cons
                        const double* wbf, const double* q, const double* F, const double* T,
                        const int* type_by_id, const int* inst_by_id, cudaStream_t st);
 void launch_vstats(DevState const& S, double* part, double* out, cudaStream_t st);
+void launch_set_velocities(DevState const& S, const double* v, const double* w, cudaStream_t st);
 void launch_pair_counts(DevState const& S, unsigned long long* out, cudaStream_t st);
 
 // gdem_contact64.cu (FP64 mode)

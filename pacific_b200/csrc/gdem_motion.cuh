@@ -20,7 +20,7 @@ namespace gdem {
 // Angular acceleration in the body frame; the gyroscopic term for
 // non-spherical classes (predictor mode).
 __device__ __forceinline__ d3 dOmega(TypeDesc const& t, d3 tbf, d3 om) {
-  const double c = 1.;
+  const double c = t.coupling;
   if (t.shape == 0)
     return mk(tbf.x / (c * t.inertia[0]), tbf.y / (c * t.inertia[1]), tbf.z / (c * t.inertia[2]));
   const double* I = t.inertia;
@@ -52,7 +52,7 @@ __device__ __forceinline__ void kick(TypeDesc const& tp, d3 F, d3 T, d3& v, d3& 
                                      dq q, double h) {
   dq pc = conj(q);
   d3 tbf = multToVector3(pc, vecq(T, q));
-  const double c = 1.;
+  const double c = tp.coupling;
   v = v + (F / (tp.mass * c)) * h;
   wbf = rk3(tp, tbf, wbf, h);
   w = multToVector3(q, vecq(wbf, pc));
@@ -99,12 +99,13 @@ __device__ __forceinline__ void wrapToGrid(GridDesc const& g, d3& x, int* wrapd,
 // the results differ from the reference's operation order by a few ulps per
 // step, far below the FP32 force law of this mode.
 __device__ __forceinline__ d3 dOmegaFast(TypeDesc const& t, d3 tbf, d3 om) {
-  const double* iI = t.inv_inertia;
-  if (t.shape == 0) return mk(tbf.x * iI[0], tbf.y * iI[1], tbf.z * iI[2]);
+  const double* iIc = t.inv_inertia_c;
+  if (t.shape == 0) return mk(tbf.x * iIc[0], tbf.y * iIc[1], tbf.z * iIc[2]);
   const double* I = t.inertia;
-  return mk((tbf.x + om.y * om.z * (I[1] - I[2])) * iI[0],
-            (tbf.y + om.z * om.x * (I[2] - I[0])) * iI[1],
-            (tbf.z + om.x * om.y * (I[0] - I[1])) * iI[2]);
+  const double* iI = t.inv_inertia;
+  return mk(tbf.x * iIc[0] + om.y * om.z * (I[1] - I[2]) * iI[0],
+            tbf.y * iIc[1] + om.z * om.x * (I[2] - I[0]) * iI[1],
+            tbf.z * iIc[2] + om.x * om.y * (I[0] - I[1]) * iI[2]);
 }
 __device__ __forceinline__ d3 rk3Fast(TypeDesc const& t, d3 tbf, d3 wbf, double h) {
   if (t.shape == 0) return wbf + dOmegaFast(t, tbf, wbf) * h;
@@ -142,7 +143,7 @@ __device__ __forceinline__ void sinCosSmall(double a, double* s, double* c) {
 __device__ __forceinline__ void leapfrogSphere(TypeDesc const& tp, d3 F, d3 T, bool close,
                                                double hc, bool move, double h, double dt,
                                                d3& x, d3& v, d3& w, dq& q, d3& dx, int* status) {
-  const double iI = tp.inv_inertia[0];
+  const double iI = tp.inv_inertia_c[0];
   if (close) {
     v = v + F * (hc * tp.inv_mass);
     w = w + T * (hc * iI);
@@ -183,7 +184,7 @@ __device__ __forceinline__ void leapfrog(TypeDesc const& tp, d3 F, d3 T, bool cl
   if (!move) return;
   dq pc = conj(q);
   d3 tbf = multToVector3(pc, vecq(T, q));
-  const double c = 1.;
+  const double c = tp.coupling;
   if (kFast) {
     v = v + F * (h * tp.inv_mass);
     wbf = rk3Fast(tp, tbf, wbf, h);

@@ -78,8 +78,14 @@ struct TypeDesc {
   double scaling[3];     // crust shrink factors (extent - crust) / extent
   int poly_begin;        // first vertex of a polyhedron in the vertex table
   int poly_count;        // its vertex count
-  double inv_mass;       // 1 / mass and 1 / inertia (FP32-split leapfrog)
+  double inv_mass;       // 1 / (mass c) and 1 / inertia (FP32-split leapfrog)
   double inv_inertia[3];
+  double density;
+  // coupling factor c (ParticleKinematics::setCouplingFactor,
+  // ParticleKinematics.cpp:483-488): 1 - rho_f / rho in a coupled run with
+  // fluid-corrected acceleration, else 1; the kicks divide by m c and c I
+  double coupling;
+  double inv_inertia_c[3];   // 1 / (c inertia) (FP32-split leapfrog)
 };
 
 // HookeMemory / Hooke parameters (HookeMemoryContactForceModel.cpp:12-27).

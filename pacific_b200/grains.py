@@ -79,6 +79,10 @@ def library() -> ctypes.CDLL:
         "gdem_upload_history": ([_P, i64, _IP, _IP, _DP, _DP, _DP], ctypes.c_int),
         "gdem_write_reload_particles": ([_P, ctypes.c_char_p], ctypes.c_int),
         "gdem_read_reload_particles": ([_P, ctypes.c_char_p], ctypes.c_int),
+        "gdem_set_fluid": ([_P, ctypes.c_double, ctypes.c_int], ctypes.c_int),
+        "gdem_set_time_step": ([_P, ctypes.c_double], ctypes.c_int),
+        "gdem_set_velocities": ([_P, _DP, _DP], ctypes.c_int),
+        "gdem_set_hydro_forces": ([_P, _DP, _DP], ctypes.c_int),
         "gdem_init": ([_P], ctypes.c_int),
         "gdem_set_tuning": ([_P, ctypes.c_double, ctypes.c_int], ctypes.c_int),
         "gdem_autotune": ([_P, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
@@ -184,6 +188,31 @@ class Grains:
                                                  _dp(arrs[1]), _dp(arrs[2]), _dp(arrs[3]),
                                                  _dp(arrs[4])))
         self.n = n
+
+    # ---- fluid coupling (GrainsCoupledWithFluid) ----
+    def set_fluid(self, fluid_density, corrected_acceleration=True):
+        """Buoyant weight m (1 - rho_f / rho) g and, with corrected
+        acceleration, the coupling factor c = 1 - rho_f / rho of the kicks."""
+        self._check(library().gdem_set_fluid(self._h, float(fluid_density),
+                                             1 if corrected_acceleration else 0))
+
+    def set_time_step(self, dt):
+        self._check(library().gdem_set_time_step(self._h, float(dt)))
+
+    def set_velocities(self, v, w):
+        """Velocities and space-frame angular velocities from the fluid, by ID."""
+        v = _f64(v, (self.n, 3))
+        w = _f64(w, (self.n, 3))
+        self._check(library().gdem_set_velocities(self._h, _dp(v), _dp(w)))
+
+    def set_hydro_forces(self, F=None, T=None):
+        """Hydrodynamic force and torque by ID, added at every step (None: clear)."""
+        if F is None and T is None:
+            self._check(library().gdem_set_hydro_forces(self._h, None, None))
+            return
+        F = _f64(F, (self.n, 3))
+        T = _f64(T, (self.n, 3))
+        self._check(library().gdem_set_hydro_forces(self._h, _dp(F), _dp(T)))
 
     def read_reload_particles(self, path):
         """Loads a Format2024 reload particle file (state, forces, contact

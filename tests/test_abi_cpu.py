@@ -42,3 +42,23 @@ def test_bad_xml_is_rejected_before_device(lib, tmp_path):
     p.write_text("<Grains3D><Construction><LinkedCell MX='1'/></Construction>")
     with pytest.raises(GrainsError):
         Grains(p)
+
+
+# InterfaceGrains3DBasilisk.h (GRAINS_V1/Grains/InterfaceCBasilisk/include)
+BASILISK_SYMBOLS = ("Init_Grains", "Simu_Grains", "GrainsToBasilisk", "SetInitialTime",
+                    "SaveResults_Grains", "checkParaviewPostProcessing_Grains",
+                    "UpdateVelocityGrains", "SetInitialCycleNumber",
+                    "NumberOfRigidBodiesInBasilisk")
+
+
+def test_basilisk_library_exports_the_coupling_abi(lib):
+    """libgrains_b200_basilisk.so loads over libgrains_b200.so and exports the
+    reference's Basilisk coupling entry points, so a DLMFD build can link it
+    in place of the reference's interface library."""
+    b = ctypes.CDLL(str(ROOT / "pacific_b200" / "libgrains_b200_basilisk.so"))
+    for name in BASILISK_SYMBOLS:
+        assert hasattr(b, name), name
+    # with no system, the rigid-body count is zero (no crash without a device)
+    n, m = ctypes.c_size_t(7), ctypes.c_size_t(7)
+    b.NumberOfRigidBodiesInBasilisk(ctypes.byref(n), ctypes.byref(m))
+    assert n.value == 0 and m.value == 0

@@ -1,0 +1,149 @@
+"""Fluid coupling: gdem_set_fluid / set_time_step / set_velocities /
+set_hydro_forces and the Basilisk C ABI of libgrains_b200_basilisk.so
+(InterfaceGrains3DBasilisk.h: Init_Grains, Simu_Grains, GrainsToBasilisk,
+UpdateVelocityGrains, NumberOfRigidBodiesInBasilisk, ...).
+
+* Buoyancy and the coupling factor: a free sphere in a fluid of density
+  rho_f falls at g (1 - rho_f / rho) without the corrected acceleration and
+  at g with it (the reference divides the buoyant weight by m c,
+  c = 1 - rho_f / rho).
+* Simu_Grains(dt_fluid) sub-steps as GrainsCoupledWithFluid::Simulation:
+  the same state as gdem_step with dt = dt_fluid / ndt, byte for byte.
+* GrainsToBasilisk writes the GrainsToFluid stream of the state: count,
+  then per sphere its ID - 1, velocities, density, mass, space-fixed inertia,
+  orientation, centre, radius and envelope point.
+* UpdateVelocityGrains and hydrodynamic forces act on the next step.
+"""
+import ctypes
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from pacific_b200 import FP64, Grains, scenarios
+
+pytestmark = pytest.mark.gpu
+
+BASILISK = Path(__file__).resolve().parent.parent / "pacific_b200" / "libgrains_b200_basilisk.so"
+
+
+def _coupled_xml(sc, reload_name, mindt=1e-5, maxdt=2e-5, ndt=4):
+    text = sc.xml()
+    text = text.replace('<TimeStep dt="1e-05"/>',
+                        f'<TimeStep mindt="{mindt}" maxdt="{maxdt}" ndt="{ndt}"/>')
+    text = text.replace("  </Construction>",
+                        f'    <Reload Type="new" Filename="{reload_name}"/>\n  </Construction>')
+    return text
+
+
+def _free_sphere(tmp_path):
+    sc = scenarios.settling_box(n=1, seed=3, vmax=0.0)
+    sc.x[:] = [0.015, 0.015, 0.03]
+    return sc, str(sc.write_xml(tmp_path / "one.xml"))
+
+
+@pytest.mark.parametrize("corrected", [0, 1])
+def test_buoyant_free_fall(tmp_path, lib, corrected):
+    sc, xml = _free_sphere(tmp_path)
+    g = Grains(xml, FP64)
+    g.upload_state(sc.type, sc.x, sc.v, sc.w, sc.q)
+    g.set_fluid(1000.0, corrected)
+    g.do_before_time_stepping()
+    g.step(100)
+    s = g.download_state()
+    t = 100 * 1e-5
+    a = 9.81 * (1.0 if corrected else 1.0 - 1000.0 / 2500.0)
+    assert abs(s["v"][0, 2] + a * t) <= 1e-12
+    g.close()
+
+
+def _settled(tmp_path, n=200, steps=300):
+    sc = scenarios.settling_box(n=n, seed=31)
+    g = Grains(str(sc.write_xml(tmp_path / "plain.xml")), FP64)
+    g.upload_state(sc.type, sc.x, sc.v, sc.w, sc.q)
+    g.do_before_time_stepping()
+    g.step(steps)
+    g.write_reload_particles(tmp_path / "res_Particles")
+    g.close()
+    (tmp_path / "coupled.xml").write_text(_coupled_xml(sc, str(tmp_path / "res.resA")))
+    return sc
+
+
+def _basilisk():
+    b = ctypes.CDLL(str(BASILISK))
+    b.Init_Grains.argtypes = [ctypes.c_char_p, ctypes.c_double, ctypes.c_bool, ctypes.c_bool]
+    b.Simu_Grains.argtypes = [ctypes.c_double]
+    b.GrainsToBasilisk.argtypes = [ctypes.POINTER(ctypes.c_int)]
+    b.GrainsToBasilisk.restype = ctypes.c_void_p
+    b.UpdateVelocityGrains.argtypes = [ctypes.POINTER(ctypes.POINTER(ctypes.c_double)), ctypes.c_int]
+    b.NumberOfRigidBodiesInBasilisk.argtypes = [ctypes.POINTER(ctypes.c_size_t)] * 2
+    return b
+
+
+def test_basilisk_abi(tmp_path, lib):
+    sc = _settled(tmp_path)
+    b = _basilisk()
+    b.Init_Grains(str(tmp_path / "coupled.xml").encode(), 1000.0, False, True)
+    npart, nobs = ctypes.c_size_t(0), ctypes.c_size_t(0)
+    b.NumberOfRigidBodiesInBasilisk(ctypes.byref(npart), ctypes.byref(nobs))
+    assert npart.value == sc.n and nobs.value == 0
+    # a reference run through the plain ABI: same file, same fluid, ndt = 4
+    # sub-steps of dt_fluid / 4 (dt_fluid / ndt = 1e-5 lies in [mindt, maxdt])
+    ref = Grains(str(tmp_path / "coupled.xml"), FP64)
+    ref.read_reload_particles(tmp_path / "res_Particles")
+    ref.set_fluid(1000.0, True)
+    ref.set_time_step(4e-5 / 4)
+    b.Simu_Grains(4e-5)
+    ref.step(4)
+    size = ctypes.c_int(0)
+    ptr = b.GrainsToBasilisk(ctypes.byref(size))
+    text = ctypes.string_at(ptr).decode()
+    tok = text.split()
+    s = ref.download_state()
+    assert int(tok[0]) == sc.n
+    # per sphere: id ncorners, P v(3) w(3) density mass inertia(6) basis(9)
+    # centre(3), radius npoints, point(3), nfaces
+    k = 1
+    for i in range(sc.n):
+        assert int(tok[k]) == i and int(tok[k + 1]) == 1 and tok[k + 2] == "P"
+        vals = np.array(tok[k + 3:k + 3 + 26], dtype=float)
+        assert np.array_equal(vals[0:3], s["v"][i]) and np.array_equal(vals[3:6], s["w"][i])
+        assert vals[6] == 2500.0
+        assert np.array_equal(vals[23:26], s["x"][i])
+        k += 3 + 26
+        assert float(tok[k]) == 0.001 and int(tok[k + 1]) == 1
+        assert np.array_equal(np.array(tok[k + 2:k + 5], dtype=float), s["x"][i])
+        assert tok[k + 5] == "0"
+        k += 6
+    assert k == len(tok)
+    # velocities from the fluid act on the next sub-steps
+    rows = np.zeros((sc.n, 6))
+    rows[:, 2] = -0.05
+    arr = (ctypes.POINTER(ctypes.c_double) * sc.n)(
+        *[rows[i].ctypes.data_as(ctypes.POINTER(ctypes.c_double)) for i in range(sc.n)])
+    b.UpdateVelocityGrains(arr, sc.n)
+    ref.set_velocities(rows[:, :3], rows[:, 3:])
+    b.Simu_Grains(4e-5)
+    ref.step(4)
+    ptr = b.GrainsToBasilisk(ctypes.byref(size))
+    tok = ctypes.string_at(ptr).decode().split()
+    s = ref.download_state()
+    for i in range(sc.n):
+        k = 1 + i * 35
+        assert np.array_equal(np.array(tok[k + 3:k + 6], dtype=float), s["v"][i])
+    ref.close()
+
+
+def test_hydro_forces(tmp_path, lib):
+    sc, xml = _free_sphere(tmp_path)
+    g = Grains(xml, FP64)
+    g.upload_state(sc.type, sc.x, sc.v, sc.w, sc.q)
+    g.do_before_time_stepping()
+    m = 2500.0 * 4.0 / 3.0 * np.pi * 1e-9
+    F = np.array([[0.0, 0.0, m * 9.81]])   # cancels gravity
+    T = np.zeros((1, 3))
+    g.set_hydro_forces(F, T)
+    g.step(50)
+    s = g.download_state()
+    assert abs(s["v"][0, 2]) <= 1e-12
+    g.close()
