@@ -363,7 +363,7 @@ def batched_measure(n_inst, steps, warmup=3):
             "status": st, "workload": "batched_boxes (seeded), FP32-split, device time"}
 
 
-def convex_measure(n, steps, warmup=3):
+def convex_measure(n, steps, warmup=3, graphs=True):
     """Cubes (2 mm) and regular tetrahedra (3 mm edge) poured into a
     0.1 x 0.1 x 0.3 m box (GJK narrow phase, 3D rotation).  Two starts: the
     pour as specified (at rest on the lattice: no contact for the first ~9,800
@@ -380,6 +380,7 @@ def convex_measure(n, steps, warmup=3):
             row = {}
             for name, prec in (("fp64", FP64), ("fp32_split", FP32_SPLIT)):
                 g = Grains(xml, prec)
+                g.use_graphs(graphs)
                 g.upload_state(sc.type, sc.x, sc.v, sc.w, sc.q)
                 g.do_before_time_stepping()
                 g.step(warmup)
@@ -630,7 +631,8 @@ def main():
         if args.batched_instances > 0:
             line["batched"] = batched_measure(args.batched_instances, args.batched_steps)
         if args.convex_n > 0:
-            line["convex"] = convex_measure(args.convex_n, args.convex_steps)
+            line["convex"] = convex_measure(args.convex_n, args.convex_steps,
+                                            graphs=not args.no_graphs)
         if args.adjoint_n > 0:
             line["adjoint"] = adjoint_measure(args.adjoint_n, args.adjoint_steps, 50)
         if not args.no_cpu_baseline:
