@@ -241,6 +241,42 @@ int gdem_set_diagnostics(gdem_handle h, int on);
 int gdem_download_contacts(gdem_handle h, int64_t capacity, int64_t* count, int* id0,
                            int* id1, double* delta, double* force);
 
+/* Coordination number of every particle, by ID: the partners and walls it
+ * touched (negative overlap) in the last force evaluation, counted on the
+ * device from that evaluation's diagnostics records (Particle::
+ * getCoordinationNumber, Component/src/Particle.cpp:1398-1401, set by
+ * addContactingComponentID, :1702-1706).  All zero before the first
+ * evaluation after a state upload; an error when the last evaluation ran
+ * without diagnostics.  gdem_download_classes gives each particle's class
+ * (Particle::getGeometricType, Particle.cpp:1651-1654). */
+int gdem_download_coordination(gdem_handle h, int* coord);
+int gdem_download_classes(gdem_handle h, int* cls);
+
+/* RawData post-processing output of a system
+ * (PostProcessing/src/RawDataPostProcessingWriter.cpp): per output time, a
+ * line (text) or record (binary) in <root>_position_{x,y,z}.dat,
+ * _translational_velocity_{x,y,z}.dat, _angular_velocity_{x,y,z}.dat and
+ * _coordinationNumber.dat, and <root>_particleType.dat rewritten, particle
+ * ID i in column i + 1 (reference IDs 1..n).  gdem_rawdata_start opens the
+ * files (append = 0 truncates them, as a "new" run; 1 appends, as a reload
+ * of type "same") and writes the first output time (PostProcessing_start,
+ * :55-78); gdem_rawdata_write adds one (one_output_Standard, :374-600);
+ * gdem_rawdata_end closes them (PostProcessing_end, :123-141).  The
+ * coordination numbers are gdem_download_coordination's, so the step before
+ * an output time runs with diagnostics on (a start before gdem_init writes
+ * zeros, as the reference's PostProcessing_start does).  The reference's
+ * file quirks are kept: the coordination file carries no time in text mode,
+ * and in binary mode _angular_velocity_z.dat receives the time twice. */
+int gdem_rawdata_start(gdem_handle h, const char* root, int binary, int append, double time);
+int gdem_rawdata_write(gdem_handle h, double time);
+int gdem_rawdata_end(gdem_handle h);
+
+/* One line "time<TAB>vmax<TAB>vmean" of <root>_VelocityMaxMean.dat
+ * (Grains::Simulation, Base/src/Grains.cpp:401-408), from the device
+ * reduction of gdem_velocity_stats; append = 0 truncates the file first
+ * (Grains::do_before_time_stepping opens it anew, Grains.cpp:137-145). */
+int gdem_write_velocity_max_mean(gdem_handle h, const char* path, int append, double time);
+
 /* OR of the status bits raised since creation (or the last reset). */
 int gdem_status(gdem_handle h, int* bits, int reset);
 

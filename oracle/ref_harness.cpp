@@ -28,6 +28,7 @@
 #include "LinkedCell.hh"
 #include "Obstacle.hh"
 #include "Particle.hh"
+#include "RawDataPostProcessingWriter.hh"
 #include "ReaderXML.hh"
 #include "SimpleObstacle.hh"
 
@@ -127,6 +128,18 @@ class RefGrains : public Grains {
       if (it != id_to_index.end()) out[it->second] = p;
     }
     return out;
+  }
+
+  void addRawData(PostProcessingWriter* w) { m_allcomponents.addPostProcessingWriter(w); }
+  void postProcessing(double time, bool start) {
+    if (start)
+      m_allcomponents.PostProcessing_start(time, m_dt, m_collision, m_insertion_windows);
+    else
+      m_allcomponents.PostProcessing(time, m_dt, m_collision, m_insertion_windows);
+  }
+  void postProcessingEnd() { m_allcomponents.PostProcessing_end(); }
+  void maxMeanVelocity(double& vmax, double& vmean) {
+    m_allcomponents.ComputeMaxMeanVelocity(vmax, vmean, nullptr);
   }
 
   int partnerIndex(int id) {
@@ -251,6 +264,36 @@ int ref_write_particles(void* h, const char* path) {
   for (Particle* p : g->masters())
     if (p) p->write2014(out);
   return out ? 0 : 1;
+}
+
+// RawData output of the reference's own RawDataPostProcessingWriter
+// (PostProcessing/src/RawDataPostProcessingWriter.cpp), registered as the
+// one post-processing writer and driven as Grains::do_before_time_stepping
+// (PostProcessing_start, Grains.cpp:131-132), Grains::Simulation
+// (PostProcessing, Grains.cpp:417-418) and Grains::do_after_time_stepping
+// (PostProcessing_end) drive it.  writer_xml holds one <RawData Name=...
+// WritingMode=.../> element.  The reload type is set to "same" so that the
+// writer appends to (creates) its files instead of running the reference's
+// clearing script.
+int ref_rawdata_start(void* h, const char* writer_xml, double time) {
+  RefGrains* g = static_cast<RefGrains*>(h);
+  DOMElement* node = ReaderXML::getRoot(writer_xml);
+  if (!node) return 1;
+  GrainsExec::m_ReloadType = "same";
+  g->addRawData(new RawDataPostProcessingWriter(node, 0, 1, false));
+  g->postProcessing(time, true);
+  return 0;
+}
+int ref_rawdata_write(void* h, double time) {
+  static_cast<RefGrains*>(h)->postProcessing(time, false);
+  return 0;
+}
+void ref_rawdata_end(void* h) { static_cast<RefGrains*>(h)->postProcessingEnd(); }
+
+// AllComponents::ComputeMaxMeanVelocity (Component/src/AllComponents.cpp:1781-1821),
+// the figures of the _VelocityMaxMean.dat lines.
+void ref_velocity_max_mean(void* h, double* vmax, double* vmean) {
+  static_cast<RefGrains*>(h)->maxMeanVelocity(*vmax, *vmean);
 }
 
 void ref_destroy(void* h) { delete static_cast<RefGrains*>(h); }

@@ -50,6 +50,12 @@ def _load():
         lib.ref_get_history.argtypes = [V, I, I, D, D, D]
         lib.ref_write_particles.argtypes = [V, ctypes.c_char_p]
         lib.ref_write_particles.restype = ctypes.c_int
+        lib.ref_rawdata_start.argtypes = [V, ctypes.c_char_p, ctypes.c_double]
+        lib.ref_rawdata_start.restype = ctypes.c_int
+        lib.ref_rawdata_write.argtypes = [V, ctypes.c_double]
+        lib.ref_rawdata_write.restype = ctypes.c_int
+        lib.ref_rawdata_end.argtypes = [V]
+        lib.ref_velocity_max_mean.argtypes = [V, D, D]
         lib.ref_destroy.argtypes = [V]
         _lib = lib
     return _lib
@@ -108,6 +114,26 @@ class Reference:
     def write_particles(self, path):
         """The particle file of a Format2024 reload, by Particle::write2014."""
         return _load().ref_write_particles(self._h, os.fsencode(str(path)))
+
+    def rawdata_start(self, root, binary, time):
+        """Registers the reference's RawDataPostProcessingWriter with output
+        root `root` and writes its first output time (PostProcessing_start)."""
+        root = Path(root)
+        spec = root.parent / (root.name + "_writer.xml")
+        mode = "Binary" if binary else "Text"
+        spec.write_text(f'<RawData Name="{root}" WritingMode="{mode}"/>\n')
+        return _load().ref_rawdata_start(self._h, os.fsencode(str(spec)), time)
+
+    def rawdata_write(self, time):
+        return _load().ref_rawdata_write(self._h, time)
+
+    def rawdata_end(self):
+        _load().ref_rawdata_end(self._h)
+
+    def velocity_max_mean(self):
+        a, b = np.zeros(1), np.zeros(1)
+        _load().ref_velocity_max_mean(self._h, _dp(a), _dp(b))
+        return float(a[0]), float(b[0])
 
     def history(self):
         lib = _load()

@@ -33,6 +33,7 @@ UNITS = [
     ("gdem_noalloc.cu", ["-fmad=false"]),
     ("gdem_adjoint.cu", ["-fmad=false"]),
     ("xml_reader.cpp", []),
+    ("gdem_rawdata.cpp", []),
 ]
 
 

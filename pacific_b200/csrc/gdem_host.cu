@@ -537,6 +537,9 @@ struct System {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool have_state = false, started = false, diag = false, use_graphs = true;
+  // the last force evaluation: 0 none since the state was set, 1 recorded by
+  // the diagnostics, 2 run without them
+  int evaluated = 0;
   bool id_order = false;           // state arrays are in particle-ID order (not yet binned)
   double last_ms = 0.;
   int status_host = 0;
@@ -948,6 +951,7 @@ struct System {
     invalidateGraphs();
     collectTimes();
     started = true;
+    evaluated = diag ? 1 : 2;
   }
   // nsteps leapfrog steps: the opening kick and drift of the first (with the
   // stored forces), then per step a force evaluation followed by the closing
@@ -976,6 +980,7 @@ struct System {
     CK(cudaEventElapsedTime(&ms, ev0, ev1));
     last_ms = ms;
     collectTimes();
+    evaluated = diag ? 1 : 2;
   }
   int readStatus() {
     int st = 0;
@@ -1084,6 +1089,7 @@ int gdem_upload_state(gdem_handle h, int64_t n, const int* inst, const int* type
     (void)S;
     s->loadState(x, v, w, wbf, q, nullptr, nullptr);
     s->have_state = true;
+    s->evaluated = 0;
     return GDEM_OK;
   });
 }
@@ -1849,6 +1855,38 @@ int gdem_download_contacts(gdem_handle h, int64_t capacity, int64_t* count, int*
   });
 }
 
+int gdem_download_coordination(gdem_handle h, int* coord) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state || !coord) throw std::runtime_error("invalid arguments");
+    DevState& S = s->S;
+    const size_t n = (size_t)S.n;
+    if (s->evaluated == 0) {
+      // no force evaluation since the state was set: the reference's
+      // particles enter with none (Particle::InitializeForce)
+      std::fill(coord, coord + n, 0);
+      return GDEM_OK;
+    }
+    if (s->evaluated != 1 || !S.pair_delta)
+      throw std::runtime_error("the last force evaluation ran without diagnostics");
+    int* d = reinterpret_cast<int*>(s->d_stage);
+    launch_coordination_by_id(S, d, 0, s->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(coord, d, n * sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return GDEM_OK;
+  });
+}
+
+int gdem_download_classes(gdem_handle h, int* cls) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state || !cls) throw std::runtime_error("invalid arguments");
+    std::copy(s->h_type.begin(), s->h_type.end(), cls);
+    return GDEM_OK;
+  });
+}
+
 int gdem_status(gdem_handle h, int* bits, int reset) {
   return guarded([&] {
     System* s = sys(h);
@@ -1897,6 +1935,10 @@ int gdem_use_graphs(gdem_handle h, int on) {
   });
 }
 
-void gdem_destroy(gdem_handle h) { delete sys(h); }
+void gdem_destroy(gdem_handle h) {
+  if (!h) return;
+  gdem_rawdata_end(h);   // closes the system's RawData files, if open
+  delete sys(h);
+}
 
 }  // extern "C"

@@ -481,6 +481,29 @@ __global__ void k_cells_by_id(DevState S, int* ijk, int id_base) {
   for (int d = 0; d < 3; ++d) ijk[3 * i + d] = (int)floor((xs[d] - g.lc_origin[d]) / g.edge[d]);
 }
 
+// Coordination number of each particle at the last force evaluation, by ID:
+// the listed partners and the walls whose overlap recorded by that
+// evaluation is negative.  The reference counts the distinct components a
+// particle touched in its force computation (Particle::
+// addContactingComponentID, Component/src/Particle.cpp:1702-1706, called by
+// Particle::InterAction and SimpleObstacle::InterAction for each contact of
+// negative overlap, Particle.cpp:530-543, SimpleObstacle.cpp:262-270); the
+// pair list holds each partner once and each wall has one slot.
+__global__ void k_coordination_by_id(DevState S, int* out, int id_base) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= S.n) return;
+  int i = S.id[t] - id_base;
+  if (i < 0 || i >= S.n) return;
+  const int np = min(S.npairs[t], kPairCap);
+  const double* pd = S.pair_delta + (size_t)t * kPairCap;
+  int c = 0;
+  for (int e = 0; e < np; ++e) c += pd[e] < 0. ? 1 : 0;
+  const int nw = S.grids[S.inst[t]].wall_count;
+  const double* wd = S.wall_delta + (size_t)t * S.max_walls;
+  for (int k = 0; k < nw; ++k) c += wd[k] < 0. ? 1 : 0;
+  out[i] = c;
+}
+
 // Zeroes the cumulative tangential and rolling memories of every entry of
 // the given evaluation (Component::setContactMapCumulativeFeaturesToZero,
 // Component.cpp:842-851).
@@ -689,6 +712,9 @@ void launch_basis_by_id(DevState const& S, double* out, int id_base, cudaStream_
 }
 void launch_cells_by_id(DevState const& S, int* ijk, int id_base, cudaStream_t st) {
   if (S.n) k_cells_by_id<<<blocks(S.n, 256), 256, 0, st>>>(S, ijk, id_base);
+}
+void launch_coordination_by_id(DevState const& S, int* out, int id_base, cudaStream_t st) {
+  if (S.n) k_coordination_by_id<<<blocks(S.n, 256), 256, 0, st>>>(S, out, id_base);
 }
 void launch_hist_zero_cumulative(HistTable const& t, const int* ctl, int fp64, cudaStream_t st) {
   int cap = 1 << t.log2cap;

@@ -55,6 +55,8 @@ void launch_scatter_by_id(DevState const& S, double* x, double* v, double* w, do
                           double* q, double* F, double* T, int id_base, cudaStream_t st);
 void launch_basis_by_id(DevState const& S, double* out, int id_base, cudaStream_t st);
 void launch_cells_by_id(DevState const& S, int* ijk, int id_base, cudaStream_t st);
+// needs the diagnostics records (pair_delta, wall_delta) of the last evaluation
+void launch_coordination_by_id(DevState const& S, int* out, int id_base, cudaStream_t st);
 void launch_hist_zero_cumulative(HistTable const& t, const int* ctl, int fp64, cudaStream_t st);
 void launch_load_state(DevState const& S, const double* x, const double* v, const double* w,
                        const double* wbf, const double* q, const double* F, const double* T,

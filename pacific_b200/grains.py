@@ -91,6 +91,14 @@ def library() -> ctypes.CDLL:
         "gdem_step": ([_P, ctypes.c_int], ctypes.c_int),
         "gdem_download_state": ([_P, _DP, _DP, _DP, _DP, _DP, _DP, _DP], ctypes.c_int),
         "gdem_download_cells": ([_P, _IP], ctypes.c_int),
+        "gdem_download_coordination": ([_P, _IP], ctypes.c_int),
+        "gdem_download_classes": ([_P, _IP], ctypes.c_int),
+        "gdem_rawdata_start": ([_P, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double],
+                               ctypes.c_int),
+        "gdem_rawdata_write": ([_P, ctypes.c_double], ctypes.c_int),
+        "gdem_rawdata_end": ([_P], ctypes.c_int),
+        "gdem_write_velocity_max_mean": ([_P, ctypes.c_char_p, ctypes.c_int, ctypes.c_double],
+                                         ctypes.c_int),
         "gdem_upload_basis": ([_P, _DP], ctypes.c_int),
         "gdem_download_basis": ([_P, _DP], ctypes.c_int),
         "gdem_set_diagnostics": ([_P, ctypes.c_int], ctypes.c_int),
@@ -265,6 +273,35 @@ class Grains:
         b = ctypes.c_double(0.0)
         self._check(library().gdem_velocity_stats(self._h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+    def download_coordination(self):
+        """Coordination number of each particle at the last force evaluation
+        (which must have run with diagnostics on), by particle ID."""
+        c = np.empty(self.n, np.int32)
+        self._check(library().gdem_download_coordination(self._h, _ip(c)))
+        return c
+
+    def download_classes(self):
+        c = np.empty(self.n, np.int32)
+        self._check(library().gdem_download_classes(self._h, _ip(c)))
+        return c
+
+    def rawdata_start(self, root, binary=False, append=False, time=0.0):
+        """Opens the RawData post-processing files <root>_*.dat and writes
+        the first output time."""
+        self._check(library().gdem_rawdata_start(self._h, os.fsencode(str(root)), int(binary),
+                                                 int(append), float(time)))
+
+    def rawdata_write(self, time):
+        self._check(library().gdem_rawdata_write(self._h, float(time)))
+
+    def rawdata_end(self):
+        self._check(library().gdem_rawdata_end(self._h))
+
+    def write_velocity_max_mean(self, path, time, append=True):
+        """Appends (or, append=False, starts) a line of <root>_VelocityMaxMean.dat."""
+        self._check(library().gdem_write_velocity_max_mean(self._h, os.fsencode(str(path)),
+                                                           int(append), float(time)))
 
     def pair_counts(self):
         """(directed pair-list entries, live contact-memory entries) of the

@@ -157,6 +157,59 @@ def run_reload():
     print("wrote reload_settling.npz (200 particles, particle file after 600 steps)")
 
 
+RAW_SUFFIXES = ("position_x", "position_y", "position_z", "translational_velocity_x",
+                "translational_velocity_y", "translational_velocity_z", "angular_velocity_x",
+                "angular_velocity_y", "angular_velocity_z", "coordinationNumber", "particleType")
+RAW_SETTLE = 6000
+RAW_MARKS = (0, 10, 100)
+
+
+def run_rawdata(mode):
+    """The RawData fixtures: 200 spheres settling in the walled box, stepped
+    6,000 times by the reference, which writes the particle file of a
+    Format2024 reload there; then the reference's own
+    RawDataPostProcessingWriter (text or binary) is started at that time and
+    written after 10 and 100 more steps, with the reference's velocity
+    max/mean (the _VelocityMaxMean.dat figures) at each output time.  A run
+    reloaded from the file starts its writer before any force evaluation,
+    so its first coordination numbers are zero; the ones stored here for
+    that time are the reference's from step 6,000."""
+    binary = mode == "binary"
+    sc = scenarios.settling_box(n=200, seed=29)
+    dt = 1e-5
+    out = {"xml": np.array(sc.xml()), "marks": np.array(RAW_MARKS)}
+    with tempfile.TemporaryDirectory() as d:
+        xml = sc.write_xml(Path(d) / "raw.xml")
+        root = Path(d) / "res"
+        r = _quiet(reference.Reference, xml)
+        assert _quiet(r.set_particles, sc.type, sc.x, sc.v, sc.w, sc.q) == 0
+        assert _quiet(r.init) == 0
+        assert _quiet(r.step, RAW_SETTLE) == 0
+        pfile = Path(d) / "raw_Particles"
+        assert r.write_particles(pfile) == 0
+        if not binary:      # the same file for both modes: kept once
+            out["particles"] = np.array(pfile.read_text())
+        times, vstats, done = [], [], 0
+        for m in RAW_MARKS:
+            t = (RAW_SETTLE + m) * dt
+            if m == 0:
+                assert _quiet(r.rawdata_start, root, binary, t) == 0
+            else:
+                assert _quiet(r.step, m - done) == 0
+                done = m
+                assert _quiet(r.rawdata_write, t) == 0
+            times.append(t)
+            vstats.append(r.velocity_max_mean())
+        _quiet(r.rawdata_end)
+        for name in RAW_SUFFIXES:
+            data = (Path(d) / f"res_{name}.dat").read_bytes()
+            out[name] = np.frombuffer(data, np.uint8) if binary else np.array(data.decode())
+        out["times"] = np.array(times)
+        out["velocity_max_mean"] = np.array(vstats)
+    np.savez_compressed(HERE / f"rawdata_settling_{mode}.npz", **out)
+    print(f"wrote rawdata_settling_{mode}.npz (RawData files of the reference, {mode})")
+
+
 def main():
     import subprocess
     if not reference.available():
@@ -164,10 +217,17 @@ def main():
     for name in SCENARIOS:
         subprocess.run([sys.executable, __file__, name], check=True)
     subprocess.run([sys.executable, __file__, "reload"], check=True)
+    for mode in ("text", "binary"):
+        subprocess.run([sys.executable, __file__, "rawdata", mode], check=True)
 
 
 if __name__ == "__main__":
     if len(sys.argv) > 1:
-        run_reload() if sys.argv[1] == "reload" else run(sys.argv[1])
+        if sys.argv[1] == "reload":
+            run_reload()
+        elif sys.argv[1] == "rawdata":
+            run_rawdata(sys.argv[2])
+        else:
+            run(sys.argv[1])
     else:
         main()
