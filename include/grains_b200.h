@@ -224,6 +224,13 @@ int gdem_download_state(gdem_handle h, double* x, double* v, double* w, double* 
  * skipped. */
 int gdem_write_reload_particles(gdem_handle h, const char* path);
 int gdem_read_reload_particles(gdem_handle h, const char* path);
+/* The same particle file in the hybrid (binary) form of a Format2024 reload
+ * (the "<reload>_Particles.bin" file: per particle its record's byte count
+ * as a size_t, then the Particle::write2014_binary record, Component/src/
+ * Particle.cpp:1183-1193, in host byte order; AllComponents::write :1387-1404
+ * and read_particles :1163-1256). */
+int gdem_write_reload_particles_hybrid(gdem_handle h, const char* path);
+int gdem_read_reload_particles_hybrid(gdem_handle h, const char* path);
 
 /* Cell (i, j, k) of every particle, in Cell::GetCell numbering
  * (Base/src/Cell.cpp:172-184), by particle ID. */

@@ -266,6 +266,21 @@ int ref_write_particles(void* h, const char* path) {
   return out ? 0 : 1;
 }
 
+// The same file in the hybrid (binary) form: each master's byte count, then
+// its Particle::write2014_binary record (AllComponents.cpp:1387-1404).
+int ref_write_particles_hybrid(void* h, const char* path) {
+  RefGrains* g = static_cast<RefGrains*>(h);
+  std::ofstream out(path, std::ios::out | std::ios::binary);
+  if (!out) return 1;
+  for (Particle* p : g->masters())
+    if (p) {
+      size_t nb = p->get_numberOfBytes();
+      out.write(reinterpret_cast<char*>(&nb), sizeof(size_t));
+      p->write2014_binary(out);
+    }
+  return out ? 0 : 1;
+}
+
 // RawData output of the reference's own RawDataPostProcessingWriter
 // (PostProcessing/src/RawDataPostProcessingWriter.cpp), registered as the
 // one post-processing writer and driven as Grains::do_before_time_stepping

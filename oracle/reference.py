@@ -50,6 +50,8 @@ def _load():
         lib.ref_get_history.argtypes = [V, I, I, D, D, D]
         lib.ref_write_particles.argtypes = [V, ctypes.c_char_p]
         lib.ref_write_particles.restype = ctypes.c_int
+        lib.ref_write_particles_hybrid.argtypes = [V, ctypes.c_char_p]
+        lib.ref_write_particles_hybrid.restype = ctypes.c_int
         lib.ref_rawdata_start.argtypes = [V, ctypes.c_char_p, ctypes.c_double]
         lib.ref_rawdata_start.restype = ctypes.c_int
         lib.ref_rawdata_write.argtypes = [V, ctypes.c_double]
@@ -114,6 +116,10 @@ class Reference:
     def write_particles(self, path):
         """The particle file of a Format2024 reload, by Particle::write2014."""
         return _load().ref_write_particles(self._h, os.fsencode(str(path)))
+
+    def write_particles_hybrid(self, path):
+        """The same particle file in the hybrid binary form (Particle::write2014_binary)."""
+        return _load().ref_write_particles_hybrid(self._h, os.fsencode(str(path)))
 
     def rawdata_start(self, root, binary, time):
         """Registers the reference's RawDataPostProcessingWriter with output

@@ -1595,7 +1595,35 @@ struct MapEntry {
 
 }  // namespace
 
-int gdem_write_reload_particles(gdem_handle h, const char* path) {
+}  // extern "C"
+
+namespace {
+
+// Binary record helpers of the Hybrid reload format (raw host-order bytes,
+// as std::ostream::write of the reference's fields).
+template <typename V>
+void putRaw(std::string& out, V const& v) {
+  out.append(reinterpret_cast<const char*>(&v), sizeof(V));
+}
+template <typename V>
+V getRaw(const char*& p, const char* end) {
+  if (end - p < (std::ptrdiff_t)sizeof(V)) throw std::runtime_error("truncated particle record");
+  V v;
+  std::memcpy(&v, p, sizeof(V));
+  p += sizeof(V);
+  return v;
+}
+
+}  // namespace
+
+extern "C" {
+
+// The particle file of a Format2024 reload from the device state: text
+// (Particle::write2014, Component/src/Particle.cpp:1167-1176) or, hybrid,
+// binary records each preceded by its byte count (AllComponents::write,
+// AllComponents.cpp:1387-1404; Particle::write2014_binary,
+// Particle.cpp:1183-1193, get_numberOfBytes :1201-1208).
+static int writeReloadParticles(gdem_handle h, const char* path, bool hybrid) {
   return guarded([&] {
     System* s = sys(h);
     if (!s || !s->started || !path) throw std::runtime_error("no stepped state to write");
@@ -1648,6 +1676,47 @@ int gdem_write_reload_particles(gdem_handle h, const char* path) {
         maps[a].push_back(ea);
       }
     }
+    if (hybrid) {
+      std::ofstream out(path, std::ios::out | std::ios::binary);
+      if (!out) throw std::runtime_error(std::string("cannot write ") + path);
+      std::string rec;
+      for (size_t i = 0; i < n; ++i) {
+        auto& m = maps[i];
+        std::sort(m.begin(), m.end(), [](MapEntry const& p, MapEntry const& r) { return p.partner < r.partner; });
+        // class, ID, tag, activity | origin, basis, transform type | v, q
+        // (w first), omega, F, T | map size, entries (key triple, active,
+        // 9 doubles)
+        const size_t nb = 3 * sizeof(int) + sizeof(unsigned) + 12 * sizeof(double) +
+                          sizeof(unsigned) + 16 * sizeof(double) + sizeof(int) +
+                          m.size() * (4 * sizeof(int) + 9 * sizeof(double));
+        rec.clear();
+        putRaw(rec, nb);
+        putRaw(rec, s->h_type[i]);
+        putRaw(rec, refId(i));
+        putRaw(rec, 0);
+        putRaw(rec, 1u);
+        for (int d = 0; d < 3; ++d) putRaw(rec, x[3 * i + d]);
+        for (int k = 0; k < 9; ++k) putRaw(rec, B[9 * i + k]);
+        putRaw(rec, 3u);
+        for (int d = 0; d < 3; ++d) putRaw(rec, v[3 * i + d]);
+        putRaw(rec, q[4 * i + 3]);
+        for (int d = 0; d < 3; ++d) putRaw(rec, q[4 * i + d]);
+        for (int d = 0; d < 3; ++d) putRaw(rec, w[3 * i + d]);
+        for (int d = 0; d < 3; ++d) putRaw(rec, F[3 * i + d]);
+        for (int d = 0; d < 3; ++d) putRaw(rec, T[3 * i + d]);
+        putRaw(rec, (int)m.size());
+        for (auto const& e : m) {
+          putRaw(rec, 1);
+          putRaw(rec, e.partner);
+          putRaw(rec, 1);
+          putRaw(rec, 1);
+          for (int c = 0; c < 9; ++c) putRaw(rec, e.v[c]);
+        }
+        out.write(rec.data(), (std::streamsize)rec.size());
+      }
+      if (!out) throw std::runtime_error(std::string("write failed: ") + path);
+      return GDEM_OK;
+    }
     std::ofstream out(path);
     if (!out) throw std::runtime_error(std::string("cannot write ") + path);
     for (size_t i = 0; i < n; ++i) {
@@ -1676,13 +1745,24 @@ int gdem_write_reload_particles(gdem_handle h, const char* path) {
   });
 }
 
-int gdem_read_reload_particles(gdem_handle h, const char* path) {
+int gdem_write_reload_particles(gdem_handle h, const char* path) {
+  return writeReloadParticles(h, path, false);
+}
+int gdem_write_reload_particles_hybrid(gdem_handle h, const char* path) {
+  return writeReloadParticles(h, path, true);
+}
+
+// A Format2024 reload's particle file into a fresh system: text
+// (Particle::read2014, Component/src/Particle.cpp:972-1024) or hybrid binary
+// records (AllComponents::read_particles, AllComponents.cpp:1163-1256;
+// Particle::read2014_binary, Particle.cpp:1032-1080).
+static int readReloadParticles(gdem_handle h, const char* path, bool hybrid) {
   return guarded([&] {
     System* s = sys(h);
     if (!s || !path) throw std::runtime_error("invalid arguments");
     if (s->have_state) throw std::runtime_error("the system already has particles");
     if (s->inst.size() != 1) throw std::runtime_error("a reload file holds one system, not a batch");
-    std::ifstream in(path);
+    std::ifstream in(path, hybrid ? std::ios::in | std::ios::binary : std::ios::in);
     if (!in) throw std::runtime_error(std::string("cannot read ") + path);
     struct Rec {
       int cls, id;
@@ -1690,8 +1770,49 @@ int gdem_read_reload_particles(gdem_handle h, const char* path) {
       std::vector<MapEntry> map;
     };
     std::vector<Rec> recs;
+    auto keep = [&](Rec&& r, int tag, unsigned active) {
+      if (tag > 1 || !active) return;   // periodic clones and waiting particles
+      if (r.cls < 0 || r.cls >= (int)s->inst[0].types.size())
+        throw std::runtime_error("particle class out of range in " + std::string(path));
+      recs.push_back(std::move(r));
+    };
     std::string line;
-    while (std::getline(in, line)) {
+    while (hybrid) {
+      size_t nb = 0;
+      if (!in.read(reinterpret_cast<char*>(&nb), sizeof nb)) break;
+      if (nb > (size_t(1) << 24)) throw std::runtime_error("malformed particle record in " + std::string(path));
+      std::string buf(nb, '\0');
+      if (!in.read(&buf[0], (std::streamsize)nb)) throw std::runtime_error("truncated particle record in " + std::string(path));
+      const char* p = buf.data();
+      const char* end = p + nb;
+      Rec r;
+      r.cls = getRaw<int>(p, end);
+      r.id = getRaw<int>(p, end);
+      const int tag = getRaw<int>(p, end);
+      const unsigned active = getRaw<unsigned>(p, end);
+      for (double& d : r.x) d = getRaw<double>(p, end);
+      for (double& d : r.B) d = getRaw<double>(p, end);
+      (void)getRaw<unsigned>(p, end);
+      for (double& d : r.v) d = getRaw<double>(p, end);
+      r.q[3] = getRaw<double>(p, end);
+      for (int d = 0; d < 3; ++d) r.q[d] = getRaw<double>(p, end);
+      for (double& d : r.w) d = getRaw<double>(p, end);
+      for (double& d : r.F) d = getRaw<double>(p, end);
+      for (double& d : r.T) d = getRaw<double>(p, end);
+      const int nm = getRaw<int>(p, end);
+      for (int k = 0; k < nm; ++k) {
+        MapEntry e;
+        (void)getRaw<int>(p, end);
+        e.partner = getRaw<int>(p, end);
+        (void)getRaw<int>(p, end);
+        const int act = getRaw<int>(p, end);
+        for (double& d : e.v) d = getRaw<double>(p, end);
+        if (act) r.map.push_back(e);
+      }
+      if (p != end) throw std::runtime_error("particle record size mismatch in " + std::string(path));
+      keep(std::move(r), tag, active);
+    }
+    while (!hybrid && std::getline(in, line)) {
       std::istringstream is(line);
       Rec r;
       int tag = 0, ttype = 0;
@@ -1716,10 +1837,7 @@ int gdem_read_reload_particles(gdem_handle h, const char* path) {
         if (act) r.map.push_back(e);
       }
       if (!is) throw std::runtime_error("malformed particle line in " + std::string(path));
-      if (tag > 1 || !active) continue;   // periodic clones and waiting particles
-      if (r.cls < 0 || r.cls >= (int)s->inst[0].types.size())
-        throw std::runtime_error("particle class out of range in " + std::string(path));
-      recs.push_back(std::move(r));
+      keep(std::move(r), tag, active);
     }
     if (recs.empty()) throw std::runtime_error(std::string("no particle in ") + path);
     std::sort(recs.begin(), recs.end(), [](Rec const& a, Rec const& b) { return a.id < b.id; });
@@ -1770,6 +1888,13 @@ int gdem_read_reload_particles(gdem_handle h, const char* path) {
                               pn.data(), sp.data()));
     return GDEM_OK;
   });
+}
+
+int gdem_read_reload_particles(gdem_handle h, const char* path) {
+  return readReloadParticles(h, path, false);
+}
+int gdem_read_reload_particles_hybrid(gdem_handle h, const char* path) {
+  return readReloadParticles(h, path, true);
 }
 
 int gdem_download_cells(gdem_handle h, int* ijk) {

@@ -78,6 +78,8 @@ def library() -> ctypes.CDLL:
         "gdem_upload_forces": ([_P, _DP, _DP], ctypes.c_int),
         "gdem_upload_history": ([_P, i64, _IP, _IP, _DP, _DP, _DP], ctypes.c_int),
         "gdem_write_reload_particles": ([_P, ctypes.c_char_p], ctypes.c_int),
+        "gdem_write_reload_particles_hybrid": ([_P, ctypes.c_char_p], ctypes.c_int),
+        "gdem_read_reload_particles_hybrid": ([_P, ctypes.c_char_p], ctypes.c_int),
         "gdem_read_reload_particles": ([_P, ctypes.c_char_p], ctypes.c_int),
         "gdem_set_fluid": ([_P, ctypes.c_double, ctypes.c_int], ctypes.c_int),
         "gdem_set_time_step": ([_P, ctypes.c_double], ctypes.c_int),
@@ -227,6 +229,14 @@ class Grains:
         memory); stepping then continues without do_before_time_stepping."""
         self._check(library().gdem_read_reload_particles(self._h, os.fsencode(str(path))))
         self.n = library().gdem_num_particles(self._h)
+
+    def read_reload_particles_hybrid(self, path):
+        """Loads the hybrid (binary) form of a reload particle file."""
+        self._check(library().gdem_read_reload_particles_hybrid(self._h, os.fsencode(str(path))))
+        self.n = library().gdem_num_particles(self._h)
+
+    def write_reload_particles_hybrid(self, path):
+        self._check(library().gdem_write_reload_particles_hybrid(self._h, os.fsencode(str(path))))
 
     def write_reload_particles(self, path):
         """Writes the state after the last step as a Format2024 reload

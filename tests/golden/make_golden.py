@@ -136,7 +136,10 @@ def run_reload():
         assert _quiet(r.step, 600) == 0
         pfile = Path(d) / "reload_Particles"
         assert r.write_particles(pfile) == 0
+        bfile = Path(d) / "reload_Particles.bin"
+        assert r.write_particles_hybrid(bfile) == 0
         out = {"xml": np.array(sc.xml()), "particles": np.array(pfile.read_text()),
+               "particles_hybrid": np.frombuffer(bfile.read_bytes(), np.uint8),
                "marks": np.array([1, 50])}
         from oracle.oracle import Oracle
         from tests.helpers import contact_scale
