@@ -284,6 +284,11 @@ int gdem_rawdata_end(gdem_handle h);
  * (Grains::do_before_time_stepping opens it anew, Grains.cpp:137-145). */
 int gdem_write_velocity_max_mean(gdem_handle h, const char* path, int append, double time);
 
+/* The XML's RawData writer (<Simulation><PostProcessing><Writers><RawData
+ * Name=".." WritingMode="Text|Binary"/>, PostProcessingWriterBuilderFactory.cpp
+ * :19-20): its root name ("" when the XML has none) and binary flag. */
+int gdem_rawdata_spec(gdem_handle h, char* root, int capacity, int* binary);
+
 /* OR of the status bits raised since creation (or the last reset). */
 int gdem_status(gdem_handle h, int* bits, int reset);
 

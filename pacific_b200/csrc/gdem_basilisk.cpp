@@ -26,6 +26,11 @@
 //                     (a class that is not a sphere is reported as an error:
 //                     its envelope and faces are not written).
 //   UpdateVelocityGrains  velocities from the fluid (updateParticlesVelocity).
+//   SaveResults_Grains  the XML's RawData writer, if any (started at the first
+//                     call, an output time at each later one; the last
+//                     sub-step of Simu_Grains then records its contacts for
+//                     the coordination numbers), and a Format2024 particle
+//                     file "grains_b200_<cycle>_Particles".
 // Contact memory: the reference's coupled step never prunes a contact map
 // entry whose contact has ended (it skips Grains::computeParticlesForceAnd
 // Torque's setContactMapToFalse / updateContactMap), so a pair that touches
@@ -52,6 +57,10 @@ double g_min_dt = 0., g_max_dt = 0.;
 int64_t g_n = 0;
 std::vector<int> g_class;      // particle class by particle index
 std::vector<int> g_ids;        // reload IDs by particle index
+bool g_restart = false;
+std::string g_raw_root;        // the XML's RawData writer ("" if none)
+int g_raw_binary = 0;
+bool g_raw_started = false;
 
 void fail(const char* where) {
   std::fprintf(stderr, "Grains3D B200 coupling: %s: %s\n", where, gdem_last_error());
@@ -113,9 +122,12 @@ extern "C" {
 
 void Init_Grains(char const* inputfile, double fluid_rho, const bool b_restart,
                  const bool b_fluidcorrectedacc) {
-  (void)b_restart;   // the particles always come from the XML's reload file
+  // the particles always come from the XML's reload file; b_restart makes
+  // the RawData writer append (a reload of type "same")
+  g_restart = b_restart;
   if (g_sys) { gdem_destroy(g_sys); g_sys = nullptr; }
   g_error = false;
+  g_raw_started = false;
   const char* prec = std::getenv("GRAINS_B200_PRECISION");
   const int mode = (prec && std::strcmp(prec, "fp32split") == 0) ? GDEM_FP32_SPLIT : GDEM_FP64;
   if (gdem_create(inputfile, mode, &g_sys) != GDEM_OK) { fail("Init_Grains"); return; }
@@ -144,6 +156,12 @@ void Init_Grains(char const* inputfile, double fluid_rho, const bool b_restart,
     fail("Init_Grains");
     return;
   }
+  char raw[4096];
+  if (gdem_rawdata_spec(g_sys, raw, sizeof(raw), &g_raw_binary) != GDEM_OK) {
+    fail("Init_Grains");
+    return;
+  }
+  g_raw_root = raw;
   std::printf("Construction of Grains completed\n");
 }
 
@@ -154,7 +172,16 @@ void Simu_Grains(const double dt_fluid) {
   g_ndt = (int)(size_t)(dt_fluid / dteff);
   if (g_ndt < 1) g_ndt = 1;
   const double dt = dt_fluid / double(g_ndt);
-  if (gdem_set_time_step(g_sys, dt) != GDEM_OK || gdem_step(g_sys, g_ndt) != GDEM_OK) {
+  if (gdem_set_time_step(g_sys, dt) != GDEM_OK) {
+    fail("Simu_Grains");
+    return;
+  }
+  // with a RawData writer, the last sub-step records its contacts so that
+  // SaveResults_Grains can write the coordination numbers
+  const bool record = !g_raw_root.empty();
+  if (gdem_step(g_sys, record ? g_ndt - 1 : g_ndt) != GDEM_OK ||
+      (record && (gdem_set_diagnostics(g_sys, 1) != GDEM_OK || gdem_step(g_sys, 1) != GDEM_OK ||
+                  gdem_set_diagnostics(g_sys, 0) != GDEM_OK))) {
     fail("Simu_Grains");
     return;
   }
@@ -232,9 +259,17 @@ char* GrainsToBasilisk(int* pstrsize) {
 void SetInitialTime(double tinit) { g_time = tinit; }
 
 void SaveResults_Grains() {
-  // the reference's post-processing writers are not part of this library;
-  // a Format2024 particle file of the current state stands in for them
+  // GrainsCoupledWithFluid::InitialPostProcessing at the first call,
+  // doPostProcessing after (:870-893): the XML's RawData writer, if any, and
+  // a Format2024 particle file of the current state
   if (!g_sys || g_error) return;
+  if (!g_raw_root.empty()) {
+    const int rc = g_raw_started ? gdem_rawdata_write(g_sys, g_time)
+                                 : gdem_rawdata_start(g_sys, g_raw_root.c_str(), g_raw_binary,
+                                                      g_restart ? 1 : 0, g_time);
+    if (rc != GDEM_OK) { fail("SaveResults_Grains"); return; }
+    g_raw_started = true;
+  }
   char name[64];
   std::snprintf(name, sizeof(name), "grains_b200_%06d_Particles", g_cycle++);
   if (gdem_write_reload_particles(g_sys, name) != GDEM_OK) fail("SaveResults_Grains");

@@ -82,6 +82,8 @@ struct InstanceDesc {
   double min_dt, max_dt;
   int ndt;
   std::string reload_file;   // Construction/Reload Filename, if any
+  std::string rawdata_root;  // Simulation/PostProcessing/Writers/RawData Name, if any
+  bool rawdata_binary = false;
   int nmat;
   // what the pair-list grid is made from (it is remade when the skin changes)
   double box_org[3], box_max[3];
@@ -452,6 +454,16 @@ InstanceDesc readInstance(std::string const& path) {
   I.reload_file.clear();
   if (XmlNode const* rl = root->find("Reload"))
     if (rl->has("Filename")) I.reload_file = rl->attr("Filename");
+  // a RawData post-processing writer (PostProcessingWriterBuilderFactory,
+  // PostProcessing/src/PostProcessingWriterBuilderFactory.cpp:19-20;
+  // RawDataPostProcessingWriter ctor: Name, WritingMode="Binary")
+  I.rawdata_root.clear();
+  I.rawdata_binary = false;
+  if (XmlNode const* rd = root->find("RawData"))
+    if (rd->has("Name")) {
+      I.rawdata_root = rd->attr("Name");
+      I.rawdata_binary = rd->has("WritingMode") && rd->attr("WritingMode") == "Binary";
+    }
   for (auto& t : I.types)
     for (int d = 0; d < 3; ++d) t.weight[d] = I.gravity[d] * (t.mass * (1. - 0. / 1.));
   // linked cell grid (LinkedCell::set, Base/src/LinkedCell.cpp:47-160)
@@ -1416,6 +1428,18 @@ int gdem_reload_filename(gdem_handle h, char* buf, int capacity) {
     std::string const& f = s->inst[0].reload_file;
     if ((int)f.size() >= capacity) throw std::runtime_error("buffer too small");
     std::memcpy(buf, f.c_str(), f.size() + 1);
+    return GDEM_OK;
+  });
+}
+
+int gdem_rawdata_spec(gdem_handle h, char* root, int capacity, int* binary) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !root || capacity <= 0) throw std::runtime_error("invalid arguments");
+    std::string const& r = s->inst[0].rawdata_root;
+    if ((int)r.size() >= capacity) throw std::runtime_error("buffer too small");
+    std::memcpy(root, r.c_str(), r.size() + 1);
+    if (binary) *binary = s->inst[0].rawdata_binary ? 1 : 0;
     return GDEM_OK;
   });
 }

@@ -147,3 +147,43 @@ def test_hydro_forces(tmp_path, lib):
     s = g.download_state()
     assert abs(s["v"][0, 2]) <= 1e-12
     g.close()
+
+
+def test_basilisk_rawdata_output(tmp_path, lib):
+    """SaveResults_Grains with a RawData writer in the XML: the first call
+    starts the writer (GrainsCoupledWithFluid::InitialPostProcessing), later
+    ones add an output time (doPostProcessing); Simu_Grains records the last
+    sub-step's contacts, so the coordination numbers written are those of
+    the plain ABI stepped the same way with diagnostics on."""
+    sc = _settled(tmp_path)
+    raw = tmp_path / "out"
+    text = (tmp_path / "coupled.xml").read_text().replace(
+        "  </Simulation>",
+        f'    <PostProcessing>\n      <Writers>\n        <RawData Name="{raw}" WritingMode="Text"/>\n'
+        "      </Writers>\n    </PostProcessing>\n  </Simulation>")
+    (tmp_path / "coupled_raw.xml").write_text(text)
+    b = _basilisk()
+    b.SetInitialTime.argtypes = [ctypes.c_double]
+    b.Init_Grains(str(tmp_path / "coupled_raw.xml").encode(), 1000.0, False, True)
+    b.SetInitialTime(0.0)
+    b.SaveResults_Grains()
+    b.Simu_Grains(4e-5)
+    b.SaveResults_Grains()
+    ref = Grains(str(tmp_path / "coupled.xml"), FP64)
+    ref.read_reload_particles(tmp_path / "res_Particles")
+    ref.set_fluid(1000.0, True)
+    ref.set_time_step(1e-5)
+    ref.step(3)
+    ref.set_diagnostics(True)
+    ref.step(1)
+    s = ref.download_state()
+    coord = ref.download_coordination()
+    ref.close()
+    lines = (tmp_path / "out_position_x.dat").read_text().splitlines()
+    assert len(lines) == 2
+    tok = lines[1].split()
+    assert float(tok[0]) == 4e-5
+    assert np.array_equal(np.array(tok[1:], dtype=float), np.array([float(f"{x:.6e}") for x in s["x"][:, 0]]))
+    c = (tmp_path / "out_coordinationNumber.dat").read_text().splitlines()
+    assert c[0].split() == ["0"] * sc.n
+    assert np.array_equal(np.array(c[1].split(), dtype=int), coord) and coord.sum() > 0
