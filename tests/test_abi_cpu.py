@@ -62,3 +62,26 @@ def test_basilisk_library_exports_the_coupling_abi(lib):
     n, m = ctypes.c_size_t(7), ctypes.c_size_t(7)
     b.NumberOfRigidBodiesInBasilisk(ctypes.byref(n), ctypes.byref(m))
     assert n.value == 0 and m.value == 0
+
+
+def test_output_entry_points_reject_bad_arguments(lib, tmp_path):
+    """The RawData writer, the velocity line and the reload readers check
+    their arguments before touching a device: a null handle or a missing
+    file is GDEM_ERR_INVALID with a message, never a crash."""
+    import ctypes
+    lib.gdem_rawdata_start.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_double]
+    lib.gdem_write_velocity_max_mean.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int,
+                                                 ctypes.c_double]
+    lib.gdem_rawdata_write.argtypes = [ctypes.c_void_p, ctypes.c_double]
+    lib.gdem_rawdata_end.argtypes = [ctypes.c_void_p]
+    lib.gdem_read_reload_particles_hybrid.argtypes = [ctypes.c_void_p, ctypes.c_char_p]
+    lib.gdem_last_error.restype = ctypes.c_char_p
+    root = str(tmp_path / "out").encode()
+    assert lib.gdem_rawdata_start(None, root, 0, 0, 0.0) == -1
+    assert lib.gdem_write_velocity_max_mean(None, root, 0, 0.0) == -1
+    assert lib.gdem_rawdata_write(None, 0.0) == -1
+    assert b"gdem_rawdata_start" in lib.gdem_last_error()
+    assert lib.gdem_rawdata_end(None) == 0            # nothing open: nothing to close
+    assert lib.gdem_read_reload_particles_hybrid(None, root) == -1
+    assert not list(tmp_path.iterdir())
