@@ -212,3 +212,16 @@ def test_binary_matches_reference(tmp_path, lib):
     cols, coord = _cols_of(seen)
     for q in QUANT:
         assert np.array_equal(got_cols[q], cols[q])
+
+
+@pytest.mark.gpu
+def test_writer_refuses_a_batch(tmp_path, lib):
+    from pacific_b200 import GrainsError, scenarios
+    inst = scenarios.batched_boxes(n_inst=2, nmin=50, nmax=80, seed=7)
+    xmls = [str(s.write_xml(tmp_path / f"i{k}.xml")) for k, s in enumerate(inst)]
+    ins, typ, x, v, w, q = scenarios.concat_state(inst)
+    g = Grains(xmls, FP64)
+    g.upload_state(typ, x, v, w, q, inst=ins)
+    with pytest.raises(GrainsError, match="batch"):
+        g.rawdata_start(tmp_path / "out")
+    g.close()
