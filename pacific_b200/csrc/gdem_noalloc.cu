@@ -19,6 +19,12 @@
 //   * The first call on a device looks up the scratch address with
 //     cudaGetSymbolAddress while that device is current; it should come
 //     before any stream capture.  Later calls only launch two kernels.
+//   * The address belongs to the device's context.  Each call compares the
+//     current context's ID (cuCtxGetId, reached through the runtime's driver
+//     entry point, so this library needs no link to libcuda) with the one the
+//     address was looked up in, and looks it up again after a change, e.g.
+//     after cudaDeviceReset ended the previous context.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -39,6 +45,38 @@ static __device__ __align__(256) double g_speed_scratch[2 * kSpeedMaxBlocks];
 
 std::mutex g_addr_mutex;
 double* g_addr[kMaxDevices] = {nullptr};
+// ID of the context each cached address was looked up in (0: none)
+unsigned long long g_ctx_id[kMaxDevices] = {0};
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// ID of the calling thread's current context, 0 when there is none (or the
+// driver cannot tell).  Caller holds g_addr_mutex.
+unsigned long long currentContextId() {
+  static CtxGetCurrentFn get_current = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    looked_up = true;
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<CtxGetIdFn>(f);
+    cudaGetLastError();
+  }
+  if (!get_current || !get_id) return 0;
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+  unsigned long long id = 0;
+  if (get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 // |v| of particle i from AoS velocities (3 per particle)
 __device__ __forceinline__ double speed(const double* v, int i) {
@@ -124,11 +162,16 @@ int gdem_speed_stats_static(const double* v, int64_t n, double* out, void* strea
   double* part;
   {
     std::lock_guard<std::mutex> lock(g_addr_mutex);
-    if (!g_addr[dev]) {
+    // the cached address is valid while the context it was looked up in is
+    // still the current one (a context ID is never reused)
+    const unsigned long long ctx = currentContextId();
+    if (!g_addr[dev] || ctx == 0 || ctx != g_ctx_id[dev]) {
       void* p = nullptr;
       e = cudaGetSymbolAddress(&p, g_speed_scratch);
       if (e != cudaSuccess) return fail(GDEM_ERR_CUDA, cudaGetErrorString(e));
       g_addr[dev] = static_cast<double*>(p);
+      // the lookup has made the device's context current on this thread
+      g_ctx_id[dev] = currentContextId();
     }
     part = g_addr[dev];
   }
