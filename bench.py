@@ -110,26 +110,33 @@ def algorithmic_bytes(kernel, n, entries, contacts, ncells, fp64):
     step: each input read once, each output written once, neighbour re-reads
     counted as cache hits.  Per particle unless noted.  The particle state is
     x, v, w, w_bf, q in FP64; FP32-split spheres keep no w_bf (w is their
-    angular state)."""
+    angular state).  entries: pair-list entries (each pair twice); contacts:
+    pairs in contact (the pairs the contact filter keeps are these, up to the
+    FP32 margin of the test)."""
     vel = 24
     state = 24 + (3 if fp64 else 2) * vel + 32
-    touched = min(n, 2 * contacts)    # particles with a contact (the force work list)
+    pairs = entries // 2
+    touched = min(n, 2 * contacts)    # particles with a contact
+    share = 64 if fp64 else 32        # one side of a contact, per row entry
+    hist = 8 + (72 if fp64 else 36)   # history key + values
     if kernel == "filter":
-        # posf, instance | next flags; per pair (half the directed entries)
-        # its compact-list word pair; per contact the two flags and the
-        # work-list entries
-        return n * (16 + 4 + 4) + (entries // 2) * 8 + contacts * 16
-    if kernel in ("forces64", "forces32"):
-        # per particle of the work list: cellc id type x v w nact | F T; per
-        # contact the entry word, the partner's id type x v w and the history
-        # key + values, read and written
-        per_p = 16 + 4 + 4 + 24 + 2 * vel + 4 + 48
-        per_c = 4 + (4 + 4 + 24 + 2 * vel) + 2 * (8 + (72 if fp64 else 36))
-        return touched * per_p + contacts * per_c
+        # per particle its FP32 position; per pair its compact-list word
+        # pair; per kept pair its index in the kept list and the two
+        # candidate marks
+        return n * 16 + pairs * 8 + contacts * (4 + 8)
+    if kernel in ("pairlaw64", "pairlaw32"):
+        # per kept pair: its index, compact-list words and row positions;
+        # both partners' id type wrap x v w and row offsets; the history
+        # read and written; the two shares and the two flags
+        return contacts * (4 + 8 + 4 + 2 * (4 + 4 + 4 + 24 + 2 * vel + 4) + 2 * hist
+                           + 2 * share + 2 * 4)
     if kernel == "move":
-        # state type inst disp wrap nact (+ F T of the particles in contact)
-        # | state disp wrap posf
-        return n * (state + 8 + 12 + 4 + 4 + state + 12 + 4 + 16) + touched * 48
+        # state type inst disp wrap flags | state disp wrap posf flags, and
+        # for a particle in contact its row offset and length, the first
+        # word of each share of its row and the rest of each share in use
+        rowlen = entries / max(n, 1)
+        return int(n * (state + 8 + 12 + 4 + 4 + state + 12 + 4 + 16 + 4)
+                   + touched * (8 + rowlen * 16) + 2 * contacts * (share - 16))
     if kernel == "bin":          # x inst | skey rank; cell-count RMW
         return n * (24 + 4 + 8 + 8)
     if kernel == "scan":         # counts | starts (per cell)
@@ -142,8 +149,15 @@ def algorithmic_bytes(kernel, n, entries, contacts, ncells, fp64):
         return n * (4 + 4 + 12 + 2 * (state + 48) + 16 + (32 if fp64 else 16))
     if kernel == "copyback":     # ids state F T | ids state F T disp wrap
         return n * (12 + 2 * (state + 48) + 12 + 12 + 4)
-    if kernel in ("pairs64", "pairs32"):   # cellc + own position | npairs; entries; starts
-        return n * (16 + (32 if fp64 else 16) + 4) + 4 * entries + 4 * ncells
+    if kernel in ("pairs_count64", "pairs_count32"):   # cellc + own position | row length
+        return n * (16 + (32 if fp64 else 16) + 4) + 4 * ncells
+    if kernel == "row_scan":     # row lengths | row offsets
+        return n * 8
+    if kernel in ("pairs_fill64", "pairs_fill32"):
+        # cellc + own position + row offset and length | rows, compact list
+        return n * (16 + (32 if fp64 else 16) + 8) + 4 * ncells + 4 * entries + 12 * pairs
+    if kernel == "link":         # compact list, partner's row | row positions
+        return pairs * (8 + 4 + 4 + 4)
     return None
 
 
@@ -209,10 +223,14 @@ def pinned(a):
     return t
 
 
-def e2e_run(g, dist, steps):
-    """Public-API run with host buffers: the state goes up from pinned host
-    memory, each step reads back max/mean |v| (the per-step result Grains3D
-    writes to *_VelocityMaxMean.dat), the final state comes back down."""
+def e2e_run(g, dist, steps, every):
+    """Public-API run with host buffers, as a Grains3D run between two
+    outputs: the state goes up from pinned host memory (gdem_set_state), the
+    leapfrog runs `every` steps per call of Grains.Simulation (which reads
+    back the status word, the reference's exceptions), each output time
+    reads back max/mean |v| (what Grains::Simulation writes to
+    *_VelocityMaxMean.dat at its output times, Grains.cpp:390-408), and the
+    final state comes back down into pinned memory."""
     s = g.download_state()
     host = {k: pinned(s[k]) for k in ("x", "v", "w", "q", "F", "T")}
     outs = {k: pinned(np.zeros_like(s[k])) for k in ("x", "v", "w", "q", "F", "T")}
@@ -220,9 +238,14 @@ def e2e_run(g, dist, steps):
     t0 = time.perf_counter()
     g.set_state(host["x"].numpy(), host["v"].numpy(), host["w"].numpy(), host["q"].numpy(),
                 host["F"].numpy(), host["T"].numpy())
-    for _ in range(steps):
-        g.step(1)
+    done = 0
+    outputs = 0
+    while done < steps:
+        k = min(every, steps - done)
+        g.Simulation(k)
         g.velocity_stats()
+        done += k
+        outputs += 1
     from pacific_b200.grains import _dp, library
     lib = library()
     rc = lib.gdem_download_state(g._h, _dp(outs["x"].numpy()), _dp(outs["v"].numpy()),
@@ -234,7 +257,8 @@ def e2e_run(g, dist, steps):
     n = g.n
     up = n * 8 * (3 + 3 + 3 + 4 + 3 + 3)
     down = up
-    return dt, up / steps, 16 + down / steps
+    # per output: the status word (4 B) and max/mean |v| (16 B)
+    return dt, up / steps, (down + outputs * 20) / steps, outputs
 
 
 def error_sample(n_fcc, steps_before, precision):
@@ -271,6 +295,34 @@ def error_sample(n_fcc, steps_before, precision):
     return out
 
 
+def error_full(sc, xml, advance, tmpdir):
+    """Parity of one step at the full size against the Grains3D reference
+    itself: the GPU FP64 system advanced `advance` steps (a state with
+    contacts) writes its Format2024 particle file; the reference (oracle/_ref,
+    own process, its reload path) and the GPU in both precisions each read
+    that file and take one step.  Cells and contact sets are compared
+    exactly, forces per particle (normaliser: the particle's sum of
+    contact-force magnitudes)."""
+    from pacific_b200 import FP32_SPLIT, FP64
+    from tests.helpers import radii_of, step_parity
+    g = make_system(xml, sc, FP64)
+    g.step(advance)
+    pfile = Path(tmpdir) / "state_Particles"
+    t0 = time.perf_counter()
+    g.write_reload_particles(pfile)
+    t_write = time.perf_counter() - t0
+    g.close()
+    period = np.subtract(sc.maxc, sc.origin) * np.asarray(sc.periodic, float)
+    r = step_parity(xml, pfile, sc.n, radii_of(sc), (FP64, FP32_SPLIT), period=period)
+    out = {"sample": f"periodic_gas n={sc.n}, one step from the FP64 GPU state after "
+                     f"{advance} steps (written as a Format2024 particle file), vs the Grains3D "
+                     "reference itself (oracle/_ref) reading the same file",
+           "n": sc.n, "reference": r["reference"], "write_s": t_write,
+           "fp64": r[FP64], "fp32_split": r[FP32_SPLIT],
+           "tolerance": {"fp64": 1e-10, "fp32_split": 1e-5}}
+    return out
+
+
 def _quiet(f, *a):
     """Runs f with the process's stdout silenced (the reference prints its
     construction log)."""
@@ -296,7 +348,7 @@ def cpu_system(sc, xml):
         assert _quiet(r.set_particles, sc.type, sc.x, sc.v, sc.w, sc.q) == 0
         assert _quiet(r.init) == 0
         return "reference", (lambda k: _quiet(r.step, k)), \
-            "Grains3D reference sources (serial Type=Standard step), g++ -O2"
+            "Grains3D reference sources (serial Type=Standard step), g++ -O3"
     from tests.helpers import oracle_for
     o = oracle_for(sc, xml)
     o.init()
@@ -494,6 +546,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n-fcc", type=int, default=63)
     ap.add_argument("--e2e-steps", type=int, default=200)
+    ap.add_argument("--output-every", type=int, default=50,
+                    help="e2e: steps between two output times (status + max/mean |v| read back)")
+    ap.add_argument("--advance", type=int, default=1000,
+                    help="untimed steps before the warm-up, so that the timed window starts "
+                         "from a state with contacts, in the middle of the configured run")
+    ap.add_argument("--no-full-config", action="store_true",
+                    help="skip the device-timed run of the whole configured run from its start")
     ap.add_argument("--profile-steps", type=int, default=50)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-error", action="store_true")
@@ -505,6 +564,8 @@ def main():
     ap.add_argument("--no-graphs", action="store_true",
                     help="plain kernel launches instead of graph replay (for per-kernel profilers)")
     ap.add_argument("--convex-steps", type=int, default=500)
+    ap.add_argument("--only-fp32-split", action="store_true",
+                    help="skip the FP64 leg (profiling the FP32-split step alone)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -527,8 +588,12 @@ def main():
     n = sc.n
 
     res = {}
-    for name, prec in (("fp64", FP64), ("fp32_split", FP32_SPLIT)):
+    legs = (("fp32_split", FP32_SPLIT),) if args.only_fp32_split else \
+        (("fp64", FP64), ("fp32_split", FP32_SPLIT))
+    for name, prec in legs:
         g = make_system(xml, sc, prec, graphs=not args.no_graphs)
+        if args.advance > 0:
+            g.step(args.advance)
         g.step(args.warmup)
         e0, r0 = g.step_counts()
         if name == "fp32_split":
@@ -551,12 +616,26 @@ def main():
             g.close()
 
     g = res["fp32_split"]["g"]
-    e2e_dt, h2d, d2h = e2e_run(g, dist, args.e2e_steps)
+    e2e_dt, h2d, d2h, e2e_outputs = e2e_run(g, dist, args.e2e_steps, args.output_every)
     g.close()
+
+    # the whole configured run (2,000 steps from the start), device-timed
+    full = None
+    if not args.no_full_config:
+        full = {}
+        for name, prec in (("fp32_split", FP32_SPLIT), ("fp64", FP64)):
+            gf = make_system(xml, sc, prec, graphs=not args.no_graphs)
+            ms = timed_steps(gf, dist, 2000)
+            _, rb = gf.step_counts()
+            full[name] = {"value": world * n * 2000 / (ms * 1e-3), "ms_per_step": ms / 2000,
+                          "rebuilds": rb, "status": gf.status()}
+            gf.close()
+        full["fp32_split_speedup"] = full["fp32_split"]["value"] / full["fp64"]["value"]
+        full["steps"] = 2000
 
     if rank == 0:
         fp32 = res["fp32_split"]
-        fp64 = res["fp64"]
+        fp64 = res.get("fp64", fp32)
         value = world * n * args.steps / (fp32["ms"] * 1e-3)
         v64 = world * n * args.steps / (fp64["ms"] * 1e-3)
         # roofline of the dominant kernel of the FP32-split step
@@ -586,6 +665,17 @@ def main():
                 out[k] = row
             return out
         phases = phase_table(kt, fp32, False)
+        # whole step: the step kernels once per step, the rebuild kernels as
+        # often as the timed window rebuilt
+        per_step = ("filter", "pairlaw32", "move")
+        rebuild_k = ("bin", "scan", "place", "cellsort", "permute", "copyback", "pairs_count32",
+                     "row_scan", "pairs_fill32", "link")
+        step_bytes = sum(algorithmic_bytes(k, n, fp32["entries"], fp32["contacts"], ncells, False)
+                         for k in per_step)
+        step_bytes += (fp32["rebuilds"] / max(args.steps, 1)) * sum(
+            algorithmic_bytes(k, n, fp32["entries"], fp32["contacts"], ncells, False)
+            for k in rebuild_k)
+        step_achieved = step_bytes / (fp32["ms"] / args.steps * 1e-3) / 1e9
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
@@ -595,6 +685,9 @@ def main():
             "config": {"workload": "periodic_gas_1M", "n": n, "steps_config": 2000,
                        "dt": sc.dt, "phi": scenarios.solid_fraction(sc),
                        "parallelism": f"replicas{world}",
+                       "window": f"steps {args.advance + args.warmup + 1}-"
+                                 f"{args.advance + args.warmup + args.steps} of the run "
+                                 f"({args.advance} untimed + {args.warmup} warm-up steps first)",
                        "l2": "inputs larger than L2 (~0.5 GB of state per replica)"},
             "fp64": {"value": v64, "ms_per_step": fp64["ms"] / args.steps,
                      "fp32_split_speedup": value / v64, "status": fp64["status"]},
@@ -604,30 +697,51 @@ def main():
                          "peak_source": peak_src, "unit": "GB/s",
                          "frac": (achieved / hbm) if achieved else None,
                          "algorithmic_bytes_per_launch": ab, "avg_launch_us": 1e3 * avg_ms,
-                         "traffic": traffic},
+                         "traffic": traffic,
+                         "step": {"algorithmic_bytes_per_step": step_bytes,
+                                  "achieved": step_achieved, "frac": step_achieved / hbm,
+                                  "note": "whole graph-replayed step: filter + pair kernel + "
+                                          "leapfrog + the window's rebuilds, over ms_per_step"}},
             "phases_fp32_split": phases,
-            "phases_fp64": phase_table(fp64["kt"], fp64, True),
+            "phases_fp64": phase_table(fp64["kt"], fp64, True) if "fp64" in res else None,
             "clocks": clocks,
             "e2e": {"value": world * n * args.e2e_steps / e2e_dt, "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "steps": args.e2e_steps},
+                    "steps": args.e2e_steps, "output_every": args.output_every,
+                    "outputs": e2e_outputs,
+                    "how": "Grains.set_state from pinned host memory, Grains.Simulation per "
+                           "output interval (status read back), max/mean |v| read back at "
+                           "each output time, final state downloaded to pinned memory; "
+                           "host wall clock"},
             "gpu_launches": None,
         }
         # kernels launched in the timed region: the opening move, per step
-        # k_decide, the contact filter, the force kernel and the move, per
-        # pair-list rebuild its 9 kernels (bin, scan x3, place, cellsort,
-        # permute, copyback, pairs), and the history-table refills (every 512
-        # evaluations per table)
+        # k_decide, the contact filter, the pair kernel and the move, per
+        # pair-list rebuild its 14 kernels (bin, scan x3, place, cellsort,
+        # permute, copyback, row count, row scan x3, row fill, link), and the
+        # history-table refills (every 512 evaluations per table)
         e0, e1 = fp32["evals"]
         fills = sum(1 for e in range(e0 + 1, e1 + 1) if e % 512 < 2)
-        line["gpu_launches"] = 1 + 4 * args.steps + 9 * fp32["rebuilds"] + fills
+        line["gpu_launches"] = 1 + 4 * args.steps + 14 * fp32["rebuilds"] + fills
+        if "fp64" not in res:
+            line["fp64"] = None
         line["pair_list"] = {"rebuilds_fp32_split": fp32["rebuilds"],
                              "rebuilds_fp64": fp64["rebuilds"], "steps": args.steps}
+        line["window"] = {"contacts_at_end": fp32["contacts"], "rebuilds": fp32["rebuilds"],
+                          "first_step": args.advance + args.warmup + 1, "steps": args.steps}
+        if full is not None:
+            line["full_config"] = full
         if not args.no_error:
-            line["error"] = {"sample": "periodic_gas n_fcc=20 (32,000 spheres), one step "
-                                       "after 100 oracle steps, vs the CPU FP64 oracle",
-                             "fp32_split": error_sample(20, 100, FP32_SPLIT),
-                             "fp64": error_sample(20, 100, FP64)}
+            from oracle import reference
+            if reference.available():
+                line["error"] = error_full(sc, xml, args.advance, tmp.name)
+            else:
+                line["error"] = {"unavailable": "oracle/_ref was not built"}
+            line["error"]["restatement_32k"] = {
+                "sample": "periodic_gas n_fcc=20 (32,000 spheres), one step after 100 steps of "
+                          "the CPU FP64 restatement, from its state",
+                "fp32_split": error_sample(20, 100, FP32_SPLIT),
+                "fp64": error_sample(20, 100, FP64)}
         if args.batched_instances > 0:
             line["batched"] = batched_measure(args.batched_instances, args.batched_steps)
         if args.convex_n > 0:

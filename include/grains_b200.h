@@ -95,6 +95,17 @@ int gdem_upload_basis(gdem_handle h, const double* basis);
  * identity for a spheres-only system. */
 int gdem_download_basis(gdem_handle h, double* basis);
 
+/* The polyhedron support search's current vertex of every particle, by
+ * particle ID (Polyhedron::m_curr_vertex, Geometry/src/Polyhedron.cpp:
+ * 265-293: the search climbs the vertex graph from it and, among vertices
+ * tied within 1e-16, stays where it is, so it decides the witness points of
+ * face contacts).  A particle's vertex after an evaluation is the one its
+ * last GJK call in row order left (its wall calls come last).  A new or
+ * reloaded particle starts at the first vertex with a neighbour, as the
+ * reference's does; 0 for other shapes.  Upload after gdem_upload_state. */
+int gdem_upload_support_vertices(gdem_handle h, const int* vertex);
+int gdem_download_support_vertices(gdem_handle h, int* vertex);
+
 /* Maximum and mean translational speed over the particles
  * (AllComponents::ComputeMaxMeanVelocity, Component/src/AllComponents.cpp:
  * 1781-1811), the quantity Grains3D writes to *_VelocityMaxMean.dat. */
@@ -121,6 +132,19 @@ int gdem_law_counts(gdem_handle h, int64_t* evaluated, int64_t* reevaluated, int
 int gdem_gjk_counts(gdem_handle h, int64_t* calls, int64_t* iterations, int64_t* max_iterations,
                     int reset);
 
+/* Contact features over the evaluations since the state was created (or the
+ * last reset), as Grains3D prints them at the end of a run (Grains.cpp:
+ * 228-244, AppCollision::addToContactsFeatures, Base/src/AppCollision.cpp:
+ * 159-179): the largest and the mean |overlap| over the contacts (each pair
+ * and each particle-wall contact once per force evaluation), the evaluation
+ * at which the largest was first reached (0 is the leapfrog start at t0,
+ * k the evaluation at t0 + k dt; -1 without contact) and the mean GJK
+ * iterations per GJK call (0 for spheres only).  Accumulated on the device;
+ * the mean's last bits depend on the order of the warps' additions.  Any
+ * pointer may be NULL. */
+int gdem_contact_features(gdem_handle h, double* overlap_max, double* overlap_mean,
+                          int64_t* evaluation_of_max, double* gjk_iterations_mean, int reset);
+
 /* Per-kernel device timing with CUDA events (replaces the SCT_* phase timers,
  * Base/include/solvercomputingtime.hh:46-75).  While on, gdem_step uses plain
  * launches instead of graph replay.  gdem_kernel_times returns, per timed
@@ -134,6 +158,12 @@ int gdem_kernel_times(gdem_handle h, int capacity, int* count, char* names, doub
  * owner's instance), kdelta, previous normal, spring torque (3 each). */
 int gdem_upload_history(gdem_handle h, int64_t n, const int* owner, const int* partner,
                         const double* kdelta, const double* prevn, const double* spring);
+/* The contact memory of the last force evaluation in the same layout, both
+ * views of a pair (the second body's is the negation), ordered by owner then
+ * partner: *count receives the entry count; the arrays are filled when
+ * capacity >= *count (spring may be NULL). */
+int gdem_download_history(gdem_handle h, int64_t capacity, int64_t* count, int* owner,
+                          int* partner, double* kdelta, double* prevn, double* spring);
 
 /* Launch tuning, before gdem_init.  No counterpart in the reference (its
  * LinkedCell has a cell size only, Grains.cpp:1005-1022).  skin_factor is
@@ -258,6 +288,10 @@ int gdem_download_contacts(gdem_handle h, int64_t capacity, int64_t* count, int*
  * (Particle::getGeometricType, Particle.cpp:1651-1654). */
 int gdem_download_coordination(gdem_handle h, int* coord);
 int gdem_download_classes(gdem_handle h, int* cls);
+/* Reference particle IDs (Component::getID, 1-based) by particle index: the
+ * IDs of the Format2024 particle file the state was read from, else
+ * index + 1. */
+int gdem_download_ids(gdem_handle h, int* ids);
 
 /* RawData post-processing output of a system
  * (PostProcessing/src/RawDataPostProcessingWriter.cpp): per output time, a
@@ -299,6 +333,10 @@ int gdem_grid(gdem_handle h, int k, int* nb, double* edge, double* origin);
  * candidate pair appears once per partner) and live contact-memory entries
  * (active contacts, particle-particle and particle-wall). */
 int gdem_pair_counts(gdem_handle h, int64_t* entries, int64_t* contacts);
+
+/* Instances of a system (1 unless made by gdem_create_batch), or
+ * GDEM_ERR_INVALID for a null handle. */
+int gdem_num_instances(gdem_handle h);
 
 /* Particle count and device time of the last gdem_step in ms. */
 int64_t gdem_num_particles(gdem_handle h);
@@ -350,7 +388,8 @@ void gdem_adjoint_destroy(gdem_adjoint_handle h);
  * so n is limited to 1,048,576 (larger n returns GDEM_ERR_INVALID).  Calls
  * that overlap in time on one device race on that scratch.  The first call on
  * a device sets up the scratch address and should come before any stream
- * capture. */
+ * capture; the set-up is repeated when the device's context has changed
+ * since (after a cudaDeviceReset). */
 int gdem_speed_stats_static(const double* v, int64_t n, double* out, void* stream);
 
 #ifdef __cplusplus

@@ -2,22 +2,36 @@
 # Builds oracle/_ref/libgrains_ref.so: the Grains3D reference (GRAINS_V1/Grains
 # sources, compiled unmodified where they lie) + the single-rank MPI and
 # Xerces DOM stand-ins in oracle/shim/ + the step harness ref_harness.cpp.
-# TEST INFRASTRUCTURE: it pins the CPU restatement and produces the golden
-# vectors under tests/golden/.  Needs the reference tree (default
-# /root/reference); outputs go to oracle/_ref/ only.
+# TEST INFRASTRUCTURE: it pins the CPU restatement, produces the golden
+# vectors under tests/golden/ and is the timed CPU baseline.  Outputs go to
+# oracle/_ref/ only.
 #
-# Flags: -O2 -ffp-contract=off, x86-64 baseline ISA (no FMA), as the
-# reference's own g++ build on x86-64 (GRAINS_V1/Env, -O3 without -march).
+# Environment:
+#   GRAINS_REFERENCE  root of the PacIFiC checkout (the directory holding
+#                     GRAINS_V1/); default /root/reference
+#   GRAINS_REF_CXX    C++ compiler (default g++)
+#   JOBS              parallel compilations (default 8)
+#
+# Flags: -O3 as the reference's own GNU build (GRAINS_V1/Env/
+# grains-OpenMPI-2.1.1-GNU-9.4.0.env.sh: -O3 without -march, so the x86-64
+# baseline ISA and no FMA), plus -ffp-contract=off, which keeps every FP64
+# expression rounded in source order (the restatement and the device FP64
+# mode follow that order).  A change of flags rebuilds every object.
 set -e
 HERE=$(cd "$(dirname "$0")" && pwd)
 REF=${GRAINS_REFERENCE:-/root/reference}/GRAINS_V1/Grains
 OUT=$HERE/_ref
 JOBS=${JOBS:-8}
-[ -d "$REF" ] || { echo "reference tree not found: $REF" >&2; exit 1; }
+[ -d "$REF" ] || { echo "reference tree not found: $REF (set GRAINS_REFERENCE)" >&2; exit 1; }
 mkdir -p "$OUT/obj"
 # the system g++ (its libstdc++ is the shared one Python processes load)
 CXX=${GRAINS_REF_CXX:-g++}
-FLAGS="-std=c++17 -O2 -ffp-contract=off -fPIC -w -I$HERE/shim -I$REF/include"
+FLAGS="-std=c++17 -O3 -ffp-contract=off -fPIC -w -I$HERE/shim -I$REF/include"
+STAMP="$OUT/obj/flags"
+if [ ! -f "$STAMP" ] || [ "$(cat "$STAMP")" != "$CXX $FLAGS" ]; then
+  rm -f "$OUT"/obj/*.o
+  echo "$CXX $FLAGS" > "$STAMP"
+fi
 SRCS=$(ls "$REF"/Base/src/*.cpp "$REF"/Component/src/*.cpp "$REF"/Geometry/src/*.cpp \
           "$REF"/TimeIntegration/src/*.cpp "$REF"/XML/src/*.cpp "$REF"/PostProcessing/src/*.cpp \
           "$REF"/Fluid/src/*.cpp)

@@ -1308,6 +1308,12 @@ void or_get_basis(void* h, double* basis) {
     for (int k = 0; k < 9; ++k) basis[9 * i + k] = s.parts[i].basis[k];
 }
 
+// Polyhedron::m_curr_vertex of every particle (0 for other shapes).
+void or_get_curv(void* h, int* out) {
+  System& s = *static_cast<System*>(h);
+  for (size_t i = 0; i < s.parts.size(); ++i) out[i] = s.parts[i].curv;
+}
+
 void or_get_cells(void* h, int* ijk) {
   System& s = *static_cast<System*>(h);
   for (size_t i = 0; i < s.parts.size(); ++i)

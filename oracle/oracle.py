@@ -86,6 +86,7 @@ def _load():
         lib.or_step.restype = ctypes.c_int
         lib.or_get_state.argtypes = [V, D, D, D, D, D, D, D]
         lib.or_get_cells.argtypes = [V, I]
+        lib.or_get_curv.argtypes = [V, I]
         lib.or_get_basis.argtypes = [V, D]
         lib.or_get_grid.argtypes = [V, I, D, D]
         lib.or_num_contacts.argtypes = [V]
@@ -292,6 +293,12 @@ class Oracle:
         b = np.empty((self.n, 9))
         _load().or_get_basis(self._h, _dp(b))
         return b
+
+    def support_vertices(self):
+        """Each particle's polyhedron support vertex (Polyhedron::m_curr_vertex)."""
+        out = np.empty(self.n, np.int32)
+        _load().or_get_curv(self._h, _ip(out))
+        return out
 
     def cells(self):
         ijk = np.empty((self.n, 3), np.int32)

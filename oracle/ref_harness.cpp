@@ -15,6 +15,8 @@
 // computeParticlesForceAndTorque + setAllContactMapCumulativeFeaturesToZero;
 // a step is moveParticlesAndObstacles(dt/2, dt, dt),
 // computeParticlesForceAndTorque, advanceParticlesVelocity(dt/2).
+#include <cstdio>
+#include <exception>
 #include <fstream>
 #include <map>
 #include <vector>
@@ -130,6 +132,31 @@ class RefGrains : public Grains {
     return out;
   }
 
+  // A particle state read from a Format2024 particle file with the
+  // reference's own reload path (Grains::Construction, Grains.cpp:1024-1026:
+  // AllComponents::read_particles; Grains::InsertCreateNewParticles,
+  // :1970-1976: AllComponents::Link and, when periodic, checkClonesReload).
+  // The particles keep the forces and contact memory of the file, so the
+  // next step continues the leapfrog from there (a reload: no force
+  // initialisation).  Particle ID i + 1 is caller index i.
+  int load(const char* stem, int npart) {
+    m_allcomponents.read_particles(stem, (size_t)npart, m_collision, 0, 1, nullptr);
+    m_allcomponents.Link(*m_collision);
+    if (m_periodic) checkClonesReload();
+    m_allcomponents.computeNumberParticles(m_wrapper);
+    by_index.assign(npart, nullptr);
+    for (Particle* p : *m_allcomponents.getActiveParticles()) {
+      if (p->getTag() == 2) continue;
+      const int i = p->getID() - 1;
+      if (i < 0 || i >= npart) return 1;
+      id_to_index[p->getID()] = i;
+      by_index[i] = p;
+    }
+    for (Particle* p : by_index)
+      if (!p) return 1;
+    return 0;
+  }
+
   void addRawData(PostProcessingWriter* w) { m_allcomponents.addPostProcessingWriter(w); }
   void postProcessing(double time, bool start) {
     if (start)
@@ -140,6 +167,14 @@ class RefGrains : public Grains {
   void postProcessingEnd() { m_allcomponents.PostProcessing_end(); }
   void maxMeanVelocity(double& vmax, double& vmean) {
     m_allcomponents.ComputeMaxMeanVelocity(vmax, vmean, nullptr);
+  }
+  // the contact features Grains::do_after_time_stepping prints
+  // (Base/src/Grains.cpp:228-244)
+  void contactFeatures(double* out) {
+    out[0] = m_collision->getOverlapMax();
+    out[1] = m_collision->getOverlapMean();
+    out[2] = m_collision->getTimeOverlapMax();
+    out[3] = m_collision->getNbIterGJKMean();
   }
 
   int partnerIndex(int id) {
@@ -175,6 +210,20 @@ int ref_set_particles(void* h, int n, const int* type, const double* x, const do
 }
 
 int ref_init(void* h) { return static_cast<RefGrains*>(h)->init(); }
+// Reads "<stem>_Particles.result" for a reload name "<stem>.<ext>" (the
+// reference cuts the name at its first '.', so stem holds none), a particle
+// file in the Format2024 layout.
+int ref_load_particles(void* h, const char* stem, int npart) {
+  try {
+    return static_cast<RefGrains*>(h)->load(stem, npart);
+  } catch (std::exception const& e) {
+    std::fprintf(stderr, "ref_load_particles: %s\n", e.what());
+    return 2;
+  } catch (...) {
+    std::fprintf(stderr, "ref_load_particles: exception from the reference\n");
+    return 2;
+  }
+}
 int ref_step(void* h, int nsteps) { return static_cast<RefGrains*>(h)->step(nsteps); }
 
 void ref_get_state(void* h, double* x, double* v, double* w, double* q, double* F, double* T) {
@@ -309,6 +358,14 @@ void ref_rawdata_end(void* h) { static_cast<RefGrains*>(h)->postProcessingEnd();
 // the figures of the _VelocityMaxMean.dat lines.
 void ref_velocity_max_mean(void* h, double* vmax, double* vmean) {
   static_cast<RefGrains*>(h)->maxMeanVelocity(*vmax, *vmean);
+}
+
+// AppCollision's contact features (Base/src/AppCollision.cpp:159-179):
+// maximum overlap, mean overlap, time of the maximum, mean GJK iterations;
+// accumulated over every evaluation of the process (the reference keeps the
+// counters in function statics).
+void ref_contact_features(void* h, double* out) {
+  static_cast<RefGrains*>(h)->contactFeatures(out);
 }
 
 void ref_destroy(void* h) { delete static_cast<RefGrains*>(h); }

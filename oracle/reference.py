@@ -22,6 +22,12 @@ def available() -> bool:
     return LIB.exists()
 
 
+def tree_present() -> bool:
+    """The reference's sources are where build_ref.sh looks for them."""
+    root = Path(os.environ.get("GRAINS_REFERENCE", "/root/reference"))
+    return (root / "GRAINS_V1" / "Grains").is_dir()
+
+
 def build() -> Path:
     subprocess.run(["sh", str(HERE / "build_ref.sh")], check=True)
     return LIB
@@ -38,6 +44,8 @@ def _load():
         lib.ref_create.restype = V
         lib.ref_set_particles.argtypes = [V, ctypes.c_int, I, D, D, D, D]
         lib.ref_set_particles.restype = ctypes.c_int
+        lib.ref_load_particles.argtypes = [V, ctypes.c_char_p, ctypes.c_int]
+        lib.ref_load_particles.restype = ctypes.c_int
         lib.ref_init.argtypes = [V]
         lib.ref_init.restype = ctypes.c_int
         lib.ref_step.argtypes = [V, ctypes.c_int]
@@ -58,6 +66,7 @@ def _load():
         lib.ref_rawdata_write.restype = ctypes.c_int
         lib.ref_rawdata_end.argtypes = [V]
         lib.ref_velocity_max_mean.argtypes = [V, D, D]
+        lib.ref_contact_features.argtypes = [V, D]
         lib.ref_destroy.argtypes = [V]
         _lib = lib
     return _lib
@@ -88,6 +97,14 @@ class Reference:
         rc = _load().ref_set_particles(self._h, n, _ip(self._t), *[_dp(a) for a in arrs])
         self.n = n
         return rc
+
+    def load_particles(self, stem, n):
+        """Reads <stem>_Particles.result (a Format2024 particle file) through
+        the reference's own reload path; stem must hold no '.'."""
+        if "." in str(stem):
+            raise ValueError("the reference cuts the reload name at its first '.'")
+        self.n = n
+        return _load().ref_load_particles(self._h, os.fsencode(str(stem) + ".reload"), n)
 
     def init(self):
         return _load().ref_init(self._h)
@@ -140,6 +157,13 @@ class Reference:
         a, b = np.zeros(1), np.zeros(1)
         _load().ref_velocity_max_mean(self._h, _dp(a), _dp(b))
         return float(a[0]), float(b[0])
+
+    def contact_features(self):
+        """(overlap max, overlap mean, time of the max, mean GJK iterations)
+        over every evaluation of this process."""
+        out = np.zeros(4)
+        _load().ref_contact_features(self._h, _dp(out))
+        return out
 
     def history(self):
         lib = _load()

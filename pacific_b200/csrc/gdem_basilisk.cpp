@@ -12,7 +12,9 @@
 //   Init_Grains       the XML's system (FP64; GRAINS_B200_PRECISION=fp32split
 //                     selects the FP32-split mode) with the particles of its
 //                     Construction/Reload file (the "<stem>_Particles" file of
-//                     the Format2024 reload, AllComponents::read_particles),
+//                     the Format2024 reload, or "<stem>_Particles.bin" when the
+//                     reload's reading mode is Hybrid, AllComponents::read and
+//                     read_particles),
 //                     the fluid density in the weight and, with
 //                     b_fluidcorrectedacc, in the coupling factor
 //                     (GrainsCoupledWithFluid::do_before_time_stepping, :54-97).
@@ -75,25 +77,34 @@ std::string d16(double v) {
   return buf;
 }
 
-// The reference particle file's IDs (1-based, in particle-index order).
-bool readIds(const std::string& pfile) {
-  FILE* f = std::fopen(pfile.c_str(), "r");
+// The reading mode of a Format2024 reload file: the word after the
+// "NbFiles <n>" line, "Hybrid" or "Text" (AllComponents::write, Component/
+// src/AllComponents.cpp:1370-1374; AllComponents::read, :1114-1126).  Returns
+// false when the file cannot be read or has no such line.
+bool readReloadMode(const std::string& reload, bool& hybrid) {
+  FILE* f = std::fopen(reload.c_str(), "r");
   if (!f) return false;
-  std::vector<std::pair<int, int>> rec;   // (ID, class)
-  char line[1 << 16];
-  while (std::fgets(line, sizeof(line), f)) {
-    int cls, id, tag;
-    unsigned act;
-    if (std::sscanf(line, "%d %d %d %u", &cls, &id, &tag, &act) != 4) continue;
-    if (tag > 1 || !act) continue;
-    rec.push_back({id, cls});
+  char tok[4096];
+  bool found = false;
+  while (std::fscanf(f, "%4095s", tok) == 1) {
+    if (std::strcmp(tok, "NbFiles") != 0) continue;
+    long nfiles = 0;
+    if (std::fscanf(f, "%ld %4095s", &nfiles, tok) == 2) {
+      hybrid = std::strcmp(tok, "Hybrid") == 0;
+      found = true;
+    }
+    break;
   }
   std::fclose(f);
-  std::sort(rec.begin(), rec.end());
-  g_ids.clear();
-  g_class.clear();
-  for (auto const& r : rec) { g_ids.push_back(r.first); g_class.push_back(r.second); }
-  return true;
+  return found;
+}
+
+// Particle IDs (1-based) and classes, by particle index, from the handle.
+bool readIds() {
+  g_ids.assign((size_t)g_n, 0);
+  g_class.assign((size_t)g_n, 0);
+  return g_n == 0 || (gdem_download_ids(g_sys, g_ids.data()) == GDEM_OK &&
+                      gdem_download_classes(g_sys, g_class.data()) == GDEM_OK);
 }
 
 // Matrix::setRotation (Geometry/src/Matrix.cpp:114-127) of q = (x, y, z, w):
@@ -139,15 +150,27 @@ void Init_Grains(char const* inputfile, double fluid_rho, const bool b_restart,
     g_error = true;
     return;
   }
-  // AllComponents::read_particles: the reload name up to its first '.',
-  // then "_Particles"
+  // AllComponents::read_particles (:1152-1164): the reload name up to its
+  // first '.', then "_Particles", with ".bin" in the Hybrid reading mode
   std::string pfile(reload);
   const size_t dot = pfile.find_first_of('.');
   if (dot != std::string::npos) pfile.erase(dot);
   pfile += "_Particles";
-  if (gdem_read_reload_particles(g_sys, pfile.c_str()) != GDEM_OK) { fail("Init_Grains"); return; }
-  if (!readIds(pfile)) { fail("Init_Grains"); return; }
+  bool hybrid = false;
+  if (!readReloadMode(reload, hybrid)) {
+    // no reload header beside the particle file: the binary particle file
+    // alone means the Hybrid mode
+    FILE* ft = std::fopen(pfile.c_str(), "r");
+    FILE* fb = ft ? nullptr : std::fopen((pfile + ".bin").c_str(), "rb");
+    hybrid = fb != nullptr;
+    if (ft) std::fclose(ft);
+    if (fb) std::fclose(fb);
+  }
+  const int rc = hybrid ? gdem_read_reload_particles_hybrid(g_sys, (pfile + ".bin").c_str())
+                        : gdem_read_reload_particles(g_sys, pfile.c_str());
+  if (rc != GDEM_OK) { fail("Init_Grains"); return; }
   g_n = gdem_num_particles(g_sys);
+  if (!readIds()) { fail("Init_Grains"); return; }
   if (gdem_set_fluid(g_sys, fluid_rho, b_fluidcorrectedacc ? 1 : 0) != GDEM_OK) {
     fail("Init_Grains");
     return;
@@ -284,12 +307,27 @@ void UpdateVelocityGrains(double** arrayv, const int m) {
                          "different in UpdateVelocityGrains\n");
     if (m < g_n) return;
   }
+  // the particles' current velocities: a particle whose row is missing keeps
+  // its own
   std::vector<double> v(3 * g_n), w(3 * g_n);
+  if (gdem_download_state(g_sys, nullptr, v.data(), w.data(), nullptr, nullptr, nullptr,
+                          nullptr) != GDEM_OK) {
+    fail("UpdateVelocityGrains");
+    return;
+  }
+  int64_t missing = 0;
   for (int64_t i = 0; i < g_n; ++i) {
-    // row i belongs to the particle of ID i + 1 (GrainsCoupledWithFluid.cpp:1150)
-    const double* row = arrayv[g_ids[i] - 1];
+    // row i belongs to the particle of ID i + 1 (GrainsCoupledWithFluid.cpp:1150);
+    // an ID beyond the m rows the fluid sent has no row
+    const int row_index = g_ids[i] - 1;
+    if (row_index < 0 || row_index >= m) { ++missing; continue; }
+    const double* row = arrayv[row_index];
     for (int d = 0; d < 3; ++d) { v[3 * i + d] = row[d]; w[3 * i + d] = row[3 + d]; }
   }
+  if (missing)
+    std::fprintf(stderr, "WARNING: UpdateVelocityGrains: %lld particles have an ID beyond the %d "
+                         "rows of the fluid solver and keep their velocities\n",
+                 (long long)missing, m);
   if (gdem_set_velocities(g_sys, v.data(), w.data()) != GDEM_OK) fail("UpdateVelocityGrains");
 }
 

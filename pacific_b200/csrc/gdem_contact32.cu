@@ -263,12 +263,16 @@ __device__ __forceinline__ void contactLaw32(ModelDesc const& m, double dt, Cont
 
 // Lists a candidate when its bounding spheres are closer than the skin, with
 // a relative margin of 4e-6 that covers the FP32 rounding of the test.
-// The list of slot t; returns its number of upper entries.
+// kFill = false: returns the row length of slot t.  kFill = true: writes the
+// row (its length known from the counting pass), orders it and returns its
+// number of upper entries.
+template <bool kFill>
 __device__ __forceinline__ int listPairs32(DevState const& S, int t) {
   const int4 cc = S.cellc[t];
   GridDesc const& g = S.bgrids[cc.w];
   const float4 ha = S.offh[t];
-  int* out = S.pairs + (size_t)t * kPairCap;
+  int* out = kFill ? S.pairs + S.pair_off[t] : nullptr;
+  const int room = kFill ? S.npairs[t] : 0;
   int cnt = 0;
   const float4* __restrict__ offh = S.offh;
   const float ex = g.edge_f[0], ey = g.edge_f[1], ez = g.edge_f[2];
@@ -285,22 +289,27 @@ __device__ __forceinline__ int listPairs32(DevState const& S, int t) {
     float dz = fmaf(s * (float)dk, ez, h1.z - h0.z);
     float R = (h0.w + h1.w + g.skin_f) * (1.f + 4.e-6f);
     if (dx * dx + dy * dy + dz * dz > R * R) return;
-    if (cnt < kPairCap) out[cnt] = u | (shiftCode(sx, sy, sz) << 27);
+    if (kFill && cnt < room) out[cnt] = u | (shiftCode(sx, sy, sz) << 27);
     ++cnt;
   });
-  if (cnt > kPairCap) { raise(S.status, kErrPairsFull); cnt = kPairCap; }
-  const int nu = sortEntriesUpperFirst(out, cnt, S.id, S.id[t]);
-  S.npairs[t] = cnt;
-  return nu;
+  if (!kFill) return cnt;
+  return sortEntriesUpperFirst(out, min(cnt, room), S.id, S.id[t]);
 }
 
-__global__ void __launch_bounds__(256) k_pairs32(DevState S, const int* gate) {
+__global__ void __launch_bounds__(256) k_pairs_count32(DevState S, const int* gate) {
   if (gate && !*gate) return;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool valid = t < S.n;
-  const int nu = valid ? listPairs32(S, t) : 0;
+  if (t >= S.n) return;
+  S.npairs[t] = rowLength(S, listPairs32<false>(S, t));
+}
+
+__global__ void __launch_bounds__(256) k_pairs_fill32(DevState S, const int* gate) {
+  if (gate && !*gate) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = t < S.n && rowFits(S, t);
+  const int nu = valid ? listPairs32<true>(S, t) : 0;
   // each pair once, from its lower ID, into the compact list of the filter
-  appendUpperPairs(S, t, valid ? S.pairs + (size_t)t * kPairCap : S.pairs, nu, S.status);
+  appendUpperPairs(S, t, valid ? S.pairs + S.pair_off[t] : S.pairs, nu, S.status);
 }
 
 // One pair in the canonical orientation -- p0 (slot s0, the lower ID) at its
@@ -315,7 +324,8 @@ __global__ void __launch_bounds__(256) k_pairs32(DevState S, const int* gate) {
 // kernel, whose registers it would triple).
 template <bool kConvex>
 __device__ __forceinline__ bool evalPair32(DevState const& S, GridDesc const& g, int s0, int s1,
-                                           int id0, int id1, TypeDesc const& tp0,
+                                           int prio0, int prio1, int id0, int id1,
+                                           TypeDesc const& tp0,
                                            TypeDesc const& tp1, d3 x0, d3 x1, d3 v0, d3 v1,
                                            d3 w0, d3 w1, bool insert, int& nlaw, int& nre,
                                            GjkTally& gjk, double& delta, float3& f, float3& c0,
@@ -326,10 +336,15 @@ __device__ __forceinline__ bool evalPair32(DevState const& S, GridDesc const& g,
   if (!kConvex || (tp0.shape == 0 && tp1.shape == 0)) {
     ct = sphereSphere64(x0, tp0.radius, tp0.crust, x1, tp1.radius, tp1.crust);
   } else {
-    ct = convexContact64(convexOf(tp0, S.poly_verts),
-                         crustXForm(S.basis, cap, s0, tp0.scaling, x0), tp0.radius, tp0.crust,
-                         convexOf(tp1, S.poly_verts),
-                         crustXForm(S.basis, cap, s1, tp1.scaling, x1), tp1.radius, tp1.crust);
+    int c0v = startVertex(S, tp0, s0), c1v = startVertex(S, tp1, s1);
+    ct = convexContact64(convexOf(tp0, S), crustXForm(S.basis, cap, s0, tp0.scaling, x0),
+                         tp0.radius, tp0.crust, convexOf(tp1, S),
+                         crustXForm(S.basis, cap, s1, tp1.scaling, x1), tp1.radius, tp1.crust,
+                         c0v, c1v);
+    if (ct.gjk_iters > 0) {
+      recordVertex(S, tp0, s0, prio0, c0v);
+      recordVertex(S, tp1, s1, prio1, c1v);
+    }
     if (insert) gjk.add(ct.gjk_iters);   // each pair counted once
   }
   delta = ct.contact && ct.dist < 0. ? ct.dist : __longlong_as_double(0x7ff0000000000000ll);
@@ -345,13 +360,20 @@ __device__ __forceinline__ bool evalPair32(DevState const& S, GridDesc const& g,
   int re;
   if (insert) ++nlaw;   // each pair counted once, by its lower ID
   if (m.memory) {
-    const unsigned long long key = pairKey(id0, id1);
+    // the table holds the lower ID's view; p0 may be the higher ID (the
+    // reference's pair orientation), whose view is the negation
+    const bool flip = id0 > id1;
+    const unsigned long long key = pairKey(min(id0, id1), max(id0, id1));
     int old = histFind(S.hist_old, key, tag_old);
-    if (old >= 0) loadHistF(S.hist_old, old, kd, pn, sp);
+    if (old >= 0) {
+      loadHistF(S.hist_old, old, kd, pn, sp);
+      if (flip) { kd = -kd; pn = -pn; sp = -sp; }
+    }
     contactLaw32(m, S.dt, ct, b0, b1, old >= 0, kd, pn, sp, f, mr, re);
     if (insert) {
       int slot = histInsert(S.hist_new, key, tag);
       if (slot < 0) raise(S.status, kErrHashFull);
+      else if (flip) storeHistF(S.hist_new, slot, -kd, -pn, -sp);
       else storeHistF(S.hist_new, slot, kd, pn, sp);
     }
   } else {
@@ -365,112 +387,49 @@ __device__ __forceinline__ bool evalPair32(DevState const& S, GridDesc const& g,
   return true;
 }
 
-// Position in slot t's list of the entry whose partner is slot u.
-__device__ __forceinline__ int findEntry(DevState const& S, int t, int u) {
-  const int n = S.npairs[t];
-  const int* seg = S.pairs + (size_t)t * kPairCap;
-  for (int e = 0; e < n; ++e)
-    if ((int)((unsigned)seg[e] & ((1u << 27) - 1u)) == u) return e;
-  return -1;
+// One side of a pair in contact, as the leapfrog kernel adds it: the force
+// on the row's particle with the evaluation tag in its fourth word, then the
+// torque (lever arm x force, plus the rolling torque).
+__device__ __forceinline__ void storeShare32(DevState const& S, int64_t entry, int tag, float3 f,
+                                             float3 c) {
+  float4* sh = static_cast<float4*>(S.share) + 2 * entry;
+  sh[0] = make_float4(f.x, f.y, f.z, __int_as_float(tag));
+  sh[1] = make_float4(c.x, c.y, c.z, 0.f);
 }
 
-// One side's share of a pair (two-phase path): force and torque terms in the
-// order the per-particle sum adds them.
-struct PairShare32 { float f[3], c[3], mr[3]; };
-
-// Forces and torques on particle t.  kSums (two-phase path, systems with
-// convex bodies): the pairs were evaluated once each by k_pairforces32, and
-// each kept entry's share is read back; otherwise both partners of a pair
-// evaluate it, with identical operands, and the lower ID writes the history.
-// Either way the shares are added in list order, then the walls.
-template <bool kConvex, bool kSums>
-__device__ __forceinline__ void forcesOn32(DevState const& S, int t, int na, int sparse,
-                                           int& nlaw, int& nre, GjkTally& gjk) {
+// The wall contacts of particle t (near a wall per the contact filter): the
+// geometry from the FP64 position, the force law in FP32 (FP64 when
+// ill-conditioned); their sum is the particle's wall share.
+template <bool kConvex>
+__device__ __forceinline__ void wallsOf32(DevState const& S, int t, int tag, int& nlaw, int& nre,
+                                          GjkTally& gjk, StatsTally& st) {
   const int cap = S.cap;
-  const int4 cc = S.cellc[t];
-  GridDesc const& g = S.grids[cc.w];
-  const unsigned tag = (unsigned)S.ctl[kCtlEpoch], tag_old = tag - 1u;
+  const int inst = S.inst[t];
+  GridDesc const& g = S.grids[inst];
+  const unsigned utag = (unsigned)tag, tag_old = utag - 1u;
   const int ida = S.id[t];
   TypeDesc const& ta = S.types[S.type[t]];
   const d3 xt = ld3(S.x, cap, t), vt = ld3(S.v, cap, t), wt = ld3(S.w, cap, t);
-  float3 Fs = f3(0.f, 0.f, 0.f), Ts = f3(0.f, 0.f, 0.f);
-  // the pair-list entries that pass the contact filter's test
-  const int np = (!sparse || (na & kHasPair)) ? S.npairs[t] : 0;
-  const int* seg = S.pairs + (size_t)t * kPairCap;
-  GridDesc const& bg = S.bgrids[cc.w];
-  const float4 pt = S.posf[t];
-  for (int e0 = 0; e0 < np; e0 += kProbe) {
-    unsigned keep = probeEntries(S, bg, pt, seg, e0, np);
-    if (S.diag)
-      for (int e = e0; e < min(e0 + kProbe, np); ++e)
-        if (!(keep >> (e - e0) & 1u))
-          S.pair_delta[(size_t)t * kPairCap + e] = __longlong_as_double(0x7ff0000000000000ll);
-    // the kept entries in list order; lane by lane the k-th kept entries run
-    // together, as the warp's lanes hold different particles
-    while (keep) {
-      const int e = e0 + __ffs(keep) - 1;
-      keep &= keep - 1u;
-      if constexpr (kSums) {
-        const PairShare32 r = reinterpret_cast<const PairShare32*>(S.pshare)[S.eslot[(size_t)t * kPairCap + e]];
-        Fs = Fs + f3(r.f[0], r.f[1], r.f[2]);
-        Ts = Ts + f3(r.c[0], r.c[1], r.c[2]);
-        Ts = Ts + f3(r.mr[0], r.mr[1], r.mr[2]);
-        continue;
-      }
-      const uint32_t ent = (uint32_t)seg[e];
-      const int u = (int)(ent & ((1u << 27) - 1));
-      const int idb = S.id[u];
-      const bool t0 = ida < idb;
-      TypeDesc const& tb = S.types[S.type[u]];
-      // lower ID at its own position, the other at its periodic image seen
-      // from it
-      int sh[3];
-      entryShift(S, ent, t, u, sh);
-      const d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
-      // (the partner's velocities are loaded with its position: a kept entry
-      // is nearly always a contact, and the loads then overlap)
-      const d3 xu = ld3(S.x, cap, u), vu = ld3(S.v, cap, u), wu = ld3(S.w, cap, u);
-      float3 f, c0, c1, mr;
-      double dl;
-      bool rolling;
-      const bool hit = evalPair32<kConvex>(
-          S, g, t0 ? t : u, t0 ? u : t, t0 ? ida : idb, t0 ? idb : ida, t0 ? ta : tb,
-          t0 ? tb : ta, t0 ? xt : xu, t0 ? xu + shift : xt + (-shift), t0 ? vt : vu,
-          t0 ? vu : vt, t0 ? wt : wu, t0 ? wu : wt, t0, nlaw, nre, gjk, dl, f, c0, c1, mr,
-          rolling);
-      if (S.diag) {
-        S.pair_delta[(size_t)t * kPairCap + e] = dl;
-        if (hit) {
-          double* fd = S.pair_force + 3 * ((size_t)t * kPairCap + e);
-          fd[0] = f.x; fd[1] = f.y; fd[2] = f.z;
-        }
-      }
-      if (!hit) continue;
-      if (t0) {
-        Fs = Fs + f;
-        Ts = Ts + c0;
-        if (rolling) Ts = Ts + mr;
-      } else {
-        Fs = Fs - f;
-        Ts = Ts - c1;
-        if (rolling) Ts = Ts - mr;
-      }
-    }
-  }
-  // walls: geometry from the FP64 master position, force law in FP32
-  const int nwalls = (!sparse || (na & kNearWall)) ? g.wall_count : 0;
-  for (int k = 0; k < nwalls; ++k) {
+  float3 Fw = f3(0.f, 0.f, 0.f), Tw = f3(0.f, 0.f, 0.f);
+  bool any = false;
+  // the particle's polyhedron vertex runs through its wall calls in order
+  int curw = kConvex ? startVertex(S, ta, t) : 0;
+  bool walls_gjk = false;
+  for (int k = 0; k < g.wall_count; ++k) {
     WallDesc const& wd = S.walls[g.wall_begin + k];
+    int cw = 0;
     Contact64 ct = (!kConvex || ta.shape == 0)
         ? sphereWall64(xt, ta.radius, ta.crust, wd)
-        : convexContact64(convexOf(ta, S.poly_verts), crustXForm(S.basis, cap, t, ta.scaling, xt),
+        : convexContact64(convexOf(ta, S), crustXForm(S.basis, cap, t, ta.scaling, xt),
                           ta.radius, ta.crust, convexOf(wd),
                           identityXForm(wd.scaling, mk(wd.centre[0], wd.centre[1], wd.centre[2])),
-                          wd.radius, wd.crust);
+                          wd.radius, wd.crust, curw, cw);
     if (kConvex) gjk.add(ct.gjk_iters);
+    if (kConvex && ct.gjk_iters > 0) walls_gjk = true;
     if (S.diag) S.wall_delta[(size_t)t * S.max_walls + k] = ct.contact ? ct.dist : __longlong_as_double(0x7ff0000000000000ll);
     if (ct.error) raise(S.status, kErrContactOverlap);
     if (!ct.contact || !(ct.dist < 0.)) continue;
+    st.add(ct.dist);
     ModelDesc const& m = S.models[g.model_base + ta.mat * kMaxMat + wd.mat];
     const float3 lev0 = tof(ct.point - xt);
     const d3 zero = mk(0., 0., 0.);
@@ -484,7 +443,7 @@ __device__ __forceinline__ void forcesOn32(DevState const& S, int t, int na, int
       int old = histFind(S.hist_old, key, tag_old);
       if (old >= 0) loadHistF(S.hist_old, old, kd, pn, sp);
       contactLaw32(m, S.dt, ct, b0, b1, old >= 0, kd, pn, sp, f, mr, re);
-      int slot = histInsert(S.hist_new, key, tag);
+      int slot = histInsert(S.hist_new, key, utag);
       if (slot < 0) raise(S.status, kErrHashFull);
       else storeHistF(S.hist_new, slot, kd, pn, sp);
     } else {
@@ -495,100 +454,96 @@ __device__ __forceinline__ void forcesOn32(DevState const& S, int t, int na, int
       double* fd = S.wall_force + 3 * ((size_t)t * S.max_walls + k);
       fd[0] = f.x; fd[1] = f.y; fd[2] = f.z;
     }
-    Fs = Fs + f;
-    Ts = Ts + crossf(lev0, f);
-    if (m.rolling) Ts = Ts + mr;
+    Fw = Fw + f;
+    Tw = Tw + crossf(lev0, f);
+    if (m.rolling) Tw = Tw + mr;
+    any = true;
   }
-  const d3 F = mk(ta.weight[0] + (double)Fs.x, ta.weight[1] + (double)Fs.y,
-                  ta.weight[2] + (double)Fs.z);
-  const d3 T = mk((double)Ts.x, (double)Ts.y, (double)Ts.z);
-  st3(S.F, cap, t, F);
-  st3(S.T, cap, t, T);
+  if (walls_gjk) recordVertex(S, ta, t, kWallPriority, curw);
+  if (!any) return;
+  float4* ws = static_cast<float4*>(S.wshare) + 2 * (size_t)t;
+  ws[0] = make_float4(Fw.x, Fw.y, Fw.z, 0.f);
+  ws[1] = make_float4(Tw.x, Tw.y, Tw.z, 0.f);
+  atomicOr(reinterpret_cast<unsigned*>(&contactFlags(S)[t]), kNearWall);
 }
 
-// Persistent grid.  sparse: only the particles of the work list (those with
-// a listed contact or near a wall); the others keep their weight, which
-// k_move applies without reading F, T.  Otherwise every particle.
-template <bool kConvex, bool kSums>
-__global__ void __launch_bounds__(256) k_forces32(DevState S, int sparse) {
-  const int stride = gridDim.x * blockDim.x;
-  pdlWait();      // the contact filter's work list and flags
-  pdlTrigger();   // the move kernel may be scheduled; it waits for this one
-  const int nw = sparse ? S.ctl[kCtlWork] : S.n;
-  const int* flags = contactFlags(S);
-  int nlaw = 0, nre = 0;   // contacts evaluated / re-evaluated in FP64
-  GjkTally gjk;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += stride) {
-    const int t = sparse ? S.work[i] : i;
-    forcesOn32<kConvex, kSums>(S, t, flags[t], sparse, nlaw, nre, gjk);
-  }
-  if constexpr (kConvex) gjk.flush(S.gjk_counts);
-  // warp-aggregated counters of the FP64 re-evaluations (every lane of the
-  // warp reaches this point: no thread leaves the loop early)
-  const int wl = __reduce_add_sync(0xffffffffu, nlaw), wr = __reduce_add_sync(0xffffffffu, nre);
-  if ((threadIdx.x & 31) == 0 && wl) {
-    atomicAdd(S.law_counts, (unsigned long long)wl);
-    if (wr) atomicAdd(S.law_counts + 1, (unsigned long long)wr);
-  }
-}
-
-// First phase of the two-phase force path (systems with convex bodies):
-// each pair kept by the contact filter is evaluated once, by one thread -- a
-// GJK pair is far more work than the sum that follows -- and its two shares
-// are written for the partners' sums (forcesOn32 with kSums).  The pair is
-// seen from its lower ID (an upper entry), which writes the history, as in
-// the one-phase path, so both paths give the same forces.
+// One pair kept by the contact filter (compact pair c), seen from its lower
+// ID, which writes the history: exact narrow phase, force law, and for a
+// contact its two shares written into the rows of both partners and their
+// entry bits set.  The leapfrog kernel adds each particle's shares in row
+// order, so the sums are deterministic and need no float atomics.
 template <bool kConvex>
-__global__ void __launch_bounds__(128) k_pairforces32(DevState S) {
-  pdlWait();      // the contact filter's kept pairs
-  pdlTrigger();   // the force sums may be scheduled; they wait for this kernel
-  const int nk = S.ctl[kCtlKept];
-  const int stride = gridDim.x * blockDim.x;
+__device__ __forceinline__ void pairItem32(DevState const& S, int c, int tag, int& nlaw, int& nre,
+                                           GjkTally& gjk, StatsTally& st) {
   const int cap = S.cap;
-  int nlaw = 0, nre = 0;
-  GjkTally gjk;
-  PairShare32* share = static_cast<PairShare32*>(S.pshare);
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nk; k += stride) {
-    const int2 pr = S.upairs[S.kept[k]];
-    const int t = pr.x;
-    const unsigned ent = (unsigned)pr.y;
-    const int u = (int)(ent & ((1u << 27) - 1u));
-    const int et = findEntry(S, t, u), eu = findEntry(S, u, t);
-    GridDesc const& g = S.grids[S.inst[t]];
-    int sh[3];
-    entryShift(S, ent, t, u, sh);
-    const d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
-    const d3 xt = ld3(S.x, cap, t), xu = ld3(S.x, cap, u);
-    float3 f, c0, c1, mr;
-    double dl;
-    bool rolling;
-    const bool hit = evalPair32<kConvex>(
-        S, g, t, u, S.id[t], S.id[u], S.types[S.type[t]], S.types[S.type[u]], xt, xu + shift,
-        ld3(S.v, cap, t), ld3(S.v, cap, u), ld3(S.w, cap, t), ld3(S.w, cap, u), true, nlaw, nre,
-        gjk, dl, f, c0, c1, mr, rolling);
-    PairShare32 a, b;
-    const float3 zero = f3(0.f, 0.f, 0.f);
-    const float3 fa = hit ? f : zero, ca = hit ? c0 : zero, ma = hit ? mr : zero;
-    const float3 fb = hit ? -f : zero, cb = hit ? -c1 : zero, mb = hit ? -mr : zero;
-    a.f[0] = fa.x; a.f[1] = fa.y; a.f[2] = fa.z; a.c[0] = ca.x; a.c[1] = ca.y; a.c[2] = ca.z;
-    a.mr[0] = ma.x; a.mr[1] = ma.y; a.mr[2] = ma.z;
-    b.f[0] = fb.x; b.f[1] = fb.y; b.f[2] = fb.z; b.c[0] = cb.x; b.c[1] = cb.y; b.c[2] = cb.z;
-    b.mr[0] = mb.x; b.mr[1] = mb.y; b.mr[2] = mb.z;
-    share[2 * k] = a;
-    share[2 * k + 1] = b;
-    if (et >= 0) S.eslot[(size_t)t * kPairCap + et] = 2 * k;
-    if (eu >= 0) S.eslot[(size_t)u * kPairCap + eu] = 2 * k + 1;
-    if (S.diag) {
-      for (int side = 0; side < 2; ++side) {
-        const int s = side ? u : t, e = side ? eu : et;
-        if (e < 0) continue;
-        S.pair_delta[(size_t)s * kPairCap + e] = dl;
-        if (hit) {
-          double* fd = S.pair_force + 3 * ((size_t)s * kPairCap + e);
-          fd[0] = f.x; fd[1] = f.y; fd[2] = f.z;
-        }
+  const int2 pr = S.upairs[c];
+  const int ep = S.epos[c];
+  const int t = pr.x;
+  const unsigned ent = (unsigned)pr.y;
+  const int u = (int)(ent & ((1u << 27) - 1u));
+  const int et = ep & 0xFFFF, eu = (int)((unsigned)ep >> 16);
+  GridDesc const& g = S.grids[S.inst[t]];
+  int sh[3];
+  entryShift(S, ent, t, u, sh);
+  const d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
+  const d3 xt = ld3(S.x, cap, t), xu = ld3(S.x, cap, u);
+  // p0 as in the reference (flip: u is p0, at its own position)
+  const bool flip = referenceFlip(g, xt, xu, sh);
+  const int a = flip ? u : t, b = flip ? t : u;
+  const int pa = min((flip ? eu : et) + 1, kWallPriority - 1),
+            pb = min((flip ? et : eu) + 1, kWallPriority - 1);
+  float3 f, c0, c1, mr;
+  double dl;
+  bool rolling;
+  const bool hit = evalPair32<kConvex>(
+      S, g, a, b, pa, pb, S.id[a], S.id[b], S.types[S.type[a]], S.types[S.type[b]],
+      flip ? xu : xt, flip ? xt + (-shift) : xu + shift, ld3(S.v, cap, a), ld3(S.v, cap, b),
+      ld3(S.w, cap, a), ld3(S.w, cap, b), true, nlaw, nre, gjk, dl, f, c0, c1, mr, rolling);
+  const int64_t rt = (int64_t)S.pair_off[t] + et, ru = (int64_t)S.pair_off[u] + eu;
+  // force on t (the lower ID) and the two torques
+  const float3 mt = rolling ? mr : f3(0.f, 0.f, 0.f);
+  const float3 ft = flip ? -f : f;
+  const float3 tt = flip ? -(c1 + mt) : c0 + mt, tu = flip ? c0 + mt : -(c1 + mt);
+  if (S.diag) {
+    S.pair_delta[rt] = dl;
+    if (eu != 0xFFFF) S.pair_delta[ru] = dl;
+    if (hit) {
+      double* fd = S.pair_force + 3 * rt;
+      fd[0] = ft.x; fd[1] = ft.y; fd[2] = ft.z;
+      if (eu != 0xFFFF) {
+        fd = S.pair_force + 3 * ru;
+        fd[0] = ft.x; fd[1] = ft.y; fd[2] = ft.z;
       }
     }
+  }
+  if (!hit) return;
+  st.add(dl);
+  int* flags = contactFlags(S);
+  storeShare32(S, rt, tag, ft, tt);
+  atomicOr(reinterpret_cast<unsigned*>(&flags[t]), entryBit(et));
+  if (eu != 0xFFFF) {
+    storeShare32(S, ru, tag, -ft, tu);
+    atomicOr(reinterpret_cast<unsigned*>(&flags[u]), entryBit(eu));
+  }
+}
+
+// The pair kernel of an evaluation, one thread per item over a persistent
+// grid: first the pairs the contact filter kept, then the particles near a
+// wall.  Its trigger comes after its wait, so the leapfrog kernel, which
+// starts at the trigger, sees the filter's candidate marks complete.
+template <bool kConvex>
+__global__ void __launch_bounds__(128) k_pairlaw32(DevState S) {
+  pdlWait();      // the contact filter's lists
+  pdlTrigger();   // the leapfrog kernel may start; its candidates wait for this kernel
+  const int nk = S.ctl[kCtlKept], nw = S.ctl[kCtlWork];
+  const int tag = S.ctl[kCtlEpoch];
+  const int stride = gridDim.x * blockDim.x;
+  int nlaw = 0, nre = 0;   // contacts evaluated / re-evaluated in FP64
+  GjkTally gjk;
+  StatsTally st;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nk + nw; i += stride) {
+    if (i < nk) pairItem32<kConvex>(S, S.kept[i], tag, nlaw, nre, gjk, st);
+    else wallsOf32<kConvex>(S, S.work[i - nk], tag, nlaw, nre, gjk, st);
   }
   // warp-aggregated counters (every lane of the warp reaches this point)
   const int wl = __reduce_add_sync(0xffffffffu, nlaw), wr = __reduce_add_sync(0xffffffffu, nre);
@@ -597,23 +552,21 @@ __global__ void __launch_bounds__(128) k_pairforces32(DevState S) {
     if (wr) atomicAdd(S.law_counts + 1, (unsigned long long)wr);
   }
   if constexpr (kConvex) gjk.flush(S.gjk_counts);
+  st.flush(S.cstats, tag);
 }
 
 }  // namespace
 
-void launch_pairs32(DevState const& S, const int* gate, cudaStream_t st) {
-  if (S.n) k_pairs32<<<(S.n + 255) / 256, 256, 0, st>>>(S, gate);
-}
-void launch_forces32(DevState const& S, int sparse, cudaStream_t st) {
+void launch_pairs32(DevState const& S, const int* gate, int fill, cudaStream_t st) {
   if (!S.n) return;
-  const int grid = std::min((S.n + 255) / 256, (S.forces_bps > 0 ? S.forces_bps : 4) * S.nsm);
-  if (S.any_convex) {
-    // two phases: each kept pair once, then the sums
-    launchAfterPrevious(k_pairforces32<true>, 4 * S.nsm, 128, st, S);
-    launchAfterPrevious(k_forces32<true, true>, grid, 256, st, S, sparse);
-  } else {
-    launchAfterPrevious(k_forces32<false, false>, grid, 256, st, S, sparse);
-  }
+  if (fill) k_pairs_fill32<<<(S.n + 255) / 256, 256, 0, st>>>(S, gate);
+  else k_pairs_count32<<<(S.n + 255) / 256, 256, 0, st>>>(S, gate);
+}
+void launch_pairlaw32(DevState const& S, cudaStream_t st) {
+  if (!S.n) return;
+  const int grid = (S.forces_bps > 0 ? S.forces_bps : 4) * S.nsm;
+  if (S.any_convex) launchAfterPrevious(k_pairlaw32<true>, grid, 128, st, S);
+  else launchAfterPrevious(k_pairlaw32<false>, grid, 128, st, S);
 }
 
 }  // namespace gdem

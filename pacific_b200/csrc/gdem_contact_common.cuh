@@ -36,6 +36,40 @@ struct GjkTally {
   }
 };
 
+// Overlap statistics of one thread's contacts (AppCollision::
+// addToContactsFeatures, Base/src/AppCollision.cpp:159-179), flushed once
+// per warp into the system's ContactStats.
+struct StatsTally {
+  double sum = 0., mx = 0.;
+  int count = 0;
+  __device__ __forceinline__ void add(double dist) {
+    const double o = -dist;
+    sum += o;
+    mx = fmax(mx, o);
+    ++count;
+  }
+  // every lane of the warp calls this
+  __device__ __forceinline__ void flush(ContactStats* cs, int epoch) const {
+    const unsigned full = 0xffffffffu;
+    const int c = __reduce_add_sync(full, count);
+    if (!c || !cs) return;
+    double s = sum, m = mx;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s += __shfl_down_sync(full, s, o);
+      m = fmax(m, __shfl_down_sync(full, m, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(&cs->sum, s);
+      atomicAdd(&cs->count, (unsigned long long)c);
+      const unsigned long long bits = (unsigned long long)__double_as_longlong(m);
+      // the first evaluation at which the largest overlap was reached: later
+      // evaluations only write when they exceed it
+      if (atomicMax(&cs->max_bits, bits) < bits) cs->max_epoch = epoch;
+    }
+  }
+};
+
 // ClosestPointSPHERESPHERE (Geometry/src/RigidBodyWithCrust.cpp:596-639).
 // On overlap >= crustA + crustB the reference retries with a 10x crust
 // shrink (ClosestPoint_ErreurHandling, :534-588): for spheres the imposed
@@ -176,9 +210,10 @@ __device__ __forceinline__ Contact64 sphereWall64(d3 xa, double ra, double ca, W
 // witness direction, contact at the witness midpoint.  A GJK distance below
 // 1e-10 is the reference's ContactError (it then retries with a 10x crust
 // shrink); here it raises the overlap status and no force is applied.
+// curA, curB: the bodies' current polyhedron vertices (updated by the GJK).
 __device__ inline Contact64 convexContact64(ConvexRef const& a, XForm64 const& a2w, double Ra,
                                             double ca, ConvexRef const& b, XForm64 const& b2w,
-                                            double Rb, double cb) {
+                                            double Rb, double cb, int& curA, int& curB) {
   Contact64 c;
   c.contact = false;
   c.error = false;
@@ -187,7 +222,7 @@ __device__ inline Contact64 convexContact64(ConvexRef const& a, XForm64 const& a
   if (!(norm(gg) < Ra + Rb)) return c;
   d3 pA, pB;
   int it = 0;
-  double distance = closestPoints64(a, a2w, b, b2w, pA, pB, &it);
+  double distance = closestPoints64(a, a2w, b, b2w, pA, pB, &it, curA, curB);
   c.gjk_iters = it;
   if (distance < 1.0e-10) { c.error = true; return c; }
   d3 ba = pA - pB;
@@ -205,14 +240,20 @@ __device__ inline Contact64 convexContact64(ConvexRef const& a, XForm64 const& a
   return c;
 }
 
-__device__ __forceinline__ ConvexRef convexOf(TypeDesc const& t, const double* verts) {
+__device__ __forceinline__ ConvexRef convexOf(TypeDesc const& t, const double* verts,
+                                              const int* adj_off, const int* adj) {
   ConvexRef r;
   r.kind = t.shape;
   r.radius = t.radius;
   r.extent = mk(t.extent[0], t.extent[1], t.extent[2]);
   r.verts = verts ? verts + 3 * t.poly_begin : nullptr;
   r.nverts = t.poly_count;
+  r.adj_off = adj_off ? adj_off + t.poly_begin : nullptr;
+  r.adj = adj;
   return r;
+}
+__device__ __forceinline__ ConvexRef convexOf(TypeDesc const& t, DevState const& S) {
+  return convexOf(t, S.poly_verts, S.poly_adj_off, S.poly_adj);
 }
 __device__ __forceinline__ ConvexRef convexOf(WallDesc const& w) {
   ConvexRef r;
@@ -221,7 +262,49 @@ __device__ __forceinline__ ConvexRef convexOf(WallDesc const& w) {
   r.extent = mk(w.extent[0], w.extent[1], w.extent[2]);
   r.verts = nullptr;
   r.nverts = 0;
+  r.adj_off = nullptr;
+  r.adj = nullptr;
   return r;
+}
+
+// Which partner the reference takes as p0 (the body whose InterAction runs)
+// for a pair t, u (t the lower ID) without a periodic image shift: its force
+// loop (LinkedCell::ComputeForces, Base/src/LinkedCell.cpp:1019-1103) takes
+// each particle with the later particles of its own cell and the particles of
+// the 13 cells of its contact neighbourhood (setCellContactNeighborhood,
+// :958-984), which are exactly the adjacent cells with a larger cell number
+// (j nbk nbi + k nbi + i); within a cell the earlier particle of the cell's
+// list, which is the lower ID after a reload.  Returns true when u is p0.
+// The contact law is evaluated with the reference's p0 so that its FP64
+// result has the reference's rounding.
+__device__ __forceinline__ int referenceCellNumber(GridDesc const& g, d3 x) {
+  const int i = (int)floor((x.x - g.lc_origin[0]) / g.edge[0]);
+  const int j = (int)floor((x.y - g.lc_origin[1]) / g.edge[1]);
+  const int k = (int)floor((x.z - g.lc_origin[2]) / g.edge[2]);
+  return j * g.nb[2] * g.nb[0] + k * g.nb[0] + i;
+}
+__device__ __forceinline__ bool referenceFlip(GridDesc const& g, d3 xt, d3 xu, const int* sh) {
+  // across a periodic boundary the reference pairs a particle with the other's
+  // clone in its ghost cells; there the lower ID stays p0
+  if (sh[0] | sh[1] | sh[2]) return false;
+  return referenceCellNumber(g, xu) < referenceCellNumber(g, xt);
+}
+
+// The current polyhedron vertex of the particle in slot s at the start of
+// this evaluation (Polyhedron::m_curr_vertex), and the record of the one a
+// GJK call left: of all the calls of an evaluation on one particle, the one
+// of its last row entry (priority = entry + 1, below kWallPriority) or of its
+// walls (after every entry) is kept, so the choice does not depend on the
+// order in which the calls run; the leapfrog kernel makes it the current
+// vertex.
+__device__ __forceinline__ int startVertex(DevState const& S, TypeDesc const& t, int s) {
+  return t.shape == 2 ? S.curv[s] : 0;
+}
+constexpr int kWallPriority = 0x7FFF;
+__device__ __forceinline__ void recordVertex(DevState const& S, TypeDesc const& t, int s,
+                                             int priority, int vertex) {
+  if (t.shape == 2)
+    atomicMax(&S.curv_next[s], (priority << 16) | (vertex & 0xFFFF));
 }
 
 // HookeMemoryContactForceModel::computeTangentialVector (:54-65)

@@ -88,6 +88,19 @@ __device__ inline int histInsert(HistTable const& t, unsigned long long base, un
   return -1;
 }
 
+// Overlap statistics of the contacts over the evaluations since the last
+// reset (AppCollision::addToContactsFeatures, Base/src/AppCollision.cpp:
+// 159-179): the sum and the count of |overlap| over the contacts (pairs and
+// walls, each once per evaluation), the largest |overlap| (its FP64 bits:
+// non-negative doubles order like their bit patterns) and the evaluation
+// counter at which it was first reached.
+struct ContactStats {
+  double sum;
+  unsigned long long count;
+  unsigned long long max_bits;
+  long long max_epoch;
+};
+
 // Whole device state of one batch of instances.  Per-particle arrays are in
 // the current sorted (cell) order; component d of particle s of an n-vector
 // field lives at [d * cap + s] (structure of arrays).
@@ -124,24 +137,33 @@ struct DevState {
   double4* omg64;         // w (space frame), equivalent radius
   float4* offh;           // FP32 cell-relative offset; FP32 radius
   int4* cellc;            // pair-list cell i, j, k and instance at the last rebuild
-  // pair list: per-particle segments of kPairCap entries
-  int* pairs; int* npairs;   // skin list (rebuilt on demand)
+  // skin pair list, compressed rows: the entries of slot t are
+  // pairs[pair_off[t] .. pair_off[t] + npairs[t]), pair_off the exclusive
+  // scan of npairs; pair_cap entries are allocated (kCtlEntries holds the
+  // total of the last rebuild)
+  int* pairs; int* npairs; int* pair_off;
+  int pair_cap;
+  int* pair_scan_tmp;     // tile sums of the pair-count scan
   double* hydro;          // coupled runs: hydrodynamic force and torque by particle ID (6 each), or null
   int2* upairs;           // compact pair list: (slot, entry) of every upper entry, ctl[kCtlPairs] of them
-  // two-phase force path (systems with convex bodies; null otherwise)
+  int* epos;              // per compact pair: position of the pair in its two rows, e_t | e_u << 16
   int* kept;              // compact-list indices of the pairs kept by the filter, ctl[kCtlKept]
-  int* eslot;             // per list entry: index of its share in pshare (this step)
-  void* pshare;           // per kept pair: the two partners' force and torque shares
-  int* nact;              // contact-filter flags, two buffers of cap (contactFlags)
+  // per list entry: this evaluation's force and torque on the row's particle
+  // from that pair (written by the pair kernel for a contact, tagged with the
+  // evaluation counter), summed in row order by the leapfrog kernel
+  void* share;
+  void* wshare;           // per particle: the sum of its wall contacts (this evaluation)
+  int* nact;              // flag words, two buffers of cap (contactFlags)
   float4* posf;           // FP32 continuous position since the last rebuild + circumscribed radius
-  int* work;              // particles with a listed contact or near a wall (this step)
+  int* work;              // particles near a wall (this evaluation), ctl[kCtlWork]
   int nsm;                // multiprocessors of the device (persistent grids)
-  int forces_bps;         // blocks per multiprocessor of the force kernels' persistent grid (0: 4)
+  int forces_bps;         // blocks per multiprocessor of the pair kernel's persistent grid (0: 4)
   double* pair_delta;     // diagnostics: overlap of each entry (+inf: no contact)
   double* wall_delta;     // diagnostics: overlap with each wall slot
   double* pair_force;     // diagnostics: contact force on the lower ID (3 per entry)
   unsigned long long* gjk_counts;   // convex: GJK calls, iterations, most iterations of a call
   unsigned long long* law_counts;   // FP32-split: contacts evaluated, re-evaluated in FP64
+  ContactStats* cstats;   // overlap statistics over all evaluations
   double* wall_force;     // diagnostics: wall contact force on the particle (3 per slot)
   int diag;
   HistTable hist_old, hist_new;
@@ -151,8 +173,15 @@ struct DevState {
   TypeDesc const* types; ModelDesc const* models;
   WallDesc const* walls;
   const double* poly_verts;   // polyhedron vertices of all classes (x, y, z)
+  const int* poly_adj_off;    // vertex graph of the polyhedra: per global vertex, its first neighbour
+  const int* poly_adj;        // neighbours (vertex indices within their polyhedron)
+  // current polyhedron vertex of each particle (Polyhedron::m_curr_vertex),
+  // its permutation buffer, and the record this evaluation's GJK calls leave
+  // (0: none; else priority << 16 | vertex, see recordVertex)
+  int* curv; int* curv2; int* curv_next;
   int max_walls;          // walls of the largest instance
   int any_convex;         // some class is not a sphere (GJK narrow phase)
+  int any_poly;           // some class is a polyhedron (carried support vertices)
   int any_walls;          // some instance has walls
   float filt_margin_max;  // largest contact-filter margin of the instances
   int filter_qblocks;     // contact filter: blocks for the pairs (0: from the particle count)
@@ -317,9 +346,30 @@ __device__ __forceinline__ int sortEntriesUpperFirst(int* seg, int cnt, const in
   return nup;
 }
 
-// Appends the first nu entries of slot t's list to the compact pair list
-// (one atomic per warp).  Every lane of the warp calls it; valid lanes only
-// contribute.
+// Row length of a particle with cnt candidates: at most kRowMax (an entry's
+// position in its row is kept in 16 bits); more raises kErrPairsFull.
+__device__ __forceinline__ int rowLength(DevState const& S, int cnt) {
+  if (cnt > kRowMax) {
+    raise(S.status, kErrPairsFull);
+    return kRowMax;
+  }
+  return cnt;
+}
+// Whether slot t's row, placed by the scan of the row lengths, lies inside
+// the allocation of the pair list; a row that does not is emptied (its
+// particle then sees no partner) and kErrPairsFull raised -- the host grows
+// the allocation before the next call.
+__device__ __forceinline__ bool rowFits(DevState const& S, int t) {
+  const int off = S.pair_off[t];   // negative when the scan's total overflowed
+  if (off >= 0 && (long long)off + S.npairs[t] <= (long long)S.pair_cap) return true;
+  S.npairs[t] = 0;
+  raise(S.status, kErrPairsFull);
+  return false;
+}
+
+// Appends the first nu entries of slot t's row (seg) to the compact pair
+// list (one atomic per warp), with each entry's position in the row.  Every
+// lane of the warp calls it; valid lanes only contribute.
 __device__ __forceinline__ void appendUpperPairs(DevState const& S, int t, const int* seg, int nu,
                                                  int* status) {
   const unsigned full = 0xffffffffu;
@@ -335,13 +385,16 @@ __device__ __forceinline__ void appendUpperPairs(DevState const& S, int t, const
   int base = 0;
   if (lane == 31) base = atomicAdd(&S.ctl[kCtlPairs], total);
   base = __shfl_sync(full, base, 31);
-  const long long cap = (long long)S.cap * kUpperCap;
+  const long long cap = (long long)S.pair_cap / 2 + 1;
   if (base + (long long)total > cap) {
     if (lane == 0) raise(status, kErrPairsFull);
     return;
   }
   const int first = base + incl - nu;
-  for (int e = 0; e < nu; ++e) S.upairs[first + e] = make_int2(t, seg[e]);
+  for (int e = 0; e < nu; ++e) {
+    S.upairs[first + e] = make_int2(t, seg[e]);
+    S.epos[first + e] = e;
+  }
 }
 
 // Programmatic dependent launch (sm_90 and later): a kernel launched with

@@ -7,9 +7,13 @@
 // iterations.  Bodies are shrunk by their crust thickness
 // (RigidBodyWithCrust::getTransformWithCrust, RigidBodyWithCrust.cpp:
 // 749-760): the local-to-world map is  x = basis * diag(scaling) * p + origin.
-// Support functions: Sphere.cpp:99-108, Box.cpp:307-316, and for polyhedra the
-// vertex of largest projection (the reference climbs the vertex graph from the
-// clone's last vertex; both give that vertex, up to exact ties).
+// Support functions: Sphere.cpp:99-108, Box.cpp:307-316, Cylinder.cpp:
+// 112-133, and for polyhedra Polyhedron::support (Polyhedron.cpp:265-293):
+// a climb over the vertex graph from the body's current vertex, moving to the
+// first neighbour whose projection gains at least 1e-16, so that among tied
+// vertices (a face or an edge facing the direction) the search stays where it
+// is.  Each body's current vertex is carried from call to call (its
+// m_curr_vertex); the caller passes it in and gets the final one back.
 #pragma once
 #include "gdem_device.cuh"
 
@@ -21,6 +25,11 @@ struct ConvexRef {
   d3 extent;             // box half lengths
   const double* verts;   // polyhedron vertices (x, y, z), local frame
   int nverts;
+  // polyhedron vertex graph (Polyhedron::m_cobound, built from the faces by
+  // Polyhedron::BuildPolyhedron): the neighbours of vertex v are
+  // adj[adj_off[v] .. adj_off[v + 1]), in the reference's order
+  const int* adj_off;
+  const int* adj;
 };
 
 struct XForm64 { double M[9]; d3 o; };   // row-major M = basis * diag(scaling)
@@ -55,7 +64,15 @@ __device__ __forceinline__ d3 tmul(d3 v, XForm64 const& t) {
             t.M[2] * v.x + t.M[5] * v.y + t.M[8] * v.z);
 }
 
-__device__ __forceinline__ d3 support(ConvexRef const& s, d3 v) {
+__device__ __forceinline__ d3 vertexOf(ConvexRef const& s, int i) {
+  return mk(s.verts[3 * i], s.verts[3 * i + 1], s.verts[3 * i + 2]);
+}
+__device__ __forceinline__ double projection(ConvexRef const& s, int i, d3 v) {
+  return s.verts[3 * i] * v.x + s.verts[3 * i + 1] * v.y + s.verts[3 * i + 2] * v.z;
+}
+
+// cur: the body's current polyhedron vertex (ignored for other shapes)
+__device__ __forceinline__ d3 support(ConvexRef const& s, d3 v, int& cur) {
   if (s.kind == 0) {
     double n = norm(v);
     if (n > 1.0e-10) { double r = s.radius / n; return mk(v.x * r, v.y * r, v.z * r); }
@@ -79,13 +96,26 @@ __device__ __forceinline__ d3 support(ConvexRef const& s, d3 v) {
               v.z < 0. ? -s.extent.z : s.extent.z);
   }
   if (!(norm(v) > 1.0e-10)) return mk(0., 0., 0.);
-  int best = 0;
-  double h = s.verts[0] * v.x + s.verts[1] * v.y + s.verts[2] * v.z;
-  for (int i = 1; i < s.nverts; ++i) {
-    double d = s.verts[3 * i] * v.x + s.verts[3 * i + 1] * v.y + s.verts[3 * i + 2] * v.z;
-    if (d - h >= 1.e-16) { best = i; h = d; }
+  if (cur < 0 || cur >= s.nverts) cur = 0;
+  int last = -1;
+  double h = projection(s, cur, v);
+  // each move gains at least 1e-16, so the climb ends; the bound also covers
+  // a direction with a NaN component
+  for (int moves = 0; moves < s.nverts * s.nverts; ++moves) {
+    const int b = s.adj_off[cur], e = s.adj_off[cur + 1];
+    int i = b;
+    double d = 0.;
+    for (; i < e; ++i) {
+      if (s.adj[i] == last) continue;
+      d = projection(s, s.adj[i], v);
+      if (!(d - h < 1.e-16)) break;
+    }
+    if (i == e) break;
+    last = cur;
+    cur = s.adj[i];
+    h = d;
   }
-  return mk(s.verts[3 * best], s.verts[3 * best + 1], s.verts[3 * best + 2]);
+  return vertexOf(s, cur);
 }
 
 struct Simplex64 {
@@ -182,9 +212,10 @@ __device__ inline bool closestSub(Simplex64& S, unsigned& bits, unsigned last, u
 
 // closest_points: distance between the two shrunk bodies and the witness
 // points in world coordinates; *iters receives the iteration count.
+// curA, curB: the bodies' current polyhedron vertices, updated.
 __device__ inline double closestPoints64(ConvexRef const& a, XForm64 const& a2w,
                                          ConvexRef const& b, XForm64 const& b2w, d3& pa, d3& pb,
-                                         int* iters) {
+                                         int* iters, int& curA, int& curB) {
   unsigned bits = 0, last = 0, last_bit = 0, all_bits = 0;
   Simplex64 S;
 #pragma unroll
@@ -199,7 +230,7 @@ __device__ inline double closestPoints64(ConvexRef const& a, XForm64 const& a2w,
   }
   int numIterations = 0;
   const double relError = 1.e-10, absError = 1.e-4 * relError;
-  d3 v = apply(a2w, support(a, mk(0., 0., 0.))) - apply(b2w, support(b, mk(0., 0., 0.)));
+  d3 v = apply(a2w, support(a, mk(0., 0., 0.), curA)) - apply(b2w, support(b, mk(0., 0., 0.), curB));
   d3 w = v;
   double dist = norm(v);
   while (bits < 15 && dist > 1.0e-15 && numIterations < 1000) {
@@ -208,8 +239,8 @@ __device__ inline double closestPoints64(ConvexRef const& a, XForm64 const& a2w,
     last_bit = 1;
     while (bits & last_bit) { ++last; last_bit <<= 1; }
     d3 d = v;
-    S.p[last] = support(a, tmul(-d, a2w));
-    S.q[last] = support(b, tmul(d, b2w));
+    S.p[last] = support(a, tmul(-d, a2w), curA);
+    S.q[last] = support(b, tmul(d, b2w), curB);
     w = apply(a2w, S.p[last]) - apply(b2w, S.q[last]);
     double mu = dist - dot(v, w) / dist;
     if (mu < dist * relError || mu < absError) break;

@@ -4,20 +4,21 @@
 // attribute names as Grains::Construction, Base/src/Grains.cpp:535-1030, and
 // the contact-model factory, Component/src/ContactBuilderFactory.cpp:88-169),
 // owns every device buffer, and sequences the kernels of one leapfrog step
-// (Grains::Simulation, Grains.cpp:344-364):
+// (Grains::Simulation, Grains.cpp:344-364).  A gdem_step call is:
 //
-//   memset(cell counts) -> k_move (kick dt/2 + drift dt, cell key, histogram)
-//   -> scan / place / cellsort / gather (counting sort into cell order)
-//   -> k_pairs (27-cell stencil) -> memset(new history keys)
-//   -> k_forces (narrow phase + HODC + history + per-particle reduction)
-//   -> [next step's k_move applies this step's closing kick first]
-//   -> k_kick (closing kick dt/2 of the last step of the call)
+//   k_move (opening kick dt/2 + drift dt with the stored F, T), then per step
+//   k_decide -> [pair-list rebuild, when some particle moved half the skin:
+//                k_bin, scan, k_place, k_cellsort, k_permute, k_copyback,
+//                k_pairs_count, row scan, k_pairs_fill, k_link]
+//   -> k_filter (kept pairs, particles near a wall)
+//   -> k_pairlaw (narrow phase, contact law, history; shares into the rows)
+//   -> k_move (sums of the shares; closing kick, next opening kick + drift)
 //
-// Steps after the first of a gdem_step call are replayed from two captured
-// CUDA graphs (the double-buffered state and history tables alternate with
-// period two).
+// Each step is one captured CUDA graph (the rebuild inside a conditional
+// node); two graphs alternate with the contact-history tables.
 #include <algorithm>
 #include <array>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -40,6 +41,8 @@ namespace {
 
 thread_local std::string g_last_error;
 const double PI = 3.14159265358979323846;
+// steps between two checks of the pair list's allocation within a call
+constexpr int kCapacityCheck = 512;
 
 struct CudaError : std::runtime_error {
   using std::runtime_error::runtime_error;
@@ -73,6 +76,9 @@ struct InstanceDesc {
   std::vector<TypeDesc> types;
   std::vector<WallDesc> walls;
   std::vector<double> poly_verts;   // polyhedron vertices of this instance (x, y, z)
+  // each polyhedron vertex's neighbours (Polyhedron::m_cobound), aligned with
+  // poly_verts: indices within the vertex's polyhedron
+  std::vector<std::vector<int>> poly_cob;
   ModelDesc models[kMaxMat * kMaxMat];
   double gravity[3];
   double dt;
@@ -337,6 +343,19 @@ InstanceDesc readInstance(std::string const& path) {
       t.poly_count = (int)P.verts.size();
       for (auto const& v : P.verts)
         for (int d = 0; d < 3; ++d) I.poly_verts.push_back(v[d]);
+      // the vertex graph as Polyhedron::BuildPolyhedron builds it
+      // (Geometry/src/Polyhedron.cpp:322-365): along each face, vertex k gets
+      // its successor j; a new particle's search starts at the first vertex
+      // with a neighbour
+      std::vector<std::vector<int>> cob(P.verts.size());
+      for (auto const& f : P.faces) {
+        const int nf = (int)f.size();
+        for (int j = 0, k = nf - 1; j < nf; k = j++) cob[f[k]].push_back(f[j]);
+      }
+      t.poly_start = 0;
+      while (t.poly_start < (int)cob.size() && cob[t.poly_start].empty()) ++t.poly_start;
+      if (t.poly_start == (int)cob.size()) throw std::runtime_error("polyhedron without faces");
+      for (auto& c : cob) I.poly_cob.push_back(std::move(c));
     } else {
       throw std::runtime_error("unsupported particle shape in <Convex>");
     }
@@ -545,6 +564,8 @@ struct System {
   GridDesc* d_grids = nullptr; TypeDesc* d_types = nullptr; ModelDesc* d_models = nullptr;
   WallDesc* d_walls = nullptr;
   double* d_poly = nullptr;        // polyhedron vertex table of all instances
+  int* d_poly_adj_off = nullptr;   // polyhedron vertex graphs
+  int* d_poly_adj = nullptr;
   GridDesc* d_bgrids = nullptr;    // pair-list grids
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -558,6 +579,7 @@ struct System {
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   long parity = 0;                 // force evaluations so far (state and history swap together)
   long epoch = 0;                  // host copy of the evaluation counter (history tags)
+  long epoch_t0 = 0;               // evaluation counter at the leapfrog's t0 (contact features)
   bool graph_conditional = false;  // the graphs rebuild through a conditional node
   std::vector<void*> allocs;
   double* d_stage = nullptr;       // AoS staging, ID order (x v w wbf q F T: 22 doubles/particle)
@@ -584,6 +606,9 @@ struct System {
     if (d_models) cudaFree(d_models);
     if (d_walls) cudaFree(d_walls);
     if (d_poly) cudaFree(d_poly);
+    if (d_poly_adj_off) cudaFree(d_poly_adj_off);
+    if (d_poly_adj) cudaFree(d_poly_adj);
+    d_poly_adj_off = d_poly_adj = nullptr;
     if (d_bgrids) cudaFree(d_bgrids);
     d_bgrids = nullptr;
     d_grids = nullptr; d_types = nullptr; d_models = nullptr; d_walls = nullptr; d_poly = nullptr;
@@ -682,6 +707,7 @@ struct System {
     std::vector<ModelDesc> models;
     std::vector<WallDesc> walls;
     std::vector<double> poly;
+    std::vector<int> adj_off, adj;   // polyhedron vertex graphs (CSR over all vertices)
     int cell_offset = 0, max_walls = 1;
     S.any_convex = 0;
     std::vector<GridDesc> bgrids;
@@ -708,6 +734,10 @@ struct System {
         if (t.shape != 0) S.any_convex = 1;
       }
       poly.insert(poly.end(), I.poly_verts.begin(), I.poly_verts.end());
+      for (auto const& c : I.poly_cob) {
+        adj_off.push_back((int)adj.size());
+        adj.insert(adj.end(), c.begin(), c.end());
+      }
       for (auto const& w : I.walls) walls.push_back(w);
       for (int k = 0; k < kMaxMat * kMaxMat; ++k) models.push_back(I.models[k]);
       max_walls = std::max(max_walls, (int)I.walls.size());
@@ -730,8 +760,13 @@ struct System {
       CK(cudaMalloc(reinterpret_cast<void**>(&dst), std::max<size_t>(1, vec.size()) * sizeof(T)));
       if (!vec.empty()) CK(cudaMemcpy(dst, vec.data(), vec.size() * sizeof(T), cudaMemcpyHostToDevice));
     };
+    adj_off.push_back((int)adj.size());
+    S.any_poly = 0;
+    for (auto const& t : types) if (t.shape == 2) S.any_poly = 1;
     up(d_grids, grids); up(d_types, types); up(d_models, models); up(d_walls, walls);
-    up(d_poly, poly); up(d_bgrids, bgrids);
+    up(d_poly, poly); up(d_bgrids, bgrids); up(d_poly_adj_off, adj_off); up(d_poly_adj, adj);
+    S.poly_adj_off = d_poly_adj_off;
+    S.poly_adj = d_poly_adj;
     h_bgrids = bgrids;
     h_types = types;
     S.grids = d_grids; S.types = d_types; S.models = d_models; S.walls = d_walls;
@@ -758,6 +793,13 @@ struct System {
     // orientation matrices, SoA (9 x cap), only when some class is not a sphere
     S.basis = S.any_convex ? alloc<double>(9 * c) : nullptr;
     S.basis2 = S.any_convex ? alloc<double>(9 * c) : nullptr;
+    if (S.any_poly) {
+      S.curv = alloc<int>(c); S.curv2 = alloc<int>(c); S.curv_next = alloc<int>(c);
+      CK(cudaMemset(S.curv, 0, c * sizeof(int)));
+      CK(cudaMemset(S.curv_next, 0, c * sizeof(int)));
+    } else {
+      S.curv = S.curv2 = S.curv_next = nullptr;
+    }
     S.skey = alloc<int>(c); S.rank = alloc<int>(c); S.order = alloc<int>(c);
     S.cell_count = alloc<int>(S.ncells); S.cell_start = alloc<int>(S.ncells + 1);
     S.scan_tmp = alloc<int>((S.ncells + 1023) / 1024 + 1);
@@ -770,26 +812,28 @@ struct System {
       S.offh = alloc<float4>(c);
       S.pos64 = nullptr;
     }
-    S.pairs = alloc<int>(c * kPairCap); S.npairs = alloc<int>(c);
-    S.upairs = alloc<int2>(c * kUpperCap);
-    if (S.any_convex) {
-      S.kept = alloc<int>(c * kUpperCap);
-      S.eslot = alloc<int>(c * kPairCap);
-      S.pshare = alloc<char>(c * kUpperCap * 2 * (precision == GDEM_FP64 ? 72 : 36));
-    } else {
-      S.kept = nullptr; S.eslot = nullptr; S.pshare = nullptr;
-    }
+    S.npairs = alloc<int>(c);
+    S.pair_off = alloc<int>(c + 1);
+    S.pair_scan_tmp = alloc<int>((c + 1023) / 1024 + 1);
+    CK(cudaMemset(S.npairs, 0, c * sizeof(int)));
+    CK(cudaMemset(S.pair_off, 0, (c + 1) * sizeof(int)));
+    S.pairs = nullptr; S.upairs = nullptr; S.epos = nullptr; S.kept = nullptr; S.share = nullptr;
+    S.pair_cap = 0;
+    S.pair_delta = nullptr; S.wall_delta = nullptr; S.diag = 0;
+    S.pair_force = nullptr; S.wall_force = nullptr;
+    allocatePairs((long long)16 * (long long)c + 4096);
+    S.wshare = alloc<char>(c * (precision == GDEM_FP64 ? 48 : 32));
     S.nact = alloc<int>(2 * c);
     CK(cudaMemset(S.nact, 0, 2 * c * sizeof(int)));
     S.work = alloc<int>(c);
+    S.cstats = alloc<ContactStats>(1);
+    CK(cudaMemset(S.cstats, 0, sizeof(ContactStats)));
     {
       int dev = 0;
       CK(cudaGetDevice(&dev));
       CK(cudaDeviceGetAttribute(&S.nsm, cudaDevAttrMultiProcessorCount, dev));
     }
     S.posf = alloc<float4>(c);
-    S.pair_delta = nullptr; S.wall_delta = nullptr; S.diag = 0;
-    S.pair_force = nullptr; S.wall_force = nullptr;
     int l2 = nextPow2Log((size_t)8 * c + 64);
     size_t hc = size_t(1) << l2;
     size_t vsz = precision == GDEM_FP64 ? sizeof(double) : sizeof(float);
@@ -813,6 +857,77 @@ struct System {
     d_type_id = alloc<int>(c);
     d_inst_id = alloc<int>(c);
     d_vstats = alloc<double>(2 * ((c + 255) / 256) + 2);
+    // the memsets above ran on the legacy default stream
+    CK(cudaDeviceSynchronize());
+  }
+
+  // The arrays sized by the pair list's entries: the rows, the compact pair
+  // list with the pairs' positions in their rows, the contact filter's kept
+  // list, the shares (tag words all ones: no evaluation's tag) and, when on,
+  // the diagnostics records.  The rows are rebuilt before the next
+  // evaluation (the contents are not carried over).
+  void allocatePairs(long long entries) {
+    if (entries > (long long)INT_MAX - 64)
+      throw std::runtime_error("pair list too large for 32-bit row offsets");
+    for (void* p : {(void*)S.pairs, (void*)S.upairs, (void*)S.epos, (void*)S.kept, S.share,
+                    (void*)S.pair_delta, (void*)S.pair_force})
+      if (p) freeAlloc(p);
+    const size_t e = (size_t)entries, pc = e / 2 + 1;
+    S.pair_cap = (int)entries;
+    S.pairs = alloc<int>(e);
+    S.upairs = alloc<int2>(pc);
+    S.epos = alloc<int>(pc);
+    S.kept = alloc<int>(pc);
+    const size_t sb = precision == GDEM_FP64 ? 64 : 32;
+    S.share = alloc<char>(e * sb);
+    // (on the library's stream, which does not synchronise with the legacy
+    // default stream)
+    CK(cudaMemsetAsync(S.share, 0xFF, e * sb, stream));
+    if (S.wall_delta) {
+      S.pair_delta = alloc<double>(e);
+      S.pair_force = alloc<double>(3 * e);
+    } else {
+      S.pair_delta = nullptr;
+      S.pair_force = nullptr;
+    }
+    static const int one = 1;
+    if (S.ctl) CK(cudaMemcpyAsync(S.ctl + kCtlNeed, &one, sizeof(int), cudaMemcpyHostToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+    invalidateGraphs();
+  }
+  // Grows the pair list when the most entries a rebuild needed since the
+  // last check exceed 80 % of the allocation (to 1.5 times that need);
+  // the next evaluation rebuilds.  Synchronises the stream.  Returns whether
+  // it grew.
+  bool checkPairCapacity() {
+    int hwm = 0;
+    CK(cudaStreamSynchronize(stream));
+    CK(cudaMemcpy(&hwm, S.ctl + kCtlEntriesMax, sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemsetAsync(S.ctl + kCtlEntriesMax, 0, sizeof(int), stream));
+    CK(cudaStreamSynchronize(stream));
+    if ((double)hwm <= 0.8 * (double)S.pair_cap) return false;
+    allocatePairs(std::max((long long)(1.5 * (double)hwm) + 4096, (long long)S.pair_cap));
+    return true;
+  }
+  // Sizes the pair list for the current state before the leapfrog start: the
+  // rebuild up to the scan of the row lengths (it only reorders the state),
+  // then the allocation check.
+  void sizePairList() {
+    static const int one = 1;
+    CK(cudaMemcpyAsync(S.ctl + kCtlActive, &one, sizeof(int), cudaMemcpyHostToDevice, stream));
+    const int* gate = S.ctl + kCtlActive;
+    launch_bin(S, gate, stream);
+    launch_scan(S, gate, stream);
+    launch_place(S, gate, stream);
+    launch_cellsort(S, gate, stream);
+    launch_permute(S, gate, stream);
+    launch_copyback(S, gate, stream);
+    if (precision == GDEM_FP64) launch_pairs64(S, gate, 0, stream);
+    else launch_pairs32(S, gate, 0, stream);
+    launch_row_scan(S, gate, stream);
+    CK(cudaGetLastError());
+    id_order = false;
+    checkPairCapacity();
   }
 
   // Host AoS arrays (by ID) -> staging -> SoA state in ID order.
@@ -861,20 +976,26 @@ struct System {
     timed("cellsort", [&] { launch_cellsort(S, gate, stream); });
     timed("permute", [&] { launch_permute(S, gate, stream); });
     timed("copyback", [&] { launch_copyback(S, gate, stream); });
-    if (precision == GDEM_FP64) timed("pairs64", [&] { launch_pairs64(S, gate, stream); });
-    else timed("pairs32", [&] { launch_pairs32(S, gate, stream); });
+    if (precision == GDEM_FP64) {
+      timed("pairs_count64", [&] { launch_pairs64(S, gate, 0, stream); });
+      timed("row_scan", [&] { launch_row_scan(S, gate, stream); });
+      timed("pairs_fill64", [&] { launch_pairs64(S, gate, 1, stream); });
+    } else {
+      timed("pairs_count32", [&] { launch_pairs32(S, gate, 0, stream); });
+      timed("row_scan", [&] { launch_row_scan(S, gate, stream); });
+      timed("pairs_fill32", [&] { launch_pairs32(S, gate, 1, stream); });
+    }
+    timed("link", [&] { launch_link(S, gate, stream); });
   }
-  // Contact filter, forces, then the leapfrog parts in flags (none at the
-  // leapfrog start).
+  // Contact filter, pair kernel (contacts and walls), then the leapfrog
+  // kernel: the sums of the shares and the leapfrog parts in flags (at the
+  // leapfrog start only the sums, stored as F, T).
   void forcesAndMove(int flags) {
+    if (diag) timed("diag_prefill", [&] { launch_diag_prefill(S, stream); });
     timed("filter", [&] { launch_filter(S, stream); });
-    // the leapfrog start evaluates every particle; later evaluations skip the
-    // particles without contact (k_move applies their weight), except with
-    // diagnostics on, which record every particle's wall overlaps
-    const int sparse = (flags && !diag) ? 1 : 0;
-    if (precision == GDEM_FP64) timed("forces64", [&] { launch_forces64(S, sparse, stream); });
-    else timed("forces32", [&] { launch_forces32(S, sparse, stream); });
-    if (flags) timed("move", [&] { launch_move(S, flags, precision == GDEM_FP32_SPLIT, stream); });
+    if (precision == GDEM_FP64) timed("pairlaw64", [&] { launch_pairlaw64(S, stream); });
+    else timed("pairlaw32", [&] { launch_pairlaw32(S, stream); });
+    timed("move", [&] { launch_move(S, flags | kStepSum, precision == GDEM_FP32_SPLIT, stream); });
   }
   // One force evaluation with plain launches: decide, gated rebuild, filter,
   // forces, move.
@@ -950,8 +1071,9 @@ struct System {
   }
 
   void init() {
-    id_order = false;
-    evaluate(0);
+    sizePairList();
+    epoch_t0 = epoch + 1;   // the evaluation at t0 is the next one
+    evaluate(kStepStoreFT);
     ++parity;
     launch_hist_zero_cumulative(S.hist_old, S.ctl, precision == GDEM_FP64, stream);
     CK(cudaStreamSynchronize(stream));
@@ -975,9 +1097,12 @@ struct System {
     timed("move", [&] { launch_move(S, kStepMove, precision == GDEM_FP32_SPLIT, stream); });
     const int mid = kStepClose | kStepMove;
     const int last = kStepClose | kStepStoreFT;
-    const bool graphs = use_graphs && !diag && !profiling;
     for (int k = 0; k < nsteps; ++k) {
       const bool is_last = k == nsteps - 1;
+      // the pair list's allocation is checked every kCapacityCheck steps
+      // within a call (and at its end); it grows before it can run short
+      if (k > 0 && k % kCapacityCheck == 0) checkPairCapacity();
+      const bool graphs = use_graphs && !diag && !profiling;
       if (graphs) {
         launchEvaluation(is_last ? 1 : 0, is_last ? last : mid);
       } else {
@@ -993,6 +1118,7 @@ struct System {
     last_ms = ms;
     collectTimes();
     evaluated = diag ? 1 : 2;
+    checkPairCapacity();
   }
   int readStatus() {
     int st = 0;
@@ -1120,6 +1246,7 @@ int gdem_upload_forces(gdem_handle h, const double* F, const double* T) {
     CK(cudaMemcpy(S.F, hF.data(), 3 * c * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(S.T, hT.data(), 3 * c * sizeof(double), cudaMemcpyHostToDevice));
     s->started = true;
+    s->epoch_t0 = s->epoch;   // the forces are those of t0; the next evaluation is t0 + dt
     return GDEM_OK;
   });
 }
@@ -1133,6 +1260,7 @@ int gdem_set_state(gdem_handle h, const double* x, const double* v, const double
     if ((F == nullptr) != (T == nullptr)) throw std::runtime_error("give both F and T, or neither");
     s->loadState(x, v, w, wbf, q, F, T);
     s->started = F != nullptr;
+    if (F) s->epoch_t0 = s->epoch;
     return GDEM_OK;
   });
 }
@@ -1212,6 +1340,30 @@ int gdem_gjk_counts(gdem_handle h, int64_t* calls, int64_t* iterations, int64_t*
   });
 }
 
+int gdem_contact_features(gdem_handle h, double* overlap_max, double* overlap_mean,
+                          int64_t* evaluation_of_max, double* gjk_iterations_mean, int reset) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state) throw std::runtime_error("upload the state first");
+    ContactStats cs{};
+    CK(cudaStreamSynchronize(s->stream));
+    CK(cudaMemcpy(&cs, s->S.cstats, sizeof(ContactStats), cudaMemcpyDeviceToHost));
+    unsigned long long g[3] = {0, 0, 0};
+    CK(cudaMemcpy(g, s->S.gjk_counts, sizeof(g), cudaMemcpyDeviceToHost));
+    double mx = 0.;
+    std::memcpy(&mx, &cs.max_bits, sizeof(double));
+    if (overlap_max) *overlap_max = cs.count ? mx : 0.;
+    if (overlap_mean) *overlap_mean = cs.count ? cs.sum / (double)cs.count : 0.;
+    if (evaluation_of_max) *evaluation_of_max = cs.count ? (int64_t)(cs.max_epoch - s->epoch_t0) : -1;
+    if (gjk_iterations_mean) *gjk_iterations_mean = g[0] ? (double)g[1] / (double)g[0] : 0.;
+    if (reset) {
+      CK(cudaMemsetAsync(s->S.cstats, 0, sizeof(ContactStats), s->stream));
+      CK(cudaStreamSynchronize(s->stream));
+    }
+    return GDEM_OK;
+  });
+}
+
 int gdem_set_profiling(gdem_handle h, int on) {
   return guarded([&] {
     System* s = sys(h);
@@ -1281,6 +1433,64 @@ int gdem_upload_history(gdem_handle h, int64_t n, const int* owner, const int* p
     CK(cudaMemcpy(t.keys, keys.data(), hc * sizeof(unsigned long long), cudaMemcpyHostToDevice));
     if (fp64) CK(cudaMemcpy(t.vals, vd.data(), vd.size() * sizeof(double), cudaMemcpyHostToDevice));
     else CK(cudaMemcpy(t.vals, vf.data(), vf.size() * sizeof(float), cudaMemcpyHostToDevice));
+    return GDEM_OK;
+  });
+}
+
+int gdem_download_history(gdem_handle h, int64_t capacity, int64_t* count, int* owner,
+                          int* partner, double* kdelta, double* prevn, double* spring) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state || !count) throw std::runtime_error("invalid arguments");
+    DevState& S = s->S;
+    CK(cudaStreamSynchronize(s->stream));
+    HistTable& t = S.hist_old;   // written by the last force evaluation
+    const size_t hc = size_t(1) << t.log2cap;
+    std::vector<unsigned long long> keys(hc);
+    CK(cudaMemcpy(keys.data(), t.keys, hc * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    const bool fp64 = s->precision == GDEM_FP64;
+    std::vector<double> vd(fp64 ? 9 * hc : 0);
+    std::vector<float> vf(fp64 ? 0 : 9 * hc);
+    if (fp64) CK(cudaMemcpy(vd.data(), t.vals, vd.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    else CK(cudaMemcpy(vf.data(), t.vals, vf.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    struct Rec { int a, b; double v[9]; };
+    std::vector<Rec> recs;
+    const unsigned tag = (unsigned)s->epoch & kTagMask;
+    const unsigned idmask = (1u << kMaxIdBits) - 1u;
+    const unsigned n = (unsigned)S.n;
+    for (size_t k = 0; k < hc; ++k) {
+      if (tagOf(keys[k]) != tag) continue;
+      const unsigned hi = (unsigned)((keys[k] >> kMaxIdBits) & idmask);
+      const unsigned lo = (unsigned)(keys[k] & idmask);
+      if (hi >= n) continue;
+      Rec r;
+      for (int c = 0; c < 9; ++c) r.v[c] = fp64 ? vd[9 * k + c] : (double)vf[9 * k + c];
+      r.a = (int)hi;
+      if (lo < n) {
+        r.b = (int)lo;
+        recs.push_back(r);
+        Rec q{(int)lo, (int)hi, {}};   // the other body's view is the negation
+        for (int c = 0; c < 9; ++c) q.v[c] = -r.v[c];
+        recs.push_back(q);
+      } else {
+        r.b = -((int)(idmask - lo) + 2);
+        recs.push_back(r);
+      }
+    }
+    std::sort(recs.begin(), recs.end(),
+              [](Rec const& x, Rec const& y) { return x.a != y.a ? x.a < y.a : x.b < y.b; });
+    *count = (int64_t)recs.size();
+    if (capacity >= *count && owner && partner) {
+      for (size_t e = 0; e < recs.size(); ++e) {
+        owner[e] = recs[e].a;
+        partner[e] = recs[e].b;
+        for (int d = 0; d < 3; ++d) {
+          if (kdelta) kdelta[3 * e + d] = recs[e].v[d];
+          if (prevn) prevn[3 * e + d] = recs[e].v[3 + d];
+          if (spring) spring[3 * e + d] = recs[e].v[6 + d];
+        }
+      }
+    }
     return GDEM_OK;
   });
 }
@@ -1940,14 +2150,15 @@ int gdem_set_diagnostics(gdem_handle h, int on) {
     if (!s || !s->have_state) throw std::runtime_error("upload the state first");
     DevState& S = s->S;
     if (on && !S.pair_delta) {
-      S.pair_delta = s->alloc<double>((size_t)S.cap * kPairCap);
+      S.pair_delta = s->alloc<double>((size_t)S.pair_cap);
       S.wall_delta = s->alloc<double>((size_t)S.cap * S.max_walls);
-      S.pair_force = s->alloc<double>((size_t)S.cap * kPairCap * 3);
+      S.pair_force = s->alloc<double>((size_t)S.pair_cap * 3);
       S.wall_force = s->alloc<double>((size_t)S.cap * S.max_walls * 3);
     }
+    // the graphs hold the evaluation without diagnostics (an evaluation with
+    // them runs as plain launches), so they stay valid either way
     S.diag = on ? 1 : 0;
     s->diag = on != 0;
-    s->invalidateGraphs();
     return GDEM_OK;
   });
 }
@@ -1960,13 +2171,17 @@ int gdem_download_contacts(gdem_handle h, int64_t capacity, int64_t* count, int*
     DevState& S = s->S;
     if (!S.pair_delta) throw std::runtime_error("enable diagnostics before the step");
     size_t n = (size_t)S.n;
-    std::vector<int> ids(n), np(n), pairs(n * kPairCap);
-    std::vector<double> pd(n * kPairCap), pf(3 * n * kPairCap);
-    std::vector<double> wd(n * S.max_walls), wf(3 * n * S.max_walls);
-    std::vector<int4> cells(n);
+    std::vector<int> ids(n), np(n), off(n + 1);
     CK(cudaMemcpy(ids.data(), S.id, n * sizeof(int), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(np.data(), S.npairs, n * sizeof(int), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(pairs.data(), S.pairs, n * kPairCap * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(off.data(), S.pair_off, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+    size_t ne = 0;
+    for (size_t t = 0; t < n; ++t) ne = std::max(ne, (size_t)off[t] + (size_t)np[t]);
+    std::vector<int> pairs(ne);
+    std::vector<double> pd(ne), pf(3 * ne);
+    std::vector<double> wd(n * S.max_walls), wf(3 * n * S.max_walls);
+    std::vector<int4> cells(n);
+    CK(cudaMemcpy(pairs.data(), S.pairs, ne * sizeof(int), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(pd.data(), S.pair_delta, pd.size() * sizeof(double), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(wd.data(), S.wall_delta, wd.size() * sizeof(double), cudaMemcpyDeviceToHost));
     if (force) {
@@ -1977,8 +2192,8 @@ int gdem_download_contacts(gdem_handle h, int64_t capacity, int64_t* count, int*
     int64_t c = 0;
     for (size_t t = 0; t < n; ++t) {
       for (int e = 0; e < np[t]; ++e) {
-        int u = pairs[t * kPairCap + e] & ((1 << 27) - 1);   // pair-list entries
-        size_t slot = t * kPairCap + e;
+        size_t slot = (size_t)off[t] + e;
+        int u = pairs[slot] & ((1 << 27) - 1);   // pair-list entries
         double dl = pd[slot];
         if (!(dl < 0.) || !(ids[t] < ids[u])) continue;
         if (c < capacity && id0) {
@@ -2027,6 +2242,59 @@ int gdem_download_coordination(gdem_handle h, int* coord) {
   });
 }
 
+int gdem_upload_support_vertices(gdem_handle h, const int* vertex) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state || !vertex) throw std::runtime_error("invalid arguments");
+    DevState& S = s->S;
+    if (!S.curv) return GDEM_OK;   // no polyhedron class
+    const size_t n = (size_t)S.n;
+    std::vector<int> ids(n), slot(n);
+    CK(cudaStreamSynchronize(s->stream));
+    CK(cudaMemcpy(ids.data(), S.id, n * sizeof(int), cudaMemcpyDeviceToHost));
+    for (size_t t = 0; t < n; ++t) {
+      const int i = ids[t];
+      TypeDesc const& tp = s->h_types[s->type_base[s->h_inst[i]] + s->h_type[i]];
+      const int v = vertex[i];
+      if (tp.shape == 2 && (v < 0 || v >= tp.poly_count))
+        throw std::runtime_error("support vertex out of range for particle " + std::to_string(i));
+      slot[t] = tp.shape == 2 ? v : 0;
+    }
+    CK(cudaMemcpyAsync(S.curv, slot.data(), n * sizeof(int), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return GDEM_OK;
+  });
+}
+
+int gdem_download_support_vertices(gdem_handle h, int* vertex) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state || !vertex) throw std::runtime_error("invalid arguments");
+    DevState& S = s->S;
+    const size_t n = (size_t)S.n;
+    if (!S.curv) {
+      std::fill(vertex, vertex + n, 0);
+      return GDEM_OK;
+    }
+    std::vector<int> ids(n), cur(n);
+    CK(cudaStreamSynchronize(s->stream));
+    CK(cudaMemcpy(ids.data(), S.id, n * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(cur.data(), S.curv, n * sizeof(int), cudaMemcpyDeviceToHost));
+    for (size_t t = 0; t < n; ++t) vertex[ids[t]] = cur[t];
+    return GDEM_OK;
+  });
+}
+
+int gdem_download_ids(gdem_handle h, int* ids) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !s->have_state || !ids) throw std::runtime_error("invalid arguments");
+    const size_t n = s->h_type.size();
+    for (size_t i = 0; i < n; ++i) ids[i] = s->ref_ids.empty() ? (int)i + 1 : s->ref_ids[i];
+    return GDEM_OK;
+  });
+}
+
 int gdem_download_classes(gdem_handle h, int* cls) {
   return guarded([&] {
     System* s = sys(h);
@@ -2062,6 +2330,15 @@ int gdem_grid(gdem_handle h, int k, int* nb, double* edge, double* origin) {
     }
     return GDEM_OK;
   });
+}
+
+int gdem_num_instances(gdem_handle h) {
+  System* s = sys(h);
+  if (!s) {
+    setLastError("invalid handle");
+    return GDEM_ERR_INVALID;
+  }
+  return (int)s->inst.size();
 }
 
 int64_t gdem_num_particles(gdem_handle h) {

@@ -21,12 +21,19 @@
 //   k_permute / k_copyback
 //               the whole state into cell order (through the second
 //               buffers), with the compact copies the pair search reads.
-//   k_filter    flags the particles with a pair of the skin list whose
-//               bounding spheres overlap now, or near a wall, and lists them
-//               for the force kernel.
-//   k_move      the leapfrog of each particle in place: closing kick of the
-//               step that ends and opening kick + drift of the next
-//               (SecondOrderLeapFrog::Move / advanceVelocity,
+//   k_pairs_*   (gdem_contact64/32.cu) the rows of the skin pair list:
+//               counted, placed by a scan of the counts, written; k_link
+//               then records where each pair of the compact list sits in
+//               its partner's row.
+//   k_filter    lists the pairs of the skin list whose bounding spheres
+//               overlap now, and the particles near a wall, and marks them
+//               as candidates; the pair kernel (gdem_contact64/32.cu)
+//               evaluates them exactly and writes each contact's two shares
+//               into the partners' rows.
+//   k_move      the leapfrog of each particle in place: its force and torque
+//               as the weight plus its shares in row order, then the closing
+//               kick of the step that ends and the opening kick + drift of
+//               the next (SecondOrderLeapFrog::Move / advanceVelocity,
 //               ParticleKinematics::Move).
 // Rebuild kernels take a gate: with a non-null gate they return at once
 // unless this step rebuilds (plain launches); inside the graph's conditional
@@ -48,9 +55,9 @@ __global__ void k_decide(DevState S, cudaGraphConditionalHandle h, int use_handl
   S.ctl[kCtlActive] = need;
   S.ctl[kCtlNeed] = 0;
   S.ctl[kCtlEpoch] += 1;
-  S.ctl[kCtlRebuilds] += need ? 1 : 0;
   S.ctl[kCtlWork] = 0;
   S.ctl[kCtlKept] = 0;
+  S.ctl[kCtlRebuilds] += need ? 1 : 0;
   if (need) S.ctl[kCtlPairs] = 0;
   if (use_handle) cudaGraphSetConditional(h, need ? 1u : 0u);
 }
@@ -143,13 +150,21 @@ __global__ void k_scan_sums(int* sums, int ntiles, const int* gate) {
 // Adds the tile offsets; out[n] receives the total so that cell c spans
 // [out[c], out[c + 1]).
 __global__ void k_scan_add(int* out, const int* tile_sums, const int* in, int n,
-                           const int* gate) {
+                           const int* gate, int* ctl) {
   if (gatedOff(gate)) return;
   int i = blockIdx.x * kScanTile + threadIdx.x;
   if (i < n) {
     int v = out[i] + tile_sums[blockIdx.x];
     out[i] = v;
-    if (i == n - 1) out[n] = v + in[i];
+    if (i == n - 1) {
+      // (a total beyond 2^31 - 1 wraps negative: the rows then do not fit)
+      const int total = v + in[i];
+      out[n] = total;
+      if (ctl) {
+        ctl[kCtlEntries] = total;
+        atomicMax(&ctl[kCtlEntriesMax], total < 0 ? INT_MAX : total);
+      }
+    }
   }
 }
 
@@ -208,6 +223,7 @@ __global__ void k_permute(DevState S, const int* gate) {
 #pragma unroll
     for (int k = 0; k < 9; ++k) S.basis2[k * cap + t] = S.basis[k * cap + s];
   }
+  if (S.curv) S.curv2[t] = S.curv[s];
   GridDesc const& bg = S.bgrids[in];
   const int c = S.skey[s] - bg.cell_offset;
   const int ci = c % bg.nb[0];
@@ -245,34 +261,153 @@ __global__ void k_copyback(DevState S, const int* gate) {
 #pragma unroll
     for (int k = 0; k < 9; ++k) S.basis[k * cap + t] = S.basis2[k * cap + t];
   }
+  if (S.curv) S.curv[t] = S.curv2[t];
   S.wrap[t] = 0;
   const d3 x = ld3(S.x, cap, t);
   S.posf[t] = make_float4((float)x.x, (float)x.y, (float)x.z,
                           (float)S.types[S.type[t]].radius);
 }
 
-// Leapfrog of each particle with the stored F, T: the closing kick of the
-// step that ends (flags & kStepClose) and the opening kick + drift of the
-// next (flags & kStepMove).  Per particle only, so it runs in place (the
-// launcher aliases the second buffers to the current ones).
-// A particle that the contact filter left without contact carries only its
-// weight: the force kernel skipped it and its F, T are taken as such here
-// (and written back at the end of a call, kStepStoreFT).
+// Force and torque of particle t in this evaluation: its weight plus the
+// shares the pair kernel wrote into its row, in row order, then its wall
+// share.  The entry bits of the flag word name the shares of the first
+// kMaskEntries entries, so their loads are issued together, two at a time
+// (a particle rarely has more contacts, and larger batches spill);
+// entries beyond (kFarEntry) are found by their evaluation tags.  FP32-split
+// (kFast): FP32 shares summed in FP32; FP64: FP64 shares summed in FP64 onto
+// the weight.
+template <bool kFast>
+__device__ __forceinline__ void sumShares(DevState const& S, int t, TypeDesc const& tp,
+                                          unsigned na, int off, int tag, d3& F, d3& T) {
+  constexpr int kBatch = 2;
+  if constexpr (kFast) {
+    float fx = 0.f, fy = 0.f, fz = 0.f, tx = 0.f, ty = 0.f, tz = 0.f;
+    const float4* sh = static_cast<const float4*>(S.share) + 2 * (size_t)off;
+    unsigned m = na & kEntryBits;
+    while (m) {
+      float4 a[kBatch], b[kBatch];
+      int cnt = 0;
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) {
+        if (m) {
+          const int e = __ffs(m) - 1;
+          m &= m - 1u;
+          a[j] = sh[2 * e];
+          b[j] = sh[2 * e + 1];
+          cnt = j + 1;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) {
+        if (j < cnt) {
+          fx += a[j].x; fy += a[j].y; fz += a[j].z;
+          tx += b[j].x; ty += b[j].y; tz += b[j].z;
+        }
+      }
+    }
+    if (na & kFarEntry) {
+      const int np = S.npairs[t];
+      for (int e = kMaskEntries; e < np; ++e) {
+        const float4 a = sh[2 * e];
+        if (__float_as_int(a.w) != tag) continue;
+        const float4 b = sh[2 * e + 1];
+        fx += a.x; fy += a.y; fz += a.z;
+        tx += b.x; ty += b.y; tz += b.z;
+      }
+    }
+    if (na & kNearWall) {
+      const float4* ws = static_cast<const float4*>(S.wshare) + 2 * (size_t)t;
+      const float4 a = ws[0], b = ws[1];
+      fx += a.x; fy += a.y; fz += a.z;
+      tx += b.x; ty += b.y; tz += b.z;
+    }
+    F = mk(tp.weight[0] + (double)fx, tp.weight[1] + (double)fy, tp.weight[2] + (double)fz);
+    T = mk((double)tx, (double)ty, (double)tz);
+  } else {
+    F = mk(tp.weight[0], tp.weight[1], tp.weight[2]);
+    T = mk(0., 0., 0.);
+    const double2* sh = static_cast<const double2*>(S.share) + 4 * (size_t)off;
+    unsigned m = na & kEntryBits;
+    while (m) {
+      double2 a[kBatch], b[kBatch], c[kBatch], d[kBatch];
+      int cnt = 0;
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) {
+        if (m) {
+          const int e = __ffs(m) - 1;
+          m &= m - 1u;
+          a[j] = sh[4 * e]; b[j] = sh[4 * e + 1]; c[j] = sh[4 * e + 2]; d[j] = sh[4 * e + 3];
+          cnt = j + 1;
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) {
+        if (j < cnt) {
+          F = F + mk(a[j].y, b[j].x, b[j].y);
+          T = T + mk(c[j].x, c[j].y, d[j].x);
+        }
+      }
+    }
+    if (na & kFarEntry) {
+      const int np = S.npairs[t];
+      for (int e = kMaskEntries; e < np; ++e) {
+        const double2 a = sh[4 * e];
+        if ((int)__double_as_longlong(a.x) != tag) continue;
+        const double2 b = sh[4 * e + 1], c = sh[4 * e + 2], d = sh[4 * e + 3];
+        F = F + mk(a.y, b.x, b.y);
+        T = T + mk(c.x, c.y, d.x);
+      }
+    }
+    if (na & kNearWall) {
+      const double2* ws = static_cast<const double2*>(S.wshare) + 3 * (size_t)t;
+      const double2 a = ws[0], b = ws[1], c = ws[2];
+      F = F + mk(a.x, a.y, b.x);
+      T = T + mk(b.y, c.x, c.y);
+    }
+  }
+}
+
+// Leapfrog of each particle.  With kStepSum the force and torque of this
+// evaluation: the weight for a particle the contact filter did not mark as a
+// candidate, else the weight plus its shares (sumShares); without it, the
+// stored F, T (the opening kick of a call continues from the last evaluation
+// of the previous one).  Then the closing kick of the step that ends
+// (flags & kStepClose) and the opening kick + drift of the next
+// (flags & kStepMove); kStepStoreFT writes F, T back (the last evaluation of
+// a call, and the leapfrog start, which only stores them).  Per particle
+// only, so it runs in place (the launcher aliases the second buffers to the
+// current ones).
+//
+// The kernel starts while the pair kernel still runs (programmatic launch:
+// the pair kernel triggers after its own wait, so the filter has completed
+// and its candidate marks are final).  A particle that is not a candidate
+// takes no share and is not read by the pair kernel, so its leapfrog runs at
+// once; a candidate waits for the pair kernel before it reads its shares.
 template <bool kFast, bool kBasis>
 __global__ void __launch_bounds__(256, (kFast && kBasis) ? 2 : 3) k_move(DevState S, int flags) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
   TypeDesc const& tp = S.types[S.type[t]];
   MoveIn m;
-  loadMoveIn<kFast, kBasis>(S, t, m);   // nothing the force kernel writes
-  pdlWait();
+  loadMoveIn<kFast, kBasis>(S, t, m);   // nothing the contact kernels write
+  const bool sum = (flags & kStepSum) != 0;
   d3 F, T;
-  const int na = contactFlags(S)[t];
-  if ((flags & kStepClose) && na == 0) {
-    F = mk(tp.weight[0], tp.weight[1], tp.weight[2]);
-    T = mk(0., 0., 0.);
+  bool candidate = false;
+  if (sum) {
+    int* fl = contactFlags(S);
+    candidate = ((unsigned)fl[t] & kCandidate) != 0u;
+    if (!candidate) {
+      F = mk(tp.weight[0], tp.weight[1], tp.weight[2]);
+      T = mk(0., 0., 0.);
+    } else {
+      // the row of t (written by the last rebuild, before the filter)
+      const int off = S.pair_off[t];
+      pdlWait();
+      sumShares<kFast>(S, t, tp, (unsigned)fl[t], off, S.ctl[kCtlEpoch], F, T);
+    }
     if (flags & kStepStoreFT) { st3(S.F, S.cap, t, F); st3(S.T, S.cap, t, T); }
   } else {
+    pdlWait();
     F = ld3(S.F, S.cap, t);
     T = ld3(S.T, S.cap, t);
   }
@@ -283,38 +418,33 @@ __global__ void __launch_bounds__(256, (kFast && kBasis) ? 2 : 3) k_move(DevStat
     F = F + mk(hy[0], hy[1], hy[2]);
     T = T + mk(hy[3], hy[4], hy[5]);
   }
-  advanceParticle<kFast, kBasis>(S, t, tp, F, T, (flags & kStepClose) != 0, (flags & kStepMove) != 0,
-                                 m);
-  // the next evaluation's contact flags start clear (no other kernel touches
+  if (flags & (kStepClose | kStepMove))
+    advanceParticle<kFast, kBasis>(S, t, tp, F, T, (flags & kStepClose) != 0,
+                                   (flags & kStepMove) != 0, m);
+  // the next evaluation's flag words start clear (no other kernel touches
   // that buffer until the next contact filter)
   contactFlags(S, 1)[t] = 0;
+  if (candidate && S.curv_next) {
+    // the polyhedron vertex this evaluation's GJK calls left (recordVertex;
+    // only candidates take part in GJK calls)
+    const int r = S.curv_next[t];
+    if (r) {
+      S.curv[t] = r & 0xFFFF;
+      S.curv_next[t] = 0;
+    }
+  }
 }
 
 // Contact filter.  One lane per pair of the compact pair list (each pair
-// once, from its lower ID): the FP32 bounding-sphere test (a superset of the
-// contacts; the force kernels test both entries of the pair again with
-// boundingOverlap and decide each kept one exactly in FP64); both particles
-// of a kept pair are flagged and each flagged particle is appended once to
-// the force kernels' work list.  One lane per particle: the next
-// evaluation's flags are cleared by k_move.  With walls, the first pblocks
-// blocks take the particles and flag those near a wall; the others take the
-// pairs, in chunks
-// of kFilterUnroll rounds of 32 per warp with their loads issued together
-// (a grid-stride loop over chunks: the grid is sized for the pair count at
-// the leapfrog start, the count itself is known on the device only).
+// once, from its lower ID): the FP32 bounding-sphere test, a superset of the
+// contacts; the kept pairs are listed for the pair kernel, which decides each
+// exactly, and both partners marked as candidates.  With walls, the first
+// pblocks blocks take one particle per thread and list (and mark) those near
+// a wall.  The pairs are taken in chunks of kFilterUnroll rounds of 32 per
+// warp with their loads issued together (a grid-stride loop over chunks: the
+// grid is sized for the pair count at the leapfrog start, the count itself is
+// known on the device only).
 constexpr int kFilterUnroll = 4;
-
-// Appends idx for every lane whose pred holds (one atomic per warp); every
-// lane of the warp calls it.
-__device__ __forceinline__ void appendWork(DevState const& S, bool pred, int idx) {
-  const unsigned m = __ballot_sync(0xffffffffu, pred);
-  if (!m) return;
-  const int lane = threadIdx.x & 31;
-  int base = 0;
-  if (lane == 0) base = atomicAdd(&S.ctl[kCtlWork], __popc(m));
-  base = __shfl_sync(0xffffffffu, base, 0);
-  if (pred) S.work[base + __popc(m & ((1u << lane) - 1u))] = idx;
-}
 
 // Appends idx to list (length *count) for every lane whose pred holds (one
 // atomic per warp); every lane of the warp calls it.
@@ -328,50 +458,45 @@ __device__ __forceinline__ void appendList(int* list, int* count, bool pred, int
   if (pred) list[base + __popc(m & ((1u << lane) - 1u))] = idx;
 }
 
-// Sets flag bits of particle i; true for the caller that lists it first.
-__device__ __forceinline__ bool flagParticle(int* flags, int i, int bits) {
-  return !(atomicOr(&flags[i], bits | kListed) & kListed);
+// Whether particle t (posf: its FP32 continuous position) comes within the
+// margin of a wall box of its instance: the wall contacts can only come
+// from such particles.
+__device__ __forceinline__ bool nearWall(DevState const& S, int t) {
+  const int inst = S.inst[t];
+  GridDesc const& g = S.grids[inst];
+  if (!g.wall_count) return false;
+  // the centre wrapped back into the box, against the bounding radius
+  GridDesc const& bg = S.bgrids[inst];
+  const float4 pt = S.posf[t];
+  const int wt = S.wrap[t];
+  const float q[3] = {pt.x - (float)wrapGet(wt, 0) * bg.Lf[0],
+                      pt.y - (float)wrapGet(wt, 1) * bg.Lf[1],
+                      pt.z - (float)wrapGet(wt, 2) * bg.Lf[2]};
+  for (int w = 0; w < g.wall_count; ++w) {
+    WallDesc const& wd = S.walls[g.wall_begin + w];
+    float d2 = 0.f;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const float o = fabsf(q[d] - (float)wd.centre[d]) - (float)wd.extent[d];
+      if (o > 0.f) d2 += o * o;
+    }
+    const float R = pt.w + bg.filt_margin;
+    if (d2 <= R * R) return true;
+  }
+  return false;
 }
 
 __global__ void __launch_bounds__(256) k_filter(DevState S, int pblocks) {
-  pdlTrigger();   // the force kernel may be scheduled; it waits for this one
+  pdlTrigger();   // the pair kernel may be scheduled; it waits for this one
   const int lane = threadIdx.x & 31;
-  int* flags = contactFlags(S);
+  unsigned* flags = reinterpret_cast<unsigned*>(contactFlags(S));
   if ((int)blockIdx.x < pblocks) {
-    // particles near a wall
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    bool newW = false;
-    if (t < S.n) {
-      const int inst = S.inst[t];
-      GridDesc const& g = S.grids[inst];
-      if (g.wall_count) {
-        // distance from the centre (wrapped back into the box) to each wall
-        // box against the bounding radius
-        GridDesc const& bg = S.bgrids[inst];
-        const float4 pt = S.posf[t];
-        const int wt = S.wrap[t];
-        const float q[3] = {pt.x - (float)wrapGet(wt, 0) * bg.Lf[0],
-                            pt.y - (float)wrapGet(wt, 1) * bg.Lf[1],
-                            pt.z - (float)wrapGet(wt, 2) * bg.Lf[2]};
-        bool near = false;
-        for (int w = 0; w < g.wall_count && !near; ++w) {
-          WallDesc const& wd = S.walls[g.wall_begin + w];
-          float d2 = 0.f;
-#pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            const float o = fabsf(q[d] - (float)wd.centre[d]) - (float)wd.extent[d];
-            if (o > 0.f) d2 += o * o;
-          }
-          const float R = pt.w + bg.filt_margin;
-          near = d2 <= R * R;
-        }
-        if (near) newW = flagParticle(flags, t, kNearWall);
-      }
-    }
-    appendWork(S, newW, t);
+    const bool near = t < S.n && nearWall(S, t);
+    if (near) atomicOr(&flags[t], kCandidate);
+    appendList(S.work, S.ctl + kCtlWork, near, t);
     return;
   }
-  // pairs
   const int np = S.ctl[kCtlPairs];
   constexpr int chunk = 32 * kFilterUnroll;
   const long long wq = ((long long)((int)blockIdx.x - pblocks) * blockDim.x + threadIdx.x) >> 5;
@@ -398,9 +523,9 @@ __global__ void __launch_bounds__(256) k_filter(DevState S, int pblocks) {
       const int t = pr[j].x, u = (int)((unsigned)pr[j].y & ((1u << 27) - 1u));
       bool keep = false;
       if (c0 + 32 * j + lane < np) {
-        // the largest margin of the instances (a superset of the force
-        // kernels' decisions); the period only for an entry with an image
-        // shift (code 13 is none), which needs the instance's grid
+        // the largest margin of the instances (a superset of the contacts);
+        // the period only for an entry with an image shift (code 13 is
+        // none), which needs the instance's grid
         const unsigned code = (unsigned)pr[j].y >> 27;
         float sx = 0.f, sy = 0.f, sz = 0.f;
         if (code != 13u) {
@@ -415,15 +540,46 @@ __global__ void __launch_bounds__(256) k_filter(DevState S, int pblocks) {
         const float R = pa[j].w + pb[j].w + S.filt_margin_max;
         keep = dx * dx + dy * dy + dz * dz <= R * R;
       }
-      bool newT = false, newU = false;
       if (keep) {
-        newT = flagParticle(flags, t, kHasPair);
-        newU = flagParticle(flags, u, kHasPair);
+        atomicOr(&flags[t], kCandidate);
+        atomicOr(&flags[u], kCandidate);
       }
-      appendWork(S, newT, t);
-      appendWork(S, newU, u);
-      if (S.kept) appendList(S.kept, S.ctl + kCtlKept, keep, c0 + 32 * j + lane);
+      appendList(S.kept, S.ctl + kCtlKept, keep, c0 + 32 * j + lane);
     }
+  }
+}
+
+// Where each pair of the compact list sits in its partner's row: the entry of
+// the lower-ID slot t in the row of u (rows are symmetric: the pair search
+// decides both directions with the same expression).  0xFFFF when absent (a
+// row emptied for lack of room).  Grid-stride over the pairs, whose count is
+// known on the device only.
+__global__ void __launch_bounds__(256) k_link(DevState S, const int* gate) {
+  if (gatedOff(gate)) return;
+  const int np = S.ctl[kCtlPairs];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < np; k += gridDim.x * blockDim.x) {
+    const int2 pr = S.upairs[k];
+    const int t = pr.x;
+    const int u = (int)((unsigned)pr.y & ((1u << 27) - 1u));
+    const int nu = S.npairs[u];
+    const int* row = S.pairs + S.pair_off[u];
+    int eu = 0xFFFF;
+    for (int e = 0; e < nu; ++e)
+      if ((int)((unsigned)row[e] & ((1u << 27) - 1u)) == t) { eu = e; break; }
+    S.epos[k] = (S.epos[k] & 0xFFFF) | (eu << 16);
+  }
+}
+
+// Diagnostics: every entry and wall slot starts at +inf (no contact); the
+// pair kernel records the pairs it evaluates.
+__global__ void k_diag_prefill(DevState S) {
+  const double inf = __longlong_as_double(0x7ff0000000000000ll);
+  const long long ne = S.ctl[kCtlEntries] < 0 ? 0 : min(S.ctl[kCtlEntries], S.pair_cap);
+  const long long nw = (long long)S.n * S.max_walls;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ne + nw; i += stride) {
+    if (i < ne) S.pair_delta[i] = inf;
+    else S.wall_delta[i - ne] = inf;
   }
 }
 
@@ -494,8 +650,8 @@ __global__ void k_coordination_by_id(DevState S, int* out, int id_base) {
   if (t >= S.n) return;
   int i = S.id[t] - id_base;
   if (i < 0 || i >= S.n) return;
-  const int np = min(S.npairs[t], kPairCap);
-  const double* pd = S.pair_delta + (size_t)t * kPairCap;
+  const int np = S.npairs[t];
+  const double* pd = S.pair_delta + S.pair_off[t];
   int c = 0;
   for (int e = 0; e < np; ++e) c += pd[e] < 0. ? 1 : 0;
   const int nw = S.grids[S.inst[t]].wall_count;
@@ -559,6 +715,9 @@ __global__ void k_load_state(DevState S, const double* x, const double* v, const
   }
   S.disp[i] = 0.f; S.disp[cap + i] = 0.f; S.disp[2 * cap + i] = 0.f;
   S.wrap[i] = 0;
+  // a new (or reloaded) polyhedron starts its support search where
+  // Polyhedron::BuildPolyhedron leaves it
+  if (S.curv) S.curv[i] = S.types[type_by_id[i]].poly_start;
   if (!wbf) {
     // q* (w, q) (ParticleKinematics.cpp:220-221)
     dq qq = qmk(mk(q[4 * i], q[4 * i + 1], q[4 * i + 2]), q[4 * i + 3]);
@@ -651,7 +810,30 @@ void launch_scan(DevState const& S, const int* gate, cudaStream_t st) {
   int ntiles = blocks(S.ncells, kScanTile);
   k_scan_tiles<<<ntiles, kScanTile, 0, st>>>(S.cell_count, S.cell_start, S.scan_tmp, S.ncells, gate);
   k_scan_sums<<<1, kScanTile, 0, st>>>(S.scan_tmp, ntiles, gate);
-  k_scan_add<<<ntiles, kScanTile, 0, st>>>(S.cell_start, S.scan_tmp, S.cell_count, S.ncells, gate);
+  k_scan_add<<<ntiles, kScanTile, 0, st>>>(S.cell_start, S.scan_tmp, S.cell_count, S.ncells, gate,
+                                           nullptr);
+}
+void launch_row_scan(DevState const& S, const int* gate, cudaStream_t st) {
+  if (!S.n) return;
+  int ntiles = blocks(S.n, kScanTile);
+  k_scan_tiles<<<ntiles, kScanTile, 0, st>>>(S.npairs, S.pair_off, S.pair_scan_tmp, S.n, gate);
+  k_scan_sums<<<1, kScanTile, 0, st>>>(S.pair_scan_tmp, ntiles, gate);
+  k_scan_add<<<ntiles, kScanTile, 0, st>>>(S.pair_off, S.pair_scan_tmp, S.npairs, S.n, gate, S.ctl);
+}
+void launch_filter(DevState const& S, cudaStream_t st) {
+  if (!S.n) return;
+  const int pblocks = S.any_walls ? blocks(S.n, 256) : 0;
+  // about 4 pairs per particle until the leapfrog start has counted them
+  const int qblocks = S.filter_qblocks > 0
+                          ? S.filter_qblocks
+                          : (S.n + 64 * kFilterUnroll - 1) / (64 * kFilterUnroll);
+  k_filter<<<pblocks + qblocks, 256, 0, st>>>(S, pblocks);
+}
+void launch_link(DevState const& S, const int* gate, cudaStream_t st) {
+  if (S.n) k_link<<<4 * S.nsm, 256, 0, st>>>(S, gate);
+}
+void launch_diag_prefill(DevState const& S, cudaStream_t st) {
+  if (S.n && S.pair_delta) k_diag_prefill<<<8 * S.nsm, 256, 0, st>>>(S);
 }
 void launch_place(DevState const& S, const int* gate, cudaStream_t st) {
   if (S.n) k_place<<<blocks(S.n, 256), 256, 0, st>>>(S, gate);
@@ -674,14 +856,6 @@ void launch_move(DevState const& S, int flags, int fast, cudaStream_t st) {
   if (!fast) launchAfterPrevious(k_move<false, false>, nb, 256, st, M, flags);   // basis tested at run time
   else if (S.basis) launchAfterPrevious(k_move<true, true>, nb, 256, st, M, flags);
   else launchAfterPrevious(k_move<true, false>, nb, 256, st, M, flags);
-}
-void launch_filter(DevState const& S, cudaStream_t st) {
-  if (!S.n) return;
-  const int pblocks = S.any_walls ? blocks(S.n, 256) : 0;
-  // about 4 pairs per particle until the leapfrog start has counted them
-  const int qblocks =
-      S.filter_qblocks > 0 ? S.filter_qblocks : (S.n + 64 * kFilterUnroll - 1) / (64 * kFilterUnroll);
-  k_filter<<<pblocks + qblocks, 256, 0, st>>>(S, pblocks);
 }
 void launch_fill64(unsigned long long* p, size_t n, unsigned long long value, cudaStream_t st) {
   if (n) k_fill64<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p, n, value);

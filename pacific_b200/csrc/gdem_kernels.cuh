@@ -27,21 +27,36 @@ inline void launchAfterPrevious(void (*k)(KArgs...), unsigned grid, unsigned blo
 enum StepFlags : int {
   kStepClose = 2,     // closing kick of the step that ends here (dt / 2)
   kStepMove = 4,      // opening kick (dt / 2) and drift (dt) of the next step
-  kStepStoreFT = 8,   // write F, T of particles without contact (last step of a call)
+  kStepStoreFT = 8,   // write F, T back (last evaluation of a call, leapfrog start)
+  kStepSum = 16,      // F, T of this evaluation from the pair kernel's shares
 };
-// nact[t], set by the contact filter (atomically: both particles of a kept
-// pair are flagged) and cleared by k_move: kHasPair when a pair-list entry
-// of t passed the bounding-sphere test, kNearWall when a wall may touch t,
-// kListed once t is on the force kernels' work list (0: no contact possible).
-constexpr int kHasPair = 1;
-constexpr int kNearWall = 2;
-constexpr int kListed = 4;
+// nact[t], the particle's flag word for this evaluation, cleared by k_move:
+// kCandidate, set by the contact filter, when the particle is a partner of a
+// pair the filter kept or near a wall (only then can it receive a share);
+// then, set by the pair kernel (atomically: both partners of a pair in
+// contact set theirs), bit e (e < kMaskEntries) when entry e of its row holds
+// a share of this evaluation, kFarEntry when an entry at or beyond
+// kMaskEntries does (those are found by their tags), kNearWall when its wall
+// share is set.  A particle without kCandidate carries its weight only.
+constexpr int kMaskEntries = 29;
+constexpr unsigned kEntryBits = (1u << kMaskEntries) - 1u;
+constexpr unsigned kCandidate = 1u << 29;
+constexpr unsigned kFarEntry = 1u << 30;
+constexpr unsigned kNearWall = 1u << 31;
+__device__ __forceinline__ unsigned entryBit(int e) {
+  return e < kMaskEntries ? (1u << e) : kFarEntry;
+}
 
 // gdem_integrate.cu
 void launch_decide(DevState const& S, cudaGraphConditionalHandle h, int use_handle,
                    cudaStream_t st);
 void launch_bin(DevState const& S, const int* gate, cudaStream_t st);
 void launch_scan(DevState const& S, const int* gate, cudaStream_t st);
+// exclusive scan of the row lengths into pair_off (total into kCtlEntries)
+void launch_row_scan(DevState const& S, const int* gate, cudaStream_t st);
+void launch_filter(DevState const& S, cudaStream_t st);
+void launch_link(DevState const& S, const int* gate, cudaStream_t st);
+void launch_diag_prefill(DevState const& S, cudaStream_t st);
 void launch_place(DevState const& S, const int* gate, cudaStream_t st);
 void launch_cellsort(DevState const& S, const int* gate, cudaStream_t st);
 void launch_permute(DevState const& S, const int* gate, cudaStream_t st);
@@ -49,7 +64,6 @@ void launch_copyback(DevState const& S, const int* gate, cudaStream_t st);
 // fast: the FP32-split leapfrog (reciprocals, series; not the reference's
 // operation order)
 void launch_move(DevState const& S, int flags, int fast, cudaStream_t st);
-void launch_filter(DevState const& S, cudaStream_t st);
 void launch_fill64(unsigned long long* p, size_t n, unsigned long long value, cudaStream_t st);
 void launch_scatter_by_id(DevState const& S, double* x, double* v, double* w, double* wbf,
                           double* q, double* F, double* T, int id_base, cudaStream_t st);
@@ -65,12 +79,12 @@ void launch_vstats(DevState const& S, double* part, double* out, cudaStream_t st
 void launch_set_velocities(DevState const& S, const double* v, const double* w, cudaStream_t st);
 void launch_pair_counts(DevState const& S, unsigned long long* out, cudaStream_t st);
 
-// gdem_contact64.cu (FP64 mode)
-void launch_pairs64(DevState const& S, const int* gate, cudaStream_t st);
-void launch_forces64(DevState const& S, int sparse, cudaStream_t st);
+// gdem_contact64.cu (FP64 mode); fill = 0 counts the rows, 1 writes them
+void launch_pairs64(DevState const& S, const int* gate, int fill, cudaStream_t st);
+void launch_pairlaw64(DevState const& S, cudaStream_t st);
 
 // gdem_contact32.cu (FP32-split mode)
-void launch_pairs32(DevState const& S, const int* gate, cudaStream_t st);
-void launch_forces32(DevState const& S, int sparse, cudaStream_t st);
+void launch_pairs32(DevState const& S, const int* gate, int fill, cudaStream_t st);
+void launch_pairlaw32(DevState const& S, cudaStream_t st);
 
 }  // namespace gdem

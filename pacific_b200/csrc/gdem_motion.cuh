@@ -318,41 +318,6 @@ __device__ __forceinline__ void advanceParticle(DevState const& S, int t, TypeDe
                           (float)x.z + (float)wrapGet(wr, 2) * bg.Lf[2], (float)tp.radius);
 }
 
-// The FP32 bounding-sphere test of a pair-list entry: the centres of the two
-// bounding spheres (FP32 continuous positions, entry image shift) are closer
-// than the sum of the radii plus the margin that covers the FP32 rounding, so
-// the kept entries are a superset of the contacts.  The contact filter and the
-// force kernels call this same function and so take the same decisions.
-__device__ __forceinline__ bool boundingOverlap(GridDesc const& bg, float4 pt, float4 pu,
-                                                unsigned ent) {
-  const int code = (int)(ent >> 27);
-  const float dx = (pu.x - pt.x) + (float)(code % 3 - 1) * bg.Lf[0];
-  const float dy = (pu.y - pt.y) + (float)((code / 3) % 3 - 1) * bg.Lf[1];
-  const float dz = (pu.z - pt.z) + (float)(code / 9 - 1) * bg.Lf[2];
-  const float R = pt.w + pu.w + bg.filt_margin;
-  return dx * dx + dy * dy + dz * dz <= R * R;
-}
-
-// Bounding-sphere tests of the entries e0 .. e0 + kProbe - 1 of a pair list
-// of np entries (seg), with all their loads issued before the first test;
-// bit j of the result is set when entry e0 + j is kept.
-constexpr int kProbe = 8;
-__device__ __forceinline__ unsigned probeEntries(DevState const& S, GridDesc const& bg, float4 pt,
-                                                 const int* seg, int e0, int np) {
-  unsigned en[kProbe];
-  float4 pu[kProbe];
-#pragma unroll
-  for (int j = 0; j < kProbe; ++j) en[j] = e0 + j < np ? (unsigned)seg[e0 + j] : 0u;
-#pragma unroll
-  for (int j = 0; j < kProbe; ++j)
-    pu[j] = e0 + j < np ? S.posf[en[j] & ((1u << 27) - 1u)] : make_float4(0.f, 0.f, 0.f, 0.f);
-  unsigned keep = 0u;
-#pragma unroll
-  for (int j = 0; j < kProbe; ++j)
-    if (e0 + j < np && boundingOverlap(bg, pt, pu[j], en[j])) keep |= 1u << j;
-  return keep;
-}
-
 // Image shift (in periods) of list entry ent (partner u) of slot t: the
 // shift recorded at the rebuild (bits 27-31 of the entry, shiftCode),
 // corrected by the wraps of both particles since the rebuild.

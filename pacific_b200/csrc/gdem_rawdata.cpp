@@ -142,8 +142,8 @@ extern "C" {
 int gdem_rawdata_start(gdem_handle h, const char* root, int binary, int append, double time) {
   return guardedIo([&] {
     if (!h || !root) throw std::runtime_error("invalid arguments");
-    // one system: a batch has a second instance grid
-    if (gdem_grid(h, 1, nullptr, nullptr, nullptr) == GDEM_OK)
+    // one system, not a batch of instances
+    if (gdem_num_instances(h) != 1)
       throw std::runtime_error("a RawData writer covers one system, not a batch");
     std::lock_guard<std::mutex> lock(g_mu);
     auto it = g_writers.find(h);

@@ -5,11 +5,9 @@
 
 namespace gdem {
 
-// Maximum number of candidate partners recorded per particle in the
-// per-particle segment of the pair list.
-constexpr int kPairCap = 32;
-// compact pair list (each pair once, from its lower ID): entries per particle
-constexpr int kUpperCap = 16;
+// Most entries of one particle's row of the pair list (an entry's position
+// in its row is kept in 16 bits).
+constexpr int kRowMax = 65535;
 // Material indices per instance (materials are bits in the reference,
 // ContactBuilderFactory.cpp:176-192; here they are indices 0..kMaxMat-1).
 constexpr int kMaxMat = 8;
@@ -24,7 +22,7 @@ enum StatusBits : int {
   kErrHashFull = 1 << 3,         // contact-history table has no free slot
   kErrGjkMaxIter = 1 << 4,       // GJK hit its iteration cap
   kErrTimeout = 1 << 5,          // a bounded device wait gave up
-  kErrPairsFull = 1 << 6,        // a particle has more than kPairCap candidates
+  kErrPairsFull = 1 << 6,        // the pair list outgrew its allocation (or a row kRowMax)
 };
 
 // Words of the device control block (DevState::ctl).
@@ -33,10 +31,12 @@ enum CtlWords : int {
   kCtlActive = 1,   // this step rebuilds the pair list (set by k_decide)
   kCtlEpoch = 2,    // force evaluations so far (tags the contact-history keys)
   kCtlRebuilds = 3, // pair-list rebuilds so far
-  kCtlWork = 4,     // particles the force kernel must evaluate this step (work list length)
+  kCtlWork = 4,     // particles near a wall this evaluation (contact filter)
   kCtlPairs = 5,    // pairs of the compact pair list (set by the rebuild)
-  kCtlKept = 6,     // pairs kept by this step's contact filter (two-phase force path)
-  kCtlWords = 8
+  kCtlKept = 6,     // pairs kept by this evaluation's contact filter
+  kCtlEntries = 7,  // pair-list entries of the last rebuild
+  kCtlEntriesMax = 8,  // most entries any rebuild needed since the last allocation check
+  kCtlWords = 16
 };
 
 // One independent simulation ("instance").  A single Grains3D system is a
@@ -78,6 +78,9 @@ struct TypeDesc {
   double scaling[3];     // crust shrink factors (extent - crust) / extent
   int poly_begin;        // first vertex of a polyhedron in the vertex table
   int poly_count;        // its vertex count
+  int poly_start;        // the current vertex of a new particle (Polyhedron::BuildPolyhedron:
+                         // the first vertex with a neighbour)
+  int pad_p;
   double inv_mass;       // 1 / (mass c) and 1 / inertia (FP32-split leapfrog)
   double inv_inertia[3];
   double density;

@@ -95,6 +95,12 @@ def library() -> ctypes.CDLL:
         "gdem_download_cells": ([_P, _IP], ctypes.c_int),
         "gdem_download_coordination": ([_P, _IP], ctypes.c_int),
         "gdem_download_classes": ([_P, _IP], ctypes.c_int),
+        "gdem_download_ids": ([_P, _IP], ctypes.c_int),
+        "gdem_upload_support_vertices": ([_P, _IP], ctypes.c_int),
+        "gdem_download_support_vertices": ([_P, _IP], ctypes.c_int),
+        "gdem_contact_features": ([_P, _DP, _DP, ctypes.POINTER(ctypes.c_int64), _DP, ctypes.c_int],
+                                  ctypes.c_int),
+        "gdem_num_instances": ([_P], ctypes.c_int),
         "gdem_rawdata_start": ([_P, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_double],
                                ctypes.c_int),
         "gdem_rawdata_write": ([_P, ctypes.c_double], ctypes.c_int),
@@ -294,6 +300,33 @@ class Grains:
     def download_classes(self):
         c = np.empty(self.n, np.int32)
         self._check(library().gdem_download_classes(self._h, _ip(c)))
+        return c
+
+    def contact_features(self, reset=False):
+        """{overlap_max, overlap_mean, evaluation_of_max, gjk_iterations_mean}
+        over the evaluations since the last reset (the contact features
+        Grains3D prints at the end of a run)."""
+        a, b, d = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        c = ctypes.c_int64()
+        self._check(library().gdem_contact_features(self._h, ctypes.byref(a), ctypes.byref(b),
+                                                    ctypes.byref(c), ctypes.byref(d), int(reset)))
+        return {"overlap_max": a.value, "overlap_mean": b.value, "evaluation_of_max": c.value,
+                "gjk_iterations_mean": d.value}
+
+    def upload_support_vertices(self, vertex):
+        """Current polyhedron support vertex of each particle, by ID."""
+        v = np.ascontiguousarray(vertex, dtype=np.int32)
+        self._check(library().gdem_upload_support_vertices(self._h, _ip(v)))
+
+    def download_support_vertices(self):
+        v = np.empty(self.n, np.int32)
+        self._check(library().gdem_download_support_vertices(self._h, _ip(v)))
+        return v
+
+    def download_ids(self):
+        """Reference particle IDs (1-based) by particle index."""
+        c = np.empty(self.n, np.int32)
+        self._check(library().gdem_download_ids(self._h, _ip(c)))
         return c
 
     def rawdata_start(self, root, binary=False, append=False, time=0.0):

@@ -118,6 +118,11 @@ def run(name):
                 snapshot(r, f"s{m}", out)
                 id0, id1, dl, pt, f = o.contacts()
                 out[f"s{m}_scale"] = contact_scale(len(sc.type), id0, id1, f)
+                # each particle's polyhedron support vertex (Polyhedron::
+                # m_curr_vertex): hidden state of the reference, taken from the
+                # restatement, which reproduces the reference bit for bit
+                assert np.array_equal(o.state()["x"], out[f"s{m}_x"])
+                out[f"s{m}_curv"] = o.support_vertices()
         np.savez_compressed(HERE / f"{name}.npz", **out)
         print(f"wrote {name}.npz ({len(sc.type)} particles, steps {marks})")
 
@@ -213,6 +218,35 @@ def run_rawdata(mode):
     print(f"wrote rawdata_settling_{mode}.npz (RawData files of the reference, {mode})")
 
 
+FEATURE_MARKS = (0, 400, 1200)
+
+
+def run_features():
+    """The contact-features fixture: 300 spheres settling in the walled box
+    from their inserted state, with the reference's own contact features
+    (AppCollision: largest and mean overlap over all contacts of all
+    evaluations so far, time of the largest, mean GJK iterations) after the
+    leapfrog start and after 400 and 1,200 steps."""
+    sc = scenarios.settling_box(n=300, seed=41)
+    out = {"xml": np.array(sc.xml()), "type": sc.type, "marks": np.array(FEATURE_MARKS)}
+    with tempfile.TemporaryDirectory() as d:
+        xml = sc.write_xml(Path(d) / "features.xml")
+        r = _quiet(reference.Reference, xml)
+        assert _quiet(r.set_particles, sc.type, sc.x, sc.v, sc.w, sc.q) == 0
+        s0 = r.state()
+        for k in ("x", "v", "w", "q"):
+            out[f"{k}0"] = s0[k]
+        assert _quiet(r.init) == 0
+        done = 0
+        for m in FEATURE_MARKS:
+            assert _quiet(r.step, m - done) == 0
+            done = m
+            out[f"s{m}_features"] = r.contact_features()
+            out[f"s{m}_x"] = r.state()["x"]
+    np.savez_compressed(HERE / "contact_features.npz", **out)
+    print("wrote contact_features.npz (300 particles, features at steps", FEATURE_MARKS, ")")
+
+
 def main():
     import subprocess
     if not reference.available():
@@ -222,6 +256,7 @@ def main():
     subprocess.run([sys.executable, __file__, "reload"], check=True)
     for mode in ("text", "binary"):
         subprocess.run([sys.executable, __file__, "rawdata", mode], check=True)
+    subprocess.run([sys.executable, __file__, "features"], check=True)
 
 
 if __name__ == "__main__":
@@ -230,6 +265,8 @@ if __name__ == "__main__":
             run_reload()
         elif sys.argv[1] == "rawdata":
             run_rawdata(sys.argv[2])
+        elif sys.argv[1] == "features":
+            run_features()
         else:
             run(sys.argv[1])
     else:

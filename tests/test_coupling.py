@@ -187,3 +187,32 @@ def test_basilisk_rawdata_output(tmp_path, lib):
     c = (tmp_path / "out_coordinationNumber.dat").read_text().splitlines()
     assert c[0].split() == ["0"] * sc.n
     assert np.array_equal(np.array(c[1].split(), dtype=int), coord) and coord.sum() > 0
+
+
+def test_basilisk_hybrid_reload(tmp_path, lib):
+    """Init_Grains reads the reload's reading mode (the word after its
+    "NbFiles" line, AllComponents::read) and, for "Hybrid", the binary
+    particle file <stem>_Particles.bin: the state it starts from is the one
+    of the same reload written as text, token for token in the stream, and
+    the IDs and classes come from the loaded file."""
+    sc = _settled(tmp_path)
+    g = Grains(str(tmp_path / "coupled.xml"), FP64)
+    g.read_reload_particles(tmp_path / "res_Particles")
+    g.write_reload_particles_hybrid(tmp_path / "resH_Particles.bin")
+    g.close()
+    (tmp_path / "resH.resA").write_text(f"NbFiles 1\nHybrid {sc.n}\n")
+    (tmp_path / "coupledH.xml").write_text(
+        (tmp_path / "coupled.xml").read_text().replace(str(tmp_path / "res.resA"),
+                                                       str(tmp_path / "resH.resA")))
+    b = _basilisk()
+    size = ctypes.c_int(0)
+    streams = []
+    for xml in ("coupled.xml", "coupledH.xml"):
+        b.Init_Grains(str(tmp_path / xml).encode(), 1000.0, False, True)
+        npart, nobs = ctypes.c_size_t(0), ctypes.c_size_t(0)
+        b.NumberOfRigidBodiesInBasilisk(ctypes.byref(npart), ctypes.byref(nobs))
+        assert npart.value == sc.n
+        b.Simu_Grains(4e-5)
+        streams.append(ctypes.string_at(b.GrainsToBasilisk(ctypes.byref(size))).decode())
+    assert streams[0] == streams[1]
+    assert int(streams[0].split()[0]) == sc.n

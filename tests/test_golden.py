@@ -97,6 +97,9 @@ def _gpu_step_from_golden(g, xml, k, k1, precision, tol):
     G.upload_state(g["type"], g[f"s{k}_x"], g[f"s{k}_v"], g[f"s{k}_w"], g[f"s{k}_q"])
     G.upload_basis(g[f"s{k}_basis"])
     G.upload_forces(g[f"s{k}_F"], g[f"s{k}_T"])
+    if f"s{k}_curv" in g:
+        # the reference's polyhedron support vertices at that state
+        G.upload_support_vertices(g[f"s{k}_curv"])
     own, par = g[f"s{k}_hist_owner"], g[f"s{k}_hist_partner"]
     G.upload_history(own, par, g[f"s{k}_hist_kdelta"], g[f"s{k}_hist_prevn"])
     G.set_diagnostics(True)
@@ -139,6 +142,9 @@ def test_gpu_fp64_step_matches_reference(tmp_path, lib, name):
             # vertex 0.  Such contacts agree in overlap and normal but their
             # contact point can move within the contact face.
             if fe.size:
+                print(f"{name} step {k1}: {fe.size} particles in contact, "
+                      f"{int((fe > 1e-10).sum())} above 1e-10 (force), "
+                      f"{int((te > 1e-10).sum())} (torque); max {fe.max():.2e} / {te.max():.2e}")
                 assert np.median(fe) <= 1e-9 and fe.max() <= 1e-5
                 assert np.median(te) <= 1e-9 and te.max() <= 1e-4
         else:
