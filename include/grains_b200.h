@@ -48,7 +48,7 @@ typedef struct gdem_system* gdem_handle;
 #define GDEM_ST_HASH_FULL 0x08        /* contact-history table full */
 #define GDEM_ST_GJK_MAXITER 0x10      /* GJK iteration cap reached */
 #define GDEM_ST_TIMEOUT 0x20          /* a bounded device wait gave up */
-#define GDEM_ST_PAIRS_FULL 0x40       /* per-particle candidate list overflowed */
+#define GDEM_ST_PAIRS_FULL 0x40       /* the pair list's allocation was too small at a rebuild (rows emptied; grown before the next call) */
 
 /* Builds a system from a Grains3D XML input (Construction: LinkedCell,
  * Origin, Periodicity, Particles, Obstacles, ContactForceModels; Forces:
@@ -251,7 +251,9 @@ int gdem_download_state(gdem_handle h, double* x, double* v, double* w, double* 
  * gdem_upload_state + gdem_upload_basis + gdem_upload_forces +
  * gdem_upload_history: the leapfrog continues from the stored forces,
  * without gdem_init); periodic clones (tag 2) and inactive particles are
- * skipped. */
+ * skipped.  When the XML's Construction/Reload has Velocity="Reset", the
+ * loaded velocities are zero and the quaternions the identity
+ * (AllComponents::resetKinematics, AllComponents.cpp:762-771). */
 int gdem_write_reload_particles(gdem_handle h, const char* path);
 int gdem_read_reload_particles(gdem_handle h, const char* path);
 /* The same particle file in the hybrid (binary) form of a Format2024 reload

@@ -41,3 +41,12 @@ for s in $SRCS "$HERE/shim/grains_shim.cpp" "$HERE/ref_harness.cpp"; do
 done | xargs -r -P "$JOBS" -I{} sh -c "$CXX $FLAGS -c {} -o $OUT/obj/\$(basename {} .cpp).o"
 $CXX -shared -o "$OUT/libgrains_ref.so" "$OUT"/obj/*.o -lz
 echo "built $OUT/libgrains_ref.so"
+# the reference's Basilisk coupling interface over the same objects (the
+# checker of the coupling library libgrains_b200_basilisk.so)
+BAS=$REF/InterfaceCBasilisk
+if [ ! -f "$OUT/basilisk.o" ] || [ "$BAS/src/InterfaceGrains3DBasilisk.cpp" -nt "$OUT/basilisk.o" ]; then
+  $CXX $FLAGS -I"$BAS/include" -c "$BAS/src/InterfaceGrains3DBasilisk.cpp" -o "$OUT/basilisk.o"
+fi
+$CXX -shared -o "$OUT/libgrains_ref_basilisk.so" "$OUT/basilisk.o" \
+    $(ls "$OUT"/obj/*.o | grep -v ref_harness.o) -lz
+echo "built $OUT/libgrains_ref_basilisk.so"

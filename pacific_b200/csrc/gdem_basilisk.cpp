@@ -11,10 +11,10 @@
 // What each entry does:
 //   Init_Grains       the XML's system (FP64; GRAINS_B200_PRECISION=fp32split
 //                     selects the FP32-split mode) with the particles of its
-//                     Construction/Reload file (the "<stem>_Particles" file of
-//                     the Format2024 reload, or "<stem>_Particles.bin" when the
-//                     reload's reading mode is Hybrid, AllComponents::read and
-//                     read_particles),
+//                     Construction/Reload file (the "<stem>_Particles.result"
+//                     file of the Format2024 reload, or
+//                     "<stem>_Particles.result.bin" when the reload's reading
+//                     mode is Hybrid, AllComponents::read and read_particles),
 //                     the fluid density in the weight and, with
 //                     b_fluidcorrectedacc, in the coupling factor
 //                     (GrainsCoupledWithFluid::do_before_time_stepping, :54-97).
@@ -80,9 +80,13 @@ std::string d16(double v) {
 // The reading mode of a Format2024 reload file: the word after the
 // "NbFiles <n>" line, "Hybrid" or "Text" (AllComponents::write, Component/
 // src/AllComponents.cpp:1370-1374; AllComponents::read, :1114-1126).  Returns
-// false when the file cannot be read or has no such line.
+// false when the file cannot be read or has no such line.  The header is
+// the reload name with ".result" appended (Grains::Construction, Base/src/
+// Grains.cpp:811, GrainsExec::fullResultFileName); the name as written is
+// tried when that file does not exist.
 bool readReloadMode(const std::string& reload, bool& hybrid) {
-  FILE* f = std::fopen(reload.c_str(), "r");
+  FILE* f = std::fopen((reload + ".result").c_str(), "r");
+  if (!f) f = std::fopen(reload.c_str(), "r");
   if (!f) return false;
   char tok[4096];
   bool found = false;
@@ -151,11 +155,13 @@ void Init_Grains(char const* inputfile, double fluid_rho, const bool b_restart,
     return;
   }
   // AllComponents::read_particles (:1152-1164): the reload name up to its
-  // first '.', then "_Particles", with ".bin" in the Hybrid reading mode
+  // first '.', then "_Particles" and ".result" (GrainsExec::
+  // fullResultFileName, Base/src/GrainsExec.cpp:708-716), with ".bin" after
+  // it in the Hybrid reading mode
   std::string pfile(reload);
   const size_t dot = pfile.find_first_of('.');
   if (dot != std::string::npos) pfile.erase(dot);
-  pfile += "_Particles";
+  pfile += "_Particles.result";
   bool hybrid = false;
   if (!readReloadMode(reload, hybrid)) {
     // no reload header beside the particle file: the binary particle file

@@ -88,6 +88,7 @@ struct InstanceDesc {
   double min_dt, max_dt;
   int ndt;
   std::string reload_file;   // Construction/Reload Filename, if any
+  bool reload_reset = false; // Reload Velocity="Reset": kinematics zeroed on reading
   std::string rawdata_root;  // Simulation/PostProcessing/Writers/RawData Name, if any
   bool rawdata_binary = false;
   int nmat;
@@ -471,8 +472,13 @@ InstanceDesc readInstance(std::string const& path) {
   I.max_dt = ts->has("maxdt") ? ts->attrD("maxdt") : I.dt;
   I.ndt = ts->has("ndt") ? ts->attrI("ndt") : 1;
   I.reload_file.clear();
-  if (XmlNode const* rl = root->find("Reload"))
+  I.reload_reset = false;
+  if (XmlNode const* rl = root->find("Reload")) {
     if (rl->has("Filename")) I.reload_file = rl->attr("Filename");
+    // Grains::Construction (Base/src/Grains.cpp:842-843) then
+    // AllComponents::resetKinematics (Component/src/AllComponents.cpp:762-771)
+    I.reload_reset = rl->has("Velocity") && rl->attr("Velocity") == "Reset";
+  }
   // a RawData post-processing writer (PostProcessingWriterBuilderFactory,
   // PostProcessing/src/PostProcessingWriterBuilderFactory.cpp:19-20;
   // RawDataPostProcessingWriter ctor: Name, WritingMode="Binary")
@@ -2090,6 +2096,14 @@ static int readReloadParticles(gdem_handle h, const char* path, bool hybrid) {
       }
       for (int d = 0; d < 4; ++d) q[4 * i + d] = r.q[d];
       for (int k = 0; k < 9; ++k) B[9 * i + k] = r.B[k];
+      if (s->inst[0].reload_reset) {
+        // ParticleKinematics::reset (Component/src/ParticleKinematics.cpp:
+        // 165-170): both velocities and the kinematics quaternion; the
+        // orientation of the transform (the basis) is kept
+        for (int d = 0; d < 3; ++d) v[3 * i + d] = w[3 * i + d] = 0.;
+        q[4 * i] = q[4 * i + 1] = q[4 * i + 2] = 0.;
+        q[4 * i + 3] = 1.;
+      }
     }
     auto check = [](int code) {
       if (code != GDEM_OK) throw std::runtime_error(g_last_error);

@@ -63,7 +63,7 @@ def _settled(tmp_path, n=200, steps=300):
     g.upload_state(sc.type, sc.x, sc.v, sc.w, sc.q)
     g.do_before_time_stepping()
     g.step(steps)
-    g.write_reload_particles(tmp_path / "res_Particles")
+    g.write_reload_particles(tmp_path / "res_Particles.result")
     g.close()
     (tmp_path / "coupled.xml").write_text(_coupled_xml(sc, str(tmp_path / "res.resA")))
     return sc
@@ -90,7 +90,7 @@ def test_basilisk_abi(tmp_path, lib):
     # a reference run through the plain ABI: same file, same fluid, ndt = 4
     # sub-steps of dt_fluid / 4 (dt_fluid / ndt = 1e-5 lies in [mindt, maxdt])
     ref = Grains(str(tmp_path / "coupled.xml"), FP64)
-    ref.read_reload_particles(tmp_path / "res_Particles")
+    ref.read_reload_particles(tmp_path / "res_Particles.result")
     ref.set_fluid(1000.0, True)
     ref.set_time_step(4e-5 / 4)
     b.Simu_Grains(4e-5)
@@ -170,7 +170,7 @@ def test_basilisk_rawdata_output(tmp_path, lib):
     b.Simu_Grains(4e-5)
     b.SaveResults_Grains()
     ref = Grains(str(tmp_path / "coupled.xml"), FP64)
-    ref.read_reload_particles(tmp_path / "res_Particles")
+    ref.read_reload_particles(tmp_path / "res_Particles.result")
     ref.set_fluid(1000.0, True)
     ref.set_time_step(1e-5)
     ref.step(3)
@@ -192,15 +192,16 @@ def test_basilisk_rawdata_output(tmp_path, lib):
 def test_basilisk_hybrid_reload(tmp_path, lib):
     """Init_Grains reads the reload's reading mode (the word after its
     "NbFiles" line, AllComponents::read) and, for "Hybrid", the binary
-    particle file <stem>_Particles.bin: the state it starts from is the one
+    particle file <stem>_Particles.result.bin: the state it starts from is the one
     of the same reload written as text, token for token in the stream, and
     the IDs and classes come from the loaded file."""
     sc = _settled(tmp_path)
     g = Grains(str(tmp_path / "coupled.xml"), FP64)
-    g.read_reload_particles(tmp_path / "res_Particles")
-    g.write_reload_particles_hybrid(tmp_path / "resH_Particles.bin")
+    g.read_reload_particles(tmp_path / "res_Particles.result")
+    g.write_reload_particles_hybrid(tmp_path / "resH_Particles.result.bin")
     g.close()
-    (tmp_path / "resH.resA").write_text(f"NbFiles 1\nHybrid {sc.n}\n")
+    # the reload header: the reload name with ".result" appended
+    (tmp_path / "resH.resA.result").write_text(f"NbFiles 1\nHybrid {sc.n}\n")
     (tmp_path / "coupledH.xml").write_text(
         (tmp_path / "coupled.xml").read_text().replace(str(tmp_path / "res.resA"),
                                                        str(tmp_path / "resH.resA")))
@@ -216,3 +217,80 @@ def test_basilisk_hybrid_reload(tmp_path, lib):
         streams.append(ctypes.string_at(b.GrainsToBasilisk(ctypes.byref(size))).decode())
     assert streams[0] == streams[1]
     assert int(streams[0].split()[0]) == sc.n
+
+
+REF_EXE = Path(__file__).resolve().parent.parent / "oracle" / "_ref" / "grains_b200"
+REF_BASILISK = Path(__file__).resolve().parent.parent / "oracle" / "_ref" / "libgrains_ref_basilisk.so"
+
+
+@pytest.mark.skipif(not (REF_EXE.exists() and REF_BASILISK.exists()),
+                    reason="the reference's executable and Basilisk library were not built")
+def test_basilisk_matches_reference_interface(tmp_path, lib):
+    """The coupling library against the reference's own Basilisk interface
+    (InterfaceGrains3DBasilisk.cpp over the reference's objects) on the same
+    reload: 200 spheres settled for 300 steps by the reference's serial step
+    (Type="Standard", insertion at the initial time, reload written at the
+    end), then Init_Grains (fluid density 1000, corrected acceleration),
+    Simu_Grains over a fluid step of 4e-5 s (4 sub-steps), GrainsToBasilisk,
+    UpdateVelocityGrains, a second fluid step, GrainsToBasilisk.  Both
+    streams agree token for token in their words and counts and to FP64
+    round-off in their numbers; the rigid-body counts are the same."""
+    import os
+    import re
+    import subprocess
+
+    from oracle import ref_basilisk_run
+
+    sc = scenarios.settling_box(n=200, seed=31)
+    np.savetxt(tmp_path / "positions.txt", sc.x, fmt="%.17g")
+    end = 300 * 1e-5
+    text = re.sub(r"<TimeInterval[^>]*/>", f'<TimeInterval Start="0." End="{end!r}"/>', sc.xml())
+    sim = (f'    <RestartFile Name="{tmp_path}/res" WritingMode="Text"/>\n'
+           f'    <TimeSave Start="0." End="{end!r}" Every="{end!r}"/>\n'
+           "    <ParticleInsertion>\n      <Mode Type=\"InitialTime\"/>\n"
+           "      <Order Type=\"Ordered\"/>\n"
+           "      <RandomGeneratorSeed Type=\"UserDefined\" Value=\"7\"/>\n"
+           f"      <ParticlePosition>\n        <File Name=\"{tmp_path}/positions.txt\"/>\n"
+           "      </ParticlePosition>\n      <InitialVelocity Mode=\"Random\">\n"
+           "        <Translational Amplitude=\"0.3\"/>\n        <Angular Amplitude=\"0.\"/>\n"
+           "      </InitialVelocity>\n    </ParticleInsertion>\n")
+    (tmp_path / "settle.xml").write_text(text.replace("  </Simulation>", sim + "  </Simulation>"))
+    r = subprocess.run([str(REF_EXE), "settle.xml"], cwd=str(tmp_path), capture_output=True,
+                       text=True, timeout=600, env=dict(os.environ, GRAINS_HOME=str(tmp_path)))
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    reload = (tmp_path / "res_RFTable.txt").read_text().split()[-1]
+    # the reference's coupled application is built for Type="CoupledFluid"
+    # (GrainsBuilderFactory::createCoupledWithFluid)
+    coupled = sc.xml().replace('<Grains3D Type="Standard">', '<Grains3D Type="CoupledFluid">')
+    coupled = coupled.replace('<TimeStep dt="1e-05"/>',
+                              '<TimeStep mindt="1e-05" maxdt="2e-05" ndt="4"/>')
+    coupled = coupled.replace(
+        "  </Construction>",
+        f'    <Reload Type="new" Filename="{reload}" Velocity="Keep"/>\n  </Construction>')
+    coupled = coupled.replace(
+        "  </Simulation>",
+        f'    <RestartFile Name="{tmp_path}/cres" WritingMode="Text"/>\n  </Simulation>')
+    xml = tmp_path / "coupled.xml"
+    xml.write_text(coupled)
+    rows = np.zeros((sc.n, 6))
+    rows[:, 2] = -0.05
+    rows[:, 3] = np.linspace(-1.0, 1.0, sc.n)
+    ref = ref_basilisk_run.run(REF_BASILISK, xml, 1000.0, 4e-5, rows)
+    ours = ref_basilisk_run.run(BASILISK, xml, 1000.0, 4e-5, rows)
+    assert (ours["particles"], ours["obstacles"]) == (ref["particles"], ref["obstacles"]) == (sc.n, 0)
+    for sa, sb in zip(ref["streams"], ours["streams"]):
+        ta, tb = sa.split(), sb.split()
+        assert len(ta) == len(tb) == 1 + 35 * sc.n
+        num_a, num_b = [], []
+        for a, b in zip(ta, tb):
+            try:
+                num_a.append(float(a))
+                num_b.append(float(b))
+            except ValueError:
+                assert a == b
+        fa, fb = np.array(num_a), np.array(num_b)
+        # integers (counts, IDs) and exact constants compare equal; the rest
+        # to FP64 round-off of a contact-laden settled state
+        err = np.abs(fa - fb) / np.maximum(np.abs(fa), 1e-6)
+        print("max relative token difference", err.max())
+        assert err.max() <= 1e-9

@@ -114,3 +114,31 @@ def test_round_trip_continues_the_run(tmp_path, lib, precision):
             assert np.max(np.abs(sa[k] - sb[k])) <= 1e-7 * np.abs(sa[k]).max(), k
     a.close()
     b.close()
+
+
+def test_reload_velocity_reset(golden, tmp_path):
+    """<Reload ... Velocity="Reset"/> (Grains::Construction then
+    AllComponents::resetKinematics, ParticleKinematics::reset): the particles
+    of the file with zero translational and angular velocities and identity
+    quaternions; positions, orientation matrices, forces and contact memory
+    as read."""
+    g, xml, pf = golden
+    text = Path(xml).read_text()
+    assert "<Construction>" in text
+    rxml = tmp_path / "reset.xml"
+    rxml.write_text(text.replace(
+        "<Construction>",
+        f'<Construction>\n    <Reload Type="new" Filename="{tmp_path}/none" Velocity="Reset"/>', 1))
+    keep = Grains(xml, FP64)
+    keep.read_reload_particles(pf)
+    sk = keep.download_state()
+    keep.close()
+    sim = Grains(str(rxml), FP64)
+    sim.read_reload_particles(pf)
+    s = sim.download_state()
+    sim.close()
+    assert np.abs(sk["v"]).max() > 0
+    assert not s["v"].any() and not s["w"].any()
+    assert np.array_equal(s["q"], np.tile([0.0, 0.0, 0.0, 1.0], (len(s["q"]), 1)))
+    for k in ("x", "F", "T"):
+        assert np.array_equal(s[k], sk[k]), k
