@@ -347,6 +347,28 @@ double gdem_last_step_ms(gdem_handle h);
 /* Runs gdem_step's loop as captured CUDA graphs (1) or plain launches (0). */
 int gdem_use_graphs(gdem_handle h, int on);
 
+/* Contact memory of contacts that have ended: dropped at the next force
+ * evaluation (prune = 1, the default: Grains::computeParticlesForceAndTorque,
+ * Base/src/Grains.cpp:459-482, with Component::setContactMapToFalse /
+ * updateContactMap) or kept, so that a pair that touches again resumes its
+ * tangential spring (prune = 0: GrainsCoupledWithFluid::Simulation,
+ * Fluid/src/GrainsCoupledWithFluid.cpp:123-228, which never prunes).  Set it
+ * before the particles are uploaded or read; with prune = 0 the history
+ * tables are four times larger, and a run that fills them raises
+ * GDEM_ST_HASH_FULL. */
+int gdem_set_contact_memory_pruning(gdem_handle h, int prune);
+
+/* The contact force models of a Format2024 reload, in place of the XML's:
+ * header is the reload file ("<name>.result"), whose "<ContactForceModels>
+ * <file> </ContactForceModels>" line names the material-contact file that
+ * ContactBuilderFactory::save wrote beside it; that file (looked for in the
+ * header's directory) gives each material pair's model and parameters as
+ * printed there (ContactBuilderFactory::reload, Component/src/
+ * ContactBuilderFactory.cpp:199-262).  GrainsCoupledWithFluid::Construction
+ * (Fluid/src/GrainsCoupledWithFluid.cpp:238-420) takes its models from there
+ * only, so a coupled run reloads them this way.  One system (not a batch). */
+int gdem_read_reload_contact_models(gdem_handle h, const char* header);
+
 const char* gdem_last_error(void);
 void gdem_destroy(gdem_handle h);
 

@@ -15,9 +15,15 @@
 //                     file of the Format2024 reload, or
 //                     "<stem>_Particles.result.bin" when the reload's reading
 //                     mode is Hybrid, AllComponents::read and read_particles),
-//                     the fluid density in the weight and, with
-//                     b_fluidcorrectedacc, in the coupling factor
-//                     (GrainsCoupledWithFluid::do_before_time_stepping, :54-97).
+//                     the contact force models of the reload's
+//                     material-contact file (GrainsCoupledWithFluid::
+//                     Construction reads them there, not in the XML), the
+//                     fluid density in the weight; the coupling factor
+//                     stays 1, as for the reference's reloaded particles
+//                     whatever b_fluidcorrectedacc is (see Init_Grains).
+//                     The particle classes and obstacles come from the XML,
+//                     which must describe the system the reload was written
+//                     from (the reference takes them from the reload header).
 //   Simu_Grains       sub-steps over the fluid step as
 //                     GrainsCoupledWithFluid::Simulation (:123-133): ndt from
 //                     the XML's TimeStep, dt = dt_fluid / ndt within
@@ -36,8 +42,8 @@
 // Contact memory: the reference's coupled step never prunes a contact map
 // entry whose contact has ended (it skips Grains::computeParticlesForceAnd
 // Torque's setContactMapToFalse / updateContactMap), so a pair that touches
-// again resumes an old tangential spring; here an ended contact's memory is
-// dropped, as in the uncoupled step.
+// again resumes its old tangential spring; the same here
+// (gdem_set_contact_memory_pruning(h, 0)).
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -103,6 +109,22 @@ bool readReloadMode(const std::string& reload, bool& hybrid) {
   return found;
 }
 
+// The reload header (the reload name with ".result" appended, else the
+// name as written) when it names a material-contact file, else "".
+std::string headerWithContactModels(const std::string& reload) {
+  for (const std::string& path : {reload + ".result", reload}) {
+    FILE* f = std::fopen(path.c_str(), "r");
+    if (!f) continue;
+    char tok[4096];
+    bool named = false;
+    while (!named && std::fscanf(f, "%4095s", tok) == 1)
+      named = std::strcmp(tok, "<ContactForceModels>") == 0;
+    std::fclose(f);
+    return named ? path : std::string();
+  }
+  return std::string();
+}
+
 // Particle IDs (1-based) and classes, by particle index, from the handle.
 bool readIds() {
   g_ids.assign((size_t)g_n, 0);
@@ -146,6 +168,9 @@ void Init_Grains(char const* inputfile, double fluid_rho, const bool b_restart,
   const char* prec = std::getenv("GRAINS_B200_PRECISION");
   const int mode = (prec && std::strcmp(prec, "fp32split") == 0) ? GDEM_FP32_SPLIT : GDEM_FP64;
   if (gdem_create(inputfile, mode, &g_sys) != GDEM_OK) { fail("Init_Grains"); return; }
+  // the coupled step keeps the memory of ended contacts
+  // (GrainsCoupledWithFluid::Simulation never prunes it)
+  if (gdem_set_contact_memory_pruning(g_sys, 0) != GDEM_OK) { fail("Init_Grains"); return; }
   char reload[4096];
   if (gdem_reload_filename(g_sys, reload, sizeof(reload)) != GDEM_OK) { fail("Init_Grains"); return; }
   if (!reload[0]) {
@@ -162,6 +187,17 @@ void Init_Grains(char const* inputfile, double fluid_rho, const bool b_restart,
   const size_t dot = pfile.find_first_of('.');
   if (dot != std::string::npos) pfile.erase(dot);
   pfile += "_Particles.result";
+  // GrainsCoupledWithFluid::Construction (Fluid/src/GrainsCoupledWithFluid.
+  // cpp:238-420) takes the contact force models from the reload, as printed
+  // in its material-contact file, and never reads the XML's
+  // <ContactForceModels>
+  // (a particle file without such a header, as this library's
+  // gdem_write_reload_particles writes, keeps the XML's models)
+  const std::string header = headerWithContactModels(reload);
+  if (!header.empty() && gdem_read_reload_contact_models(g_sys, header.c_str()) != GDEM_OK) {
+    fail("Init_Grains");
+    return;
+  }
   bool hybrid = false;
   if (!readReloadMode(reload, hybrid)) {
     // no reload header beside the particle file: the binary particle file
@@ -177,7 +213,16 @@ void Init_Grains(char const* inputfile, double fluid_rho, const bool b_restart,
   if (rc != GDEM_OK) { fail("Init_Grains"); return; }
   g_n = gdem_num_particles(g_sys);
   if (!readIds()) { fail("Init_Grains"); return; }
-  if (gdem_set_fluid(g_sys, fluid_rho, b_fluidcorrectedacc ? 1 : 0) != GDEM_OK) {
+  // The reference's particles of a reload keep a coupling factor of 1 with
+  // either value of b_fluidcorrectedacc: Particle::read2014 (Component/src/
+  // Particle.cpp:984-1023) gives them a new kinematics object (factor 1) and
+  // the buoyant weight, and Init_Grains resets the factors
+  // (GrainsCoupledWithFluid::setFluidCorrectedAcceleration,
+  // setParticlesCouplingFactor) only when b_fluidcorrectedacc is false.  The
+  // particles here all come from the reload, so they get the same: the
+  // buoyant weight, no corrected acceleration.
+  (void)b_fluidcorrectedacc;
+  if (gdem_set_fluid(g_sys, fluid_rho, 0) != GDEM_OK) {
     fail("Init_Grains");
     return;
   }

@@ -340,7 +340,7 @@ __device__ __forceinline__ bool evalPair32(DevState const& S, GridDesc const& g,
     ct = convexContact64(convexOf(tp0, S), crustXForm(S.basis, cap, s0, tp0.scaling, x0),
                          tp0.radius, tp0.crust, convexOf(tp1, S),
                          crustXForm(S.basis, cap, s1, tp1.scaling, x1), tp1.radius, tp1.crust,
-                         c0v, c1v);
+                         c0v, c1v, true);
     if (ct.gjk_iters > 0) {
       recordVertex(S, tp0, s0, prio0, c0v);
       recordVertex(S, tp1, s1, prio1, c1v);
@@ -423,7 +423,7 @@ __device__ __forceinline__ void wallsOf32(DevState const& S, int t, int tag, int
         : convexContact64(convexOf(ta, S), crustXForm(S.basis, cap, t, ta.scaling, xt),
                           ta.radius, ta.crust, convexOf(wd),
                           identityXForm(wd.scaling, mk(wd.centre[0], wd.centre[1], wd.centre[2])),
-                          wd.radius, wd.crust, curw, cw);
+                          wd.radius, wd.crust, curw, cw, true);
     if (kConvex) gjk.add(ct.gjk_iters);
     if (kConvex && ct.gjk_iters > 0) walls_gjk = true;
     if (S.diag) S.wall_delta[(size_t)t * S.max_walls + k] = ct.contact ? ct.dist : __longlong_as_double(0x7ff0000000000000ll);

@@ -211,9 +211,14 @@ __device__ __forceinline__ Contact64 sphereWall64(d3 xa, double ra, double ca, W
 // 1e-10 is the reference's ContactError (it then retries with a 10x crust
 // shrink); here it raises the overlap status and no force is applied.
 // curA, curB: the bodies' current polyhedron vertices (updated by the GJK).
+// early: the closest-point search stops once the shrunk bodies are known to
+// be farther apart than the sum of the crusts (no contact: the same decision,
+// without the witness points and with the polyhedron vertices the shortened
+// search reached).
 __device__ inline Contact64 convexContact64(ConvexRef const& a, XForm64 const& a2w, double Ra,
                                             double ca, ConvexRef const& b, XForm64 const& b2w,
-                                            double Rb, double cb, int& curA, int& curB) {
+                                            double Rb, double cb, int& curA, int& curB,
+                                            bool early = false) {
   Contact64 c;
   c.contact = false;
   c.error = false;
@@ -222,8 +227,12 @@ __device__ inline Contact64 convexContact64(ConvexRef const& a, XForm64 const& a
   if (!(norm(gg) < Ra + Rb)) return c;
   d3 pA, pB;
   int it = 0;
-  double distance = closestPoints64(a, a2w, b, b2w, pA, pB, &it, curA, curB);
+  bool separated = false;
+  // a relative margin far above the rounding of the bound
+  const double sep = early ? (ca + cb) * (1. + 1.e-9) : 0.;
+  double distance = closestPoints64(a, a2w, b, b2w, pA, pB, &it, curA, curB, sep, &separated);
   c.gjk_iters = it;
+  if (separated) return c;
   if (distance < 1.0e-10) { c.error = true; return c; }
   d3 ba = pA - pB;
   d3 contact = pA / 2.0 + pB / 2.0;

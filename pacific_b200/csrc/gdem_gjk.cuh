@@ -213,21 +213,33 @@ __device__ inline bool closestSub(Simplex64& S, unsigned& bits, unsigned last, u
 // closest_points: distance between the two shrunk bodies and the witness
 // points in world coordinates; *iters receives the iteration count.
 // curA, curB: the bodies' current polyhedron vertices, updated.
+// sep > 0: the search stops as soon as the distance is known to exceed sep
+// -- the lower bound v.w / |v| that each support point gives (w the support
+// point of A - B in direction -v) is above it -- and returns that bound
+// with *separated set; pa, pb are then not computed.  The bound is a lower
+// bound of the distance the full search would return, so a caller that only
+// needs "distance > sep" decides the same.
 __device__ inline double closestPoints64(ConvexRef const& a, XForm64 const& a2w,
                                          ConvexRef const& b, XForm64 const& b2w, d3& pa, d3& pb,
-                                         int* iters, int& curA, int& curB) {
+                                         int* iters, int& curA, int& curB, double sep = 0.,
+                                         bool* separated = nullptr) {
   unsigned bits = 0, last = 0, last_bit = 0, all_bits = 0;
   Simplex64 S;
+  // the simplex starts zeroed; that is done just before its first use, so a
+  // search that ends at its first separation test never touches it
+  bool ready = false;
+  auto clear = [&S]() {
 #pragma unroll
-  for (int i = 0; i < 16; ++i)
+    for (int i = 0; i < 16; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) S.det[i][j] = 0.;
+      for (int j = 0; j < 4; ++j) S.det[i][j] = 0.;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    S.y[i] = S.p[i] = S.q[i] = mk(0., 0., 0.);
+    for (int i = 0; i < 4; ++i) {
+      S.y[i] = S.p[i] = S.q[i] = mk(0., 0., 0.);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) S.dp[i][j] = 0.;
-  }
+      for (int j = 0; j < 4; ++j) S.dp[i][j] = 0.;
+    }
+  };
   int numIterations = 0;
   const double relError = 1.e-10, absError = 1.e-4 * relError;
   d3 v = apply(a2w, support(a, mk(0., 0., 0.), curA)) - apply(b2w, support(b, mk(0., 0., 0.), curB));
@@ -239,9 +251,17 @@ __device__ inline double closestPoints64(ConvexRef const& a, XForm64 const& a2w,
     last_bit = 1;
     while (bits & last_bit) { ++last; last_bit <<= 1; }
     d3 d = v;
-    S.p[last] = support(a, tmul(-d, a2w), curA);
-    S.q[last] = support(b, tmul(d, b2w), curB);
-    w = apply(a2w, S.p[last]) - apply(b2w, S.q[last]);
+    const d3 pl = support(a, tmul(-d, a2w), curA);
+    const d3 ql = support(b, tmul(d, b2w), curB);
+    w = apply(a2w, pl) - apply(b2w, ql);
+    if (sep > 0. && dot(v, w) > sep * dist) {
+      *iters = numIterations;
+      *separated = true;
+      return dot(v, w) / dist;
+    }
+    if (!ready) { clear(); ready = true; }
+    S.p[last] = pl;
+    S.q[last] = ql;
     double mu = dist - dot(v, w) / dist;
     if (mu < dist * relError || mu < absError) break;
     bool degen = false;
@@ -253,6 +273,7 @@ __device__ inline double closestPoints64(ConvexRef const& a, XForm64 const& a2w,
     if (!closestSub(S, bits, last, last_bit, all_bits, v)) break;
     dist = norm(v);
   }
+  if (!ready) clear();
   // computePoints: barycentric witnesses in the local frames, then to world
   double sum = 0.;
   d3 p1 = mk(0., 0., 0.), p2 = mk(0., 0., 0.);

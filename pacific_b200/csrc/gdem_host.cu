@@ -92,6 +92,7 @@ struct InstanceDesc {
   std::string rawdata_root;  // Simulation/PostProcessing/Writers/RawData Name, if any
   bool rawdata_binary = false;
   int nmat;
+  std::vector<std::string> mat_names;   // material name of each index
   // what the pair-list grid is made from (it is remade when the skin changes)
   double box_org[3], box_max[3];
   int box_per[3];
@@ -440,6 +441,7 @@ InstanceDesc readInstance(std::string const& path) {
     }
   }
   I.nmat = (int)morder.size();
+  I.mat_names = morder;
   for (int a = 0; a < kMaxMat; ++a)
     for (int b = 0; b < kMaxMat; ++b) {
       ModelDesc m{};
@@ -576,6 +578,11 @@ struct System {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool have_state = false, started = false, diag = false, use_graphs = true;
+  // contact memory of ended contacts dropped each evaluation (the plain
+  // step) or carried (the coupled step); the tables are four times larger
+  // when it is carried, since the entries of every pair that ever touched
+  // stay
+  bool prune_memory = true;
   // the last force evaluation: 0 none since the state was set, 1 recorded by
   // the diagnostics, 2 run without them
   int evaluated = 0;
@@ -705,6 +712,16 @@ struct System {
     }
     pending.clear();
     evused = 0;
+  }
+
+  // The instances' contact-force-model tables to the device (read by the
+  // kernels when they run: captured graphs stay valid).
+  void uploadModels() {
+    std::vector<ModelDesc> models;
+    for (auto const& I : inst)
+      for (int k = 0; k < kMaxMat * kMaxMat; ++k) models.push_back(I.models[k]);
+    CK(cudaMemcpy(d_models, models.data(), models.size() * sizeof(ModelDesc),
+                  cudaMemcpyHostToDevice));
   }
 
   void setupTables() {
@@ -840,7 +857,7 @@ struct System {
       CK(cudaDeviceGetAttribute(&S.nsm, cudaDevAttrMultiProcessorCount, dev));
     }
     S.posf = alloc<float4>(c);
-    int l2 = nextPow2Log((size_t)8 * c + 64);
+    int l2 = nextPow2Log((size_t)8 * c + 64) + (prune_memory ? 0 : 2);
     size_t hc = size_t(1) << l2;
     size_t vsz = precision == GDEM_FP64 ? sizeof(double) : sizeof(float);
     for (HistTable* t : {&S.hist_old, &S.hist_new}) {
@@ -1002,6 +1019,8 @@ struct System {
     if (precision == GDEM_FP64) timed("pairlaw64", [&] { launch_pairlaw64(S, stream); });
     else timed("pairlaw32", [&] { launch_pairlaw32(S, stream); });
     timed("move", [&] { launch_move(S, flags | kStepSum, precision == GDEM_FP32_SPLIT, stream); });
+    if (!prune_memory)
+      timed("hist_carry", [&] { launch_hist_carry(S, precision == GDEM_FP64, stream); });
   }
   // One force evaluation with plain launches: decide, gated rebuild, filter,
   // forces, move.
@@ -2363,6 +2382,86 @@ int64_t gdem_num_particles(gdem_handle h) {
 double gdem_last_step_ms(gdem_handle h) {
   System* s = sys(h);
   return s ? s->last_ms : 0.;
+}
+
+int gdem_read_reload_contact_models(gdem_handle h, const char* header) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !header) throw std::runtime_error("invalid arguments");
+    if (s->inst.size() != 1) throw std::runtime_error("a reload holds one system, not a batch");
+    // the header's "<ContactForceModels> <file> </ContactForceModels>" line
+    // (ContactBuilderFactory::save); the file is looked for in the header's
+    // directory (ContactBuilderFactory::reload, Component/src/
+    // ContactBuilderFactory.cpp:199-212)
+    std::ifstream in(header);
+    if (!in) throw std::runtime_error(std::string("cannot read ") + header);
+    std::string tok, file;
+    while (in >> tok)
+      if (tok == "<ContactForceModels>") { in >> file; break; }
+    if (file.empty()) throw std::runtime_error(std::string("no contact force models named in ") + header);
+    const std::string hp(header);
+    const size_t cut = hp.find_last_of('/');
+    const std::string dir = cut == std::string::npos ? std::string(".") : hp.substr(0, cut);
+    const size_t fcut = file.find_last_of('/');
+    const std::string name = fcut == std::string::npos ? file : file.substr(fcut + 1);
+    auto root = parseXmlFile(dir + "/" + name);
+    // material values (powers of two) by name; a model's key is the OR of
+    // its two materials' values (ContactBuilderFactory::contactForceModel)
+    std::map<std::string, int> matval;
+    if (XmlNode const* mats = root->name == "Materials" ? root.get() : root->find("Materials"))
+      for (auto const& c : mats->children)
+        if (c->name == "Material") matval[c->valueS()] = (int)c->attrD("value");
+    std::map<int, ModelDesc> bykey;
+    if (XmlNode const* cms = root->find("ContactForceModels"))
+      for (auto const& c : cms->children) {
+        if (c->name != "ContactForceModel") continue;
+        const int type = (int)c->attrD("type"), key = (int)c->attrD("value");
+        // the models' constructors from a parameter map (Hooke[Memory]
+        // ContactForceModel.cpp:11-25): a parameter absent from the file is 0
+        std::map<std::string, double> P;
+        if (XmlNode const* ps = c->child("Parameters"))
+          for (auto const& q : ps->children)
+            if (q->name == "Parameter") P[q->attr("name")] = q->valueD();
+        auto get = [&P](const char* k) { auto it = P.find(k); return it == P.end() ? 0. : it->second; };
+        ModelDesc m{};
+        m.kn = get("kn"); m.en = get("en"); m.etat = get("etat"); m.muc = get("muc");
+        if (type == 1) {          // HookeMemory
+          m.kt = get("kt"); m.mur = get("mur"); m.etarpf = get("etarpf"); m.epst = get("epst");
+          m.memory = 1;
+          m.rolling = m.mur != 0. ? 1 : 0;
+        } else if (type == 0) {   // Hooke
+          m.kr = get("kr");
+          m.memory = 0;
+          m.rolling = m.kr != 0. ? 1 : 0;
+        } else {
+          throw std::runtime_error("Hertz contact models are not supported");
+        }
+        m.beta = std::log(m.en) / std::sqrt(PI * PI + std::log(m.en) * std::log(m.en));
+        m.valid = 1;
+        bykey[key] = m;
+      }
+    InstanceDesc& I = s->inst[0];
+    for (int a = 0; a < I.nmat; ++a)
+      for (int b = 0; b < I.nmat; ++b) {
+        auto ia = matval.find(I.mat_names[a]), ib = matval.find(I.mat_names[b]);
+        if (ia == matval.end() || ib == matval.end()) continue;
+        auto it = bykey.find(ia->second | ib->second);
+        if (it != bykey.end()) I.models[a * kMaxMat + b] = it->second;
+      }
+    s->uploadModels();
+    return GDEM_OK;
+  });
+}
+
+int gdem_set_contact_memory_pruning(gdem_handle h, int prune) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s) throw std::runtime_error("invalid handle");
+    if (s->have_state) throw std::runtime_error("set the contact-memory pruning before the particles");
+    s->prune_memory = prune != 0;
+    s->invalidateGraphs();
+    return GDEM_OK;
+  });
 }
 
 int gdem_use_graphs(gdem_handle h, int on) {

@@ -890,6 +890,37 @@ void launch_cells_by_id(DevState const& S, int* ijk, int id_base, cudaStream_t s
 void launch_coordination_by_id(DevState const& S, int* out, int id_base, cudaStream_t st) {
   if (S.n) k_coordination_by_id<<<blocks(S.n, 256), 256, 0, st>>>(S, out, id_base);
 }
+// Contact memory of a step that does not prune it (GrainsCoupledWithFluid::
+// Simulation, Fluid/src/GrainsCoupledWithFluid.cpp:135-205, runs the
+// collision application without Grains::computeParticlesForceAndTorque's
+// setContactMapToFalse / updateContactMap, Component/src/Component.cpp:
+// 567-593): every entry of the previous evaluation's table that this
+// evaluation did not rewrite -- a contact that has ended -- is carried into
+// this evaluation's table unchanged, so that the pair, if it touches again,
+// resumes its tangential spring.  Runs after the pair kernel.
+template <typename T>
+__global__ void k_hist_carry(HistTable old_t, HistTable new_t, const int* ctl, int* status) {
+  const unsigned tag = (unsigned)ctl[kCtlEpoch], tag_old = tag - 1u;
+  const size_t cap = size_t(1) << old_t.log2cap;
+  const T* src = static_cast<const T*>(old_t.vals);
+  T* dst = static_cast<T*>(new_t.vals);
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < cap;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const unsigned long long k = old_t.keys[i];
+    if (tagOf(k) != (tag_old & kTagMask)) continue;
+    const unsigned long long base = k & ((1ull << kTagShift) - 1ull);
+    if (histFind(new_t, base, tag) >= 0) continue;   // rewritten this evaluation
+    const int s = histInsert(new_t, base, tag);
+    if (s < 0) { raise(status, kErrHashFull); continue; }
+#pragma unroll
+    for (int j = 0; j < 9; ++j) dst[(size_t)s * 9 + j] = src[i * 9 + j];
+  }
+}
+void launch_hist_carry(DevState const& S, int fp64, cudaStream_t st) {
+  if (fp64) k_hist_carry<double><<<4 * S.nsm, 256, 0, st>>>(S.hist_old, S.hist_new, S.ctl, S.status);
+  else k_hist_carry<float><<<4 * S.nsm, 256, 0, st>>>(S.hist_old, S.hist_new, S.ctl, S.status);
+}
+
 void launch_hist_zero_cumulative(HistTable const& t, const int* ctl, int fp64, cudaStream_t st) {
   int cap = 1 << t.log2cap;
   if (fp64) k_hist_zero_cumulative<double><<<blocks(cap, 256), 256, 0, st>>>(t, ctl);

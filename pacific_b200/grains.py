@@ -110,6 +110,8 @@ def library() -> ctypes.CDLL:
         "gdem_upload_basis": ([_P, _DP], ctypes.c_int),
         "gdem_download_basis": ([_P, _DP], ctypes.c_int),
         "gdem_set_diagnostics": ([_P, ctypes.c_int], ctypes.c_int),
+        "gdem_download_history": ([_P, i64, ctypes.POINTER(i64), _IP, _IP, _DP, _DP, _DP],
+                                  ctypes.c_int),
         "gdem_download_contacts": ([_P, i64, ctypes.POINTER(i64), _IP, _IP, _DP, _DP],
                                    ctypes.c_int),
         "gdem_status": ([_P, _IP, ctypes.c_int], ctypes.c_int),
@@ -117,6 +119,7 @@ def library() -> ctypes.CDLL:
         "gdem_num_particles": ([_P], i64),
         "gdem_last_step_ms": ([_P], ctypes.c_double),
         "gdem_use_graphs": ([_P, ctypes.c_int], ctypes.c_int),
+        "gdem_set_contact_memory_pruning": ([_P, ctypes.c_int], ctypes.c_int),
         "gdem_set_state": ([_P, _DP, _DP, _DP, _DP, _DP, _DP, _DP], ctypes.c_int),
         "gdem_velocity_stats": ([_P, _DP, _DP], ctypes.c_int),
         "gdem_set_profiling": ([_P, ctypes.c_int], ctypes.c_int),
@@ -428,6 +431,22 @@ class Grains:
                                                _dp(dl), _dp(f)))
         return (id0, id1, dl, f) if forces else (id0, id1, dl)
 
+    def download_history(self):
+        """The contact memory of the last force evaluation (both views of a
+        pair): owner and partner IDs (a wall k as -(k + 2)), kdelta, previous
+        normal and spring torque (m, 3) each."""
+        lib = library()
+        cnt = ctypes.c_int64(0)
+        self._check(lib.gdem_download_history(self._h, 0, ctypes.byref(cnt), None, None, None,
+                                              None, None))
+        m = cnt.value
+        own = np.empty(m, np.int32)
+        par = np.empty(m, np.int32)
+        kd, pn, sp = np.empty((m, 3)), np.empty((m, 3)), np.empty((m, 3))
+        self._check(lib.gdem_download_history(self._h, m, ctypes.byref(cnt), _ip(own), _ip(par),
+                                              _dp(kd), _dp(pn), _dp(sp)))
+        return {"owner": own, "partner": par, "kdelta": kd, "prevn": pn, "spring": sp}
+
     def grid(self, k=0):
         nb = np.empty(3, np.int32)
         edge = np.empty(3)
@@ -442,6 +461,12 @@ class Grains:
 
     def use_graphs(self, on=True):
         self._check(library().gdem_use_graphs(self._h, 1 if on else 0))
+
+    def set_contact_memory_pruning(self, prune=True):
+        """Whether the memory of ended contacts is dropped (the plain step,
+        the default) or kept (GrainsCoupledWithFluid's step); before the
+        particles are uploaded or read."""
+        self._check(library().gdem_set_contact_memory_pruning(self._h, 1 if prune else 0))
 
     @property
     def last_step_ms(self) -> float:

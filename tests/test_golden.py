@@ -131,9 +131,14 @@ def test_gpu_fp64_step_matches_reference(tmp_path, lib, name):
         assert np.array_equal(cells, g[f"s{k1}_cells"])
         assert gc == rc or name in NO_MEMORY
         assert np.max(np.abs(s["x"] - g[f"s{k1}_x"])) <= 1e-15
+        print(f"{name} step {k1}: quaternions differ in {int((s['q'] != g[f's{k1}_q']).any(axis=1).sum())}"
+              f" particles (max {np.max(np.abs(s['q'] - g[f's{k1}_q'])):.1e})")
         if name in CONVEX:
             # orientation matrices are state for non-spherical classes only
-            assert np.max(np.abs(s["basis"] - g[f"s{k1}_basis"])) <= 1e-14
+            db = np.abs(s["basis"] - g[f"s{k1}_basis"])
+            print(f"{name} step {k1}: orientation matrices differ in {int((db > 0).any(axis=1).sum())}"
+                  f" particles (max {db.max():.1e})")
+            assert db.max() <= 1e-14
         if name in CONVEX:
             # A face-to-face contact has no unique pair of closest points: the
             # reference's witness points depend on where its polyhedron
@@ -145,6 +150,17 @@ def test_gpu_fp64_step_matches_reference(tmp_path, lib, name):
                 print(f"{name} step {k1}: {fe.size} particles in contact, "
                       f"{int((fe > 1e-10).sum())} above 1e-10 (force), "
                       f"{int((te > 1e-10).sum())} (torque); max {fe.max():.2e} / {te.max():.2e}")
+                # the particles above 1e-10: class, partners (class) and walls
+                c = g[f"s{k1}_scale"] > 0
+                rows = np.flatnonzero(c)
+                own, par = g[f"s{k1}_hist_owner"], g[f"s{k1}_hist_partner"]
+                for j in np.flatnonzero((fe > 1e-10) | (te > 1e-10)):
+                    i = int(rows[j])
+                    partners = sorted({int(b) if a == i else int(a)
+                                       for a, b in zip(own.tolist(), par.tolist()) if i in (a, b)})
+                    print(f"   particle {i} class {int(g['type'][i])}: partners "
+                          f"{[(q, int(g['type'][q])) if q >= 0 else ('wall', q) for q in partners]}, "
+                          f"force err {fe[j]:.2e}, torque err {te[j]:.2e}")
                 assert np.median(fe) <= 1e-9 and fe.max() <= 1e-5
                 assert np.median(te) <= 1e-9 and te.max() <= 1e-4
         else:
