@@ -200,11 +200,13 @@ def max_over_ranks(dist, value):
     return float(t.item())
 
 
-def make_system(xml, sc, precision, graphs=True):
+def make_system(xml, sc, precision, graphs=True, skin_factor=None):
     from pacific_b200 import Grains
     g = Grains(xml, precision)
     g.use_graphs(graphs)
     g.upload_state(sc.type, sc.x, sc.v, sc.w, sc.q)
+    if skin_factor is not None:
+        g.set_tuning(skin_factor=skin_factor)
     g.do_before_time_stepping()
     return g
 
@@ -472,7 +474,8 @@ def adjoint_measure(n, steps, every):
     velocities after `steps` steps against the trajectory at kn = 2e4,
     en = 0.6, muc = 0.35, gradients at parameters perturbed by 5 %, with
     checkpoints every `every` steps; checked against dual-number forward
-    mode.  Wall-clock time of each call (device work dominates)."""
+    mode and against central differences of the loss (relative steps 1e-5
+    and 1e-6).  Wall-clock time of each call (device work dominates)."""
     from pacific_b200 import scenarios
     from pacific_b200.adjoint import Adjoint
     p_t = np.array([2.0e4, 0.6, 0.35])
@@ -491,11 +494,40 @@ def adjoint_measure(n, steps, every):
         t0 = time.perf_counter()
         loss_f, gp_f = a.forward_mode(p_s, tx, tv, steps)
         t_dual = time.perf_counter() - t0
+        # central differences of the loss, two step sizes (relative to each
+        # parameter), over the full horizon and over a short one.  Over the
+        # full horizon thousands of contacts open and close between p - h
+        # and p + h, so the loss is rough at these scales and the quotients
+        # disagree with each other as much as with the adjoint; over the
+        # short horizon the contact set holds and they converge to it.
+        def differences(p, n_steps, x_t, v_t, g_adj):
+            out = {}
+            for h_rel in (1e-5, 1e-6):
+                g_fd = np.zeros(3)
+                for j in range(3):
+                    dp = np.zeros(3)
+                    dp[j] = h_rel * p[j]
+                    lp = a.run(p + dp, n_steps, x_t, v_t)[2]
+                    lm = a.run(p - dp, n_steps, x_t, v_t)[2]
+                    g_fd[j] = (lp - lm) / (2 * dp[j])
+                out[f"{h_rel:g}"] = {
+                    "dL_dparams": g_fd.tolist(),
+                    "rel_diff_vs_adjoint": (np.abs(g_adj - g_fd) /
+                                            np.maximum(np.abs(g_adj), 1e-300)).tolist()}
+            return out
+
+        short = max(1, min(steps, 20))
+        sx, sv, _ = a.run(p_t, short)
+        _, gp_short, _ = a.gradients(p_s, sx, sv, short, every)
+        fd = {f"{steps}_steps": differences(p_s, steps, tx, tv, gp),
+              f"{short}_steps": {"dL_dparams_adjoint": gp_short.tolist(),
+                                 **differences(p_s, short, sx, sv, gp_short)}}
         a.close()
     rel = np.abs(gp - gp_f) / np.abs(gp_f)
     return {"workload": f"adjoint_box n={n}, {steps} steps, checkpoint every {every}",
             "loss": loss, "dL_dparams": gp.tolist(), "dL_dparams_forward_mode": gp_f.tolist(),
             "max_rel_diff_vs_forward_mode": float(rel.max()),
+            "central_differences": fd,
             "dL_dv0_norm": float(np.linalg.norm(gv)),
             "forward_s": t_fwd, "gradient_s": t_adj, "forward_mode_s": t_dual}
 
@@ -566,6 +598,11 @@ def main():
     ap.add_argument("--convex-steps", type=int, default=500)
     ap.add_argument("--only-fp32-split", action="store_true",
                     help="skip the FP64 leg (profiling the FP32-split step alone)")
+    ap.add_argument("--skin-factor", type=float, default=None,
+                    help="pair-list skin as a multiple of the largest circumscribed radius "
+                         "(default: the library's)")
+    ap.add_argument("--only-convex", action="store_true",
+                    help="run the convex-pour leg alone and print its result (profiling)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -582,6 +619,11 @@ def main():
         build.build()
     if dist is not None:
         dist.barrier()
+    if args.only_convex:
+        out = convex_measure(args.convex_n, args.convex_steps, graphs=not args.no_graphs)
+        if rank == 0:
+            print(json.dumps({"convex": out}), flush=True)
+        return
     sc = scenarios.periodic_gas(n_fcc=args.n_fcc, seed=1236 + 1000 * rank)
     tmp = tempfile.TemporaryDirectory()
     xml = str(sc.write_xml(Path(tmp.name) / f"gas{rank}.xml"))
@@ -591,7 +633,7 @@ def main():
     legs = (("fp32_split", FP32_SPLIT),) if args.only_fp32_split else \
         (("fp64", FP64), ("fp32_split", FP32_SPLIT))
     for name, prec in legs:
-        g = make_system(xml, sc, prec, graphs=not args.no_graphs)
+        g = make_system(xml, sc, prec, graphs=not args.no_graphs, skin_factor=args.skin_factor)
         if args.advance > 0:
             g.step(args.advance)
         g.step(args.warmup)
@@ -624,7 +666,7 @@ def main():
     if not args.no_full_config:
         full = {}
         for name, prec in (("fp32_split", FP32_SPLIT), ("fp64", FP64)):
-            gf = make_system(xml, sc, prec, graphs=not args.no_graphs)
+            gf = make_system(xml, sc, prec, graphs=not args.no_graphs, skin_factor=args.skin_factor)
             ms = timed_steps(gf, dist, 2000)
             _, rb = gf.step_counts()
             full[name] = {"value": world * n * 2000 / (ms * 1e-3), "ms_per_step": ms / 2000,

@@ -213,6 +213,21 @@ int gdem_reload_filename(gdem_handle h, char* buf, int capacity);
  * 2 polyhedron, 3 cylinder. */
 int gdem_particle_class(gdem_handle h, int cls, double* props, int* shape);
 
+/* The envelope of class cls (of the first instance) as GrainsCoupledWithFluid::
+ * GrainsToFluid writes it (Fluid/src/GrainsCoupledWithFluid.cpp:912-1120,
+ * RigidBody::writePositionInFluid, Geometry/src/RigidBody.cpp:445-500):
+ * *code = Convex::getNbCorners (1 sphere, 666 box, 777 cylinder, a
+ * polyhedron's vertex count); *npoints body-frame points of the shape without
+ * its crust shrink (Convex::getEnvelope: the sphere's centre, the box's eight
+ * corners in Box::setCornersFaces's order, the cylinder's bottom centre,
+ * bottom rim point and top centre, the polyhedron's vertices in file order),
+ * 3 doubles each in points; the faces (Convex::getFaces; none for a sphere or
+ * a cylinder): *nfaces runs of (vertex count, vertex indices) in faces,
+ * *nwords ints in all.  points / faces are filled when their capacities
+ * (points, ints) suffice; the sizes are always returned. */
+int gdem_class_envelope(gdem_handle h, int cls, int* code, int point_capacity, int* npoints,
+                        double* points, int word_capacity, int* nwords, int* nfaces, int* faces);
+
 /* Velocities and space-frame angular velocities from the fluid solver, by
  * particle ID, 3 each (GrainsCoupledWithFluid::updateParticlesVelocity,
  * :1126-1180; the body-frame angular velocity follows as q* w q). */

@@ -30,9 +30,9 @@
 //                     [mindt, maxdt].
 //   GrainsToBasilisk  the rigid-body stream of GrainsCoupledWithFluid::
 //                     GrainsToFluid (:912-1120), tokens separated by one
-//                     space (InterfaceGrains3DBasilisk.cpp:62-82); spheres
-//                     (a class that is not a sphere is reported as an error:
-//                     its envelope and faces are not written).
+//                     space (InterfaceGrains3DBasilisk.cpp:62-82), for every
+//                     class: corner code, envelope points through the
+//                     particle's transform, faces (gdem_class_envelope).
 //   UpdateVelocityGrains  velocities from the fluid (updateParticlesVelocity).
 //   SaveResults_Grains  the XML's RawData writer, if any (started at the first
 //                     call, an output time at each later one; the last
@@ -276,11 +276,37 @@ char* GrainsToBasilisk(int* pstrsize) {
   char buf[64];
   const int64_t n = g_sys && !g_error ? g_n : 0;
   std::vector<double> x(3 * n), v(3 * n), w(3 * n), q(4 * n), B(9 * n);
-  if (n) {
+  // the classes' envelopes (Convex::getNbCorners / getEnvelope / getFaces)
+  struct Env { int code = 0; std::vector<double> pts; std::vector<int> faces; int nfaces = 0; };
+  std::vector<Env> env;
+  bool all_spheres = true;
+  for (int c = 0; n && !g_error; ++c) {
+    Env e;
+    int np = 0, nw = 0;
+    if (gdem_class_envelope(g_sys, c, &e.code, 0, &np, nullptr, 0, &nw, &e.nfaces, nullptr) != GDEM_OK)
+      break;   // past the last class
+    e.pts.resize(3 * (size_t)np);
+    e.faces.resize((size_t)nw);
+    if (gdem_class_envelope(g_sys, c, &e.code, np, &np, e.pts.data(), nw, &nw, &e.nfaces,
+                            e.faces.data()) != GDEM_OK) {
+      fail("GrainsToBasilisk");
+      break;
+    }
+    if (e.code != 1) all_spheres = false;
+    env.push_back(std::move(e));
+  }
+  if (n && !g_error) {
     if (gdem_download_state(g_sys, x.data(), v.data(), w.data(), nullptr, q.data(), nullptr,
                             nullptr) != GDEM_OK)
       fail("GrainsToBasilisk");
-    for (int64_t i = 0; i < n; ++i) rotationOf(&q[4 * i], &B[9 * i]);
+    // the transform's basis: integrated with the rotation (the reference's
+    // composeLeftByRotation) where the system keeps orientation matrices,
+    // else the matrix of the quaternion
+    if (!all_spheres) {
+      if (gdem_download_basis(g_sys, B.data()) != GDEM_OK) fail("GrainsToBasilisk");
+    } else {
+      for (int64_t i = 0; i < n; ++i) rotationOf(&q[4 * i], &B[9 * i]);
+    }
   }
   std::snprintf(buf, sizeof(buf), "%lld", (long long)n);
   tok(buf);
@@ -288,11 +314,8 @@ char* GrainsToBasilisk(int* pstrsize) {
     double props[7];
     int shape = 0;
     if (gdem_particle_class(g_sys, g_class[i], props, &shape) != GDEM_OK) { fail("GrainsToBasilisk"); break; }
-    if (shape != 0) {
-      std::fprintf(stderr, "Grains3D B200 coupling: GrainsToBasilisk: only spheres are written\n");
-      g_error = true;
-      break;
-    }
+    if (g_class[i] < 0 || g_class[i] >= (int)env.size()) { fail("GrainsToBasilisk"); break; }
+    Env const& e = env[g_class[i]];
     const double* mr = &B[9 * i];
     // Particle::computeInertiaTensorSpaceFixed (Particle.cpp:1797-1821):
     // Mr (I_body Mr^t), I_body diagonal in the body frame
@@ -306,7 +329,8 @@ char* GrainsToBasilisk(int* pstrsize) {
     // v, w, density, mass, space-fixed inertia, orientation, centre
     std::snprintf(buf, sizeof(buf), "%d", g_ids[i] - 1);
     tok(buf);
-    tok("1");
+    std::snprintf(buf, sizeof(buf), "%d", e.code);
+    tok(buf);
     tok("P");
     for (int d = 0; d < 3; ++d) tok(d16(v[3 * i + d]));
     for (int d = 0; d < 3; ++d) tok(d16(w[3 * i + d]));
@@ -316,13 +340,25 @@ char* GrainsToBasilisk(int* pstrsize) {
     for (int k = 0; k < 9; ++k) tok(d16(mr[k]));
     for (int d = 0; d < 3; ++d) tok(d16(x[3 * i + d]));
     // radius in the stream's default format (%g), then RigidBody::
-    // writePositionInFluid (RigidBody.cpp:445-500): one envelope point (the
-    // centre) and no face
+    // writePositionInFluid (RigidBody.cpp:445-500): the envelope points
+    // through the particle's transform (Transform::operator(), Transform.cpp:
+    // 309-314: basis row . p + origin), then the faces (count, indices) or 0
     std::snprintf(buf, sizeof(buf), "%g", props[5]);
     tok(buf);
-    tok("1");
-    for (int d = 0; d < 3; ++d) tok(d16(x[3 * i + d]));
-    tok("0");
+    const int np = (int)e.pts.size() / 3;
+    std::snprintf(buf, sizeof(buf), "%d", np);
+    tok(buf);
+    for (int k = 0; k < np; ++k) {
+      const double* pt = &e.pts[3 * (size_t)k];
+      for (int d = 0; d < 3; ++d)
+        tok(d16(mr[3 * d] * pt[0] + mr[3 * d + 1] * pt[1] + mr[3 * d + 2] * pt[2] + x[3 * i + d]));
+    }
+    std::snprintf(buf, sizeof(buf), "%d", e.nfaces);
+    tok(buf);
+    for (int w = 0; w < (int)e.faces.size(); ++w) {
+      std::snprintf(buf, sizeof(buf), "%d", e.faces[w]);
+      tok(buf);
+    }
   }
   *pstrsize = (int)out.size() + 1;
   char* res = new char[*pstrsize];

@@ -417,6 +417,24 @@ __device__ __forceinline__ void wallsOf32(DevState const& S, int t, int tag, int
   bool walls_gjk = false;
   for (int k = 0; k < g.wall_count; ++k) {
     WallDesc const& wd = S.walls[g.wall_begin + k];
+    if (kConvex && ta.shape != 0) {
+      // the shrunk body lies inside its circumscribed sphere and the shrunk
+      // wall inside the wall's box: when the sphere is farther from the box
+      // than the two crusts (with a margin far above the rounding), the
+      // closest-point search would decide "no contact"; skip it
+      double d2 = 0.;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const double c = d == 0 ? xt.x : (d == 1 ? xt.y : xt.z);
+        const double e = fabs(c - wd.centre[d]) - wd.extent[d];
+        if (e > 0.) d2 += e * e;
+      }
+      const double lim = (ta.radius + ta.crust + wd.crust) * (1. + 1.e-9);
+      if (d2 > lim * lim) {
+        if (S.diag) S.wall_delta[(size_t)t * S.max_walls + k] = __longlong_as_double(0x7ff0000000000000ll);
+        continue;
+      }
+    }
     int cw = 0;
     Contact64 ct = (!kConvex || ta.shape == 0)
         ? sphereWall64(xt, ta.radius, ta.crust, wd)

@@ -79,6 +79,8 @@ struct InstanceDesc {
   // each polyhedron vertex's neighbours (Polyhedron::m_cobound), aligned with
   // poly_verts: indices within the vertex's polyhedron
   std::vector<std::vector<int>> poly_cob;
+  // per class, a polyhedron's faces as its file lists them (empty otherwise)
+  std::vector<std::vector<std::vector<int>>> class_faces;
   ModelDesc models[kMaxMat * kMaxMat];
   double gravity[3];
   double dt;
@@ -292,6 +294,7 @@ InstanceDesc readInstance(std::string const& path) {
          return v;
        }()) {
     TypeDesc t{};
+    std::vector<std::vector<int>> class_faces_of_this;
     double density = pn->attrD("Density");
     XmlNode const* cv = pn->child("Convex");
     if (!cv) throw std::runtime_error("<Particle> without <Convex>");
@@ -331,6 +334,7 @@ InstanceDesc readInstance(std::string const& path) {
     } else if (XmlNode const* ph = cv->child("Polyhedron")) {
       t.shape = 2;
       PolyFile P = readPolyFile(ph->attr("Name"));
+      class_faces_of_this = P.faces;
       polyMassProperties(P, vol, Iv);
       double ray = 0.;
       for (auto const& v : P.verts) ray = std::max(ray, v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
@@ -380,6 +384,7 @@ InstanceDesc readInstance(std::string const& path) {
     t.r_f = (float)t.radius;
     maxR = std::max(maxR, t.radius);
     I.types.push_back(t);
+    I.class_faces.push_back(class_faces_of_this);
   }
   if (I.types.empty()) throw std::runtime_error("no <Particle> class");
   // obstacles: boxes with identity orientation
@@ -2382,6 +2387,61 @@ int64_t gdem_num_particles(gdem_handle h) {
 double gdem_last_step_ms(gdem_handle h) {
   System* s = sys(h);
   return s ? s->last_ms : 0.;
+}
+
+int gdem_class_envelope(gdem_handle h, int cls, int* code, int point_capacity, int* npoints,
+                        double* points, int word_capacity, int* nwords, int* nfaces, int* faces) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !code || !npoints || !nwords || !nfaces) throw std::runtime_error("invalid arguments");
+    InstanceDesc const& I = s->inst[0];
+    if (cls < 0 || cls >= (int)I.types.size()) throw std::runtime_error("class out of range");
+    TypeDesc const& t = I.types[cls];
+    std::vector<double> P;
+    std::vector<int> W;
+    int nf = 0;
+    const double ex = t.extent[0], ey = t.extent[1], ez = t.extent[2];
+    if (t.shape == 0) {
+      // Sphere::getEnvelope (Geometry/src/Sphere.cpp:116-123): the centre
+      *code = 1;
+      P = {0., 0., 0.};
+    } else if (t.shape == 1) {
+      // Box::getNbCorners 666; Box::setCornersFaces (Geometry/src/Box.cpp:
+      // 91-147): the eight corners and the six faces in its order
+      *code = 666;
+      P = {-ex, -ey, -ez, ex, -ey, -ez, ex, -ey, ez, -ex, -ey, ez,
+           -ex, ey, -ez, ex, ey, -ez, ex, ey, ez, -ex, ey, ez};
+      const int F[6][4] = {{4, 5, 6, 7}, {5, 1, 2, 6}, {1, 0, 3, 2},
+                           {0, 4, 7, 3}, {4, 0, 1, 5}, {3, 7, 6, 2}};
+      for (auto const& f : F) {
+        W.push_back(4);
+        W.insert(W.end(), f, f + 4);
+      }
+      nf = 6;
+    } else if (t.shape == 3) {
+      // Cylinder::getNbCorners 777; getEnvelope (Geometry/src/Cylinder.cpp:
+      // 142-151): the bottom centre, a bottom rim point, the top centre
+      *code = 777;
+      P = {0., -ey, 0., ex, -ey, 0., 0., ey, 0.};
+    } else {
+      // Polytope::getNbCorners / getEnvelope (Geometry/src/Polytope.cpp:
+      // 76-95): the vertices in file order; the faces as the file lists them
+      *code = t.poly_count;
+      P.assign(I.poly_verts.begin() + 3 * (size_t)t.poly_begin,
+               I.poly_verts.begin() + 3 * (size_t)(t.poly_begin + t.poly_count));
+      for (auto const& f : I.class_faces[cls]) {
+        W.push_back((int)f.size());
+        W.insert(W.end(), f.begin(), f.end());
+      }
+      nf = (int)I.class_faces[cls].size();
+    }
+    *npoints = (int)P.size() / 3;
+    *nwords = (int)W.size();
+    *nfaces = nf;
+    if (points && point_capacity >= *npoints) std::copy(P.begin(), P.end(), points);
+    if (faces && word_capacity >= *nwords) std::copy(W.begin(), W.end(), faces);
+    return GDEM_OK;
+  });
 }
 
 int gdem_read_reload_contact_models(gdem_handle h, const char* header) {

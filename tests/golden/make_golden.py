@@ -121,8 +121,20 @@ def run(name):
                 # each particle's polyhedron support vertex (Polyhedron::
                 # m_curr_vertex): hidden state of the reference, taken from the
                 # restatement, which reproduces the reference bit for bit
-                assert np.array_equal(o.state()["x"], out[f"s{m}_x"])
-                out[f"s{m}_curv"] = o.support_vertices()
+                # (the periodic gas's restatement agrees to round-off only,
+                # minimum image against clones: it records neither)
+                st = o.state()
+                if name != "periodic_gas":
+                    assert np.array_equal(st["x"], out[f"s{m}_x"])
+                    out[f"s{m}_curv"] = o.support_vertices()
+                    # the body-frame angular velocity, which the reference
+                    # integrates (ParticleKinematics::m_angularVelocity_bf, no
+                    # accessor): taken from the restatement too, whose
+                    # space-frame angular velocity and quaternion equal the
+                    # reference's to the bit
+                    assert np.array_equal(st["w"], out[f"s{m}_w"])
+                    assert np.array_equal(st["q"], out[f"s{m}_q"])
+                    out[f"s{m}_wbf"] = st["wbf"]
         np.savez_compressed(HERE / f"{name}.npz", **out)
         print(f"wrote {name}.npz ({len(sc.type)} particles, steps {marks})")
 

@@ -236,27 +236,22 @@ REF_EXE = Path(__file__).resolve().parent.parent / "oracle" / "_ref" / "grains_b
 REF_BASILISK = Path(__file__).resolve().parent.parent / "oracle" / "_ref" / "libgrains_ref_basilisk.so"
 
 
-@pytest.mark.skipif(not (REF_EXE.exists() and REF_BASILISK.exists()),
-                    reason="the reference's executable and Basilisk library were not built")
-def test_basilisk_matches_reference_interface(tmp_path, lib):
-    """The coupling library against the reference's own Basilisk interface
-    (InterfaceGrains3DBasilisk.cpp over the reference's objects) on the same
-    reload: 200 spheres settled for 300 steps by the reference's serial step
-    (Type="Standard", insertion at the initial time, reload written at the
-    end), then Init_Grains (fluid density 1000, corrected acceleration),
-    Simu_Grains over a fluid step of 4e-5 s (4 sub-steps), GrainsToBasilisk,
-    UpdateVelocityGrains, a second fluid step, GrainsToBasilisk.  Both
-    streams agree token for token in their words and counts and to FP64
-    round-off in their numbers; the rigid-body counts are the same."""
+def _reference_parity(tmp_path, sc, settle_steps, dt, rows, dt_fluid):
+    """Settles sc with the reference's serial step (Type="Standard",
+    insertion at the initial time from its positions, reload written at the
+    end), then drives the reference's Basilisk interface and this library's
+    through the same calls on that reload: Init_Grains (fluid density 1000,
+    corrected acceleration), Simu_Grains(dt_fluid) (4 sub-steps),
+    GrainsToBasilisk, UpdateVelocityGrains(rows), Simu_Grains, GrainsToBasilisk.
+    Returns both runs' results."""
     import os
     import re
     import subprocess
 
     from oracle import ref_basilisk_run
 
-    sc = scenarios.settling_box(n=200, seed=31)
     np.savetxt(tmp_path / "positions.txt", sc.x, fmt="%.17g")
-    end = 300 * 1e-5
+    end = settle_steps * dt
     text = re.sub(r"<TimeInterval[^>]*/>", f'<TimeInterval Start="0." End="{end!r}"/>', sc.xml())
     sim = (f'    <RestartFile Name="{tmp_path}/res" WritingMode="Text"/>\n'
            f'    <TimeSave Start="0." End="{end!r}" Every="{end!r}"/>\n'
@@ -269,14 +264,14 @@ def test_basilisk_matches_reference_interface(tmp_path, lib):
            "      </InitialVelocity>\n    </ParticleInsertion>\n")
     (tmp_path / "settle.xml").write_text(text.replace("  </Simulation>", sim + "  </Simulation>"))
     r = subprocess.run([str(REF_EXE), "settle.xml"], cwd=str(tmp_path), capture_output=True,
-                       text=True, timeout=600, env=dict(os.environ, GRAINS_HOME=str(tmp_path)))
+                       text=True, timeout=900, env=dict(os.environ, GRAINS_HOME=str(tmp_path)))
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     reload = (tmp_path / "res_RFTable.txt").read_text().split()[-1]
     # the reference's coupled application is built for Type="CoupledFluid"
     # (GrainsBuilderFactory::createCoupledWithFluid)
     coupled = sc.xml().replace('<Grains3D Type="Standard">', '<Grains3D Type="CoupledFluid">')
-    coupled = coupled.replace('<TimeStep dt="1e-05"/>',
-                              '<TimeStep mindt="1e-05" maxdt="2e-05" ndt="4"/>')
+    coupled = re.sub(r'<TimeStep dt="[^"]*"/>',
+                     f'<TimeStep mindt="{dt!r}" maxdt="{2 * dt!r}" ndt="4"/>', coupled)
     coupled = coupled.replace(
         "  </Construction>",
         f'    <Reload Type="new" Filename="{reload}" Velocity="Keep"/>\n  </Construction>')
@@ -285,15 +280,18 @@ def test_basilisk_matches_reference_interface(tmp_path, lib):
         f'    <RestartFile Name="{tmp_path}/cres" WritingMode="Text"/>\n  </Simulation>')
     xml = tmp_path / "coupled.xml"
     xml.write_text(coupled)
-    rows = np.zeros((sc.n, 6))
-    rows[:, 2] = -0.05
-    rows[:, 3] = np.linspace(-1.0, 1.0, sc.n)
-    ref = ref_basilisk_run.run(REF_BASILISK, xml, 1000.0, 4e-5, rows)
-    ours = ref_basilisk_run.run(BASILISK, xml, 1000.0, 4e-5, rows)
-    assert (ours["particles"], ours["obstacles"]) == (ref["particles"], ref["obstacles"]) == (sc.n, 0)
+    ref = ref_basilisk_run.run(REF_BASILISK, xml, 1000.0, dt_fluid, rows)
+    ours = ref_basilisk_run.run(BASILISK, xml, 1000.0, dt_fluid, rows)
+    return ref, ours
+
+
+def _compare_streams(ref, ours, n, record=None):
+    assert (ours["particles"], ours["obstacles"]) == (ref["particles"], ref["obstacles"]) == (n, 0)
     for k, (sa, sb) in enumerate(zip(ref["streams"], ours["streams"])):
         ta, tb = sa.split(), sb.split()
-        assert len(ta) == len(tb) == 1 + 35 * sc.n
+        assert len(ta) == len(tb) and int(ta[0]) == n
+        if record:
+            assert len(ta) == 1 + record * n
         where, num_a, num_b = [], [], []
         for i, (a, b) in enumerate(zip(ta, tb)):
             try:
@@ -303,14 +301,50 @@ def test_basilisk_matches_reference_interface(tmp_path, lib):
             except ValueError:
                 assert a == b
         fa, fb = np.array(num_a), np.array(num_b)
-        # integers (counts, IDs) and exact constants compare equal; the rest
-        # to FP64 round-off of a contact-laden settled state
+        # integers (counts, IDs, corner codes, face indices) and exact
+        # constants compare equal; the rest to FP64 round-off
         err = np.abs(fa - fb) / np.maximum(np.abs(fa), 1e-6)
         worst = np.argsort(err)[::-1][:8]
         print(f"stream {k}: max relative token difference {err.max():.3g}; "
-              f"{int((err > 1e-9).sum())} tokens above 1e-9; worst (particle, field, ref, ours):",
-              [((where[j] - 1) // 35, (where[j] - 1) % 35, ta[where[j]], tb[where[j]]) for j in worst])
+              f"{int((err > 1e-9).sum())} tokens above 1e-9; worst (token, ref, ours):",
+              [(where[j], ta[where[j]], tb[where[j]]) for j in worst])
         assert err.max() <= 1e-9
+
+
+@pytest.mark.skipif(not (REF_EXE.exists() and REF_BASILISK.exists()),
+                    reason="the reference's executable and Basilisk library were not built")
+def test_basilisk_matches_reference_interface(tmp_path, lib):
+    """The coupling library against the reference's own Basilisk interface
+    (InterfaceGrains3DBasilisk.cpp over the reference's objects) on the same
+    reload: 200 spheres settled for 300 steps by the reference's serial
+    step, then two fluid steps of 4 sub-steps around an UpdateVelocityGrains.
+    Both streams agree token for token in their words and counts and to FP64
+    round-off in their numbers; the rigid-body counts are the same."""
+    sc = scenarios.settling_box(n=200, seed=31)
+    rows = np.zeros((sc.n, 6))
+    rows[:, 2] = -0.05
+    rows[:, 3] = np.linspace(-1.0, 1.0, sc.n)
+    ref, ours = _reference_parity(tmp_path, sc, 300, 1e-5, rows, 4e-5)
+    _compare_streams(ref, ours, sc.n, record=35)
+
+
+@pytest.mark.skipif(not (REF_EXE.exists() and REF_BASILISK.exists()),
+                    reason="the reference's executable and Basilisk library were not built")
+def test_basilisk_convex_matches_reference_interface(tmp_path, lib):
+    """The same comparison for cubes, tetrahedra and cylinders: each record
+    carries the class's corner code (666 box, the vertex count of a
+    polyhedron, 777 cylinder), the envelope points through the particle's
+    transform and the faces (RigidBody::writePositionInFluid)."""
+    poly = scenarios.write_tetrahedron(tmp_path / "tet.poly")
+    sc = scenarios.convex_pour(n=120, seed=1239, poly_path=poly, box=(0.02, 0.02, 0.06),
+                               vmax=0.5, cylinders=True)
+    rows = np.zeros((sc.n, 6))
+    rows[:, 1] = 0.02
+    rows[:, 5] = np.linspace(-2.0, 2.0, sc.n)
+    ref, ours = _reference_parity(tmp_path, sc, 1000, 2e-6, rows, 8e-6)
+    _compare_streams(ref, ours, sc.n)
+    # every class's record is there: box and cylinder corner codes
+    assert {"666", "777"} <= set(ours["streams"][0].split())
 
 
 def _glancing_pair(tmp_path):
