@@ -23,6 +23,13 @@
 // Dual<3> numbers seeded on (kn, en, muc) gives the forward-mode gradient
 // that checks the parameter part of the adjoint.
 //
+// Pair search: a linked-cell grid over the domain box (cells at least the
+// largest contact distance wide, coordinates outside the box clamped into the
+// edge cells) is rebuilt at every force evaluation; each particle collects
+// the partners of its 27 cells whose centres pass the contact-distance test
+// and takes them in ascending index, the order of an all-pairs loop, so the
+// sums and lists do not depend on the grid.
+//
 // Scope: spheres (any number of classes), box walls, Hooke / HookeMemory
 // without rolling resistance, non-periodic domains.  kt and the other law
 // parameters come from the XML; kn, en and muc of every contact model are
@@ -169,15 +176,91 @@ struct ListsT {
   T* wpn;
 };
 
+// ---------------------------------------------------------- pair search --
+// The linked-cell grid of the forward model: cell (i, j, k) has key
+// (k nb1 + j) nb0 + i; start[c] .. start[c + 1] index its particles in items.
+struct AdjGrid {
+  double org[3], inv_edge[3];
+  int nb[3];
+  int ncells;
+  const int* cell;    // cell key of each particle
+  const int* start;   // ncells + 1 offsets
+  const int* items;   // particles in cell order
+};
+
+__device__ __forceinline__ int adjCellIndex(AdjGrid const& g, int d, double x) {
+  const double f = floor((x - g.org[d]) * g.inv_edge[d]);
+  return f < 0. ? 0 : (f >= (double)g.nb[d] ? g.nb[d] - 1 : (int)f);
+}
+
+template <typename T>
+__global__ void k_adj_bin(int n, AdjGrid g, const T* x, int* cell, int* count) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int i = adjCellIndex(g, 0, val(x[3 * t]));
+  const int j = adjCellIndex(g, 1, val(x[3 * t + 1]));
+  const int k = adjCellIndex(g, 2, val(x[3 * t + 2]));
+  const int c = (k * g.nb[1] + j) * g.nb[0] + i;
+  cell[t] = c;
+  atomicAdd(&count[c], 1);
+}
+
+// Exclusive scan of the cell counts by one block of 1024 threads, chunk by
+// chunk; start[ncells] receives the total.
+__global__ void __launch_bounds__(1024) k_adj_scan(int ncells, const int* count, int* start) {
+  __shared__ int warp_sum[32];
+  __shared__ int carry_s;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry_s = 0;
+  __syncthreads();
+  for (int base = 0; base < ncells; base += 1024) {
+    const int i = base + threadIdx.x;
+    const int v = i < ncells ? count[i] : 0;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sum[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      int y = warp_sum[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int z = __shfl_up_sync(0xffffffffu, y, o);
+        if (lane >= o) y += z;
+      }
+      warp_sum[lane] = y;
+    }
+    __syncthreads();
+    const int carry = carry_s;
+    const int before = wid > 0 ? warp_sum[wid - 1] : 0;
+    if (i < ncells) start[i] = carry + before + x - v;
+    __syncthreads();
+    if (threadIdx.x == 0) carry_s = carry + warp_sum[31];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) start[ncells] = carry_s;
+}
+
+__global__ void k_adj_place(int n, const int* cell, const int* start, int* fill, int* items) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int c = cell[t];
+  items[start[c] + atomicAdd(&fill[c], 1)] = t;
+}
+
 // ------------------------------------------------------------- forward --
 // Contact forces and the new contact lists at one step.  vel/omg are the
 // velocities the law sees (half-step ones, or the initial ones at the
 // leapfrog start).  zero_spring: the leapfrog start zeroes the cumulative
 // spring after the evaluation.
 template <typename T>
-__global__ void k_fwd_forces(int n, AdjTables A, const int* type, const T* x, const T* vel,
-                             const T* omg, ListsT<T> prev, int has_prev, ListsT<T> cur, T* F,
-                             T* Tq, T kn, T en, T muc, int zero_spring, int* overflow) {
+__global__ void k_fwd_forces(int n, AdjTables A, AdjGrid G, const int* type, const T* x,
+                             const T* vel, const T* omg, ListsT<T> prev, int has_prev,
+                             ListsT<T> cur, T* F, T* Tq, T kn, T en, T muc, int zero_spring,
+                             int* overflow) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   TypeDesc const& tp = A.types[type[t]];
@@ -185,14 +268,43 @@ __global__ void k_fwd_forces(int n, AdjTables A, const int* type, const T* x, co
   V3<T> Ft = vconst<T>(tp.weight[0], tp.weight[1], tp.weight[2]);
   V3<T> Tt = vconst<T>(0., 0., 0.);
   const V3<T> zero = vconst<T>(0., 0., 0.);
+  // partners whose centres pass the contact-distance test, from the 27
+  // cells around t's, in ascending index
+  int cand[kAdjCap];
+  int nc = 0;
+  {
+    const int c = G.cell[t];
+    const int ci = c % G.nb[0], cj = (c / G.nb[0]) % G.nb[1], ck = c / (G.nb[0] * G.nb[1]);
+    for (int k3 = max(ck - 1, 0); k3 <= min(ck + 1, G.nb[2] - 1); ++k3)
+      for (int j3 = max(cj - 1, 0); j3 <= min(cj + 1, G.nb[1] - 1); ++j3)
+        for (int i3 = max(ci - 1, 0); i3 <= min(ci + 1, G.nb[0] - 1); ++i3) {
+          const int cc = (k3 * G.nb[1] + j3) * G.nb[0] + i3;
+          for (int e = G.start[cc]; e < G.start[cc + 1]; ++e) {
+            const int u = G.items[e];
+            if (u == t) continue;
+            TypeDesc const& tu = A.types[type[u]];
+            const V3<T> xu = ldv(x, u);
+            const double dx = val(xu.x) - val(xt.x), dy = val(xu.y) - val(xt.y),
+                         dz = val(xu.z) - val(xt.z);
+            const double R = (tp.radius + tu.radius) * (1. + 1.e-9);
+            if (dx * dx + dy * dy + dz * dz >= R * R) continue;
+            if (nc < kAdjCap) cand[nc++] = u;
+            else atomicOr(overflow, 1);
+          }
+        }
+    for (int i = 1; i < nc; ++i) {
+      const int u = cand[i];
+      int j = i - 1;
+      while (j >= 0 && cand[j] > u) {
+        cand[j + 1] = cand[j];
+        --j;
+      }
+      cand[j + 1] = u;
+    }
+  }
   int k = 0;
-  for (int u = 0; u < n; ++u) {
-    if (u == t) continue;
-    TypeDesc const& tu = A.types[type[u]];
-    const V3<T> xu = ldv(x, u);
-    const double dx = val(xu.x) - val(xt.x), dy = val(xu.y) - val(xt.y), dz = val(xu.z) - val(xt.z);
-    const double R = (tp.radius + tu.radius) * (1. + 1.e-9);
-    if (dx * dx + dy * dy + dz * dz >= R * R) continue;
+  for (int q = 0; q < nc; ++q) {
+    const int u = cand[q];
     const int a = t < u ? t : u, b = t < u ? u : t;
     TypeDesc const& ta = A.types[type[a]];
     TypeDesc const& tb = A.types[type[b]];
@@ -494,6 +606,9 @@ struct AdjointSystem {
   int* d_type = nullptr;
   double *d_x0 = nullptr, *d_v0 = nullptr, *d_w0 = nullptr;
   int* d_overflow = nullptr;
+  AdjGrid G{};
+  int *d_cell = nullptr, *d_count = nullptr, *d_fill = nullptr, *d_start = nullptr,
+      *d_items = nullptr;
   std::vector<void*> allocs;
   cudaStream_t st = nullptr;
 
@@ -557,6 +672,31 @@ struct AdjointSystem {
     A.nwalls = (int)setup.walls.size();
     A.dt = setup.dt;
     d_overflow = alloc<int>(1);
+    // pair-search grid: cells at least the largest contact distance wide,
+    // at most 2^22 of them
+    double rmax = 0.;
+    for (auto const& t : setup.types) rmax = std::max(rmax, t.radius);
+    const double emin = 2. * rmax * (1. + 1.e-6);
+    for (int d = 0; d < 3; ++d) {
+      const double L = setup.maxc[d] - setup.origin[d];
+      G.nb[d] = (L > 0. && emin > 0.) ? std::max(1, (int)std::min(std::floor(L / emin), 1.e6)) : 1;
+      G.org[d] = setup.origin[d];
+    }
+    while ((long long)G.nb[0] * G.nb[1] * G.nb[2] > (1ll << 22)) {
+      int dm = 0;
+      for (int d = 1; d < 3; ++d)
+        if (G.nb[d] > G.nb[dm]) dm = d;
+      G.nb[dm] = (G.nb[dm] + 1) / 2;
+    }
+    for (int d = 0; d < 3; ++d) {
+      const double L = setup.maxc[d] - setup.origin[d];
+      G.inv_edge[d] = L > 0. ? G.nb[d] / L : 0.;
+    }
+    G.ncells = G.nb[0] * G.nb[1] * G.nb[2];
+    d_count = alloc<int>(G.ncells);
+    d_fill = alloc<int>(G.ncells);
+    d_start = alloc<int>((size_t)G.ncells + 1);
+    G.start = d_start;
   }
 
   void setParticles(int64_t nn, const int* type, const double* x0, const double* v0,
@@ -571,6 +711,10 @@ struct AdjointSystem {
     d_x0 = alloc<double>(3 * (size_t)n);
     d_v0 = alloc<double>(3 * (size_t)n);
     d_w0 = alloc<double>(3 * (size_t)n);
+    d_cell = alloc<int>(n);
+    d_items = alloc<int>(n);
+    G.cell = d_cell;
+    G.items = d_items;
     ACK(cudaMemcpy(d_type, type, n * sizeof(int), cudaMemcpyHostToDevice));
     ACK(cudaMemcpy(d_x0, x0, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
     ACK(cudaMemcpy(d_v0, v0, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
@@ -617,6 +761,19 @@ struct AdjointSystem {
       ACK(cudaMemcpyAsync(pr.first, pr.second, b, cudaMemcpyDeviceToDevice, st));
   }
 
+  // Contact forces at positions x (the grid is rebuilt from them first).
+  template <typename T>
+  void forces(const T* x, const T* vel, const T* omg, ListsT<T> const& prev, int has_prev,
+              ListsT<T> const& cur, T* F, T* Tq, T kn, T en, T muc, int zero_spring) {
+    ACK(cudaMemsetAsync(d_count, 0, (size_t)G.ncells * sizeof(int), st));
+    ACK(cudaMemsetAsync(d_fill, 0, (size_t)G.ncells * sizeof(int), st));
+    k_adj_bin<T><<<nblk(n), 128, 0, st>>>(n, G, x, d_cell, d_count);
+    k_adj_scan<<<1, 1024, 0, st>>>(G.ncells, d_count, d_start);
+    k_adj_place<<<nblk(n), 128, 0, st>>>(n, d_cell, d_start, d_fill, d_items);
+    k_fwd_forces<T><<<nblk(n), 128, 0, st>>>(n, A, G, d_type, x, vel, omg, prev, has_prev, cur,
+                                             F, Tq, kn, en, muc, zero_spring, d_overflow);
+  }
+
   // Leapfrog start: forces at (x0, v0, w0) with no history, spring zeroed.
   template <typename T>
   void start(State<T>& S, ListsT<T>& L, T kn, T en, T muc, int seed_v0 = -1) {
@@ -625,8 +782,7 @@ struct AdjointSystem {
     k_promote<T><<<nblk(n3), 128, 0, st>>>(n3, d_v0, S.v);
     if (seed_v0 >= 0) k_seed<T><<<1, 1, 0, st>>>(S.v, seed_v0);
     k_promote<T><<<nblk(n3), 128, 0, st>>>(n3, d_w0, S.w);
-    k_fwd_forces<T><<<nblk(n), 128, 0, st>>>(n, A, d_type, S.x, S.v, S.w, L, 0, L, S.F, S.Tq,
-                                             kn, en, muc, 1, d_overflow);
+    forces<T>(S.x, S.v, S.w, L, 0, L, S.F, S.Tq, kn, en, muc, 1);
     ACK(cudaGetLastError());
   }
   // One step: move into (xs, vh, wh), forces with history prev -> cur,
@@ -635,8 +791,7 @@ struct AdjointSystem {
   void advance(State<T>& S, T* xs, T* vh, T* wh, ListsT<T> const& prev, ListsT<T> const& cur,
                T kn, T en, T muc) {
     k_fwd_move<T><<<nblk(n), 128, 0, st>>>(n, A, d_type, S.x, S.v, S.w, S.F, S.Tq, xs, vh, wh);
-    k_fwd_forces<T><<<nblk(n), 128, 0, st>>>(n, A, d_type, xs, vh, wh, prev, 1, cur, S.F, S.Tq,
-                                             kn, en, muc, 0, d_overflow);
+    forces<T>(xs, vh, wh, prev, 1, cur, S.F, S.Tq, kn, en, muc, 0);
     k_fwd_close<T><<<nblk(n), 128, 0, st>>>(n, A, d_type, vh, wh, S.F, S.Tq, S.v, S.w);
     ACK(cudaMemcpyAsync(S.x, xs, 3 * (size_t)n * sizeof(T), cudaMemcpyDeviceToDevice, st));
     ACK(cudaGetLastError());

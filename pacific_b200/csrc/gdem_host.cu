@@ -1183,7 +1183,11 @@ void readAdjointSetup(std::string const& path, AdjointSetup& out) {
   out.walls = I.walls;
   for (int k = 0; k < kMaxMat * kMaxMat; ++k) out.models[k] = I.models[k];
   out.dt = I.dt;
-  for (int d = 0; d < 3; ++d) out.periodic[d] = I.grid.periodic[d];
+  for (int d = 0; d < 3; ++d) {
+    out.periodic[d] = I.grid.periodic[d];
+    out.origin[d] = I.box_org[d];
+    out.maxc[d] = I.box_max[d];
+  }
 }
 
 }  // namespace gdem

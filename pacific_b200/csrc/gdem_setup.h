@@ -14,6 +14,7 @@ struct AdjointSetup {
   ModelDesc models[kMaxMat * kMaxMat];
   double dt = 0.;
   int periodic[3] = {0, 0, 0};
+  double origin[3] = {0., 0., 0.}, maxc[3] = {0., 0., 0.};   // the domain box
 };
 
 // Throws std::runtime_error on malformed input.
