@@ -367,7 +367,9 @@ __device__ __forceinline__ void sumShares(DevState const& S, int t, TypeDesc con
   }
 }
 
-// Leapfrog of each particle.  With kStepSum the force and torque of this
+// Leapfrog of each particle (FP32-split spheres: four 256-thread blocks per
+// multiprocessor, which measured faster than three or five; the kernel is
+// bound by the latency of its loads).  With kStepSum the force and torque of this
 // evaluation: the weight for a particle the contact filter did not mark as a
 // candidate, else the weight plus its shares (sumShares); without it, the
 // stored F, T (the opening kick of a call continues from the last evaluation
@@ -384,7 +386,7 @@ __device__ __forceinline__ void sumShares(DevState const& S, int t, TypeDesc con
 // takes no share and is not read by the pair kernel, so its leapfrog runs at
 // once; a candidate waits for the pair kernel before it reads its shares.
 template <bool kFast, bool kBasis>
-__global__ void __launch_bounds__(256, (kFast && kBasis) ? 2 : 3) k_move(DevState S, int flags) {
+__global__ void __launch_bounds__(256, (kFast && kBasis) ? 2 : (kFast ? 4 : 3)) k_move(DevState S, int flags) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
   TypeDesc const& tp = S.types[S.type[t]];
