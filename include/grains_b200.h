@@ -74,6 +74,37 @@ int gdem_upload_state(gdem_handle h, int64_t n, const int* inst, const int* type
  * them, SecondOrderLeapFrog.cpp:102-109); marks the leapfrog as started. */
 int gdem_upload_forces(gdem_handle h, const double* F, const double* T);
 
+/* Room for `extra` particles inserted after the upload (gdem_insert_particle):
+ * the particle buffers are sized for n + extra when the state is uploaded.
+ * Call before gdem_upload_state.  Replaces the reference's waiting particles
+ * (AllComponents::m_WaitParticles, activated by Grains::insertParticle,
+ * Base/src/Grains.cpp:2063-2139). */
+int gdem_reserve(gdem_handle h, int64_t extra);
+
+/* One insertion attempt (Grains::insertParticle with
+ * LinkedCell::insertParticleSerial, Base/src/LinkedCell.cpp:1765-1840): a
+ * particle of class `type` at position x, velocity v, space-fixed angular
+ * velocity w, quaternion q (qx, qy, qz, qw) and, when basis is not NULL, that
+ * orientation matrix (row-major; otherwise the matrix of q).  Unless force,
+ * it is inserted only when it touches no particle (at its periodic images
+ * within one period where the domain is periodic) and no wall, as
+ * RigidBodyWithCrust::isContact (Geometry/src/RigidBodyWithCrust.cpp:
+ * 840-958) decides: two spheres when their centres are closer than the sum
+ * of their radii, a sphere and a box when the sphere overlaps the box,
+ * other shapes when their circumscribed spheres overlap and -- unless bv_only
+ * (GeometricOverlap Value="BV") -- the GJK distance of the shrunk bodies is
+ * below the sum of the crusts minus 1e-10.  On insertion *inserted = 1 and
+ * *id (may be NULL) = its particle ID (the particle count before the call);
+ * its force is its weight and its torque zero (Particle::InitializeForce),
+ * and the next gdem_step starts its leapfrog with the others'.  ref_id: its
+ * ID in reload files written later (<= 0: its particle ID + 1).  Single
+ * systems, between gdem_step calls; needs room from gdem_reserve.  A
+ * polyhedron's GJK search starts from the particle's and the candidate's
+ * current vertices and moves neither. */
+int gdem_insert_particle(gdem_handle h, int type, const double* x, const double* v,
+                         const double* w, const double* q, const double* basis, int force,
+                         int bv_only, int ref_id, int* inserted, int* id);
+
 /* Replaces the whole particle state of an uploaded system (same particle
  * count) without allocating: x, v, w, q (and optionally wbf) by particle ID
  * from caller memory (pinned memory gives full-speed copies).  With F and T

@@ -317,6 +317,94 @@ __global__ void __launch_bounds__(128) k_pairlaw64(DevState S) {
   st.flush(S.cstats, tag);
 }
 
+
+// ------------------------------------------------------------- insertion --
+// The overlap test of one insertion attempt (LinkedCell::isContactWithCrust,
+// Base/src/LinkedCell.cpp:1211-1240, through Cell::isContactWithCrust,
+// Base/src/Cell.cpp:250-290): the candidate against every particle (at its
+// periodic images within one period where the domain is periodic, as the
+// reference tests the candidate and its clones against the cells' particles
+// and clones) and every wall.  The test of two bodies is
+// RigidBodyWithCrust::isContact (Geometry/src/RigidBodyWithCrust.cpp:
+// 840-958): two spheres touch when their centres are closer than the sum of
+// the radii (isContactSPHERESPHERE), a sphere and a box when the sphere
+// overlaps the box (isContactSPHEREBOX, the box's own frame: a wall's is its
+// centre); otherwise when the circumscribed spheres overlap and -- unless
+// bv_only (GeometricOverlap Value="BV") -- the GJK distance of the shrunk
+// bodies is below the sum of the crusts minus 1e-10.  A polyhedron's search
+// starts from the particle's current vertex and from the candidate's first
+// vertex with a neighbour, and moves neither.
+__device__ bool insertTouch(DevState const& S, TypeDesc const& ta, XForm64 const& a2w,
+                            const double* basis_a, int stride_a, int slot_a, int cur_a,
+                            TypeDesc const& tb, d3 xb, const double* basis_b, int bv_only) {
+  const d3 xa = a2w.o;
+  if (ta.shape == 0 && tb.shape == 0) return norm(xb - xa) - (ta.radius + tb.radius) < 0.;
+  if ((ta.shape == 0 && tb.shape == 1) || (ta.shape == 1 && tb.shape == 0)) {
+    // the sphere's centre in the box's frame: R^T (p - o)
+    const bool a_sphere = ta.shape == 0;
+    TypeDesc const& box = a_sphere ? tb : ta;
+    const d3 p = (a_sphere ? xa : xb) - (a_sphere ? xb : xa);
+    double R[9];
+    if (a_sphere) {
+      for (int k = 0; k < 9; ++k) R[k] = basis_b[k];
+    } else {
+      for (int k = 0; k < 9; ++k) R[k] = basis_a[k * stride_a + slot_a];
+    }
+    const d3 local = mk(R[0] * p.x + R[3] * p.y + R[6] * p.z, R[1] * p.x + R[4] * p.y + R[7] * p.z,
+                        R[2] * p.x + R[5] * p.y + R[8] * p.z);
+    double ov = 1.;
+    boxSphere(mk(box.extent[0], box.extent[1], box.extent[2]), local,
+              a_sphere ? ta.radius : tb.radius, ov);
+    return ov < 0.;
+  }
+  if (!(norm(xa - xb) < ta.radius + tb.radius)) return false;
+  if (bv_only) return true;
+  const XForm64 b2w = crustXForm(basis_b, 1, 0, tb.scaling, xb);
+  d3 pA, pB;
+  int it = 0, ca = cur_a, cb = tb.poly_start;
+  const double d = closestPoints64(convexOf(ta, S), a2w, convexOf(tb, S), b2w, pA, pB, &it, ca, cb);
+  return d < ta.crust + tb.crust - 1.0e-10;
+}
+
+__global__ void k_insert_test(DevState S, NewParticle p, int bv_only, int* hit) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  GridDesc const& g = S.grids[0];
+  TypeDesc const& tc = S.types[p.type];
+  const d3 xc = mk(p.x[0], p.x[1], p.x[2]);
+  bool touch = false;
+  if (i < S.n) {
+    TypeDesc const& tu = S.types[S.type[i]];
+    const d3 xu = ld3(S.x, S.cap, i);
+    const int cur = S.curv ? S.curv[i] : 0;
+    for (int sx = g.periodic[0] ? -1 : 0; sx <= (g.periodic[0] ? 1 : 0) && !touch; ++sx)
+      for (int sy = g.periodic[1] ? -1 : 0; sy <= (g.periodic[1] ? 1 : 0) && !touch; ++sy)
+        for (int sz = g.periodic[2] ? -1 : 0; sz <= (g.periodic[2] ? 1 : 0) && !touch; ++sz) {
+          const d3 xi = xu + mk(sx * g.L[0], sy * g.L[1], sz * g.L[2]);
+          const XForm64 a2w = (tu.shape == 0 || !S.basis)
+                                  ? identityXForm(tu.scaling, xi)
+                                  : crustXForm(S.basis, S.cap, i, tu.scaling, xi);
+          touch = insertTouch(S, tu, a2w, S.basis, S.cap, i, cur, tc, xc, p.basis, bv_only);
+        }
+  } else if (i < S.n + g.wall_count) {
+    WallDesc const& wd = S.walls[g.wall_begin + (i - S.n)];
+    const d3 o = mk(wd.centre[0], wd.centre[1], wd.centre[2]);
+    if (tc.shape == 0) {
+      double ov = 1.;
+      boxSphere(mk(wd.extent[0], wd.extent[1], wd.extent[2]), xc - o, tc.radius, ov);
+      touch = ov < 0.;
+    } else if (norm(xc - o) < wd.radius + tc.radius) {
+      touch = true;
+      if (!bv_only) {
+        d3 pA, pB;
+        int it = 0, cw = 0, cb = tc.poly_start;
+        const double d = closestPoints64(convexOf(wd), identityXForm(wd.scaling, o), convexOf(tc, S),
+                                         crustXForm(p.basis, 1, 0, tc.scaling, xc), pA, pB, &it, cw, cb);
+        touch = d < wd.crust + tc.crust - 1.0e-10;
+      }
+    }
+  }
+  if (touch) atomicOr(hit, 1);
+}
 }  // namespace
 
 void launch_pairs64(DevState const& S, const int* gate, int fill, cudaStream_t st) {
@@ -329,6 +417,11 @@ void launch_pairlaw64(DevState const& S, cudaStream_t st) {
   const int grid = (S.forces_bps > 0 ? S.forces_bps : 4) * S.nsm;
   if (S.any_convex) launchAfterPrevious(k_pairlaw64<true>, grid, 128, st, S);
   else launchAfterPrevious(k_pairlaw64<false>, grid, 128, st, S);
+}
+void launch_insert_test(DevState const& S, NewParticle const& p, int bv_only, int* hit,
+                        cudaStream_t st) {
+  const int n = S.n + S.max_walls;
+  k_insert_test<<<(n + 127) / 128, 128, 0, st>>>(S, p, bv_only, hit);
 }
 
 }  // namespace gdem

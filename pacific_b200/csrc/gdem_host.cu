@@ -573,6 +573,8 @@ struct System {
   std::vector<int> type_base;     // first global type of each instance
   std::vector<int> id_base;       // first particle ID of each instance
   std::vector<int> inst_n;
+  int reserve_extra = 0;           // room for particles inserted after the upload
+  int* d_hit = nullptr;            // insertion overlap flag
   DevState S{};
   GridDesc* d_grids = nullptr; TypeDesc* d_types = nullptr; ModelDesc* d_models = nullptr;
   WallDesc* d_walls = nullptr;
@@ -804,7 +806,7 @@ struct System {
 
   void allocateParticles(int n) {
     S.n = n;
-    S.cap = std::max(n, 1);
+    S.cap = std::max(n + reserve_extra, 1);
     size_t c = (size_t)S.cap;
     S.id = alloc<int>(c); S.type = alloc<int>(c); S.inst = alloc<int>(c);
     S.id2 = alloc<int>(c); S.type2 = alloc<int>(c); S.inst2 = alloc<int>(c);
@@ -1231,8 +1233,10 @@ int gdem_upload_state(gdem_handle h, int64_t n, const int* inst, const int* type
                       const double* q) {
   return guarded([&] {
     System* s = sys(h);
-    if (!s || n <= 0 || !type || !x || !v || !w || !q) throw std::runtime_error("invalid arguments");
-    if (n > (int64_t(1) << kMaxIdBits) - 64)
+    // (an empty system only when particles are to be inserted into it)
+    if (!s || n < 0 || (n == 0 && s->reserve_extra == 0) || !type || !x || !v || !w || !q)
+      throw std::runtime_error("invalid arguments");
+    if (n + s->reserve_extra > (int64_t(1) << kMaxIdBits) - 64)
       throw std::runtime_error("too many particles for the 27-bit particle IDs of the contact keys");
     if (s->have_state) throw std::runtime_error("state already uploaded");
     int N = (int)n;
@@ -1262,6 +1266,82 @@ int gdem_upload_state(gdem_handle h, int64_t n, const int* inst, const int* type
     s->loadState(x, v, w, wbf, q, nullptr, nullptr);
     s->have_state = true;
     s->evaluated = 0;
+    return GDEM_OK;
+  });
+}
+
+int gdem_reserve(gdem_handle h, int64_t extra) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || extra < 0 || extra > (int64_t(1) << kMaxIdBits)) throw std::runtime_error("invalid arguments");
+    if (s->have_state) throw std::runtime_error("reserve before the state is uploaded");
+    s->reserve_extra = (int)extra;
+    return GDEM_OK;
+  });
+}
+
+int gdem_insert_particle(gdem_handle h, int type, const double* x, const double* v,
+                         const double* w, const double* q, const double* basis, int force,
+                         int bv_only, int ref_id, int* inserted, int* id) {
+  return guarded([&] {
+    System* s = sys(h);
+    if (!s || !x || !v || !w || !q || !inserted) throw std::runtime_error("invalid arguments");
+    if (!s->have_state) throw std::runtime_error("upload the state first");
+    if (s->inst.size() != 1) throw std::runtime_error("insertion is for single systems");
+    if (type < 0 || type >= (int)s->inst[0].types.size())
+      throw std::runtime_error("particle type out of range");
+    DevState& S = s->S;
+    if (S.n >= S.cap) throw std::runtime_error("no room for another particle (gdem_reserve)");
+    NewParticle p{};
+    p.type = s->type_base[0] + type;
+    p.id = S.n;
+    p.slot = S.n;
+    p.has_basis = basis ? 1 : 0;
+    for (int d = 0; d < 3; ++d) { p.x[d] = x[d]; p.v[d] = v[d]; p.w[d] = w[d]; }
+    for (int k = 0; k < 4; ++k) p.q[k] = q[k];
+    if (basis) {
+      for (int k = 0; k < 9; ++k) p.basis[k] = basis[k];
+    } else {
+      // Matrix::setRotation (Geometry/src/Matrix.cpp:114-127), for the test
+      const double qx = q[0], qy = q[1], qz = q[2], qw = q[3];
+      const double sc = 2.0 / (qx * qx + qy * qy + qz * qz + qw * qw);
+      const double xs = qx * sc, ys = qy * sc, zs = qz * sc;
+      const double wx = qw * xs, wy = qw * ys, wz = qw * zs;
+      const double xx = qx * xs, xy = qx * ys, xz = qx * zs, yy = qy * ys, yz = qy * zs,
+                   zz = qz * zs;
+      const double m[9] = {1.0 - (yy + zz), xy - wz, xz + wy, xy + wz, 1.0 - (xx + zz),
+                           yz - wx, xz - wy, yz + wx, 1.0 - (xx + yy)};
+      for (int k = 0; k < 9; ++k) p.basis[k] = m[k];
+    }
+    *inserted = 0;
+    if (!force) {
+      if (!s->d_hit) s->d_hit = s->alloc<int>(1);
+      CK(cudaMemsetAsync(s->d_hit, 0, sizeof(int), s->stream));
+      launch_insert_test(S, p, bv_only, s->d_hit, s->stream);
+      CK(cudaGetLastError());
+      int hit = 0;
+      CK(cudaMemcpyAsync(&hit, s->d_hit, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+      CK(cudaStreamSynchronize(s->stream));
+      if (hit) return GDEM_OK;
+    }
+    launch_append_particle(S, p, s->stream);
+    CK(cudaGetLastError());
+    S.n += 1;
+    s->h_type.push_back(type);
+    s->h_inst.push_back(0);
+    s->inst_n[0] += 1;
+    if (!s->ref_ids.empty()) s->ref_ids.push_back(ref_id > 0 ? ref_id : S.n);
+    // the pair list does not hold the new particle: rebuild before the next
+    // force evaluation; the graphs hold the old particle count
+    static const int one = 1;
+    CK(cudaMemcpyAsync(S.ctl + kCtlNeed, &one, sizeof(int), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    // the contact filter's grid, for about 4 pairs per particle (its kernel
+    // loops over any excess)
+    S.filter_qblocks = std::max(S.filter_qblocks, (4 * S.n + 1023) / 1024);
+    s->invalidateGraphs();
+    *inserted = 1;
+    if (id) *id = p.id;
     return GDEM_OK;
   });
 }

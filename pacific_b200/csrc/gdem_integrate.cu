@@ -680,6 +680,63 @@ __global__ void k_fill64(unsigned long long* p, size_t n, unsigned long long val
   if (i < n) p[i] = value;
 }
 
+// Orientation matrix of the quaternion q (x, y, z, w) with the expression
+// order of Matrix::setRotation (Geometry/src/Matrix.cpp:114-127).
+__device__ __forceinline__ void basisOfQuaternion(const double* q, double* m) {
+  const double x = q[0], y = q[1], z = q[2], w4 = q[3];
+  const double s = 2.0 / (x * x + y * y + z * z + w4 * w4);
+  const double xs = x * s, ys = y * s, zs = z * s;
+  const double wx = w4 * xs, wy = w4 * ys, wz = w4 * zs;
+  const double xx = x * xs, xy = x * ys, xz = x * zs, yy = y * ys, yz = y * zs, zz = z * zs;
+  m[0] = 1.0 - (yy + zz); m[1] = xy - wz; m[2] = xz + wy;
+  m[3] = xy + wz; m[4] = 1.0 - (xx + zz); m[5] = yz - wx;
+  m[6] = xz - wy; m[7] = yz + wx; m[8] = 1.0 - (xx + yy);
+}
+
+// An inserted particle (Grains::insertParticle, Base/src/Grains.cpp:
+// 2063-2139) written into slot p.slot, after the others: position,
+// velocities, quaternion and its orientation matrix (or the given one), the
+// body-frame angular velocity q* w q, its weight as force and a zero torque
+// (Particle::InitializeForce(true)), the start vertex of a new polyhedron,
+// no displacement, wraps or contact marks.  The host asks for a pair-list
+// rebuild before the next force evaluation.
+__global__ void k_append_particle(DevState S, NewParticle p) {
+  if (threadIdx.x || blockIdx.x) return;
+  const int cap = S.cap, i = p.slot;
+  TypeDesc const& tp = S.types[p.type];
+  S.id[i] = p.id;
+  S.type[i] = p.type;
+  S.inst[i] = 0;
+  const d3 x = mk(p.x[0], p.x[1], p.x[2]), w = mk(p.w[0], p.w[1], p.w[2]);
+  st3(S.x, cap, i, x);
+  st3(S.v, cap, i, mk(p.v[0], p.v[1], p.v[2]));
+  st3(S.w, cap, i, w);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) S.q[k * cap + i] = p.q[k];
+  if (S.basis) {
+    double m[9];
+    if (p.has_basis) {
+      for (int k = 0; k < 9; ++k) m[k] = p.basis[k];
+    } else {
+      basisOfQuaternion(p.q, m);
+    }
+    for (int k = 0; k < 9; ++k) S.basis[k * cap + i] = m[k];
+  }
+  const dq qq = qmk(mk(p.q[0], p.q[1], p.q[2]), p.q[3]);
+  st3(S.wbf, cap, i, multToVector3(conj(qq), vecq(w, qq)));
+  st3(S.F, cap, i, mk(tp.weight[0], tp.weight[1], tp.weight[2]));
+  st3(S.T, cap, i, mk(0., 0., 0.));
+  S.disp[i] = 0.f; S.disp[cap + i] = 0.f; S.disp[2 * cap + i] = 0.f;
+  S.wrap[i] = 0;
+  if (S.curv) {
+    S.curv[i] = tp.poly_start;
+    S.curv_next[i] = 0;
+  }
+  S.nact[i] = 0;
+  S.nact[cap + i] = 0;
+  S.posf[i] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)tp.radius);
+}
+
 // Loads host-layout state (AoS, by particle ID, staged in device memory)
 // into the SoA arrays, in ID order.
 __global__ void k_load_state(DevState S, const double* x, const double* v, const double* w,
@@ -703,15 +760,9 @@ __global__ void k_load_state(DevState S, const double* x, const double* v, const
 #pragma unroll
   for (int k = 0; k < 4; ++k) S.q[k * cap + i] = q[4 * i + k];
   if (S.basis) {
-    // orientation matrix of q with the expression order of Matrix::setRotation
-    // (Geometry/src/Matrix.cpp:114-127); gdem_upload_basis may replace it
-    double x = q[4 * i], y = q[4 * i + 1], z = q[4 * i + 2], w4 = q[4 * i + 3];
-    double s = 2.0 / (x * x + y * y + z * z + w4 * w4);
-    double xs = x * s, ys = y * s, zs = z * s;
-    double wx = w4 * xs, wy = w4 * ys, wz = w4 * zs;
-    double xx = x * xs, xy = x * ys, xz = x * zs, yy = y * ys, yz = y * zs, zz = z * zs;
-    double m[9] = {1.0 - (yy + zz), xy - wz, xz + wy, xy + wz, 1.0 - (xx + zz), yz - wx,
-                   xz - wy, yz + wx, 1.0 - (xx + yy)};
+    // gdem_upload_basis may replace it
+    double m[9];
+    basisOfQuaternion(q + 4 * i, m);
 #pragma unroll
     for (int k = 0; k < 9; ++k) S.basis[k * cap + i] = m[k];
   }
@@ -859,6 +910,9 @@ void launch_move(DevState const& S, int flags, int fast, cudaStream_t st) {
   else if (S.basis) launchAfterPrevious(k_move<true, true>, nb, 256, st, M, flags);
   else launchAfterPrevious(k_move<true, false>, nb, 256, st, M, flags);
 }
+void launch_append_particle(DevState const& S, NewParticle const& p, cudaStream_t st) {
+  k_append_particle<<<1, 32, 0, st>>>(S, p);
+}
 void launch_fill64(unsigned long long* p, size_t n, unsigned long long value, cudaStream_t st) {
   if (n) k_fill64<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p, n, value);
 }
@@ -876,7 +930,7 @@ void launch_set_velocities(DevState const& S, const double* v, const double* w, 
 }
 void launch_vstats(DevState const& S, double* part, double* out, cudaStream_t st) {
   int nb = blocks(S.n, 256);
-  k_vstats_partial<<<nb, 256, 0, st>>>(S, part);
+  if (nb) k_vstats_partial<<<nb, 256, 0, st>>>(S, part);   // (none: an empty system)
   k_vstats_final<<<1, 256, 0, st>>>(part, nb, S.n, out);
 }
 void launch_scatter_by_id(DevState const& S, double* x, double* v, double* w, double* wbf,

@@ -84,6 +84,21 @@ void launch_pair_counts(DevState const& S, unsigned long long* out, cudaStream_t
 void launch_pairs64(DevState const& S, const int* gate, int fill, cudaStream_t st);
 void launch_pairlaw64(DevState const& S, cudaStream_t st);
 
+// A particle inserted during the run (gdem_insert_particle): its class
+// (global index), device ID and slot, position, velocity, space-frame
+// angular velocity, quaternion (x, y, z, w) and, when has_basis, its
+// orientation matrix (row-major; otherwise the matrix of q).
+struct NewParticle {
+  int type, id, slot, has_basis;
+  double x[3], v[3], w[3], q[4], basis[9];
+};
+// Sets *hit when the particle p would touch a particle or a wall
+// (LinkedCell::insertParticleSerial's test); FP64.
+void launch_insert_test(DevState const& S, NewParticle const& p, int bv_only, int* hit,
+                        cudaStream_t st);
+// Writes p into slot p.slot with its weight as force (Particle::InitializeForce).
+void launch_append_particle(DevState const& S, NewParticle const& p, cudaStream_t st);
+
 // gdem_contact32.cu (FP32-split mode)
 void launch_pairs32(DevState const& S, const int* gate, int fill, cudaStream_t st);
 void launch_pairlaw32(DevState const& S, cudaStream_t st);

@@ -76,6 +76,9 @@ def library() -> ctypes.CDLL:
                                ctypes.POINTER(_P)], ctypes.c_int),
         "gdem_upload_state": ([_P, i64, _IP, _IP, _DP, _DP, _DP, _DP, _DP], ctypes.c_int),
         "gdem_upload_forces": ([_P, _DP, _DP], ctypes.c_int),
+        "gdem_reserve": ([_P, i64], ctypes.c_int),
+        "gdem_insert_particle": ([_P, ctypes.c_int, _DP, _DP, _DP, _DP, _DP, ctypes.c_int,
+                                  ctypes.c_int, ctypes.c_int, _IP, _IP], ctypes.c_int),
         "gdem_upload_history": ([_P, i64, _IP, _IP, _DP, _DP, _DP], ctypes.c_int),
         "gdem_write_reload_particles": ([_P, ctypes.c_char_p], ctypes.c_int),
         "gdem_write_reload_particles_hybrid": ([_P, ctypes.c_char_p], ctypes.c_int),
@@ -262,6 +265,28 @@ class Grains:
         out = np.empty((self.n, 9))
         self._check(library().gdem_download_basis(self._h, _dp(out)))
         return out
+
+    def reserve(self, extra):
+        """Room for `extra` particles inserted after the upload (before
+        upload_state)."""
+        self._check(library().gdem_reserve(self._h, int(extra)))
+
+    def insert_particle(self, type, x, v=(0., 0., 0.), w=(0., 0., 0.), q=(0., 0., 0., 1.),
+                        basis=None, force=False, bv_only=False, ref_id=0):
+        """One insertion attempt (Grains::insertParticle): the particle goes in
+        unless it touches a particle or a wall (or force).  Returns its
+        particle ID, or None when it was not inserted."""
+        arr = [_f64(a, (k,)) for a, k in ((x, 3), (v, 3), (w, 3), (q, 4))]
+        b = _f64(basis, (9,))
+        ins = ctypes.c_int(0)
+        pid = ctypes.c_int(-1)
+        self._check(library().gdem_insert_particle(
+            self._h, int(type), *[_dp(a) for a in arr], _dp(b), 1 if force else 0,
+            1 if bv_only else 0, int(ref_id), ctypes.byref(ins), ctypes.byref(pid)))
+        if not ins.value:
+            return None
+        self.n += 1
+        return pid.value
 
     def upload_forces(self, F, T):
         F = _f64(F, (self.n, 3))

@@ -24,7 +24,7 @@ void fail(char const* where) {
 
 }  // namespace
 
-GrainsB200::GrainsB200() : Grains(), m_dev(nullptr), m_convex(false) {}
+GrainsB200::GrainsB200() : Grains(), m_dev(nullptr), m_convex(false), m_insert_counter(0) {}
 
 GrainsB200::~GrainsB200() {
   if (m_dev) gdem_destroy(m_dev);
@@ -57,9 +57,13 @@ void GrainsB200::do_before_time_stepping(DOMElement* rootElement) {
   m_byIndex.clear();
   for (auto const& e : byId) m_byIndex.push_back(e.second);
   const size_t n = m_byIndex.size();
-  vector<int> type(n);
-  vector<double> x(3 * n), v(3 * n), w(3 * n), q(4 * n), basis(9 * n);
+  // (arrays of at least one entry: an over-time insertion may start empty)
+  vector<int> type(max<size_t>(n, 1));
+  vector<double> x(3 * max<size_t>(n, 1)), v(x.size()), w(x.size()), q(4 * max<size_t>(n, 1)),
+      basis(9 * max<size_t>(n, 1));
   m_convex = false;
+  for (Particle const* r : *m_allcomponents.getReferenceParticles())
+    if (r->getRigidBody()->getConvex()->getConvexType() != SPHERE) m_convex = true;
   for (size_t i = 0; i < n; ++i) {
     Particle* p = m_byIndex[i];
     type[i] = p->getGeometricType();
@@ -80,13 +84,88 @@ void GrainsB200::do_before_time_stepping(DOMElement* rootElement) {
     q[4 * i + 3] = (*qr)[W];
     if (p->getRigidBody()->getConvex()->getConvexType() != SPHERE) m_convex = true;
   }
-  if (gdem_upload_state(m_dev, (int64_t)n, nullptr, type.data(), x.data(), v.data(), w.data(),
+  const size_t waiting =
+      m_insertion_mode == IM_OVERTIME ? m_allcomponents.getNumberPhysicalParticlesToInsert() : 0;
+  if ((waiting && gdem_reserve(m_dev, (int64_t)waiting) != GDEM_OK) ||
+      gdem_upload_state(m_dev, (int64_t)n, nullptr, type.data(), x.data(), v.data(), w.data(),
                         nullptr, q.data()) != GDEM_OK ||
       (m_convex && gdem_upload_basis(m_dev, basis.data()) != GDEM_OK) ||
       gdem_set_time_step(m_dev, m_dt) != GDEM_OK || gdem_init(m_dev) != GDEM_OK) {
     fail("device set-up");
     m_error_occured = true;
   }
+}
+
+// Grains::insertParticle (Base/src/Grains.cpp:2063-2139) during the run: the
+// particle to insert, its position (the list of positions, else a random
+// point of a random window), its angular position and its velocities come
+// from the reference's own members in the reference's order (so the random
+// draws are the same); LinkedCell::insertParticleSerial's overlap test and
+// the insertion are gdem_insert_particle.  The attempt counter and the
+// bookkeeping of the position lists are the reference's.
+bool GrainsB200::insertParticle(PullMode const& mode) {
+  if (!m_dev) return Grains::insertParticle(mode);
+  bool insert = true;
+  const size_t npositions = m_insertion_position->size();
+  const size_t nangpositions = m_insertion_angular_position->size();
+  if (m_insert_counter == 0) {
+    Particle* particle = m_allcomponents.getParticleToInsert(mode);
+    if (particle) {
+      particle->setPosition(getInsertionPoint());
+      if (m_init_angpos != IAP_FIXED) {
+        Transform trot;
+        if (m_init_angpos == IAP_RANDOM) {
+          trot.setBasis(GrainsExec::RandomRotationMatrix(m_dimension));
+        } else {
+          m_il_sap = m_insertion_angular_position->begin();
+          trot.setBasis(*m_il_sap);
+        }
+        particle->composePositionRightByTransform(trot);
+      }
+      Vector3 vtrans, vrot;
+      computeInitVit(vtrans, vrot);
+      particle->setTranslationalVelocity(vtrans);
+      particle->setAngularVelocity(vrot);
+      particle->initialize_transformWithCrust_to_notComputed();
+      Quaternion qrot;
+      qrot.setQuaternion(particle->getRigidBody()->getTransform()->getBasis());
+      particle->setQuaternionRotation(qrot);
+      double x[3], v[3], w[3], q[4] = {qrot[X], qrot[Y], qrot[Z], qrot[W]}, basis[9];
+      Matrix const& b = particle->getRigidBody()->getTransform()->getBasis();
+      for (int d = 0; d < 3; ++d) {
+        x[d] = (*particle->getPosition())[d];
+        v[d] = vtrans[d];
+        w[d] = vrot[d];
+        for (int k = 0; k < 3; ++k) basis[3 * d + k] = b[d][k];
+      }
+      int inserted = 0, id = -1;
+      if (gdem_insert_particle(m_dev, particle->getGeometricType(), x, v, w, q, basis,
+                               m_force_insertion ? 1 : 0,
+                               GrainsExec::m_InsertionWithBVonly ? 1 : 0, particle->getID(),
+                               &inserted, &id) != GDEM_OK) {
+        fail("gdem_insert_particle");
+        m_error_occured = true;
+        inserted = 0;
+      }
+      insert = inserted != 0;
+      if (insert) {
+        m_allcomponents.WaitToActive();
+        particle->InitializeForce(true);
+        m_byIndex.push_back(particle);   // device particle index id
+        if (npositions) {
+          if (m_insertion_order == PM_RANDOM)
+            (*m_insertion_position)[m_i_sp] = m_insertion_position->back();
+          m_insertion_position->pop_back();
+          if (m_insertion_position->size() < size_t(0.5 * double(m_insertion_position->capacity())))
+            m_insertion_position->shrink_to_fit();
+        }
+        if (nangpositions) m_insertion_angular_position->erase(m_il_sap);
+      }
+    }
+  }
+  ++m_insert_counter;
+  if (m_insert_counter == m_insertion_frequency) m_insert_counter = 0;
+  return insert || m_force_insertion;
 }
 
 bool GrainsB200::checkStatus() {
@@ -199,7 +278,9 @@ void GrainsB200::downloadToParticles(bool contacts) {
 // steps between two output times on the device: the same time counter and
 // output schedule, the steps up to an output time (or the end) in one
 // gdem_step call, the last of them recording its contacts; at an output time
-// the reference's outputs from the downloaded state.
+// the reference's outputs from the downloaded state.  Over-time insertion
+// runs at the start of a step, before its move, as in the reference: the
+// steps before an insertion attempt are run first.
 void GrainsB200::Simulation(double) {
   if (!m_dev || m_error_occured) return;
   double vmax = 0., vmean = 0.;
@@ -211,6 +292,25 @@ void GrainsB200::Simulation(double) {
     if (m_timeSave != m_save.end() && *m_timeSave - m_time < 0.01 * m_dt) {
       output = true;
       m_timeSave++;
+    }
+    m_insertion_windows.Move(m_time, m_dt);
+    if (m_insertion_mode == IM_OVERTIME) {
+      if (m_insert_counter == 0 && m_allcomponents.getNumberPhysicalParticlesToInsert() &&
+          pending) {
+        if (gdem_step(m_dev, pending) != GDEM_OK) {
+          fail("gdem_step");
+          m_error_occured = true;
+          break;
+        }
+        pending = 0;
+        if (checkStatus()) {
+          m_error_occured = true;
+          break;
+        }
+      }
+      insertParticle(m_insertion_order);
+      m_allcomponents.computeNumberParticles(m_wrapper);
+      if (m_error_occured) break;
     }
     ++pending;
     if (!output && m_tend - m_time > 0.01 * m_dt) continue;

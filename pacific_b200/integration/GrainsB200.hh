@@ -9,24 +9,33 @@
 // writer stay the reference's; only the steps between two output times run on
 // the device:
 //
-//   do_before_time_stepping  Grains::do_before_time_stepping (XML, insertion,
-//                            first post-processing output), then the particles
-//                            go to the device (gdem_create on the same input
-//                            file, gdem_upload_state, gdem_upload_basis) and the
-//                            leapfrog starts there (gdem_init);
+//   do_before_time_stepping  Grains::do_before_time_stepping (XML, insertion
+//                            at the initial time, first post-processing
+//                            output), then the particles go to the device
+//                            (gdem_create on the same input file, gdem_reserve
+//                            for the particles still waiting, gdem_upload_state,
+//                            gdem_upload_basis) and the leapfrog starts there
+//                            (gdem_init);
 //   Simulation               the reference's output schedule (m_save): the steps
-//                            up to the next output time in one gdem_step call,
-//                            the last one with the contact diagnostics on; at an
-//                            output time the device state, forces and contacts
-//                            come back into the particles and the reference's
-//                            own outputs run (velocity max/mean line, reload,
-//                            post-processing writers);
+//                            up to the next output time (or insertion attempt)
+//                            in one gdem_step call, the last one with the
+//                            contact diagnostics on; at an output time the
+//                            device state, forces and contacts come back into
+//                            the particles and the reference's own outputs run
+//                            (velocity max/mean line, reload, post-processing
+//                            writers);
+//   insertParticle           insertion over time (Grains::insertParticle): the
+//                            reference picks the particle, its position,
+//                            orientation and velocities as usual; the overlap
+//                            test and the insertion run on the device
+//                            (gdem_insert_particle);
 //   do_after_time_stepping   the final state back into the particles, then
 //                            Grains::do_after_time_stepping.
 //
 // Precision: FP64 unless the environment sets GRAINS_B200_PRECISION=fp32split.
-// Not covered: insertion over time (only insertion at the initial time),
-// moving obstacles, MPI.
+// Not covered: moving obstacles, MPI.  An inserted
+// polyhedron's overlap test starts its GJK searches from the current support
+// vertices without moving them (the reference's moves them).
 #ifndef _GRAINSB200_HH_
 #define _GRAINSB200_HH_
 
@@ -45,6 +54,10 @@ class GrainsB200 : public Grains {
   void do_after_time_stepping();
 
  protected:
+  // One insertion attempt every m_insertion_frequency calls, as the
+  // reference's; before the device is set up (insertion at the initial
+  // time), the reference's own.
+  bool insertParticle(PullMode const& mode);
   // The device's status bits as the reference's exceptions would have ended
   // the run (ContactError, MotionError, SimulationError); true on an error.
   bool checkStatus();
@@ -56,6 +69,7 @@ class GrainsB200 : public Grains {
   gdem_handle m_dev;
   std::vector<Particle*> m_byIndex;   // device particle index -> particle
   bool m_convex;
+  size_t m_insert_counter;            // Grains::insertParticle's attempt counter
 };
 
 #endif

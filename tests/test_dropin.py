@@ -13,6 +13,13 @@ writers produce must agree: output times, coordination numbers and particle
 classes exactly, the printed positions and velocities (%.6e) to their last
 digit, the velocity max/mean lines, the contact memory of the final reload
 file (pairs exactly, values to round-off) and its positions to 1e-12.
+
+A second input pours particles over time (Mode Type="OverTime": one attempt
+every 20 steps at a random point of a box window, seeded random velocities):
+the reference picks each particle, point and velocity in both runs, the
+overlap test runs on the reference's host particles in one and on the device
+(gdem_insert_particle) in the other, so the same particles must go in at the
+same steps and end at the same positions.
 """
 import os
 import re
@@ -54,6 +61,39 @@ def _input(d, kind, n=200, seed=11, steps=400, every=100, dt=1e-5):
            "      </ParticlePosition>\n"
            '      <InitialVelocity Mode="Random">\n'
            '        <Translational Amplitude="0.3"/>\n'
+           '        <Angular Amplitude="0."/>\n'
+           "      </InitialVelocity>\n"
+           "    </ParticleInsertion>\n"
+           "    <PostProcessing>\n      <Writers>\n"
+           f'        <RawData Name="{d}/raw" WritingMode="Text"/>\n'
+           "      </Writers>\n    </PostProcessing>\n")
+    (d / "input.xml").write_text(text.replace("  </Simulation>", sim + "  </Simulation>"))
+    return d / "input.xml"
+
+
+def _input_overtime(d, kind, n=120, seed=5, steps=3000, every=1000, dt=1e-5):
+    """The walled box filled over time: n spheres, one insertion attempt every
+    20 steps at a random point of a window in the upper part of the box."""
+    d.mkdir(parents=True, exist_ok=True)
+    sc = scenarios.settling_box(n=n, seed=seed)
+    end = steps * dt
+    text = sc.xml().replace('<Grains3D Type="Standard">', f'<Grains3D Type="{kind}">')
+    text = re.sub(r"<TimeInterval[^>]*/>", f'<TimeInterval Start="0." End="{end!r}"/>', text)
+    sim = (f'    <RestartFile Name="{d}/res" WritingMode="Text"/>\n'
+           f'    <TimeSave Start="0." End="{end!r}" Every="{every * dt!r}"/>\n'
+           "    <ParticleInsertion>\n"
+           '      <Mode Type="OverTime"/>\n'
+           '      <Order Type="Ordered"/>\n'
+           '      <RandomGeneratorSeed Type="UserDefined" Value="3"/>\n'
+           '      <Frequency TryEvery="20"/>\n'
+           "      <ParticlePosition>\n        <Windows>\n"
+           '          <Window Type="Box">\n'
+           '            <Point X="0.004" Y="0.004" Z="0.030"/>\n'
+           '            <Point X="0.026" Y="0.026" Z="0.056"/>\n'
+           "          </Window>\n        </Windows>\n"
+           "      </ParticlePosition>\n"
+           '      <InitialVelocity Mode="Random">\n'
+           '        <Translational Amplitude="0.2"/>\n'
            '        <Angular Amplitude="0."/>\n'
            "      </InitialVelocity>\n"
            "    </ParticleInsertion>\n"
@@ -141,3 +181,23 @@ def test_type_b200_under_reference_driver_matches_standard(tmp_path, lib):
             nmem += 1
             assert np.allclose(va_, mb[partner], rtol=1e-7, atol=1e-15), (pid, partner)
     assert nmem > 0
+
+
+@pytest.mark.skipif(not EXE.exists(), reason="oracle/_ref/grains_b200 was not built")
+def test_type_b200_insertion_over_time_matches_standard(tmp_path, lib):
+    std = _input_overtime(tmp_path / "std", "Standard")
+    b200 = _input_overtime(tmp_path / "b200", "B200")
+    _run(std)
+    _run(b200)
+    sd, bd = std.parent, b200.parent
+    ra = sorted(sd.glob("res*_Particles.result"), key=lambda p: p.stat().st_mtime)[-1]
+    pa, pb = _reload_particles(ra), _reload_particles(bd / ra.name)
+    # the same particles inserted, at the same places
+    assert pa.keys() == pb.keys() and len(pa) > 40, (len(pa), len(pb))
+    for pid, (xa, ma) in pa.items():
+        xb, mb = pb[pid]
+        assert np.abs(xa - xb).max() <= 1e-12, pid
+        assert ma.keys() == mb.keys(), pid
+    for name in ("coordinationNumber", "particleType"):
+        assert (sd / f"raw_{name}.dat").read_text().split() == \
+            (bd / f"raw_{name}.dat").read_text().split(), name
