@@ -553,14 +553,16 @@ template <bool kConvex>
 __global__ void __launch_bounds__(128) k_pairlaw32(DevState S) {
   pdlWait();      // the contact filter's lists
   pdlTrigger();   // the leapfrog kernel may start; its candidates wait for this kernel
-  const int nk = S.ctl[kCtlKept], nw = S.ctl[kCtlWork];
+  const int nh = S.ctl[kCtlKept], nc = S.ctl[kCtlKeptCold], nw = S.ctl[kCtlWork];
+  const int nk = nh + nc;
   const int tag = S.ctl[kCtlEpoch];
   const int stride = gridDim.x * blockDim.x;
   int nlaw = 0, nre = 0;   // contacts evaluated / re-evaluated in FP64
   GjkTally gjk;
   StatsTally st;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nk + nw; i += stride) {
-    if (i < nk) pairItem32<kConvex>(S, S.kept[i], tag, nlaw, nre, gjk, st);
+    if (i < nh) pairItem32<kConvex>(S, S.kept[i], tag, nlaw, nre, gjk, st);
+    else if (i < nk) pairItem32<kConvex>(S, S.kept[S.pair_cap / 2 - (i - nh)], tag, nlaw, nre, gjk, st);
     else wallsOf32<kConvex>(S, S.work[i - nk], tag, nlaw, nre, gjk, st);
   }
   // warp-aggregated counters (every lane of the warp reaches this point)

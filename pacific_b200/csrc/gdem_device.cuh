@@ -147,7 +147,11 @@ struct DevState {
   double* hydro;          // coupled runs: hydrodynamic force and torque by particle ID (6 each), or null
   int2* upairs;           // compact pair list: (slot, entry) of every upper entry, ctl[kCtlPairs] of them
   int* epos;              // per compact pair: position of the pair in its two rows, e_t | e_u << 16
-  int* kept;              // compact-list indices of the pairs kept by the filter, ctl[kCtlKept]
+  // compact-list indices of the pairs kept by the filter: ctl[kCtlKept] from
+  // the front and, in FP32-split with non-spherical classes, the pairs not in
+  // contact at the last evaluation, ctl[kCtlKeptCold], from slot pair_cap / 2
+  // downwards
+  int* kept;
   // per list entry: this evaluation's force and torque on the row's particle
   // from that pair (written by the pair kernel for a contact, tagged with the
   // evaluation counter), summed in row order by the leapfrog kernel

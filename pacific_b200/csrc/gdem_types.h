@@ -36,6 +36,7 @@ enum CtlWords : int {
   kCtlKept = 6,     // pairs kept by this evaluation's contact filter
   kCtlEntries = 7,  // pair-list entries of the last rebuild
   kCtlEntriesMax = 8,  // most entries any rebuild needed since the last allocation check
+  kCtlKeptCold = 9,  // kept pairs not in contact at the last evaluation (listed from the back)
   kCtlWords = 16
 };
 
