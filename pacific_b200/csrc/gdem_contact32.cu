@@ -545,6 +545,86 @@ __device__ __forceinline__ void pairItem32(DevState const& S, int c, int tag, in
   }
 }
 
+// First pass over the kept pairs that were not in contact at the last
+// evaluation (FP32-split with non-spherical classes: the back of the kept
+// list): the bounding-sphere test and the first iteration of the
+// closest-point search (separatedAtFirst), in a kernel without the
+// search's simplex and the force law.  A pair they prove apart ends here
+// with what the pair kernel would have recorded for it -- no contact, its
+// GJK call and the polyhedron vertices its search reached (recordVertex) --
+// and the others are listed in kept2 for the pair kernel, which then runs
+// their full searches in warps of their own instead of beside searches that
+// stop at once.  Pairs of two spheres go to the pair kernel as they are.
+__device__ __forceinline__ bool apartAtFirst(DevState const& S, int c, GjkTally& gjk) {
+  const int cap = S.cap;
+  const int2 pr = S.upairs[c];
+  const int ep = S.epos[c];
+  const int t = pr.x;
+  const unsigned ent = (unsigned)pr.y;
+  const int u = (int)(ent & ((1u << 27) - 1u));
+  const int et = ep & 0xFFFF, eu = (int)((unsigned)ep >> 16);
+  GridDesc const& g = S.grids[S.inst[t]];
+  int sh[3];
+  entryShift(S, ent, t, u, sh);
+  const d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
+  const d3 xt = ld3(S.x, cap, t), xu = ld3(S.x, cap, u);
+  // the orientation and priorities of pairItem32
+  const bool flip = referenceFlip(g, xt, xu, sh);
+  const int a = flip ? u : t, b = flip ? t : u;
+  const int pa = min((flip ? eu : et) + 1, kWallPriority - 1),
+            pb = min((flip ? et : eu) + 1, kWallPriority - 1);
+  TypeDesc const& tp0 = S.types[S.type[a]];
+  TypeDesc const& tp1 = S.types[S.type[b]];
+  if (tp0.shape == 0 && tp1.shape == 0) return false;
+  const d3 x0 = flip ? xu : xt, x1 = flip ? xt + (-shift) : xu + shift;
+  const XForm64 a2w = crustXForm(S.basis, cap, a, tp0.scaling, x0);
+  const XForm64 b2w = crustXForm(S.basis, cap, b, tp1.scaling, x1);
+  // convexContact64's bounding-sphere test, then its search's first
+  // iteration with the same separation margin
+  if (norm(a2w.o - b2w.o) < tp0.radius + tp1.radius) {
+    int c0v = startVertex(S, tp0, a), c1v = startVertex(S, tp1, b);
+    const double sep = (tp0.crust + tp1.crust) * (1. + 1.e-9);
+    if (!separatedAtFirst(convexOf(tp0, S), a2w, convexOf(tp1, S), b2w, c0v, c1v, sep))
+      return false;
+    recordVertex(S, tp0, a, pa, c0v);
+    recordVertex(S, tp1, b, pb, c1v);
+    gjk.add(1);
+  }
+  if (S.diag) {
+    const double inf = __longlong_as_double(0x7ff0000000000000ll);
+    S.pair_delta[(int64_t)S.pair_off[t] + et] = inf;
+    if (eu != 0xFFFF) S.pair_delta[(int64_t)S.pair_off[u] + eu] = inf;
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(128) k_pairsep32(DevState S) {
+  pdlWait();      // the contact filter's lists
+  pdlTrigger();   // the pair kernel may be scheduled; it waits for this one
+  const int nc = S.ctl[kCtlKeptCold];
+  const int* cold = S.kept + S.pair_cap / 2;   // listed downwards
+  const int lane = threadIdx.x & 31;
+  GjkTally gjk;
+  for (int j0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31); j0 < nc;
+       j0 += gridDim.x * blockDim.x) {   // warp-uniform
+    const int j = j0 + lane;
+    int c = 0;
+    bool open = false;
+    if (j < nc) {
+      c = cold[-j];
+      open = !apartAtFirst(S, c, gjk);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, open);
+    if (m) {
+      int base = 0;
+      if (lane == 0) base = atomicAdd(S.ctl + kCtlKept2, __popc(m));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (open) S.kept2[base + __popc(m & ((1u << lane) - 1u))] = c;
+    }
+  }
+  gjk.flush(S.gjk_counts);
+}
+
 // The pair kernel of an evaluation, one thread per item over a persistent
 // grid: first the pairs the contact filter kept, then the particles near a
 // wall.  Its trigger comes after its wait, so the leapfrog kernel, which
@@ -553,8 +633,11 @@ template <bool kConvex>
 __global__ void __launch_bounds__(128) k_pairlaw32(DevState S) {
   pdlWait();      // the contact filter's lists
   pdlTrigger();   // the leapfrog kernel may start; its candidates wait for this kernel
-  const int nh = S.ctl[kCtlKept], nc = S.ctl[kCtlKeptCold], nw = S.ctl[kCtlWork];
-  const int nk = nh + nc;
+  // the pairs in contact at the last evaluation (all kept pairs, without
+  // non-spherical classes), then those k_pairsep32 left undecided, then the
+  // particles near a wall
+  const int nh = S.ctl[kCtlKept], n2 = kConvex ? S.ctl[kCtlKept2] : 0, nw = S.ctl[kCtlWork];
+  const int nk = nh + n2;
   const int tag = S.ctl[kCtlEpoch];
   const int stride = gridDim.x * blockDim.x;
   int nlaw = 0, nre = 0;   // contacts evaluated / re-evaluated in FP64
@@ -562,7 +645,7 @@ __global__ void __launch_bounds__(128) k_pairlaw32(DevState S) {
   StatsTally st;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nk + nw; i += stride) {
     if (i < nh) pairItem32<kConvex>(S, S.kept[i], tag, nlaw, nre, gjk, st);
-    else if (i < nk) pairItem32<kConvex>(S, S.kept[S.pair_cap / 2 - (i - nh)], tag, nlaw, nre, gjk, st);
+    else if (i < nk) pairItem32<kConvex>(S, S.kept2[i - nh], tag, nlaw, nre, gjk, st);
     else wallsOf32<kConvex>(S, S.work[i - nk], tag, nlaw, nre, gjk, st);
   }
   // warp-aggregated counters (every lane of the warp reaches this point)
@@ -581,6 +664,10 @@ void launch_pairs32(DevState const& S, const int* gate, int fill, cudaStream_t s
   if (!S.n) return;
   if (fill) k_pairs_fill32<<<(S.n + 255) / 256, 256, 0, st>>>(S, gate);
   else k_pairs_count32<<<(S.n + 255) / 256, 256, 0, st>>>(S, gate);
+}
+void launch_pairsep32(DevState const& S, cudaStream_t st) {
+  if (!S.n || !S.any_convex) return;
+  launchAfterPrevious(k_pairsep32, 8 * S.nsm, 128, st, S);
 }
 void launch_pairlaw32(DevState const& S, cudaStream_t st) {
   if (!S.n) return;

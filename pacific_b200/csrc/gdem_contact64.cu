@@ -303,15 +303,13 @@ template <bool kConvex>
 __global__ void __launch_bounds__(128) k_pairlaw64(DevState S) {
   pdlWait();      // the contact filter's lists
   pdlTrigger();   // the leapfrog kernel may start; its candidates wait for this kernel
-  const int nh = S.ctl[kCtlKept], nc = S.ctl[kCtlKeptCold], nw = S.ctl[kCtlWork];
-  const int nk = nh + nc;
+  const int nk = S.ctl[kCtlKept], nw = S.ctl[kCtlWork];
   const int tag = S.ctl[kCtlEpoch];
   const int stride = gridDim.x * blockDim.x;
   GjkTally gjk;
   StatsTally st;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nk + nw; i += stride) {
-    if (i < nh) pairItem64<kConvex>(S, S.kept[i], tag, gjk, st);
-    else if (i < nk) pairItem64<kConvex>(S, S.kept[S.pair_cap / 2 - (i - nh)], tag, gjk, st);
+    if (i < nk) pairItem64<kConvex>(S, S.kept[i], tag, gjk, st);
     else wallsOf64<kConvex>(S, S.work[i - nk], tag, gjk, st);
   }
   // (every lane of the warp reaches this point: no thread leaves the loop early)

@@ -152,6 +152,7 @@ struct DevState {
   // contact at the last evaluation, ctl[kCtlKeptCold], from slot pair_cap / 2
   // downwards
   int* kept;
+  int* kept2;             // the cold pairs k_pairsep32 left undecided, ctl[kCtlKept2]
   // per list entry: this evaluation's force and torque on the row's particle
   // from that pair (written by the pair kernel for a contact, tagged with the
   // evaluation counter), summed in row order by the leapfrog kernel

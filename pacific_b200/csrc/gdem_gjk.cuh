@@ -290,4 +290,22 @@ __device__ inline double closestPoints64(ConvexRef const& a, XForm64 const& a2w,
   return dist;
 }
 
+// The first iteration of closestPoints64 alone (its start from the
+// supports in direction 0, then the supports in direction -v and v): true
+// when their lower bound v.w/|v| on the distance of the bodies already
+// exceeds sep, the test that ends the full search there; curA, curB as that
+// search leaves them.  False when it does not, or when the start points
+// coincide (the full search decides those).
+__device__ inline bool separatedAtFirst(ConvexRef const& a, XForm64 const& a2w, ConvexRef const& b,
+                                        XForm64 const& b2w, int& curA, int& curB, double sep) {
+  const d3 v = apply(a2w, support(a, mk(0., 0., 0.), curA)) -
+               apply(b2w, support(b, mk(0., 0., 0.), curB));
+  const double dist = norm(v);
+  if (!(dist > 1.0e-15)) return false;
+  const d3 pl = support(a, tmul(-v, a2w), curA);
+  const d3 ql = support(b, tmul(v, b2w), curB);
+  const d3 w = apply(a2w, pl) - apply(b2w, ql);
+  return dot(v, w) > sep * dist;
+}
+
 }  // namespace gdem

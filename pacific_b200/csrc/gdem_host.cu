@@ -847,7 +847,8 @@ struct System {
     S.pair_scan_tmp = alloc<int>((c + 1023) / 1024 + 1);
     CK(cudaMemset(S.npairs, 0, c * sizeof(int)));
     CK(cudaMemset(S.pair_off, 0, (c + 1) * sizeof(int)));
-    S.pairs = nullptr; S.upairs = nullptr; S.epos = nullptr; S.kept = nullptr; S.share = nullptr;
+    S.pairs = nullptr; S.upairs = nullptr; S.epos = nullptr; S.kept = nullptr; S.kept2 = nullptr;
+    S.share = nullptr;
     S.pair_cap = 0;
     S.pair_delta = nullptr; S.wall_delta = nullptr; S.diag = 0;
     S.pair_force = nullptr; S.wall_force = nullptr;
@@ -899,7 +900,7 @@ struct System {
   void allocatePairs(long long entries) {
     if (entries > (long long)INT_MAX - 64)
       throw std::runtime_error("pair list too large for 32-bit row offsets");
-    for (void* p : {(void*)S.pairs, (void*)S.upairs, (void*)S.epos, (void*)S.kept, S.share,
+    for (void* p : {(void*)S.pairs, (void*)S.upairs, (void*)S.epos, (void*)S.kept, (void*)S.kept2, S.share,
                     (void*)S.pair_delta, (void*)S.pair_force})
       if (p) freeAlloc(p);
     const size_t e = (size_t)entries, pc = e / 2 + 1;
@@ -908,6 +909,8 @@ struct System {
     S.upairs = alloc<int2>(pc);
     S.epos = alloc<int>(pc);
     S.kept = alloc<int>(pc);
+    // the cold pairs' first pass (FP32-split, non-spherical classes)
+    S.kept2 = (precision == GDEM_FP32_SPLIT && S.any_convex) ? alloc<int>(pc) : nullptr;
     const size_t sb = precision == GDEM_FP64 ? 64 : 32;
     S.share = alloc<char>(e * sb);
     // (on the library's stream, which does not synchronise with the legacy
@@ -1024,7 +1027,10 @@ struct System {
     if (diag) timed("diag_prefill", [&] { launch_diag_prefill(S, stream); });
     timed("filter", [&] { launch_filter(S, stream); });
     if (precision == GDEM_FP64) timed("pairlaw64", [&] { launch_pairlaw64(S, stream); });
-    else timed("pairlaw32", [&] { launch_pairlaw32(S, stream); });
+    else {
+      if (S.any_convex) timed("pairsep32", [&] { launch_pairsep32(S, stream); });
+      timed("pairlaw32", [&] { launch_pairlaw32(S, stream); });
+    }
     timed("move", [&] { launch_move(S, flags | kStepSum, precision == GDEM_FP32_SPLIT, stream); });
     if (!prune_memory)
       timed("hist_carry", [&] { launch_hist_carry(S, precision == GDEM_FP64, stream); });

@@ -58,6 +58,7 @@ __global__ void k_decide(DevState S, cudaGraphConditionalHandle h, int use_handl
   S.ctl[kCtlWork] = 0;
   S.ctl[kCtlKept] = 0;
   S.ctl[kCtlKeptCold] = 0;
+  S.ctl[kCtlKept2] = 0;
   S.ctl[kCtlRebuilds] += need ? 1 : 0;
   if (need) S.ctl[kCtlPairs] = 0;
   if (use_handle) cudaGraphSetConditional(h, need ? 1u : 0u);

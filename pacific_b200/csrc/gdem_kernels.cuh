@@ -102,5 +102,7 @@ void launch_append_particle(DevState const& S, NewParticle const& p, cudaStream_
 // gdem_contact32.cu (FP32-split mode)
 void launch_pairs32(DevState const& S, const int* gate, int fill, cudaStream_t st);
 void launch_pairlaw32(DevState const& S, cudaStream_t st);
+// First pass over the cold kept pairs (FP32-split, non-spherical classes).
+void launch_pairsep32(DevState const& S, cudaStream_t st);
 
 }  // namespace gdem

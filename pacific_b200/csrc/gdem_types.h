@@ -37,6 +37,7 @@ enum CtlWords : int {
   kCtlEntries = 7,  // pair-list entries of the last rebuild
   kCtlEntriesMax = 8,  // most entries any rebuild needed since the last allocation check
   kCtlKeptCold = 9,  // kept pairs not in contact at the last evaluation (listed from the back)
+  kCtlKept2 = 10,    // of those, the pairs the first search iteration left undecided (kept2)
   kCtlWords = 16
 };
 
