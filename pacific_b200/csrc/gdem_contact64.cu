@@ -106,6 +106,20 @@ __device__ __forceinline__ bool evalPair64(DevState const& S, GridDesc const& g,
                                            bool& rolling) {
   const int cap = S.cap;
   const unsigned tag = (unsigned)S.ctl[kCtlEpoch], tag_old = tag - 1u;
+  // spheres: the history lookup's first probe (key and values) is read
+  // before the narrow phase -- the key depends on the two IDs only -- so its
+  // loads overlap the narrow phase
+  const unsigned long long hkey = pairKey(min(id0, id1), max(id0, id1));
+  uint32_t hslot = 0;
+  unsigned long long hfirst = 0;
+  double hv[9];
+  if constexpr (!kConvex) {
+    hslot = hashSlot(hkey, S.hist_old.log2cap);
+    hfirst = S.hist_old.keys[hslot];
+    const double* p = static_cast<const double*>(S.hist_old.vals) + 9 * (size_t)hslot;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) hv[k] = p[k];
+  }
   Contact64 ct;
   if (!kConvex || (tp0.shape == 0 && tp1.shape == 0)) {
     ct = sphereSphere64(x0, tp0.radius, tp0.crust, x1, tp1.radius, tp1.crust);
@@ -129,11 +143,22 @@ __device__ __forceinline__ bool evalPair64(DevState const& S, GridDesc const& g,
     // the table holds the lower ID's view; p0 may be the higher ID (the
     // reference's pair orientation), whose view is the negation
     const bool flip = id0 > id1;
-    const unsigned long long key = pairKey(min(id0, id1), max(id0, id1));
-    int old = histFind(S.hist_old, key, tag_old);
+    const unsigned long long key = hkey;
+    int old;
+    if constexpr (!kConvex) {
+      if (hfirst == tagged(key, tag_old)) old = (int)hslot;
+      else if (tagOf(hfirst) != (tag_old & kTagMask)) old = -1;
+      else old = histFindAfter(S.hist_old, key, tag_old, hslot);
+    } else {
+      old = histFind(S.hist_old, key, tag_old);
+    }
     d3 kd, pn, sp;
     if (old >= 0) {
-      loadHist(S.hist_old, old, kd, pn, sp);
+      if (!kConvex && old == (int)hslot) {
+        kd = mk(hv[0], hv[1], hv[2]); pn = mk(hv[3], hv[4], hv[5]); sp = mk(hv[6], hv[7], hv[8]);
+      } else {
+        loadHist(S.hist_old, old, kd, pn, sp);
+      }
       if (flip) { kd = -kd; pn = -pn; sp = -sp; }
     }
     hodc64(m, S.dt, ct.point, ct.overlap, x0, v0, w0, tp0.mass, tp0.eqrad, x1, v1, w1, tp1.mass,
@@ -256,6 +281,7 @@ __device__ __forceinline__ void pairItem64(DevState const& S, int c, int tag, Gj
   entryShift(S, ent, t, u, sh);
   const d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
   const d3 xt = ld3(S.x, cap, t), xu = ld3(S.x, cap, u);
+  const int idt = S.id[t], idu = S.id[u];
   // p0 as in the reference (flip: u is p0, at its own position)
   const bool flip = referenceFlip(g, xt, xu, sh);
   const int a = flip ? u : t, b = flip ? t : u;
@@ -265,7 +291,7 @@ __device__ __forceinline__ void pairItem64(DevState const& S, int c, int tag, Gj
   double dl;
   bool rolling;
   const bool hit = evalPair64<kConvex>(
-      S, g, a, b, pa, pb, S.id[a], S.id[b], S.types[S.type[a]], S.types[S.type[b]],
+      S, g, a, b, pa, pb, flip ? idu : idt, flip ? idt : idu, S.types[S.type[a]], S.types[S.type[b]],
       flip ? xu : xt, flip ? xt + (-shift) : xu + shift, ld3(S.v, cap, a), ld3(S.v, cap, b),
       ld3(S.w, cap, a), ld3(S.w, cap, b), true, gjk, dl, f, c0, c1m, mr, rolling);
   const int64_t rt = (int64_t)S.pair_off[t] + et, ru = (int64_t)S.pair_off[u] + eu;

@@ -66,6 +66,21 @@ __device__ inline int histFind(HistTable const& t, unsigned long long base, unsi
   }
   return -1;
 }
+// histFind after its first probe (slot first, key k0 read there) matched
+// neither the key nor an empty slot: the lookup from the next slot on.
+__device__ inline int histFindAfter(HistTable const& t, unsigned long long base, unsigned tag,
+                                    uint32_t first) {
+  const uint32_t mask = (1u << t.log2cap) - 1;
+  const unsigned long long key = tagged(base, tag);
+  uint32_t s = (first + 1) & mask;
+  for (uint32_t probe = 1; probe <= mask; ++probe) {
+    const unsigned long long k = t.keys[s];
+    if (k == key) return (int)s;
+    if (tagOf(k) != (tag & kTagMask)) return -1;
+    s = (s + 1) & mask;
+  }
+  return -1;
+}
 // Claims a slot for base with tag (one writer per key and evaluation); -1
 // when every slot carries the tag already (table full).
 __device__ inline int histInsert(HistTable const& t, unsigned long long base, unsigned tag) {
