@@ -1115,11 +1115,12 @@ struct System {
     ++parity;
     launch_hist_zero_cumulative(S.hist_old, S.ctl, precision == GDEM_FP64, stream);
     CK(cudaStreamSynchronize(stream));
-    // size the contact filter's grid for the pair list just built (a quarter
-    // more for growth; the kernel loops over any excess)
+    // size the contact filter's grid for the pair list just built: one block
+    // per 2,048 pairs (kFilterPairsPerBlock) and a quarter more for growth
+    // (the kernel loops over any excess)
     int np = 0;
     CK(cudaMemcpy(&np, S.ctl + kCtlPairs, sizeof(int), cudaMemcpyDeviceToHost));
-    S.filter_qblocks = std::max(1, (int)((1.25 * np + 1023.) / 1024.));
+    S.filter_qblocks = std::max(1, (int)((1.25 * np + 2047.) / 2048.));
     invalidateGraphs();
     collectTimes();
     started = true;
@@ -1344,7 +1345,7 @@ int gdem_insert_particle(gdem_handle h, int type, const double* x, const double*
     CK(cudaStreamSynchronize(s->stream));
     // the contact filter's grid, for about 4 pairs per particle (its kernel
     // loops over any excess)
-    S.filter_qblocks = std::max(S.filter_qblocks, (4 * S.n + 1023) / 1024);
+    S.filter_qblocks = std::max(S.filter_qblocks, (4 * S.n + 2047) / 2048);
     s->invalidateGraphs();
     *inserted = 1;
     if (id) *id = p.id;

@@ -445,10 +445,14 @@ __global__ void __launch_bounds__(256, (kFast && kBasis) ? 2 : (kFast ? 4 : 3)) 
 // exactly, and both partners marked as candidates.  With walls, the first
 // pblocks blocks take one particle per thread and list (and mark) those near
 // a wall.  The pairs are taken in chunks of kFilterUnroll rounds of 32 per
-// warp with their loads issued together (a grid-stride loop over chunks: the
-// grid is sized for the pair count at the leapfrog start, the count itself is
-// known on the device only).
-constexpr int kFilterUnroll = 4;
+// warp with their loads issued together, in a grid-stride loop over chunks
+// (the count is known on the device only) on a grid of one block per 2,048
+// pairs at the leapfrog start (kFilterPairsPerBlock; the host resizes it
+// then).  Measured at 1M spheres: one round per chunk and that grid take
+// 21.3 us, four rounds on a grid of one block per 1,024 pairs 27.0 us (the
+// kernel is bound by the latency of its gathers: fewer registers, more warps).
+constexpr int kFilterUnroll = 1;
+constexpr int kFilterPairsPerBlock = 2048;
 
 // Appends idx to list (length *count) for every lane whose pred holds (one
 // atomic per warp); every lane of the warp calls it.
@@ -915,7 +919,7 @@ void launch_filter(DevState const& S, cudaStream_t st) {
   // about 4 pairs per particle until the leapfrog start has counted them
   const int qblocks = S.filter_qblocks > 0
                           ? S.filter_qblocks
-                          : (S.n + 64 * kFilterUnroll - 1) / (64 * kFilterUnroll);
+                          : (4 * S.n + kFilterPairsPerBlock - 1) / kFilterPairsPerBlock;
   k_filter<<<pblocks + qblocks, 256, 0, st>>>(S, pblocks);
 }
 void launch_link(DevState const& S, const int* gate, cudaStream_t st) {
