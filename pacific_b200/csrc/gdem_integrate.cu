@@ -369,9 +369,15 @@ __device__ __forceinline__ void sumShares(DevState const& S, int t, TypeDesc con
   }
 }
 
-// Leapfrog of each particle (FP32-split spheres: four 256-thread blocks per
-// multiprocessor, which measured faster than three or five; the kernel is
-// bound by the latency of its loads).  With kStepSum the force and torque of this
+// Threads per block of k_move.
+template <bool kFast, bool kBasis>
+constexpr int kMoveBlock() { return kBasis ? 256 : 128; }
+
+// Leapfrog of each particle (128-thread blocks: FP32-split spheres eight per
+// multiprocessor at 64 registers, FP64 six at 80; both measured faster at 1M
+// than 256-thread blocks -- three, four or five per multiprocessor for
+// FP32-split, three or four for FP64; the kernel is bound by the latency of
+// its loads).  FP32-split with an orientation matrix: two 256-thread blocks.  With kStepSum the force and torque of this
 // evaluation: the weight for a particle the contact filter did not mark as a
 // candidate, else the weight plus its shares (sumShares); without it, the
 // stored F, T (the opening kick of a call continues from the last evaluation
@@ -388,7 +394,8 @@ __device__ __forceinline__ void sumShares(DevState const& S, int t, TypeDesc con
 // takes no share and is not read by the pair kernel, so its leapfrog runs at
 // once; a candidate waits for the pair kernel before it reads its shares.
 template <bool kFast, bool kBasis>
-__global__ void __launch_bounds__(256, (kFast && kBasis) ? 2 : (kFast ? 4 : 3)) k_move(DevState S, int flags) {
+__global__ void __launch_bounds__(kMoveBlock<kFast, kBasis>(), (kFast && kBasis) ? 2 : (kFast ? 8 : 6))
+    k_move(DevState S, int flags) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= S.n) return;
   TypeDesc const& tp = S.types[S.type[t]];
@@ -946,9 +953,9 @@ void launch_move(DevState const& S, int flags, int fast, cudaStream_t st) {
   M.x2 = S.x; M.v2 = S.v; M.w2 = S.w; M.wbf2 = S.wbf; M.q2 = S.q; M.basis2 = S.basis;
   M.wrap2 = S.wrap;
   const int nb = blocks(S.n, 256);
-  if (!fast) launchAfterPrevious(k_move<false, false>, nb, 256, st, M, flags);   // basis tested at run time
+  if (!fast) launchAfterPrevious(k_move<false, false>, blocks(S.n, kMoveBlock<false, false>()), kMoveBlock<false, false>(), st, M, flags);   // basis tested at run time
   else if (S.basis) launchAfterPrevious(k_move<true, true>, nb, 256, st, M, flags);
-  else launchAfterPrevious(k_move<true, false>, nb, 256, st, M, flags);
+  else launchAfterPrevious(k_move<true, false>, blocks(S.n, kMoveBlock<true, false>()), kMoveBlock<true, false>(), st, M, flags);
 }
 void launch_append_particle(DevState const& S, NewParticle const& p, cudaStream_t st) {
   k_append_particle<<<1, 32, 0, st>>>(S, p);
