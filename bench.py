@@ -563,7 +563,11 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
             "n_gpus": world, "steps": k, "warmup": 1 + w, "ms_per_step": 1e3 * dt / k,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": "periodic_gas_1M", "n": sc.n},
+            "data": "synthetic",
+            "config": {"workload": "periodic_gas_1M", "n": sc.n, "steps_config": 2000,
+                       "dt": sc.dt, "phi": scenarios.solid_fraction(sc),
+                       "parallelism": f"replicas{world}",
+                       "l2": "inputs larger than L2 (~0.5 GB of state per replica)"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": kind,
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
