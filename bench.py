@@ -131,11 +131,11 @@ def algorithmic_bytes(kernel, n, entries, contacts, ncells, fp64):
         return contacts * (4 + 8 + 4 + 2 * (4 + 4 + 4 + 24 + 2 * vel + 4) + 2 * hist
                            + 2 * share + 2 * 4)
     if kernel == "move":
-        # state type inst disp wrap flags | state disp wrap posf flags, and
+        # state type inst posf0 wrap flags | state wrap posf flags, and
         # for a particle in contact its row offset and length, the first
         # word of each share of its row and the rest of each share in use
         rowlen = entries / max(n, 1)
-        return int(n * (state + 8 + 12 + 4 + 4 + state + 12 + 4 + 16 + 4)
+        return int(n * (state + 8 + 16 + 4 + 4 + state + 4 + 16 + 4)
                    + touched * (8 + rowlen * 16) + 2 * contacts * (share - 16))
     if kernel == "bin":          # x inst | skey rank; cell-count RMW
         return n * (24 + 4 + 8 + 8)
@@ -147,8 +147,8 @@ def algorithmic_bytes(kernel, n, entries, contacts, ncells, fp64):
         return ncells * 8 + n * 8
     if kernel == "permute":      # order skey ids state F T | ids state F T cellc + pos / offset
         return n * (4 + 4 + 12 + 2 * (state + 48) + 16 + (32 if fp64 else 16))
-    if kernel == "copyback":     # ids state F T | ids state F T disp wrap
-        return n * (12 + 2 * (state + 48) + 12 + 12 + 4)
+    if kernel == "copyback":     # ids state F T | ids state F T wrap posf posf0
+        return n * (12 + 2 * (state + 48) + 12 + 4 + 32)
     if kernel in ("pairs_count64", "pairs_count32"):   # cellc + own position | row length
         return n * (16 + (32 if fp64 else 16) + 4) + 4 * ncells
     if kernel == "row_scan":     # row lengths | row offsets

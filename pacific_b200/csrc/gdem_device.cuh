@@ -137,9 +137,10 @@ struct DevState {
   int* id2; int* type2; int* inst2;
   double* x2; double* v2; double* w2; double* wbf2; double* q2; double* basis2;
   double* F2; double* T2;
-  // pair-list validity: displacement since the last rebuild (FP32, SoA) and
-  // periodic wraps since then (signed bytes x, y, z)
-  float* disp; int* wrap; int* wrap2;
+  // pair-list validity: the FP32 position at the last rebuild (the posf
+  // value written then; displacement = posf - posf0) and the periodic wraps
+  // since then (signed bytes x, y, z)
+  float4* posf0; int* wrap; int* wrap2;
   int* ctl;               // control words (CtlWords)
   // binning
   int* skey;              // cell key in the old order

@@ -816,7 +816,7 @@ struct System {
     S.wbf2 = alloc<double>(3 * c); S.q2 = alloc<double>(4 * c);
     S.F = alloc<double>(3 * c); S.T = alloc<double>(3 * c);
     S.F2 = alloc<double>(3 * c); S.T2 = alloc<double>(3 * c);
-    S.disp = alloc<float>(3 * c); S.wrap = alloc<int>(c); S.wrap2 = alloc<int>(c);
+    S.posf0 = alloc<float4>(c); S.wrap = alloc<int>(c); S.wrap2 = alloc<int>(c);
     S.ctl = alloc<int>(kCtlWords);
     CK(cudaMemset(S.ctl, 0, kCtlWords * sizeof(int)));
     epoch = 0;

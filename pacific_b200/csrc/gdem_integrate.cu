@@ -241,8 +241,8 @@ __global__ void k_permute(DevState S, const int* gate) {
   }
 }
 
-// Second buffers back into the current ones; the displacement and the wraps
-// since the rebuild start again from zero.
+// Second buffers back into the current ones; the wraps since the rebuild
+// start again from zero and the FP32 position becomes the rebuild's.
 __global__ void k_copyback(DevState S, const int* gate) {
   if (gatedOff(gate)) return;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -255,7 +255,6 @@ __global__ void k_copyback(DevState S, const int* gate) {
     S.x[k] = S.x2[k]; S.v[k] = S.v2[k]; S.w[k] = S.w2[k];
     if (S.wbf_state) S.wbf[k] = S.wbf2[k];
     S.F[k] = S.F2[k]; S.T[k] = S.T2[k];
-    S.disp[k] = 0.f;
   }
 #pragma unroll
   for (int k = 0; k < 4; ++k) S.q[k * cap + t] = S.q2[k * cap + t];
@@ -266,8 +265,10 @@ __global__ void k_copyback(DevState S, const int* gate) {
   if (S.curv) S.curv[t] = S.curv2[t];
   S.wrap[t] = 0;
   const d3 x = ld3(S.x, cap, t);
-  S.posf[t] = make_float4((float)x.x, (float)x.y, (float)x.z,
-                          (float)S.types[S.type[t]].radius);
+  const float4 p = make_float4((float)x.x, (float)x.y, (float)x.z,
+                               (float)S.types[S.type[t]].radius);
+  S.posf[t] = p;
+  S.posf0[t] = p;
 }
 
 // Force and torque of particle t in this evaluation: its weight plus the
@@ -773,7 +774,6 @@ __global__ void k_append_particle(DevState S, NewParticle p) {
   st3(S.wbf, cap, i, multToVector3(conj(qq), vecq(w, qq)));
   st3(S.F, cap, i, mk(tp.weight[0], tp.weight[1], tp.weight[2]));
   st3(S.T, cap, i, mk(0., 0., 0.));
-  S.disp[i] = 0.f; S.disp[cap + i] = 0.f; S.disp[2 * cap + i] = 0.f;
   S.wrap[i] = 0;
   if (S.curv) {
     S.curv[i] = tp.poly_start;
@@ -781,7 +781,9 @@ __global__ void k_append_particle(DevState S, NewParticle p) {
   }
   S.nact[i] = 0;
   S.nact[cap + i] = 0;
-  S.posf[i] = make_float4((float)x.x, (float)x.y, (float)x.z, (float)tp.radius);
+  const float4 pf = make_float4((float)x.x, (float)x.y, (float)x.z, (float)tp.radius);
+  S.posf[i] = pf;
+  S.posf0[i] = pf;
 }
 
 // Loads host-layout state (AoS, by particle ID, staged in device memory)
@@ -813,7 +815,8 @@ __global__ void k_load_state(DevState S, const double* x, const double* v, const
 #pragma unroll
     for (int k = 0; k < 9; ++k) S.basis[k * cap + i] = m[k];
   }
-  S.disp[i] = 0.f; S.disp[cap + i] = 0.f; S.disp[2 * cap + i] = 0.f;
+  // the host requests a pair-list rebuild after a load, which sets posf and
+  // posf0 from these positions
   S.wrap[i] = 0;
   // a new (or reloaded) polyhedron starts its support search where
   // Polyhedron::BuildPolyhedron leaves it

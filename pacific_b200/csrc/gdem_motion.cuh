@@ -261,7 +261,7 @@ struct MoveIn {
   dq q;
   double bas[9];
   int wrap;
-  float3 disp;
+  float4 p0;   // FP32 position at the last rebuild
 };
 template <bool kFast, bool kBasis>
 __device__ __forceinline__ void loadMoveIn(DevState const& S, int t, MoveIn& m) {
@@ -280,12 +280,12 @@ __device__ __forceinline__ void loadMoveIn(DevState const& S, int t, MoveIn& m) 
     for (int k = 0; k < 9; ++k) m.bas[k] = S.basis[k * cap + t];
   }
   m.wrap = S.wrap[t];
-  m.disp = make_float3(S.disp[t], S.disp[cap + t], S.disp[2 * cap + t]);
+  m.p0 = S.posf0[t];
 }
 
 // Moves particle t (state m, F, T as given) and writes the result to the
-// second buffers; updates the pair-list displacement and wraps and flags a
-// rebuild when the particle has moved more than half the skin.  close/move
+// second buffers; updates the wraps and the FP32 position and flags a
+// pair-list rebuild when the particle has moved half the skin or more.  close/move
 // select the kicks as in leapfrog().
 template <bool kFast, bool kBasis>
 __device__ __forceinline__ void advanceParticle(DevState const& S, int t, TypeDesc const& tp,
@@ -317,11 +317,6 @@ __device__ __forceinline__ void advanceParticle(DevState const& S, int t, TypeDe
 #pragma unroll
     for (int d = 0; d < 3; ++d)
       if (wd[d]) wr = wrapSet(wr, d, wrapGet(wr, d) + wd[d]);
-    float3 ds = make_float3(m.disp.x + (float)dx.x, m.disp.y + (float)dx.y,
-                            m.disp.z + (float)dx.z);
-    S.disp[t] = ds.x; S.disp[cap + t] = ds.y; S.disp[2 * cap + t] = ds.z;
-    const float half = 0.5f * S.bgrids[S.inst[t]].skin_f;
-    if (ds.x * ds.x + ds.y * ds.y + ds.z * ds.z > half * half) S.ctl[kCtlNeed] = 1;
   }
   st3(S.x2, cap, t, x); st3(S.v2, cap, t, v); st3(S.w2, cap, t, w);
   if (!kSphereW) st3(S.wbf2, cap, t, wbf);
@@ -336,9 +331,22 @@ __device__ __forceinline__ void advanceParticle(DevState const& S, int t, TypeDe
   // recorded in a list entry at the rebuild stays valid
   // (in FP32: its rounding is covered by the filter's margin)
   GridDesc const& bg = S.bgrids[S.inst[t]];
-  S.posf[t] = make_float4((float)x.x + (float)wrapGet(wr, 0) * bg.Lf[0],
-                          (float)x.y + (float)wrapGet(wr, 1) * bg.Lf[1],
-                          (float)x.z + (float)wrapGet(wr, 2) * bg.Lf[2], (float)tp.radius);
+  const float4 pf = make_float4((float)x.x + (float)wrapGet(wr, 0) * bg.Lf[0],
+                                (float)x.y + (float)wrapGet(wr, 1) * bg.Lf[1],
+                                (float)x.z + (float)wrapGet(wr, 2) * bg.Lf[2], (float)tp.radius);
+  S.posf[t] = pf;
+  if (move) {
+    // displacement since the rebuild as the difference of the two FP32
+    // positions; each coordinate of either carries at most three roundings
+    // of its own magnitude (the conversion, the wrap product, the sum), so
+    // half the skin less 2.4e-7 times the summed magnitudes still bounds
+    // the exact FP64 displacement
+    const float ex = pf.x - m.p0.x, ey = pf.y - m.p0.y, ez = pf.z - m.p0.z;
+    const float tol = 2.4e-7f * (fabsf(pf.x) + fabsf(pf.y) + fabsf(pf.z) + fabsf(m.p0.x) +
+                                 fabsf(m.p0.y) + fabsf(m.p0.z));
+    const float half = fmaxf(0.5f * bg.skin_f - tol, 0.f);
+    if (ex * ex + ey * ey + ez * ez >= half * half) S.ctl[kCtlNeed] = 1;
+  }
 }
 
 // Image shift (in periods) of list entry ent (partner u) of slot t: the
