@@ -531,19 +531,36 @@ __device__ __forceinline__ void pairItem32(DevState const& S, int c, int tag, in
   const d3 shift = mk(sh[0] * g.L[0], sh[1] * g.L[1], sh[2] * g.L[2]);
   const d3 xt = ld3(S.x, cap, t), xu = ld3(S.x, cap, u);
   const int idt = S.id[t], idu = S.id[u];
+  // the rest of both particles' inputs and their row offsets load with the
+  // positions (the stores of the history update would otherwise hold the
+  // later loads back); a pair of non-spherical bodies loads its velocities
+  // after the closest-point search, which keeps them out of its registers
+  const int tyt = S.type[t], tyu = S.type[u];
+  const int offt = S.pair_off[t], offu = S.pair_off[u];
+  d3 vt, vu, wt, wu;
+  if constexpr (!kConvex) {
+    vt = ld3(S.v, cap, t); vu = ld3(S.v, cap, u);
+    wt = ld3(S.w, cap, t); wu = ld3(S.w, cap, u);
+  }
   // p0 as in the reference (flip: u is p0, at its own position)
   const bool flip = referenceFlip(g, xt, xu, sh);
   const int a = flip ? u : t, b = flip ? t : u;
+  if constexpr (kConvex) {
+    vt = ld3(S.v, cap, a); vu = ld3(S.v, cap, b);
+    wt = ld3(S.w, cap, a); wu = ld3(S.w, cap, b);
+  } else if (flip) {
+    const d3 sv = vt, sw = wt;
+    vt = vu; vu = sv; wt = wu; wu = sw;
+  }
   const int pa = min((flip ? eu : et) + 1, kWallPriority - 1),
             pb = min((flip ? et : eu) + 1, kWallPriority - 1);
   float3 f, c0, c1, mr;
   double dl;
   bool rolling;
   const bool hit = evalPair32<kConvex>(
-      S, g, a, b, pa, pb, flip ? idu : idt, flip ? idt : idu, S.types[S.type[a]], S.types[S.type[b]],
-      flip ? xu : xt, flip ? xt + (-shift) : xu + shift, ld3(S.v, cap, a), ld3(S.v, cap, b),
-      ld3(S.w, cap, a), ld3(S.w, cap, b), true, nlaw, nre, gjk, dl, f, c0, c1, mr, rolling);
-  const int64_t rt = (int64_t)S.pair_off[t] + et, ru = (int64_t)S.pair_off[u] + eu;
+      S, g, a, b, pa, pb, flip ? idu : idt, flip ? idt : idu, S.types[flip ? tyu : tyt], S.types[flip ? tyt : tyu],
+      flip ? xu : xt, flip ? xt + (-shift) : xu + shift, vt, vu, wt, wu, true, nlaw, nre, gjk, dl, f, c0, c1, mr, rolling);
+  const int64_t rt = (int64_t)offt + et, ru = (int64_t)offu + eu;
   // force on t (the lower ID) and the two torques
   const float3 mt = rolling ? mr : f3(0.f, 0.f, 0.f);
   const float3 ft = flip ? -f : f;
